@@ -1,0 +1,90 @@
+"""ctypes binding of the in-tree C-ABI library ``libdgfs_sm100.so``.
+
+The library is built in place by ``dgfs1d_gpu_b200.build.build()`` (nvcc,
+sm_100a).  There is no fallback: if the library is missing or a call fails,
+the error is raised.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, 'libdgfs_sm100.so')
+
+DGFS_OK = 0
+DGFS_F32, DGFS_F64 = 0, 1
+DGFS_PREC_FP64, DGFS_PREC_FP32 = 0, 1
+
+_c_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class VhsDesc(ctypes.Structure):
+    """Mirror of ``dgfs_vhs_desc`` (include/dgfs_sm100.h)."""
+    _fields_ = [
+        ('N', ctypes.c_int32), ('Nrho', ctypes.c_int32), ('M', ctypes.c_int32),
+        ('L', ctypes.c_double),
+        ('qz', _c_dp), ('qw', _c_dp), ('sz', _c_dp),
+        ('sw', ctypes.c_double), ('sphere_factor', ctypes.c_double),
+        ('gamma', ctypes.c_double), ('prefac', ctypes.c_double),
+        ('sinc_eps', ctypes.c_double), ('cw', ctypes.c_double),
+        ('c0', _c_dp),
+        ('precision', ctypes.c_int32), ('max_evals', ctypes.c_int32),
+    ]
+
+
+class DgfsError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f'dgfs_sm100 error {code}: {msg}')
+        self.code = code
+
+
+_lib = None
+
+# (name, restype, argtypes) of every exported entry point
+_SIGNATURES = [
+    ('dgfs_version', ctypes.c_char_p, []),
+    ('dgfs_last_error_string', ctypes.c_char_p, []),
+    ('dgfs_vhs_create', ctypes.c_int,
+     [ctypes.POINTER(VhsDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    ('dgfs_vhs_eval', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
+    ('dgfs_vhs_fs', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_void_p]),
+    ('dgfs_vhs_last_moments', ctypes.c_void_p, [ctypes.c_void_p]),
+    ('dgfs_vhs_destroy', ctypes.c_int, [ctypes.c_void_p]),
+]
+
+
+def lib():
+    """Load the library (once) and declare the signatures."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise ImportError(
+                f'{LIBPATH} is missing: build it with '
+                '`python -m dgfs1d_gpu_b200.build` (nvcc, sm_100a)')
+        L = ctypes.CDLL(LIBPATH)
+        for name, res, args in _SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    """Raise DgfsError for a non-zero status."""
+    if rc != DGFS_OK:
+        msg = lib().dgfs_last_error_string()
+        raise DgfsError(rc, msg.decode() if msg else '')
+    return rc
+
+
+def exported_symbols():
+    """Names of every entry point the binding declares."""
+    return [s[0] for s in _SIGNATURES]

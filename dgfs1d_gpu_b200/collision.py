@@ -1,0 +1,103 @@
+"""Host handles of the native fast-spectral collision operators.
+
+Thin owners of the C-ABI handles in ``libdgfs_sm100.so``; arrays are torch
+CUDA tensors (or anything exposing ``data_ptr()``), passed by pointer.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as nat
+
+_DT = {torch.float32: nat.DGFS_F32, torch.float64: nat.DGFS_F64}
+_PREC = {'fp64': nat.DGFS_PREC_FP64, 'fp32': nat.DGFS_PREC_FP32}
+
+
+def _dptr(a):
+    return ctypes.cast(a.ctypes.data, ctypes.POINTER(ctypes.c_double))
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def _check_dist(t, name):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f'{name} must be a CUDA tensor')
+    if t.dtype not in _DT:
+        raise TypeError(f'{name} must be float32 or float64')
+    if not t.is_contiguous():
+        raise ValueError(f'{name} must be contiguous')
+
+
+class VHSOperator:
+    """Batched single-species VHS Q(f,f) (``vhs-gll``).
+
+    precision: 'fp64' (all FP64, reference parity) or 'fp32' (FP32 3-D FFTs
+    on f - M with the local Maxwellian M in FP64).
+    """
+
+    def __init__(self, N, L, qz, qw, sz, sw, sphere_factor, gamma, prefac,
+                 cw, c0, precision='fp64', max_evals=64, sinc_eps=1e-15):
+        if precision not in _PREC:
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        self.N, self.n = int(N), int(N) ** 3
+        self.precision = precision
+        self.prefac = float(prefac)
+        self.max_evals = int(max_evals)
+        self._keep = [np.ascontiguousarray(x, dtype=np.float64)
+                      for x in (qz, qw, np.asarray(sz).reshape(-1), c0)]
+        qz_, qw_, sz_, c0_ = self._keep
+        d = nat.VhsDesc()
+        d.N, d.Nrho, d.M = self.N, len(qz_), len(sz_) // 3
+        d.L = float(L)
+        d.qz, d.qw, d.sz, d.c0 = _dptr(qz_), _dptr(qw_), _dptr(sz_), _dptr(c0_)
+        d.sw, d.sphere_factor = float(sw), float(sphere_factor)
+        d.gamma, d.prefac, d.sinc_eps = float(gamma), float(prefac), float(sinc_eps)
+        d.cw = float(cw)
+        d.precision = _PREC[precision]
+        d.max_evals = self.max_evals
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().dgfs_vhs_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        self.Nrho, self.M = d.Nrho, d.M
+
+    def eval(self, f, Q, src=None, dst=None, src_base=0, dst_base=0,
+             nevals=None, stream=None):
+        """Q[dst(i)] += Q(f[src(i)]) for i < nevals (slot-major arrays)."""
+        _check_dist(f, 'f')
+        _check_dist(Q, 'Q')
+        nf, nq = f.numel() // self.n, Q.numel() // self.n
+        if f.numel() % self.n or Q.numel() % self.n:
+            raise ValueError('array sizes must be multiples of N^3')
+        if nevals is None:
+            nevals = len(src) if src is not None else nf - src_base
+        for sl, base, cnt, name in ((src, src_base, nf, 'src'),
+                                    (dst, dst_base, nq, 'dst')):
+            if sl is None:
+                if base < 0 or base + nevals > cnt:
+                    raise IndexError(f'{name} slots out of range')
+            else:
+                if sl.dtype != torch.int32 or not sl.is_cuda or len(sl) < nevals:
+                    raise TypeError(f'{name} must be a CUDA int32 tensor of '
+                                    f'length >= nevals')
+        nat.check(nat.lib().dgfs_vhs_eval(
+            self._h, ctypes.c_void_p(f.data_ptr()), _DT[f.dtype],
+            ctypes.c_void_p(Q.data_ptr()), _DT[Q.dtype],
+            ctypes.c_void_p(src.data_ptr() if src is not None else 0), int(src_base),
+            ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
+            int(nevals), _stream_ptr(stream)))
+
+    def close(self):
+        if getattr(self, '_h', None):
+            nat.lib().dgfs_vhs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,437 @@
+// C ABI of the sm_100a DGFS collision operators (single translation unit).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dgfs_sm100.h"
+#include "fft_reg.cuh"
+#include "cluster_slab.cuh"
+#include "vhs_kernels.cuh"
+
+using namespace dgfs;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define DGFS_CUDA(call)                                                      \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      return fail(DGFS_ERR_CUDA, std::string(#call) + ": " +                 \
+                                     cudaGetErrorString(e_));                \
+  } while (0)
+
+extern "C" const char* dgfs_last_error_string(void) { return g_err.c_str(); }
+extern "C" const char* dgfs_version(void) { return "dgfs_sm100 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------------------
+// twiddle tables (uploaded once per device)
+// ---------------------------------------------------------------------------
+static std::mutex g_tw_mu;
+static bool g_tw_done[64];
+
+static int ensure_twiddles() {
+  int dev = 0;
+  DGFS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(DGFS_ERR_INVALID, "device id out of range");
+  std::lock_guard<std::mutex> lk(g_tw_mu);
+  if (g_tw_done[dev]) return DGFS_OK;
+  std::vector<double2> t64(kTwTotal);
+  std::vector<float2> t32(kTwTotal);
+  for (int i = 0; i < kNumTw; ++i) {
+    const int nt = tw_size(i), off = tw_offset(nt);
+    for (int k = 0; k < nt; ++k) {
+      // exp(-2 pi i k / nt), argument reduced to the first half-turn
+      const long double ang = 2.0L * 3.141592653589793238462643383279502884L *
+                              (long double)k / (long double)nt;
+      const double c = (double)std::cos(ang), s = -(double)std::sin(ang);
+      t64[off + k] = make_double2(c, s);
+      t32[off + k] = make_float2((float)c, (float)s);
+    }
+  }
+  DGFS_CUDA(cudaMemcpyToSymbol(c_tw64, t64.data(), sizeof(double2) * kTwTotal));
+  DGFS_CUDA(cudaMemcpyToSymbol(c_tw32, t32.data(), sizeof(float2) * kTwTotal));
+  g_tw_done[dev] = true;
+  return DGFS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// cluster launch helper
+// ---------------------------------------------------------------------------
+template <typename K, typename A>
+static int launch_cluster(K kernel, dim3 grid, dim3 block, int cluster,
+                          size_t smem, cudaStream_t st, const A& args) {
+  DGFS_CUDA(cudaFuncSetAttribute(kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  if (cluster > 8)
+    DGFS_CUDA(cudaFuncSetAttribute(
+        kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  DGFS_CUDA(cudaLaunchKernelEx(&cfg, kernel, args));
+  return DGFS_OK;
+}
+
+template <typename K, typename A>
+static int launch_plain(K kernel, dim3 grid, dim3 block, size_t smem,
+                        cudaStream_t st, const A& args) {
+  if (smem > 48 * 1024)
+    DGFS_CUDA(cudaFuncSetAttribute(
+        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kernel<<<grid, block, smem, st>>>(args);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// VHS handle
+// ---------------------------------------------------------------------------
+struct dgfs_vhs_s {
+  int N = 0, Nrho = 0, M = 0, Mu = 0, n = 0;
+  int precision = DGFS_PREC_FP64;
+  int max_evals = 0;
+  double prefac = 0, cw = 0;
+  int device = 0;
+  // constant tables
+  double* c0 = nullptr;      // [N]
+  double* b2 = nullptr;      // [n]
+  double* b1w64 = nullptr;   // [Nrho][n]
+  float* b1w32 = nullptr;    // [Nrho][n] (FP32 mode)
+  void* ph = nullptr;        // [Nrho][Mu][3][N] precision R
+  double* kappa = nullptr;   // [Nrho][Mu][3]
+  float* mult = nullptr;     // [Mu]
+  // scratch
+  void* Fg = nullptr;        // [E][n] complex R
+  void* H = nullptr;         // [E][Nrho][n] complex R
+  double* ReLf = nullptr;    // [E][n]
+  double2* mhat = nullptr;   // [E][3][N]
+  double* moments = nullptr; // [E][5]
+  void* uv = nullptr;        // [E][Nrho][Mu][2][3][N] R
+  double2* hh = nullptr;     // [E][Nrho][Mu][3][N]
+  double2* GM = nullptr;     // [E][n]
+};
+
+// FP64-kernel and FP32-terms cluster sizes per N (shared memory per CTA
+// must hold three padded slabs of N^3/C complex elements).
+static int c64_of(int N) {
+  switch (N) {
+    case 8: return 1;
+    case 16: return 2;
+    case 32: return 8;
+    default: return 0;
+  }
+}
+static int c32_of(int N) {
+  switch (N) {
+    case 8: return 1;
+    case 16: return 1;
+    case 32: return 4;
+    default: return 0;
+  }
+}
+
+static size_t slab_bytes(int N, int C, size_t elem) {
+  return (size_t)(N / C) * N * (N + 1) * elem;
+}
+
+static void free_handle(dgfs_vhs_s* h) {
+  void* ptrs[] = {h->c0, h->b2, h->b1w64, h->b1w32, h->ph, h->kappa, h->mult,
+                  h->Fg, h->H, h->ReLf, h->mhat, h->moments, h->uv, h->hh,
+                  h->GM};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete h;
+}
+
+template <typename T>
+static int upload(T** dst, const std::vector<T>& v) {
+  DGFS_CUDA(cudaMalloc((void**)dst, sizeof(T) * v.size()));
+  DGFS_CUDA(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(),
+                       cudaMemcpyHostToDevice));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_create(const dgfs_vhs_desc* d, dgfs_vhs_handle* out) {
+  if (!d || !out) return fail(DGFS_ERR_INVALID, "null descriptor or handle");
+  *out = nullptr;
+  if (d->N <= 0 || d->Nrho <= 0 || d->M <= 0 || d->max_evals <= 0)
+    return fail(DGFS_ERR_INVALID, "N, Nrho, M and max_evals must be positive");
+  if (!d->qz || !d->qw || !d->sz || !d->c0)
+    return fail(DGFS_ERR_INVALID, "qz, qw, sz and c0 are required");
+  if (d->precision != DGFS_PREC_FP64 && d->precision != DGFS_PREC_FP32)
+    return fail(DGFS_ERR_INVALID, "unknown precision");
+  if (c64_of(d->N) == 0 || c32_of(d->N) == 0)
+    return fail(DGFS_ERR_UNSUPPORTED,
+                "velocity grid N=" + std::to_string(d->N) +
+                    " is not compiled in (supported: 8, 16, 32)");
+  if (int rc = ensure_twiddles()) return rc;
+
+  const int N = d->N, n = N * N * N, Nrho = d->Nrho, M = d->M;
+  const bool fp32 = d->precision == DGFS_PREC_FP32;
+
+  // unique directions: merge exact antipodal pairs (identical h, weight 2)
+  std::vector<int> uq;
+  std::vector<float> mult;
+  std::vector<char> used(M, 0);
+  for (int q = 0; q < M; ++q) {
+    if (used[q]) continue;
+    used[q] = 1;
+    float m = 1.f;
+    for (int r = q + 1; r < M; ++r) {
+      if (!used[r] && d->sz[3 * r] == -d->sz[3 * q] &&
+          d->sz[3 * r + 1] == -d->sz[3 * q + 1] &&
+          d->sz[3 * r + 2] == -d->sz[3 * q + 2]) {
+        used[r] = 1;
+        m = 2.f;
+        break;
+      }
+    }
+    uq.push_back(q);
+    mult.push_back(m);
+  }
+  const int Mu = (int)uq.size();
+
+  auto* h = new dgfs_vhs_s();
+  h->N = N; h->n = n; h->Nrho = Nrho; h->M = M; h->Mu = Mu;
+  h->precision = d->precision;
+  h->max_evals = d->max_evals;
+  h->prefac = d->prefac;
+  h->cw = d->cw;
+  cudaGetDevice(&h->device);
+
+  // l-vectors in FFT order, x slowest (std/scattering.py:116-128)
+  std::vector<double> l0(N);
+  for (int i = 0; i < N; ++i) l0[i] = (i < N / 2) ? i : i - N;
+  auto sinc = [&](double s) {
+    return std::sin(s + d->sinc_eps) / (s + d->sinc_eps);
+  };
+  // b1 (weighted), b2 (vhs-gll.mako:69-99); W_p = sf*qw_p*sw/n (:188-193)
+  std::vector<double> b1w((size_t)Nrho * n), b2(n, 0.0);
+  for (int ix = 0; ix < N; ++ix)
+    for (int iy = 0; iy < N; ++iy)
+      for (int iz = 0; iz < N; ++iz) {
+        const size_t l = ((size_t)ix * N + iy) * N + iz;
+        const double cS = std::sqrt(l0[ix] * l0[ix] + l0[iy] * l0[iy] +
+                                    l0[iz] * l0[iz]);
+        double bsum = 0.0;
+        for (int p = 0; p < Nrho; ++p) {
+          const double qz = d->qz[p];
+          const double b1 = std::pow(qz, d->gamma + 2.) * 4 * M_PI *
+                            sinc(M_PI / d->L * qz / 2. * cS);
+          b1w[(size_t)p * n + l] =
+              (d->sphere_factor * d->qw[p] * d->sw / n) * b1;
+          bsum += d->qw[p] * std::pow(qz, d->gamma + 2.) * 16 * M_PI * M_PI *
+                  sinc(M_PI / d->L * qz * cS);
+        }
+        b2[l] = bsum;
+      }
+  // phase tables exp(i kappa_a rep(l)) and kappa
+  std::vector<double> kappa((size_t)Nrho * Mu * 3);
+  std::vector<double2> ph64((size_t)Nrho * Mu * 3 * N);
+  for (int p = 0; p < Nrho; ++p)
+    for (int u = 0; u < Mu; ++u)
+      for (int a = 0; a < 3; ++a) {
+        const double k = M_PI / d->L * d->qz[p] / 2. * d->sz[3 * uq[u] + a];
+        kappa[((size_t)p * Mu + u) * 3 + a] = k;
+        for (int l = 0; l < N; ++l)
+          ph64[(((size_t)p * Mu + u) * 3 + a) * N + l] =
+              make_double2(std::cos(k * l0[l]), std::sin(k * l0[l]));
+      }
+  std::vector<double> c0(d->c0, d->c0 + N);
+
+  int rc = DGFS_OK;
+  if ((rc = upload(&h->c0, c0)) || (rc = upload(&h->b2, b2)) ||
+      (rc = upload(&h->b1w64, b1w)) || (rc = upload(&h->kappa, kappa)) ||
+      (rc = upload(&h->mult, mult))) {
+    free_handle(h);
+    return rc;
+  }
+  if (fp32) {
+    std::vector<float> b1w32(b1w.begin(), b1w.end());
+    std::vector<float2> ph32(ph64.size());
+    for (size_t i = 0; i < ph64.size(); ++i)
+      ph32[i] = make_float2((float)ph64[i].x, (float)ph64[i].y);
+    float2* p32 = nullptr;
+    if ((rc = upload(&h->b1w32, b1w32)) || (rc = upload(&p32, ph32))) {
+      free_handle(h);
+      return rc;
+    }
+    h->ph = p32;
+  } else {
+    double2* p64 = nullptr;
+    if ((rc = upload(&p64, ph64))) { free_handle(h); return rc; }
+    h->ph = p64;
+  }
+
+  const size_t E = (size_t)d->max_evals;
+  const size_t ce = fp32 ? sizeof(float2) : sizeof(double2);
+  cudaError_t ce_ = cudaSuccess;
+  auto alloc = [&](void** p, size_t bytes) {
+    if (ce_ == cudaSuccess) ce_ = cudaMalloc(p, bytes);
+  };
+  alloc(&h->Fg, E * n * ce);
+  alloc(&h->H, E * Nrho * n * ce);
+  alloc((void**)&h->ReLf, E * n * sizeof(double));
+  if (fp32) {
+    alloc((void**)&h->mhat, E * 3 * N * sizeof(double2));
+    alloc((void**)&h->moments, E * 5 * sizeof(double));
+    alloc(&h->uv, E * Nrho * Mu * 6 * N * sizeof(float2));
+    alloc((void**)&h->hh, E * Nrho * Mu * 3 * N * sizeof(double2));
+    alloc((void**)&h->GM, E * n * sizeof(double2));
+  }
+  if (ce_ != cudaSuccess) {
+    free_handle(h);
+    return fail(DGFS_ERR_CUDA,
+                std::string("scratch allocation: ") + cudaGetErrorString(ce_));
+  }
+  *out = h;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_destroy(dgfs_vhs_handle h) {
+  if (!h) return DGFS_OK;
+  free_handle(h);
+  return DGFS_OK;
+}
+
+extern "C" const double* dgfs_vhs_last_moments(dgfs_vhs_handle h) {
+  return h ? h->moments : nullptr;
+}
+
+template <int N>
+static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
+                   int q_double, const int32_t* src_slots, int src_base,
+                   const int32_t* dst_slots, int dst_base, int nevals,
+                   cudaStream_t st) {
+  constexpr int C64 = (N == 8) ? 1 : (N == 16 ? 2 : 8);
+  constexpr int C32 = (N == 8) ? 1 : (N == 16 ? 1 : 4);
+  using G64 = Geo<N, C64>;
+  using G32 = Geo<N, C32>;
+  const bool fp32 = h->precision == DGFS_PREC_FP32;
+  int rc;
+  // prologue
+  {
+    VhsPrologueArgs a{};
+    a.f = f; a.f_double = f_double; a.src_slots = src_slots; a.src_base = src_base;
+    a.c0 = h->c0; a.b2 = h->b2; a.cw = h->cw; a.split = fp32 ? 1 : 0;
+    a.Fg = h->Fg; a.ReLf = h->ReLf; a.mhat = h->mhat; a.moments = h->moments;
+    const size_t smem = 2 * slab_bytes(N, C64, sizeof(double2)) +
+                        3 * N * sizeof(double2) + 8 * sizeof(double);
+    if ((rc = launch_cluster(vhs_prologue_kernel<N, C64>, dim3(C64, nevals),
+                             dim3(G64::NT), C64, smem, st, a)))
+      return rc;
+  }
+  if (fp32) {
+    VhsTablesArgs t{};
+    t.mhat = h->mhat; t.kappa = h->kappa; t.uv = h->uv; t.hh = h->hh;
+    t.Mu = h->Mu; t.Nrho = h->Nrho; t.nevals = nevals; t.uv_double = 0;
+    const int total = nevals * h->Nrho * h->Mu * 3;
+    if ((rc = launch_plain(vhs_tables_kernel<N>, dim3((total + 95) / 96),
+                           dim3(96), 0, st, t)))
+      return rc;
+    VhsGainArgs g{};
+    g.hh = h->hh; g.mult = h->mult; g.b1w = h->b1w64; g.GM = h->GM;
+    g.Mu = h->Mu; g.Nrho = h->Nrho;
+    const size_t smem = (size_t)h->Mu * (2 * N + 1) * sizeof(double2);
+    if ((rc = launch_plain(vhs_maxwell_gain_kernel<N>, dim3(N, nevals),
+                           dim3(256), smem, st, g)))
+      return rc;
+    VhsTermsArgs a{};
+    a.Fg = h->Fg; a.ph = h->ph; a.uv = h->uv; a.mult = h->mult;
+    a.b1w = h->b1w32; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
+    const size_t smem2 = 3 * slab_bytes(N, C32, sizeof(float2)) +
+                         9 * N * sizeof(float2);
+    if ((rc = launch_cluster(vhs_terms_kernel<float, N, C32, true>,
+                             dim3(C32, h->Nrho, nevals), dim3(G32::NT), C32,
+                             smem2, st, a)))
+      return rc;
+  } else {
+    VhsTermsArgs a{};
+    a.Fg = h->Fg; a.ph = h->ph; a.uv = nullptr; a.mult = h->mult;
+    a.b1w = h->b1w64; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
+    const size_t smem = 3 * slab_bytes(N, C64, sizeof(double2)) +
+                        9 * N * sizeof(double2);
+    if ((rc = launch_cluster(vhs_terms_kernel<double, N, C64, false>,
+                             dim3(C64, h->Nrho, nevals), dim3(G64::NT), C64,
+                             smem, st, a)))
+      return rc;
+  }
+  // epilogue
+  {
+    VhsEpilogueArgs a{};
+    a.H = h->H; a.h_double = fp32 ? 0 : 1; a.GM = fp32 ? h->GM : nullptr;
+    a.ReLf = h->ReLf; a.f = f; a.f_double = f_double;
+    a.src_slots = src_slots; a.src_base = src_base;
+    a.Q = Q; a.q_double = q_double; a.dst_slots = dst_slots; a.dst_base = dst_base;
+    a.prefac = h->prefac; a.Nrho = h->Nrho;
+    const size_t smem = 2 * slab_bytes(N, C64, sizeof(double2));
+    if ((rc = launch_cluster(vhs_epilogue_kernel<N, C64>, dim3(C64, nevals),
+                             dim3(G64::NT), C64, smem, st, a)))
+      return rc;
+  }
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_eval(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
+                             void* Q, int32_t q_dtype,
+                             const int32_t* src_slots, int32_t src_base,
+                             const int32_t* dst_slots, int32_t dst_base,
+                             int32_t nevals, void* stream) {
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  if (nevals < 0) return fail(DGFS_ERR_INVALID, "negative nevals");
+  if (nevals == 0) return DGFS_OK;
+  if (!f || !Q) return fail(DGFS_ERR_INVALID, "null f or Q");
+  if ((f_dtype != DGFS_F32 && f_dtype != DGFS_F64) ||
+      (q_dtype != DGFS_F32 && q_dtype != DGFS_F64))
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  if (src_base < 0 || dst_base < 0)
+    return fail(DGFS_ERR_INVALID, "negative slot base");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  for (int off = 0; off < nevals; off += h->max_evals) {
+    const int cnt = std::min(h->max_evals, nevals - off);
+    const int32_t* ss = src_slots ? src_slots + off : nullptr;
+    const int32_t* ds = dst_slots ? dst_slots + off : nullptr;
+    int rc;
+    switch (h->N) {
+      case 8: rc = vhs_run<8>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 16: rc = vhs_run<16>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 32: rc = vhs_run<32>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      default: return fail(DGFS_ERR_UNSUPPORTED, "N not compiled in");
+    }
+    if (rc) return rc;
+  }
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_fs(dgfs_vhs_handle h, const void* f, void* Q,
+                           int32_t dtype, int32_t Ne, int32_t elem,
+                           int32_t modein, int32_t modeout, void* stream) {
+  if (Ne <= 0 || elem < 0 || elem >= Ne || modein < 0 || modeout < 0)
+    return fail(DGFS_ERR_INVALID, "bad Ne/elem/mode");
+  return dgfs_vhs_eval(h, f, dtype, Q, dtype, nullptr, modein * Ne + elem,
+                       nullptr, modeout * Ne + elem, 1, stream);
+}

@@ -1,0 +1,585 @@
+// Fused fast-spectral VHS collision operator Q(f,f) for a batch of spatial
+// points ("evals").  Reference: DGFSVHSGLLScatteringModelStd.fs
+// (dgfs1D/std/scattering.py:251-313) and its kernels in
+// dgfs1D/std/kernels/scattering/vhs-gll.mako.
+//
+// Per eval the reference computes (cuFFT conventions, F = FFT(f)/n):
+//   t3_pq = IFFT(cos a_pq F), t4_pq = IFFT(sin a_pq F),
+//   a_pq(l) = (pi/L)(rho_p/2) sigma_q . l
+//   Ghat  = sum_p (sf w_p s_w / n) b1_p sum_q FFT(t3^2 + t4^2)
+//   Q    += prefac * (Re IFFT(Ghat) - f * Re IFFT(b2 F))
+// The kernels below restructure this without changing its value:
+//   * linearity: sum_q FFT(h_pq) = FFT(sum_q h_pq) (one forward FFT per p);
+//   * antipodal pairs sigma_q' = -sigma_q give identical h, so only one of
+//     each pair is transformed, with multiplicity 2;
+//   * a_pq is linear in l, so exp(i a) is the product of three 1-D phase
+//     tables and is never stored;
+//   * in the FP32 mode, f = M + g with M the separable local Maxwellian: the
+//     M-parts of t3, t4, h and FFT(h) are products of 1-D transforms computed
+//     in FP64, and only the small remainder g runs through FP32 3-D FFTs.
+//
+// Kernels (one stage = prologue, [tables, maxwell_gain], terms, epilogue):
+//   prologue   (cluster per eval, FP64): F, moments, Maxwellian spectra,
+//              F_g = F - M_hat, Re IFFT(b2 F)
+//   tables     (FP64): per (eval,p,q) 1-D u_a, v_a and FFT(u_a v_a)
+//   maxwell_gain (FP64): Ghat_M = sum_p W_p b1_p sum_q m_q prod_a FFT(u_a v_a)
+//   terms      (cluster per (eval,p), precision R): H_p = W_p b1_p FFT(S_p)
+//   epilogue   (cluster per eval, FP64): Ghat = Ghat_M + sum_p H_p,
+//              Q += prefac (Re IFFT(Ghat) - f Re IFFT(b2 F))
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cluster_slab.cuh"
+#include "fft_reg.cuh"
+
+namespace dgfs {
+
+struct VhsPrologueArgs {
+  const void* f;              // input distribution (float or double)
+  int f_double;               // 1: f is double
+  const int32_t* src_slots;   // device slot list or null
+  int src_base;               // slot(i) = src_slots ? src_slots[i] : src_base+i
+  const double* c0;           // [N] velocity grid (x, y and z)
+  const double* b2;           // [n] loss kernel b2(l)
+  double cw;                  // velocity cell volume
+  int split;                  // 1: Maxwellian split (FP32 mode)
+  void* Fg;                   // out [nevals][n] complex (float2 if split else double2)
+  double* ReLf;               // out [nevals][n] Re IFFT(b2 F)
+  double2* mhat;              // out [nevals][3][N] Maxwellian 1-D spectra (split)
+  double* moments;            // out [nevals][5] rho, ux, uy, uz, T (split)
+};
+
+struct VhsTermsArgs {
+  const void* Fg;             // [nevals][n] complex, precision R
+  const void* ph;             // [Nrho][Mu][3][N] exp(i kappa_a rep(l)), precision R
+  const void* uv;             // [nevals][Nrho][Mu][2][3][N] u_a, v_a (split)
+  const float* mult;          // [Mu] multiplicity of each transformed direction
+  const void* b1w;            // [Nrho][n] W_p b1_p(l), precision R
+  void* H;                    // out [nevals][Nrho][n] complex, precision R
+  int Mu;
+  int Nrho;
+};
+
+struct VhsTablesArgs {
+  const double2* mhat;        // [nevals][3][N]
+  const double* kappa;        // [Nrho][Mu][3] kappa_a = (pi/L)(rho_p/2) sigma_qa
+  void* uv;                   // out [nevals][Nrho][Mu][2][3][N] precision R
+  double2* hh;                // out [nevals][Nrho][Mu][3][N] FFT(u_a v_a)
+  int Mu;
+  int Nrho;
+  int nevals;
+  int uv_double;              // 1: uv stored as double2
+};
+
+struct VhsGainArgs {
+  const double2* hh;          // [nevals][Nrho][Mu][3][N]
+  const float* mult;          // [Mu]
+  const double* b1w;          // [Nrho][n] W_p b1_p(l)
+  double2* GM;                // out [nevals][n]
+  int Mu;
+  int Nrho;
+};
+
+struct VhsEpilogueArgs {
+  const void* H;              // [nevals][Nrho][n] precision R
+  int h_double;
+  const double2* GM;          // [nevals][n] or null
+  const double* ReLf;         // [nevals][n]
+  const void* f;              // input distribution
+  int f_double;
+  const int32_t* src_slots;
+  int src_base;
+  void* Q;                    // output distribution (+=)
+  int q_double;
+  const int32_t* dst_slots;
+  int dst_base;
+  double prefac;
+  int Nrho;
+};
+
+__device__ __forceinline__ int slot_of(const int32_t* slots, int base, int i) {
+  return slots ? slots[i] : base + i;
+}
+__device__ __forceinline__ double load_real(const void* p, int is_double,
+                                            size_t idx) {
+  return is_double ? static_cast<const double*>(p)[idx]
+                   : (double)static_cast<const float*>(p)[idx];
+}
+
+// ---------------------------------------------------------------------------
+// Prologue: one cluster (C CTAs, FP64) per eval.
+// ---------------------------------------------------------------------------
+template <int N, int C>
+__global__ void __launch_bounds__(Geo<N, C>::NT, 1)
+vhs_prologue_kernel(VhsPrologueArgs a) {
+  using G = Geo<N, C>;
+  using T = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);
+  T* Rb = A + G::SLAB;
+  T* mh = Rb + G::SLAB;                                    // [3][N]
+  double* mom = reinterpret_cast<double*>(mh + 3 * N);     // [8]
+  // moment partials [5][NT] + [5] borrow the receive slab, unused until the
+  // loss transform (peers write it only two cluster barriers later)
+  double* red = reinterpret_cast<double*>(Rb);
+
+  const int t = threadIdx.x;
+  const unsigned rank = cluster_rank();
+  const int e = blockIdx.y;
+  const int yl = t / N, z = t % N, y = rank * G::P + yl;
+  const size_t fbase = (size_t)slot_of(a.src_slots, a.src_base, e) * G::n;
+
+  T v[N];
+#pragma unroll
+  for (int x = 0; x < N; ++x) {
+    v[x].x = load_real(a.f, a.f_double, fbase + ((size_t)x * N + y) * N + z);
+    v[x].y = 0.0;
+  }
+
+  if (a.split) {
+    // moments of f on the grid (sum f, sum f c, sum f |c|^2); deterministic
+    // two-level reduction: per-thread partials -> CTA -> cluster.
+    double s[5] = {0, 0, 0, 0, 0};
+    const double cy = a.c0[y], cz = a.c0[z];
+#pragma unroll
+    for (int x = 0; x < N; ++x) {
+      const double cx = a.c0[x], fv = v[x].x;
+      s[0] += fv;
+      s[1] += fv * cx;
+      s[2] += fv * cy;
+      s[3] += fv * cz;
+      s[4] += fv * (cx * cx + cy * cy + cz * cz);
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) red[k * G::NT + t] = s[k];
+    __syncthreads();
+    if (t < 5) {
+      double acc = 0;
+      for (int i = 0; i < G::NT; ++i) acc += red[t * G::NT + i];
+      red[5 * G::NT + t] = acc;  // this CTA's partial
+    }
+    cluster_sync_all();
+    if (t < 5) {
+      double acc = 0;
+      for (int c = 0; c < C; ++c)
+        acc += peer_ptr(red, (unsigned)c)[5 * G::NT + t];
+      mom[t] = acc;
+    }
+    __syncthreads();
+    if (t == 0) {
+      double rho = mom[0] * a.cw, ux = 0, uy = 0, uz = 0, Tm = 1;
+      if (rho > 1e-300) {
+        ux = mom[1] * a.cw / rho; uy = mom[2] * a.cw / rho; uz = mom[3] * a.cw / rho;
+        Tm = (2.0 / 3.0) * (mom[4] * a.cw / rho - (ux * ux + uy * uy + uz * uz));
+        if (!(Tm > 1e-6)) { rho = 0; Tm = 1; }  // no useful Maxwellian
+      } else {
+        rho = 0;
+      }
+      mom[0] = rho; mom[1] = ux; mom[2] = uy; mom[3] = uz; mom[4] = Tm;
+      if (rank == 0)
+        for (int k = 0; k < 5; ++k) a.moments[(size_t)e * 5 + k] = mom[k];
+    }
+    __syncthreads();
+    // 1-D Maxwellian factors and their spectra (direct DFT, table twiddles)
+    for (int i = t; i < 3 * N; i += G::NT) {
+      const int ax = i / N, k = i % N;
+      const double rho = mom[0], Tm = mom[4], u = mom[1 + ax];
+      const double amp = (ax == 0) ? rho / pow(M_PI * Tm, 1.5) : 1.0;
+      double re = 0, im = 0;
+      for (int j = 0; j < N; ++j) {
+        const double d = a.c0[j] - u;
+        const double m = amp * exp(-d * d / Tm);
+        constexpr int off = tw_offset(N);
+        const double2 w = c_tw64[off + (j * k) % N];
+        re += m * w.x;
+        im += m * w.y;
+      }
+      mh[ax * N + k] = make_double2(re / N, im / N);
+    }
+    // (visibility of mh is ensured by the barriers below)
+  }
+
+  // forward x-pass and exchange into X-slabs
+  fft<double, N, -1>(v);
+  push_pencils_to_xslab<double, N, C>(A, t, rank, v);
+  cluster_sync_all();
+  {
+    T w[N];
+    slab_col_load_fft<double, N, C, -1>(A, t, w);
+    const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+    for (int k = 0; k < N; ++k) A[base + k * G::ROW] = w[k];
+  }
+  __syncthreads();
+  slab_row_pass<double, N, C, -1>(A, t);
+  __syncthreads();
+
+  // F = FFT(f)/n; write F (FP64) or F_g = F - mhat (FP32); then A <- b2 F
+  const double inv_n = 1.0 / (double)G::n;
+  const size_t gbase = (size_t)e * G::n + (size_t)rank * G::P * N * N;
+  for (int j = t; j < G::P * N * N; j += G::NT) {
+    const int si = slab_index<N, C>(j);
+    T Fv = A[si];
+    Fv.x *= inv_n;
+    Fv.y *= inv_n;
+    if (a.split) {
+      const int lx = rank * G::P + j / (N * N), ly = (j / N) % N, lz = j % N;
+      const T mm = cmul(cmul(mh[lx], mh[N + ly]), mh[2 * N + lz]);
+      float2 g;
+      g.x = (float)(Fv.x - mm.x);
+      g.y = (float)(Fv.y - mm.y);
+      static_cast<float2*>(a.Fg)[gbase + j] = g;
+    } else {
+      static_cast<double2*>(a.Fg)[gbase + j] = Fv;
+    }
+    const double b = a.b2[(size_t)rank * G::P * N * N + j];
+    Fv.x *= b;
+    Fv.y *= b;
+    A[si] = Fv;
+  }
+  if (a.split && rank == 0)
+    for (int i = t; i < 3 * N; i += G::NT) a.mhat[(size_t)e * 3 * N + i] = mh[i];
+  __syncthreads();
+  // loss: Re IFFT(b2 F)
+  slab_row_pass<double, N, C, +1>(A, t);
+  __syncthreads();
+  {
+    T w[N];
+    slab_col_load_fft<double, N, C, +1>(A, t, w);
+    push_cols_to_yslab<double, N, C>(Rb, t, rank, w);
+  }
+  cluster_sync_all();
+  yslab_load_pencil<double, N, C>(Rb, t, v);
+  fft<double, N, +1>(v);
+#pragma unroll
+  for (int x = 0; x < N; ++x)
+    a.ReLf[(size_t)e * G::n + ((size_t)x * N + y) * N + z] = v[x].x;
+}
+
+// ---------------------------------------------------------------------------
+// Tables: per (eval, p, q, axis) u_a = IFFT(e^{+i k l} mhat_a),
+// v_a = IFFT(e^{-i k l} mhat_a), hh_a = FFT(u_a v_a)  (FP64, one thread each).
+// ---------------------------------------------------------------------------
+template <int N>
+__global__ void vhs_tables_kernel(VhsTablesArgs a) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int total = a.nevals * a.Nrho * a.Mu * 3;
+  if (gid >= total) return;
+  const int ax = gid % 3;
+  const int q = (gid / 3) % a.Mu;
+  const int p = (gid / (3 * a.Mu)) % a.Nrho;
+  const int e = gid / (3 * a.Mu * a.Nrho);
+  const double kap = a.kappa[((size_t)p * a.Mu + q) * 3 + ax];
+  const double2* mh = a.mhat + (size_t)e * 3 * N + ax * N;
+  double2 u[N], w[N];
+#pragma unroll
+  for (int l = 0; l < N; ++l) {
+    const int rl = (l < N / 2) ? l : l - N;
+    double s, c;
+    sincos(kap * (double)rl, &s, &c);
+    const double2 m = mh[l];
+    u[l] = cmul(m, make_double2(c, s));
+    w[l] = cmul(m, make_double2(c, -s));
+  }
+  fft<double, N, +1>(u);
+  fft<double, N, +1>(w);
+  const size_t tb = (((size_t)e * a.Nrho + p) * a.Mu + q);
+  if (a.uv_double) {
+    double2* uv = static_cast<double2*>(a.uv) + tb * 6 * N;
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      uv[ax * N + l] = u[l];
+      uv[(3 + ax) * N + l] = w[l];
+    }
+  } else {
+    float2* uv = static_cast<float2*>(a.uv) + tb * 6 * N;
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      uv[ax * N + l] = make_float2((float)u[l].x, (float)u[l].y);
+      uv[(3 + ax) * N + l] = make_float2((float)w[l].x, (float)w[l].y);
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < N; ++l) u[l] = cmul(u[l], w[l]);
+  fft<double, N, -1>(u);
+  double2* hh = a.hh + tb * 3 * N + ax * N;
+#pragma unroll
+  for (int l = 0; l < N; ++l) hh[l] = u[l];
+}
+
+// ---------------------------------------------------------------------------
+// Maxwellian gain: Ghat_M(l) = sum_p W_p b1_p(l) sum_q m_q hx(lx) hy(ly) hz(lz)
+// grid (N [lx], nevals), block N*N threads (ly, lz) -- one point each.
+// ---------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(256)
+vhs_maxwell_gain_kernel(VhsGainArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* hyz = reinterpret_cast<double2*>(smem_raw);   // [Mu][2][N]
+  double2* hx = hyz + (size_t)a.Mu * 2 * N;              // [Mu]
+  const int lx = blockIdx.x, e = blockIdx.y;
+  const int t = threadIdx.x;
+  constexpr int PTS = (N * N + 255) / 256;  // points per thread
+  double2 Gs[PTS];
+#pragma unroll
+  for (int k = 0; k < PTS; ++k) Gs[k] = make_double2(0, 0);
+  for (int p = 0; p < a.Nrho; ++p) {
+    const double2* hh = a.hh + ((size_t)e * a.Nrho + p) * a.Mu * 3 * N;
+    __syncthreads();
+    for (int i = t; i < a.Mu * 2 * N; i += blockDim.x) {
+      const int q = i / (2 * N), r = i % (2 * N);
+      hyz[i] = hh[(size_t)q * 3 * N + N + r];
+    }
+    for (int i = t; i < a.Mu; i += blockDim.x) hx[i] = hh[(size_t)i * 3 * N + lx];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) {
+      const int pt = t + k * 256;
+      if (pt < N * N) {
+        const int ly = pt / N, lz = pt % N;
+        double2 acc = make_double2(0, 0);
+        for (int q = 0; q < a.Mu; ++q) {
+          const double m = (double)a.mult[q];
+          const double2 xy = cmul(hx[q], hyz[(size_t)q * 2 * N + ly]);
+          const double2 xyz = cmul(xy, hyz[(size_t)q * 2 * N + N + lz]);
+          acc.x += m * xyz.x;
+          acc.y += m * xyz.y;
+        }
+        const double w = a.b1w[(size_t)p * N * N * N + (size_t)lx * N * N + pt];
+        Gs[k].x += w * acc.x;
+        Gs[k].y += w * acc.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < PTS; ++k) {
+    const int pt = t + k * 256;
+    if (pt < N * N) a.GM[(size_t)e * N * N * N + (size_t)lx * N * N + pt] = Gs[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Terms: one cluster per (eval, p).  Precision R; SPLIT selects the
+// Maxwellian-split combine.  FP32 keeps the running S_p in registers and the
+// F slab resident in shared memory; FP64 keeps S_p in shared memory and
+// streams F rows from global memory.
+// ---------------------------------------------------------------------------
+template <typename R, int N, int C, bool SPLIT>
+__global__ void __launch_bounds__(Geo<N, C>::NT, 1)
+vhs_terms_kernel(VhsTermsArgs a) {
+  using G = Geo<N, C>;
+  using T = c2_t<R>;
+  constexpr bool S_REG = (sizeof(R) == 4);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);
+  T* Rb = A + G::SLAB;
+  T* F = Rb + G::SLAB;              // S_REG: resident F slab; else S slab
+  T* tab = F + G::SLAB;             // [3][N] phase + [6][N] u,v
+  const int t = threadIdx.x;
+  const unsigned rank = cluster_rank();
+  const int p = blockIdx.y, e = blockIdx.z;
+  const T* Fg = static_cast<const T*>(a.Fg) + (size_t)e * G::n;
+  const T* ph = static_cast<const T*>(a.ph);
+  const T* uvg = static_cast<const T*>(a.uv);
+
+  T S[S_REG ? N : 1];
+  if constexpr (S_REG) {
+#pragma unroll
+    for (int x = 0; x < N; ++x) S[x] = T{0, 0};
+    for (int j = t; j < G::P * N * N; j += G::NT)
+      F[slab_index<N, C>(j)] = Fg[(size_t)rank * G::P * N * N + j];
+  } else {
+    const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+    for (int x = 0; x < N; ++x) F[base + x * G::ROW] = T{0, 0};
+  }
+
+  const int yl = t / N, zz = t % N, yy = rank * G::P + yl;
+  bool first = true;
+  for (int q = 0; q < a.Mu; ++q) {
+    __syncthreads();  // previous term's table readers are done
+    for (int i = t; i < 3 * N; i += G::NT)
+      tab[i] = ph[((size_t)p * a.Mu + q) * 3 * N + i];
+    if constexpr (SPLIT) {
+      for (int i = t; i < 6 * N; i += G::NT)
+        tab[3 * N + i] =
+            uvg[((((size_t)e * a.Nrho) + p) * a.Mu + q) * 6 * N + i];
+    }
+    __syncthreads();
+    const R mq = (R)a.mult[q];
+#pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+      // z-pass: multiplier cos/sin of a(l), inverse FFT along z
+      {
+        const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
+        const T bxy = cmul(tab[lx], tab[N + ly]);
+        T v[N];
+        if constexpr (S_REG) {
+          const int base = pl * G::PLANE + ly * G::ROW;
+#pragma unroll
+          for (int k = 0; k < N; ++k) v[k] = F[base + k];
+        } else {
+          const T* row = Fg + ((size_t)lx * N + ly) * N;
+#pragma unroll
+          for (int k = 0; k < N; ++k) v[k] = row[k];
+        }
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const T ph3 = cmul(bxy, tab[2 * N + k]);
+          const R m = s == 0 ? ph3.x : ph3.y;
+          v[k].x *= m;
+          v[k].y *= m;
+        }
+        fft<R, N, +1>(v);
+        const int base = pl * G::PLANE + ly * G::ROW;
+#pragma unroll
+        for (int k = 0; k < N; ++k) A[base + k] = v[k];
+      }
+      __syncthreads();
+      {
+        T v[N];
+        slab_col_load_fft<R, N, C, +1>(A, t, v);
+        if (!first) cluster_wait();  // receive buffers are free
+        push_cols_to_yslab<R, N, C>(Rb, t, rank, v);
+      }
+      first = false;
+      cluster_arrive();
+      cluster_wait();
+      T v[N];
+      yslab_load_pencil<R, N, C>(Rb, t, v);
+      cluster_arrive();  // done reading the receive buffer
+      fft<R, N, +1>(v);
+      T sv[N];
+      if constexpr (!S_REG) {
+        const int base = yl * G::PLANE + zz;
+#pragma unroll
+        for (int x = 0; x < N; ++x) sv[x] = F[base + x * G::ROW];
+      }
+      if constexpr (SPLIT) {
+        const T* ut = tab + 3 * N;
+        const T* vt = tab + 6 * N;
+        const T uyz = cmul(ut[N + yy], ut[2 * N + zz]);
+        const T vyz = cmul(vt[N + yy], vt[2 * N + zz]);
+#pragma unroll
+        for (int x = 0; x < N; ++x) {
+          const T um = cmul(ut[x], uyz), vm = cmul(vt[x], vyz);
+          T XM;
+          if (s == 0) { XM.x = R(0.5) * (um.x + vm.x); XM.y = R(0.5) * (um.y + vm.y); }
+          else        { XM.x = R(0.5) * (um.y - vm.y); XM.y = R(-0.5) * (um.x - vm.x); }
+          // h_rest = 2 XM X + X^2 = X (2 XM + X)
+          T w; w.x = R(2) * XM.x + v[x].x; w.y = R(2) * XM.y + v[x].y;
+          const T h = cmul(v[x], w);
+          if constexpr (S_REG) { S[x].x += mq * h.x; S[x].y += mq * h.y; }
+          else { sv[x].x += mq * h.x; sv[x].y += mq * h.y; }
+        }
+      } else {
+#pragma unroll
+        for (int x = 0; x < N; ++x) {
+          const T h = cmul(v[x], v[x]);
+          if constexpr (S_REG) { S[x].x += mq * h.x; S[x].y += mq * h.y; }
+          else { sv[x].x += mq * h.x; sv[x].y += mq * h.y; }
+        }
+      }
+      if constexpr (!S_REG) {
+        const int base = yl * G::PLANE + zz;
+#pragma unroll
+        for (int x = 0; x < N; ++x) F[base + x * G::ROW] = sv[x];
+      }
+    }
+  }
+
+  // forward FFT of S_p: x-pass, exchange into X-slabs, y-pass, z-pass
+  T v[N];
+  if constexpr (S_REG) {
+#pragma unroll
+    for (int x = 0; x < N; ++x) v[x] = S[x];
+  } else {
+    const int base = yl * G::PLANE + zz;
+#pragma unroll
+    for (int x = 0; x < N; ++x) v[x] = F[base + x * G::ROW];
+  }
+  fft<R, N, -1>(v);
+  if (!first) cluster_wait();
+  push_pencils_to_xslab<R, N, C>(A, t, rank, v);
+  cluster_arrive();
+  cluster_wait();
+  {
+    T w[N];
+    slab_col_load_fft<R, N, C, -1>(A, t, w);
+    const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+    for (int k = 0; k < N; ++k) A[base + k * G::ROW] = w[k];
+  }
+  __syncthreads();
+  slab_row_pass<R, N, C, -1>(A, t);
+  __syncthreads();
+  const R* b1w = static_cast<const R*>(a.b1w) + (size_t)p * G::n +
+                 (size_t)rank * G::P * N * N;
+  T* H = static_cast<T*>(a.H) + ((size_t)e * a.Nrho + p) * G::n +
+         (size_t)rank * G::P * N * N;
+  for (int j = t; j < G::P * N * N; j += G::NT) {
+    T hv = A[slab_index<N, C>(j)];
+    const R w = b1w[j];
+    hv.x *= w;
+    hv.y *= w;
+    H[j] = hv;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Epilogue: one cluster (FP64) per eval.
+// ---------------------------------------------------------------------------
+template <int N, int C>
+__global__ void __launch_bounds__(Geo<N, C>::NT, 1)
+vhs_epilogue_kernel(VhsEpilogueArgs a) {
+  using G = Geo<N, C>;
+  using T = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);
+  T* Rb = A + G::SLAB;
+  const int t = threadIdx.x;
+  const unsigned rank = cluster_rank();
+  const int e = blockIdx.y;
+  const size_t off = (size_t)rank * G::P * N * N;
+  for (int j = t; j < G::P * N * N; j += G::NT) {
+    T g = a.GM ? a.GM[(size_t)e * G::n + off + j] : T{0, 0};
+    for (int p = 0; p < a.Nrho; ++p) {
+      const size_t hi = ((size_t)e * a.Nrho + p) * G::n + off + j;
+      if (a.h_double) {
+        const double2 h = static_cast<const double2*>(a.H)[hi];
+        g.x += h.x; g.y += h.y;
+      } else {
+        const float2 h = static_cast<const float2*>(a.H)[hi];
+        g.x += (double)h.x; g.y += (double)h.y;
+      }
+    }
+    A[slab_index<N, C>(j)] = g;
+  }
+  __syncthreads();
+  slab_row_pass<double, N, C, +1>(A, t);
+  __syncthreads();
+  {
+    T w[N];
+    slab_col_load_fft<double, N, C, +1>(A, t, w);
+    push_cols_to_yslab<double, N, C>(Rb, t, rank, w);
+  }
+  cluster_sync_all();
+  T v[N];
+  yslab_load_pencil<double, N, C>(Rb, t, v);
+  fft<double, N, +1>(v);
+  const int yl = t / N, z = t % N, y = rank * G::P + yl;
+  const size_t fb = (size_t)slot_of(a.src_slots, a.src_base, e) * G::n;
+  const size_t qb = (size_t)slot_of(a.dst_slots, a.dst_base, e) * G::n;
+#pragma unroll
+  for (int x = 0; x < N; ++x) {
+    const size_t idx = ((size_t)x * N + y) * N + z;
+    const double fv = load_real(a.f, a.f_double, fb + idx);
+    const double qv =
+        a.prefac * (v[x].x - fv * a.ReLf[(size_t)e * G::n + idx]);
+    if (a.q_double) static_cast<double*>(a.Q)[qb + idx] += qv;
+    else static_cast<float*>(a.Q)[qb + idx] += (float)qv;
+  }
+}
+
+}  // namespace dgfs

@@ -1,0 +1,107 @@
+/*
+ * dgfs_sm100 -- C ABI of the B200 (sm_100a) fast-spectral Boltzmann
+ * collision operators of DGFS.
+ *
+ * Plain pointers and sizes only.  Every call returns 0 on success or a
+ * negative DGFS_ERR_* code; dgfs_last_error_string() describes the last
+ * failure on the calling thread.  Device pointers are CUDA device addresses
+ * on the current device; `stream` is a cudaStream_t (NULL = legacy default
+ * stream).  Evaluation calls launch work asynchronously, allocate nothing and
+ * never synchronise the host.  A handle owns its scratch: calls on one
+ * handle must be ordered (same stream, or externally synchronised).
+ *
+ * Layout (as in the reference): a distribution array holds `slots` of n =
+ * N^3 values, slot s at offset s*n, velocity index v = (i*N + j)*N + k with
+ * i <-> c_x slowest.  The reference addresses slot (mode*Ne + elem)
+ * (dgfs1D/std/kernels/scattering/vhs-gll.mako:408).
+ */
+#ifndef DGFS_SM100_H
+#define DGFS_SM100_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGFS_OK 0
+#define DGFS_ERR_INVALID (-1)      /* bad argument or descriptor */
+#define DGFS_ERR_UNSUPPORTED (-2)  /* shape/precision not compiled in */
+#define DGFS_ERR_CUDA (-3)         /* CUDA runtime or launch failure */
+#define DGFS_ERR_CAPACITY (-4)     /* size beyond a fixed maximum */
+
+#define DGFS_F32 0                 /* float arrays */
+#define DGFS_F64 1                 /* double arrays */
+
+#define DGFS_PREC_FP64 0           /* all arithmetic in FP64 */
+#define DGFS_PREC_FP32 1           /* FP32 3-D FFTs on f - M (local
+                                      Maxwellian M handled in FP64) */
+
+typedef struct dgfs_vhs_s* dgfs_vhs_handle;
+
+/*
+ * Single-species VHS/HS fast-spectral model, `vhs-gll` and `vhs` in the
+ * reference (dgfs1D/std/scattering.py:51-313, 317-429).  The descriptor
+ * carries what DGFSVHSGLLScatteringModelStd.perform_precomputation reads
+ * from the velocity mesh (std/scattering.py:106-191): grid size N, radial
+ * Gauss rule qz/qw (Nrho points on [0, R]), spherical rule sz (M x 3) with
+ * weight sw, the factor 2 of computeQG for a half-sphere rule
+ * (vhs-gll.mako:192; 1 for a full-sphere rule), gamma = 2(1-omega), the
+ * collision prefactor, the sinc regulariser (1e-15 double, 1e-6 float), the
+ * cell volume cw and the 1-D velocity grid c0[N].
+ */
+typedef struct {
+  int32_t N;
+  int32_t Nrho;
+  int32_t M;
+  double L;
+  const double* qz;        /* [Nrho] host */
+  const double* qw;        /* [Nrho] host */
+  const double* sz;        /* [M*3] host, row-major */
+  double sw;
+  double sphere_factor;
+  double gamma;
+  double prefac;
+  double sinc_eps;
+  double cw;
+  const double* c0;        /* [N] host */
+  int32_t precision;       /* DGFS_PREC_* */
+  int32_t max_evals;       /* evaluations per launch batch (scratch size) */
+} dgfs_vhs_desc;
+
+/* Replaces DGFSVHSGLLScatteringModelStd.__init__/perform_precomputation
+ * (std/scattering.py:51-246): builds tables, allocates scratch. */
+int dgfs_vhs_create(const dgfs_vhs_desc* desc, dgfs_vhs_handle* out);
+
+/* Batched Q(f,f):  for i in [0, nevals):
+ *     Q[dst(i)] += prefac * (gain(f[src(i)]) - f[src(i)] * loss(f[src(i)]))
+ * with src(i) = src_slots ? src_slots[i] : src_base + i (device int32
+ * array), likewise dst.  One call replaces nevals calls of
+ * DGFSVHSGLLScatteringModelStd.fs (std/scattering.py:251-313). */
+int dgfs_vhs_eval(dgfs_vhs_handle h, const void* f, int32_t f_dtype, void* Q,
+                  int32_t q_dtype, const int32_t* src_slots, int32_t src_base,
+                  const int32_t* dst_slots, int32_t dst_base, int32_t nevals,
+                  void* stream);
+
+/* Reference-shaped single evaluation: fs(d_f, d_g, d_Q, elem, modein,
+ * modeout) of std/scattering.py:251 (d_g unused there as here):
+ * src = modein*Ne + elem, dst = modeout*Ne + elem. */
+int dgfs_vhs_fs(dgfs_vhs_handle h, const void* f, void* Q, int32_t dtype,
+                int32_t Ne, int32_t elem, int32_t modein, int32_t modeout,
+                void* stream);
+
+/* Per-eval local moments (rho, ux, uy, uz, T) of the last FP32 evaluation
+ * batch, device pointer owned by the handle ([max_evals][5] doubles). */
+const double* dgfs_vhs_last_moments(dgfs_vhs_handle h);
+
+int dgfs_vhs_destroy(dgfs_vhs_handle h);
+
+/* Library identification and error reporting. */
+const char* dgfs_version(void);
+const char* dgfs_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGFS_SM100_H */
