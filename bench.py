@@ -1,0 +1,349 @@
+"""Benchmark of the fused fast-spectral collision operator Q(f,f) on B200.
+
+Workload: the batched FP32 VHS configuration -- 24 spatial points (Ne=8,
+K=3), velocity grid N=32^3 on [-6,6]^3, full-sphere M=12 design, Nrho=16,
+omega=0.81 -- with seeded synthetic Couette-like distributions (Maxwellians
+with u_y in [-0.1,0.1], T in [0.95,1.05], times 1 +- 1% uniform noise).
+One step = one batched evaluation of Q(f,f) at all 24 points (one RHS stage).
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the CPU oracle
+(the reference algorithm restated in NumPy/SciPy, all host cores) instead.
+Multi-GPU (torchrun): every rank evaluates its own 24 points (weak scaling,
+no data-path collective); time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(workload='vhs-couette-fp32-batched', N=32, M=12, Nrho=16,
+                L=6.0, points=24, Ne=8, K=3, omega=0.81, sphere='full-12pt')
+METRIC = 'Q(f,f) evals/s at N=32^3 (FP32 fused, M=12, Nrho=16, 24 points)'
+UNIT = 'evals/s'
+
+
+def make_inputs(rank=0):
+    from dgfs1d_gpu_b200.workloads import couette_distributions, vhs_mesh_params
+    prm = vhs_mesh_params(32, 12, 16, 6., True)
+    f = couette_distributions(prm['c0'], 24, seed=20261203 + rank)
+    return prm, f
+
+
+def cpu_oracle_rate(prm, f, budget_s=12.0, max_evals=4):
+    """Evals/s of the oracle (CPU checker) on this host's cores, bounded."""
+    from oracle.collision import VHSTables, vhs_gll_fs
+    tab = VHSTables(prm['N'], prm['L'], prm['qz'], prm['qw'], prm['sz'],
+                    prm['sw'], prm['gamma'],
+                    sphere_factor=prm['sphere_factor'])
+    prefac = prm['prefac']
+    vhs_gll_fs(tab, prefac, f[0])  # warm-up
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_evals and (n == 0 or time.perf_counter() - t0 < budget_s):
+        vhs_gll_fs(tab, prefac, f[n % len(f)])
+        n += 1
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.idx), '--query-gpu=' + self.Q,
+                 '--format=csv,noheader,nounits', '-lms', '100'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def summary(self):
+        if not getattr(self, 'rows', None):
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+        sm = [float(r[0]) for r in self.rows if r[0].replace('.', '').isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+                 'sw_power_cap']
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[4 + i].lower() == 'active'})
+        return {'sm_mhz': float(np.median(sm)) if sm else None,
+                'sm_max_mhz': max(mx) if mx else None,
+                'reasons': reasons, 'samples': len(self.rows)}
+
+
+def fp32_fma_peak(torch):
+    """Measured FP32 FMA throughput (TFLOP/s) of this GPU, own kernel."""
+    from dgfs1d_gpu_b200 import _native as nat
+    import ctypes
+    L = nat.lib()
+    out = ctypes.c_double(0)
+    nat.check(L.dgfs_fma_peak(ctypes.byref(out), ctypes.c_void_p(
+        torch.cuda.current_stream().cuda_stream)))
+    return out.value
+
+
+def run_reference(args, rank, world):
+    """CPU oracle arm: rank 0 only, all host cores."""
+    if rank != 0:
+        return
+    prm, f = make_inputs(0)
+    cores = os.cpu_count() or 1
+    rates = []
+    for _ in range(args.warmup):
+        cpu_oracle_rate(prm, f, budget_s=2.0, max_evals=1)
+    t_all = 0.0
+    n_all = 0
+    for _ in range(args.steps):
+        r, n, dt = cpu_oracle_rate(prm, f, budget_s=6.0, max_evals=2)
+        rates.append(r)
+        t_all += dt
+        n_all += n
+    value = n_all / t_all
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT,
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': 1e3 * 24 / value, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+        'data': 'synthetic', 'config': dict(WORKLOAD),
+        'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores,
+                         'kind': 'port',
+                         'sample': f'{n_all} single-point evals of the NumPy/'
+                                   'SciPy oracle (reference algorithm, 3T+3 '
+                                   'FFTs per eval, complex128, '
+                                   f'scipy.fft workers={cores})'},
+        'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+                'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='native', choices=['native', 'reference'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--kernel-only', action='store_true',
+                    help='run only warm-up + timed FP32 evaluations (for ncu '
+                         'launch lists); prints ms per step')
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get('RANK', 0))
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+
+    if args.impl == 'reference':
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from dgfs1d_gpu_b200 import build
+    if rank == 0 or not os.path.exists(build.OUT):
+        build.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device('cuda', local))
+    from dgfs1d_gpu_b200.collision import VHSOperator
+
+    prm, f = make_inputs(rank)
+    E = f.shape[0]
+    fd = torch.tensor(f, dtype=torch.float64, device='cuda')
+    op32 = VHSOperator(**prm, precision='fp32', max_evals=E)
+    op64 = VHSOperator(**prm, precision='fp64', max_evals=E)
+    Q = torch.zeros_like(fd)
+    flush = torch.empty(64 * 2 ** 20, dtype=torch.float32, device='cuda')
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        barrier()
+        tot = 0.0
+        for _ in range(steps):
+            flush.fill_(1.0)  # evict L2 (256 MB > 126 MB) outside the events
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            e.synchronize()
+            tot += s.elapsed_time(e)
+        barrier()
+        t = torch.tensor([tot], device='cuda', dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()) / steps  # ms per step, max over ranks
+
+    if args.kernel_only:
+        ms = timed(lambda: op32.eval(fd, Q), args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({'kernel_only_ms_per_step': ms}), flush=True)
+        return
+
+    # headline: FP32 fused operator, inputs resident in HBM
+    with ClockSampler(local) as clk:
+        ms32 = timed(lambda: op32.eval(fd, Q), args.steps, args.warmup)
+    # plain FP64 path (same kernels, FP64 arithmetic, no split)
+    ms64 = timed(lambda: op64.eval(fd, Q), max(3, args.steps // 2), 3)
+
+    # error of the FP32 mode vs the FP64 mode on this workload
+    Q32 = torch.zeros_like(fd)
+    Q64 = torch.zeros_like(fd)
+    op32.eval(fd, Q32)
+    op64.eval(fd, Q64)
+    torch.cuda.synchronize()
+    err = float(torch.linalg.norm(Q32 - Q64) / torch.linalg.norm(Q64))
+
+    # end to end through the C ABI with host buffers: H2D f, eval, D2H Q
+    fh = torch.tensor(f, dtype=torch.float64).pin_memory()
+    qh = torch.empty_like(fh).pin_memory()
+    fdev = torch.empty_like(fd)
+    qdev = torch.empty_like(fd)
+
+    def e2e_step():
+        fdev.copy_(fh, non_blocking=True)
+        qdev.zero_()
+        op32.eval(fdev, qdev)
+        qh.copy_(qdev, non_blocking=True)
+
+    ms_e2e = timed(e2e_step, args.steps, args.warmup)
+
+    # per-kernel durations inside the timed region: CUDA events recorded by
+    # the library on the launching stream between its kernels
+    from dgfs1d_gpu_b200 import _native as nat
+    import ctypes
+    nat.check(nat.lib().dgfs_vhs_profile(op32._h, 1))
+    stage = np.zeros(5)
+    buf = (ctypes.c_double * 5)()
+    for _ in range(args.warmup):
+        op32.eval(fd, Q)
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        op32.eval(fd, Q)
+        nat.check(nat.lib().dgfs_vhs_stage_ms(op32._h, buf))
+        stage += np.array(buf[:])
+    stage /= args.steps
+    nat.check(nat.lib().dgfs_vhs_profile(op32._h, 0))
+    terms_ms = float(stage[3])
+
+    fma_peak = fp32_fma_peak(torch)
+
+    barrier()
+    if rank == 0:
+        peaks = {}
+        pth = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+        if os.path.exists(pth):
+            peaks = json.load(open(pth))
+        hbm_peak = peaks.get('hbm_gbs', 6650.0)
+        peak_src = 'measured' if 'hbm_gbs' in peaks else 'fallback'
+        n = 32 ** 3
+        Nrho, Mu = 16, 6
+        # terms kernel, per launch: read F_g (n complex FP32) per eval and
+        # b1w (Nrho*n FP32) once, write H (Nrho*n complex FP32) per eval
+        alg_bytes = E * (n * 8 + Nrho * n * 8) + Nrho * n * 4
+        # algorithmic flops of the terms kernel per eval: 2*Mu*Nrho inverse
+        # and Nrho forward 3-D FFTs (5 n log2 n each) + pointwise combine
+        fft = 5 * n * np.log2(n)
+        alg_flops = E * ((2 * Mu * Nrho + Nrho) * fft + 2 * Mu * Nrho * n * 30)
+        evals = E * world
+        traffic = None
+        tp = os.path.join(ROOT, 'profiles', 'vhs_terms_fp32_traffic.json')
+        if os.path.exists(tp):
+            traffic = json.load(open(tp)).get('bytes_per_launch_24_evals')
+        cores = os.cpu_count() or 1
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            rate, ns, dt = cpu_oracle_rate(prm, f, budget_s=12.0,
+                                           max_evals=3)
+            cpu = {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+                   'sample': f'{ns} single-point evals ({dt:.1f} s) of the '
+                             'NumPy/SciPy oracle of this workload '
+                             f'(complex128, scipy.fft workers={cores})'}
+        line = {
+            'metric': METRIC,
+            'value': evals / (ms32 * 1e-3),
+            'unit': UNIT,
+            'n_gpus': world,
+            'steps': args.steps,
+            'warmup': args.warmup,
+            'ms_per_step': ms32,
+            'higher_is_better': True,
+            'scaling': 'weak',
+            'vs_baseline': None,
+            'dtype': 'f32',
+            'data': 'synthetic',
+            'config': dict(WORKLOAD, parallelism=f'points-sharded x{world}',
+                           l2='flushed between timed steps (256 MB write)'),
+            'fp64_plain': {'value': evals / (ms64 * 1e-3), 'unit': UNIT,
+                           'ms_per_step': ms64},
+            'speedup_fp32_vs_fp64': ms64 / ms32,
+            'err_fp32_vs_fp64_rel_l2': err,
+            'e2e': {'value': evals / (ms_e2e * 1e-3), 'unit': UNIT,
+                    'h2d_bytes_per_step': int(fh.numel() * 8),
+                    'd2h_bytes_per_step': int(qh.numel() * 8)},
+            'roofline': {'bound': 'hbm', 'kernel': 'vhs_terms_kernel<float,32,4>',
+                         'achieved': alg_bytes / (terms_ms * 1e-3) / 1e9,
+                         'peak': hbm_peak, 'unit': 'GB/s',
+                         'frac': alg_bytes / (terms_ms * 1e-3) / 1e9 / hbm_peak,
+                         'traffic': traffic, 'peak_source': peak_src,
+                         'launch_ms': terms_ms},
+            'roofline_fp32': {'bound': 'fp32-fma',
+                              'achieved': alg_flops / (terms_ms * 1e-3) / 1e12,
+                              'peak': fma_peak, 'unit': 'TFLOP/s',
+                              'frac': alg_flops / (terms_ms * 1e-3) / 1e12 / fma_peak,
+                              'peak_source': 'measured by dgfs_fma_peak'},
+            'stage_ms': dict(zip(['prologue', 'tables', 'maxwell_gain',
+                                  'terms', 'epilogue'],
+                                 [round(float(x), 4) for x in stage])),
+            'cpu_baseline': cpu,
+            'clocks': clk.summary(),
+            'gpu_launches': 5 * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -57,6 +57,11 @@ _SIGNATURES = [
       ctypes.c_void_p]),
     ('dgfs_vhs_last_moments', ctypes.c_void_p, [ctypes.c_void_p]),
     ('dgfs_vhs_destroy', ctypes.c_int, [ctypes.c_void_p]),
+    ('dgfs_vhs_profile', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ('dgfs_vhs_stage_ms', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ('dgfs_fma_peak', ctypes.c_int,
+     [ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
 ]
 
 

@@ -133,6 +133,10 @@ struct dgfs_vhs_s {
   void* uv = nullptr;        // [E][Nrho][Mu][2][3][N] R
   double2* hh = nullptr;     // [E][Nrho][Mu][3][N]
   double2* GM = nullptr;     // [E][n]
+  // optional per-kernel timing (events recorded between the launches)
+  bool profile = false;
+  cudaEvent_t ev[6] = {};
+  int ev_used = 0;
 };
 
 // FP64-kernel and FP32-terms cluster sizes per N (shared memory per CTA
@@ -164,6 +168,8 @@ static void free_handle(dgfs_vhs_s* h) {
                   h->GM};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (cudaEvent_t e : h->ev)
+    if (e) cudaEventDestroy(e);
   delete h;
 }
 
@@ -333,6 +339,11 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
   using G32 = Geo<N, C32>;
   const bool fp32 = h->precision == DGFS_PREC_FP32;
   int rc;
+  int evi = 0;
+  auto mark = [&]() {
+    if (h->profile) cudaEventRecord(h->ev[evi++], st);
+  };
+  mark();
   // prologue
   {
     VhsPrologueArgs a{};
@@ -345,6 +356,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                              dim3(G64::NT), C64, smem, st, a)))
       return rc;
   }
+  mark();
   if (fp32) {
     VhsTablesArgs t{};
     t.mhat = h->mhat; t.kappa = h->kappa; t.uv = h->uv; t.hh = h->hh;
@@ -353,6 +365,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     if ((rc = launch_plain(vhs_tables_kernel<N>, dim3((total + 95) / 96),
                            dim3(96), 0, st, t)))
       return rc;
+    mark();
     VhsGainArgs g{};
     g.hh = h->hh; g.mult = h->mult; g.b1w = h->b1w64; g.GM = h->GM;
     g.Mu = h->Mu; g.Nrho = h->Nrho;
@@ -360,6 +373,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     if ((rc = launch_plain(vhs_maxwell_gain_kernel<N>, dim3(N, nevals),
                            dim3(256), smem, st, g)))
       return rc;
+    mark();
     VhsTermsArgs a{};
     a.Fg = h->Fg; a.ph = h->ph; a.uv = h->uv; a.mult = h->mult;
     a.b1w = h->b1w32; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
@@ -369,7 +383,9 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                              dim3(C32, h->Nrho, nevals), dim3(G32::NT), C32,
                              smem2, st, a)))
       return rc;
+    mark();
   } else {
+    mark(); mark();  // no tables / Maxwellian-gain stages in FP64 mode
     VhsTermsArgs a{};
     a.Fg = h->Fg; a.ph = h->ph; a.uv = nullptr; a.mult = h->mult;
     a.b1w = h->b1w64; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
@@ -379,6 +395,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                              dim3(C64, h->Nrho, nevals), dim3(G64::NT), C64,
                              smem, st, a)))
       return rc;
+    mark();
   }
   // epilogue
   {
@@ -393,6 +410,8 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                              dim3(G64::NT), C64, smem, st, a)))
       return rc;
   }
+  mark();
+  h->ev_used = evi;
   return DGFS_OK;
 }
 
@@ -434,4 +453,74 @@ extern "C" int dgfs_vhs_fs(dgfs_vhs_handle h, const void* f, void* Q,
     return fail(DGFS_ERR_INVALID, "bad Ne/elem/mode");
   return dgfs_vhs_eval(h, f, dtype, Q, dtype, nullptr, modein * Ne + elem,
                        nullptr, modeout * Ne + elem, 1, stream);
+}
+
+// ---------------------------------------------------------------------------
+// profiling helpers
+// ---------------------------------------------------------------------------
+extern "C" int dgfs_vhs_profile(dgfs_vhs_handle h, int32_t enable) {
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  if (enable && !h->ev[0])
+    for (auto& e : h->ev) DGFS_CUDA(cudaEventCreate(&e));
+  h->profile = enable != 0;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_stage_ms(dgfs_vhs_handle h, double* out5) {
+  if (!h || !out5) return fail(DGFS_ERR_INVALID, "null argument");
+  if (!h->profile || h->ev_used != 6)
+    return fail(DGFS_ERR_INVALID, "profiling was not enabled for the last call");
+  DGFS_CUDA(cudaEventSynchronize(h->ev[5]));
+  for (int i = 0; i < 5; ++i) {
+    float ms = 0.f;
+    DGFS_CUDA(cudaEventElapsedTime(&ms, h->ev[i], h->ev[i + 1]));
+    out5[i] = ms;
+  }
+  return DGFS_OK;
+}
+
+// FP32 fused multiply-add throughput of the current GPU (TFLOP/s), measured
+// with independent FMA chains on every SM; the roofline denominator of the
+// FFT-bound kernels.
+__global__ void __launch_bounds__(256) fma_peak_kernel(float* out, int iters) {
+  float a0 = threadIdx.x * 1e-3f, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3;
+  float a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
+  const float b = 0.999999f, c = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      a0 = fmaf(a0, b, c); a1 = fmaf(a1, b, c); a2 = fmaf(a2, b, c);
+      a3 = fmaf(a3, b, c); a4 = fmaf(a4, b, c); a5 = fmaf(a5, b, c);
+      a6 = fmaf(a6, b, c); a7 = fmaf(a7, b, c);
+    }
+  }
+  const float s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 12345.678f) out[0] = s;  // keep the chains alive
+}
+
+extern "C" int dgfs_fma_peak(double* tflops, void* stream) {
+  if (!tflops) return fail(DGFS_ERR_INVALID, "null output");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int dev = 0, sms = 0;
+  DGFS_CUDA(cudaGetDevice(&dev));
+  DGFS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  float* out = nullptr;
+  DGFS_CUDA(cudaMalloc(&out, sizeof(float)));
+  const int iters = 4096, blocks = sms * 8, threads = 256;
+  cudaEvent_t e0, e1;
+  DGFS_CUDA(cudaEventCreate(&e0));
+  DGFS_CUDA(cudaEventCreate(&e1));
+  fma_peak_kernel<<<blocks, threads, 0, st>>>(out, iters / 8);  // warm-up
+  DGFS_CUDA(cudaEventRecord(e0, st));
+  fma_peak_kernel<<<blocks, threads, 0, st>>>(out, iters);
+  DGFS_CUDA(cudaEventRecord(e1, st));
+  DGFS_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  DGFS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return DGFS_OK;
 }

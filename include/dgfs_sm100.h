@@ -96,6 +96,18 @@ const double* dgfs_vhs_last_moments(dgfs_vhs_handle h);
 
 int dgfs_vhs_destroy(dgfs_vhs_handle h);
 
+/* Profiling (no reference counterpart: the reference times whole runs with
+ * timeit, std/std.py:394-423).  When enabled, dgfs_vhs_eval records CUDA
+ * events on its stream between its five kernels; dgfs_vhs_stage_ms waits
+ * for the last call and returns the durations in ms of: prologue, tables,
+ * Maxwellian gain, terms, epilogue (zero for stages the mode skips). */
+int dgfs_vhs_profile(dgfs_vhs_handle h, int32_t enable);
+int dgfs_vhs_stage_ms(dgfs_vhs_handle h, double* out5);
+
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (the
+ * roofline denominator of the CUDA-core FFT kernels). */
+int dgfs_fma_peak(double* tflops, void* stream);
+
 /* Library identification and error reporting. */
 const char* dgfs_version(void);
 const char* dgfs_last_error_string(void);

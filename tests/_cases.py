@@ -1,6 +1,5 @@
 """Shared seeded test cases (velocity meshes, distributions) for the tests."""
-import numpy as np
-
+from dgfs1d_gpu_b200.workloads import couette_distributions, vhs_mesh_params
 from oracle.collision import VHSTables
 from oracle.mesh import VelocityMeshStd, vhs_prefactor
 
@@ -9,18 +8,11 @@ SEED = 20261203
 
 def vhs_case(N, M, Nrho, dev, full_sphere, omega=0.81, nslots=1, noise=0.01,
              seed=SEED):
+    """Oracle mesh, prefactor, gamma and seeded distributions."""
     vm = VelocityMeshStd(Nv=N, M=M, Nrho=Nrho, dev=dev, full_sphere=full_sphere)
     invKn, prefac = vhs_prefactor(vm, omega, 4.17e-10, 273.)
     gamma = 2.0 * (1 - omega)
-    rng = np.random.default_rng(seed)
-    f = np.empty((nslots, N ** 3))
-    cv = vm.cv
-    for s in range(nslots):
-        uy = rng.uniform(-0.1, 0.1)
-        T = rng.uniform(0.95, 1.05)
-        m = np.exp(-(cv[0] ** 2 + (cv[1] - uy) ** 2 + cv[2] ** 2) / T) \
-            / (np.pi * T) ** 1.5
-        f[s] = m * (1 + noise * rng.uniform(-1, 1, m.shape))
+    f = couette_distributions(vm.cv[2, :N], nslots, noise=noise, seed=seed)
     return vm, prefac, gamma, f
 
 
