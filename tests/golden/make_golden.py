@@ -1,0 +1,455 @@
+"""Generate the golden vectors of tests/golden from the reference itself.
+
+Run in a container where the reference checkout exists (``$DGFS_REF``,
+default /root/reference)::
+
+    python tests/golden/make_golden.py
+
+What runs from the reference:
+  * its pure-Python setup code, imported directly with stand-ins for the
+    GPU/MPI packages it imports but that this setup does not use (pycuda,
+    mpi4py, gimmik, the cuFFT/cuBLAS ctypes bindings): quadratures,
+    spherical-design loading, velocity meshes, the VHS/VSS prefactors
+    (load_parameters) and the nodal DG bases;
+  * its Mako CUDA kernels, rendered and compiled for the CPU by
+    ``oracle/ref_build.py``, driven in the exact call sequence of
+    ``DGFSVHSGLLScatteringModelStd.fs``, ``DGFSVHSScatteringModelStd.fs`` and
+    ``DGFSBiVSSScatteringModel.fs``; the cuFFT calls of those sequences are
+    replaced by pocketfft with cuFFT's conventions (cuFFT is a closed library
+    with no CPU build).
+
+Inputs are seeded; outputs are written as small .npz files beside this script.
+"""
+import configparser
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+REF = os.environ.get('DGFS_REF', '/root/reference')
+SEED = 20261203
+
+
+# -- stand-ins for modules the setup code imports but does not use -----------
+
+def _install_stubs():
+    def mod(name, **attrs):
+        m = types.ModuleType(name)
+        m.__dict__.update(attrs)
+        sys.modules[name] = m
+        return m
+
+    class _Arr(np.ndarray):
+        pass
+
+    def to_gpu(a):
+        return np.asarray(a)
+
+    gpuarray = mod('pycuda.gpuarray', to_gpu=to_gpu, empty=np.empty,
+                   zeros=np.zeros, empty_like=np.empty_like,
+                   GPUArray=np.ndarray)
+    compiler = mod('pycuda.compiler', SourceModule=lambda *a, **k: None)
+    driver = mod('pycuda.driver', func_cache=types.SimpleNamespace(
+        PREFER_L1=None), memcpy_dtod=lambda *a: None)
+    mod('pycuda', gpuarray=gpuarray, compiler=compiler, driver=driver)
+
+    class _Comm:
+        rank, size = 0, 1
+
+        def Get_rank(self):
+            return 0
+
+        def Get_size(self):
+            return 1
+
+    mpi = types.SimpleNamespace(COMM_WORLD=_Comm(), PROC_NULL=-1)
+    mod('mpi4py', MPI=mpi, rc=types.SimpleNamespace(initialize=False))
+    mod('mpi4py.MPI', COMM_WORLD=mpi.COMM_WORLD, PROC_NULL=-1)
+    mod('mpi4py.rc', initialize=False)
+    mod('gimmik', generate_mm=lambda *a, **k: '')
+
+    class _Lookup:
+        def __init__(self, *a, **k):
+            pass
+
+    class _Template:
+        def __init__(self, *a, **k):
+            pass
+
+    mako = mod('mako')
+    mako.lookup = mod('mako.lookup', TemplateLookup=_Lookup)
+    mako.template = mod('mako.template', Template=_Template)
+    for name in ('cufft', 'cublas', 'cusolver', 'cusparse'):
+        m = mod('dgfs1D.' + name)
+        m.__getattr__ = lambda attr: (lambda *a, **k: None)
+    # Python 3.12 removed the deprecated alias the reference imports
+    configparser.SafeConfigParser = configparser.ConfigParser
+
+
+def _import_reference():
+    _install_stubs()
+    sys.path.insert(0, REF)
+    import dgfs1D.nputil as nputil
+    nputil.get_comm_rank_root = lambda: (sys.modules['mpi4py'].MPI.COMM_WORLD,
+                                         0, 0)
+    from dgfs1D import quadratures, basis, dictionary  # noqa: F401
+    import dgfs1D.util as util
+    util.get_mm_kernel = lambda *a, **k: None
+    import dgfs1D.basis as basis
+    basis.get_mm_kernel = lambda *a, **k: None
+    from dgfs1D.std import velocitymesh as vstd
+    from dgfs1D.bi import velocitymesh as vbi
+    from dgfs1D.std import scattering as sstd
+    from dgfs1D.bi import scattering as sbi
+    # the module re-binds the class name DGFSVHSGLLScatteringModelStd later
+    # (std/scattering.py:708-741); resolve the model as the drivers do
+    vhsgll = nputil.subclass_where(sstd.DGFSScatteringModelStd,
+                                   scattering_model='vhs-gll')
+    return types.SimpleNamespace(quadratures=quadratures, basis=basis,
+                                 Dictionary=dictionary.Dictionary, vstd=vstd,
+                                 vbi=vbi, sstd=sstd, sbi=sbi, VHSGLL=vhsgll)
+
+
+STD_INI = """
+[config]
+precision = double
+[mesh]
+xlo = 0.
+xhi = 1e-3
+Ne = 4
+H0 = 1e-3
+[basis]
+kind = {basis}
+K = 3
+Nqr = 8
+[non-dim]
+T0 = 273
+rho0 = 0.00023
+molarMass0 = 39.96e-3
+[velocity-mesh]
+Nv = {Nv}
+Nrho = {Nrho}
+dev = {dev}
+cmax = 0
+Tmax = 273
+[spherical-design-rule]
+ssrule = womersley
+M = {M}
+[scattering-model]
+type = vhs-gll
+omega = 0.81
+dRef = 4.17e-10
+Tref = 273
+muRef = 2.117e-5
+"""
+
+BI_INI = """
+[config]
+precision = double
+[mesh]
+xlo = 0.
+xhi = 1e-3
+Ne = 2
+H0 = 1e-3
+[non-dim]
+T0 = 273
+rho0 = 0.00011140244750324529
+molarMass0 = 39.96e-3
+[velocity-mesh]
+nspcs = 2
+Nv = {Nv}
+Nrho = {Nrho}
+dev = {dev}
+cmax = 0
+Tmax = 273
+molarMass1 = 39.96e-3
+molarMass2 = 83.77e-3
+[spherical-design-rule]
+ssrule = womersley
+M = {M}
+[scattering-model]
+type = vss
+ssrulepre = womersley
+Mpre = {Mpre}
+alpha00 = 1.4
+omega00 = 0.81
+dRef00 = 4.11e-10
+Tref00 = 273
+alpha01 = 1.36
+omega01 = 0.805
+dRef01 = 4.405e-10
+Tref01 = 273
+alpha10 = 1.36
+omega10 = 0.805
+dRef10 = 4.405e-10
+Tref10 = 273
+alpha11 = 1.32
+omega11 = 0.80
+dRef11 = 4.7e-10
+Tref11 = 273
+"""
+
+
+def _fwd(x):
+    """CUFFT_FORWARD on the last three axes (batched like cufftPlanMany)."""
+    return np.fft.fftn(x, axes=(-3, -2, -1))
+
+
+def _inv(x):
+    """CUFFT_INVERSE (unnormalised) on the last three axes."""
+    n = x.shape[-1] * x.shape[-2] * x.shape[-3]
+    return np.fft.ifftn(x, axes=(-3, -2, -1)) * n
+
+
+def _maxwellian_noise(cv, rng, rho=1.0, noise=0.02):
+    uy, T = rng.uniform(-0.1, 0.1), rng.uniform(0.9, 1.1)
+    m = rho * np.exp(-(cv[0] ** 2 + (cv[1] - uy) ** 2 + cv[2] ** 2) / T) \
+        / (np.pi * T) ** 1.5
+    return m * (1 + noise * rng.uniform(-1, 1, m.shape))
+
+
+def golden_vhs(R, Nv=8, Nrho=4, M=6, dev=5.0, Ne=3):
+    """Reference kernels of vhs-gll / vhs, driven like fs()."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    cfg = R.Dictionary(STD_INI.format(basis='nodal-sem-gll', Nv=Nv,
+                                      Nrho=Nrho, M=M, dev=dev))
+    vm = R.vstd.DGFSVelocityMeshStd(cfg)
+    sm = object.__new__(R.VHSGLL)
+    sm.cfg, sm.vm, sm._Ne = cfg, vm, Ne
+    sm.load_parameters()
+    vsize, N = vm.vsize(), vm.Nv()
+    l0 = np.concatenate((np.arange(0, N / 2), np.arange(-N / 2, 0)))
+    l = np.zeros((3, vsize))
+    for idv in range(vsize):
+        l[0, idv] = l0[idv // (N * N)]
+        l[1, idv] = l0[(idv % (N * N)) // N]
+        l[2, idv] = l0[(idv % (N * N)) % N]
+    src = render_template(
+        'dgfs1D/std/kernels/scattering/vhs-gll.mako', dtype='double',
+        Nrho=Nrho, M=vm.M(), vsize=vsize, sw=vm.sw(), prefac=sm._prefactor,
+        qw=vm.qw(), sz=vm.sz(), gamma=sm._gamma, L=vm.L(), qz=vm.qz(),
+        Ne=Ne, block_size=128, cw=vm.cw())
+    K = RefModule(src, tag='vhs-gll')
+    blk = 128
+    g = grid_for(vsize, blk)
+    lx, ly, lz = (np.ascontiguousarray(l[i]) for i in range(3))
+    aa = np.empty(Nrho * M * vsize)
+    K.launch('precompute_aa', g, blk, lx, ly, lz, aa)
+    bb1, bb2 = np.empty(Nrho * vsize), np.empty(vsize)
+    K.launch('precompute_bb', g, blk, lx, ly, lz, bb1, bb2)
+
+    rng = np.random.default_rng(SEED)
+    Kb = 2  # modes
+    f = np.stack([_maxwellian_noise(vm.cv(), rng) for _ in range(Kb * Ne)])
+    gfun = np.stack([_maxwellian_noise(vm.cv(), rng) for _ in range(Kb * Ne)])
+    f = np.ascontiguousarray(f.ravel())
+    gfun = np.ascontiguousarray(gfun.ravel())
+
+    def cplx(n):
+        return np.zeros(n, dtype=np.complex128)
+
+    shape = (N, N, N)
+    Qgll = np.zeros(Kb * Ne * vsize)
+    Qvhs = np.zeros(Kb * Ne * vsize)
+    for m in range(Kb):
+        for e in range(Ne):
+            # DGFSVHSGLLScatteringModelStd.fs (std/scattering.py:251-313)
+            fC = cplx(vsize)
+            K.launch('r2z_', g, blk, e, m, f, fC)
+            FTf = _fwd(fC.reshape(shape)).ravel()
+            t1, t2 = cplx(Nrho * M * vsize), cplx(Nrho * M * vsize)
+            K.launch('cosSinMul', g, blk, aa, FTf, t1, t2)
+            t3 = _inv(t1.reshape(-1, *shape)).ravel()
+            t4 = _inv(t2.reshape(-1, *shape)).ravel()
+            K.launch('magSqr', g, blk, t3, t4, t2)
+            t1 = _fwd(t2.reshape(-1, *shape)).ravel()
+            K.launch('computeQG', g, blk, bb1, t1, fC)
+            QG = _inv(fC.reshape(shape)).ravel()
+            K.launch('ax', g, blk, bb2, FTf)
+            fC = _inv(FTf.reshape(shape)).ravel()
+            K.launch('output_append_', g, blk, e, m, m, QG, fC, f, Qgll)
+            # DGFSVHSScatteringModelStd.fs (std/scattering.py:346-429)
+            fC, gC = cplx(vsize), cplx(vsize)
+            K.launch('r2z_', g, blk, e, m, f, fC)
+            K.launch('r2z_', g, blk, e, m, gfun, gC)
+            FTf = _fwd(fC.reshape(shape)).ravel()
+            FTg = _fwd(gC.reshape(shape)).ravel()
+            t1, t2 = cplx(Nrho * M * vsize), cplx(Nrho * M * vsize)
+            K.launch('cosMul', g, blk, aa, FTf, FTg, t1, t2)
+            t3 = _inv(t1.reshape(-1, *shape)).ravel()
+            t4 = _inv(t2.reshape(-1, *shape)).ravel()
+            t5 = cplx(Nrho * M * vsize)
+            K.launch('cplxMul', g, blk, t3, t4, t5)
+            K.launch('sinMul', g, blk, aa, FTf, FTg, t1, t2)
+            t3 = _inv(t1.reshape(-1, *shape)).ravel()
+            t4 = _inv(t2.reshape(-1, *shape)).ravel()
+            K.launch('cplxMulAdd', g, blk, t3, t4, t5)
+            t1 = _fwd(t5.reshape(-1, *shape)).ravel()
+            fC = cplx(vsize)
+            K.launch('computeQG', g, blk, bb1, t1, fC)
+            QG = _inv(fC.reshape(shape)).ravel()
+            K.launch('ax', g, blk, bb2, FTg)
+            fC = _inv(FTg.reshape(shape)).ravel()
+            K.launch('output_append_', g, blk, e, m, m, QG, fC, f, Qvhs)
+    return dict(Nv=Nv, Nrho=Nrho, M=M, Ne=Ne, L=vm.L(), qz=vm.qz(),
+                qw=vm.qw(), sz=vm.sz(), sw=vm.sw(), cw=vm.cw(), cv=vm.cv(),
+                prefac=sm._prefactor, gamma=sm._gamma, aa=aa, bb1=bb1,
+                bb2=bb2, f=f, g=gfun, Q_vhs_gll=Qgll, Q_vhs=Qvhs,
+                prefacBGK=sm._prefactorBGK)
+
+
+def golden_vss(R, Nv=8, Nrho=4, M=6, Mpre=12, dev=5.0, Ne=2):
+    """Reference kernels of vss, driven like DGFSBiVSSScatteringModel.fs."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    cfg = R.Dictionary(BI_INI.format(Nv=Nv, Nrho=Nrho, M=M, Mpre=Mpre,
+                                     dev=dev))
+    vm = R.vbi.DGFSVelocityMeshBi(cfg)
+    sm = object.__new__(R.sbi.DGFSBiVSSScatteringModel)
+    sm.cfg, sm.vm, sm._Ne, sm._nspcs = cfg, vm, Ne, vm.nspcs()
+    sm.load_parameters()
+    vsize, N = vm.vsize(), vm.Nv()
+    l0 = np.concatenate((np.arange(0, N / 2, dtype=np.int32),
+                         np.arange(-N / 2, 0, dtype=np.int32)))
+    l = np.zeros((3, vsize), dtype=np.int32)
+    for idv in range(vsize):
+        l[0, idv] = l0[idv // (N * N)]
+        l[1, idv] = l0[(idv % (N * N)) // N]
+        l[2, idv] = l0[(idv % (N * N)) % N]
+    sz, qz, qw, sw = vm.sz(), vm.qz(), vm.qw(), vm.sw()
+    src = render_template(
+        'dgfs1D/bi/kernels/scattering/vss.mako', dtype='double', Nrho=Nrho,
+        M=M, vsize=vsize, sw=sw, prefac=sm._prefactor, cases=sm._cases,
+        masses=vm.masses(), qw=qw, qz=qz, L=vm.L(), sz=sz, gamma=sm._gamma,
+        eta=sm._eta, Mpre=sm._Mpre, szpre=sm._szpre, swpre=sm._swpre)
+    K = RefModule(src, tag='vss')
+    blk = 256
+    g = grid_for(vsize, blk)
+    lx, ly, lz = (np.ascontiguousarray(l[i]) for i in range(3))
+    aa = np.empty(Nrho * M * vsize)
+    K.launch('precompute_a', g, blk, lx, ly, lz, aa)
+    szx, szy, szz = (np.ascontiguousarray(sz[:, i]) for i in range(3))
+    bb, cc = {}, {}
+    for cp, cq in sm._cases:
+        pq = f'{cp}{cq}'
+        bb[pq] = np.empty(Nrho * M * vsize, dtype=np.complex128)
+        cc[pq] = np.zeros(vsize, dtype=np.complex128)
+        for p in range(Nrho):
+            fac = np.pi / vm.L() * qz[p]
+            fac_b = sm._swpre * pow(qz[p], sm._gamma[pq] + 2)
+            fac_c = qw[p] * sw * fac_b
+            for q in range(M):
+                K.launch('precompute_bc_' + pq, g, blk, p, q, float(fac),
+                         float(fac_b), float(fac_c), lx, ly, lz, szx, szy,
+                         szz, bb[pq], cc[pq])
+    rng = np.random.default_rng(SEED + 1)
+    Kb = 2
+    fs = []
+    for sp in range(2):
+        rho = [0.5, 0.5][sp]
+        fs.append(np.ascontiguousarray(np.stack(
+            [_maxwellian_noise(vm.cv(), rng, rho=rho) for _ in range(Kb * Ne)]
+        ).ravel()))
+    shape = (N, N, N)
+
+    def cplx(n):
+        return np.zeros(n, dtype=np.complex128)
+
+    Q = {pq: np.zeros(Kb * Ne * vsize) for pq in bb}
+    for cp, cq in sm._cases:
+        pq = f'{cp}{cq}'
+        for m in range(Kb):
+            for e in range(Ne):
+                f1C, f2C = cplx(vsize), cplx(vsize)
+                K.launch('r2z', g, blk, Ne, e, m, fs[cp], f1C)
+                K.launch('r2z', g, blk, Ne, e, m, fs[cq], f2C)
+                FTf = _fwd(f1C.reshape(shape)).ravel()
+                FTg = _fwd(f2C.reshape(shape)).ravel()
+                t1, t2 = cplx(Nrho * M * vsize), cplx(Nrho * M * vsize)
+                K.launch('cosSinMul_' + pq, g, blk, aa, FTf, FTg, t1, t2)
+                t3 = _inv(t1.reshape(-1, *shape)).ravel()
+                t1 = _inv(t2.reshape(-1, *shape)).ravel()
+                K.launch('prod', g, blk, t3, t1, t2)
+                t1 = _fwd(t2.reshape(-1, *shape)).ravel()
+                # computeQG writes QG[idx] also for idx >= vsize
+                # (vss.mako:240); give it a grid-sized buffer
+                QGh = cplx(g * blk)
+                K.launch('computeQG', g, blk, bb[pq], t1, QGh)
+                QG = _inv(QGh[:vsize].reshape(shape)).ravel()
+                K.launch('ax2', g, blk, cc[pq], FTg, FTf)
+                f2C = _inv(FTf.reshape(shape)).ravel()
+                K.launch('output_' + pq, g, blk, Ne, e, m, m, QG, f2C,
+                         fs[cp], Q[pq])
+    out = dict(Nv=Nv, Nrho=Nrho, M=M, Mpre=Mpre, Ne=Ne, L=vm.L(),
+               qz=qz, qw=qw, sz=sz, sw=sw, szpre=sm._szpre, cw=vm.cw(),
+               cv=vm.cv(), masses=np.array(vm.masses()), f0=fs[0], f1=fs[1],
+               aa=aa)
+    for pq in bb:
+        out['prefac' + pq] = sm._prefactor[pq]
+        out['gamma' + pq] = sm._gamma[pq]
+        out['eta' + pq] = sm._eta[pq]
+        out['b' + pq] = bb[pq]
+        out['c' + pq] = cc[pq]
+        out['Q' + pq] = Q[pq]
+    return out
+
+
+def golden_setup(R):
+    """Velocity meshes, rules and DG bases from the reference setup code."""
+    out = {}
+    for Nv, Nrho, M, dev in [(16, 8, 6, 5.0), (32, 16, 16, 6.0),
+                             (24, 12, 6, 5.0)]:
+        cfg = R.Dictionary(STD_INI.format(basis='nodal-sem-gll', Nv=Nv,
+                                          Nrho=Nrho, M=M, dev=dev))
+        vm = R.vstd.DGFSVelocityMeshStd(cfg)
+        sm = object.__new__(R.VHSGLL)
+        sm.cfg, sm.vm = cfg, vm
+        sm.load_parameters()
+        key = f'std_N{Nv}_M{M}_R{Nrho}'
+        out[key + '_L'] = vm.L()
+        out[key + '_qz'] = vm.qz()
+        out[key + '_qw'] = vm.qw()
+        out[key + '_sz'] = vm.sz()
+        out[key + '_sw'] = vm.sw()
+        out[key + '_cw'] = vm.cw()
+        out[key + '_c0'] = vm.cv()[2, :Nv]
+        out[key + '_prefac'] = sm._prefactor
+    for kind in ('nodal-sem-gll', 'nodal-gll'):
+        cfg = R.Dictionary(STD_INI.format(basis=kind, Nv=8, Nrho=4, M=6,
+                                          dev=5.0))
+        cls = {'nodal-sem-gll': R.basis.NodalSemGLL,
+               'nodal-gll': R.basis.NodalGLL}[kind]
+        b = cls(cfg)
+        key = 'basis_' + kind.replace('-', '_')
+        out[key + '_z'] = b.z
+        out[key + '_gLD'] = np.asarray(b.gLD)
+        out[key + '_gRD'] = np.asarray(b.gRD)
+        out[key + '_derivMat'] = b.derivMat
+        out[key + '_interpMat'] = b.interpMat
+        out[key + '_U'] = np.stack(b._U)
+        out[key + '_V'] = np.stack(b._V)
+        out[key + '_sigModes'] = np.array([list(s) for s in b.sigModes])
+        out[key + '_Bqf'] = b._Bqf
+    for n in (2, 3, 4, 6, 8, 12, 16, 24):
+        z, w = R.quadratures.zwgj(n, 0., 0.)
+        out[f'zwgj_{n}_z'], out[f'zwgj_{n}_w'] = z, w
+        z, w = R.quadratures.zwglj(n, 0., 0.)
+        out[f'zwglj_{n}_z'], out[f'zwglj_{n}_w'] = z, w
+    return out
+
+
+def main():
+    R = _import_reference()
+    np.savez_compressed(os.path.join(HERE, 'setup.npz'), **golden_setup(R))
+    np.savez_compressed(os.path.join(HERE, 'vhs_N8.npz'), **golden_vhs(R))
+    np.savez_compressed(os.path.join(HERE, 'vss_N8.npz'), **golden_vss(R))
+    for fn in sorted(os.listdir(HERE)):
+        if fn.endswith('.npz'):
+            print(fn, os.path.getsize(os.path.join(HERE, fn)), 'bytes')
+
+
+if __name__ == '__main__':
+    main()

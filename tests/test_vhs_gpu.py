@@ -90,3 +90,26 @@ def test_float32_arrays(lib):
     for s in range(2):
         ref = vhs_gll_fs(tab, prefac, f[s].astype(np.float32).astype(np.float64))
         assert _rel(Q.cpu().numpy()[s].astype(np.float64), ref) < FP32_TOL
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_matches_reference_kernel_golden(lib, precision):
+    """CUDA path vs the reference's own kernels (tests/golden/vhs_N8.npz)."""
+    import os
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    g = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'vhs_N8.npz'))
+    N = int(g['Nv'])
+    op = VHSOperator(N=N, L=float(g['L']), qz=g['qz'], qw=g['qw'], sz=g['sz'],
+                     sw=float(g['sw']), sphere_factor=2.0,
+                     gamma=float(g['gamma']), prefac=float(g['prefac']),
+                     cw=float(g['cw']), c0=g['cv'][2, :N], precision=precision,
+                     max_evals=8)
+    f = torch.tensor(g['f'], device='cuda')
+    Q = torch.zeros_like(f)
+    op.eval(f, Q)
+    torch.cuda.synchronize()
+    tol = FP64_TOL if precision == 'fp64' else FP32_TOL
+    ref = g['Q_vhs_gll'].reshape(-1, N ** 3)
+    got = Q.cpu().numpy().reshape(-1, N ** 3)
+    for s in range(ref.shape[0]):
+        assert _rel(got[s], ref[s]) < tol, s
