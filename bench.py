@@ -73,6 +73,11 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        # wait for the first sample so the timed region is covered
+        import select
+        r, _, _ = select.select([self.proc.stdout], [], [], 5.0)
+        self.first = self.proc.stdout.readline() if r else ''
         return self
 
     def __exit__(self, *a):
@@ -85,7 +90,7 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
-        for line in out.strip().splitlines():
+        for line in (getattr(self, 'first', '') + out).strip().splitlines():
             parts = [p.strip() for p in line.split(',')]
             if len(parts) >= 8:
                 self.rows.append(parts)
@@ -153,7 +158,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='native', choices=['native', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
