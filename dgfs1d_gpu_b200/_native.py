@@ -62,6 +62,10 @@ _SIGNATURES = [
      [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ('dgfs_fma_peak', ctypes.c_int,
      [ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ('dgfs_vhs_eval_noalloc', ctypes.c_int,
+     [ctypes.POINTER(VhsDesc), ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_void_p]),
 ]
 
 

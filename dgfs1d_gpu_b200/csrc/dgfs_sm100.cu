@@ -524,3 +524,223 @@ extern "C" int dgfs_fma_peak(double* tflops, void* stream) {
   *tflops = flops / (ms * 1e-3) / 1e12;
   return DGFS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free VHS evaluation.
+//
+// For callers that cannot allocate device memory -- code running while a
+// CUDA stream is being captured into a graph by someone else, hosts whose
+// memory is owned by a pool they must not grow, or plugins loaded into a
+// process that forbids cudaMalloc after start-up.  All scratch of the FP64
+// evaluation (tables and per-evaluation buffers) lives in one file-scope
+// device array of kNoallocBytes; every GPU that loads this library holds it
+// until the process exits.  The array is shared by every call: two calls
+// whose kernels overlap on the GPU (different streams, no ordering) race on
+// it.  Nothing in it needs to start at zero: each call rebuilds the tables
+// and every buffer is fully written before it is read.
+// ---------------------------------------------------------------------------
+static constexpr size_t kNoallocBytes = size_t(16) << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+static constexpr int kNoallocMaxNrho = 48;
+static constexpr int kNoallocMaxMu = 96;
+
+struct NoallocTableArgs {
+  double* b1w;       // [Nrho][n]
+  double* b2;        // [n]
+  double2* ph;       // [Nrho][Mu][3][N]
+  float* mult_out;   // [Mu]
+  double L, gamma, sw, sphere_factor, sinc_eps;
+  int Nrho, Mu;
+  double qz[kNoallocMaxNrho];
+  double qw[kNoallocMaxNrho];
+  double sz[kNoallocMaxMu * 3];  // unique directions
+  float mult[kNoallocMaxMu];     // their multiplicities
+};
+
+// b1 (weighted), b2 and the 1-D phase tables of vhs-gll.mako:43-99, built on
+// the device from the descriptor values carried in the kernel parameters.
+template <int N>
+__global__ void noalloc_tables_kernel(NoallocTableArgs a) {
+  constexpr int n = N * N * N;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  auto rep = [](int i) { return (double)((i < N / 2) ? i : i - N); };
+  if (gid < n) {
+    const int ix = gid / (N * N), iy = (gid / N) % N, iz = gid % N;
+    const double cS = sqrt(rep(ix) * rep(ix) + rep(iy) * rep(iy) +
+                           rep(iz) * rep(iz));
+    double bsum = 0.0;
+    for (int p = 0; p < a.Nrho; ++p) {
+      const double qz = a.qz[p];
+      const double s1 = M_PI / a.L * qz / 2. * cS + a.sinc_eps;
+      const double s2 = M_PI / a.L * qz * cS + a.sinc_eps;
+      const double b1 = pow(qz, a.gamma + 2.) * 4 * M_PI * (sin(s1) / s1);
+      a.b1w[(size_t)p * n + gid] = (a.sphere_factor * a.qw[p] * a.sw / n) * b1;
+      bsum += a.qw[p] * pow(qz, a.gamma + 2.) * 16 * M_PI * M_PI * (sin(s2) / s2);
+    }
+    a.b2[gid] = bsum;
+  }
+  if (gid < a.Mu) a.mult_out[gid] = a.mult[gid];
+  const int nph = a.Nrho * a.Mu * 3 * N;
+  if (gid < nph) {
+    const int l = gid % N, ax = (gid / N) % 3, u = (gid / (3 * N)) % a.Mu,
+              p = gid / (3 * N * a.Mu);
+    const double k = M_PI / a.L * a.qz[p] / 2. * a.sz[3 * u + ax];
+    double s, c;
+    sincos(k * rep(l), &s, &c);
+    a.ph[gid] = make_double2(c, s);
+  }
+}
+
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_ptr[64];  // device address per device id
+
+// Per-device set-up, done by the first call on each device: upload the FFT
+// twiddles from static host buffers and resolve the device address of the
+// scratch array (its name is only a host-side stand-in in host code).
+static int noalloc_setup(unsigned char** out) {
+  int dev = 0;
+  DGFS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(DGFS_ERR_INVALID, "device id out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    static double2 t64[kTwTotal];
+    static float2 t32[kTwTotal];
+    std::lock_guard<std::mutex> lk2(g_tw_mu);
+    if (!g_tw_done[dev]) {
+      for (int i = 0; i < kNumTw; ++i) {
+        const int nt = tw_size(i), off = tw_offset(nt);
+        for (int k = 0; k < nt; ++k) {
+          const long double ang = 2.0L * 3.141592653589793238462643383279502884L *
+                                  (long double)k / (long double)nt;
+          const double c = (double)std::cos(ang), s = -(double)std::sin(ang);
+          t64[off + k] = make_double2(c, s);
+          t32[off + k] = make_float2((float)c, (float)s);
+        }
+      }
+      DGFS_CUDA(cudaMemcpyToSymbol(c_tw64, t64, sizeof(t64)));
+      DGFS_CUDA(cudaMemcpyToSymbol(c_tw32, t32, sizeof(t32)));
+      g_tw_done[dev] = true;
+    }
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(DGFS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") +
+                                     cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return DGFS_OK;
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+extern "C" int dgfs_vhs_eval_noalloc(const dgfs_vhs_desc* d, const double* f,
+                                     double* Q, const int32_t* src_slots,
+                                     int32_t src_base, const int32_t* dst_slots,
+                                     int32_t dst_base, int32_t nevals,
+                                     void* stream) {
+  if (!d) return fail(DGFS_ERR_INVALID, "null descriptor");
+  if (nevals < 0 || src_base < 0 || dst_base < 0)
+    return fail(DGFS_ERR_INVALID, "negative nevals or slot base");
+  if (d->precision != DGFS_PREC_FP64)
+    return fail(DGFS_ERR_UNSUPPORTED, "the allocation-free path is FP64 only");
+  if (d->N != 8 && d->N != 16 && d->N != 32)
+    return fail(DGFS_ERR_UNSUPPORTED, "N must be 8, 16 or 32");
+  if (d->Nrho <= 0 || d->Nrho > kNoallocMaxNrho || d->M <= 0 ||
+      !d->qz || !d->qw || !d->sz)
+    return fail(DGFS_ERR_INVALID, "bad Nrho, M or rule arrays");
+  if (nevals == 0) return DGFS_OK;
+  if (!f || !Q) return fail(DGFS_ERR_INVALID, "null f or Q");
+
+  NoallocTableArgs ta{};
+  float* mult = ta.mult;
+  bool used[4 * kNoallocMaxMu] = {};
+  if (d->M > 4 * kNoallocMaxMu)
+    return fail(DGFS_ERR_CAPACITY, "M exceeds the allocation-free maximum");
+  int Mu = 0;
+  for (int q = 0; q < d->M; ++q) {
+    if (used[q]) continue;
+    used[q] = true;
+    float m = 1.f;
+    for (int r = q + 1; r < d->M; ++r)
+      if (!used[r] && d->sz[3 * r] == -d->sz[3 * q] &&
+          d->sz[3 * r + 1] == -d->sz[3 * q + 1] &&
+          d->sz[3 * r + 2] == -d->sz[3 * q + 2]) {
+        used[r] = true;
+        m = 2.f;
+        break;
+      }
+    if (Mu >= kNoallocMaxMu)
+      return fail(DGFS_ERR_CAPACITY, "too many sphere directions");
+    for (int a = 0; a < 3; ++a) ta.sz[3 * Mu + a] = d->sz[3 * q + a];
+    mult[Mu++] = m;
+  }
+  const int N = d->N, n = N * N * N, Nrho = d->Nrho;
+  // layout of the scratch array: tables, then per-evaluation buffers
+  const size_t b_b1w = align256(sizeof(double) * Nrho * n);
+  const size_t b_b2 = align256(sizeof(double) * n);
+  const size_t b_ph = align256(sizeof(double2) * Nrho * Mu * 3 * N);
+  const size_t b_mult = align256(sizeof(float) * Mu);
+  const size_t tables = b_b1w + b_b2 + b_ph + b_mult;
+  const size_t per_eval = align256(sizeof(double2) * n) +
+                          align256(sizeof(double2) * Nrho * n) +
+                          align256(sizeof(double) * n);
+  if (tables + per_eval > kNoallocBytes)
+    return fail(DGFS_ERR_CAPACITY,
+                "N=" + std::to_string(N) + ", Nrho=" + std::to_string(Nrho) +
+                    " needs " + std::to_string(tables + per_eval) +
+                    " bytes of scratch; the allocation-free maximum is " +
+                    std::to_string(kNoallocBytes));
+  const int E = (int)std::min<size_t>((kNoallocBytes - tables) / per_eval, 1024);
+
+  unsigned char* base = nullptr;
+  if (int rc = noalloc_setup(&base)) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+  // a handle that only points into the scratch array (nothing allocated)
+  dgfs_vhs_s h;
+  h.N = N; h.n = n; h.Nrho = Nrho; h.M = d->M; h.Mu = Mu;
+  h.precision = DGFS_PREC_FP64; h.max_evals = E;
+  h.prefac = d->prefac; h.cw = d->cw;
+  unsigned char* p = base;
+  h.b1w64 = reinterpret_cast<double*>(p); p += b_b1w;
+  h.b2 = reinterpret_cast<double*>(p); p += b_b2;
+  h.ph = p; p += b_ph;
+  h.mult = reinterpret_cast<float*>(p); p += b_mult;
+  h.Fg = p; p += align256(sizeof(double2) * n) * E;
+  h.H = p; p += align256(sizeof(double2) * Nrho * n) * E;
+  h.ReLf = reinterpret_cast<double*>(p);
+  // (the per-eval buffers above are contiguous [E][...] blocks: every
+  // per-eval size is already a multiple of 256 bytes for N >= 8)
+
+  ta.b1w = h.b1w64; ta.b2 = h.b2; ta.ph = static_cast<double2*>(h.ph);
+  ta.mult_out = h.mult;
+  ta.L = d->L; ta.gamma = d->gamma; ta.sw = d->sw;
+  ta.sphere_factor = d->sphere_factor; ta.sinc_eps = d->sinc_eps;
+  ta.Nrho = Nrho; ta.Mu = Mu;
+  for (int i = 0; i < Nrho; ++i) { ta.qz[i] = d->qz[i]; ta.qw[i] = d->qw[i]; }
+  const int work = std::max(std::max(n, Nrho * Mu * 3 * N), Mu);
+  int rc = DGFS_OK;
+  switch (N) {
+    case 8: rc = launch_plain(noalloc_tables_kernel<8>, dim3((work + 255) / 256), dim3(256), 0, st, ta); break;
+    case 16: rc = launch_plain(noalloc_tables_kernel<16>, dim3((work + 255) / 256), dim3(256), 0, st, ta); break;
+    default: rc = launch_plain(noalloc_tables_kernel<32>, dim3((work + 255) / 256), dim3(256), 0, st, ta); break;
+  }
+  if (rc) return rc;
+  for (int off = 0; off < nevals; off += E) {
+    const int cnt = std::min(E, nevals - off);
+    const int32_t* ss = src_slots ? src_slots + off : nullptr;
+    const int32_t* ds = dst_slots ? dst_slots + off : nullptr;
+    switch (N) {
+      case 8: rc = vhs_run<8>(&h, f, 1, Q, 1, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 16: rc = vhs_run<16>(&h, f, 1, Q, 1, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      default: rc = vhs_run<32>(&h, f, 1, Q, 1, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+    }
+    if (rc) break;
+  }
+  // the stack handle owns nothing: detach before it goes out of scope
+  h.c0 = h.b2 = h.b1w64 = h.ReLf = nullptr;
+  h.b1w32 = nullptr; h.ph = h.Fg = h.H = nullptr; h.mult = nullptr;
+  return rc;
+}

@@ -108,6 +108,25 @@ int dgfs_vhs_stage_ms(dgfs_vhs_handle h, double* out5);
  * roofline denominator of the CUDA-core FFT kernels). */
 int dgfs_fma_peak(double* tflops, void* stream);
 
+/* Allocation-free Q(f,f) in FP64, for callers that cannot allocate device
+ * memory (code running inside someone else's stream capture, processes whose
+ * device memory belongs to a pool they must not grow, plugins barred from
+ * cudaMalloc after start-up).  No counterpart in the reference.  Same
+ * semantics as creating a DGFS_PREC_FP64 handle from `desc` and calling
+ * dgfs_vhs_eval with double f and Q, but no handle is created and nothing is
+ * allocated: tables and scratch live in one static 16 MiB device array that
+ * the library holds on every GPU that loads it.  Limits: N in {8, 16, 32},
+ * Nrho <= 48, at most 96 sphere directions after merging antipodal pairs,
+ * and the tables plus one evaluation must fit in 16 MiB (N=32 with
+ * Nrho <= 16 does); larger shapes return DGFS_ERR_CAPACITY.  The first call
+ * on a device sets it up (twiddle upload, symbol lookup) -- make that call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race. */
+int dgfs_vhs_eval_noalloc(const dgfs_vhs_desc* desc, const double* f,
+                          double* Q, const int32_t* src_slots,
+                          int32_t src_base, const int32_t* dst_slots,
+                          int32_t dst_base, int32_t nevals, void* stream);
+
 /* Library identification and error reporting. */
 const char* dgfs_version(void);
 const char* dgfs_last_error_string(void);
