@@ -12,6 +12,7 @@
 #pragma once
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "fft_reg.cuh"
 
@@ -121,6 +122,29 @@ template <int N, int C>
 __device__ __forceinline__ int slab_index(int j) {
   using G = Geo<N, C>;
   return (j / (N * N)) * G::PLANE + ((j / N) % N) * G::ROW + (j % N);
+}
+
+}  // namespace dgfs
+
+namespace dgfs {
+
+// 32-bit shared-window addressing for distributed shared memory stores.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint32_t mapa_u32(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n"
+               : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_cluster(uint32_t addr, float2 v) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};\n"
+               :: "r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t addr, double2 v) {
+  asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};\n"
+               :: "r"(addr), "d"(v.x), "d"(v.y) : "memory");
 }
 
 }  // namespace dgfs

@@ -63,6 +63,7 @@ struct VhsTermsArgs {
 
 struct VhsTablesArgs {
   const double2* mhat;        // [nevals][3][N]
+  const float* mult;          // [Mu] (FP32 tables carry sqrt(mult) on axis x)
   const double* kappa;        // [Nrho][Mu][3] kappa_a = (pi/L)(rho_p/2) sigma_qa
   void* uv;                   // out [nevals][Nrho][Mu][2][3][N] precision R
   double2* hh;                // out [nevals][Nrho][Mu][3][N] FFT(u_a v_a)
@@ -294,10 +295,11 @@ __global__ void vhs_tables_kernel(VhsTablesArgs a) {
     }
   } else {
     float2* uv = static_cast<float2*>(a.uv) + tb * 6 * N;
+    const double sc = (ax == 0) ? sqrt((double)a.mult[q]) : 1.0;
 #pragma unroll
     for (int l = 0; l < N; ++l) {
-      uv[ax * N + l] = make_float2((float)u[l].x, (float)u[l].y);
-      uv[(3 + ax) * N + l] = make_float2((float)w[l].x, (float)w[l].y);
+      uv[ax * N + l] = make_float2((float)(sc * u[l].x), (float)(sc * u[l].y));
+      uv[(3 + ax) * N + l] = make_float2((float)(sc * w[l].x), (float)(sc * w[l].y));
     }
   }
 #pragma unroll
@@ -333,23 +335,34 @@ vhs_maxwell_gain_kernel(VhsGainArgs a) {
     }
     for (int i = t; i < a.Mu; i += blockDim.x) hx[i] = hh[(size_t)i * 3 * N + lx];
     __syncthreads();
+    double wk[PTS];
 #pragma unroll
     for (int k = 0; k < PTS; ++k) {
       const int pt = t + k * 256;
-      if (pt < N * N) {
+      wk[k] = pt < N * N
+                  ? a.b1w[(size_t)p * N * N * N + (size_t)lx * N * N + pt]
+                  : 0.0;
+    }
+    double2 acc[PTS];
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) acc[k] = make_double2(0, 0);
+    for (int q = 0; q < a.Mu; ++q) {
+      const double m = (double)a.mult[q];
+      const double2 hxq = make_double2(m * hx[q].x, m * hx[q].y);
+#pragma unroll
+      for (int k = 0; k < PTS; ++k) {
+        const int pt = min(t + k * 256, N * N - 1);
         const int ly = pt / N, lz = pt % N;
-        double2 acc = make_double2(0, 0);
-        for (int q = 0; q < a.Mu; ++q) {
-          const double m = (double)a.mult[q];
-          const double2 xy = cmul(hx[q], hyz[(size_t)q * 2 * N + ly]);
-          const double2 xyz = cmul(xy, hyz[(size_t)q * 2 * N + N + lz]);
-          acc.x += m * xyz.x;
-          acc.y += m * xyz.y;
-        }
-        const double w = a.b1w[(size_t)p * N * N * N + (size_t)lx * N * N + pt];
-        Gs[k].x += w * acc.x;
-        Gs[k].y += w * acc.y;
+        const double2 xy = cmul(hxq, hyz[(size_t)q * 2 * N + ly]);
+        const double2 xyz = cmul(xy, hyz[(size_t)q * 2 * N + N + lz]);
+        acc[k].x += xyz.x;
+        acc[k].y += xyz.y;
       }
+    }
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) {
+      Gs[k].x += wk[k] * acc[k].x;
+      Gs[k].y += wk[k] * acc[k].y;
     }
   }
 #pragma unroll
@@ -528,6 +541,197 @@ vhs_terms_kernel(VhsTermsArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Terms, FP32 Maxwellian-split path: one cluster per (eval, p), S_p in
+// registers, software-pipelined over the 2*Mu inverse transforms:
+//   y-pass(k) -> exchange(k) into receive buffer k%2 -> arrive
+//   -> [load F_g slab, z-pass(k+1)]  (overlaps the exchange latency)
+//   -> wait -> x-pass(k) + combine into S_p
+// Two receive buffers make one cluster barrier per transform sufficient: a
+// CTA stores into buffer k%2 of a peer only after the barrier of transform
+// k-1, which that peer joined after reading its buffer k%2 for transform k-2.
+// The multiplicity m_q is folded into the tables as sqrt(m_q) (on the x-phase
+// and on u_x, v_x), so S_p += X (2 X_M + X) carries it.
+// ---------------------------------------------------------------------------
+// Asynchronous copy of this CTA's F_g slab (global, dense) into the padded
+// X-slab A: 8-byte cp.async per complex element, one commit group.
+template <int N, int C>
+__device__ __forceinline__ void fp32_issue_slab_copy(float2* A,
+                                                     const float2* Fg, int t) {
+  using G = Geo<N, C>;
+  const uint32_t a0 = smem_u32(A);
+  constexpr int TOT = G::P * N * N;
+#pragma unroll 4
+  for (int j = t; j < TOT; j += G::NT) {
+    const uint32_t dst = a0 + (uint32_t)slab_index<N, C>(j) * 8u;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
+                 :: "r"(dst), "l"(Fg + j) : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+template <int N, int C>
+__device__ __forceinline__ void fp32_zpass(float2* A, const float2* tb, int s,
+                                           int t, unsigned rank) {
+  using G = Geo<N, C>;
+  const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
+  const float2 bxy = cmul(tb[lx], tb[N + ly]);
+  const int base = pl * G::PLANE + ly * G::ROW;
+  float2 v[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const float2 ph3 = cmul(bxy, tb[2 * N + k]);
+    const float m = s == 0 ? ph3.x : ph3.y;
+    const float2 f = A[base + k];
+    v[k] = make_float2(f.x * m, f.y * m);
+  }
+  fft<float, N, +1>(v);
+#pragma unroll
+  for (int k = 0; k < N; ++k) A[base + k] = v[k];
+}
+
+template <int N, int C>
+__global__ void __launch_bounds__(Geo<N, C>::NT, 1)
+vhs_terms_fp32_kernel(VhsTermsArgs a) {
+  using G = Geo<N, C>;
+  using T = float2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);
+  T* R0 = A + G::SLAB;          // receive buffer b at R0 + b*SLAB
+  // tables of two terms (ring): phase x,y,z | u x,y,z | v x,y,z
+  T* tab = R0 + 2 * G::SLAB;    // [2][9N]
+  const int t = threadIdx.x;
+  const unsigned rank = cluster_rank();
+  const int p = blockIdx.y, e = blockIdx.z;
+  const int Mu = a.Mu;
+  const T* Fg = static_cast<const T*>(a.Fg) + (size_t)e * G::n +
+                (size_t)rank * G::P * N * N;
+  const T* ph = static_cast<const T*>(a.ph) + (size_t)p * Mu * 3 * N;
+  const T* uvg = static_cast<const T*>(a.uv) +
+                 ((size_t)e * a.Nrho + p) * Mu * 6 * N;
+  auto load_tables = [&](int q) {
+    T* dst = tab + (q & 1) * 9 * N;
+    for (int i = t; i < 3 * N; i += G::NT) dst[i] = ph[(size_t)q * 3 * N + i];
+    for (int i = t; i < 6 * N; i += G::NT)
+      dst[3 * N + i] = uvg[(size_t)q * 6 * N + i];
+  };
+  load_tables(0);
+  uint32_t rbase[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) rbase[c] = mapa_u32(smem_u32(R0), (uint32_t)c);
+
+  const int yl = t / N, zz = t % N, yy = rank * G::P + yl;
+  T S[N];
+#pragma unroll
+  for (int x = 0; x < N; ++x) S[x] = make_float2(0.f, 0.f);
+
+  fp32_issue_slab_copy<N, C>(A, Fg, t);
+  cp_async_wait_all();
+  __syncthreads();
+  fp32_zpass<N, C>(A, tab, 0, t, rank);
+  __syncthreads();
+  const int npass = 2 * Mu;
+#pragma unroll 1
+  for (int k = 0; k < npass; ++k) {
+    const int q = k >> 1, s = k & 1;
+    T v[N];
+    {
+      const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+      for (int y = 0; y < N; ++y) v[y] = A[base + y * G::ROW];
+    }
+    __syncthreads();  // every thread has read A: refill it asynchronously
+    if (k + 1 < npass) {
+      // term (k+1)/2 starts: its tables go to the ring slot last read by
+      // term (k-1)/2, whose readers all passed the barrier above
+      if (((k + 1) & 1) == 0) load_tables((k + 1) >> 1);
+      fp32_issue_slab_copy<N, C>(A, Fg, t);
+    }
+    fft<float, N, +1>(v);
+    {
+      const int lx = rank * G::P + t / N, z = t % N;
+      const uint32_t off = (uint32_t)((k & 1) * G::SLAB + lx * G::ROW + z) * 8u;
+#pragma unroll
+      for (int c = 0; c < C; ++c)
+#pragma unroll
+        for (int j = 0; j < G::P; ++j)
+          st_cluster(rbase[c] + off + (uint32_t)(j * G::PLANE) * 8u,
+                     v[c * G::P + j]);
+    }
+    cluster_arrive();
+    if (k + 1 < npass) {
+      cp_async_wait_all();
+      __syncthreads();
+      fp32_zpass<N, C>(A, tab + (((k + 1) >> 1) & 1) * 9 * N, (k + 1) & 1,
+                       t, rank);
+      __syncthreads();
+    }
+    cluster_wait();
+    {
+      const T* Rk = R0 + (k & 1) * G::SLAB;
+      const int base = yl * G::PLANE + zz;
+#pragma unroll
+      for (int x = 0; x < N; ++x) v[x] = Rk[base + x * G::ROW];
+    }
+    fft<float, N, +1>(v);
+    const T* tb = tab + (q & 1) * 9 * N;
+    const T* ut = tb + 3 * N;
+    const T* vt = tb + 6 * N;
+    const T uyz = cmul(ut[N + yy], ut[2 * N + zz]);
+    const T vyz = cmul(vt[N + yy], vt[2 * N + zz]);
+#pragma unroll
+    for (int x = 0; x < N; ++x) {
+      const T um = cmul(ut[x], uyz), vm = cmul(vt[x], vyz);
+      T W;
+      if (s == 0) { W.x = um.x + vm.x; W.y = um.y + vm.y; }
+      else { W.x = um.y - vm.y; W.y = vm.x - um.x; }
+      W.x += v[x].x;
+      W.y += v[x].y;
+      const T h = cmul(v[x], W);
+      S[x].x += h.x;
+      S[x].y += h.y;
+    }
+  }
+
+  // forward FFT of S_p: x-pass, exchange into X-slabs, y-pass, z-pass
+  fft<float, N, -1>(S);
+  {
+    const uint32_t a0 = smem_u32(A);
+    const uint32_t off = (uint32_t)(yy * G::ROW + zz) * 8u;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const uint32_t ab = mapa_u32(a0, (uint32_t)c) + off;
+#pragma unroll
+      for (int j = 0; j < G::P; ++j)
+        st_cluster(ab + (uint32_t)(j * G::PLANE) * 8u, S[c * G::P + j]);
+    }
+  }
+  cluster_arrive();
+  cluster_wait();
+  {
+    T w[N];
+    slab_col_load_fft<float, N, C, -1>(A, t, w);
+    const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+    for (int k = 0; k < N; ++k) A[base + k * G::ROW] = w[k];
+  }
+  __syncthreads();
+  slab_row_pass<float, N, C, -1>(A, t);
+  __syncthreads();
+  const float* b1w = static_cast<const float*>(a.b1w) + (size_t)p * G::n +
+                     (size_t)rank * G::P * N * N;
+  T* H = static_cast<T*>(a.H) + ((size_t)e * a.Nrho + p) * G::n +
+         (size_t)rank * G::P * N * N;
+  for (int j = t; j < G::P * N * N; j += G::NT) {
+    T hv = A[slab_index<N, C>(j)];
+    const float w = b1w[j];
+    H[j] = make_float2(hv.x * w, hv.y * w);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Epilogue: one cluster (FP64) per eval.
 // ---------------------------------------------------------------------------
 template <int N, int C>
@@ -542,19 +746,59 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   const unsigned rank = cluster_rank();
   const int e = blockIdx.y;
   const size_t off = (size_t)rank * G::P * N * N;
-  for (int j = t; j < G::P * N * N; j += G::NT) {
-    T g = a.GM ? a.GM[(size_t)e * G::n + off + j] : T{0, 0};
-    for (int p = 0; p < a.Nrho; ++p) {
-      const size_t hi = ((size_t)e * a.Nrho + p) * G::n + off + j;
-      if (a.h_double) {
-        const double2 h = static_cast<const double2*>(a.H)[hi];
-        g.x += h.x; g.y += h.y;
+  // Ghat = Ghat_M + sum_p H_p over this CTA's slab: elements in pairs,
+  // UNR pairs per thread in flight per p so that the loads overlap
+  constexpr int TOT2 = G::P * N * N / 2;
+  constexpr int UNR = 8;
+  for (int b0 = t; b0 < TOT2; b0 += G::NT * UNR) {
+    T acc[UNR][2];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      const int j2 = b0 + u * G::NT;
+      if (a.GM && j2 < TOT2) {
+        acc[u][0] = a.GM[(size_t)e * G::n + off + 2 * j2];
+        acc[u][1] = a.GM[(size_t)e * G::n + off + 2 * j2 + 1];
       } else {
-        const float2 h = static_cast<const float2*>(a.H)[hi];
-        g.x += (double)h.x; g.y += (double)h.y;
+        acc[u][0] = T{0, 0};
+        acc[u][1] = T{0, 0};
       }
     }
-    A[slab_index<N, C>(j)] = g;
+    for (int p = 0; p < a.Nrho; ++p) {
+      const size_t hb = ((size_t)e * a.Nrho + p) * G::n + off;
+      if (a.h_double) {
+        const double2* Hp = static_cast<const double2*>(a.H) + hb;
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          const int j2 = b0 + u * G::NT;
+          if (j2 < TOT2) {
+            const double2 h0 = Hp[2 * j2], h1 = Hp[2 * j2 + 1];
+            acc[u][0].x += h0.x; acc[u][0].y += h0.y;
+            acc[u][1].x += h1.x; acc[u][1].y += h1.y;
+          }
+        }
+      } else {
+        const float4* Hp =
+            reinterpret_cast<const float4*>(static_cast<const float2*>(a.H) + hb);
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          const int j2 = b0 + u * G::NT;
+          if (j2 < TOT2) {
+            const float4 h = Hp[j2];
+            acc[u][0].x += (double)h.x; acc[u][0].y += (double)h.y;
+            acc[u][1].x += (double)h.z; acc[u][1].y += (double)h.w;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      const int j2 = b0 + u * G::NT;
+      if (j2 < TOT2) {
+        const int si = slab_index<N, C>(2 * j2);
+        A[si] = acc[u][0];
+        A[si + 1] = acc[u][1];
+      }
+    }
   }
   __syncthreads();
   slab_row_pass<double, N, C, +1>(A, t);
