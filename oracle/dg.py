@@ -1,0 +1,265 @@
+"""Oracle restatement of the single-species DG solver around Q (float64).
+
+Test infrastructure only (see ``oracle/__init__.py``).  Follows
+dgfs1D/std/std.py:37-423 (driver and ``rhs``), dgfs1D/std/kernels/std.mako
+(face extraction, upwind flux, lifting), dgfs1D/basis.py:206-421 (nodal
+bases), dgfs1D/std/bc.py + kernels/bcs/*.mako (boundary conditions),
+dgfs1D/std/integrator.py (explicit schemes), dgfs1D/axnpby.py and
+dgfs1D/std/moments.py:11-70 (bulk moments).
+"""
+import numpy as np
+
+from .mesh import (gauss_lobatto_jacobi, jac_nodal_basis_at, nodal_basis_at,
+                   ortho_basis_at)
+
+
+def filter_tol(mat, tol=1e-15):
+    """Zero entries below tol, as the gimmik kernels see them (util.py:16-18)."""
+    mat = np.array(mat, dtype=np.float64)
+    mat[abs(mat) < tol] = 0.
+    return mat
+
+
+class NodalBasis:
+    """``nodal-sem-gll`` (basis.py:206-329) and ``nodal-gll`` (333-421)."""
+
+    def __init__(self, kind, K, Nqr):
+        self.kind, self.K = kind, K
+        z, w = gauss_lobatto_jacobi(K, 0., 0.)
+        self.z, self.w = z, w
+        I = np.eye(K)
+        zr, _ = gauss_lobatto_jacobi(Nqr, 0., 0.)
+        self.interpMat = nodal_basis_at(K, z, zr).T
+        D = jac_nodal_basis_at(K, z, z)
+        self.derivMat = D.T
+        if kind == 'nodal-sem-gll':
+            B = nodal_basis_at(K, z, z).T
+            M = np.einsum('mq,q,lq->ml', B, w, B)
+            invM = np.linalg.inv(M)
+            H = np.einsum('mq,aq,bq,q->mab', B, B, B, w)
+            invM_H = np.einsum('ml,mab->lab', invM, H)
+            self.Nqf = 2
+            zqf, _ = gauss_lobatto_jacobi(2, 0., 0.)
+            self.Bqf = nodal_basis_at(K, z, zqf).T
+            self.gLD = self.Bqf[:, 0] / w[0]
+            self.gRD = self.Bqf[:, -1] / w[-1]
+            self.invMassMat = B.T
+        elif kind == 'nodal-gll':
+            B = ortho_basis_at(K, z).T
+            invM = B @ B.T
+            invM_H = np.einsum('mq,aq,bq->mab', I, I, I)
+            self.Nqf = K
+            self.Bqf = I
+            self.gLD, self.gRD = invM[0, :], invM[-1, :]
+            self.invMassMat = I
+        else:
+            raise ValueError(kind)
+        U, V, sig = [], [], []
+        for m in range(K):
+            u, s, v = np.linalg.svd(invM_H[m, :, :])
+            Um, Vm = filter_tol(u), filter_tol(np.dot(np.diag(s), v))
+            nnzU = np.where(np.sum(Um, axis=0) != 0)[0]
+            nnzV = np.where(np.sum(Vm, axis=1) != 0)[0]
+            U.append(Um)
+            V.append(Vm)
+            sig.append(np.intersect1d(nnzU, nnzV))
+        self.U, self.V, self.sigModes = U, V, sig
+        # the operators as the kernels apply them (C = A . B, filtered)
+        self.bwdFaceOp = filter_tol(self.Bqf.T)      # (Nqf, K)
+        self.derivOp = filter_tol(D.T)               # (K, K): ux = D^T u
+        self.invMassOp = filter_tol(self.invMassMat)
+
+
+def classic_mesh(xlo, xhi, Ne, H0):
+    """``Mesh.classic`` + non-dimensionalisation (mesh.py:10-18, 88-128)."""
+    xmesh = np.linspace(xlo, xhi, Ne + 1) / H0
+    h = np.diff(xmesh).reshape(-1, 1)
+    return xmesh, h / 2., 2. / h
+
+
+def face_maps(Ne, Nqf):
+    """mapL/mapR of std.py:63-66."""
+    mapL, mapR = np.arange(Ne + 1) + (Nqf - 1) * Ne - 1, np.arange(Ne + 1)
+    mapL[0], mapR[-1] = 0, Ne * Nqf - 1
+    return mapL, mapR
+
+
+class WallDiffuseBC:
+    """Purely diffuse wall (std/bc.py:25-78, dgfs-wall-diffuse.mako)."""
+
+    def __init__(self, cv, cw, T, u, nl):
+        self.cx, self.cw, self.nl = cv[0], cw, nl
+        self.ux = u[0]
+        self.f0 = (1.0 / (np.pi * T) ** 1.5) * np.exp(
+            -np.sum((cv - np.reshape(u, (3, 1))) ** 2, axis=0) / T)
+        self.nden = None
+
+    def update(self, ul):
+        fac = (self.cx - self.ux) * self.nl
+        num = (fac >= 0.) * (fac * ul * self.cw)
+        den = (fac < 0.) * (fac * self.f0 * self.cw)
+        self.nden = -(np.sum(num) / np.sum(den))
+
+    def apply(self, ul):
+        fac = (self.cx - self.ux) * self.nl
+        return (fac < 0) * (self.f0 * self.nden) + (fac >= 0) * ul
+
+
+class InletBC:
+    """Inlet: incoming from a fixed Maxwellian (dgfs-inlet.mako)."""
+
+    def __init__(self, cv, rho, T, u, nl):
+        self.cx, self.nl = cv[0], nl
+        self.f0 = (rho / (np.pi * T) ** 1.5) * np.exp(
+            -np.sum((cv - np.reshape(u, (3, 1))) ** 2, axis=0) / T)
+
+    def update(self, ul):
+        pass
+
+    def apply(self, ul):
+        fac = self.cx * self.nl
+        return (fac < 0) * self.f0 + (fac >= 0) * ul
+
+
+class PeriodicBC:
+    """Single-rank ``dgfs-periodic``: ghost = the interior trace
+    (dgfs-periodic.mako)."""
+
+    def update(self, ul):
+        pass
+
+    def apply(self, ul):
+        return ul.copy()
+
+
+def dg_rhs(basis, invjac, cx, bcl, bcr, u_in, collide=None):
+    """Right-hand side of std.py:281-366 for u_in of shape (K, Ne, Nv).
+
+    ``collide(u_in, ux)`` adds the collision term (the fs loop of :349-356).
+    """
+    K, Ne, Nv = u_in.shape
+    usolF = np.einsum('qk,kev->qev', basis.bwdFaceOp, u_in)
+    usolF = usolF.reshape(-1, Nv)
+    mapL, mapR = face_maps(Ne, basis.Nqf)
+    uL = usolF[mapL].copy()
+    uR = usolF[mapR].copy()
+    bcL = uL[0].copy()
+    bcR = uR[Ne].copy()
+    bcl.update(bcL)
+    uL[0] = bcl.apply(bcL)
+    bcr.update(bcR)
+    uR[Ne] = bcr.apply(bcR)
+    ac = 0.5 * np.abs(cx)
+    jL = ac * (uL - uR)
+    jR = jL.copy()
+    jL = jL + 0.5 * cx * (uR - uL)
+    jR = jR + 0.5 * cx * (uL - uR)
+    ux = np.einsum('km,mev->kev', basis.derivOp, u_in)
+    ux = ux * (-cx)
+    for k in range(K):
+        for e in range(Ne):
+            ux[k, e] += -jL[e + 1] * basis.gRD[k] + jR[e] * basis.gLD[k]
+    ux = ux * invjac.reshape(1, Ne, 1)
+    if collide is not None:
+        collide(u_in, ux)
+    return np.einsum('km,mev->kev', basis.invMassOp, ux)
+
+
+def collide_fs(basis, fs):
+    """The collision loop of std.py:349-356 with fs(f, g) -> increment."""
+    def collide(u_in, ux):
+        K, Ne, Nv = u_in.shape
+        for m in range(K):
+            d_f = np.einsum('ar,aev->rev', basis.U[m], u_in)
+            d_g = np.einsum('rb,bev->rev', basis.V[m], u_in)
+            for r in basis.sigModes[m]:
+                for e in range(Ne):
+                    ux[m, e] += fs(d_f[r, e], d_g[r, e])
+    return collide
+
+
+def axnpby(x0, a0, *terms):
+    """x0 <- a0 x0 + sum a_i x_i with the a0 in {0, 1} branches (axnpby.py)."""
+    acc = 0.0
+    for a, x in zip(terms[::2], terms[1::2]):
+        acc = acc + a * x
+    if a0 == 0.0:
+        x0[...] = acc
+    elif a0 == 1.0:
+        x0[...] = x0 + acc
+    else:
+        x0[...] = a0 * x0 + acc
+
+
+def integrate(kind, rhs, t, dt, u):
+    """One step of std/integrator.py:37-157 (in place on u)."""
+    if kind == 'euler':
+        r0 = rhs(t, u)
+        axnpby(u, 1.0, dt, r0)
+    elif kind == 'ssp-rk2':
+        r0 = rhs(t, u)
+        axnpby(r0, dt, 1.0, u)
+        r1 = rhs(t + dt, r0)
+        axnpby(u, 0.5, 0.5, r0, 0.5 * dt, r1)
+    elif kind == 'ssp-rk3':
+        r1 = rhs(t, u)
+        r0 = np.empty_like(u)
+        axnpby(r0, 0.0, 1.0, u, dt, r1)
+        r1 = rhs(t + dt, r0)
+        axnpby(r0, 0.25, 0.75, u, 0.25 * dt, r1)
+        r1 = rhs(t + 0.5 * dt, r0)
+        axnpby(u, 1.0 / 3.0, 2.0 / 3.0, r0, 2.0 / 3.0 * dt, r1)
+    elif kind == 'lse-rk45':
+        a = [0.0, -567301805773.0 / 1357537059087.0,
+             -2404267990393.0 / 2016746695238.0,
+             -3550918686646.0 / 2091501179385.0,
+             -1275806237668.0 / 842570457699.0]
+        b = [1432997174477.0 / 9575080441755.0,
+             5161836677717.0 / 13612068292357.0,
+             1720146321549.0 / 2090206949498.0,
+             3134564353537.0 / 4481467310338.0,
+             2277821191437.0 / 14882151754819.0]
+        c = [0.0, 1432997174477.0 / 9575080441755.0,
+             2526269341429.0 / 6820363962896.0,
+             2006345519317.0 / 3224310063776.0,
+             2802321613138.0 / 2924317926251.0]
+        r1 = np.zeros_like(u)
+        for s in range(5):
+            r0 = rhs(t + c[s] * dt, u)
+            axnpby(r1, a[s], dt, r0)
+            axnpby(u, 1., b[s], r1)
+    else:
+        raise ValueError(kind)
+
+
+def moments(basis, coeff, cv, cw, T0=1.0, rho0=1.0, u0=1.0, R0=8.3144598,
+            molarMass0=1.0):
+    """Bulk moments of std/moments.py:11-70 at the reconstruction points.
+
+    Returns (Nqr, Ne, 10): rho, Ux, Uy, T, Qx, Qy, Pxx, Pyy, Pxy, p with the
+    dimensional scaling of :61-68 (pass T0=rho0=u0=1 for nondimensional).
+    """
+    K, Ne, Nv = coeff.shape
+    soln = np.einsum('mr,mej->rej', basis.interpMat, coeff)
+    mcw = cw
+    out = np.zeros(soln.shape[:2] + (10,))
+    out[:, :, 0] = np.einsum('...j->...', soln) * mcw
+    out[:, :, 1] = np.einsum('rej,j->re', soln, cv[0]) * mcw / out[:, :, 0]
+    out[:, :, 2] = np.einsum('rej,j->re', soln, cv[1]) * mcw / out[:, :, 0]
+    Nqr = soln.shape[0]
+    cx = cv[0].reshape(1, 1, Nv) - out[:, :, 1].reshape(Nqr, Ne, 1)
+    cy = cv[1].reshape(1, 1, Nv) - out[:, :, 2].reshape(Nqr, Ne, 1)
+    cz = cv[2].reshape(1, 1, Nv) - np.zeros((Nqr, Ne, 1))
+    cSqr = cx * cx + cy * cy + cz * cz
+    out[:, :, 3] = np.einsum('...j,...j->...', soln, cSqr) * (2. / 3. * mcw)
+    out[:, :, 3] /= out[:, :, 0]
+    out[:, :, 4] = np.einsum('...j,...j,...j->...', soln, cSqr, cx) * mcw
+    out[:, :, 5] = np.einsum('...j,...j,...j->...', soln, cSqr, cy) * mcw
+    out[:, :, 6] = 2 * np.einsum('...j,...j,...j->...', soln, cx, cx) * mcw
+    out[:, :, 7] = 2 * np.einsum('...j,...j,...j->...', soln, cy, cy) * mcw
+    out[:, :, 8] = 2 * np.einsum('...j,...j,...j->...', soln, cx, cy) * mcw
+    out[:, :, 0:9] *= np.array([rho0, u0, u0, T0, 0.5 * rho0 * u0 ** 3,
+                                0.5 * rho0 * u0 ** 3, 0.5 * rho0 * u0 ** 2,
+                                0.5 * rho0 * u0 ** 2, 0.5 * rho0 * u0 ** 2])
+    out[:, :, 9] = (R0 / molarMass0) * out[:, :, 0] * out[:, :, 3]
+    return out

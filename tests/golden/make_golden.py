@@ -397,6 +397,142 @@ def golden_vss(R, Nv=8, Nrho=4, M=6, Mpre=12, dev=5.0, Ne=2):
     return out
 
 
+def _vhs_ref_fs(R, cfg, vm, Ne, Kb):
+    """fs(f_slots, Q_slots, e, m) driving the reference vhs-gll kernels."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    sm = object.__new__(R.VHSGLL)
+    sm.cfg, sm.vm, sm._Ne = cfg, vm, Ne
+    sm.load_parameters()
+    vsize, N, Nrho, M = vm.vsize(), vm.Nv(), vm.Nrho(), vm.M()
+    l0 = np.concatenate((np.arange(0, N / 2), np.arange(-N / 2, 0)))
+    l = np.zeros((3, vsize))
+    for idv in range(vsize):
+        l[0, idv] = l0[idv // (N * N)]
+        l[1, idv] = l0[(idv % (N * N)) // N]
+        l[2, idv] = l0[(idv % (N * N)) % N]
+    src = render_template(
+        'dgfs1D/std/kernels/scattering/vhs-gll.mako', dtype='double',
+        Nrho=Nrho, M=M, vsize=vsize, sw=vm.sw(), prefac=sm._prefactor,
+        qw=vm.qw(), sz=vm.sz(), gamma=sm._gamma, L=vm.L(), qz=vm.qz(),
+        Ne=Ne, block_size=128, cw=vm.cw())
+    K = RefModule(src, tag='vhs-gll')
+    blk = 128
+    g = grid_for(vsize, blk)
+    lx, ly, lz = (np.ascontiguousarray(l[i]) for i in range(3))
+    aa = np.empty(Nrho * M * vsize)
+    K.launch('precompute_aa', g, blk, lx, ly, lz, aa)
+    bb1, bb2 = np.empty(Nrho * vsize), np.empty(vsize)
+    K.launch('precompute_bb', g, blk, lx, ly, lz, bb1, bb2)
+    shape = (N, N, N)
+
+    def fs(f, Q, e, r, m):
+        fC = np.zeros(vsize, dtype=np.complex128)
+        K.launch('r2z_', g, blk, e, r, f, fC)
+        FTf = _fwd(fC.reshape(shape)).ravel()
+        t1 = np.zeros(Nrho * M * vsize, dtype=np.complex128)
+        t2 = np.zeros_like(t1)
+        K.launch('cosSinMul', g, blk, aa, FTf, t1, t2)
+        t3 = _inv(t1.reshape(-1, *shape)).ravel()
+        t4 = _inv(t2.reshape(-1, *shape)).ravel()
+        K.launch('magSqr', g, blk, t3, t4, t2)
+        t1 = _fwd(t2.reshape(-1, *shape)).ravel()
+        K.launch('computeQG', g, blk, bb1, t1, fC)
+        QG = _inv(fC.reshape(shape)).ravel()
+        K.launch('ax', g, blk, bb2, FTf)
+        fC = _inv(FTf.reshape(shape)).ravel()
+        K.launch('output_append_', g, blk, e, r, m, QG, fC, f, Q)
+    return fs, sm
+
+
+def golden_dg(R, kind, Nv=8, Nrho=4, M=6, dev=5.0, Ne=3, Kb=3):
+    """One std.py rhs() through the reference's own std.mako and diffuse-wall
+    kernels (+ the vhs-gll fs loop), on seeded data."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    ini = STD_INI.format(basis=kind, Nv=Nv, Nrho=Nrho, M=M, dev=dev)
+    ini = ini.replace('Ne = 4', f'Ne = {Ne}').replace('K = 3', f'K = {Kb}')
+    cfg = R.Dictionary(ini)
+    vm = R.vstd.DGFSVelocityMeshStd(cfg)
+    cls = {'nodal-sem-gll': R.basis.NodalSemGLL,
+           'nodal-gll': R.basis.NodalGLL}[kind]
+    basis = cls(cfg)
+    K, Nqf, vsize = basis.K, basis.Nqf, vm.vsize()
+    import dgfs1D.util as util
+    xmesh = np.linspace(0., 1e-3, Ne + 1) / 1e-3
+    h = np.diff(xmesh).reshape(-1, 1)
+    jac, invjac = h / 2., 2. / h
+    mapL, mapR = np.arange(Ne + 1) + (Nqf - 1) * Ne - 1, np.arange(Ne + 1)
+    mapL[0], mapR[-1] = 0, Ne * Nqf - 1
+    xsol = np.array([0.5 * (xmesh[j] + xmesh[j + 1]) + jac[j] * basis.z
+                     for j in range(Ne)]).T
+    src = render_template('dgfs1D/std/kernels/std.mako', K=K, Ne=Ne, Nq=K,
+                          vsize=vsize, dtype='double', mapL=mapL, mapR=mapR,
+                          offsetL=0, offsetR=len(mapR) - 1, invjac=invjac,
+                          gRD=basis.gRD, gLD=basis.gLD, xsol=xsol)
+    SK = RefModule(src, tag='std')
+    walls = {}
+    u0 = vm.u0()
+    for side, nl, uy in (('L', -1., -0.1), ('R', 1., 0.1)):
+        u_w = np.array([0., uy, 0.]).reshape(3, 1)
+        T_w = 1.0
+        f0 = ((1.0 / (np.pi * T_w) ** 1.5)
+              * np.exp(-np.sum((vm.cv() - u_w) ** 2, axis=0) / T_w))
+        bsrc = render_template('dgfs1D/std/kernels/bcs/dgfs-wall-diffuse.mako',
+                               dtype='double', vsize=vsize, cw=vm.cw(),
+                               ux=0.0, nl=nl, x=0.0)
+        walls[side] = (RefModule(bsrc, tag='wall' + side), f0)
+    blk = 128
+    gv = grid_for(vsize, blk)
+    filt = util.filter_tol
+
+    def mm(A, B):
+        return np.ascontiguousarray(
+            (filt(np.array(A, dtype=np.float64)) @ B.reshape(A.shape[1], -1))
+            .ravel())
+
+    rng = np.random.default_rng(SEED + 7)
+    u = np.stack([_maxwellian_noise(vm.cv(), rng, rho=1.0)
+                  for _ in range(K * Ne)]).reshape(K, Ne, vsize)
+    u = np.ascontiguousarray(u.ravel())
+    fs, sm = _vhs_ref_fs(R, cfg, vm, Ne, K)
+    out = {}
+    for with_q in (False, True):
+        usolF = mm(basis._Bqf.T, u)
+        uL, uR = np.zeros((Ne + 1) * vsize), np.zeros((Ne + 1) * vsize)
+        SK.launch('extract_left', gv, blk, usolF, uL)
+        SK.launch('extract_right', gv, blk, usolF, uR)
+        bcL, bcR, bcT = np.zeros(vsize), np.zeros(vsize), np.zeros(vsize)
+        SK.launch('transfer_bc_left', gv, blk, uL, bcL)
+        SK.launch('transfer_bc_right', gv, blk, uR, bcR)
+        cvx = np.ascontiguousarray(vm.cv()[0])
+        for side, bcv, ins in (('L', bcL, 'insert_bc_left'),
+                               ('R', bcR, 'insert_bc_right')):
+            BK, f0 = walls[side]
+            num, den = np.zeros(vsize), np.zeros(vsize)
+            BK.launch('updateBC', gv, blk, bcv, cvx, f0, num, den, 0.0)
+            nden = np.array([-(np.sum(num) / np.sum(den))])
+            BK.launch('applyBC', gv, blk, bcv, bcT, cvx, f0, nden, 0.0)
+            SK.launch(ins, gv, blk, bcT, uL if side == 'L' else uR)
+        jL, jR = np.zeros_like(uL), np.zeros_like(uR)
+        SK.launch('flux', gv, blk, uL, uR, cvx, jL, jR)
+        ux = mm(basis.derivMat, u)
+        SK.launch('mul_by_adv', grid_for(K * Ne * vsize, blk), blk, cvx, ux)
+        SK.launch('totalFlux', gv, blk, ux, cvx, jL, jR)
+        SK.launch('mul_by_invjac', gv, blk, ux)
+        if with_q:
+            for m in range(K):
+                d_f = mm(basis._U[m].T, u)
+                d_g = mm(basis._V[m], u)
+                for r in basis.sigModes[m]:
+                    for e in range(Ne):
+                        fs(d_f, ux, e, int(r), m)
+        uout = mm(basis._B.T if kind == "nodal-sem-gll" else np.eye(K), ux)
+        out['rhs_q' if with_q else 'rhs_adv'] = uout
+    out.update(u=u, K=K, Ne=Ne, Nv=Nv, Nrho=Nrho, M=M, L=vm.L(), qz=vm.qz(),
+               qw=vm.qw(), sz=vm.sz(), sw=vm.sw(), cw=vm.cw(), cv=vm.cv(),
+               prefac=sm._prefactor, gamma=sm._gamma, invjac=invjac.ravel())
+    return out
+
+
 def golden_setup(R):
     """Velocity meshes, rules and DG bases from the reference setup code."""
     out = {}
@@ -446,6 +582,10 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'setup.npz'), **golden_setup(R))
     np.savez_compressed(os.path.join(HERE, 'vhs_N8.npz'), **golden_vhs(R))
     np.savez_compressed(os.path.join(HERE, 'vss_N8.npz'), **golden_vss(R))
+    for kind in ('nodal-sem-gll', 'nodal-gll'):
+        np.savez_compressed(
+            os.path.join(HERE, 'dg_%s_N8.npz' % kind.replace('-', '_')),
+            **golden_dg(R, kind))
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith('.npz'):
             print(fn, os.path.getsize(os.path.join(HERE, fn)), 'bytes')
