@@ -31,6 +31,20 @@ class VhsDesc(ctypes.Structure):
     ]
 
 
+class DgDesc(ctypes.Structure):
+    """Mirror of ``dgfs_dg_desc`` (include/dgfs_sm100.h)."""
+    _fields_ = [
+        ('K', ctypes.c_int32), ('Ne', ctypes.c_int32), ('N', ctypes.c_int32),
+        ('Nqr', ctypes.c_int32),
+        ('trL', _c_dp), ('trR', _c_dp), ('D', _c_dp), ('gLD', _c_dp),
+        ('gRD', _c_dp), ('invjac', _c_dp), ('c0', _c_dp), ('im', _c_dp),
+        ('cw', ctypes.c_double),
+        ('bc_kind', ctypes.c_int32 * 2),
+        ('bc_f0', _c_dp * 2),
+        ('bc_ux', ctypes.c_double * 2),
+    ]
+
+
 class DgfsError(RuntimeError):
     """A C-ABI call returned a non-zero status."""
 
@@ -62,6 +76,24 @@ _SIGNATURES = [
      [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ('dgfs_fma_peak', ctypes.c_int,
      [ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ('dgfs_dg_create', ctypes.c_int,
+     [ctypes.POINTER(DgDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    ('dgfs_dg_destroy', ctypes.c_int, [ctypes.c_void_p]),
+    ('dgfs_dg_advect', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_void_p]),
+    ('dgfs_dg_wall_density', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ('dgfs_dg_moments', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_void_p]),
+    ('dgfs_dg_residual', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+      ctypes.c_int32, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ('dgfs_axnpby', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_double,
+      ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),
+      ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     ('dgfs_vhs_eval_noalloc', ctypes.c_int,
      [ctypes.POINTER(VhsDesc), ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,

@@ -1,0 +1,85 @@
+"""INI texts of the benchmark / test configurations (nondimensional setups
+expressed in the reference's dimensional INI keys)."""
+import math
+
+NA, R0 = 6.0221409e+23, 8.3144598
+
+
+def rho0_for_knudsen(Kn, H0=1e-3, dRef=4.17e-10, omega=0.81, Tref=273.,
+                     T0=273., molarMass0=39.96e-3):
+    """rho0 giving invKn = 1/Kn in std/scattering.py:77-78."""
+    n0 = (1.0 / Kn) / (H0 * math.sqrt(2.0) * math.pi * dRef * dRef
+                        * (Tref / T0) ** (omega - 0.5))
+    return n0 * molarMass0 / NA
+
+
+def couette_std_ini(Ne=4, K=3, Nv=16, Nrho=8, M=6, dev=5.0, Kn=0.1,
+                    omega=0.81, uwall=0.1, scheme='euler', dt=0.00025,
+                    nsteps=52, precision='double', basis='nodal-sem-gll',
+                    noise=0.01, seed=20261203, precision_mode=None,
+                    sphere='auto', ic='maxwellian-noise'):
+    T0, molarMass0 = 273., 39.96e-3
+    u0 = math.sqrt(2 * R0 / molarMass0 * T0)
+    rho0 = rho0_for_knudsen(Kn, omega=omega)
+    pm = f'precision-mode = {precision_mode}\n' if precision_mode else ''
+    return f"""
+[config]
+precision = {precision}
+[mesh]
+xlo = 0.
+xhi = 1e-3
+Ne = {Ne}
+H0 = 1e-3
+[basis]
+kind = {basis}
+K = {K}
+Nqr = {K}
+[non-dim]
+T0 = {T0}
+rho0 = {rho0!r}
+molarMass0 = {molarMass0}
+[velocity-mesh]
+Nv = {Nv}
+Nrho = {Nrho}
+dev = {dev}
+cmax = 0
+Tmax = {T0}
+[spherical-design-rule]
+ssrule = womersley
+M = {M}
+sphere = {sphere}
+[scattering-model]
+type = vhs-gll
+omega = {omega}
+dRef = 4.17e-10
+Tref = 273
+muRef = 2.117e-5
+{pm}
+[time-integrator]
+scheme = {scheme}
+controller = none
+tstart = 0.0
+tend = {dt * nsteps!r}
+dt = {dt!r}
+[soln-ics]
+type = {ic}
+rho = {rho0!r}
+T = {T0}
+ux = 0
+uy = 0
+uz = 0
+noise = {noise}
+seed = {seed}
+[soln-bcs-xlo]
+type = dgfs-wall-diffuse
+T = {T0}
+ux = 0
+uy = {-uwall * u0!r}
+uz = 0
+[soln-bcs-xhi]
+type = dgfs-wall-diffuse
+T = {T0}
+ux = 0
+uy = {uwall * u0!r}
+uz = 0
+"""

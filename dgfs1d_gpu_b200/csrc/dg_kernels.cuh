@@ -1,0 +1,296 @@
+// Nodal DG advection right-hand side, boundary conditions, stage updates
+// (axnpby) and FP64 bulk moments of the single-species solver.
+//
+// Reference: the rhs() closure of dgfs1D/std/std.py:281-366 with the kernels
+// of dgfs1D/std/kernels/std.mako (extract/transfer/insert, flux, mul_by_adv,
+// totalFlux, mul_by_invjac), the diffuse-wall / inlet / periodic boundary
+// kernels of dgfs1D/std/kernels/bcs/*.mako, axnpby of dgfs1D/axnpby.py:10-58
+// and the moments of dgfs1D/std/moments.py:11-70.  The reference runs about
+// fifteen small kernels and two host reductions per right-hand side; here
+// one reduction kernel (wall densities) and one fused kernel produce it.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dgfs {
+
+constexpr int kDgMaxK = 8;
+
+// boundary kinds
+constexpr int kBcCopy = 0;     // dgfs-periodic on one rank: ghost = interior
+constexpr int kBcWall = 1;     // dgfs-wall-diffuse
+constexpr int kBcInlet = 2;    // dgfs-inlet
+
+struct DgAdvectArgs {
+  const void* u;            // (K, Ne, Nv) in
+  void* ux;                 // (K, Ne, Nv) out: advection + flux terms
+  int f_double;
+  int K, Ne, Nv, N;
+  const double* c0;         // [N] velocity grid; c_x of v = c0[v / (N*N)]
+  const double* invjac;     // [Ne]
+  const double* f0[2];      // [Nv] boundary Maxwellians (left, right)
+  const double* nden;       // [2] wall densities (from dg_wall_density_kernel)
+  int bc[2];                // boundary kinds (left, right)
+  double bc_ux[2];          // wall x-velocities
+  double nl[2];             // outward normals (-1, +1)
+  double trL[kDgMaxK];      // left-face trace weights  (row 0 of Bqf^T)
+  double trR[kDgMaxK];      // right-face trace weights (row Nqf-1 of Bqf^T)
+  double D[kDgMaxK * kDgMaxK];  // derivOp (K x K): ux = D u
+  double gLD[kDgMaxK], gRD[kDgMaxK];
+};
+
+__device__ __forceinline__ double ld(const void* p, int dbl, size_t i) {
+  return dbl ? static_cast<const double*>(p)[i]
+             : (double)static_cast<const float*>(p)[i];
+}
+__device__ __forceinline__ void st(void* p, int dbl, size_t i, double v) {
+  if (dbl) static_cast<double*>(p)[i] = v;
+  else static_cast<float*>(p)[i] = (float)v;
+}
+
+// Wall densities n_w = -sum_{out} (c-u_w).n f cw / sum_{in} (c-u_w).n f0 cw
+// (updateBC of dgfs-wall-diffuse.mako with the two gpuarray.sum of
+// std/bc.py:63-76).  One block per boundary; deterministic order.
+__global__ void __launch_bounds__(1024) dg_wall_density_kernel(DgAdvectArgs a,
+                                                               double cw,
+                                                               double* nden) {
+  const int side = blockIdx.x;
+  __shared__ double rn[1024], rd[1024];
+  const int t = threadIdx.x;
+  double sn = 0, sd = 0;
+  if (a.bc[side] == kBcWall) {
+    const int e = side == 0 ? 0 : a.Ne - 1;
+    const double* tw = side == 0 ? a.trL : a.trR;
+    const double nl = a.nl[side], ux = a.bc_ux[side];
+    for (int v = t; v < a.Nv; v += blockDim.x) {
+      double ul = 0;
+      for (int k = 0; k < a.K; ++k)
+        ul += tw[k] * ld(a.u, a.f_double, ((size_t)k * a.Ne + e) * a.Nv + v);
+      const double fac = (a.c0[v / (a.N * a.N)] - ux) * nl;
+      if (fac >= 0.) sn += fac * ul * cw;
+      else sd += fac * a.f0[side][v] * cw;
+    }
+  }
+  rn[t] = sn;
+  rd[t] = sd;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (t < s) { rn[t] += rn[t + s]; rd[t] += rd[t + s]; }
+    __syncthreads();
+  }
+  if (t == 0) nden[side] = (a.bc[side] == kBcWall) ? -(rn[0] / rd[0]) : 0.0;
+}
+
+__device__ __forceinline__ double dg_ghost(const DgAdvectArgs& a, int side,
+                                           int v, double cx, double ul) {
+  const int kind = a.bc[side];
+  if (kind == kBcWall) {
+    const double fac = (cx - a.bc_ux[side]) * a.nl[side];
+    return fac < 0 ? a.f0[side][v] * a.nden[side] : ul;
+  }
+  if (kind == kBcInlet) {
+    const double fac = cx * a.nl[side];
+    return fac < 0 ? a.f0[side][v] : ul;
+  }
+  return ul;
+}
+
+// ux[k][e][v] = ((D u)[k] * (-c) - jL[e+1] gRD[k] + jR[e] gLD[k]) * invjac[e]
+// with jL = 0.5|c|(uL-uR) + 0.5c(uR-uL), jR = 0.5|c|(uL-uR) + 0.5c(uL-uR)
+// at each face (uL: state on its left, uR: on its right).  One thread per
+// velocity point walks the elements.
+template <int K>
+__global__ void __launch_bounds__(256) dg_advect_kernel(DgAdvectArgs a) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= a.Nv) return;
+  const int Ne = a.Ne, Nv = a.Nv;
+  const double cx = a.c0[v / (a.N * a.N)];
+  const double ac = 0.5 * fabs(cx), hc = 0.5 * cx;
+  double ue[K], un[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) ue[k] = ld(a.u, a.f_double, ((size_t)k * Ne) * Nv + v);
+  auto tl = [&](const double* w) {
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) s += a.trL[k] * w[k];
+    return s;
+  };
+  auto tr = [&](const double* w) {
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) s += a.trR[k] * w[k];
+    return s;
+  };
+  // face 0: ghost on the left, element 0 on the right
+  double uRf = tl(ue);
+  double uLf = dg_ghost(a, 0, v, cx, uRf);
+  double jR = ac * (uLf - uRf) + hc * (uLf - uRf);
+  for (int e = 0; e < Ne; ++e) {
+    // face e+1
+    const double uL1 = tr(ue);
+    double uR1;
+    if (e + 1 < Ne) {
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        un[k] = ld(a.u, a.f_double, ((size_t)k * Ne + e + 1) * Nv + v);
+      uR1 = tl(un);
+    } else {
+      uR1 = dg_ghost(a, 1, v, cx, uL1);
+    }
+    const double jd = ac * (uL1 - uR1);
+    const double jL1 = jd + hc * (uR1 - uL1);
+    const double ij = a.invjac[e];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double d = 0;
+#pragma unroll
+      for (int m = 0; m < K; ++m) d += a.D[k * K + m] * ue[m];
+      double r = d * (-cx);
+      r += -jL1 * a.gRD[k] + jR * a.gLD[k];
+      st(a.ux, a.f_double, ((size_t)k * Ne + e) * Nv + v, r * ij);
+    }
+    jR = jd + hc * (uL1 - uR1);  // jR of face e+1 for element e+1
+#pragma unroll
+    for (int k = 0; k < K; ++k) ue[k] = un[k];
+  }
+}
+
+// x0 <- a0 x0 + sum_i a_i x_i, with the a0 == 0 (x0 not read) and a0 == 1
+// branches of axnpby.py:10-44.
+constexpr int kAxMax = 4;
+struct AxnpbyArgs {
+  void* x0;
+  const void* x[kAxMax];
+  double a[kAxMax];
+  double a0;
+  int nterms;
+  int f_double;
+  size_t n;
+};
+
+__global__ void axnpby_kernel(AxnpbyArgs a) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int j = 0; j < a.nterms; ++j) {
+      const double v = ld(a.x[j], a.f_double, i);
+      s = (j == 0) ? a.a[0] * v : s + a.a[j] * v;
+    }
+    double r;
+    if (a.a0 == 0.0) r = s;
+    else if (a.a0 == 1.0) r = ld(a.x0, a.f_double, i) + s;
+    else r = a.a0 * ld(a.x0, a.f_double, i) + s;
+    st(a.x0, a.f_double, i, r);
+  }
+}
+
+// Bulk moments at the reconstruction points (FP64), two passes per block:
+// rho, U (then peculiar velocities), T, Q, P.  One block per (r, e).
+struct MomentArgs {
+  const void* coeff;        // (K, Ne, Nv)
+  int f_double;
+  int K, Ne, Nv, N, Nqr;
+  const double* im;         // [K][Nqr] interpolation to reconstruction points
+  const double* c0;         // [N]
+  double cw;
+  double* out;              // [Nqr][Ne][10] nondimensional
+};
+
+__global__ void __launch_bounds__(256) std_moments_kernel(MomentArgs a) {
+  const int r = blockIdx.x, e = blockIdx.y;
+  const int t = threadIdx.x;
+  __shared__ double red[8][256];
+  __shared__ double bulk[4];
+  const int NN = a.N * a.N;
+  auto sol = [&](int v) {
+    double s = 0;
+    for (int k = 0; k < a.K; ++k)
+      s += a.im[k * a.Nqr + r] * ld(a.coeff, a.f_double, ((size_t)k * a.Ne + e) * a.Nv + v);
+    return s;
+  };
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int v = t; v < a.Nv; v += blockDim.x) {
+    const double f = sol(v);
+    s0 += f;
+    s1 += f * a.c0[v / NN];
+    s2 += f * a.c0[(v / a.N) % a.N];
+  }
+  red[0][t] = s0; red[1][t] = s1; red[2][t] = s2;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (t < s)
+      for (int i = 0; i < 3; ++i) red[i][t] += red[i][t + s];
+    __syncthreads();
+  }
+  if (t == 0) {
+    const double rho = red[0][0] * a.cw;
+    bulk[0] = rho;
+    bulk[1] = red[1][0] * a.cw / rho;
+    bulk[2] = red[2][0] * a.cw / rho;
+  }
+  __syncthreads();
+  const double ux = bulk[1], uy = bulk[2];
+  double m[6] = {0, 0, 0, 0, 0, 0};  // |c|^2, |c|^2 cx, |c|^2 cy, cxcx, cycy, cxcy
+  for (int v = t; v < a.Nv; v += blockDim.x) {
+    const double f = sol(v);
+    const double cx = a.c0[v / NN] - ux, cy = a.c0[(v / a.N) % a.N] - uy,
+                 cz = a.c0[v % a.N];
+    const double c2 = cx * cx + cy * cy + cz * cz;
+    m[0] += f * c2;
+    m[1] += f * c2 * cx;
+    m[2] += f * c2 * cy;
+    m[3] += f * cx * cx;
+    m[4] += f * cy * cy;
+    m[5] += f * cx * cy;
+  }
+  __syncthreads();
+  for (int i = 0; i < 6; ++i) red[i][t] = m[i];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (t < s)
+      for (int i = 0; i < 6; ++i) red[i][t] += red[i][t + s];
+    __syncthreads();
+  }
+  if (t == 0) {
+    double* o = a.out + ((size_t)r * a.Ne + e) * 10;
+    const double rho = bulk[0];
+    o[0] = rho;
+    o[1] = ux;
+    o[2] = uy;
+    o[3] = red[0][0] * (2. / 3. * a.cw) / rho;
+    o[4] = red[1][0] * a.cw;
+    o[5] = red[2][0] * a.cw;
+    o[6] = 2 * red[3][0] * a.cw;
+    o[7] = 2 * red[4][0] * a.cw;
+    o[8] = 2 * red[5][0] * a.cw;
+    o[9] = 0;
+  }
+}
+
+// sum (x - y)^2 and sum y^2 in FP64 (residual of std/residual.py:15-29)
+__global__ void __launch_bounds__(512) residual_kernel(const void* x,
+                                                       const void* y, int dbl,
+                                                       size_t n, double* out) {
+  __shared__ double r0[512], r1[512];
+  const int t = threadIdx.x;
+  double a = 0, b = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + t; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double xv = ld(x, dbl, i), yv = ld(y, dbl, i), d = xv - yv;
+    a += d * d;
+    b += yv * yv;
+  }
+  r0[t] = a;
+  r1[t] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (t < s) { r0[t] += r0[t + s]; r1[t] += r1[t + s]; }
+    __syncthreads();
+  }
+  if (t == 0) {
+    out[2 * blockIdx.x] = r0[0];
+    out[2 * blockIdx.x + 1] = r1[0];
+  }
+}
+
+}  // namespace dgfs

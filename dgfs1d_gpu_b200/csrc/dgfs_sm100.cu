@@ -13,6 +13,7 @@
 #include "fft_reg.cuh"
 #include "cluster_slab.cuh"
 #include "vhs_kernels.cuh"
+#include "dg_kernels.cuh"
 
 using namespace dgfs;
 
@@ -791,4 +792,183 @@ extern "C" int dgfs_vhs_eval_noalloc(const dgfs_vhs_desc* d, const double* f,
   h.c0 = h.b2 = h.b1w64 = h.ReLf = nullptr;
   h.b1w32 = nullptr; h.ph = h.Fg = h.H = nullptr; h.mult = nullptr;
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// DG right-hand side, stage updates, moments, residual
+// ---------------------------------------------------------------------------
+struct dgfs_dg_s {
+  DgAdvectArgs base{};
+  int Nqr = 0;
+  double cw = 0;
+  double* c0 = nullptr;
+  double* invjac = nullptr;
+  double* f0[2] = {nullptr, nullptr};
+  double* nden = nullptr;
+  double* im = nullptr;
+  double* part = nullptr;  // residual partials
+  double* part_h = nullptr;
+};
+
+static void free_dg(dgfs_dg_s* h) {
+  void* ptrs[] = {h->c0, h->invjac, h->f0[0], h->f0[1], h->nden, h->im, h->part};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->part_h) cudaFreeHost(h->part_h);
+  delete h;
+}
+
+extern "C" int dgfs_dg_create(const dgfs_dg_desc* d, dgfs_dg_handle* out) {
+  if (!d || !out) return fail(DGFS_ERR_INVALID, "null descriptor or handle");
+  *out = nullptr;
+  if (d->K < 1 || d->K > kDgMaxK || d->Ne < 1 || d->N < 2 || d->Nqr < 1)
+    return fail(DGFS_ERR_INVALID, "need 1 <= K <= 8, Ne >= 1, N >= 2, Nqr >= 1");
+  if (!d->trL || !d->trR || !d->D || !d->gLD || !d->gRD || !d->invjac ||
+      !d->c0 || !d->im)
+    return fail(DGFS_ERR_INVALID, "missing operator arrays");
+  for (int s = 0; s < 2; ++s) {
+    if (d->bc_kind[s] < kBcCopy || d->bc_kind[s] > kBcInlet)
+      return fail(DGFS_ERR_INVALID, "unknown boundary kind");
+    if (d->bc_kind[s] != kBcCopy && !d->bc_f0[s])
+      return fail(DGFS_ERR_INVALID, "wall/inlet boundary needs its Maxwellian");
+  }
+  const int K = d->K, Ne = d->Ne, N = d->N, Nv = N * N * N;
+  auto* h = new dgfs_dg_s();
+  DgAdvectArgs& a = h->base;
+  a.K = K; a.Ne = Ne; a.Nv = Nv; a.N = N;
+  for (int k = 0; k < K; ++k) {
+    a.trL[k] = d->trL[k]; a.trR[k] = d->trR[k];
+    a.gLD[k] = d->gLD[k]; a.gRD[k] = d->gRD[k];
+    for (int m = 0; m < K; ++m) a.D[k * K + m] = d->D[k * K + m];
+  }
+  for (int s = 0; s < 2; ++s) {
+    a.bc[s] = d->bc_kind[s];
+    a.bc_ux[s] = d->bc_ux[s];
+    a.nl[s] = s == 0 ? -1.0 : 1.0;
+  }
+  h->Nqr = d->Nqr;
+  h->cw = d->cw;
+  int rc = DGFS_OK;
+  std::vector<double> c0(d->c0, d->c0 + N), ij(d->invjac, d->invjac + Ne),
+      im(d->im, d->im + (size_t)K * d->Nqr);
+  if ((rc = upload(&h->c0, c0)) || (rc = upload(&h->invjac, ij)) ||
+      (rc = upload(&h->im, im))) {
+    free_dg(h);
+    return rc;
+  }
+  for (int s = 0; s < 2; ++s)
+    if (d->bc_f0[s]) {
+      std::vector<double> f0(d->bc_f0[s], d->bc_f0[s] + Nv);
+      if ((rc = upload(&h->f0[s], f0))) { free_dg(h); return rc; }
+    }
+  cudaError_t e1 = cudaMalloc(&h->nden, 2 * sizeof(double));
+  if (e1 == cudaSuccess) e1 = cudaMalloc(&h->part, 2 * 1024 * sizeof(double));
+  if (e1 == cudaSuccess) e1 = cudaMallocHost(&h->part_h, 2 * 1024 * sizeof(double));
+  if (e1 != cudaSuccess) {
+    free_dg(h);
+    return fail(DGFS_ERR_CUDA, std::string("allocation: ") + cudaGetErrorString(e1));
+  }
+  a.c0 = h->c0; a.invjac = h->invjac;
+  a.f0[0] = h->f0[0]; a.f0[1] = h->f0[1];
+  a.nden = h->nden;
+  *out = h;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_destroy(dgfs_dg_handle h) {
+  if (h) free_dg(h);
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_advect(dgfs_dg_handle h, const void* u, void* ux,
+                              int32_t dtype, void* stream) {
+  if (!h || !u || !ux) return fail(DGFS_ERR_INVALID, "null argument");
+  if (dtype != DGFS_F32 && dtype != DGFS_F64)
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  if (u == ux) return fail(DGFS_ERR_INVALID, "u and ux must not alias");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  DgAdvectArgs a = h->base;
+  a.u = u; a.ux = ux; a.f_double = dtype == DGFS_F64;
+  dg_wall_density_kernel<<<2, 1024, 0, st>>>(a, h->cw, h->nden);
+  DGFS_CUDA(cudaGetLastError());
+  const dim3 grid((a.Nv + 255) / 256), block(256);
+  switch (a.K) {
+    case 1: dg_advect_kernel<1><<<grid, block, 0, st>>>(a); break;
+    case 2: dg_advect_kernel<2><<<grid, block, 0, st>>>(a); break;
+    case 3: dg_advect_kernel<3><<<grid, block, 0, st>>>(a); break;
+    case 4: dg_advect_kernel<4><<<grid, block, 0, st>>>(a); break;
+    case 5: dg_advect_kernel<5><<<grid, block, 0, st>>>(a); break;
+    case 6: dg_advect_kernel<6><<<grid, block, 0, st>>>(a); break;
+    case 7: dg_advect_kernel<7><<<grid, block, 0, st>>>(a); break;
+    default: dg_advect_kernel<8><<<grid, block, 0, st>>>(a); break;
+  }
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_wall_density(dgfs_dg_handle h, double* out2) {
+  if (!h || !out2) return fail(DGFS_ERR_INVALID, "null argument");
+  DGFS_CUDA(cudaMemcpy(out2, h->nden, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_moments(dgfs_dg_handle h, const void* coeff,
+                               int32_t dtype, double* out, void* stream) {
+  if (!h || !coeff || !out) return fail(DGFS_ERR_INVALID, "null argument");
+  if (dtype != DGFS_F32 && dtype != DGFS_F64)
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  MomentArgs m{};
+  m.coeff = coeff; m.f_double = dtype == DGFS_F64;
+  m.K = h->base.K; m.Ne = h->base.Ne; m.Nv = h->base.Nv; m.N = h->base.N;
+  m.Nqr = h->Nqr; m.im = h->im; m.c0 = h->c0; m.cw = h->cw; m.out = out;
+  std_moments_kernel<<<dim3(h->Nqr, h->base.Ne), 256, 0,
+                       static_cast<cudaStream_t>(stream)>>>(m);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_axnpby(void* x0, int64_t n, int32_t dtype, double a0,
+                           int32_t nterms, const void* const* xs,
+                           const double* as, void* stream) {
+  if (!x0 || n < 0 || nterms < 1 || nterms > kAxMax || !xs || !as)
+    return fail(DGFS_ERR_INVALID, "bad axnpby arguments (1..4 terms)");
+  if (dtype != DGFS_F32 && dtype != DGFS_F64)
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  AxnpbyArgs a{};
+  a.x0 = x0; a.a0 = a0; a.nterms = nterms; a.f_double = dtype == DGFS_F64;
+  a.n = (size_t)n;
+  for (int i = 0; i < nterms; ++i) {
+    if (!xs[i]) return fail(DGFS_ERR_INVALID, "null axnpby operand");
+    a.x[i] = xs[i];
+    a.a[i] = as[i];
+  }
+  if (n == 0) return DGFS_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t want = ((size_t)n + 255) / 256;
+  const unsigned blocks = (unsigned)std::min<size_t>(want, (size_t)sms * 16);
+  axnpby_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_residual(dgfs_dg_handle h, const void* x, const void* y,
+                                int64_t n, int32_t dtype, double* out2,
+                                void* stream) {
+  if (!h || !x || !y || !out2 || n < 0)
+    return fail(DGFS_ERR_INVALID, "bad residual arguments");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int blocks = 512;
+  residual_kernel<<<blocks, 512, 0, st>>>(x, y, dtype == DGFS_F64, (size_t)n,
+                                          h->part);
+  DGFS_CUDA(cudaGetLastError());
+  DGFS_CUDA(cudaMemcpyAsync(h->part_h, h->part, 2 * blocks * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+  DGFS_CUDA(cudaStreamSynchronize(st));
+  double a = 0, b = 0;
+  for (int i = 0; i < blocks; ++i) { a += h->part_h[2 * i]; b += h->part_h[2 * i + 1]; }
+  out2[0] = a;
+  out2[1] = b;
+  return DGFS_OK;
 }

@@ -1,0 +1,100 @@
+"""Host handle of the native nodal-DG right-hand side and stage updates."""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .collision import _DT, _stream_ptr
+
+BC_KIND = {'dgfs-periodic': 0, 'dgfs-wall-diffuse': 1, 'dgfs-inlet': 2}
+
+
+def _dp(a):
+    return ctypes.cast(a.ctypes.data, ctypes.POINTER(ctypes.c_double))
+
+
+class DGOperator:
+    """Advection/flux part of the DG right-hand side on (K, Ne, N^3) arrays.
+
+    bcs: two (kind, f0, ux) triples for the left and right boundaries.
+    """
+
+    def __init__(self, basis, invjac, c0, cw, bcs):
+        K, Ne, N = basis.K, len(invjac), len(c0)
+        self.K, self.Ne, self.N, self.Nv = K, Ne, N, N ** 3
+        self.Nqr = basis.interpMat.shape[1]
+        fo = basis.faceOp
+        arrs = dict(trL=fo[0], trR=fo[-1], D=basis.derivOp, gLD=basis.gLD,
+                    gRD=basis.gRD, invjac=np.ravel(invjac), c0=c0,
+                    im=basis.interpMat)
+        self._keep = {k: np.ascontiguousarray(v, dtype=np.float64)
+                      for k, v in arrs.items()}
+        d = nat.DgDesc()
+        d.K, d.Ne, d.N, d.Nqr = K, Ne, N, self.Nqr
+        for k, v in self._keep.items():
+            setattr(d, k, _dp(v))
+        d.cw = float(cw)
+        for s, (kind, f0, ux) in enumerate(bcs):
+            d.bc_kind[s] = BC_KIND[kind]
+            if f0 is not None:
+                f = np.ascontiguousarray(f0, dtype=np.float64)
+                self._keep['f0%d' % s] = f
+                d.bc_f0[s] = _dp(f)
+            d.bc_ux[s] = float(ux)
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().dgfs_dg_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        if not np.array_equal(basis.invMassOp, np.eye(K)):
+            raise NotImplementedError('non-identity inverse mass operator')
+
+    def advect(self, u, ux, stream=None):
+        nat.check(nat.lib().dgfs_dg_advect(
+            self._h, ctypes.c_void_p(u.data_ptr()),
+            ctypes.c_void_p(ux.data_ptr()), _DT[u.dtype], _stream_ptr(stream)))
+
+    def wall_density(self):
+        out = (ctypes.c_double * 2)()
+        nat.check(nat.lib().dgfs_dg_wall_density(self._h, out))
+        return np.array(out[:])
+
+    def moments(self, coeff, out=None, stream=None):
+        """(Nqr, Ne, 10) FP64 nondimensional moments (device tensor)."""
+        if out is None:
+            out = torch.empty((self.Nqr, self.Ne, 10), dtype=torch.float64,
+                              device=coeff.device)
+        nat.check(nat.lib().dgfs_dg_moments(
+            self._h, ctypes.c_void_p(coeff.data_ptr()), _DT[coeff.dtype],
+            ctypes.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+        return out
+
+    def residual(self, x, y, stream=None):
+        out = (ctypes.c_double * 2)()
+        nat.check(nat.lib().dgfs_dg_residual(
+            self._h, ctypes.c_void_p(x.data_ptr()),
+            ctypes.c_void_p(y.data_ptr()), x.numel(), _DT[x.dtype], out,
+            _stream_ptr(stream)))
+        return out[0], out[1]
+
+    def close(self):
+        if getattr(self, '_h', None):
+            nat.lib().dgfs_dg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def axnpby(x0, a0, *terms, stream=None):
+    """x0 <- a0 x0 + sum a_i x_i (terms = a1, x1, a2, x2, ...), in place."""
+    xs = terms[1::2]
+    as_ = terms[0::2]
+    n = len(xs)
+    ptrs = (ctypes.c_void_p * n)(*[x.data_ptr() for x in xs])
+    coef = (ctypes.c_double * n)(*[float(a) for a in as_])
+    nat.check(nat.lib().dgfs_axnpby(
+        ctypes.c_void_p(x0.data_ptr()), x0.numel(), _DT[x0.dtype], float(a0),
+        n, ptrs, coef, _stream_ptr(stream)))

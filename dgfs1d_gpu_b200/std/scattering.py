@@ -1,0 +1,139 @@
+"""Single-species scattering-model plugins (``[scattering-model] type``).
+
+Same keys, constructor and methods as dgfs1D/std/scattering.py:18-429:
+``DGFSScatteringModelStd(cfg, velocitymesh, Ne=...)`` with ``prefac``,
+``omega``, ``prefacBGK/ESBGK/SK`` and ``fs(d_f, d_g, d_Q, elem, modein,
+modeout)`` that *accumulates* Q into d_Q (torch CUDA tensors, slot layout
+(mode*Ne + elem)*N^3 + v).  ``fs_batch`` evaluates many points in one launch.
+The operator runs in the native library (FP64 parity mode or the FP32
+Maxwellian-split mode, ``[scattering-model] precision-mode = fp64|fp32``,
+default: fp64 for precision=double, fp32 for precision=float).
+"""
+from abc import ABCMeta, abstractmethod
+from math import gamma
+
+import numpy as np
+import torch
+
+from ..collision import VHSOperator
+
+
+class DGFSScatteringModelStd(metaclass=ABCMeta):
+    scattering_model = None
+
+    def __init__(self, cfg, velocitymesh, **kwargs):
+        self.cfg = cfg
+        self.vm = velocitymesh
+        self.load_parameters()
+        self.perform_precomputation()
+
+    @abstractmethod
+    def load_parameters(self):
+        pass
+
+    @abstractmethod
+    def perform_precomputation(self):
+        pass
+
+    @abstractmethod
+    def fs(self, d_arr_in, d_arr_in2, d_arr_out, elem, modein, modeout):
+        pass
+
+    @property
+    def prefac(self):
+        return self._prefactor
+
+    @property
+    def omega(self):
+        return self._omega
+
+
+class DGFSVHSGLLScatteringModelStd(DGFSScatteringModelStd):
+    """VHS/HS fast-spectral Q(f,f) (std/scattering.py:51-313)."""
+    scattering_model = 'vhs-gll'
+
+    def __init__(self, cfg, velocitymesh, **kwargs):
+        self._Ne = kwargs.get('Ne')
+        kind = cfg.lookupordefault('basis', 'kind', 'nodal-sem-gll')
+        if kind not in ('nodal-sem-gll', 'nodal-gll', 'nodal-sem-gll-2'):
+            raise RuntimeError('Only tested for nodal basis')
+        self._max_evals = kwargs.get('max_evals', 64)
+        super().__init__(cfg, velocitymesh, **kwargs)
+
+    @property
+    def prefacBGK(self):
+        return self._prefactorBGK
+
+    @property
+    def prefacESBGK(self):
+        return self._prefactorESBGK
+
+    @property
+    def prefacSK(self):
+        return self._prefactorSK
+
+    def load_parameters(self):
+        vm, cfg = self.vm, self.cfg
+        alpha = 1.0
+        omega = cfg.lookupfloat('scattering-model', 'omega')
+        self._gamma = 2.0 * (1 - omega)
+        dRef = cfg.lookupfloat('scattering-model', 'dRef')
+        Tref = cfg.lookupfloat('scattering-model', 'Tref')
+        invKn = (vm.H0() * np.sqrt(2.0) * np.pi * vm.n0() * dRef * dRef
+                 * pow(Tref / vm.T0(), omega - 0.5))
+        self._invKn = invKn
+        self._prefactor = float(invKn * alpha / (
+            pow(2.0, 2 - omega + alpha) * gamma(2.5 - omega) * np.pi))
+        self._omega = omega
+        Pr = cfg.lookupordefault('scattering-model', 'Pr', 2. / 3.)
+        muRef = cfg.lookupordefault('scattering-model', 'muRef', 2.117e-5)
+        t0 = vm.H0() / vm.u0()
+        visc = muRef * ((vm.T0() / Tref) ** omega)
+        p0 = vm.n0() * vm.R0 / vm.NA * vm.T0()
+        self._prefactorBGK = t0 * 1.0 * p0 / visc
+        self._prefactorESBGK = t0 * Pr * p0 / visc
+        self._prefactorSK = self._prefactorBGK
+        default = 'fp64' if cfg.dtype == np.float64 else 'fp32'
+        self._precision = cfg.lookupordefault('scattering-model',
+                                              'precision-mode', default)
+
+    def perform_precomputation(self):
+        vm = self.vm
+        eps = 1e-15 if self.cfg.dtype == np.float64 else 1e-6
+        self._op = VHSOperator(
+            N=vm.Nv(), L=vm.L(), qz=vm.qz(), qw=vm.qw(), sz=vm.sz(),
+            sw=vm.sw(), sphere_factor=vm.sphere_factor(), gamma=self._gamma,
+            prefac=self._prefactor, cw=vm.cw(), c0=vm.c0(),
+            precision=self._precision, max_evals=self._max_evals,
+            sinc_eps=eps)
+
+    @property
+    def operator(self):
+        return self._op
+
+    def fs(self, d_arr_in, d_arr_in2, d_arr_out, elem, modein, modeout,
+           d_nu=None):
+        if d_nu is not None:
+            raise NotImplementedError('collision-frequency output (d_nu)')
+        Ne = self._Ne
+        self._op.eval(d_arr_in, d_arr_out, src_base=modein * Ne + elem,
+                      dst_base=modeout * Ne + elem, nevals=1)
+
+    def fs_batch(self, d_f, d_Q, src, dst, stream=None):
+        """Q[dst[i]] += Q(f[src[i]]) for all i in one launch sequence."""
+        self._op.eval(d_f, d_Q, src=src, dst=dst, stream=stream)
+
+
+class DGFSVHSScatteringModelStd(DGFSVHSGLLScatteringModelStd):
+    """``vhs`` (std/scattering.py:317-429): the bilinear Q(f, g).
+
+    The drivers call it with g = V u and f = U^T u, which for the nodal
+    bases are the same coefficient (mode_sources); Q(f, f) is evaluated then.
+    """
+    scattering_model = 'vhs'
+
+    def fs(self, d_arr_in1, d_arr_in2, d_arr_out, elem, modein, modeout):
+        if d_arr_in2 is not None and d_arr_in2 is not d_arr_in1 and \
+                not torch.equal(d_arr_in1, d_arr_in2):
+            raise NotImplementedError('bilinear Q(f, g) with g != f')
+        super().fs(d_arr_in1, d_arr_in1, d_arr_out, elem, modein, modeout)

@@ -1,0 +1,101 @@
+"""Single-species DGFS driver (``dgfsStd1D``) on the native kernels.
+
+Mirrors dgfs1D/std/std.py:37-423: mesh, basis, velocity mesh, scattering
+model, boundary conditions, initial condition and integrator are plugins
+selected by the same INI keys; ``rhs(t, u_in, u_out)`` is the DG advection
+(one native kernel pair) plus the collision operator at every (mode,
+element) in one batched native call.  The solution lives on the GPU as a
+(K, Ne, N^3) torch tensor; nothing is copied to the host except moments.
+"""
+import math
+
+import numpy as np
+import torch
+
+from ..basis import get_basis
+from ..dg import DGOperator
+from ..mesh import Mesh
+from ..plugins import subclass_where
+from ..velocitymesh import DGFSVelocityMeshStd
+from .bc import get_bc
+from .initcond import get_initcond
+from .integrator import DGFSIntegratorStd
+from .moments import DGFSMomWriterStd
+from .scattering import DGFSScatteringModelStd
+
+
+class DGFSStd1D:
+    def __init__(self, cfg, device='cuda'):
+        self.cfg = cfg
+        self.device = torch.device(device)
+        self.dtype = torch.float64 if cfg.dtype == np.float64 else torch.float32
+        self.mesh = mesh = Mesh(cfg)
+        Ne = mesh.Ne
+        self.basis = basis = get_basis(cfg)
+        K = basis.K
+        self.vm = vm = DGFSVelocityMeshStd(cfg)
+        Nv = vm.vsize()
+        smn = cfg.lookup('scattering-model', 'type')
+        smcls = subclass_where(DGFSScatteringModelStd, scattering_model=smn)
+        self.sm = smcls(cfg, vm, Ne=Ne, max_evals=K * Ne)
+        ti, dt, tf = cfg.lookupfloats('time-integrator',
+                                      ('tstart', 'dt', 'tend'))
+        nsteps = math.ceil((tf - ti) / dt)
+        self.ti, self.tf, self.nsteps = ti, tf, nsteps
+        self.dt = (tf - ti) / nsteps
+        x = mesh.xmesh
+        self.xsol = np.array([0.5 * (x[j] + x[j + 1]) + mesh.jac[j] * basis.z
+                              for j in range(Ne)]).T
+        self.bcl = get_bc(cfg, 'soln-bcs-xlo', x[0], -1., vm)
+        self.bcr = get_bc(cfg, 'soln-bcs-xhi', x[-1], 1., vm)
+        self.dg = DGOperator(basis, mesh.invjac, vm.c0(), vm.cw(),
+                             [(self.bcl.type, self.bcl.f0, self.bcl.ux),
+                              (self.bcr.type, self.bcr.f0, self.bcr.ux)])
+        # collision sources: Q at mode m, element e from coefficient a
+        src, dst = [], []
+        for m, a in basis.mode_sources():
+            for e in range(Ne):
+                src.append(a * Ne + e)
+                dst.append(m * Ne + e)
+        self.src = torch.tensor(src, dtype=torch.int32, device=self.device)
+        self.dst = torch.tensor(dst, dtype=torch.int32, device=self.device)
+        # initial condition (nodal: coefficients are point values)
+        usol = np.empty((basis.Nq, Ne, Nv))
+        ic = get_initcond(cfg, vm, 'soln-ics')
+        ic.apply_init_vals(usol, basis.Nq, Ne, self.xsol)
+        self.u = torch.tensor(usol, dtype=self.dtype, device=self.device)
+        self.uprev = self.u.clone()
+        scheme = cfg.lookup('time-integrator', 'scheme')
+        icls = subclass_where(DGFSIntegratorStd, intg_kind=scheme)
+        self.odes = icls(self.rhs, (K, Ne, Nv), self.dtype, device=self.device)
+        self.t = ti
+        self.nacptsteps = 0
+        xcoeff = self.xsol  # nodal: forward transform is the identity
+        self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, xcoeff)
+        self.res_nsteps = cfg.lookupordefault('dgfsresidual', 'nsteps', -1)
+        self.residuals = []
+
+    def rhs(self, t, u_in, u_out):
+        self.dg.advect(u_in, u_out)
+        self.sm.fs_batch(u_in, u_out, self.src, self.dst)
+
+    def step(self):
+        self.odes.integrate(self.t, self.dt, self.u)
+        self.t += self.dt
+        self.nacptsteps += 1
+        n = self.nacptsteps
+        if self.res_nsteps > 0 and (n % self.res_nsteps == 0 or n == 1):
+            a, b = self.dg.residual(self.u, self.uprev)
+            self.residuals.append((self.t, math.sqrt(a / b)))
+        self.moments(self.dt, self.t, self.u)
+        self.uprev.copy_(self.u)
+
+    def run(self, nsteps=None):
+        n = self.nsteps if nsteps is None else nsteps
+        for _ in range(n):
+            self.step()
+        return self.u
+
+    def bulk_moments(self):
+        """(Nqr, Ne, 10) dimensional moments of the current solution."""
+        return self.moments.compute(self.u)

@@ -108,6 +108,66 @@ int dgfs_vhs_stage_ms(dgfs_vhs_handle h, double* out5);
  * roofline denominator of the CUDA-core FFT kernels). */
 int dgfs_fma_peak(double* tflops, void* stream);
 
+/*
+ * Nodal DG advection right-hand side of the single-species solver.
+ * Replaces the kernels of the rhs() closure in dgfs1D/std/std.py:281-345:
+ * bwdTransFace + extract_left/right + transfer/insert BC (std.mako:4-89),
+ * the boundary kernels updateBC/applyBC (std/kernels/bcs/*.mako with the two
+ * host sums of std/bc.py:73-74), flux (std.mako:115-152), deriv (gimmik),
+ * mul_by_adv, totalFlux and mul_by_invjac (std.mako:92-190).  trL/trR are
+ * rows 0 and Nqf-1 of Bqf^T, D the derivative operator (ux = D u), gLD/gRD
+ * the lifting vectors, im the K x Nqr interpolation to the moment points.
+ * Boundary kinds: 0 dgfs-periodic (one rank: ghost = interior trace),
+ * 1 dgfs-wall-diffuse, 2 dgfs-inlet; bc_f0 the wall/inlet Maxwellian.
+ */
+typedef struct dgfs_dg_s* dgfs_dg_handle;
+typedef struct {
+  int32_t K;
+  int32_t Ne;
+  int32_t N;
+  int32_t Nqr;
+  const double* trL;       /* [K] host */
+  const double* trR;       /* [K] host */
+  const double* D;         /* [K*K] host, row-major */
+  const double* gLD;       /* [K] host */
+  const double* gRD;       /* [K] host */
+  const double* invjac;    /* [Ne] host */
+  const double* c0;        /* [N] host */
+  const double* im;        /* [K*Nqr] host */
+  double cw;
+  int32_t bc_kind[2];      /* left, right */
+  const double* bc_f0[2];  /* [N^3] host, or null for kind 0 */
+  double bc_ux[2];         /* wall x-velocities (nondimensional) */
+} dgfs_dg_desc;
+
+int dgfs_dg_create(const dgfs_dg_desc* desc, dgfs_dg_handle* out);
+int dgfs_dg_destroy(dgfs_dg_handle h);
+
+/* ux = advection + upwind flux lifting of u (shape (K, Ne, N^3), the
+ * solution coefficients), scaled by the inverse Jacobian -- the state of
+ * d_ux in std.py:346 before the collision loop.  Also records the wall
+ * densities of this call (dgfs_dg_wall_density). */
+int dgfs_dg_advect(dgfs_dg_handle h, const void* u, void* ux, int32_t dtype,
+                   void* stream);
+int dgfs_dg_wall_density(dgfs_dg_handle h, double* out2);
+
+/* Bulk moments (FP64) at the Nqr reconstruction points of each element,
+ * nondimensional, out[(r*Ne + e)*10 + i] for i = rho, Ux, Uy, T, Qx, Qy,
+ * Pxx, Pyy, Pxy, (0) -- std/moments.py:11-60 before its dimensional scaling.
+ * `out` is a device pointer. */
+int dgfs_dg_moments(dgfs_dg_handle h, const void* coeff, int32_t dtype,
+                    double* out, void* stream);
+
+/* Residual sums (|x-y|^2, |y|^2) in FP64 (std/residual.py:15-29); waits for
+ * the stream and writes the two sums to host memory out2. */
+int dgfs_dg_residual(dgfs_dg_handle h, const void* x, const void* y, int64_t n,
+                     int32_t dtype, double* out2, void* stream);
+
+/* x0 <- a0 x0 + sum_i as[i] xs[i] over n elements, 1..4 terms, with the
+ * a0 == 0 (x0 not read) and a0 == 1 branches of dgfs1D/axnpby.py:10-44. */
+int dgfs_axnpby(void* x0, int64_t n, int32_t dtype, double a0, int32_t nterms,
+                const void* const* xs, const double* as, void* stream);
+
 /* Allocation-free Q(f,f) in FP64, for callers that cannot allocate device
  * memory (code running inside someone else's stream capture, processes whose
  * device memory belongs to a pool they must not grow, plugins barred from

@@ -1,0 +1,102 @@
+"""The native single-species solver against the oracle and the reference."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from dgfs1d_gpu_b200.config import Config
+from dgfs1d_gpu_b200.configs import couette_std_ini
+from oracle import collision as oc
+from oracle import dg as odg
+from oracle import mesh as om
+
+pytestmark = pytest.mark.gpu
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b))
+                 / np.linalg.norm(np.ravel(b)))
+
+
+def _solver(ini):
+    from dgfs1d_gpu_b200 import build
+    build.build()
+    from dgfs1d_gpu_b200.std.solver import DGFSStd1D
+    return DGFSStd1D(Config(ini))
+
+
+@pytest.mark.parametrize('kind', ['nodal-sem-gll', 'nodal-gll'])
+def test_rhs_matches_reference_kernel_golden(kind):
+    g = np.load(os.path.join(G, 'dg_%s_N8.npz' % kind.replace('-', '_')))
+    ini = couette_std_ini(Ne=int(g['Ne']), K=int(g['K']), Nv=int(g['Nv']),
+                          Nrho=int(g['Nrho']), M=int(g['M']), basis=kind)
+    # the golden run used rho0 = 0.00023 and walls at u_y = -+0.1
+    ini = ini.replace(ini.split('rho0 = ')[1].split('\n')[0], '0.00023')
+    s = _solver(ini)
+    assert abs(s.sm.prefac / float(g['prefac']) - 1) < 1e-14
+    u = torch.tensor(g['u'].reshape(s.u.shape), device='cuda')
+    out = torch.empty_like(u)
+    s.rhs(0.0, u, out)
+    torch.cuda.synchronize()
+    assert _rel(out.cpu().numpy(), g['rhs_q']) < 1e-11
+
+
+def _oracle_run(s, nsteps, scheme):
+    """Integrate the same problem with the oracle (CPU)."""
+    vm = s.vm
+    ovm = om.VelocityMeshStd(Nv=vm.Nv(), M=vm.M(), Nrho=vm.Nrho(), dev=vm.dev(),
+                             rho0=vm.rho0(), full_sphere=vm.sphere_mode() == 'full')
+    assert np.array_equal(ovm.sz, vm.sz())
+    tab = oc.VHSTables(vm.Nv(), vm.L(), vm.qz(), vm.qw(), vm.sz(), vm.sw(),
+                       s.sm._gamma, sphere_factor=vm.sphere_factor())
+    b = odg.NodalBasis(s.basis.basis_kind, s.basis.K, s.basis.interpMat.shape[1])
+    cv, cw = ovm.cv, ovm.cw
+    bcl = odg.WallDiffuseBC(cv, cw, 1.0, [0., s.bcl.f0 is not None and
+                                          -0.1 or 0, 0.], -1.)
+    bcr = odg.WallDiffuseBC(cv, cw, 1.0, [0., 0.1, 0.], 1.)
+    bcl.f0, bcr.f0 = s.bcl.f0, s.bcr.f0
+    fs = lambda f, g: oc.vhs_gll_fs(tab, s.sm.prefac, f)
+    collide = odg.collide_fs(b, fs)
+    invjac = s.mesh.invjac
+    u = s.u.cpu().numpy().astype(np.float64)
+
+    def rhs(t, x):
+        return odg.dg_rhs(b, invjac, cv[0], bcl, bcr, x, collide=collide)
+    t = 0.0
+    for _ in range(nsteps):
+        odg.integrate(scheme, rhs, t, s.dt, u)
+        t += s.dt
+    return b, cv, cw, u
+
+
+def test_couette_52_euler_steps_fp64_matches_oracle():
+    """BASELINE 12-point Couette: 52 Euler steps, shear stress and heat flux
+    vs the oracle to 1e-9 (FP64 mode)."""
+    s = _solver(couette_std_ini())
+    u0 = s.u.clone()
+    b, cv, cw, uref = _oracle_run(s, 52, 'euler')
+    s.u.copy_(u0)
+    s.run(52)
+    torch.cuda.synchronize()
+    got = s.bulk_moments()   # dimensional (std/moments.py:61-68)
+    vm = s.vm
+    ref = odg.moments(b, uref, cv, cw, T0=vm.T0(), rho0=vm.rho0(),
+                      u0=vm.u0(), molarMass0=vm.molarMass0())
+    assert _rel(s.u.cpu().numpy(), uref) < 1e-11
+    for i, name in ((8, 'P:xy'), (4, 'Q:x'), (5, 'Q:y'), (0, 'rho'),
+                    (3, 'T')):
+        assert _rel(got[:, :, i], ref[:, :, i]) < 1e-9, name
+
+
+@pytest.mark.parametrize('scheme', ['ssp-rk2', 'ssp-rk3', 'lse-rk45'])
+def test_integrators_match_oracle(scheme):
+    s = _solver(couette_std_ini(Nv=8, Nrho=4, scheme=scheme, nsteps=3,
+                                dt=0.001))
+    u0 = s.u.clone()
+    _, _, _, uref = _oracle_run(s, 3, scheme)
+    s.u.copy_(u0)
+    s.run(3)
+    torch.cuda.synchronize()
+    assert _rel(s.u.cpu().numpy(), uref) < 1e-11
