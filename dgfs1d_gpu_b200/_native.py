@@ -31,6 +31,18 @@ class VhsDesc(ctypes.Structure):
     ]
 
 
+class VssDesc(ctypes.Structure):
+    """Mirror of ``dgfs_vss_desc`` (include/dgfs_sm100.h)."""
+    _fields_ = [
+        ('N', ctypes.c_int32), ('Nrho', ctypes.c_int32), ('M', ctypes.c_int32),
+        ('Mpre', ctypes.c_int32), ('nspcs', ctypes.c_int32),
+        ('L', ctypes.c_double), ('qz', _c_dp), ('qw', _c_dp), ('sz', _c_dp),
+        ('sw', ctypes.c_double), ('szpre', _c_dp), ('masses', _c_dp),
+        ('gamma', _c_dp), ('eta', _c_dp), ('prefac', _c_dp),
+        ('max_evals', ctypes.c_int32),
+    ]
+
+
 class DgDesc(ctypes.Structure):
     """Mirror of ``dgfs_dg_desc`` (include/dgfs_sm100.h)."""
     _fields_ = [
@@ -76,6 +88,14 @@ _SIGNATURES = [
      [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ('dgfs_fma_peak', ctypes.c_int,
      [ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ('dgfs_vss_create', ctypes.c_int,
+     [ctypes.POINTER(VssDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    ('dgfs_vss_destroy', ctypes.c_int, [ctypes.c_void_p]),
+    ('dgfs_vss_eval', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_void_p]),
     ('dgfs_dg_create', ctypes.c_int,
      [ctypes.POINTER(DgDesc), ctypes.POINTER(ctypes.c_void_p)]),
     ('dgfs_dg_destroy', ctypes.c_int, [ctypes.c_void_p]),

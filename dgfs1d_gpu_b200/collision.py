@@ -101,3 +101,64 @@ class VHSOperator:
             self.close()
         except Exception:
             pass
+
+
+class VSSOperator:
+    """Batched binary-mixture VSS Q_pq(f_p, f_q) (``vss``), FP64.
+
+    gamma, eta, prefac: (nspcs, nspcs) arrays (pair pq at [p, q]).
+    """
+
+    def __init__(self, N, L, qz, qw, sz, sw, szpre, masses, gamma, eta,
+                 prefac, max_evals=64):
+        self.N, self.n = int(N), int(N) ** 3
+        ns = len(masses)
+        self.nspcs = ns
+        self._keep = [np.ascontiguousarray(np.asarray(x, dtype=np.float64).ravel())
+                      for x in (qz, qw, sz, szpre, masses, gamma, eta, prefac)]
+        qz_, qw_, sz_, szp_, m_, g_, e_, p_ = self._keep
+        d = nat.VssDesc()
+        d.N, d.Nrho, d.M, d.Mpre, d.nspcs = self.N, len(qz_), len(sz_) // 3, \
+            len(szp_) // 3, ns
+        d.L, d.sw = float(L), float(sw)
+        d.qz, d.qw, d.sz, d.szpre = _dptr(qz_), _dptr(qw_), _dptr(sz_), _dptr(szp_)
+        d.masses, d.gamma, d.eta, d.prefac = _dptr(m_), _dptr(g_), _dptr(e_), \
+            _dptr(p_)
+        d.max_evals = int(max_evals)
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().dgfs_vss_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        self.prefac = np.asarray(prefac, dtype=np.float64).reshape(ns, ns)
+
+    def eval(self, p, q, fp, fq, Qp, src=None, dst=None, src_base=0,
+             dst_base=0, nevals=None, stream=None):
+        """Q_p[dst(i)] += Q_pq(f_p[src(i)], f_q[src(i)])."""
+        for t, name in ((fp, 'f_p'), (fq, 'f_q'), (Qp, 'Q_p')):
+            _check_dist(t, name)
+        if fp.dtype != fq.dtype:
+            raise TypeError('f_p and f_q must have the same dtype')
+        nf = fp.numel() // self.n
+        if nevals is None:
+            nevals = len(src) if src is not None else nf - src_base
+        for sl, base, cnt, name in ((src, src_base, nf, 'src'),
+                                    (dst, dst_base, Qp.numel() // self.n, 'dst')):
+            if sl is None and (base < 0 or base + nevals > cnt):
+                raise IndexError(f'{name} slots out of range')
+        nat.check(nat.lib().dgfs_vss_eval(
+            self._h, int(p), int(q), ctypes.c_void_p(fp.data_ptr()),
+            ctypes.c_void_p(fq.data_ptr()), _DT[fp.dtype],
+            ctypes.c_void_p(Qp.data_ptr()), _DT[Qp.dtype],
+            ctypes.c_void_p(src.data_ptr() if src is not None else 0), int(src_base),
+            ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
+            int(nevals), _stream_ptr(stream)))
+
+    def close(self):
+        if getattr(self, '_h', None):
+            nat.lib().dgfs_vss_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -14,6 +14,7 @@
 #include "cluster_slab.cuh"
 #include "vhs_kernels.cuh"
 #include "dg_kernels.cuh"
+#include "vss_kernels.cuh"
 
 using namespace dgfs;
 
@@ -152,6 +153,7 @@ static int c64_of(int N) {
   switch (N) {
     case 8: return 1;
     case 16: return 2;
+    case 24: return 4;
     case 32: return 8;
     default: return 0;
   }
@@ -160,10 +162,16 @@ static int c32_of(int N) {
   switch (N) {
     case 8: return 1;
     case 16: return 1;
+    case 24: return 3;
     case 32: return 4;
     default: return 0;
   }
 }
+template <int N> struct VhsClusters;
+template <> struct VhsClusters<8> { static constexpr int c64 = 1, c32 = 1; };
+template <> struct VhsClusters<16> { static constexpr int c64 = 2, c32 = 1; };
+template <> struct VhsClusters<24> { static constexpr int c64 = 4, c32 = 3; };
+template <> struct VhsClusters<32> { static constexpr int c64 = 8, c32 = 4; };
 
 static size_t slab_bytes(int N, int C, size_t elem) {
   return (size_t)(N / C) * N * (N + 1) * elem;
@@ -205,7 +213,7 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_desc* d, dgfs_vhs_handle* out) {
   if (c64_of(d->N) == 0 || c32_of(d->N) == 0)
     return fail(DGFS_ERR_UNSUPPORTED,
                 "velocity grid N=" + std::to_string(d->N) +
-                    " is not compiled in (supported: 8, 16, 32)");
+                    " is not compiled in (supported: 8, 16, 24, 32)");
   if (int rc = ensure_twiddles()) return rc;
 
   const int N = d->N, n = N * N * N, Nrho = d->Nrho, M = d->M;
@@ -361,8 +369,8 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                    int q_double, const int32_t* src_slots, int src_base,
                    const int32_t* dst_slots, int dst_base, int nevals,
                    cudaStream_t st) {
-  constexpr int C64 = (N == 8) ? 1 : (N == 16 ? 2 : 8);
-  constexpr int C32 = (N == 8) ? 1 : (N == 16 ? 1 : 4);
+  constexpr int C64 = VhsClusters<N>::c64;
+  constexpr int C32 = VhsClusters<N>::c32;
   using G64 = Geo<N, C64>;
   using G32 = Geo<N, C32>;
   const bool fp32 = h->precision == DGFS_PREC_FP32;
@@ -477,6 +485,7 @@ extern "C" int dgfs_vhs_eval(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
     switch (h->N) {
       case 8: rc = vhs_run<8>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
       case 16: rc = vhs_run<16>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 24: rc = vhs_run<24>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
       case 32: rc = vhs_run<32>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
       default: return fail(DGFS_ERR_UNSUPPORTED, "N not compiled in");
     }
@@ -970,5 +979,208 @@ extern "C" int dgfs_dg_residual(dgfs_dg_handle h, const void* x, const void* y,
   for (int i = 0; i < blocks; ++i) { a += h->part_h[2 * i]; b += h->part_h[2 * i + 1]; }
   out2[0] = a;
   out2[1] = b;
+  return DGFS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// VSS binary-mixture operator
+// ---------------------------------------------------------------------------
+struct VssPair {
+  double2* b = nullptr;    // [Nrho][M][n]
+  double2* c = nullptr;    // [n]
+  double2* ph = nullptr;   // [Nrho][M][2][3][N]
+  double prefac = 0;
+};
+
+struct dgfs_vss_s {
+  int N = 0, Nrho = 0, M = 0, nspcs = 0, n = 0, max_evals = 0;
+  double* w = nullptr;     // [Nrho] w_r s_w / n
+  VssPair pair[16];
+  double2* F[2] = {nullptr, nullptr};  // [E][n] spectra of the two inputs
+};
+
+static void free_vss(dgfs_vss_s* h) {
+  for (auto& p : h->pair) {
+    if (p.b) cudaFree(p.b);
+    if (p.c) cudaFree(p.c);
+    if (p.ph) cudaFree(p.ph);
+  }
+  if (h->w) cudaFree(h->w);
+  for (auto* f : h->F)
+    if (f) cudaFree(f);
+  delete h;
+}
+
+template <int N> struct VssClusters;
+template <> struct VssClusters<8> { static constexpr int c = 1; };
+template <> struct VssClusters<16> { static constexpr int c = 2; };
+template <> struct VssClusters<24> { static constexpr int c = 6; };
+template <> struct VssClusters<32> { static constexpr int c = 16; };
+
+template <int N>
+static int vss_setup_pair(dgfs_vss_s* h, const dgfs_vss_desc* d, int p, int q,
+                          cudaStream_t st) {
+  const int Nrho = d->Nrho, M = d->M, Mpre = d->Mpre, n = N * N * N;
+  const int pq = p * d->nspcs + q;
+  VssPair& P = h->pair[pq];
+  P.prefac = d->prefac[pq];
+  const double mp = d->masses[p], mq = d->masses[q];
+  const double eta = d->eta[pq], gam = d->gamma[pq];
+  const double swpre = 4 * M_PI / Mpre;
+  std::vector<double> Bmk((size_t)M * Mpre), srho(Nrho), fb(Nrho), fc(Nrho);
+  for (int m = 0; m < M; ++m)
+    for (int k = 0; k < Mpre; ++k)
+      Bmk[(size_t)m * Mpre + k] = std::pow(
+          1 + d->sz[3 * m] * d->szpre[3 * k] + d->sz[3 * m + 1] * d->szpre[3 * k + 1] +
+              d->sz[3 * m + 2] * d->szpre[3 * k + 2],
+          eta);
+  for (int r = 0; r < Nrho; ++r) {
+    srho[r] = M_PI / d->L * d->qz[r];
+    fb[r] = swpre * std::pow(d->qz[r], gam + 2);
+    fc[r] = d->qw[r] * d->sw * fb[r];
+  }
+  std::vector<double2> ph((size_t)Nrho * M * 6 * N);
+  for (int r = 0; r < Nrho; ++r)
+    for (int m = 0; m < M; ++m)
+      for (int ax = 0; ax < 3; ++ax)
+        for (int l = 0; l < N; ++l) {
+          const double rl = (l < N / 2) ? l : l - N;
+          const double a = srho[r] * d->sz[3 * m + ax] * rl;
+          const size_t base = ((size_t)r * M + m) * 6 * N;
+          const double a1 = a * (mq / (mp + mq)), a2 = -a * (mp / (mp + mq));
+          ph[base + ax * N + l] = make_double2(std::cos(a1), std::sin(a1));
+          ph[base + (3 + ax) * N + l] = make_double2(std::cos(a2), std::sin(a2));
+        }
+  double *dB = nullptr, *ds = nullptr, *dfb = nullptr, *dfc = nullptr, *dspre = nullptr;
+  double2* cpart = nullptr;
+  std::vector<double> spre(d->szpre, d->szpre + 3 * Mpre);
+  int rc = DGFS_OK;
+  if ((rc = upload(&dB, Bmk)) || (rc = upload(&ds, srho)) || (rc = upload(&dfb, fb)) ||
+      (rc = upload(&dfc, fc)) || (rc = upload(&dspre, spre)) || (rc = upload(&P.ph, ph)))
+    return rc;
+  cudaError_t e1 = cudaMalloc(&P.b, sizeof(double2) * (size_t)Nrho * M * n);
+  if (e1 == cudaSuccess) e1 = cudaMalloc(&P.c, sizeof(double2) * n);
+  if (e1 == cudaSuccess) e1 = cudaMalloc(&cpart, sizeof(double2) * (size_t)Nrho * n);
+  if (e1 != cudaSuccess)
+    return fail(DGFS_ERR_CUDA, std::string("allocation: ") + cudaGetErrorString(e1));
+  VssSetupArgs a{};
+  a.Bmk = dB; a.spre = dspre; a.srho = ds; a.fac_b = dfb; a.fac_c = dfc;
+  a.mpq = mq / (mp + mq); a.M = M; a.Mpre = Mpre; a.Nrho = Nrho;
+  a.b = P.b; a.cpart = cpart;
+  const size_t smem = (2 * kVssKChunk + 4 * kVssKChunk * N) * sizeof(double2) +
+                      (size_t)M * kVssKChunk * sizeof(double);
+  if ((rc = launch_plain(vss_setup_kernel<N>, dim3(N, Nrho),
+                         dim3(vss_setup_threads<N>()), smem, st, a)))
+    return rc;
+  vss_sum_c_kernel<<<(n + 255) / 256, 256, 0, st>>>(cpart, Nrho, (size_t)n, P.c);
+  DGFS_CUDA(cudaGetLastError());
+  DGFS_CUDA(cudaStreamSynchronize(st));
+  cudaFree(dB); cudaFree(ds); cudaFree(dfb); cudaFree(dfc); cudaFree(dspre);
+  cudaFree(cpart);
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vss_create(const dgfs_vss_desc* d, dgfs_vss_handle* out) {
+  if (!d || !out) return fail(DGFS_ERR_INVALID, "null descriptor or handle");
+  *out = nullptr;
+  if (d->nspcs < 1 || d->nspcs > 4 || d->Nrho <= 0 || d->M <= 0 || d->M > 16 ||
+      d->Mpre <= 0 || d->max_evals <= 0)
+    return fail(DGFS_ERR_INVALID, "need 1 <= nspcs <= 4, 1 <= M <= 16, Nrho, Mpre, max_evals > 0");
+  if (!d->qz || !d->qw || !d->sz || !d->szpre || !d->masses || !d->gamma ||
+      !d->eta || !d->prefac)
+    return fail(DGFS_ERR_INVALID, "missing descriptor arrays");
+  if (d->N != 8 && d->N != 16 && d->N != 24 && d->N != 32)
+    return fail(DGFS_ERR_UNSUPPORTED, "VSS: N must be 8, 16, 24 or 32");
+  if (int rc = ensure_twiddles()) return rc;
+  auto* h = new dgfs_vss_s();
+  h->N = d->N; h->n = d->N * d->N * d->N; h->Nrho = d->Nrho; h->M = d->M;
+  h->nspcs = d->nspcs; h->max_evals = d->max_evals;
+  std::vector<double> w(d->Nrho);
+  for (int r = 0; r < d->Nrho; ++r) w[r] = d->qw[r] * d->sw / h->n;
+  int rc = upload(&h->w, w);
+  for (int p = 0; p < d->nspcs && !rc; ++p)
+    for (int q = 0; q < d->nspcs && !rc; ++q) {
+      switch (d->N) {
+        case 8: rc = vss_setup_pair<8>(h, d, p, q, 0); break;
+        case 16: rc = vss_setup_pair<16>(h, d, p, q, 0); break;
+        case 24: rc = vss_setup_pair<24>(h, d, p, q, 0); break;
+        default: rc = vss_setup_pair<32>(h, d, p, q, 0); break;
+      }
+    }
+  if (!rc) {
+    cudaError_t e1 = cudaMalloc(&h->F[0], sizeof(double2) * (size_t)h->max_evals * h->n);
+    if (e1 == cudaSuccess)
+      e1 = cudaMalloc(&h->F[1], sizeof(double2) * (size_t)h->max_evals * h->n);
+    if (e1 != cudaSuccess)
+      rc = fail(DGFS_ERR_CUDA, std::string("allocation: ") + cudaGetErrorString(e1));
+  }
+  if (rc) { free_vss(h); return rc; }
+  *out = h;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vss_destroy(dgfs_vss_handle h) {
+  if (h) free_vss(h);
+  return DGFS_OK;
+}
+
+template <int N>
+static int vss_run(dgfs_vss_s* h, int p, int q, const void* fp, const void* fq,
+                   int f_double, void* Q, int q_double, const int32_t* ss,
+                   int sb, const int32_t* ds, int db, int nevals,
+                   cudaStream_t st) {
+  constexpr int C = VssClusters<N>::c;
+  using G = Geo<N, C>;
+  int rc;
+  const VssPair& P = h->pair[p * h->nspcs + q];
+  for (int s = 0; s < 2; ++s) {
+    Fft3Args fa{};
+    fa.f = s == 0 ? fp : fq; fa.f_double = f_double; fa.slots = ss; fa.base = sb;
+    fa.out = h->F[s];
+    if ((rc = launch_cluster(fft3_forward_kernel<N, C>, dim3(C, nevals),
+                             dim3(G::NT), C, slab_bytes(N, C, sizeof(double2)),
+                             st, fa)))
+      return rc;
+  }
+  VssPairArgs a{};
+  a.Fp = h->F[0]; a.Fq = h->F[1]; a.b = P.b; a.c = P.c; a.ph = P.ph; a.w = h->w;
+  a.fp = fp; a.f_double = f_double; a.src_slots = ss; a.src_base = sb;
+  a.Q = Q; a.q_double = q_double; a.dst_slots = ds; a.dst_base = db;
+  a.prefac = P.prefac; a.Nrho = h->Nrho; a.M = h->M;
+  const size_t smem = 4 * slab_bytes(N, C, sizeof(double2)) + 6 * N * sizeof(double2);
+  return launch_cluster(vss_pair_kernel<N, C>, dim3(C, nevals), dim3(G::NT), C,
+                        smem, st, a);
+}
+
+extern "C" int dgfs_vss_eval(dgfs_vss_handle h, int32_t p, int32_t q,
+                             const void* f_p, const void* f_q, int32_t f_dtype,
+                             void* Q_p, int32_t q_dtype,
+                             const int32_t* src_slots, int32_t src_base,
+                             const int32_t* dst_slots, int32_t dst_base,
+                             int32_t nevals, void* stream) {
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  if (p < 0 || q < 0 || p >= h->nspcs || q >= h->nspcs)
+    return fail(DGFS_ERR_INVALID, "species index out of range");
+  if (nevals < 0 || src_base < 0 || dst_base < 0)
+    return fail(DGFS_ERR_INVALID, "negative nevals or slot base");
+  if (nevals == 0) return DGFS_OK;
+  if (!f_p || !f_q || !Q_p) return fail(DGFS_ERR_INVALID, "null array");
+  if ((f_dtype != DGFS_F32 && f_dtype != DGFS_F64) ||
+      (q_dtype != DGFS_F32 && q_dtype != DGFS_F64))
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  for (int off = 0; off < nevals; off += h->max_evals) {
+    const int cnt = std::min(h->max_evals, nevals - off);
+    const int32_t* ss = src_slots ? src_slots + off : nullptr;
+    const int32_t* ds = dst_slots ? dst_slots + off : nullptr;
+    int rc;
+    switch (h->N) {
+      case 8: rc = vss_run<8>(h, p, q, f_p, f_q, f_dtype == DGFS_F64, Q_p, q_dtype == DGFS_F64, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 16: rc = vss_run<16>(h, p, q, f_p, f_q, f_dtype == DGFS_F64, Q_p, q_dtype == DGFS_F64, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 24: rc = vss_run<24>(h, p, q, f_p, f_q, f_dtype == DGFS_F64, Q_p, q_dtype == DGFS_F64, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      default: rc = vss_run<32>(h, p, q, f_p, f_q, f_dtype == DGFS_F64, Q_p, q_dtype == DGFS_F64, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+    }
+    if (rc) return rc;
+  }
   return DGFS_OK;
 }

@@ -1,0 +1,380 @@
+// Fused fast-spectral VSS collision operator of a binary mixture, one
+// species pair (p, q) per call.  Reference: DGFSBiVSSScatteringModel
+// (dgfs1D/bi/scattering.py:47-321) and dgfs1D/bi/kernels/scattering/vss.mako.
+//
+// Per point the reference computes, with F = FFT(f_p)/n, G = FFT(f_q)/n and
+// a_rm(l) = (pi/L) rho_r sigma_m . l:
+//   t1 = e^{+i a m_q/(m_p+m_q)} F,  t2 = e^{-i a m_p/(m_p+m_q)} G,
+//   Qhat = sum_{r,m} (w_r s_w / n) b_{pq,rm}(l) FFT(IFFT(t1) IFFT(t2)),
+//   Q_p += prefac_pq (Re IFFT(Qhat) - f_p Re IFFT(c_pq G)).
+// The weights b_{pq,rm} depend on both r and m, so every term needs its own
+// forward transform (3 transforms per term).  Here one thread-block cluster
+// evaluates one point completely: per term the two inverse transforms and
+// the forward transform exchange through distributed shared memory, the
+// spectral accumulator stays in shared memory, and the final inverse
+// transform, the loss and the output run in the same kernel.  FP64.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cluster_slab.cuh"
+#include "fft_reg.cuh"
+
+namespace dgfs {
+
+// F = FFT(f)/n for a batch of slots (one cluster per slot, FP64).
+struct Fft3Args {
+  const void* f;
+  int f_double;
+  const int32_t* slots;
+  int base;
+  double2* out;        // [nevals][n]
+};
+
+template <int N, int C>
+__global__ void __launch_bounds__(Geo<N, C>::NT, 1)
+fft3_forward_kernel(Fft3Args a) {
+  using G = Geo<N, C>;
+  using T = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);
+  const int t = threadIdx.x;
+  const unsigned rank = cluster_rank();
+  const int e = blockIdx.y;
+  const int yl = t / N, z = t % N, y = rank * G::P + yl;
+  const int slot = a.slots ? a.slots[e] : a.base + e;
+  const size_t fb = (size_t)slot * G::n;
+  T v[N];
+#pragma unroll
+  for (int x = 0; x < N; ++x) {
+    v[x].x = a.f_double ? static_cast<const double*>(a.f)[fb + ((size_t)x * N + y) * N + z]
+                        : (double)static_cast<const float*>(a.f)[fb + ((size_t)x * N + y) * N + z];
+    v[x].y = 0.0;
+  }
+  fft<double, N, -1>(v);
+  push_pencils_to_xslab<double, N, C>(A, t, rank, v);
+  cluster_sync_all();
+  {
+    T w[N];
+    slab_col_load_fft<double, N, C, -1>(A, t, w);
+    const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+    for (int k = 0; k < N; ++k) A[base + k * G::ROW] = w[k];
+  }
+  __syncthreads();
+  slab_row_pass<double, N, C, -1>(A, t);
+  __syncthreads();
+  const double inv_n = 1.0 / (double)G::n;
+  T* out = a.out + (size_t)e * G::n + (size_t)rank * G::P * N * N;
+  for (int j = t; j < G::P * N * N; j += G::NT) {
+    T w = A[slab_index<N, C>(j)];
+    w.x *= inv_n;
+    w.y *= inv_n;
+    out[j] = w;
+  }
+  cluster_sync_all();  // no CTA leaves while peers may still write into it
+}
+
+// Weights of one pair (vss.mako:51-93, launch loop bi/scattering.py:185-204):
+//   b_rm(l) = sum_k B_mk fac_b(r) e^{-i mpq s_r sigma'_k . l}
+//   c(l)   += sum_r sum_m sum_k B_mk fac_c(r) e^{-i s_r sigma'_k . l}
+// with B_mk = (1 + sigma_m . sigma'_k)^eta, s_r = (pi/L) rho_r.  The phases
+// are products of per-axis factors; k is processed in chunks so that the
+// factor tables of a chunk fit in shared memory.
+struct VssSetupArgs {
+  const double* Bmk;         // [M][Mpre]
+  const double* spre;        // [Mpre][3]
+  const double* srho;        // [Nrho] s_r = (pi/L) rho_r
+  const double* fac_b;       // [Nrho]
+  const double* fac_c;       // [Nrho]
+  double mpq;
+  int M, Mpre, Nrho;
+  double2* b;                // out [Nrho][M][n]
+  double2* cpart;            // out [Nrho][n]: the r-th term of c
+};
+
+constexpr int kVssKChunk = 16;
+
+template <int N>
+__host__ __device__ constexpr int vss_setup_threads() { return N * N < 1024 ? N * N : 1024; }
+
+template <int N>
+__global__ void __launch_bounds__(vss_setup_threads<N>())
+vss_setup_kernel(VssSetupArgs a) {
+  constexpr int n = N * N * N;
+  constexpr int NTH = vss_setup_threads<N>();
+  const int lx = blockIdx.x, r = blockIdx.y;
+  const int t = threadIdx.x;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // per chunk: x factor [K] (b, c), y/z factors [K][N] (b, c), B [M][K]
+  double2* xb = reinterpret_cast<double2*>(smem_raw);
+  double2* xc = xb + kVssKChunk;
+  double2* yb = xc + kVssKChunk;
+  double2* yc = yb + kVssKChunk * N;
+  double2* zb = yc + kVssKChunk * N;
+  double2* zc = zb + kVssKChunk * N;
+  double* Bs = reinterpret_cast<double*>(zc + kVssKChunk * N);
+  auto rep = [](int i) { return (double)((i < N / 2) ? i : i - N); };
+  constexpr int PTS = (N * N + NTH - 1) / NTH;
+  double2 accb[PTS][16];  // M <= 16
+  double2 accc[PTS];
+#pragma unroll
+  for (int k = 0; k < PTS; ++k) {
+    accc[k] = make_double2(0, 0);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) accb[k][m] = make_double2(0, 0);
+  }
+  const double s = a.srho[r];
+  for (int k0 = 0; k0 < a.Mpre; k0 += kVssKChunk) {
+    const int kc = min(kVssKChunk, a.Mpre - k0);
+    __syncthreads();
+    for (int i = t; i < kc * (2 * N + 1); i += blockDim.x) {
+      const int k = i / (2 * N + 1), j = i % (2 * N + 1);
+      const double* sp = a.spre + 3 * (k0 + k);
+      double sn, cs;
+      if (j == 0) {
+        const double ph = s * sp[0] * rep(lx);
+        sincos(a.mpq * ph, &sn, &cs); xb[k] = make_double2(cs, -sn);
+        sincos(ph, &sn, &cs); xc[k] = make_double2(cs, -sn);
+      } else if (j <= N) {
+        const int l = j - 1;
+        const double ph = s * sp[1] * rep(l);
+        sincos(a.mpq * ph, &sn, &cs); yb[k * N + l] = make_double2(cs, -sn);
+        sincos(ph, &sn, &cs); yc[k * N + l] = make_double2(cs, -sn);
+      } else {
+        const int l = j - 1 - N;
+        const double ph = s * sp[2] * rep(l);
+        sincos(a.mpq * ph, &sn, &cs); zb[k * N + l] = make_double2(cs, -sn);
+        sincos(ph, &sn, &cs); zc[k * N + l] = make_double2(cs, -sn);
+      }
+    }
+    for (int i = t; i < a.M * kc; i += blockDim.x)
+      Bs[i] = a.Bmk[(i / kc) * a.Mpre + k0 + i % kc];
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PTS; ++p) {
+      const int pt = min(t + p * NTH, N * N - 1);
+      const int ly = pt / N, lz = pt % N;
+      for (int k = 0; k < kc; ++k) {
+        const double2 eb = cmul(cmul(xb[k], yb[k * N + ly]), zb[k * N + lz]);
+        const double2 ec = cmul(cmul(xc[k], yc[k * N + ly]), zc[k * N + lz]);
+        double bsum = 0;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+          if (m < a.M) {
+            const double B = Bs[m * kc + k];
+            accb[p][m].x += B * eb.x;
+            accb[p][m].y += B * eb.y;
+            bsum += B;
+          }
+        }
+        accc[p].x += bsum * ec.x;
+        accc[p].y += bsum * ec.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < PTS; ++p) {
+    const int pt = t + p * NTH;
+    if (pt < N * N) {
+      const size_t l = (size_t)lx * N * N + pt;
+#pragma unroll
+      for (int m = 0; m < 16; ++m)
+        if (m < a.M) {
+          double2 v = accb[p][m];
+          v.x *= a.fac_b[r];
+          v.y *= a.fac_b[r];
+          a.b[((size_t)r * a.M + m) * n + l] = v;
+        }
+      a.cpart[(size_t)r * n + l] =
+          make_double2(a.fac_c[r] * accc[p].x, a.fac_c[r] * accc[p].y);
+    }
+  }
+}
+
+// c(l) = sum_r cpart[r][l], in ascending r.
+__global__ void vss_sum_c_kernel(const double2* cpart, int Nrho, size_t n,
+                                 double2* c) {
+  const size_t l = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= n) return;
+  double2 s = make_double2(0, 0);
+  for (int r = 0; r < Nrho; ++r) {
+    s.x += cpart[(size_t)r * n + l].x;
+    s.y += cpart[(size_t)r * n + l].y;
+  }
+  c[l] = s;
+}
+
+struct VssPairArgs {
+  const double2* Fp;       // [nevals][n]  FFT(f_p)/n
+  const double2* Fq;       // [nevals][n]  FFT(f_q)/n
+  const double2* b;        // [Nrho][M][n]
+  const double2* c;        // [n]
+  const double2* ph;       // [Nrho][M][2][3][N]: e^{+i a mq'}, e^{-i a mp'} factors
+  const double* w;         // [Nrho] w_r s_w / n
+  const void* fp;          // f_p (for the loss product)
+  int f_double;
+  const int32_t* src_slots;
+  int src_base;
+  void* Q;                 // Q_p output (+=)
+  int q_double;
+  const int32_t* dst_slots;
+  int dst_base;
+  double prefac;
+  int Nrho, M;
+};
+
+template <int N, int C>
+__device__ __forceinline__ void vss_zpass_inverse(double2* A, const double2* Frow0,
+                                                  const double2* tb, int t,
+                                                  unsigned rank) {
+  using G = Geo<N, C>;
+  const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
+  const double2 bxy = cmul(tb[lx], tb[N + ly]);
+  const double2* row = Frow0 + ((size_t)lx * N + ly) * N;
+  double2 v[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = cmul(row[k], cmul(bxy, tb[2 * N + k]));
+  fft<double, N, +1>(v);
+  const int base = pl * G::PLANE + ly * G::ROW;
+#pragma unroll
+  for (int k = 0; k < N; ++k) A[base + k] = v[k];
+}
+
+template <int N, int C>
+__global__ void __launch_bounds__(Geo<N, C>::NT, 1)
+vss_pair_kernel(VssPairArgs a) {
+  using G = Geo<N, C>;
+  using T = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);   // X-slab work buffer
+  T* Rb = A + G::SLAB;                     // Y-slab receive buffer
+  T* U = Rb + G::SLAB;                     // Y-slab: u pencils / loss
+  T* Qh = U + G::SLAB;                     // X-slab spectral accumulator
+  T* tab = Qh + G::SLAB;                   // [2][3][N] phase factors
+  const int t = threadIdx.x;
+  const unsigned rank = cluster_rank();
+  const int e = blockIdx.y;
+  const int yl = t / N, zz = t % N;
+  const int ybase = yl * G::PLANE + zz;    // thread's pencil in a Y-slab
+  const T* Fp = a.Fp + (size_t)e * G::n;
+  const T* Fq = a.Fq + (size_t)e * G::n;
+  bool pending = false;  // an arrive is outstanding (receive buffer in use)
+
+  // exchange this thread's y-pass column into the owners' receive buffers
+  auto exchange_cols = [&](const T* v) {
+    if (pending) cluster_wait();
+    push_cols_to_yslab<double, N, C>(Rb, t, rank, v);
+    cluster_arrive();
+    cluster_wait();
+  };
+  auto release_receive = [&]() {
+    cluster_arrive();
+    pending = true;
+  };
+  // inverse 3-D FFT of F * tables; result pencil (x) left in v
+  auto inverse = [&](const T* F, const T* tb, T* v) {
+    vss_zpass_inverse<N, C>(A, F, tb, t, rank);
+    __syncthreads();
+    slab_col_load_fft<double, N, C, +1>(A, t, v);
+    exchange_cols(v);
+    yslab_load_pencil<double, N, C>(Rb, t, v);
+    release_receive();
+    fft<double, N, +1>(v);
+  };
+
+  for (int j = t; j < G::SLAB; j += G::NT) Qh[j] = T{0, 0};
+  const int T_terms = a.Nrho * a.M;
+#pragma unroll 1
+  for (int term = 0; term < T_terms; ++term) {
+    const int r = term / a.M;
+    __syncthreads();
+    for (int i = t; i < 6 * N; i += G::NT) tab[i] = a.ph[(size_t)term * 6 * N + i];
+    __syncthreads();
+    T v[N];
+    inverse(Fp, tab, v);                       // u = IFFT(e^{+i a mq'} F)
+#pragma unroll
+    for (int x = 0; x < N; ++x) U[ybase + x * G::ROW] = v[x];
+    inverse(Fq, tab + 3 * N, v);               // v = IFFT(e^{-i a mp'} G)
+#pragma unroll
+    for (int x = 0; x < N; ++x) v[x] = cmul(U[ybase + x * G::ROW], v[x]);
+    fft<double, N, -1>(v);                     // forward: x pass
+    if (pending) cluster_wait();
+    push_pencils_to_xslab<double, N, C>(A, t, rank, v);
+    cluster_arrive();
+    cluster_wait();
+    pending = false;
+    {
+      T w[N];
+      slab_col_load_fft<double, N, C, -1>(A, t, w);
+      const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+      for (int k = 0; k < N; ++k) A[base + k * G::ROW] = w[k];
+    }
+    __syncthreads();
+    {
+      // z pass (rows) and accumulation W_r b_rm (*) FFT(h) into Qhat
+      const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
+      const int base = pl * G::PLANE + ly * G::ROW;
+      T w[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) w[k] = A[base + k];
+      fft<double, N, -1>(w);
+      const T* brow = a.b + (size_t)term * G::n + ((size_t)lx * N + ly) * N;
+      const double wr = a.w[r];
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        const T bb = brow[k];
+        const T pr = cmul(w[k], bb);
+        Qh[base + k].x += wr * pr.x;
+        Qh[base + k].y += wr * pr.y;
+      }
+    }
+  }
+
+  // loss: Re IFFT(c (*) G) -> U (real parts), then the gain IFFT(Qhat)
+  {
+    __syncthreads();
+    const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
+    const T* row = Fq + ((size_t)lx * N + ly) * N;
+    const T* crow = a.c + ((size_t)lx * N + ly) * N;
+    T w[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) w[k] = cmul(crow[k], row[k]);
+    fft<double, N, +1>(w);
+    const int base = pl * G::PLANE + ly * G::ROW;
+#pragma unroll
+    for (int k = 0; k < N; ++k) A[base + k] = w[k];
+  }
+  __syncthreads();
+  T v[N];
+  slab_col_load_fft<double, N, C, +1>(A, t, v);
+  exchange_cols(v);
+  yslab_load_pencil<double, N, C>(Rb, t, v);
+  release_receive();
+  fft<double, N, +1>(v);
+#pragma unroll
+  for (int x = 0; x < N; ++x) U[ybase + x * G::ROW] = v[x];
+  slab_row_pass<double, N, C, +1>(Qh, t);
+  __syncthreads();
+  slab_col_load_fft<double, N, C, +1>(Qh, t, v);
+  exchange_cols(v);
+  yslab_load_pencil<double, N, C>(Rb, t, v);
+  release_receive();
+  fft<double, N, +1>(v);
+  const int y = rank * G::P + yl;
+  const size_t fb = (size_t)(a.src_slots ? a.src_slots[e] : a.src_base + e) * G::n;
+  const size_t qb = (size_t)(a.dst_slots ? a.dst_slots[e] : a.dst_base + e) * G::n;
+#pragma unroll
+  for (int x = 0; x < N; ++x) {
+    const size_t idx = ((size_t)x * N + y) * N + zz;
+    const double fv = a.f_double ? static_cast<const double*>(a.fp)[fb + idx]
+                                 : (double)static_cast<const float*>(a.fp)[fb + idx];
+    const double qv = a.prefac * (v[x].x - fv * U[ybase + x * G::ROW].x);
+    if (a.q_double) static_cast<double*>(a.Q)[qb + idx] += qv;
+    else static_cast<float*>(a.Q)[qb + idx] += (float)qv;
+  }
+  if (pending) cluster_wait();
+}
+
+}  // namespace dgfs

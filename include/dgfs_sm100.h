@@ -109,6 +109,48 @@ int dgfs_vhs_stage_ms(dgfs_vhs_handle h, double* out5);
 int dgfs_fma_peak(double* tflops, void* stream);
 
 /*
+ * Binary-mixture VSS model, `vss` in the reference (dgfs1D/bi/scattering.py:
+ * 47-321, dgfs1D/bi/kernels/scattering/vss.mako).  Mirrors what
+ * DGFSBiVSSScatteringModel.load_parameters/perform_precomputation read: the
+ * full-sphere rule sz (M <= 16 points, weight sw = 4 pi / M), the
+ * pre-integration rule szpre (Mpre points), nondimensional masses, and per
+ * ordered pair pq = p*nspcs + q: gamma = 2(1-omega), eta = alpha - 1 and the
+ * prefactor (bi/scattering.py:66-89).  The weights b_pq and c_pq
+ * (precompute_bc_pq, vss.mako:51-93) are built on the GPU at create.  FP64.
+ */
+typedef struct dgfs_vss_s* dgfs_vss_handle;
+typedef struct {
+  int32_t N;
+  int32_t Nrho;
+  int32_t M;
+  int32_t Mpre;
+  int32_t nspcs;           /* 1..4 */
+  double L;
+  const double* qz;        /* [Nrho] host */
+  const double* qw;        /* [Nrho] host */
+  const double* sz;        /* [M*3] host */
+  double sw;
+  const double* szpre;     /* [Mpre*3] host */
+  const double* masses;    /* [nspcs] host, nondimensional */
+  const double* gamma;     /* [nspcs*nspcs] host */
+  const double* eta;       /* [nspcs*nspcs] host */
+  const double* prefac;    /* [nspcs*nspcs] host */
+  int32_t max_evals;
+} dgfs_vss_desc;
+
+int dgfs_vss_create(const dgfs_vss_desc* desc, dgfs_vss_handle* out);
+int dgfs_vss_destroy(dgfs_vss_handle h);
+
+/* Q_p[dst(i)] += Q_pq(f_p[src(i)], f_q[src(i)]) for i < nevals: the batched
+ * form of DGFSBiVSSScatteringModel.fs('pq', d_f1, d_f2, d_Q, elem, upt,
+ * uptout) (bi/scattering.py:263-321). */
+int dgfs_vss_eval(dgfs_vss_handle h, int32_t p, int32_t q, const void* f_p,
+                  const void* f_q, int32_t f_dtype, void* Q_p, int32_t q_dtype,
+                  const int32_t* src_slots, int32_t src_base,
+                  const int32_t* dst_slots, int32_t dst_base, int32_t nevals,
+                  void* stream);
+
+/*
  * Nodal DG advection right-hand side of the single-species solver.
  * Replaces the kernels of the rhs() closure in dgfs1D/std/std.py:281-345:
  * bwdTransFace + extract_left/right + transfer/insert BC (std.mako:4-89),

@@ -113,3 +113,19 @@ def test_matches_reference_kernel_golden(lib, precision):
     got = Q.cpu().numpy().reshape(-1, N ** 3)
     for s in range(ref.shape[0]):
         assert _rel(got[s], ref[s]) < tol, s
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_n24(lib, precision):
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    vm, prefac, gamma, f = vhs_case(24, 6, 12, 5., False, nslots=2)
+    tab = vhs_tables(vm, gamma)
+    op = VHSOperator(**op_kwargs(vm, prefac, gamma), precision=precision,
+                     max_evals=2)
+    fd = torch.tensor(f, device='cuda')
+    Q = torch.zeros_like(fd)
+    op.eval(fd, Q)
+    torch.cuda.synchronize()
+    tol = FP64_TOL if precision == 'fp64' else FP32_TOL
+    for s in range(2):
+        assert _rel(Q.cpu().numpy()[s], vhs_gll_fs(tab, prefac, f[s])) < tol
