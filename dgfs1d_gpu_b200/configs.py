@@ -83,3 +83,91 @@ ux = 0
 uy = {uwall * u0!r}
 uz = 0
 """
+
+
+def couette_bi_ini(Ne=3, K=3, Nv=8, Nrho=4, M=6, Mpre=12, dev=5.0,
+                   scheme='euler', dt=0.0005, nsteps=3, uwall=0.1,
+                   noise=0.02, seed=20261203, compat=0,
+                   masses=(39.96e-3, 83.77e-3)):
+    """Binary Couette (examples/bi/couette/dgfs1D.ini parameters, small)."""
+    T0, m0 = 273., masses[0]
+    u0 = math.sqrt(2 * R0 / m0 * T0)
+    rho0 = 0.00011140244750324529
+    n0 = rho0 / m0 * NA
+    return f"""
+[config]
+precision = double
+[mesh]
+xlo = 0.
+xhi = 1e-3
+Ne = {Ne}
+H0 = 1e-3
+[basis]
+kind = nodal-sem-gll
+K = {K}
+Nqr = {K}
+[non-dim]
+T0 = {T0}
+rho0 = {rho0!r}
+molarMass0 = {m0}
+[velocity-mesh]
+nspcs = 2
+Nv = {Nv}
+Nrho = {Nrho}
+dev = {dev}
+cmax = 0
+Tmax = {T0}
+molarMass1 = {masses[0]}
+molarMass2 = {masses[1]}
+[spherical-design-rule]
+ssrule = womersley
+M = {M}
+[scattering-model]
+type = vss
+ssrulepre = womersley
+Mpre = {Mpre}
+alpha00 = 1.4
+omega00 = 0.81
+dRef00 = 4.11e-10
+Tref00 = 273
+alpha01 = 1.36
+omega01 = 0.805
+dRef01 = 4.405e-10
+Tref01 = 273
+alpha10 = 1.36
+omega10 = 0.805
+dRef10 = 4.405e-10
+Tref10 = 273
+alpha11 = 1.32
+omega11 = 0.80
+dRef11 = 4.7e-10
+Tref11 = 273
+[time-integrator]
+scheme = {scheme}
+tstart = 0.0
+tend = {dt * nsteps!r}
+dt = {dt!r}
+bi-ssp-rk3-compat = {compat}
+[soln-ics]
+type = maxwellian-noise
+nden1 = {0.5 * n0!r}
+nden2 = {0.5 * n0!r}
+T = {T0}
+ux = 0
+uy = 0
+uz = 0
+noise = {noise}
+seed = {seed}
+[soln-bcs-xlo]
+type = dgfs-wall-diffuse
+T = {T0}
+ux = 0
+uy = {-uwall * u0!r}
+uz = 0
+[soln-bcs-xhi]
+type = dgfs-wall-diffuse
+T = {T0}
+ux = 0
+uy = {uwall * u0!r}
+uz = 0
+"""

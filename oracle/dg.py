@@ -263,3 +263,80 @@ def moments(basis, coeff, cv, cw, T0=1.0, rho0=1.0, u0=1.0, R0=8.3144598,
                                 0.5 * rho0 * u0 ** 2, 0.5 * rho0 * u0 ** 2])
     out[:, :, 9] = (R0 / molarMass0) * out[:, :, 0] * out[:, :, 3]
     return out
+
+
+# -- binary mixture (dgfs1D/bi/bi.py:265-349, bi/integrator.py) -------------
+
+def collide_bi(basis, p, nspcs, fs_pq):
+    """Collision loop of bi.py:336-342: sum_q Q_pq(U^T u_p, V u_q)."""
+    def collide(us):
+        def add(u_in, ux):
+            K, Ne, Nv = u_in.shape
+            for m in range(K):
+                d_f = np.einsum('ar,aev->rev', basis.U[m], us[p])
+                for q in range(nspcs):
+                    d_g = np.einsum('rb,bev->rev', basis.V[m], us[q])
+                    for r in basis.sigModes[m]:
+                        for e in range(Ne):
+                            ux[m, e] += fs_pq(p, q, d_f[r, e], d_g[r, e])
+        return add
+    return collide
+
+
+def bi_integrate(kind, rhs, t, dt, us, compat=False):
+    """One step of the mixture integrators; rhs(p, t, us) -> array."""
+    ns = len(us)
+    if kind == 'euler':
+        r0 = [rhs(p, t, us) for p in range(ns)]
+        for p in range(ns):
+            axnpby(r0[p], dt, 1.0, us[p])
+        for p in range(ns):
+            us[p][...] = r0[p]
+    elif kind == 'ssp-rk2':
+        r0 = []
+        for p in range(ns):
+            r = rhs(p, t, us)
+            axnpby(r, dt, 1.0, us[p])
+            r0.append(r)
+        for p in range(ns):
+            r1 = rhs(p, t + dt, r0)
+            axnpby(us[p], 0.5, 0.5, r0[p], 0.5 * dt, r1)
+    elif kind == 'ssp-rk3':
+        r0 = [np.empty_like(u) for u in us]
+        for p in range(ns):
+            r1 = rhs(p, t, us)
+            axnpby(r0[p], 0.0, 1.0, us[p], dt, r1)
+        r1s = []
+        for p in range(ns):
+            r1 = rhs(p, t + dt, r0)
+            axnpby(r1, 0.25 * dt, 0.75, us[p], dt if compat else 0.25, r0[p])
+            r1s.append(r1)
+        for p in range(ns):
+            r = rhs(p, t + 0.5 * dt, r1s)
+            axnpby(us[p], 1.0 / 3.0, 2.0 / 3.0, r1s[p], 2.0 / 3.0 * dt, r)
+    elif kind == 'lse-rk45':
+        a = [0.0, -567301805773.0 / 1357537059087.0,
+             -2404267990393.0 / 2016746695238.0,
+             -3550918686646.0 / 2091501179385.0,
+             -1275806237668.0 / 842570457699.0]
+        b = [1432997174477.0 / 9575080441755.0,
+             5161836677717.0 / 13612068292357.0,
+             1720146321549.0 / 2090206949498.0,
+             3134564353537.0 / 4481467310338.0,
+             2277821191437.0 / 14882151754819.0]
+        c = [0.0, 1432997174477.0 / 9575080441755.0,
+             2526269341429.0 / 6820363962896.0,
+             2006345519317.0 / 3224310063776.0,
+             2802321613138.0 / 2924317926251.0]
+        r1 = [np.zeros_like(u) for u in us]
+        for s in range(5):
+            r0 = []
+            for p in range(ns):
+                r = rhs(p, t + c[s] * dt, us)
+                axnpby(r1[p], a[s], dt, r)
+                axnpby(r, 0., 1., us[p], b[s], r1[p])
+                r0.append(r)
+            for p in range(ns):
+                us[p][...] = r0[p]
+    else:
+        raise ValueError(kind)
