@@ -82,6 +82,7 @@ _SIGNATURES = [
       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
       ctypes.c_void_p]),
     ('dgfs_vhs_last_moments', ctypes.c_void_p, [ctypes.c_void_p]),
+    ('dgfs_vhs_set_projection', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_vhs_destroy', ctypes.c_int, [ctypes.c_void_p]),
     ('dgfs_vhs_profile', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_vhs_stage_ms', ctypes.c_int,
@@ -110,6 +111,18 @@ _SIGNATURES = [
     ('dgfs_dg_residual', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
       ctypes.c_int32, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    ('dgfs_penalty_moments', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_void_p, ctypes.c_void_p]),
+    ('dgfs_penalty_implicit', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+      ctypes.c_void_p]),
+    ('dgfs_penalty_collide', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+      ctypes.c_double, ctypes.c_void_p]),
     ('dgfs_axnpby', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_double,
       ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),

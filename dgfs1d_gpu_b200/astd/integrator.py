@@ -1,0 +1,174 @@
+"""Penalised IMEX time integrators (``[time-integrator] scheme``).
+
+Keys and coefficients of dgfs1D/astd/integrator.py: ``bdf-111`` / ``bdf-222``
+(BGK penalty, explicit DG advection; :281-400) and ``imex-lm-bdf1`` /
+``imex-lm-bdf2`` (explicit L + Q - P, implicit P(f^{n+1}); :623-792).
+Differences from the reference, all in start-up or dead code: start-up
+states come from first-order substeps of the same family (the reference
+uses ARS-222/443 substeps); the explicit part of a new IMEX-LM level uses
+that level's penalty P(f^{n+1}) (the reference's two-stage path would use
+the previous level's after its circular shift, but exits the process after
+its first step, astd/integrator.py:732, so it never gets there).
+"""
+import torch
+
+from ..dg import axnpby
+
+
+def _lin(out, pairs):
+    """out = sum a_i x_i over (a, x) pairs, in chunks of the native axnpby."""
+    pairs = [(a, x) for a, x in pairs if a != 0.0]
+    if not pairs:
+        out.zero_()
+        return
+    first = True
+    while pairs:
+        chunk, pairs = pairs[:4 if first else 3], pairs[4 if first else 3:]
+        terms = []
+        for a, x in chunk:
+            terms += [a, x]
+        axnpby(out, 0.0 if first else 1.0, *terms)
+        first = False
+
+
+class DGFSIntegratorAstd:
+    intg_kind = None
+
+    def __init__(self, explicit, sm, shape, dtype, t=0.0, dt=None, f0=None,
+                 explicitQ=None, nsub=10, device='cuda', **kwargs):
+        self._explicit, self._sm, self._Q = explicit, sm, explicitQ
+        self.shape, self.dtype, self.device = shape, dtype, device
+        self.npts = shape[0] * shape[1]
+        self.dt, self.nsub = dt, nsub
+
+    def _z(self):
+        return torch.zeros(self.shape, dtype=self.dtype, device=self.device)
+
+    def _zm(self):
+        return torch.zeros((self.npts, 5), dtype=torch.float64,
+                           device=self.device)
+
+    def _mom(self, x):
+        U = self._zm()
+        self._sm.moment(0.0, x, U)
+        return U
+
+
+class Bdf111IntegratorAstd(DGFSIntegratorAstd):
+    intg_kind = 'bdf-111'
+
+    def integrate(self, t, dt, nacptsteps, f):
+        U0 = self._mom(f)
+        L0 = self._z()
+        self._explicit(t, f, L0)
+        LU0 = self._mom(L0)
+        U = self._zm()
+        _lin(U, [(1.0, U0), (dt, LU0)])
+        rhs = self._z()
+        _lin(rhs, [(1.0, f), (dt, L0)])
+        self._sm.implicit(U, rhs, f, 1.0, dt)
+
+
+class Bdf222IntegratorAstd(DGFSIntegratorAstd):
+    intg_kind = 'bdf-222'
+    A = [1. / 3., -4. / 3., 1.]
+    G = [-2. / 3., 4. / 3.]
+    B = 2. / 3.
+
+    def _state(self, t, f):
+        L = self._z()
+        self._explicit(t, f, L)
+        return dict(F=f.clone(), U=self._mom(f), L=L, LU=self._mom(L))
+
+    def integrate(self, t, dt, nacptsteps, f):
+        a1, a2, a3 = self.A
+        g1, g2 = self.G
+        if nacptsteps == 0:
+            f0 = f.clone()
+            sub = Bdf111IntegratorAstd(self._explicit, self._sm, self.shape,
+                                       self.dtype, device=self.device)
+            for i in range(self.nsub):
+                sub.integrate(t + i * dt / self.nsub, dt / self.nsub, i, f)
+            self.hist = [self._state(t, f0), self._state(t + dt, f)]
+            return
+        h0, h1 = self.hist
+        U = self._zm()
+        _lin(U, [(-a1 / a3, h0['U']), (g1 * dt / a3, h0['LU']),
+                 (-a2 / a3, h1['U']), (g2 * dt / a3, h1['LU'])])
+        rhs = self._z()
+        _lin(rhs, [(-a1, h0['F']), (g1 * dt, h0['L']), (-a2, h1['F']),
+                   (g2 * dt, h1['L'])])
+        self._sm.implicit(U, rhs, f, a3, self.B * dt)
+        self.hist = [h1, self._state(t + dt, f)]
+
+
+class IMEXLMIntegratorAstd(DGFSIntegratorAstd):
+    intg_kind = None
+    A = B = C = None
+
+    def __init__(self, explicit, sm, shape, dtype, t=0.0, dt=None, f0=None,
+                 explicitQ=None, **kwargs):
+        super().__init__(explicit, sm, shape, dtype, t=t, dt=dt, f0=f0,
+                         explicitQ=explicitQ, **kwargs)
+        s = len(self.A)
+        self.hist = []
+        if s > 1:
+            f = f0.clone()
+            sub = IMEXLMBdf1IntegratorAstd(explicit, sm, shape, dtype, t=t,
+                                           dt=dt / self.nsub, f0=f,
+                                           explicitQ=explicitQ,
+                                           device=self.device)
+            for i in range(self.nsub):
+                sub.integrate(t + i * dt / self.nsub, dt / self.nsub, i, f)
+            self.start = f
+            self.hist = [self._state(t, f0), self._state(t + dt, f)]
+        else:
+            self.hist = [self._state(t, f0)]
+
+    def _state(self, t, f):
+        U = self._mom(f)
+        P = self._z()
+        self._sm.collide(t, U, f, P)
+        E = self._z()
+        self._explicit(t, f, E)
+        if self._Q is not None:
+            self._Q(t, f, E)          # accumulates Q(f)
+        axnpby(E, 1.0, -1.0, P)
+        return dict(F=f.clone(), U=U, P=P, LM=self._mom(P), L=E,
+                    LU=self._mom(E))
+
+    def integrate(self, t, dt, nacptsteps, f):
+        A, B, C = self.A, self.B, self.C
+        s = len(A)
+        if nacptsteps < s - 1:
+            f.copy_(self.start)
+            return
+        hs = self.hist
+        U = self._zm()
+        _lin(U, [p for i in range(s) for p in (
+            (-A[s - i - 1], hs[i]['U']), (dt * B[s - i - 1], hs[i]['LU']),
+            (dt * C[s - i], hs[i]['LM']))])
+        rhs = self._z()
+        _lin(rhs, [p for i in range(s) for p in (
+            (-A[s - i - 1], hs[i]['F']), (dt * B[s - i - 1], hs[i]['L']),
+            (dt * C[s - i], hs[i]['P']))])
+        P = self._z()
+        self._sm.implicit(U, rhs, f, 1.0, C[0] * dt, P=P)
+        E = self._z()
+        self._explicit(t + dt, f, E)
+        if self._Q is not None:
+            self._Q(t + dt, f, E)
+        axnpby(E, 1.0, -1.0, P)
+        new = dict(F=f.clone(), U=U, P=P, LM=self._mom(P), L=E,
+                   LU=self._mom(E))
+        self.hist = hs[1:] + [new]
+
+
+class IMEXLMBdf1IntegratorAstd(IMEXLMIntegratorAstd):
+    intg_kind = 'imex-lm-bdf1'
+    A, B, C = [-1.], [1.], [1., 0.]
+
+
+class IMEXLMBdf2IntegratorAstd(IMEXLMIntegratorAstd):
+    intg_kind = 'imex-lm-bdf2'
+    A, B, C = [-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]

@@ -1,0 +1,99 @@
+"""Penalised IMEX DGFS driver (``dgfsABstd1D``) on the native kernels.
+
+Mirrors dgfs1D/astd/abstd.py:38-499: the Boltzmann model (``[scattering-
+model]``, explicit), the penalty model (``[penalized-scattering-model]``,
+implicit, FP64) and the IMEX integrator built as
+``odescls(explicit, psm, shape, dtype, t=, dt=, f0=, explicitQ=)``.  The
+state is kept in FP64; the Boltzmann operator may run in its FP32 mode.
+"""
+import math
+
+import numpy as np
+import torch
+
+from ..basis import get_basis
+from ..dg import DGOperator
+from ..mesh import Mesh
+from ..plugins import subclass_where
+from ..std.bc import get_bc
+from ..std.initcond import get_initcond
+from ..std.moments import DGFSMomWriterStd
+from ..std.scattering import DGFSScatteringModelStd
+from ..velocitymesh import DGFSVelocityMeshStd
+from .integrator import DGFSIntegratorAstd
+from .scattering import DGFSScatteringModelAstd
+
+
+class DGFSABstd1D:
+    def __init__(self, cfg, device='cuda', boltzmann=None):
+        self.cfg = cfg
+        self.device = torch.device(device)
+        self.dtype = torch.float64
+        self.mesh = mesh = Mesh(cfg)
+        Ne = mesh.Ne
+        self.basis = basis = get_basis(cfg)
+        K = basis.K
+        self.vm = vm = DGFSVelocityMeshStd(cfg)
+        Nv = vm.vsize()
+        smcls = subclass_where(DGFSScatteringModelStd, scattering_model=cfg.lookup(
+            'scattering-model', 'type'))
+        self.sm = smcls(cfg, vm, Ne=Ne, max_evals=K * Ne)
+        pcls = subclass_where(DGFSScatteringModelAstd, scattering_model=cfg.lookup(
+            'penalized-scattering-model', 'type'))
+        self.psm = pcls(cfg, vm, Ne=Ne, eps=self.sm.prefac)
+        ti, dt, tf = cfg.lookupfloats('time-integrator', ('tstart', 'dt', 'tend'))
+        self.nsteps = int(math.ceil((tf - ti) / dt))
+        self.dt = (tf - ti) / self.nsteps
+        x = mesh.xmesh
+        self.xsol = np.array([0.5 * (x[j] + x[j + 1]) + mesh.jac[j] * basis.z
+                              for j in range(Ne)]).T
+        bcl = get_bc(cfg, 'soln-bcs-xlo', x[0], -1., vm)
+        bcr = get_bc(cfg, 'soln-bcs-xhi', x[-1], 1., vm)
+        self.dg = DGOperator(basis, mesh.invjac, vm.c0(), vm.cw(),
+                             [(bcl.type, bcl.f0, bcl.ux),
+                              (bcr.type, bcr.f0, bcr.ux)])
+        self.psm.bind(self.dg)
+        src, dst = [], []
+        for m, a in basis.mode_sources():
+            for e in range(Ne):
+                src.append(a * Ne + e)
+                dst.append(m * Ne + e)
+        self.src = torch.tensor(src, dtype=torch.int32, device=self.device)
+        self.dst = torch.tensor(dst, dtype=torch.int32, device=self.device)
+        usol = np.empty((basis.Nq, Ne, Nv))
+        get_initcond(cfg, vm, 'soln-ics').apply_init_vals(usol, basis.Nq, Ne,
+                                                          self.xsol)
+        self.u = torch.tensor(usol, dtype=self.dtype, device=self.device)
+        self.t = ti
+        self.nacptsteps = 0
+        # the Boltzmann operator may be replaced (e.g. by a surrogate)
+        self.boltzmann = boltzmann
+        icls = subclass_where(DGFSIntegratorAstd,
+                              intg_kind=cfg.lookup('time-integrator', 'scheme'))
+        self.odes = icls(self.explicit, self.psm, (K, Ne, Nv), self.dtype,
+                         t=ti, dt=self.dt, f0=self.u, explicitQ=self.explicitQ,
+                         device=self.device)
+        self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, self.xsol)
+
+    def explicit(self, t, u_in, u_out):
+        self.dg.advect(u_in, u_out)
+
+    def explicitQ(self, t, u_in, u_out):
+        """Accumulate Q(u_in) into u_out (abstd.py:383-395)."""
+        if self.boltzmann is not None:
+            self.boltzmann(t, u_in, u_out)
+        else:
+            self.sm.fs_batch(u_in, u_out, self.src, self.dst)
+
+    def step(self):
+        self.odes.integrate(self.t, self.dt, self.nacptsteps, self.u)
+        self.t += self.dt
+        self.nacptsteps += 1
+
+    def run(self, nsteps=None):
+        for _ in range(self.nsteps if nsteps is None else nsteps):
+            self.step()
+        return self.u
+
+    def bulk_moments(self):
+        return self.moments.compute(self.u)

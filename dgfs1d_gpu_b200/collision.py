@@ -91,6 +91,10 @@ class VHSOperator:
             ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
             int(nevals), _stream_ptr(stream)))
 
+    def set_projection(self, enable=True):
+        """Toggle the FP64 conservation projection of every evaluation."""
+        nat.check(nat.lib().dgfs_vhs_set_projection(self._h, int(bool(enable))))
+
     def close(self):
         if getattr(self, '_h', None):
             nat.lib().dgfs_vhs_destroy(self._h)

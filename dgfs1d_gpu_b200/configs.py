@@ -171,3 +171,17 @@ ux = 0
 uy = {uwall * u0!r}
 uz = 0
 """
+
+
+def couette_astd_ini(scheme='imex-lm-bdf2', penalty='boltz-bgk-direct-gll',
+                     dt=0.002, nsteps=3, **kw):
+    """The Couette set-up of couette_std_ini with a penalty model and an IMEX
+    scheme (dgfsABstd1D keys)."""
+    ini = couette_std_ini(scheme=scheme, dt=dt, nsteps=nsteps, **kw)
+    return ini + """
+[penalized-scattering-model]
+type = {0}
+omega = 0.81
+muRef = 2.117e-5
+Tref = 273
+""".format(penalty)

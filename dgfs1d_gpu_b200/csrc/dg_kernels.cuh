@@ -294,3 +294,107 @@ __global__ void __launch_bounds__(512) residual_kernel(const void* x,
 }
 
 }  // namespace dgfs
+
+namespace dgfs {
+
+// ---------------------------------------------------------------------------
+// Penalty (BGK-type) model of the penalised IMEX schemes (FP64).
+// Reference: dgfs1D/astd/scattering.py:44-284 with the kernels of
+// dgfs1D/astd/kernels/scattering/bgk-direct-gll.mako (moments by a cuBLAS
+// gemm there, cmaxwellian, collide, updateDistribution{q}_BDF / _LM).
+// Moments per point: U = (rho, rho ux, rho uy, rho uz, E) with
+// E = sum f |c|^2 cw;  T = (E - |rho u|^2 / rho) / (1.5 rho);
+// nu = prefac rho T^(1-omega).
+// ---------------------------------------------------------------------------
+struct PenaltyMomentArgs {
+  const void* f;          // [npts][Nv]
+  int f_double;
+  int Nv, N;
+  const double* c0;
+  double cw;
+  double* U;              // [npts][5]
+};
+
+__global__ void __launch_bounds__(256) penalty_moments_kernel(PenaltyMomentArgs a) {
+  const int p = blockIdx.x, t = threadIdx.x;
+  __shared__ double red[5][256];
+  const int NN = a.N * a.N;
+  double s[5] = {0, 0, 0, 0, 0};
+  for (int v = t; v < a.Nv; v += blockDim.x) {
+    const double fv = ld(a.f, a.f_double, (size_t)p * a.Nv + v) * a.cw;
+    const double cx = a.c0[v / NN], cy = a.c0[(v / a.N) % a.N], cz = a.c0[v % a.N];
+    s[0] += fv;
+    s[1] += fv * cx;
+    s[2] += fv * cy;
+    s[3] += fv * cz;
+    s[4] += fv * (cx * cx + cy * cy + cz * cz);
+  }
+  for (int k = 0; k < 5; ++k) red[k][t] = s[k];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (t < st)
+      for (int k = 0; k < 5; ++k) red[k][t] += red[k][t + st];
+    __syncthreads();
+  }
+  if (t < 5) a.U[(size_t)p * 5 + t] = red[t][0];
+}
+
+struct PenaltyImplicitArgs {
+  const double* U;        // [npts][5] moments at the new level
+  const void* rhs;        // [npts][Nv] explicit combination
+  void* f;                // out [npts][Nv] new distribution
+  void* P;                // out (or null) nu (M - f)
+  void* Mout;             // out (or null) the Maxwellian
+  int f_double;
+  int Nv, N;
+  const double* c0;
+  double adiv;            // denominator constant (a_q for BDF, 1 for LM)
+  double cdt;             // implicit weight times dt (b dt, c0 dt)
+  double prefac, omega;
+  size_t total;           // npts * Nv
+};
+
+// f = (rhs + cdt nu M) / (adiv + cdt nu), optionally P = nu (M - f).
+__global__ void penalty_implicit_kernel(PenaltyImplicitArgs a) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t p = i / a.Nv;
+    const int v = (int)(i % a.Nv);
+    const double* U = a.U + p * 5;
+    const double T = (U[4] - (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]) /
+                     (1.5 * U[0]);
+    const int NN = a.N * a.N;
+    const double dx = a.c0[v / NN] - U[1] / U[0];
+    const double dy = a.c0[(v / a.N) % a.N] - U[2] / U[0];
+    const double dz = a.c0[v % a.N] - U[3] / U[0];
+    const double M = U[0] / pow(M_PI * T, 1.5) * exp(-(dx * dx + dy * dy + dz * dz) / T);
+    const double nu = a.prefac * U[0] * pow(T, 1. - a.omega);
+    const double r = ld(a.rhs, a.f_double, i);
+    const double fn = (r + a.cdt * nu * M) / (a.adiv + a.cdt * nu);
+    st(a.f, a.f_double, i, fn);
+    if (a.P) st(a.P, a.f_double, i, nu * (M - fn));
+    if (a.Mout) st(a.Mout, a.f_double, i, M);
+  }
+}
+
+// P = nu (M(U) - f) for the current f and its moments U (collide).
+__global__ void penalty_collide_kernel(PenaltyImplicitArgs a) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t p = i / a.Nv;
+    const int v = (int)(i % a.Nv);
+    const double* U = a.U + p * 5;
+    const double T = (U[4] - (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]) /
+                     (1.5 * U[0]);
+    const int NN = a.N * a.N;
+    const double dx = a.c0[v / NN] - U[1] / U[0];
+    const double dy = a.c0[(v / a.N) % a.N] - U[2] / U[0];
+    const double dz = a.c0[v % a.N] - U[3] / U[0];
+    const double M = U[0] / pow(M_PI * T, 1.5) * exp(-(dx * dx + dy * dy + dz * dz) / T);
+    const double nu = a.prefac * U[0] * pow(T, 1. - a.omega);
+    st(a.P, a.f_double, i, nu * (M - ld(a.f, a.f_double, i)));
+    if (a.Mout) st(a.Mout, a.f_double, i, M);
+  }
+}
+
+}  // namespace dgfs

@@ -118,6 +118,8 @@ struct dgfs_vhs_s {
   int max_evals = 0;
   double prefac = 0, cw = 0;
   int device = 0;
+  int project = 0;
+  double Ginv[25] = {};
   // constant tables
   double* c0 = nullptr;      // [N]
   double* b2 = nullptr;      // [n]
@@ -452,6 +454,8 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     a.src_slots = src_slots; a.src_base = src_base;
     a.Q = Q; a.q_double = q_double; a.dst_slots = dst_slots; a.dst_base = dst_base;
     a.prefac = h->prefac; a.Nrho = h->Nrho;
+    a.project = h->project; a.c0 = h->c0; a.cw = h->cw;
+    for (int i = 0; i < 25; ++i) a.Ginv[i] = h->Ginv[i];
     const size_t smem = 2 * slab_bytes(N, C64, sizeof(double2));
     if ((rc = launch_cluster(vhs_epilogue_kernel<N, C64>, dim3(C64, nevals),
                              dim3(G64::NT), C64, smem, st, a)))
@@ -1182,5 +1186,105 @@ extern "C" int dgfs_vss_eval(dgfs_vss_handle h, int32_t p, int32_t q,
     }
     if (rc) return rc;
   }
+  return DGFS_OK;
+}
+
+// Conservation projection of Q (no counterpart in the reference): after it,
+// sum_v Q phi_j cw = 0 for phi = (1, cx, cy, cz, |c|^2) to FP64 rounding.
+extern "C" int dgfs_vhs_set_projection(dgfs_vhs_handle h, int32_t enable) {
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  if (enable) {
+    // G_jk = sum_v phi_j phi_k cw, inverted by Gauss-Jordan in long double
+    const int N = h->N;
+    std::vector<double> c0(N);
+    DGFS_CUDA(cudaMemcpy(c0.data(), h->c0, N * sizeof(double),
+                         cudaMemcpyDeviceToHost));
+    long double G[5][10] = {};
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j)
+        for (int k = 0; k < N; ++k) {
+          const long double cx = c0[i], cy = c0[j], cz = c0[k];
+          const long double ph[5] = {1, cx, cy, cz, cx * cx + cy * cy + cz * cz};
+          for (int r = 0; r < 5; ++r)
+            for (int s = 0; s < 5; ++s) G[r][s] += ph[r] * ph[s] * h->cw;
+        }
+    for (int r = 0; r < 5; ++r) G[r][5 + r] = 1;
+    for (int col = 0; col < 5; ++col) {
+      int piv = col;
+      for (int r = col + 1; r < 5; ++r)
+        if (fabsl(G[r][col]) > fabsl(G[piv][col])) piv = r;
+      if (fabsl(G[piv][col]) < 1e-300L)
+        return fail(DGFS_ERR_INVALID, "singular moment Gram matrix");
+      for (int s = 0; s < 10; ++s) std::swap(G[col][s], G[piv][s]);
+      const long double d = G[col][col];
+      for (int s = 0; s < 10; ++s) G[col][s] /= d;
+      for (int r = 0; r < 5; ++r)
+        if (r != col) {
+          const long double f = G[r][col];
+          for (int s = 0; s < 10; ++s) G[r][s] -= f * G[col][s];
+        }
+    }
+    for (int r = 0; r < 5; ++r)
+      for (int s = 0; s < 5; ++s) h->Ginv[r * 5 + s] = (double)G[r][5 + s];
+  }
+  h->project = enable ? 1 : 0;
+  return DGFS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Penalty model (IMEX) entry points
+// ---------------------------------------------------------------------------
+static unsigned grid_for_total(size_t total) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return (unsigned)std::min<size_t>((total + 255) / 256, (size_t)sms * 16);
+}
+
+extern "C" int dgfs_penalty_moments(dgfs_dg_handle h, const void* f,
+                                    int32_t dtype, int32_t npts, double* U,
+                                    void* stream) {
+  if (!h || !f || !U || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
+  if (npts == 0) return DGFS_OK;
+  PenaltyMomentArgs a{};
+  a.f = f; a.f_double = dtype == DGFS_F64; a.Nv = h->base.Nv; a.N = h->base.N;
+  a.c0 = h->c0; a.cw = h->cw; a.U = U;
+  penalty_moments_kernel<<<npts, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_penalty_implicit(dgfs_dg_handle h, const double* U,
+                                     const void* rhs, void* f, void* P,
+                                     void* M, int32_t dtype, int32_t npts,
+                                     double adiv, double cdt, double prefac,
+                                     double omega, void* stream) {
+  if (!h || !U || !rhs || !f || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
+  PenaltyImplicitArgs a{};
+  a.U = U; a.rhs = rhs; a.f = f; a.P = P; a.Mout = M;
+  a.f_double = dtype == DGFS_F64; a.Nv = h->base.Nv; a.N = h->base.N;
+  a.c0 = h->c0; a.adiv = adiv; a.cdt = cdt; a.prefac = prefac; a.omega = omega;
+  a.total = (size_t)npts * h->base.Nv;
+  if (a.total == 0) return DGFS_OK;
+  penalty_implicit_kernel<<<grid_for_total(a.total), 256, 0,
+                            static_cast<cudaStream_t>(stream)>>>(a);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_penalty_collide(dgfs_dg_handle h, const double* U,
+                                    const void* f, void* P, void* M,
+                                    int32_t dtype, int32_t npts, double prefac,
+                                    double omega, void* stream) {
+  if (!h || !U || !f || !P || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
+  PenaltyImplicitArgs a{};
+  a.U = U; a.f = const_cast<void*>(f); a.P = P; a.Mout = M;
+  a.f_double = dtype == DGFS_F64; a.Nv = h->base.Nv; a.N = h->base.N;
+  a.c0 = h->c0; a.prefac = prefac; a.omega = omega;
+  a.total = (size_t)npts * h->base.Nv;
+  if (a.total == 0) return DGFS_OK;
+  penalty_collide_kernel<<<grid_for_total(a.total), 256, 0,
+                           static_cast<cudaStream_t>(stream)>>>(a);
+  DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
 }

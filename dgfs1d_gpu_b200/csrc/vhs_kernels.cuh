@@ -97,6 +97,13 @@ struct VhsEpilogueArgs {
   int dst_base;
   double prefac;
   int Nrho;
+  // conservation projection (no reference counterpart): Q <- Q - sum_k
+  // lambda_k phi_k with phi = (1, cx, cy, cz, |c|^2) and G lambda = moments
+  // of Q, G_jk = sum_v phi_j phi_k cw; Ginv = G^{-1} (row-major)
+  int project;
+  const double* c0;           // [N]
+  double cw;
+  double Ginv[25];
 };
 
 __device__ __forceinline__ int slot_of(const int32_t* slots, int base, int i) {
@@ -819,8 +826,56 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   for (int x = 0; x < N; ++x) {
     const size_t idx = ((size_t)x * N + y) * N + z;
     const double fv = load_real(a.f, a.f_double, fb + idx);
-    const double qv =
-        a.prefac * (v[x].x - fv * a.ReLf[(size_t)e * G::n + idx]);
+    v[x].y = a.prefac * (v[x].x - fv * a.ReLf[(size_t)e * G::n + idx]);
+  }
+  double lam[5] = {0, 0, 0, 0, 0};
+  if (a.project) {
+    // moments of this point's Q (FP64): thread -> CTA -> cluster, in a
+    // fixed order so every CTA derives the same multipliers
+    double* red = reinterpret_cast<double*>(A);  // A is free again
+    const double cy = a.c0[y], cz = a.c0[z];
+    double m[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+    for (int x = 0; x < N; ++x) {
+      const double cx = a.c0[x], q = v[x].y * a.cw;
+      m[0] += q; m[1] += q * cx; m[2] += q * cy; m[3] += q * cz;
+      m[4] += q * (cx * cx + cy * cy + cz * cz);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 5; ++k) red[k * G::NT + t] = m[k];
+    __syncthreads();
+    if (t < 5) {
+      double acc = 0;
+      for (int i = 0; i < G::NT; ++i) acc += red[t * G::NT + i];
+      red[5 * G::NT + t] = acc;
+    }
+    cluster_sync_all();
+    double tot[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      double acc = 0;
+      for (int c = 0; c < C; ++c) acc += peer_ptr(red, (unsigned)c)[5 * G::NT + k];
+      tot[k] = acc;
+    }
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      double l = 0;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) l += a.Ginv[j * 5 + k] * tot[k];
+      lam[j] = l;
+    }
+    cluster_sync_all();  // peers have read this CTA's partial sums
+  }
+#pragma unroll
+  for (int x = 0; x < N; ++x) {
+    const size_t idx = ((size_t)x * N + y) * N + z;
+    double qv = v[x].y;
+    if (a.project) {
+      const double cx = a.c0[x], cy = a.c0[y], cz = a.c0[z];
+      qv -= lam[0] + lam[1] * cx + lam[2] * cy + lam[3] * cz +
+            lam[4] * (cx * cx + cy * cy + cz * cz);
+    }
     if (a.q_double) static_cast<double*>(a.Q)[qb + idx] += qv;
     else static_cast<float*>(a.Q)[qb + idx] += (float)qv;
   }

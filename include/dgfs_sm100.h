@@ -90,6 +90,13 @@ int dgfs_vhs_fs(dgfs_vhs_handle h, const void* f, void* Q, int32_t dtype,
                 int32_t Ne, int32_t elem, int32_t modein, int32_t modeout,
                 void* stream);
 
+/* Conservation projection (no counterpart in the reference, which has no
+ * projection): when enabled, every evaluation subtracts from its increment
+ * the minimal-L2 combination of (1, cx, cy, cz, |c|^2) that makes the five
+ * discrete moments sum_v Q phi cw vanish (FP64 multipliers, Gram matrix
+ * inverted at enable time).  Off by default. */
+int dgfs_vhs_set_projection(dgfs_vhs_handle h, int32_t enable);
+
 /* Per-eval local moments (rho, ux, uy, uz, T) of the last FP32 evaluation
  * batch, device pointer owned by the handle ([max_evals][5] doubles). */
 const double* dgfs_vhs_last_moments(dgfs_vhs_handle h);
@@ -204,6 +211,28 @@ int dgfs_dg_moments(dgfs_dg_handle h, const void* coeff, int32_t dtype,
  * the stream and writes the two sums to host memory out2. */
 int dgfs_dg_residual(dgfs_dg_handle h, const void* x, const void* y, int64_t n,
                      int32_t dtype, double* out2, void* stream);
+
+/*
+ * Penalty (BGK-type) model of the penalised IMEX schemes, FP64 arithmetic
+ * (dgfs1D/astd/scattering.py:44-284, astd/kernels/scattering/
+ * bgk-direct-gll.mako).  Points are the npts = K*Ne slots of f; U holds five
+ * moments per point: rho, rho ux, rho uy, rho uz, E = sum f |c|^2 cw, with
+ * T = (E - |rho u|^2/rho)/(1.5 rho) and nu = prefac rho T^(1-omega).
+ */
+/* U = moments of f (replaces the cuBLAS gemm of astd/scattering.py:155-162). */
+int dgfs_penalty_moments(dgfs_dg_handle h, const void* f, int32_t dtype,
+                         int32_t npts, double* U, void* stream);
+/* Closed-form implicit stage (updateDistribution{q}_BDF / _LM):
+ * f = (rhs + cdt nu M(U)) / (adiv + cdt nu); optionally P = nu (M - f) and
+ * the Maxwellian M (null to skip). */
+int dgfs_penalty_implicit(dgfs_dg_handle h, const double* U, const void* rhs,
+                          void* f, void* P, void* M, int32_t dtype,
+                          int32_t npts, double adiv, double cdt, double prefac,
+                          double omega, void* stream);
+/* P = nu (M(U) - f) (collide, bgk-direct-gll.mako:157-181); M optional. */
+int dgfs_penalty_collide(dgfs_dg_handle h, const double* U, const void* f,
+                         void* P, void* M, int32_t dtype, int32_t npts,
+                         double prefac, double omega, void* stream);
 
 /* x0 <- a0 x0 + sum_i as[i] xs[i] over n elements, 1..4 terms, with the
  * a0 == 0 (x0 not read) and a0 == 1 branches of dgfs1D/axnpby.py:10-44. */

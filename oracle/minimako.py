@@ -82,7 +82,19 @@ def compile_template(src):
             for l in _dedent_block(tok[2:-2]):
                 emit(l)
             continue
-        lines = tok.split('\n')
+        raw = tok.split('\n')
+        # join lines inside an unterminated ${ ... } expression
+        lines, buf = [], None
+        for line in raw:
+            buf = line if buf is None else buf + '\n' + line
+            try:
+                _text_line(buf)
+            except ValueError:
+                continue
+            lines.append(buf)
+            buf = None
+        if buf is not None:
+            raise ValueError('unterminated ${ expression')
         for idx, line in enumerate(lines):
             last = idx == len(lines) - 1
             m = _CTRL.match(line)

@@ -533,6 +533,69 @@ def golden_dg(R, kind, Nv=8, Nrho=4, M=6, dev=5.0, Ne=3, Kb=3):
     return out
 
 
+def golden_penalty(R, Nv=8, npts=6, omega=0.81, prefac=3.7):
+    """The penalty kernels of astd bgk-direct-gll.mako on seeded data."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    vsize = Nv ** 3
+    src = render_template(
+        'dgfs1D/astd/kernels/scattering/bgk-direct-gll.mako', vsize=vsize,
+        nalph=5, omega=omega, Pr=1.0, dtype='double', nbdf=[1, 2], nars=[1, 2])
+    K = RefModule(src, tag='bgk')
+    rng = np.random.default_rng(SEED + 11)
+    L = 5.0
+    c0 = np.linspace(-L + L / Nv, L - L / Nv, Nv)
+    g = np.meshgrid(c0, c0, c0, indexing='ij')
+    cv = np.stack([x.ravel() for x in g])
+    cw = (2 * L / Nv) ** 3
+    f = np.stack([_maxwellian_noise(cv, rng, rho=rng.uniform(0.5, 2))
+                  for _ in range(npts)]).ravel()
+    phi = np.vstack([np.ones(vsize), cv, np.sum(cv * cv, axis=0)]) * cw
+    U = np.ascontiguousarray((f.reshape(npts, vsize) @ phi.T).ravel())
+    blk = 256
+    lda = npts * vsize
+    gg = grid_for(lda, blk)
+    cx, cy, cz = (np.ascontiguousarray(cv[i]) for i in range(3))
+    M = np.zeros(lda)
+    K.launch('cmaxwellian', gg, blk, lda, cx, cy, cz, M, U)
+    Q = np.zeros(lda)
+    K.launch('collide', gg, blk, prefac, lda, M, U, f, Q)
+    out = dict(Nv=Nv, npts=npts, omega=omega, prefac=prefac, cv=cv, cw=cw,
+               f=f, U=U, M=M, Q=Q)
+    dt = 0.01
+    L0 = rng.normal(size=lda) * 1e-3
+    L1 = rng.normal(size=lda) * 1e-3
+    f1 = f * (1 + 0.01 * rng.uniform(-1, 1, lda))
+    LU0 = rng.normal(size=npts * 5) * 1e-3
+    LU1 = rng.normal(size=npts * 5) * 1e-3
+    U1 = U * (1 + 0.01 * rng.uniform(-1, 1, U.shape))
+    Un = np.zeros(npts * 5)
+    gm = grid_for(npts, blk)
+    # bdf-222 coefficients, called as Bdf222IntegratorAstd does
+    a1, a2, a3, g1, g2, b = 1. / 3., -4. / 3., 1., -2. / 3., 4. / 3., 2. / 3.
+    K.launch('updateMom2_BDF', gm, blk, prefac, npts, dt, a1, U, -g1, LU0,
+             a2, U1, -g2, LU1, a3, Un, b)
+    fn = np.zeros(lda)
+    K.launch('updateDistribution2_BDF', gg, blk, prefac, lda, dt, a1, f, -g1,
+             L0, a2, f1, -g2, L1, b, M, a3, Un, fn)
+    out.update(dt=dt, L0=L0, L1=L1, f1=f1, LU0=LU0, LU1=LU1, U1=U1,
+               Un_bdf2=Un, fn_bdf2=fn.copy())
+    # imex-lm-bdf2 coefficients (A, B, C of IMEXLM_BDF2_IntegratorAstd)
+    A, B, C = [-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]
+    LM0 = rng.normal(size=npts * 5) * 1e-4
+    LM1 = rng.normal(size=npts * 5) * 1e-4
+    P0 = rng.normal(size=lda) * 1e-4
+    P1 = rng.normal(size=lda) * 1e-4
+    U2 = np.zeros(npts * 5)
+    K.launch('updateMom2_LM', gm, blk, prefac, npts, dt, *A, *B, *C, LU0, LU1,
+             LM0, LM1, U, U1, U2)
+    M2 = M.copy()
+    f2 = np.zeros(lda)
+    K.launch('updateDistribution2_LM', gg, blk, prefac, lda, dt, *A, *B, *C,
+             L0, L1, P0, P1, M2, f, f1, f2, U, U1, U2)
+    out.update(LM0=LM0, LM1=LM1, P0=P0, P1=P1, U2_lm2=U2, f2_lm2=f2)
+    return out
+
+
 def golden_setup(R):
     """Velocity meshes, rules and DG bases from the reference setup code."""
     out = {}
@@ -586,6 +649,8 @@ def main():
         np.savez_compressed(
             os.path.join(HERE, 'dg_%s_N8.npz' % kind.replace('-', '_')),
             **golden_dg(R, kind))
+    np.savez_compressed(os.path.join(HERE, 'penalty_N8.npz'),
+                        **golden_penalty(R))
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith('.npz'):
             print(fn, os.path.getsize(os.path.join(HERE, fn)), 'bytes')

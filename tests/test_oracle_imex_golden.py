@@ -1,0 +1,56 @@
+"""The IMEX oracle's kernels against the reference's bgk-direct-gll.mako."""
+import os
+
+import numpy as np
+
+from oracle import imex as oim
+
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b))
+                 / np.linalg.norm(np.ravel(b)))
+
+
+def test_penalty_kernels_match_reference():
+    g = np.load(os.path.join(G, 'penalty_N8.npz'))
+    npts, cv, cw = int(g['npts']), g['cv'], float(g['cw'])
+    f = g['f'].reshape(npts, -1)
+    U = oim.moments5(f, cv, cw)
+    assert _rel(U, g['U'].reshape(npts, 5)) < 1e-14
+    U = g['U'].reshape(npts, 5)
+    assert _rel(oim.maxwellian(U, cv), g['M']) < 1e-13
+    pre, om = float(g['prefac']), float(g['omega'])
+    assert _rel(oim.collide(U, f, cv, pre, om), g['Q']) < 1e-12
+    dt = float(g['dt'])
+    a1, a2, a3, g1, g2, b = 1. / 3., -4. / 3., 1., -2. / 3., 4. / 3., 2. / 3.
+    U0, U1 = U, g['U1'].reshape(npts, 5)
+    LU0, LU1 = g['LU0'].reshape(npts, 5), g['LU1'].reshape(npts, 5)
+    Un = -(a1 * U0 + (-g1) * dt * LU0 + a2 * U1 + (-g2) * dt * LU1) / a3
+    assert _rel(Un, g['Un_bdf2']) < 1e-14
+    rhs = -(a1 * g['f'] + (-g1) * dt * g['L0'] + a2 * g['f1'] + (-g2) * dt * g['L1'])
+    # the kernel takes the Maxwellian as an argument (the golden passed the
+    # one of U0); nu comes from the new moments
+    M = g['M'].reshape(npts, -1)
+    nu = oim.nu(Un, pre, om)[:, None]
+    fn = (rhs.reshape(M.shape) + b * dt * nu * M) / (a3 + b * dt * nu)
+    assert _rel(fn, g['fn_bdf2']) < 1e-13
+    # and with a consistent Maxwellian the oracle's implicit() is that formula
+    Mn = oim.maxwellian(Un, cv)
+    assert _rel(oim.implicit(Un, rhs, cv, a3, b * dt, pre, om),
+                (rhs.reshape(M.shape) + b * dt * nu * Mn) / (a3 + b * dt * nu)) < 1e-15
+    A, B, C = [-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]
+    hs = [dict(U=U0, LU=LU0, LM=g['LM0'].reshape(npts, 5), F=g['f'],
+               L=g['L0'], P=g['P0']),
+          dict(U=U1, LU=LU1, LM=g['LM1'].reshape(npts, 5), F=g['f1'],
+               L=g['L1'], P=g['P1'])]
+    s = 2
+    U2 = sum(-A[s - i - 1] * hs[i]['U'] + dt * B[s - i - 1] * hs[i]['LU']
+             + dt * C[s - i] * hs[i]['LM'] for i in range(s))
+    assert _rel(U2, g['U2_lm2']) < 1e-14
+    rhs = sum(-A[s - i - 1] * hs[i]['F'] + dt * B[s - i - 1] * hs[i]['L']
+              + dt * C[s - i] * hs[i]['P'] for i in range(s))
+    nu2 = oim.nu(U2, pre, om)[:, None]
+    f2 = (rhs.reshape(M.shape) + C[0] * dt * nu2 * M) / (1.0 + C[0] * dt * nu2)
+    assert _rel(f2, g['f2_lm2']) < 1e-13

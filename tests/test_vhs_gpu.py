@@ -129,3 +129,32 @@ def test_n24(lib, precision):
     tol = FP64_TOL if precision == 'fp64' else FP32_TOL
     for s in range(2):
         assert _rel(Q.cpu().numpy()[s], vhs_gll_fs(tab, prefac, f[s])) < tol
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_conservation_projection(lib, precision):
+    """After projection the five moments of Q vanish to 1e-12 (relative to
+    the moments of |Q|), and the correction is the minimal-L2 one."""
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    N, M, Nrho, dev, full = CASES[2]
+    vm, prefac, gamma, f = vhs_case(N, M, Nrho, dev, full, nslots=2,
+                                    noise=0.05)
+    op = VHSOperator(**op_kwargs(vm, prefac, gamma), precision=precision,
+                     max_evals=2)
+    fd = torch.tensor(f, device='cuda')
+    Q0 = torch.zeros_like(fd)
+    op.eval(fd, Q0)
+    op.set_projection(True)
+    Q1 = torch.zeros_like(fd)
+    op.eval(fd, Q1)
+    torch.cuda.synchronize()
+    cv, cw = vm.cv, vm.cw
+    phi = np.vstack([np.ones(N ** 3), cv, np.sum(cv ** 2, axis=0)])
+    G = (phi * cw) @ phi.T
+    for s in range(2):
+        q0, q1 = Q0.cpu().numpy()[s], Q1.cpu().numpy()[s]
+        scale = np.abs(phi * cw) @ np.abs(q0)
+        mom1 = (phi * cw) @ q1
+        assert np.all(np.abs(mom1) <= 1e-12 * scale), mom1 / scale
+        lam = np.linalg.solve(G, (phi * cw) @ q0)
+        assert _rel(q1, q0 - lam @ phi) < 1e-12
