@@ -226,6 +226,10 @@ def main():
             print(json.dumps({'kernel_only_ms_per_step': ms}), flush=True)
         return
 
+    # project autotuner: cluster size of the FP32 terms kernel, timed on this
+    # very batch
+    tune = op32.autotune(fd, Q, reps=3)
+
     # headline: FP32 fused operator, inputs resident in HBM
     with ClockSampler(local) as clk:
         ms32 = timed(lambda: op32.eval(fd, Q), args.steps, args.warmup)
@@ -273,6 +277,30 @@ def main():
     terms_ms = float(stage[3])
 
     fma_peak = fp32_fma_peak(torch)
+
+    # uneven multi-problem batch: 6 VHS problems (N=16/24/32) + 2 VSS
+    # mixtures, one CUDA graph launch per stage vs the same launches issued
+    # one after another on one stream
+    from dgfs1d_gpu_b200.batch import StageGraph
+    from dgfs1d_gpu_b200.workloads_c3 import build_c3
+    probs = build_c3(precision='fp32')
+    sg = StageGraph([p['fn'] for p in probs])
+    sg.capture()
+    b_evals = sum(p['nevals'] for p in probs)
+    b_steps = max(3, args.steps // 4)
+    ms_graph = timed(sg.replay, b_steps, 3)
+
+    def serial():
+        for p in probs:
+            p['fn']()
+    ms_serial = timed(serial, b_steps, 3)
+    batch = {'value': b_evals * world / (ms_graph * 1e-3), 'unit': UNIT,
+             'ms_per_stage': ms_graph, 'graph_launches_per_stage': 1,
+             'serial_stream_ms_per_stage': ms_serial,
+             'problems': [p['name'] for p in probs],
+             'evals_per_stage': b_evals,
+             'note': 'VSS evals count each (p,q) pair at each point'}
+    del sg
 
     barrier()
     if rank == 0:
@@ -327,7 +355,7 @@ def main():
             'e2e': {'value': evals / (ms_e2e * 1e-3), 'unit': UNIT,
                     'h2d_bytes_per_step': int(fh.numel() * 8),
                     'd2h_bytes_per_step': int(qh.numel() * 8)},
-            'roofline': {'bound': 'hbm', 'kernel': 'vhs_terms_kernel<float,32,4>',
+            'roofline': {'bound': 'hbm', 'kernel': f'vhs_terms_fp32_kernel<32,{op32.variant}>',
                          'achieved': alg_bytes / (terms_ms * 1e-3) / 1e9,
                          'peak': hbm_peak, 'unit': 'GB/s',
                          'frac': alg_bytes / (terms_ms * 1e-3) / 1e9 / hbm_peak,
@@ -341,6 +369,9 @@ def main():
             'stage_ms': dict(zip(['prologue', 'tables', 'maxwell_gain',
                                   'terms', 'epilogue'],
                                  [round(float(x), 4) for x in stage])),
+            'uneven_batch': batch,
+            'autotune_terms_ms': {str(k): round(v, 4) for k, v in tune.items()},
+            'terms_cluster': op32.variant,
             'cpu_baseline': cpu,
             'clocks': clk.summary(),
             'gpu_launches': 5 * args.steps,

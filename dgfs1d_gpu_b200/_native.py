@@ -83,6 +83,9 @@ _SIGNATURES = [
       ctypes.c_void_p]),
     ('dgfs_vhs_last_moments', ctypes.c_void_p, [ctypes.c_void_p]),
     ('dgfs_vhs_set_projection', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ('dgfs_vhs_variants', ctypes.c_int,
+     [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
+    ('dgfs_vhs_set_variant', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_vhs_destroy', ctypes.c_int, [ctypes.c_void_p]),
     ('dgfs_vhs_profile', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_vhs_stage_ms', ctypes.c_int,

@@ -64,6 +64,7 @@ class VHSOperator:
         nat.check(nat.lib().dgfs_vhs_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h
         self.Nrho, self.M = d.Nrho, d.M
+        self.variant = 0          # 0: the library's default cluster size
 
     def eval(self, f, Q, src=None, dst=None, src_base=0, dst_base=0,
              nevals=None, stream=None):
@@ -90,6 +91,40 @@ class VHSOperator:
             ctypes.c_void_p(src.data_ptr() if src is not None else 0), int(src_base),
             ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
             int(nevals), _stream_ptr(stream)))
+
+    def variants(self):
+        """Cluster sizes of the FP32 terms kernel compiled for this N."""
+        buf = (ctypes.c_int32 * 8)()
+        n = nat.lib().dgfs_vhs_variants(self.N, buf, 8)
+        if n < 0:
+            nat.check(n)
+        return list(buf[:n])
+
+    def set_variant(self, cluster):
+        nat.check(nat.lib().dgfs_vhs_set_variant(self._h, int(cluster)))
+        self.variant = int(cluster)
+
+    def autotune(self, f, Q, reps=3, stream=None):
+        """Time every terms-kernel variant on (f, Q) and keep the fastest.
+
+        Returns {cluster: ms per evaluation call}.  Q is overwritten.
+        """
+        if self.precision != 'fp32':
+            return {}
+        times = {}
+        for c in self.variants():
+            self.set_variant(c)
+            self.eval(f, Q, stream=stream)           # warm-up
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record()
+            for _ in range(reps):
+                self.eval(f, Q, stream=stream)
+            e.record()
+            e.synchronize()
+            times[c] = s.elapsed_time(e) / reps
+        self.set_variant(min(times, key=times.get))
+        return times
 
     def set_projection(self, enable=True):
         """Toggle the FP64 conservation projection of every evaluation."""

@@ -120,6 +120,7 @@ struct dgfs_vhs_s {
   int device = 0;
   int project = 0;
   double Ginv[25] = {};
+  int c32 = 0;  // cluster size of the FP32 terms kernel (autotuner choice)
   // constant tables
   double* c0 = nullptr;      // [N]
   double* b2 = nullptr;      // [n]
@@ -366,6 +367,41 @@ extern "C" const double* dgfs_vhs_last_moments(dgfs_vhs_handle h) {
   return h ? h->moments : nullptr;
 }
 
+// FP32 terms kernel at cluster size C (each C must divide N and fit three
+// slabs in shared memory).
+template <int N, int C>
+static int launch_terms32_c(const VhsTermsArgs& a, int nevals, int Nrho,
+                            cudaStream_t st) {
+  using G = Geo<N, C>;
+  const size_t smem = 3 * slab_bytes(N, C, sizeof(float2)) +
+                      2 * 9 * N * sizeof(float2);
+  return launch_cluster(vhs_terms_fp32_kernel<N, C>, dim3(C, Nrho, nevals),
+                        dim3(G::NT), C, smem, st, a);
+}
+
+template <int N> struct Terms32Variants;
+template <> struct Terms32Variants<8> { static constexpr int v[2] = {1, 2}; };
+template <> struct Terms32Variants<16> { static constexpr int v[2] = {1, 2}; };
+template <> struct Terms32Variants<24> { static constexpr int v[3] = {3, 4, 6}; };
+template <> struct Terms32Variants<32> { static constexpr int v[2] = {4, 8}; };
+
+template <int N>
+static int launch_terms32(int c, const VhsTermsArgs& a, int nevals, int Nrho,
+                          cudaStream_t st) {
+  if constexpr (N == 8 || N == 16) {
+    if (c == 1) return launch_terms32_c<N, 1>(a, nevals, Nrho, st);
+    if (c == 2) return launch_terms32_c<N, 2>(a, nevals, Nrho, st);
+  } else if constexpr (N == 24) {
+    if (c == 3) return launch_terms32_c<N, 3>(a, nevals, Nrho, st);
+    if (c == 4) return launch_terms32_c<N, 4>(a, nevals, Nrho, st);
+    if (c == 6) return launch_terms32_c<N, 6>(a, nevals, Nrho, st);
+  } else if constexpr (N == 32) {
+    if (c == 4) return launch_terms32_c<N, 4>(a, nevals, Nrho, st);
+    if (c == 8) return launch_terms32_c<N, 8>(a, nevals, Nrho, st);
+  }
+  return fail(DGFS_ERR_UNSUPPORTED, "terms kernel cluster size not compiled in");
+}
+
 template <int N>
 static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                    int q_double, const int32_t* src_slots, int src_base,
@@ -425,12 +461,8 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     VhsTermsArgs a{};
     a.Fg = h->Fg; a.ph = h->ph; a.uv = h->uv; a.mult = h->mult;
     a.b1w = h->b1w32; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
-    const size_t smem2 = 3 * slab_bytes(N, C32, sizeof(float2)) +
-                         2 * 9 * N * sizeof(float2);
-    if ((rc = launch_cluster(vhs_terms_fp32_kernel<N, C32>,
-                             dim3(C32, h->Nrho, nevals), dim3(G32::NT), C32,
-                             smem2, st, a)))
-      return rc;
+    const int c = h->c32 ? h->c32 : C32;
+    if ((rc = launch_terms32<N>(c, a, nevals, h->Nrho, st))) return rc;
     mark();
     if (h->aux) DGFS_CUDA(cudaStreamWaitEvent(st, h->join, 0));  // join
   } else {
@@ -1287,4 +1319,31 @@ extern "C" int dgfs_penalty_collide(dgfs_dg_handle h, const double* U,
                            static_cast<cudaStream_t>(stream)>>>(a);
   DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
+}
+
+// Variants of the FP32 terms kernel (cluster sizes) for the autotuner.
+extern "C" int dgfs_vhs_variants(int32_t N, int32_t* out, int32_t max) {
+  if (!out || max <= 0) return fail(DGFS_ERR_INVALID, "bad output buffer");
+  const int* v = nullptr;
+  int n = 0;
+  switch (N) {
+    case 8: v = Terms32Variants<8>::v; n = 2; break;
+    case 16: v = Terms32Variants<16>::v; n = 2; break;
+    case 24: v = Terms32Variants<24>::v; n = 3; break;
+    case 32: v = Terms32Variants<32>::v; n = 2; break;
+    default: return fail(DGFS_ERR_UNSUPPORTED, "N not compiled in");
+  }
+  for (int i = 0; i < n && i < max; ++i) out[i] = v[i];
+  return std::min(n, (int)max);
+}
+
+extern "C" int dgfs_vhs_set_variant(dgfs_vhs_handle h, int32_t cluster) {
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  int buf[8];
+  const int n = dgfs_vhs_variants(h->N, buf, 8);
+  if (n < 0) return n;
+  for (int i = 0; i < n; ++i)
+    if (buf[i] == cluster) { h->c32 = cluster; return DGFS_OK; }
+  if (cluster == 0) { h->c32 = 0; return DGFS_OK; }
+  return fail(DGFS_ERR_INVALID, "cluster size not a variant for this N");
 }

@@ -97,6 +97,13 @@ int dgfs_vhs_fs(dgfs_vhs_handle h, const void* f, void* Q, int32_t dtype,
  * inverted at enable time).  Off by default. */
 int dgfs_vhs_set_projection(dgfs_vhs_handle h, int32_t enable);
 
+/* Autotuning (no reference counterpart): the FP32 terms kernel comes in
+ * several thread-block-cluster sizes per N.  dgfs_vhs_variants writes the
+ * compiled cluster sizes for N into out (up to max) and returns their count;
+ * dgfs_vhs_set_variant selects one for a handle (0 = built-in default). */
+int dgfs_vhs_variants(int32_t N, int32_t* out, int32_t max);
+int dgfs_vhs_set_variant(dgfs_vhs_handle h, int32_t cluster);
+
 /* Per-eval local moments (rho, ux, uy, uz, T) of the last FP32 evaluation
  * batch, device pointer owned by the handle ([max_evals][5] doubles). */
 const double* dgfs_vhs_last_moments(dgfs_vhs_handle h);

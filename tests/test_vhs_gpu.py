@@ -158,3 +158,31 @@ def test_conservation_projection(lib, precision):
         assert np.all(np.abs(mom1) <= 1e-12 * scale), mom1 / scale
         lam = np.linalg.solve(G, (phi * cw) @ q0)
         assert _rel(q1, q0 - lam @ phi) < 1e-12
+
+
+@pytest.mark.parametrize('case', [(16, 6, 8, 5., False), (24, 12, 12, 5., True),
+                                  (32, 12, 16, 6., True)],
+                         ids=lambda c: f'N{c[0]}')
+def test_fp32_cluster_variants_match_oracle(lib, case):
+    """Every cluster size of the FP32 terms kernel (the autotuner's search
+    space) gives the oracle's Q; the autotuner keeps one of them."""
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    N, M, Nrho, dev, full = case
+    vm, prefac, gamma, f = vhs_case(N, M, Nrho, dev, full, nslots=2)
+    tab = vhs_tables(vm, gamma)
+    refs = [vhs_gll_fs(tab, prefac, f[s]) for s in range(2)]
+    op = VHSOperator(**op_kwargs(vm, prefac, gamma), precision='fp32',
+                     max_evals=2)
+    fd = torch.tensor(f, dtype=torch.float64, device='cuda')
+    variants = op.variants()
+    assert len(variants) >= 2
+    for c in variants:
+        op.set_variant(c)
+        Q = torch.zeros_like(fd)
+        op.eval(fd, Q)
+        torch.cuda.synchronize()
+        for s in range(2):
+            err = _rel(Q.cpu().numpy()[s], refs[s])
+            assert err < FP32_TOL, f'N={N} cluster {c}: rel L2 {err:.3e}'
+    times = op.autotune(fd, torch.zeros_like(fd), reps=2)
+    assert set(times) == set(variants) and op.variant in variants
