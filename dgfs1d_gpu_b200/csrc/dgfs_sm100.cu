@@ -129,7 +129,10 @@ struct dgfs_vhs_s {
   void* ph = nullptr;        // [Nrho][Mu][3][N] precision R
   double* kappa = nullptr;   // [Nrho][Mu][3]
   float* mult = nullptr;     // [Mu]
+  float2* nyq32 = nullptr;   // [Nrho][Mu][3] exp(i N kappa_a) (FP32 mode)
   // scratch
+  float2* rho = nullptr;     // [E][Nrho][Mu][3][N][N] Nyquist-plane transforms
+  float2* Fny = nullptr;     // [E][3][N][N] Nyquist planes of F_g
   void* Fg = nullptr;        // [E][n] complex R
   void* H = nullptr;         // [E][Nrho][n] complex R
   double* ReLf = nullptr;    // [E][n]
@@ -143,11 +146,14 @@ struct dgfs_vhs_s {
   cudaEvent_t ev[6] = {};
   cudaEvent_t evg[2] = {};
   int ev_used = 0;
-  // FP32 mode: the FP64 Maxwellian-gain kernel runs on a forked stream,
-  // concurrently with the FP32 terms kernel (they share SMs: the gain kernel
-  // needs little shared memory and few registers)
-  cudaStream_t aux = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  // FP32 mode, three streams: the caller's runs prologue, Nyquist planes and
+  // epilogue; `aux` (lowest priority) the tables and the FP64 Maxwellian-gain
+  // kernel; `hi` (highest priority) the FP32 terms kernel, so the block
+  // scheduler fills SMs with terms CTAs first and the gain kernel takes the
+  // SMs the terms kernel's last wave leaves idle
+  cudaStream_t aux = nullptr, hi = nullptr;
+  cudaEvent_t fork0 = nullptr, tab = nullptr, fork1 = nullptr;
+  cudaEvent_t join_hi = nullptr, join_aux = nullptr;
 };
 
 // FP64-kernel and FP32-terms cluster sizes per N (shared memory per CTA
@@ -171,10 +177,14 @@ static int c32_of(int N) {
   }
 }
 template <int N> struct VhsClusters;
-template <> struct VhsClusters<8> { static constexpr int c64 = 1, c32 = 1; };
-template <> struct VhsClusters<16> { static constexpr int c64 = 2, c32 = 1; };
-template <> struct VhsClusters<24> { static constexpr int c64 = 4, c32 = 3; };
-template <> struct VhsClusters<32> { static constexpr int c64 = 8, c32 = 4; };
+// c64: FP64 terms kernel; c32: FP32 terms kernel (default); cpro / cepi:
+// prologue / epilogue (FP64, two slabs).  At N=32 a 16-CTA epilogue cluster
+// needs 68 KB per CTA, so three CTAs share an SM and a 24-point batch runs in
+// one wave; the prologue's moment/Maxwellian set-up is faster at 8 CTAs.
+template <> struct VhsClusters<8> { static constexpr int c64 = 1, c32 = 1, cpro = 1, cepi = 1; };
+template <> struct VhsClusters<16> { static constexpr int c64 = 2, c32 = 1, cpro = 2, cepi = 2; };
+template <> struct VhsClusters<24> { static constexpr int c64 = 4, c32 = 3, cpro = 4, cepi = 4; };
+template <> struct VhsClusters<32> { static constexpr int c64 = 8, c32 = 4, cpro = 8, cepi = 16; };
 
 static size_t slab_bytes(int N, int C, size_t elem) {
   return (size_t)(N / C) * N * (N + 1) * elem;
@@ -183,16 +193,17 @@ static size_t slab_bytes(int N, int C, size_t elem) {
 static void free_handle(dgfs_vhs_s* h) {
   void* ptrs[] = {h->c0, h->b2, h->b1w64, h->b1w32, h->ph, h->kappa, h->mult,
                   h->Fg, h->H, h->ReLf, h->mhat, h->moments, h->uv, h->hh,
-                  h->GM};
+                  h->GM, h->nyq32, h->rho, h->Fny};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : h->ev)
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : h->evg)
     if (e) cudaEventDestroy(e);
-  if (h->fork) cudaEventDestroy(h->fork);
-  if (h->join) cudaEventDestroy(h->join);
+  for (cudaEvent_t e : {h->fork0, h->tab, h->fork1, h->join_hi, h->join_aux})
+    if (e) cudaEventDestroy(e);
   if (h->aux) cudaStreamDestroy(h->aux);
+  if (h->hi) cudaStreamDestroy(h->hi);
   delete h;
 }
 
@@ -308,8 +319,14 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_desc* d, dgfs_vhs_handle* out) {
       const double sc = ax == 0 ? std::sqrt((double)mult[u]) : 1.0;
       ph32[i] = make_float2((float)(sc * ph64[i].x), (float)(sc * ph64[i].y));
     }
+    // Nyquist rotation factors exp(i N kappa_a), unit modulus
+    std::vector<float2> nyq(kappa.size());
+    for (size_t i = 0; i < kappa.size(); ++i)
+      nyq[i] = make_float2((float)std::cos(N * kappa[i]),
+                           (float)std::sin(N * kappa[i]));
     float2* p32 = nullptr;
-    if ((rc = upload(&h->b1w32, b1w32)) || (rc = upload(&p32, ph32))) {
+    if ((rc = upload(&h->b1w32, b1w32)) || (rc = upload(&p32, ph32)) ||
+        (rc = upload(&h->nyq32, nyq))) {
       free_handle(h);
       return rc;
     }
@@ -335,6 +352,8 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_desc* d, dgfs_vhs_handle* out) {
     alloc(&h->uv, E * Nrho * Mu * 6 * N * sizeof(float2));
     alloc((void**)&h->hh, E * Nrho * Mu * 3 * N * sizeof(double2));
     alloc((void**)&h->GM, E * n * sizeof(double2));
+    alloc((void**)&h->rho, E * Nrho * Mu * 3 * N * N * sizeof(float2));
+    alloc((void**)&h->Fny, E * 3 * N * N * sizeof(float2));
   }
   if (ce_ != cudaSuccess) {
     free_handle(h);
@@ -342,11 +361,15 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_desc* d, dgfs_vhs_handle* out) {
                 std::string("scratch allocation: ") + cudaGetErrorString(ce_));
   }
   if (fp32) {
-    cudaError_t e1 = cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking);
+    int lo_prio = 0, hi_prio = 0;
+    cudaError_t e1 = cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
     if (e1 == cudaSuccess)
-      e1 = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+      e1 = cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, lo_prio);
     if (e1 == cudaSuccess)
-      e1 = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
+      e1 = cudaStreamCreateWithPriority(&h->hi, cudaStreamNonBlocking, hi_prio);
+    for (cudaEvent_t* ev : {&h->fork0, &h->tab, &h->fork1, &h->join_hi, &h->join_aux})
+      if (e1 == cudaSuccess)
+        e1 = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     if (e1 != cudaSuccess) {
       free_handle(h);
       return fail(DGFS_ERR_CUDA, std::string("stream/event creation: ") +
@@ -373,10 +396,13 @@ template <int N, int C>
 static int launch_terms32_c(const VhsTermsArgs& a, int nevals, int Nrho,
                             cudaStream_t st) {
   using G = Geo<N, C>;
+  // three slabs, two table slots, the staged plane transforms of one term
   const size_t smem = 3 * slab_bytes(N, C, sizeof(float2)) +
-                      2 * 9 * N * sizeof(float2);
-  return launch_cluster(vhs_terms_fp32_kernel<N, C>, dim3(C, Nrho, nevals),
-                        dim3(G::NT), C, smem, st, a);
+                      2 * (9 * N + 4) * sizeof(float2) +
+                      (size_t)(N * N + 2 * G::P * N) * sizeof(float2);
+  return launch_cluster(vhs_terms_fp32_kernel<N, C>,
+                        dim3(C, (Nrho + 1) / 2, nevals), dim3(G::NT), C, smem,
+                        st, a);
 }
 
 template <int N> struct Terms32Variants;
@@ -409,7 +435,11 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                    cudaStream_t st) {
   constexpr int C64 = VhsClusters<N>::c64;
   constexpr int C32 = VhsClusters<N>::c32;
+  constexpr int CPRO = VhsClusters<N>::cpro;
+  constexpr int CEPI = VhsClusters<N>::cepi;
   using G64 = Geo<N, C64>;
+  using GPRO = Geo<N, CPRO>;
+  using GEPI = Geo<N, CEPI>;
   using G32 = Geo<N, C32>;
   const bool fp32 = h->precision == DGFS_PREC_FP32;
   int rc;
@@ -424,47 +454,62 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     a.f = f; a.f_double = f_double; a.src_slots = src_slots; a.src_base = src_base;
     a.c0 = h->c0; a.b2 = h->b2; a.cw = h->cw; a.split = fp32 ? 1 : 0;
     a.Fg = h->Fg; a.ReLf = h->ReLf; a.mhat = h->mhat; a.moments = h->moments;
-    const size_t smem = 2 * slab_bytes(N, C64, sizeof(double2)) +
+    a.Fny = h->Fny;
+    const size_t smem = 2 * slab_bytes(N, CPRO, sizeof(double2)) +
                         3 * N * sizeof(double2) + 8 * sizeof(double);
-    if ((rc = launch_cluster(vhs_prologue_kernel<N, C64>, dim3(C64, nevals),
-                             dim3(G64::NT), C64, smem, st, a)))
+    if ((rc = launch_cluster(vhs_prologue_kernel<N, CPRO>, dim3(CPRO, nevals),
+                             dim3(GPRO::NT), CPRO, smem, st, a)))
       return rc;
   }
   mark();
   if (fp32) {
+    // aux: tables (needs the prologue's Maxwellian spectra)
+    DGFS_CUDA(cudaEventRecord(h->fork0, st));
+    DGFS_CUDA(cudaStreamWaitEvent(h->aux, h->fork0, 0));
     VhsTablesArgs t{};
     t.mhat = h->mhat; t.mult = h->mult; t.kappa = h->kappa; t.uv = h->uv;
     t.hh = h->hh;
     t.Mu = h->Mu; t.Nrho = h->Nrho; t.nevals = nevals; t.uv_double = 0;
     const int total = nevals * h->Nrho * h->Mu * 3;
     if ((rc = launch_plain(vhs_tables_kernel<N>, dim3((total + 95) / 96),
-                           dim3(96), 0, st, t)))
+                           dim3(96), 0, h->aux, t)))
       return rc;
-    mark();
-    VhsGainArgs g{};
-    g.hh = h->hh; g.mult = h->mult; g.b1w = h->b1w64; g.GM = h->GM;
-    g.Mu = h->Mu; g.Nrho = h->Nrho;
-    const size_t smem = (size_t)h->Mu * (2 * N + 1) * sizeof(double2);
-    cudaStream_t gst = st;
-    if (h->aux) {  // fork: gain runs beside the terms kernel
-      DGFS_CUDA(cudaEventRecord(h->fork, st));
-      DGFS_CUDA(cudaStreamWaitEvent(h->aux, h->fork, 0));
-      gst = h->aux;
-    }
-    if (h->profile) cudaEventRecord(h->evg[0], gst);
-    if ((rc = launch_plain(vhs_maxwell_gain_kernel<N>, dim3(N, nevals),
-                           dim3(256), smem, gst, g)))
-      return rc;
-    if (h->profile) cudaEventRecord(h->evg[1], gst);
-    if (h->aux) DGFS_CUDA(cudaEventRecord(h->join, h->aux));
-    mark();
+    DGFS_CUDA(cudaEventRecord(h->tab, h->aux));
+    // caller's stream: Nyquist-plane transforms, concurrently with the tables
     VhsTermsArgs a{};
     a.Fg = h->Fg; a.ph = h->ph; a.uv = h->uv; a.mult = h->mult;
     a.b1w = h->b1w32; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
-    const int c = h->c32 ? h->c32 : C32;
-    if ((rc = launch_terms32<N>(c, a, nevals, h->Nrho, st))) return rc;
+    a.nyq = h->nyq32; a.rho = h->rho; a.Fny = h->Fny;
+    const size_t psmem = (size_t)(9 * N * (N + 1) + 2 * (3 * N + 3)) * sizeof(float2);
+    if ((rc = launch_plain(vhs_nyq_planes_kernel<N>,
+                           dim3((h->Mu + 1) / 2, h->Nrho, nevals), dim3(6 * N),
+                           psmem, st, a)))
+      return rc;
+    DGFS_CUDA(cudaStreamWaitEvent(st, h->tab, 0));
     mark();
-    if (h->aux) DGFS_CUDA(cudaStreamWaitEvent(st, h->join, 0));  // join
+    // hi: terms
+    DGFS_CUDA(cudaEventRecord(h->fork1, st));
+    DGFS_CUDA(cudaStreamWaitEvent(h->hi, h->fork1, 0));
+    if (h->profile) cudaEventRecord(h->ev[evi++], h->hi);
+    const int c = h->c32 ? h->c32 : C32;
+    if ((rc = launch_terms32<N>(c, a, nevals, h->Nrho, h->hi))) return rc;
+    if (h->profile) cudaEventRecord(h->ev[evi++], h->hi);
+    DGFS_CUDA(cudaEventRecord(h->join_hi, h->hi));
+    // aux (after the tables): Maxwellian gain, behind the terms kernel
+    VhsGainArgs g{};
+    g.hh = h->hh; g.mult = h->mult; g.b1w = h->b1w64; g.GM = h->GM;
+    g.Mu = h->Mu; g.Nrho = h->Nrho;
+    const size_t per_p = (size_t)h->Mu * (2 * N + 1) * sizeof(double2);
+    g.pch = (int)std::max<size_t>(1, std::min<size_t>(h->Nrho, (104 * 1024) / per_p));
+    const size_t smem = per_p * g.pch;
+    if (h->profile) cudaEventRecord(h->evg[0], h->aux);
+    if ((rc = launch_plain(vhs_maxwell_gain_kernel<N>, dim3(N, nevals),
+                           dim3(GainGeo<N>::NT), smem, h->aux, g)))
+      return rc;
+    if (h->profile) cudaEventRecord(h->evg[1], h->aux);
+    DGFS_CUDA(cudaEventRecord(h->join_aux, h->aux));
+    DGFS_CUDA(cudaStreamWaitEvent(st, h->join_hi, 0));
+    DGFS_CUDA(cudaStreamWaitEvent(st, h->join_aux, 0));
   } else {
     mark(); mark();  // no tables / Maxwellian-gain stages in FP64 mode
     VhsTermsArgs a{};
@@ -485,12 +530,13 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     a.ReLf = h->ReLf; a.f = f; a.f_double = f_double;
     a.src_slots = src_slots; a.src_base = src_base;
     a.Q = Q; a.q_double = q_double; a.dst_slots = dst_slots; a.dst_base = dst_base;
-    a.prefac = h->prefac; a.Nrho = h->Nrho;
+    a.prefac = h->prefac;
+    a.Nrho = fp32 ? (h->Nrho + 1) / 2 : h->Nrho;  // FP32: packed radial pairs
     a.project = h->project; a.c0 = h->c0; a.cw = h->cw;
     for (int i = 0; i < 25; ++i) a.Ginv[i] = h->Ginv[i];
-    const size_t smem = 2 * slab_bytes(N, C64, sizeof(double2));
-    if ((rc = launch_cluster(vhs_epilogue_kernel<N, C64>, dim3(C64, nevals),
-                             dim3(G64::NT), C64, smem, st, a)))
+    const size_t smem = 2 * slab_bytes(N, CEPI, sizeof(double2));
+    if ((rc = launch_cluster(vhs_epilogue_kernel<N, CEPI>, dim3(CEPI, nevals),
+                             dim3(GEPI::NT), CEPI, smem, st, a)))
       return rc;
   }
   mark();

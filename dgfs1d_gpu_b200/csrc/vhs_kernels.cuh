@@ -48,6 +48,9 @@ struct VhsPrologueArgs {
   double* ReLf;               // out [nevals][n] Re IFFT(b2 F)
   double2* mhat;              // out [nevals][3][N] Maxwellian 1-D spectra (split)
   double* moments;            // out [nevals][5] rho, ux, uy, uz, T (split)
+  float2* Fny;                // out (split) [nevals][3][N][N] Nyquist planes of
+                              // F_g: [0][ly][lz] at lx=N/2, [1][lx][lz] at
+                              // ly=N/2, [2][lx][ly] at lz=N/2
 };
 
 struct VhsTermsArgs {
@@ -57,6 +60,10 @@ struct VhsTermsArgs {
   const float* mult;          // [Mu] multiplicity of each transformed direction
   const void* b1w;            // [Nrho][n] W_p b1_p(l), precision R
   void* H;                    // out [nevals][Nrho][n] complex, precision R
+                              // (FP32: [nevals][ceil(Nrho/2)][n], packed pairs)
+  const void* nyq;            // FP32: [Nrho][Mu][3] exp(i N kappa_a)
+  const void* Fny;            // FP32: [nevals][3][N][N] Nyquist planes of F_g
+  void* rho;                  // FP32: [nevals][Nrho][Mu][3][N][N] plane transforms
   int Mu;
   int Nrho;
 };
@@ -80,6 +87,7 @@ struct VhsGainArgs {
   double2* GM;                // out [nevals][n]
   int Mu;
   int Nrho;
+  int pch;                    // radial points staged per shared-memory chunk
 };
 
 struct VhsEpilogueArgs {
@@ -238,6 +246,10 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
       g.x = (float)(Fv.x - mm.x);
       g.y = (float)(Fv.y - mm.y);
       static_cast<float2*>(a.Fg)[gbase + j] = g;
+      float2* ny = a.Fny + (size_t)e * 3 * N * N;
+      if (lx == N / 2) ny[ly * N + lz] = g;
+      if (ly == N / 2) ny[N * N + lx * N + lz] = g;
+      if (lz == N / 2) ny[2 * N * N + lx * N + ly] = g;
     } else {
       static_cast<double2*>(a.Fg)[gbase + j] = Fv;
     }
@@ -319,63 +331,90 @@ __global__ void vhs_tables_kernel(VhsTablesArgs a) {
 
 // ---------------------------------------------------------------------------
 // Maxwellian gain: Ghat_M(l) = sum_p W_p b1_p(l) sum_q m_q hx(lx) hy(ly) hz(lz)
-// grid (N [lx], nevals), block N*N threads (ly, lz) -- one point each.
+// grid (N [lx], nevals), block N*NYB threads: thread (ly0 = t/N, lz = t%N)
+// owns the points (lx, ly0 + NYB*k, lz), k < KY.  The 1-D factors of a chunk
+// of a.pch radial points are staged in shared memory at once (m_q folded into
+// hx), hx*hz is formed once per (p, q) and reused for the KY points, and the
+// b1 weights of the next p are loaded while the current one is summed.
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(256)
+struct GainGeo {
+  static constexpr int NYB = 256 / N;                 // ly rows per pass
+  static constexpr int NT = N * NYB;                  // threads
+  static constexpr int KY = (N + NYB - 1) / NYB;      // points per thread
+};
+
+template <int N>
+__global__ void __launch_bounds__(GainGeo<N>::NT)
 vhs_maxwell_gain_kernel(VhsGainArgs a) {
+  using GG = GainGeo<N>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* hyz = reinterpret_cast<double2*>(smem_raw);   // [Mu][2][N]
-  double2* hx = hyz + (size_t)a.Mu * 2 * N;              // [Mu]
+  const int Mu = a.Mu;
+  double2* hyz = reinterpret_cast<double2*>(smem_raw);   // [pch][Mu][2][N]
+  double2* hxs = hyz + (size_t)a.pch * Mu * 2 * N;       // [pch][Mu]
   const int lx = blockIdx.x, e = blockIdx.y;
-  const int t = threadIdx.x;
-  constexpr int PTS = (N * N + 255) / 256;  // points per thread
-  double2 Gs[PTS];
+  const int t = threadIdx.x, ly0 = t / N, lz = t % N;
+  const size_t nn = (size_t)N * N;
+  const double* b1 = a.b1w + (size_t)lx * nn + lz;
+  double2 Gs[GG::KY];
+  double wk[GG::KY];
 #pragma unroll
-  for (int k = 0; k < PTS; ++k) Gs[k] = make_double2(0, 0);
-  for (int p = 0; p < a.Nrho; ++p) {
-    const double2* hh = a.hh + ((size_t)e * a.Nrho + p) * a.Mu * 3 * N;
+  for (int k = 0; k < GG::KY; ++k) {
+    Gs[k] = make_double2(0, 0);
+    const int ly = ly0 + GG::NYB * k;
+    wk[k] = ly < N ? b1[(size_t)ly * N] : 0.0;  // p = 0
+  }
+  for (int pc = 0; pc < a.Nrho; pc += a.pch) {
+    const int np = min(a.pch, a.Nrho - pc);
     __syncthreads();
-    for (int i = t; i < a.Mu * 2 * N; i += blockDim.x) {
-      const int q = i / (2 * N), r = i % (2 * N);
-      hyz[i] = hh[(size_t)q * 3 * N + N + r];
+    for (int i = t; i < np * Mu * 2 * N; i += GG::NT) {
+      const int pq = i / (2 * N), r = i % (2 * N);
+      const int pp = pc + pq / Mu, q = pq % Mu;
+      hyz[i] = a.hh[(((size_t)e * a.Nrho + pp) * Mu + q) * 3 * N + N + r];
     }
-    for (int i = t; i < a.Mu; i += blockDim.x) hx[i] = hh[(size_t)i * 3 * N + lx];
-    __syncthreads();
-    double wk[PTS];
-#pragma unroll
-    for (int k = 0; k < PTS; ++k) {
-      const int pt = t + k * 256;
-      wk[k] = pt < N * N
-                  ? a.b1w[(size_t)p * N * N * N + (size_t)lx * N * N + pt]
-                  : 0.0;
-    }
-    double2 acc[PTS];
-#pragma unroll
-    for (int k = 0; k < PTS; ++k) acc[k] = make_double2(0, 0);
-    for (int q = 0; q < a.Mu; ++q) {
+    for (int i = t; i < np * Mu; i += GG::NT) {
+      const int pp = pc + i / Mu, q = i % Mu;
+      const double2 h = a.hh[(((size_t)e * a.Nrho + pp) * Mu + q) * 3 * N + lx];
       const double m = (double)a.mult[q];
-      const double2 hxq = make_double2(m * hx[q].x, m * hx[q].y);
+      hxs[i] = make_double2(m * h.x, m * h.y);
+    }
+    __syncthreads();
+    for (int j = 0; j < np; ++j) {
+      const int p = pc + j;
+      double wn[GG::KY];
 #pragma unroll
-      for (int k = 0; k < PTS; ++k) {
-        const int pt = min(t + k * 256, N * N - 1);
-        const int ly = pt / N, lz = pt % N;
-        const double2 xy = cmul(hxq, hyz[(size_t)q * 2 * N + ly]);
-        const double2 xyz = cmul(xy, hyz[(size_t)q * 2 * N + N + lz]);
-        acc[k].x += xyz.x;
-        acc[k].y += xyz.y;
+      for (int k = 0; k < GG::KY; ++k) {
+        const int ly = ly0 + GG::NYB * k;
+        wn[k] = (p + 1 < a.Nrho && ly < N)
+                    ? b1[(size_t)(p + 1) * N * nn + (size_t)ly * N] : 0.0;
+      }
+      double2 acc[GG::KY];
+#pragma unroll
+      for (int k = 0; k < GG::KY; ++k) acc[k] = make_double2(0, 0);
+      const double2* hj = hyz + (size_t)j * Mu * 2 * N;
+      for (int q = 0; q < Mu; ++q) {
+        const double2 hxz = cmul(hxs[j * Mu + q], hj[q * 2 * N + N + lz]);
+#pragma unroll
+        for (int k = 0; k < GG::KY; ++k) {
+          const int ly = min(ly0 + GG::NYB * k, N - 1);
+          const double2 hy = hj[q * 2 * N + ly];
+          acc[k].x += hxz.x * hy.x - hxz.y * hy.y;
+          acc[k].y += hxz.x * hy.y + hxz.y * hy.x;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < GG::KY; ++k) {
+        Gs[k].x += wk[k] * acc[k].x;
+        Gs[k].y += wk[k] * acc[k].y;
+        wk[k] = wn[k];
       }
     }
-#pragma unroll
-    for (int k = 0; k < PTS; ++k) {
-      Gs[k].x += wk[k] * acc[k].x;
-      Gs[k].y += wk[k] * acc[k].y;
-    }
   }
+  double2* out = a.GM + (size_t)e * N * nn + (size_t)lx * nn + lz;
 #pragma unroll
-  for (int k = 0; k < PTS; ++k) {
-    const int pt = t + k * 256;
-    if (pt < N * N) a.GM[(size_t)e * N * N * N + (size_t)lx * N * N + pt] = Gs[k];
+  for (int k = 0; k < GG::KY; ++k) {
+    const int ly = ly0 + GG::NYB * k;
+    if (ly < N) out[(size_t)ly * N] = Gs[k];
   }
 }
 
@@ -548,16 +587,45 @@ vhs_terms_kernel(VhsTermsArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Terms, FP32 Maxwellian-split path: one cluster per (eval, p), S_p in
-// registers, software-pipelined over the 2*Mu inverse transforms:
+// Terms, FP32 Maxwellian-split path with packed real transforms.
+//
+// g = f - M is real, so F_g is Hermitian.  With the phase a(l) = kappa.l the
+// reference forms t3 = IFFT(cos a F_g) and t4 = IFFT(sin a F_g); off the
+// Nyquist planes (any l_a = -N/2) cos a F_g is Hermitian and sin a F_g
+// anti-Hermitian, so t3 = C and t4 = i s with C, s real, and ONE complex
+// inverse transform z = IFFT((cos a + sin a) F_g) = C + i s yields both.
+// On the Nyquist planes the mirror l' of l is not -l, and each product splits
+// exactly into a Hermitian and an anti-Hermitian part.  With
+// a(l') = -a(l) - theta_S(l), theta_S = N sum_{a in S} kappa_a over the set S
+// of Nyquist axes of l, f_S = exp(i theta_S) and E = exp(i a):
+//   main  multiplier m  = Re(E (1 + f_S)(1 - i)/2)  -> z  = C + i s
+//   plane multiplier mc = Re(E (1 - f_S)(1 - i)/2)  -> zc = s_R + i c_I
+// so that t3 = C + i c_I and t4 = i s + s_R exactly.  mc vanishes off the
+// Nyquist planes, so zc is a sum of three plane-extruded 2-D transforms
+//   zc(x,y,z) = (-1)^x rx(y,z) + (-1)^y ry(x,z) + (-1)^z rz(x,y)
+// (vhs_nyq_planes_kernel).  With the Maxwellian parts t3_M = (u_M + v_M)/2,
+// t4_M = (u_M - v_M)/(2i) (u_M, v_M: separable products of the FP64 1-D
+// tables), the g-dependent real part of t3^2 + t4^2 is
+//   C (A.x + C) + s (B.x - s) + s_R (B.y + s_R) - c_I (A.y + c_I),
+//   A = u_M + v_M, B = u_M - v_M
+// (only Re of the gain survives: b1 is real and even, and the epilogue takes
+// the real part of the final inverse transform).
+//
+// Two radial points p0, p1 share one cluster: their real sums S_p0, S_p1 are
+// packed as S = S_p0 + i S_p1 and forward-transformed together; since both
+// spectra are Hermitian, Re IFFT((b1_p0 - i b1_p1) FFT(S)) =
+// IFFT(b1_p0 FFT(S_p0) + b1_p1 FFT(S_p1)), so the epilogue sums the packed
+// spectra H = (b1_p0 - i b1_p1) FFT(S) unchanged.
+//
+// Pipeline per transform k (term (p, q) = (p0 + k / Mu, k % Mu)):
 //   y-pass(k) -> exchange(k) into receive buffer k%2 -> arrive
 //   -> [load F_g slab, z-pass(k+1)]  (overlaps the exchange latency)
-//   -> wait -> x-pass(k) + combine into S_p
+//   -> wait -> x-pass(k) + combine into S
 // Two receive buffers make one cluster barrier per transform sufficient: a
 // CTA stores into buffer k%2 of a peer only after the barrier of transform
 // k-1, which that peer joined after reading its buffer k%2 for transform k-2.
 // The multiplicity m_q is folded into the tables as sqrt(m_q) (on the x-phase
-// and on u_x, v_x), so S_p += X (2 X_M + X) carries it.
+// and on u_x, v_x), and so into zc.
 // ---------------------------------------------------------------------------
 // Asynchronous copy of this CTA's F_g slab (global, dense) into the padded
 // X-slab A: 8-byte cp.async per complex element, one commit group.
@@ -578,19 +646,43 @@ __device__ __forceinline__ void fp32_issue_slab_copy(float2* A,
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n"
+               :: "r"(dst), "l"(src) : "memory");
+}
 
+// (1 + f)(1 - i)/2 and (1 - f)(1 - i)/2
+__device__ __forceinline__ float2 nyq_main(float2 f) {
+  const float ux = 1.f + f.x, uy = f.y;
+  return make_float2(0.5f * (ux + uy), 0.5f * (uy - ux));
+}
+__device__ __forceinline__ float2 nyq_plane(float2 f) {
+  const float ux = 1.f - f.x, uy = -f.y;
+  return make_float2(0.5f * (ux + uy), 0.5f * (uy - ux));
+}
+
+// z-pass of the packed transform: multiply this thread's z-pencil
+// (lx, ly) by m(l) and inverse-transform it along z.
+// tb: [ph x,y,z (3N) | u (3N) | v (3N) | nu x,y,z (3)]
 template <int N, int C>
-__device__ __forceinline__ void fp32_zpass(float2* A, const float2* tb, int s,
-                                           int t, unsigned rank) {
+__device__ __forceinline__ void fp32_zpass(float2* A, const float2* tb, int t,
+                                           unsigned rank) {
   using G = Geo<N, C>;
   const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
   const float2 bxy = cmul(tb[lx], tb[N + ly]);
+  const float2* nu = tb + 9 * N;
+  float2 fxy = make_float2(1.f, 0.f);
+  if (lx == N / 2) fxy = nu[0];
+  if (ly == N / 2) fxy = cmul(fxy, nu[1]);
+  const float2 gb = cmul(nyq_main(fxy), bxy);
+  const float2 gbz = cmul(nyq_main(cmul(fxy, nu[2])), bxy);
   const int base = pl * G::PLANE + ly * G::ROW;
   float2 v[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
-    const float2 ph3 = cmul(bxy, tb[2 * N + k]);
-    const float m = s == 0 ? ph3.x : ph3.y;
+    const float2 bz = tb[2 * N + k];
+    const float2 g = (k == N / 2) ? gbz : gb;
+    const float m = g.x * bz.x - g.y * bz.y;
     const float2 f = A[base + k];
     v[k] = make_float2(f.x * m, f.y * m);
   }
@@ -599,30 +691,155 @@ __device__ __forceinline__ void fp32_zpass(float2* A, const float2* tb, int s,
   for (int k = 0; k < N; ++k) A[base + k] = v[k];
 }
 
+// Plane transforms rx, ry, rz of two directions q of one (eval e, radial p).
+// grid (ceil(Mu/2), Nrho, nevals), block 6N: thread t = half*3N + plane*N +
+// row.  The three Nyquist planes of F_g (written compactly by the prologue)
+// are staged in shared memory with coalesced loads.
+template <int N>
+__global__ void __launch_bounds__(6 * N)
+vhs_nyq_planes_kernel(VhsTermsArgs a) {
+  constexpr int ROW = N + 1, H = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* Fp = reinterpret_cast<float2*>(smem_raw);  // [3][N][ROW]
+  float2* pl = Fp + 3 * N * ROW;                      // [2][3][N][ROW]
+  float2* tph = pl + 2 * 3 * N * ROW;                 // [2][3N + 3]
+  const int q0 = 2 * blockIdx.x, p = blockIdx.y, e = blockIdx.z;
+  const int t = threadIdx.x, half = t / (3 * N), tt = t % (3 * N);
+  const int P = tt / N, i = tt % N;
+  const int Mu = a.Mu;
+  const float2* Fny = static_cast<const float2*>(a.Fny) + (size_t)e * 3 * N * N;
+  for (int j = t; j < 3 * N * N; j += 6 * N)
+    Fp[(j / N) * ROW + j % N] = Fny[j];
+  for (int j = t; j < 2 * (3 * N + 3); j += 6 * N) {
+    const int hq = j / (3 * N + 3), r = j % (3 * N + 3), q = q0 + hq;
+    if (q < Mu) {
+      const size_t pq = (size_t)p * Mu + q;
+      tph[j] = r < 3 * N ? static_cast<const float2*>(a.ph)[pq * 3 * N + r]
+                         : static_cast<const float2*>(a.nyq)[pq * 3 + r - 3 * N];
+    }
+  }
+  __syncthreads();
+  const int q = q0 + half;
+  float2* pl_h = pl + half * 3 * N * ROW;
+  const float2* tb = tph + half * (3 * N + 3);
+  float2 v[N];
+  if (q < Mu) {
+    const float2 nx = tb[3 * N], ny = tb[3 * N + 1], nz = tb[3 * N + 2];
+    // rows: P=0 (lx=H, ly=i, lz=k); P=1 (lx=i, ly=H, lz=k), lx=H excluded;
+    //       P=2 (lx=i, ly=k, lz=H), lx=H and ly=H excluded.
+    // E = rowc * tk[k]; f = f_row off k=H, f_rowH at k=H.
+    float2 rowc, f_row, f_rowH;
+    const float2* tk;
+    if (P == 0) {
+      rowc = cmul(tb[H], tb[N + i]);
+      f_row = (i == H) ? cmul(nx, ny) : nx;
+      f_rowH = cmul(f_row, nz);
+      tk = tb + 2 * N;
+    } else if (P == 1) {
+      rowc = cmul(tb[i], tb[N + H]);
+      f_row = ny;
+      f_rowH = cmul(ny, nz);
+      tk = tb + 2 * N;
+    } else {
+      rowc = cmul(tb[i], tb[2 * N + H]);
+      f_row = nz;
+      f_rowH = nz;
+      tk = tb + N;
+    }
+    if (P >= 1 && i == H) rowc = make_float2(0.f, 0.f);
+    const float2 g = cmul(nyq_plane(f_row), rowc);
+    const float2 gH = (P == 2) ? make_float2(0.f, 0.f)
+                               : cmul(nyq_plane(f_rowH), rowc);
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const float2 gk = (k == H) ? gH : g;
+      const float2 b = tk[k];
+      const float m = gk.x * b.x - gk.y * b.y;
+      const float2 F = Fp[(P * N + i) * ROW + k];
+      v[k] = make_float2(F.x * m, F.y * m);
+    }
+    fft<float, N, +1>(v);
+#pragma unroll
+    for (int k = 0; k < N; ++k) pl_h[(P * N + i) * ROW + k] = v[k];
+  }
+  __syncthreads();
+  if (q < Mu) {
+    // columns: transform pl[P][.][i] along the rows
+#pragma unroll
+    for (int r = 0; r < N; ++r) v[r] = pl_h[(P * N + r) * ROW + i];
+    fft<float, N, +1>(v);
+    float2* rho = static_cast<float2*>(a.rho) +
+                  ((((size_t)e * a.Nrho + p) * Mu + q) * 3 + P) * N * N;
+#pragma unroll
+    for (int r = 0; r < N; ++r) rho[(size_t)r * N + i] = v[r];
+  }
+}
+
+// Stage this CTA's share of the plane transforms of one term into smem:
+// rY = ry[x][z] (all), rX = rx[y][z] (own y), rZ = rz[x][y] (own y) as [x][yl].
+template <int N, int C>
+__device__ __forceinline__ void fp32_issue_rho_copy(float2* rbuf,
+                                                    const float2* rho, int t,
+                                                    unsigned rank) {
+  using G = Geo<N, C>;
+  constexpr int P = G::P;
+  const uint32_t s0 = smem_u32(rbuf);
+  // ry: N*N complex = N*N/2 chunks of 16 B
+  for (int c = t; c < N * N / 2; c += G::NT)
+    cp_async16(s0 + 16u * c, rho + N * N + 2 * c);
+  // rx rows y in [rank P, rank P + P): P*N complex
+  const uint32_t sx = s0 + 8u * N * N;
+  const float2* rx = rho + (size_t)rank * P * N;
+  for (int c = t; c < P * N / 2; c += G::NT) cp_async16(sx + 16u * c, rx + 2 * c);
+  // rz[x][rank P .. rank P + P): N segments of P complex
+  const uint32_t szz = sx + 8u * P * N;
+  const float2* rz = rho + 2 * N * N + rank * P;
+  for (int c = t; c < N * P / 2; c += G::NT) {
+    const int x = c / (P / 2), j = c % (P / 2);
+    cp_async16(szz + 16u * c, rz + (size_t)x * N + 2 * j);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
 template <int N, int C>
 __global__ void __launch_bounds__(Geo<N, C>::NT, 1)
 vhs_terms_fp32_kernel(VhsTermsArgs a) {
   using G = Geo<N, C>;
   using T = float2;
+  constexpr int TB = 9 * N + 4;  // ring slot: ph | u | v | nu (+1 pad)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* A = reinterpret_cast<T*>(smem_raw);
   T* R0 = A + G::SLAB;          // receive buffer b at R0 + b*SLAB
-  // tables of two terms (ring): phase x,y,z | u x,y,z | v x,y,z
-  T* tab = R0 + 2 * G::SLAB;    // [2][9N]
+  T* tab = R0 + 2 * G::SLAB;    // [2][TB]
+  T* rbuf = tab + 2 * TB;       // ry [N*N] | rx [P*N] | rz [N*P]
+  const T* rY = rbuf;
+  const T* rX = rbuf + N * N;
+  const T* rZ = rX + G::P * N;
   const int t = threadIdx.x;
   const unsigned rank = cluster_rank();
-  const int p = blockIdx.y, e = blockIdx.z;
+  const int pair = blockIdx.y, e = blockIdx.z;
   const int Mu = a.Mu;
+  const int p0 = 2 * pair;
+  const int npass = (p0 + 1 < a.Nrho ? 2 : 1) * Mu;
   const T* Fg = static_cast<const T*>(a.Fg) + (size_t)e * G::n +
                 (size_t)rank * G::P * N * N;
-  const T* ph = static_cast<const T*>(a.ph) + (size_t)p * Mu * 3 * N;
-  const T* uvg = static_cast<const T*>(a.uv) +
-                 ((size_t)e * a.Nrho + p) * Mu * 6 * N;
-  auto load_tables = [&](int q) {
-    T* dst = tab + (q & 1) * 9 * N;
-    for (int i = t; i < 3 * N; i += G::NT) dst[i] = ph[(size_t)q * 3 * N + i];
-    for (int i = t; i < 6 * N; i += G::NT)
-      dst[3 * N + i] = uvg[(size_t)q * 6 * N + i];
+  const T* phb = static_cast<const T*>(a.ph);
+  const T* uvb = static_cast<const T*>(a.uv);
+  const T* nyb = static_cast<const T*>(a.nyq);
+  const T* rhob = static_cast<const T*>(a.rho);
+  // term k -> (p, q) = (p0 + k / Mu, k % Mu); tables index p*Mu + q
+  auto term = [&](int k) { return (p0 + k / Mu) * Mu + k % Mu; };
+  auto load_tables = [&](int k) {
+    T* dst = tab + (k & 1) * TB;
+    const int pq = term(k);
+    const T* ph = phb + (size_t)pq * 3 * N;
+    const T* uv = uvb + ((size_t)e * a.Nrho * Mu + pq) * 6 * N;
+    for (int i = t; i < 3 * N; i += G::NT) dst[i] = ph[i];
+    for (int i = t; i < 6 * N; i += G::NT) dst[3 * N + i] = uv[i];
+    if (t < 3) dst[9 * N + t] = nyb[(size_t)pq * 3 + t];
+  };
+  auto rho_of = [&](int k) {
+    return rhob + ((size_t)e * a.Nrho * Mu + term(k)) * 3 * N * N;
   };
   load_tables(0);
   uint32_t rbase[C];
@@ -630,6 +847,7 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
   for (int c = 0; c < C; ++c) rbase[c] = mapa_u32(smem_u32(R0), (uint32_t)c);
 
   const int yl = t / N, zz = t % N, yy = rank * G::P + yl;
+  const float sy = (yy & 1) ? -1.f : 1.f, sz = (zz & 1) ? -1.f : 1.f;
   T S[N];
 #pragma unroll
   for (int x = 0; x < N; ++x) S[x] = make_float2(0.f, 0.f);
@@ -637,23 +855,20 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
   fp32_issue_slab_copy<N, C>(A, Fg, t);
   cp_async_wait_all();
   __syncthreads();
-  fp32_zpass<N, C>(A, tab, 0, t, rank);
+  fp32_zpass<N, C>(A, tab, t, rank);
   __syncthreads();
-  const int npass = 2 * Mu;
 #pragma unroll 1
   for (int k = 0; k < npass; ++k) {
-    const int q = k >> 1, s = k & 1;
     T v[N];
     {
       const int base = (t / N) * G::PLANE + (t % N);
 #pragma unroll
       for (int y = 0; y < N; ++y) v[y] = A[base + y * G::ROW];
     }
-    __syncthreads();  // every thread has read A: refill it asynchronously
+    __syncthreads();  // every thread has read A and used rbuf: refill both
+    fp32_issue_rho_copy<N, C>(rbuf, rho_of(k), t, rank);
     if (k + 1 < npass) {
-      // term (k+1)/2 starts: its tables go to the ring slot last read by
-      // term (k-1)/2, whose readers all passed the barrier above
-      if (((k + 1) & 1) == 0) load_tables((k + 1) >> 1);
+      load_tables(k + 1);
       fp32_issue_slab_copy<N, C>(A, Fg, t);
     }
     fft<float, N, +1>(v);
@@ -668,11 +883,10 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
                      v[c * G::P + j]);
     }
     cluster_arrive();
+    cp_async_wait_all();
+    __syncthreads();
     if (k + 1 < npass) {
-      cp_async_wait_all();
-      __syncthreads();
-      fp32_zpass<N, C>(A, tab + (((k + 1) >> 1) & 1) * 9 * N, (k + 1) & 1,
-                       t, rank);
+      fp32_zpass<N, C>(A, tab + ((k + 1) & 1) * TB, t, rank);
       __syncthreads();
     }
     cluster_wait();
@@ -683,26 +897,32 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
       for (int x = 0; x < N; ++x) v[x] = Rk[base + x * G::ROW];
     }
     fft<float, N, +1>(v);
-    const T* tb = tab + (q & 1) * 9 * N;
+    const T* tb = tab + (k & 1) * TB;
     const T* ut = tb + 3 * N;
     const T* vt = tb + 6 * N;
     const T uyz = cmul(ut[N + yy], ut[2 * N + zz]);
     const T vyz = cmul(vt[N + yy], vt[2 * N + zz]);
+    const T rx = rX[yl * N + zz];
+    const bool hi = k >= Mu;
 #pragma unroll
     for (int x = 0; x < N; ++x) {
       const T um = cmul(ut[x], uyz), vm = cmul(vt[x], vyz);
-      T W;
-      if (s == 0) { W.x = um.x + vm.x; W.y = um.y + vm.y; }
-      else { W.x = um.y - vm.y; W.y = vm.x - um.x; }
-      W.x += v[x].x;
-      W.y += v[x].y;
-      const T h = cmul(v[x], W);
-      S[x].x += h.x;
-      S[x].y += h.y;
+      const float Ax = um.x + vm.x, Ay = um.y + vm.y;
+      const float Bx = um.x - vm.x, By = um.y - vm.y;
+      const T ry = rY[x * N + zz], rz = rZ[x * G::P + yl];
+      const float xs = (x & 1) ? -1.f : 1.f;
+      const float sR = xs * rx.x + sy * ry.x + sz * rz.x;
+      const float cI = xs * rx.y + sy * ry.y + sz * rz.y;
+      const float Cm = v[x].x, sm = v[x].y;
+      const float h = Cm * (Ax + Cm) + sm * (Bx - sm) + sR * (By + sR) -
+                      cI * (Ay + cI);
+      if (hi) S[x].y += h;
+      else S[x].x += h;
     }
   }
 
-  // forward FFT of S_p: x-pass, exchange into X-slabs, y-pass, z-pass
+  // forward FFT of S = S_p0 + i S_p1: x-pass, exchange into X-slabs,
+  // y-pass, z-pass
   fft<float, N, -1>(S);
   {
     const uint32_t a0 = smem_u32(A);
@@ -727,14 +947,15 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
   __syncthreads();
   slab_row_pass<float, N, C, -1>(A, t);
   __syncthreads();
-  const float* b1w = static_cast<const float*>(a.b1w) + (size_t)p * G::n +
-                     (size_t)rank * G::P * N * N;
-  T* H = static_cast<T*>(a.H) + ((size_t)e * a.Nrho + p) * G::n +
-         (size_t)rank * G::P * N * N;
+  const size_t off = (size_t)rank * G::P * N * N;
+  const float* b1a = static_cast<const float*>(a.b1w) + (size_t)p0 * G::n + off;
+  const float* b1b = (p0 + 1 < a.Nrho) ? b1a + G::n : nullptr;
+  const int npairs = (a.Nrho + 1) / 2;
+  T* H = static_cast<T*>(a.H) + ((size_t)e * npairs + pair) * G::n + off;
   for (int j = t; j < G::P * N * N; j += G::NT) {
-    T hv = A[slab_index<N, C>(j)];
-    const float w = b1w[j];
-    H[j] = make_float2(hv.x * w, hv.y * w);
+    const T hv = A[slab_index<N, C>(j)];
+    const float w0 = b1a[j], w1 = b1b ? b1b[j] : 0.f;
+    H[j] = make_float2(hv.x * w0 + hv.y * w1, hv.y * w0 - hv.x * w1);
   }
 }
 
