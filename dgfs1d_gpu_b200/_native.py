@@ -68,6 +68,13 @@ class DgfsError(RuntimeError):
 _lib = None
 
 # (name, restype, argtypes) of every exported entry point
+class FnoDesc(ctypes.Structure):
+    """Mirrors dgfs_fno_desc."""
+    _fields_ = [('N', ctypes.c_int32), ('modes', ctypes.c_int32),
+                ('max_batch', ctypes.c_int32), ('L', ctypes.c_double),
+                ('q_scale', ctypes.c_double)]
+
+
 _SIGNATURES = [
     ('dgfs_version', ctypes.c_char_p, []),
     ('dgfs_last_error_string', ctypes.c_char_p, []),
@@ -86,6 +93,22 @@ _SIGNATURES = [
     ('dgfs_vhs_variants', ctypes.c_int,
      [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
     ('dgfs_vhs_set_variant', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ('dgfs_fno_create', ctypes.c_int,
+     [ctypes.POINTER(FnoDesc), ctypes.POINTER(ctypes.c_void_p)]),
+    ('dgfs_fno_destroy', ctypes.c_int, [ctypes.c_void_p]),
+    ('dgfs_fno_num_params', ctypes.c_int64, [ctypes.c_void_p]),
+    ('dgfs_fno_set_params', ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ('dgfs_fno_get_params', ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ('dgfs_fno_get_grads', ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ('dgfs_fno_eval', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
+    ('dgfs_fno_train_step', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_float, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
+    ('dgfs_fno_last_loss', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_vhs_destroy', ctypes.c_int, [ctypes.c_void_p]),
     ('dgfs_vhs_profile', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_vhs_stage_ms', ctypes.c_int,

@@ -1393,3 +1393,410 @@ extern "C" int dgfs_vhs_set_variant(dgfs_vhs_handle h, int32_t cluster) {
   if (cluster == 0) { h->c32 = 0; return DGFS_OK; }
   return fail(DGFS_ERR_INVALID, "cluster size not a variant for this N");
 }
+
+// ---------------------------------------------------------------------------
+// FNO surrogate of Q(f,f)
+// ---------------------------------------------------------------------------
+#include "fno_kernels.cuh"
+
+struct dgfs_fno_s {
+  int N = 0, K = 0, maxB = 0;
+  long n = 0;
+  double cw = 0, sQ = 1, Ginv[25] = {};
+  fno::Layout L{};
+  double* c0 = nullptr;
+  float* p32 = nullptr;              // master parameters
+  __nv_bfloat16* p16 = nullptr;      // BF16 copy read by the kernels
+  float* grad = nullptr;
+  float* am = nullptr;
+  float* av = nullptr;
+  float2 *tF = nullptr, *tG = nullptr, *tFs = nullptr, *tGs = nullptr;
+  __nv_bfloat16* x0 = nullptr;
+  __nv_bfloat16* v[5] = {};
+  __nv_bfloat16* y[4] = {};
+  float2* Vh[4] = {};
+  float2 *Uh = nullptr, *T1 = nullptr, *T2 = nullptr;
+  float* U = nullptr;
+  float* out = nullptr;
+  double* qs = nullptr;
+  float *dout = nullptr, *dz = nullptr, *aw = nullptr, *dvA = nullptr,
+        *dvB = nullptr, *dy = nullptr, *part = nullptr;
+  float2 *gUh = nullptr, *gVh = nullptr;
+  double* loss = nullptr;
+  std::vector<void*> owned;
+};
+
+static constexpr int kFnoWgradGrid = 296;
+
+static void fno_free(dgfs_fno_s* h) {
+  for (void* p : h->owned)
+    if (p) cudaFree(p);
+  delete h;
+}
+
+template <typename T>
+static cudaError_t fno_alloc(dgfs_fno_s* h, T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e == cudaSuccess) h->owned.push_back((void*)*p);
+  return e;
+}
+
+extern "C" int dgfs_fno_create(const dgfs_fno_desc* d, dgfs_fno_handle* out) {
+  if (!d || !out) return fail(DGFS_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (d->N != 16 && d->N != 32)
+    return fail(DGFS_ERR_UNSUPPORTED, "FNO velocity grid must be N=16 or N=32");
+  if ((d->N == 16 && d->modes != 8) || (d->N == 32 && d->modes != 12))
+    return fail(DGFS_ERR_UNSUPPORTED,
+                "FNO modes per axis: 8 at N=16, 12 at N=32 are compiled in");
+  if (d->max_batch < 1 || d->max_batch > 32)
+    return fail(DGFS_ERR_INVALID, "FNO max_batch must be in [1, 32]");
+  if (!(d->L > 0) || !(d->q_scale > 0))
+    return fail(DGFS_ERR_INVALID, "FNO needs L > 0 and q_scale > 0");
+  auto* h = new dgfs_fno_s();
+  h->N = d->N; h->K = d->modes; h->maxB = d->max_batch;
+  h->n = (long)h->N * h->N * h->N;
+  h->sQ = d->q_scale;
+  h->L.init(h->K);
+  const int N = h->N, K = h->K;
+  const long n = h->n, B = h->maxB;
+  std::vector<double> c0(N);
+  for (int i = 0; i < N; ++i) c0[i] = -d->L + d->L / N + i * (2.0 * d->L / N);
+  h->cw = std::pow(2.0 * d->L / N, 3);
+  // Gram matrix of (1, c, |c|^2) under cw, inverted in long double
+  {
+    long double G[5][10] = {};
+    for (int ix = 0; ix < N; ++ix)
+      for (int iy = 0; iy < N; ++iy)
+        for (int iz = 0; iz < N; ++iz) {
+          const long double cx = c0[ix], cy = c0[iy], cz = c0[iz];
+          const long double ph[5] = {1, cx, cy, cz, cx * cx + cy * cy + cz * cz};
+          for (int r = 0; r < 5; ++r)
+            for (int s = 0; s < 5; ++s) G[r][s] += ph[r] * ph[s] * h->cw;
+        }
+    for (int r = 0; r < 5; ++r) G[r][5 + r] = 1;
+    for (int c = 0; c < 5; ++c) {
+      int pv = c;
+      for (int r = c + 1; r < 5; ++r)
+        if (fabsl(G[r][c]) > fabsl(G[pv][c])) pv = r;
+      for (int s = 0; s < 10; ++s) std::swap(G[c][s], G[pv][s]);
+      const long double inv = 1.0L / G[c][c];
+      for (int s = 0; s < 10; ++s) G[c][s] *= inv;
+      for (int r = 0; r < 5; ++r)
+        if (r != c) {
+          const long double f = G[r][c];
+          for (int s = 0; s < 10; ++s) G[r][s] -= f * G[c][s];
+        }
+    }
+    for (int r = 0; r < 5; ++r)
+      for (int s = 0; s < 5; ++s) h->Ginv[r * 5 + s] = (double)G[r][5 + s];
+  }
+  // DFT tables: modes k = 0..K/2-1, -K/2..-1
+  std::vector<float2> tF(K * N), tG(N * K), tFs(K * N), tGs(N * K);
+  for (int kk = 0; kk < K; ++kk) {
+    const int k = kk < K / 2 ? kk : kk - K;
+    for (int x = 0; x < N; ++x) {
+      const double a = -2.0 * M_PI * (double)k * x / N;
+      const double c = std::cos(a), s = std::sin(a);
+      tF[kk * N + x] = make_float2((float)c, (float)s);
+      tFs[kk * N + x] = make_float2((float)(c / N), (float)(s / N));
+      tG[x * K + kk] = make_float2((float)(c / N), (float)(-s / N));
+      tGs[x * K + kk] = make_float2((float)c, (float)(-s));
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  auto A = [&](auto** p, size_t cnt) {
+    if (e == cudaSuccess) e = fno_alloc(h, p, cnt);
+  };
+  A(&h->c0, N);
+  A(&h->p32, h->L.total); A(&h->p16, h->L.total); A(&h->grad, h->L.total);
+  A(&h->am, h->L.total); A(&h->av, h->L.total);
+  A(&h->tF, K * N); A(&h->tG, K * N); A(&h->tFs, K * N); A(&h->tGs, K * N);
+  A(&h->x0, B * n * fno::CIN);
+  for (int l = 0; l < 5; ++l) A(&h->v[l], B * n * fno::WD);
+  for (int l = 0; l < 4; ++l) A(&h->y[l], B * n * fno::WD);
+  const long nm = (long)K * K * K;
+  for (int l = 0; l < 4; ++l) A(&h->Vh[l], B * nm * fno::WD);
+  A(&h->Uh, B * nm * fno::WD);
+  A(&h->gUh, B * nm * fno::WD);
+  A(&h->gVh, B * nm * fno::WD);
+  A(&h->T1, B * K * N * N * fno::WD);
+  A(&h->T2, B * K * K * N * fno::WD);
+  A(&h->U, B * n * fno::WD);
+  A(&h->out, B * n);
+  A(&h->qs, B);
+  A(&h->dout, B * n);
+  A(&h->dz, B * n * fno::PJ);
+  A(&h->aw, B * n * fno::PJ);
+  A(&h->dvA, B * n * fno::WD);
+  A(&h->dvB, B * n * fno::WD);
+  A(&h->dy, B * n * fno::WD);
+  A(&h->part, (size_t)kFnoWgradGrid * fno::WD * fno::PJ);
+  A(&h->loss, B);
+  if (e == cudaSuccess) e = cudaMemcpy(h->c0, c0.data(), N * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(h->tF, tF.data(), K * N * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(h->tG, tG.data(), K * N * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(h->tFs, tFs.data(), K * N * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(h->tGs, tGs.data(), K * N * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(h->p32, 0, h->L.total * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(h->p16, 0, h->L.total * sizeof(__nv_bfloat16));
+  if (e == cudaSuccess) e = cudaMemset(h->am, 0, h->L.total * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(h->av, 0, h->L.total * sizeof(float));
+  if (e != cudaSuccess) {
+    fno_free(h);
+    return fail(DGFS_ERR_CUDA, std::string("FNO allocation: ") + cudaGetErrorString(e));
+  }
+  *out = h;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_fno_destroy(dgfs_fno_handle h) {
+  if (h) fno_free(h);
+  return DGFS_OK;
+}
+
+extern "C" int64_t dgfs_fno_num_params(dgfs_fno_handle h) {
+  return h ? (int64_t)h->L.total : 0;
+}
+
+extern "C" int dgfs_fno_set_params(dgfs_fno_handle h, const float* host) {
+  if (!h || !host) return fail(DGFS_ERR_INVALID, "null argument");
+  DGFS_CUDA(cudaMemcpy(h->p32, host, h->L.total * sizeof(float), cudaMemcpyHostToDevice));
+  fno::fno_to_bf16_kernel<<<(unsigned)((h->L.total + 255) / 256), 256>>>(h->p32, h->p16, h->L.total);
+  DGFS_CUDA(cudaGetLastError());
+  DGFS_CUDA(cudaMemset(h->am, 0, h->L.total * sizeof(float)));
+  DGFS_CUDA(cudaMemset(h->av, 0, h->L.total * sizeof(float)));
+  DGFS_CUDA(cudaDeviceSynchronize());
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_fno_get_params(dgfs_fno_handle h, float* host) {
+  if (!h || !host) return fail(DGFS_ERR_INVALID, "null argument");
+  DGFS_CUDA(cudaDeviceSynchronize());
+  DGFS_CUDA(cudaMemcpy(host, h->p32, h->L.total * sizeof(float), cudaMemcpyDeviceToHost));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_fno_get_grads(dgfs_fno_handle h, float* host) {
+  if (!h || !host) return fail(DGFS_ERR_INVALID, "null argument");
+  DGFS_CUDA(cudaDeviceSynchronize());
+  DGFS_CUDA(cudaMemcpy(host, h->grad, h->L.total * sizeof(float), cudaMemcpyDeviceToHost));
+  return DGFS_OK;
+}
+
+template <int LIN, int LOUT, int IN, int OUT>
+static int fno_dft(const void* in, void* out, const float2* table, long outer,
+                   int inner, cudaStream_t st) {
+  const long tot = outer * inner;
+  fno::fno_dft_kernel<LIN, LOUT, IN, OUT>
+      <<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, out, table, outer, inner);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+// forward DFT of a real field [B][n][WD] (IN: 0 BF16, 1 FP32) into [B][K^3][WD]
+template <int N, int K, int IN>
+static int fno_dft3(dgfs_fno_s* h, const void* in, const float2* tab, float2* out,
+                    int B, cudaStream_t st) {
+  constexpr int WD = fno::WD;
+  int rc;
+  if ((rc = fno_dft<N, K, IN, 0>(in, h->T1, tab, B, N * N * WD, st))) return rc;
+  if ((rc = fno_dft<N, K, 2, 0>(h->T1, h->T2, tab, (long)B * K, N * WD, st))) return rc;
+  return fno_dft<N, K, 2, 0>(h->T2, out, tab, (long)B * K * K, WD, st);
+}
+
+// expand [B][K^3][WD] complex to the real part on the grid (OUT: 1 store, 2 add)
+template <int N, int K, int OUT>
+static int fno_idft3(dgfs_fno_s* h, const float2* in, const float2* tab, float* out,
+                     int B, cudaStream_t st) {
+  constexpr int WD = fno::WD;
+  int rc;
+  if ((rc = fno_dft<K, N, 2, 0>(in, h->T2, tab, (long)B * K * K, WD, st))) return rc;
+  if ((rc = fno_dft<K, N, 2, 0>(h->T2, h->T1, tab, (long)B * K, N * WD, st))) return rc;
+  return fno_dft<K, N, 2, OUT>(h->T1, out, tab, B, N * N * WD, st);
+}
+
+template <int N, int K>
+static int fno_forward(dgfs_fno_s* h, const void* f, int f_double,
+                       const int32_t* src_slots, int src_base, int B,
+                       cudaStream_t st) {
+  using namespace fno;
+  const long R = (long)B * h->n;
+  const long nm = (long)K * K * K;
+  int rc;
+  FeatArgs fa{};
+  fa.f = f; fa.f_double = f_double; fa.src_slots = src_slots; fa.src_base = src_base;
+  fa.c0 = h->c0; fa.cw = h->cw; fa.N = N; fa.w16 = h->p16; fa.L = h->L;
+  fa.x0 = h->x0; fa.v0 = h->v[0]; fa.qs = h->qs;
+  fno_features_kernel<512><<<B, 512, 0, st>>>(fa);
+  DGFS_CUDA(cudaGetLastError());
+  for (int l = 0; l < 4; ++l) {
+    if ((rc = fno_dft3<N, K, 0>(h, h->v[l], h->tF, h->Vh[l], B, st))) return rc;
+    fno_mix_kernel<0><<<(unsigned)nm, dim3(32, 8), 0, st>>>(
+        h->Vh[l], nullptr, h->p16 + h->L.W[l], h->Uh, nullptr, B, (int)nm);
+    DGFS_CUDA(cudaGetLastError());
+    if ((rc = fno_idft3<N, K, 1>(h, h->Uh, h->tG, h->U, B, st))) return rc;
+    fno_dense_fwd_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(
+        h->v[l], h->p16, h->L.D[l], h->L.d[l], h->U, h->y[l], h->v[l + 1], R,
+        l < 3 ? 1 : 0);
+    DGFS_CUDA(cudaGetLastError());
+  }
+  fno_proj_fwd_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(
+      h->v[4], h->p16, h->L, h->out, R);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+template <int KA, int KB>
+static int fno_wgrad(dgfs_fno_s* h, const __nv_bfloat16* A, const float* Bm,
+                     long R, long off, cudaStream_t st) {
+  constexpr int RI = KA < 4 ? KA : 4;
+  constexpr int NTH = (KA / RI) * (KB / 4);
+  fno::fno_wgrad_kernel<KA, KB><<<kFnoWgradGrid, NTH, 0, st>>>(A, Bm, R, h->part);
+  DGFS_CUDA(cudaGetLastError());
+  fno::fno_reduce_kernel<<<(KA * KB + 255) / 256, 256, 0, st>>>(
+      h->part, kFnoWgradGrid, KA * KB, h->grad + off);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+template <int KB>
+static int fno_colsum(dgfs_fno_s* h, const float* Bm, long R, long off,
+                      cudaStream_t st) {
+  fno::fno_colsum_kernel<KB><<<kFnoWgradGrid, 256, 0, st>>>(Bm, R, h->part);
+  DGFS_CUDA(cudaGetLastError());
+  fno::fno_reduce_kernel<<<(KB + 255) / 256, 256, 0, st>>>(h->part, kFnoWgradGrid,
+                                                           KB, h->grad + off);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+// gradients of the loss (dout already set) w.r.t. every parameter
+template <int N, int K>
+static int fno_backward(dgfs_fno_s* h, int B, cudaStream_t st) {
+  using namespace fno;
+  const long R = (long)B * h->n;
+  const long nm = (long)K * K * K;
+  const unsigned gR = (unsigned)((R + 255) / 256);
+  int rc;
+  // projection
+  fno_proj_bwd_kernel<<<gR, 256, 0, st>>>(h->v[4], h->p16, h->L, h->dout, h->dz,
+                                          h->aw, h->dvA, R);
+  DGFS_CUDA(cudaGetLastError());
+  if ((rc = fno_wgrad<WD, PJ>(h, h->v[4], h->dz, R, h->L.Q1, st))) return rc;
+  if ((rc = fno_colsum<PJ>(h, h->dz, R, h->L.q1, st))) return rc;
+  if ((rc = fno_colsum<PJ>(h, h->aw, R, h->L.q2, st))) return rc;
+  if ((rc = fno_colsum<1>(h, h->dout, R, h->L.q2b, st))) return rc;
+  float* dv = h->dvA;     // gradient w.r.t. v_{l+1}
+  float* dvn = h->dvB;
+  for (int l = 3; l >= 0; --l) {
+    const float* dyl = dv;
+    if (l < 3) {
+      fno_gelu_bwd_kernel<<<(unsigned)((R * WD + 255) / 256), 256, 0, st>>>(
+          dv, h->y[l], h->dy, R * WD);
+      DGFS_CUDA(cudaGetLastError());
+      dyl = h->dy;
+    }
+    if ((rc = fno_wgrad<WD, WD>(h, h->v[l], dyl, R, h->L.D[l], st))) return rc;
+    if ((rc = fno_colsum<WD>(h, dyl, R, h->L.d[l], st))) return rc;
+    fno_dense_bwd_kernel<<<gR, 256, 0, st>>>(dyl, h->p16, h->L.D[l], dvn, R);
+    DGFS_CUDA(cudaGetLastError());
+    // spectral path: gUh = B^H dy, gW, gVh = gUh W^H, dv += Re(A^H gVh)
+    if ((rc = fno_dft3<N, K, 1>(h, dyl, h->tFs, h->gUh, B, st))) return rc;
+    fno_mix_kernel<2><<<(unsigned)nm, dim3(32, 8), 0, st>>>(
+        h->Vh[l], h->gUh, nullptr, nullptr, h->grad + h->L.W[l], B, (int)nm);
+    DGFS_CUDA(cudaGetLastError());
+    fno_mix_kernel<1><<<(unsigned)nm, dim3(32, 8), 0, st>>>(
+        h->gUh, nullptr, h->p16 + h->L.W[l], h->gVh, nullptr, B, (int)nm);
+    DGFS_CUDA(cudaGetLastError());
+    if ((rc = fno_idft3<N, K, 2>(h, h->gVh, h->tGs, dvn, B, st))) return rc;
+    std::swap(dv, dvn);
+  }
+  // lift
+  if ((rc = fno_wgrad<CIN, WD>(h, h->x0, dv, R, h->L.P, st))) return rc;
+  return fno_colsum<WD>(h, dv, R, h->L.p, st);
+}
+
+template <int N, int K>
+static int fno_eval_t(dgfs_fno_s* h, const void* f, int f_double, void* Q,
+                      int q_double, const int32_t* src_slots, int src_base,
+                      const int32_t* dst_slots, int dst_base, int nevals,
+                      cudaStream_t st) {
+  for (int off = 0; off < nevals; off += h->maxB) {
+    const int B = std::min(h->maxB, nevals - off);
+    int rc;
+    if ((rc = fno_forward<N, K>(h, f, f_double, src_slots ? src_slots + off : nullptr,
+                                src_base + off, B, st)))
+      return rc;
+    fno::OutArgs oa{};
+    oa.out = h->out; oa.qs = h->qs; oa.sQ = h->sQ; oa.c0 = h->c0; oa.cw = h->cw;
+    oa.N = N;
+    for (int i = 0; i < 25; ++i) oa.Ginv[i] = h->Ginv[i];
+    oa.Q = Q; oa.q_double = q_double;
+    oa.dst_slots = dst_slots ? dst_slots + off : nullptr; oa.dst_base = dst_base + off;
+    fno::fno_output_kernel<512><<<B, 512, 0, st>>>(oa);
+    DGFS_CUDA(cudaGetLastError());
+  }
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_fno_eval(dgfs_fno_handle h, const void* f, int32_t f_dtype,
+                             void* Q, int32_t q_dtype, const int32_t* src_slots,
+                             int32_t src_base, const int32_t* dst_slots,
+                             int32_t dst_base, int32_t nevals, void* stream) {
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  if (nevals < 0 || src_base < 0 || dst_base < 0)
+    return fail(DGFS_ERR_INVALID, "negative count or slot base");
+  if (nevals == 0) return DGFS_OK;
+  if (!f || !Q) return fail(DGFS_ERR_INVALID, "null f or Q");
+  if ((f_dtype != DGFS_F32 && f_dtype != DGFS_F64) ||
+      (q_dtype != DGFS_F32 && q_dtype != DGFS_F64))
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int fd = f_dtype == DGFS_F64, qd = q_dtype == DGFS_F64;
+  if (h->N == 16)
+    return fno_eval_t<16, 8>(h, f, fd, Q, qd, src_slots, src_base, dst_slots,
+                             dst_base, nevals, st);
+  return fno_eval_t<32, 12>(h, f, fd, Q, qd, src_slots, src_base, dst_slots,
+                            dst_base, nevals, st);
+}
+
+template <int N, int K>
+static int fno_train_t(dgfs_fno_s* h, const double* f, const double* Qt, int B,
+                       float lr, int step, int update, cudaStream_t st) {
+  int rc;
+  if ((rc = fno_forward<N, K>(h, f, 1, nullptr, 0, B, st))) return rc;
+  fno::fno_loss_kernel<512><<<B, 512, 0, st>>>(h->out, Qt, h->qs, h->sQ, h->n,
+                                                B, h->dout, h->loss);
+  DGFS_CUDA(cudaGetLastError());
+  if ((rc = fno_backward<N, K>(h, B, st))) return rc;
+  if (update) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = 1.f - std::pow(b1, (float)step);
+    const float bc2 = 1.f - std::pow(b2, (float)step);
+    fno::fno_adam_kernel<<<(unsigned)((h->L.total + 255) / 256), 256, 0, st>>>(
+        h->p32, h->p16, h->grad, h->am, h->av, h->L.total, lr, b1, b2, 1e-8f,
+        bc1, bc2);
+    DGFS_CUDA(cudaGetLastError());
+  }
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_fno_train_step(dgfs_fno_handle h, const double* f,
+                                   const double* Qt, int32_t B, float lr,
+                                   int32_t step, int32_t update, void* stream) {
+  if (!h || !f || !Qt) return fail(DGFS_ERR_INVALID, "null argument");
+  if (B < 1 || B > h->maxB) return fail(DGFS_ERR_CAPACITY, "batch exceeds max_batch");
+  if (update && step < 1) return fail(DGFS_ERR_INVALID, "Adam step counts from 1");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (h->N == 16) return fno_train_t<16, 8>(h, f, Qt, B, lr, step, update, st);
+  return fno_train_t<32, 12>(h, f, Qt, B, lr, step, update, st);
+}
+
+extern "C" int dgfs_fno_last_loss(dgfs_fno_handle h, double* host, int32_t B) {
+  if (!h || !host) return fail(DGFS_ERR_INVALID, "null argument");
+  if (B < 1 || B > h->maxB) return fail(DGFS_ERR_INVALID, "bad batch size");
+  DGFS_CUDA(cudaDeviceSynchronize());
+  DGFS_CUDA(cudaMemcpy(host, h->loss, B * sizeof(double), cudaMemcpyDeviceToHost));
+  return DGFS_OK;
+}

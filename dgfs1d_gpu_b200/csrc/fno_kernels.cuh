@@ -1,0 +1,626 @@
+// Fourier-neural-operator surrogate of Q(f,f): forward, backward and Adam.
+//
+// Network (width WD = 32, projection width PJ = 128, GELU):
+//   features  x0 = [f/rho, g, g r, g r^2],  g = (f - M)/(rho sigma),
+//             r = |c - u|/sqrt(T), sigma = rms((f - M)/rho) per sample
+//             (M: local Maxwellian; g r^k let the lift form the local loss
+//             frequency times g, which no convolution can)
+//   lift      v0 = x0 P + p                          (4 -> 32)
+//   layer l   y_l = v_l D_l + d_l + Re IDFT(W_l . DFT(v_l)),  l = 0..3
+//             v_{l+1} = GELU(y_l) (l < 3),  v_4 = y_3
+//   project   out = GELU(v_4 Q1 + q1) q2 + q2b       (32 -> 128 -> 1)
+//   Q = rho^2 sigma sQ out (Q is nearly linear in f - M near equilibrium, so
+//   the target Q/(rho^2 sigma sQ) and the features are O(1)), then the FP64
+//   conservation projection.
+// DFT is the truncated separable transform onto K modes per axis
+// (k = 0..K/2-1, -K/2..-1): A = F_x (x) F_y (x) F_z, F[k][x] = e^{-2 pi i k x/N};
+// IDFT applies conj(F)^T / N per axis.  W_l[m] is a 32x32 complex matrix per
+// retained mode m.  Activations are stored in BF16 (features, v_l, y_l), the
+// weights are read from a BF16 copy of the FP32 master parameters, and every
+// sum accumulates in FP32 (moments, projection and loss norms in FP64).
+//
+// Layouts: point-major, channels innermost: v[b][pt][c], pt = (x*N + y)*N + z.
+// Spectral data: [b][kx][ky][kz][c] complex FP32.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dgfs {
+namespace fno {
+
+constexpr int WD = 32;   // width
+constexpr int PJ = 128;  // projection width
+constexpr int CIN = 4;   // input features
+
+__device__ __forceinline__ float gelu(float x) {
+  return 0.5f * x * (1.f + erff(x * 0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_d(float x) {
+  return 0.5f * (1.f + erff(x * 0.70710678118654752f)) +
+         x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+__device__ __forceinline__ float bf(const __nv_bfloat16 v) {
+  return __bfloat162float(v);
+}
+__device__ __forceinline__ __nv_bfloat16 tobf(float v) {
+  return __float2bfloat16_rn(v);
+}
+
+// Parameter offsets (in floats) of the flat parameter vector.
+struct Layout {
+  int K;           // modes per axis
+  long P, p;       // lift [CIN][WD], [WD]
+  long W[4];       // spectral [K^3][WD][WD] complex (2 floats)
+  long D[4], d[4]; // dense [WD][WD], [WD]
+  long Q1, q1, q2, q2b;
+  long total;
+  __host__ __device__ void init(int K_) {
+    K = K_;
+    long o = 0;
+    P = o; o += CIN * WD;
+    p = o; o += WD;
+    for (int l = 0; l < 4; ++l) {
+      W[l] = o; o += 2L * K * K * K * WD * WD;
+      D[l] = o; o += WD * WD;
+      d[l] = o; o += WD;
+    }
+    Q1 = o; o += WD * PJ;
+    q1 = o; o += PJ;
+    q2 = o; o += PJ;
+    q2b = o; o += 1;
+    total = o;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Features + lift: one CTA per sample.  FP64 moments of f, the Maxwellian,
+// x0 = [f/rho, g, g r, g r^2] (BF16) and v0 = x0 P + p (BF16).
+// ---------------------------------------------------------------------------
+struct FeatArgs {
+  const void* f; int f_double; const int32_t* src_slots; int src_base;
+  const double* c0; double cw; int N;
+  const __nv_bfloat16* w16;  // BF16 parameters
+  Layout L;
+  __nv_bfloat16* x0;  // [B][n][CIN]
+  __nv_bfloat16* v0;  // [B][n][WD]
+  double* qs;         // out [B] rho^2 sigma (output scale without sQ)
+};
+
+template <int NT>
+__device__ __forceinline__ void block_sum5(double* s, double* red) {
+  // s[5] per thread -> totals in red[0..4] (all threads see them after return)
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    double v = s[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[8 + w * 5 + k] = v;
+  }
+  __syncthreads();
+  if (t < 5) {
+    double v = 0;
+    for (int i = 0; i < NT / 32; ++i) v += red[8 + i * 5 + t];
+    red[t] = v;
+  }
+  __syncthreads();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) fno_features_kernel(FeatArgs a) {
+  __shared__ double red[8 + 5 * (NT / 32)];
+  __shared__ float wl[CIN * WD + WD];
+  const int b = blockIdx.x, t = threadIdx.x, N = a.N;
+  const long n = (long)N * N * N;
+  const long fb = (long)(a.src_slots ? a.src_slots[b] : a.src_base + b) * n;
+  for (int i = t; i < CIN * WD + WD; i += NT) wl[i] = bf(a.w16[a.L.P + i]);
+  double s[5] = {0, 0, 0, 0, 0};
+  for (long i = t; i < n; i += NT) {
+    const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
+    const double fv = a.f_double ? static_cast<const double*>(a.f)[fb + i]
+                                 : (double)static_cast<const float*>(a.f)[fb + i];
+    const double cx = a.c0[x], cy = a.c0[y], cz = a.c0[z];
+    s[0] += fv; s[1] += fv * cx; s[2] += fv * cy; s[3] += fv * cz;
+    s[4] += fv * (cx * cx + cy * cy + cz * cz);
+  }
+  block_sum5<NT>(s, red);
+  double rho = red[0] * a.cw;
+  const double ux = red[1] * a.cw / rho, uy = red[2] * a.cw / rho,
+               uz = red[3] * a.cw / rho;
+  double T = (2.0 / 3.0) * (red[4] * a.cw / rho - (ux * ux + uy * uy + uz * uz));
+  if (!(rho > 1e-300)) rho = 1.0;
+  if (!(T > 1e-6)) T = 1.0;
+  const double amp = rho / pow(M_PI * T, 1.5), irho = 1.0 / rho;
+  // sigma = rms of (f - M)/rho over the grid
+  double s2[5] = {0, 0, 0, 0, 0};
+  for (long i = t; i < n; i += NT) {
+    const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
+    const double fv = a.f_double ? static_cast<const double*>(a.f)[fb + i]
+                                 : (double)static_cast<const float*>(a.f)[fb + i];
+    const double dx = a.c0[x] - ux, dy = a.c0[y] - uy, dz = a.c0[z] - uz;
+    const double gv = (fv - amp * exp(-(dx * dx + dy * dy + dz * dz) / T)) * irho;
+    s2[0] += gv * gv;
+  }
+  block_sum5<NT>(s2, red);
+  const double sig = fmax(sqrt(red[0] / (double)n), 1e-300), isig = 1.0 / sig;
+  if (t == 0) a.qs[b] = rho * rho * sig;
+  for (long i = t; i < n; i += NT) {
+    const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
+    const double fv = a.f_double ? static_cast<const double*>(a.f)[fb + i]
+                                 : (double)static_cast<const float*>(a.f)[fb + i];
+    const double dx = a.c0[x] - ux, dy = a.c0[y] - uy, dz = a.c0[z] - uz;
+    const double r2 = (dx * dx + dy * dy + dz * dz) / T;
+    const double M = amp * exp(-r2);
+    const double g = (fv - M) * irho * isig, r = sqrt(r2);
+    const __nv_bfloat16 h[CIN] = {tobf((float)(fv * irho)), tobf((float)g),
+                                  tobf((float)(g * r)), tobf((float)(g * r2))};
+    const long pt = (long)b * n + i;
+    float xf[CIN];
+#pragma unroll
+    for (int k = 0; k < CIN; ++k) {
+      a.x0[pt * CIN + k] = h[k];
+      xf[k] = bf(h[k]);
+    }
+    __nv_bfloat16* v = a.v0 + pt * WD;
+#pragma unroll
+    for (int o = 0; o < WD; o += 2) {
+      float y0 = wl[CIN * WD + o], y1 = wl[CIN * WD + o + 1];
+#pragma unroll
+      for (int k = 0; k < CIN; ++k) {
+        y0 += xf[k] * wl[k * WD + o];
+        y1 += xf[k] * wl[k * WD + o + 1];
+      }
+      *reinterpret_cast<__nv_bfloat162*>(v + o) = __floats2bfloat162_rn(y0, y1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Truncated DFT along one axis: in [outer][LIN][inner] -> out [outer][LOUT][inner],
+// out[k] = sum_j T[k][j] in[j] with a complex table T [LOUT][LIN].
+// IN: 0 BF16 real, 1 FP32 real, 2 complex FP32.
+// OUT: 0 complex FP32, 1 Re -> FP32 store, 2 Re -> FP32 accumulate.
+// One thread per (outer, inner) pencil; consecutive threads take consecutive
+// inner indices, so every load and store is coalesced.
+// ---------------------------------------------------------------------------
+template <int LIN, int LOUT, int IN, int OUT>
+__global__ void __launch_bounds__(256)
+fno_dft_kernel(const void* in, void* out, const float2* table, long outer,
+               int inner) {
+  __shared__ float2 tb[LOUT * LIN];
+  for (int i = threadIdx.x; i < LOUT * LIN; i += blockDim.x) tb[i] = table[i];
+  __syncthreads();
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= outer * inner) return;
+  const long o = gid / inner;
+  const int i = (int)(gid % inner);
+  float2 x[LIN];
+#pragma unroll
+  for (int j = 0; j < LIN; ++j) {
+    const long idx = (o * LIN + j) * inner + i;
+    if (IN == 0) x[j] = make_float2(bf(static_cast<const __nv_bfloat16*>(in)[idx]), 0.f);
+    else if (IN == 1) x[j] = make_float2(static_cast<const float*>(in)[idx], 0.f);
+    else x[j] = static_cast<const float2*>(in)[idx];
+  }
+#pragma unroll 2
+  for (int k = 0; k < LOUT; ++k) {
+    float re = 0.f, im = 0.f;
+#pragma unroll
+    for (int j = 0; j < LIN; ++j) {
+      const float2 w = tb[k * LIN + j];
+      if (IN == 2) {
+        re += w.x * x[j].x - w.y * x[j].y;
+        im += w.x * x[j].y + w.y * x[j].x;
+      } else {
+        re += w.x * x[j].x;
+        im += w.y * x[j].x;
+      }
+    }
+    const long idx = (o * LOUT + k) * inner + i;
+    if (OUT == 0) static_cast<float2*>(out)[idx] = make_float2(re, im);
+    else if (OUT == 1) static_cast<float*>(out)[idx] = re;
+    else static_cast<float*>(out)[idx] += re;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per-mode channel mixing, one CTA per mode m, block (32, 8).
+//   MODE 0 (forward):      out[b][i'] = sum_i in[b][i] W[i][i']
+//   MODE 1 (data grad):    out[b][i]  = sum_o g[b][o] conj(W[i][o])
+//   MODE 2 (weight grad):  gW[i][o]   = sum_b conj(V[b][i]) g[b][o]
+// W: BF16 complex [K^3][WD][WD] (re, im interleaved); in/out [B][K^3][WD].
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(256)
+fno_mix_kernel(const float2* in, const float2* in2, const __nv_bfloat16* W,
+               float2* out, float* gW, int B, int nm) {
+  __shared__ float2 ws[WD * WD];
+  __shared__ float2 xs[32 * WD];   // up to 32 samples
+  __shared__ float2 gs[32 * WD];
+  const int m = blockIdx.x, tx = threadIdx.x, ty = threadIdx.y;
+  const int t = ty * 32 + tx;
+  if (MODE != 2) {
+    const __nv_bfloat162* wm =
+        reinterpret_cast<const __nv_bfloat162*>(W) + (long)m * WD * WD;
+    for (int i = t; i < WD * WD; i += 256) ws[i] = __bfloat1622float2(wm[i]);
+  }
+  for (int i = t; i < B * WD; i += 256) {
+    const int b = i / WD, c = i % WD;
+    xs[i] = in[((long)b * nm + m) * WD + c];
+    if (MODE == 2) gs[i] = in2[((long)b * nm + m) * WD + c];
+  }
+  __syncthreads();
+  if (MODE == 0 || MODE == 1) {
+    for (int b = ty; b < B; b += 8) {
+      float re = 0.f, im = 0.f;
+#pragma unroll 8
+      for (int i = 0; i < WD; ++i) {
+        const float2 x = xs[b * WD + i];
+        if (MODE == 0) {
+          const float2 w = ws[i * WD + tx];
+          re += x.x * w.x - x.y * w.y;
+          im += x.x * w.y + x.y * w.x;
+        } else {
+          const float2 w = ws[tx * WD + i];  // conj(W[tx][i])
+          re += x.x * w.x + x.y * w.y;
+          im += x.y * w.x - x.x * w.y;
+        }
+      }
+      out[((long)b * nm + m) * WD + tx] = make_float2(re, im);
+    }
+  } else {
+    for (int i = ty; i < WD; i += 8) {
+      float re = 0.f, im = 0.f;
+      for (int b = 0; b < B; ++b) {
+        const float2 v = xs[b * WD + i], g = gs[b * WD + tx];
+        re += v.x * g.x + v.y * g.y;
+        im += v.x * g.y - v.y * g.x;
+      }
+      float* o = gW + 2 * (((long)m * WD + i) * WD + tx);
+      o[0] = re;
+      o[1] = im;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dense layer, forward: y = x D + d + U; v = GELU(y) (or y for the last layer).
+// One thread per point; D staged in shared memory (FP32).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+fno_dense_fwd_kernel(const __nv_bfloat16* x, const __nv_bfloat16* w16, long offD,
+                     long offd, const float* U, __nv_bfloat16* y,
+                     __nv_bfloat16* v, long R, int act) {
+  __shared__ float Ds[WD * WD + WD];
+  for (int i = threadIdx.x; i < WD * WD; i += blockDim.x) Ds[i] = bf(w16[offD + i]);
+  for (int i = threadIdx.x; i < WD; i += blockDim.x) Ds[WD * WD + i] = bf(w16[offd + i]);
+  __syncthreads();
+  const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  float xi[WD];
+  const uint4* xp = reinterpret_cast<const uint4*>(x + r * WD);
+#pragma unroll
+  for (int q = 0; q < WD / 8; ++q) {
+    const uint4 u = xp[q];
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 f = __bfloat1622float2(h[k]);
+      xi[q * 8 + 2 * k] = f.x;
+      xi[q * 8 + 2 * k + 1] = f.y;
+    }
+  }
+  const float* Ur = U + r * WD;
+#pragma unroll 4
+  for (int o = 0; o < WD; o += 2) {
+    float a0 = Ds[WD * WD + o] + Ur[o], a1 = Ds[WD * WD + o + 1] + Ur[o + 1];
+#pragma unroll
+    for (int i = 0; i < WD; ++i) {
+      a0 += xi[i] * Ds[i * WD + o];
+      a1 += xi[i] * Ds[i * WD + o + 1];
+    }
+    const __nv_bfloat162 yy = __floats2bfloat162_rn(a0, a1);
+    *reinterpret_cast<__nv_bfloat162*>(y + r * WD + o) = yy;
+    const float2 yf = __bfloat1622float2(yy);
+    *reinterpret_cast<__nv_bfloat162*>(v + r * WD + o) =
+        act ? __floats2bfloat162_rn(gelu(yf.x), gelu(yf.y)) : yy;
+  }
+}
+
+// Dense layer, data gradient: dx = dy D^T (FP32 in/out).
+__global__ void __launch_bounds__(256)
+fno_dense_bwd_kernel(const float* dy, const __nv_bfloat16* w16, long offD,
+                     float* dx, long R) {
+  __shared__ float Ds[WD * WD];
+  for (int i = threadIdx.x; i < WD * WD; i += blockDim.x) Ds[i] = bf(w16[offD + i]);
+  __syncthreads();
+  const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  float g[WD];
+  const float4* gp = reinterpret_cast<const float4*>(dy + r * WD);
+#pragma unroll
+  for (int q = 0; q < WD / 4; ++q) {
+    const float4 u = gp[q];
+    g[4 * q] = u.x; g[4 * q + 1] = u.y; g[4 * q + 2] = u.z; g[4 * q + 3] = u.w;
+  }
+  float4* op = reinterpret_cast<float4*>(dx + r * WD);
+#pragma unroll 2
+  for (int i = 0; i < WD; i += 4) {
+    float a[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int o = 0; o < WD; ++o) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[k] += g[o] * Ds[(i + k) * WD + o];
+    }
+    op[i / 4] = make_float4(a[0], a[1], a[2], a[3]);
+  }
+}
+
+// dy = dv * GELU'(y)
+__global__ void fno_gelu_bwd_kernel(const float* dv, const __nv_bfloat16* y,
+                                    float* dy, long total) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) dy[i] = dv[i] * gelu_d(bf(y[i]));
+}
+
+// ---------------------------------------------------------------------------
+// Projection, forward: out = sum_j q2[j] GELU(x Q1[:, j] + q1[j]) + q2b.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+fno_proj_fwd_kernel(const __nv_bfloat16* x, const __nv_bfloat16* w16, Layout L,
+                    float* out, long R) {
+  __shared__ float Qs[WD * PJ + 3 * PJ + 1];
+  for (int i = threadIdx.x; i < WD * PJ; i += blockDim.x) Qs[i] = bf(w16[L.Q1 + i]);
+  for (int i = threadIdx.x; i < PJ; i += blockDim.x) {
+    Qs[WD * PJ + i] = bf(w16[L.q1 + i]);
+    Qs[WD * PJ + PJ + i] = bf(w16[L.q2 + i]);
+  }
+  if (threadIdx.x == 0) Qs[WD * PJ + 2 * PJ] = bf(w16[L.q2b]);
+  __syncthreads();
+  const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  float xi[WD];
+  const uint4* xp = reinterpret_cast<const uint4*>(x + r * WD);
+#pragma unroll
+  for (int q = 0; q < WD / 8; ++q) {
+    const uint4 u = xp[q];
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 f = __bfloat1622float2(h[k]);
+      xi[q * 8 + 2 * k] = f.x;
+      xi[q * 8 + 2 * k + 1] = f.y;
+    }
+  }
+  float acc = Qs[WD * PJ + 2 * PJ];
+#pragma unroll 2
+  for (int j = 0; j < PJ; ++j) {
+    float z = Qs[WD * PJ + j];
+#pragma unroll
+    for (int i = 0; i < WD; ++i) z += xi[i] * Qs[i * PJ + j];
+    acc += Qs[WD * PJ + PJ + j] * gelu(z);
+  }
+  out[r] = acc;
+}
+
+// Projection, backward: dz = dout q2 GELU'(z), aw = dout GELU(z) (for dq2),
+// dx = dz Q1^T.
+__global__ void __launch_bounds__(256)
+fno_proj_bwd_kernel(const __nv_bfloat16* x, const __nv_bfloat16* w16, Layout L,
+                    const float* dout, float* dz, float* aw, float* dx, long R) {
+  __shared__ float Qs[WD * PJ + 2 * PJ];
+  for (int i = threadIdx.x; i < WD * PJ; i += blockDim.x) Qs[i] = bf(w16[L.Q1 + i]);
+  for (int i = threadIdx.x; i < PJ; i += blockDim.x) {
+    Qs[WD * PJ + i] = bf(w16[L.q1 + i]);
+    Qs[WD * PJ + PJ + i] = bf(w16[L.q2 + i]);
+  }
+  __syncthreads();
+  const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  float xi[WD], gx[WD];
+  const uint4* xp = reinterpret_cast<const uint4*>(x + r * WD);
+#pragma unroll
+  for (int q = 0; q < WD / 8; ++q) {
+    const uint4 u = xp[q];
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float2 f = __bfloat1622float2(h[k]);
+      xi[q * 8 + 2 * k] = f.x;
+      xi[q * 8 + 2 * k + 1] = f.y;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < WD; ++i) gx[i] = 0.f;
+  const float go = dout[r];
+#pragma unroll 2
+  for (int j = 0; j < PJ; ++j) {
+    float z = Qs[WD * PJ + j];
+#pragma unroll
+    for (int i = 0; i < WD; ++i) z += xi[i] * Qs[i * PJ + j];
+    const float g = go * Qs[WD * PJ + PJ + j] * gelu_d(z);
+    dz[r * PJ + j] = g;
+    aw[r * PJ + j] = go * gelu(z);
+#pragma unroll
+    for (int i = 0; i < WD; ++i) gx[i] += g * Qs[i * PJ + j];
+  }
+  float4* op = reinterpret_cast<float4*>(dx + r * WD);
+#pragma unroll
+  for (int i = 0; i < WD; i += 4) op[i / 4] = make_float4(gx[i], gx[i + 1], gx[i + 2], gx[i + 3]);
+}
+
+// ---------------------------------------------------------------------------
+// Weight gradient G[i][j] = sum_r A[r][i] Bm[r][j] (A: BF16 [R][KA], Bm: FP32
+// [R][KB]).  Persistent CTAs over 64-row tiles; thread owns an RI x 4 block;
+// per-CTA partials [gridDim][KA][KB], summed by fno_reduce_kernel in a fixed
+// order (deterministic).
+// ---------------------------------------------------------------------------
+template <int KA, int KB>
+__global__ void fno_wgrad_kernel(const __nv_bfloat16* A, const float* Bm, long R,
+                                 float* partial) {
+  constexpr int RI = KA < 4 ? KA : 4;
+  constexpr int NTH = (KA / RI) * (KB / 4);
+  constexpr int TR = 64;
+  __shared__ __align__(16) float As[TR * KA];
+  __shared__ __align__(16) float Bs[TR * KB];
+  const int t = threadIdx.x;
+  const int i0 = (t / (KB / 4)) * RI, j0 = (t % (KB / 4)) * 4;
+  float acc[RI][4];
+#pragma unroll
+  for (int a = 0; a < RI; ++a)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[a][c] = 0.f;
+  for (long r0 = (long)blockIdx.x * TR; r0 < R; r0 += (long)gridDim.x * TR) {
+    const int nr = (int)min((long)TR, R - r0);
+    __syncthreads();
+    for (int k = t; k < TR * KA; k += NTH)
+      As[k] = (k / KA < nr) ? bf(A[r0 * KA + k]) : 0.f;
+    for (int k = t; k < TR * KB; k += NTH)
+      Bs[k] = (k / KB < nr) ? Bm[r0 * KB + k] : 0.f;
+    __syncthreads();
+#pragma unroll 4
+    for (int r = 0; r < TR; ++r) {
+      float av[RI];
+#pragma unroll
+      for (int a = 0; a < RI; ++a) av[a] = As[r * KA + i0 + a];
+      const float4 bv = *reinterpret_cast<const float4*>(&Bs[r * KB + j0]);
+#pragma unroll
+      for (int a = 0; a < RI; ++a) {
+        acc[a][0] += av[a] * bv.x; acc[a][1] += av[a] * bv.y;
+        acc[a][2] += av[a] * bv.z; acc[a][3] += av[a] * bv.w;
+      }
+    }
+  }
+  float* P = partial + (long)blockIdx.x * KA * KB;
+#pragma unroll
+  for (int a = 0; a < RI; ++a)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) P[(i0 + a) * KB + j0 + c] = acc[a][c];
+}
+
+// Column sums S[j] = sum_r Bm[r][j] (bias gradients); partials per CTA.
+template <int KB>
+__global__ void __launch_bounds__(256)
+fno_colsum_kernel(const float* Bm, long R, float* partial) {
+  constexpr int RPT = 256 / KB;  // rows per pass
+  __shared__ float red[256];
+  const int t = threadIdx.x, j = t % KB, rr = t / KB;
+  float s = 0.f;
+  for (long r = (long)blockIdx.x * RPT + rr; r < R; r += (long)gridDim.x * RPT)
+    s += Bm[r * KB + j];
+  red[t] = s;
+  __syncthreads();
+  if (t < KB) {
+    float v = 0.f;
+    for (int k = 0; k < RPT; ++k) v += red[k * KB + t];
+    partial[(long)blockIdx.x * KB + t] = v;
+  }
+}
+
+// out[i] = sum_g partial[g][i] (fixed order)
+__global__ void fno_reduce_kernel(const float* partial, int G, int n, float* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float s = 0.f;
+  for (int g = 0; g < G; ++g) s += partial[(long)g * n + i];
+  out[i] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Output: Q[dst] += P(rho^2 sigma sQ out) with the FP64 conservation projection P
+// (5 moments, Gram inverse Ginv).  One CTA per sample.
+// ---------------------------------------------------------------------------
+struct OutArgs {
+  const float* out; const double* qs; double sQ;
+  const double* c0; double cw; int N; double Ginv[25];
+  void* Q; int q_double; const int32_t* dst_slots; int dst_base;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(NT) fno_output_kernel(OutArgs a) {
+  __shared__ double red[8 + 5 * (NT / 32)];
+  const int b = blockIdx.x, t = threadIdx.x, N = a.N;
+  const long n = (long)N * N * N;
+  const double sc = a.qs[b] * a.sQ;
+  const float* o = a.out + (long)b * n;
+  double s[5] = {0, 0, 0, 0, 0};
+  for (long i = t; i < n; i += NT) {
+    const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
+    const double q = sc * o[i] * a.cw;
+    const double cx = a.c0[x], cy = a.c0[y], cz = a.c0[z];
+    s[0] += q; s[1] += q * cx; s[2] += q * cy; s[3] += q * cz;
+    s[4] += q * (cx * cx + cy * cy + cz * cz);
+  }
+  block_sum5<NT>(s, red);
+  double lam[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    double l = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) l += a.Ginv[j * 5 + k] * red[k];
+    lam[j] = l;
+  }
+  const long qb = (long)(a.dst_slots ? a.dst_slots[b] : a.dst_base + b) * n;
+  for (long i = t; i < n; i += NT) {
+    const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
+    const double cx = a.c0[x], cy = a.c0[y], cz = a.c0[z];
+    const double q = sc * o[i] - (lam[0] + lam[1] * cx + lam[2] * cy + lam[3] * cz +
+                                  lam[4] * (cx * cx + cy * cy + cz * cz));
+    if (a.q_double) static_cast<double*>(a.Q)[qb + i] += q;
+    else static_cast<float*>(a.Q)[qb + i] += (float)q;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Loss: per sample, t = Q/(rho^2 sigma sQ); L_b = |out - t|^2 / |t|^2;
+// dout = (2/B) (out - t)/|t|^2.  One CTA per sample.
+// ---------------------------------------------------------------------------
+template <int NT>
+__global__ void __launch_bounds__(NT)
+fno_loss_kernel(const float* out, const double* Qt, const double* qs, double sQ,
+                long n, int B, float* dout, double* loss) {
+  __shared__ double red[8 + 5 * (NT / 32)];
+  const int b = blockIdx.x, t = threadIdx.x;
+  const double isc = 1.0 / (qs[b] * sQ);
+  const float* o = out + (long)b * n;
+  const double* q = Qt + (long)b * n;
+  double s[5] = {0, 0, 0, 0, 0};
+  for (long i = t; i < n; i += NT) {
+    const double tv = q[i] * isc, e = (double)o[i] - tv;
+    s[0] += e * e;
+    s[1] += tv * tv;
+  }
+  block_sum5<NT>(s, red);
+  const double tn = red[1] > 0 ? red[1] : 1.0;
+  if (t == 0) loss[b] = red[0] / tn;
+  const double g = 2.0 / (B * tn);
+  for (long i = t; i < n; i += NT) {
+    const double tv = q[i] * isc;
+    dout[(long)b * n + i] = (float)(g * ((double)o[i] - tv));
+  }
+}
+
+// Adam on the FP32 master parameters; refreshes the BF16 copy.
+__global__ void fno_adam_kernel(float* p, __nv_bfloat16* p16, const float* g,
+                                float* m, float* v, long n, float lr, float b1,
+                                float b2, float eps, float bc1, float bc2) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+  p[i] = pi;
+  p16[i] = tobf(pi);
+}
+
+__global__ void fno_to_bf16_kernel(const float* p, __nv_bfloat16* p16, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p16[i] = tobf(p[i]);
+}
+
+}  // namespace fno
+}  // namespace dgfs

@@ -265,6 +265,51 @@ int dgfs_vhs_eval_noalloc(const dgfs_vhs_desc* desc, const double* f,
                           int32_t src_base, const int32_t* dst_slots,
                           int32_t dst_base, int32_t nevals, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Fourier-neural-operator surrogate of Q(f,f).  No counterpart in the
+ * reference (a new learned component): 4 Fourier layers of width 32 with
+ * `modes` retained modes per velocity axis (8 at N=16, 12 at N=32), GELU,
+ * a 32 -> 128 -> 1 projection; input features f/rho, g, g r, g r^2 with
+ * g = (f - M)/(rho sigma), sigma = rms((f - M)/rho), r = |c - u|/sqrt(T)
+ * (M the local Maxwellian from FP64 moments), output
+ * Q = rho^2 sigma q_scale * net(f),
+ * followed by the FP64 conservation projection.  BF16 weights and
+ * activations, FP32 accumulation.  Parameters are a flat FP32 vector
+ * (dgfs_fno_num_params floats) set by the caller.
+ * ------------------------------------------------------------------------- */
+typedef struct dgfs_fno_s* dgfs_fno_handle;
+typedef struct {
+  int32_t N;          /* velocity grid points per axis: 16 or 32 */
+  int32_t modes;      /* retained modes per axis: 8 (N=16) or 12 (N=32) */
+  int32_t max_batch;  /* samples per launch, 1..32 (activation buffers) */
+  double L;           /* velocity box half-width, grid c = linspace(-L+L/N, L-L/N, N) */
+  double q_scale;     /* output scale: Q = rho^2 sigma q_scale net(f) */
+} dgfs_fno_desc;
+
+int dgfs_fno_create(const dgfs_fno_desc* desc, dgfs_fno_handle* out);
+int dgfs_fno_destroy(dgfs_fno_handle h);
+int64_t dgfs_fno_num_params(dgfs_fno_handle h);
+/* Host FP32 parameter vector in / out (synchronous; set also resets Adam). */
+int dgfs_fno_set_params(dgfs_fno_handle h, const float* host);
+int dgfs_fno_get_params(dgfs_fno_handle h, float* host);
+/* Gradients of the last dgfs_fno_train_step (synchronous copy). */
+int dgfs_fno_get_grads(dgfs_fno_handle h, float* host);
+/* Q[dst(i)] += surrogate Q(f[src(i)]), i < nevals; same slot conventions as
+ * dgfs_vhs_eval (the drop-in replacement of that call). */
+int dgfs_fno_eval(dgfs_fno_handle h, const void* f, int32_t f_dtype, void* Q,
+                  int32_t q_dtype, const int32_t* src_slots, int32_t src_base,
+                  const int32_t* dst_slots, int32_t dst_base, int32_t nevals,
+                  void* stream);
+/* One training step on B (f, Q) pairs (FP64, [B][N^3] each): forward, loss
+ * mean_b |net - t|^2 / |t|^2 with t = Q/(rho^2 sigma q_scale), backward, and
+ * (update != 0) one Adam step (beta 0.9/0.999, eps 1e-8, bias-corrected with
+ * `step` >= 1). */
+int dgfs_fno_train_step(dgfs_fno_handle h, const double* f, const double* Qt,
+                        int32_t B, float lr, int32_t step, int32_t update,
+                        void* stream);
+/* Per-sample losses of the last training step (synchronous copy). */
+int dgfs_fno_last_loss(dgfs_fno_handle h, double* host, int32_t B);
+
 /* Library identification and error reporting. */
 const char* dgfs_version(void);
 const char* dgfs_last_error_string(void);

@@ -1,0 +1,106 @@
+"""The CUDA FNO surrogate against the CPU FP64 oracle (oracle/fno.py):
+forward output, loss and every parameter gradient; conservation and +=
+semantics of the surrogate's Q; and that training on operator pairs lowers
+the loss."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import fno as ofno
+from tests.test_fno_oracle import _maxwellians
+
+pytestmark = pytest.mark.gpu
+
+N, L, B = 16, 5.0, 2
+K = 8
+SQ = 0.05
+
+
+@pytest.fixture(scope='module')
+def built():
+    from dgfs1d_gpu_b200 import build
+    build.build()
+
+
+def _data(seed=11):
+    f = _maxwellians(N, L, B, seed)
+    Qt = np.random.default_rng(seed + 1).standard_normal((B, N ** 3)) * 1e-3
+    return f, Qt
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_loss_and_gradients_match_oracle(built):
+    from dgfs1d_gpu_b200.surrogate import FNOSurrogate, layout
+    net = FNOSurrogate(N, L, q_scale=SQ, max_batch=4, seed=7)
+    f, Qt = _data()
+    fd = torch.tensor(f, device='cuda')
+    qd = torch.tensor(Qt, device='cuda')
+    net.train_step(fd, qd, update=False)
+    torch.cuda.synchronize()
+    loss = net.last_loss(B)
+    g = net.grads()
+    ref = ofno.FNO(N, K, L, SQ, net.params(), emulate_bf16=True)
+    out, cache = ref.forward(f)
+    Lb, dout = ref.loss(out, Qt, cache['qs'])
+    gr = ref.backward(dout, cache)
+    assert np.allclose(loss, Lb, rtol=2e-3), (loss, Lb)
+    errs = {}
+    for name, sl in layout(K).items():
+        if name == 'total':
+            continue
+        o, s = sl
+        errs[name] = e = _rel(g[o:o + s], gr[o:o + s])
+        assert e < 2e-2, f'{name}: gradient rel L2 {e:.3e} ({errs})'
+    print('gradient rel L2 vs oracle:', {k: f'{v:.1e}' for k, v in errs.items()})
+
+
+def test_eval_is_conservative_accumulating_and_matches_oracle(built):
+    from dgfs1d_gpu_b200.surrogate import FNOSurrogate
+    net = FNOSurrogate(N, L, q_scale=SQ, max_batch=4, seed=8)
+    f, _ = _data(21)
+    fd = torch.tensor(f, device='cuda')
+    Q0 = torch.zeros_like(fd)
+    net.eval(fd, Q0)
+    Q1 = torch.full_like(fd, 0.25)
+    net.eval(fd, Q1)
+    torch.cuda.synchronize()
+    q = Q0.cpu().numpy()
+    assert np.allclose(Q1.cpu().numpy() - 0.25, q, rtol=0, atol=1e-15)
+    ref = ofno.FNO(N, K, L, SQ, net.params(), emulate_bf16=True)
+    out, cache = ref.forward(f)
+    c0 = ref.c0
+    g = np.meshgrid(c0, c0, c0, indexing='ij')
+    cv = np.stack([x.ravel() for x in g])
+    phi = np.vstack([np.ones(N ** 3), cv, (cv ** 2).sum(0)]) * ref.cw
+    G = phi @ np.vstack([np.ones(N ** 3), cv, (cv ** 2).sum(0)]).T
+    for b in range(B):
+        raw = cache['qs'][b] * SQ * out[b]
+        lam = np.linalg.solve(G, phi @ raw)
+        proj = raw - lam @ np.vstack([np.ones(N ** 3), cv, (cv ** 2).sum(0)])
+        assert _rel(q[b], proj) < 1e-2
+        # conserved to rounding of the FP64 projection of the raw output
+        scale = np.abs(phi) @ np.abs(raw)
+        assert np.all(np.abs(phi @ q[b]) <= 1e-12 * scale)
+
+
+def test_training_on_operator_pairs_lowers_the_loss(built):
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    from dgfs1d_gpu_b200.surrogate import FNOSurrogate
+    from dgfs1d_gpu_b200.workloads import vhs_mesh_params
+    prm = vhs_mesh_params(N, 6, 8, L, False)
+    op = VHSOperator(**prm, precision='fp64', max_evals=8)
+    f = torch.tensor(_maxwellians(N, L, 8, 31), device='cuda')
+    Qt = torch.zeros_like(f)
+    op.eval(f, Qt)
+    net = FNOSurrogate(N, L, q_scale=1.0, max_batch=8, seed=9)
+    net.train_step(f, Qt, update=False)
+    first = net.last_loss(8).mean()
+    for _ in range(100):
+        net.train_step(f, Qt, lr=3e-3)
+    net.train_step(f, Qt, update=False)
+    last = net.last_loss(8).mean()
+    print(f'training loss {first:.3e} -> {last:.3e}')
+    assert np.isfinite(last) and last < 0.5 * first, (first, last)
