@@ -109,6 +109,8 @@ _SIGNATURES = [
       ctypes.c_float, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     ('dgfs_fno_last_loss', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
+    ('dgfs_fno_set_tensor_cores', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ('dgfs_fno_error', ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ('dgfs_vhs_destroy', ctypes.c_int, [ctypes.c_void_p]),
     ('dgfs_vhs_profile', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_vhs_stage_ms', ctypes.c_int,

@@ -1423,6 +1423,8 @@ struct dgfs_fno_s {
         *dvB = nullptr, *dy = nullptr, *part = nullptr;
   float2 *gUh = nullptr, *gVh = nullptr;
   double* loss = nullptr;
+  int* err = nullptr;                // device error flag (bounded waits)
+  int use_tc = 1;                    // dense layers on tcgen05 tensor cores
   std::vector<void*> owned;
 };
 
@@ -1533,6 +1535,7 @@ extern "C" int dgfs_fno_create(const dgfs_fno_desc* d, dgfs_fno_handle* out) {
   A(&h->dy, B * n * fno::WD);
   A(&h->part, (size_t)kFnoWgradGrid * fno::WD * fno::PJ);
   A(&h->loss, B);
+  A(&h->err, 1);
   if (e == cudaSuccess) e = cudaMemcpy(h->c0, c0.data(), N * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(h->tF, tF.data(), K * N * sizeof(float2), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(h->tG, tG.data(), K * N * sizeof(float2), cudaMemcpyHostToDevice);
@@ -1540,6 +1543,7 @@ extern "C" int dgfs_fno_create(const dgfs_fno_desc* d, dgfs_fno_handle* out) {
   if (e == cudaSuccess) e = cudaMemcpy(h->tGs, tGs.data(), K * N * sizeof(float2), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(h->p32, 0, h->L.total * sizeof(float));
   if (e == cudaSuccess) e = cudaMemset(h->p16, 0, h->L.total * sizeof(__nv_bfloat16));
+  if (e == cudaSuccess) e = cudaMemset(h->err, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(h->am, 0, h->L.total * sizeof(float));
   if (e == cudaSuccess) e = cudaMemset(h->av, 0, h->L.total * sizeof(float));
   if (e != cudaSuccess) {
@@ -1616,10 +1620,28 @@ static int fno_idft3(dgfs_fno_s* h, const float2* in, const float2* tab, float* 
   return fno_dft<K, N, 2, OUT>(h->T1, out, tab, B, N * N * WD, st);
 }
 
+// Dense layer / projection on the tensor cores: persistent 128-row tiles.
+template <int NC, int EPI>
+static int fno_tc(dgfs_fno_s* h, const fno::TcArgs& a, cudaStream_t st) {
+  const long ntiles = (a.R + 127) / 128;
+  // NC=128: pad shared memory so that at most 3 CTAs share an SM (3 x 128 of
+  // the 512 TMEM columns); NC=32: 16 CTAs x 32 columns fit
+  const size_t pad = NC == 128 ? 40 * 1024 : 0;
+  const int per_sm = NC == 128 ? 3 : 8;
+  const unsigned grid = (unsigned)std::min<long>(ntiles, 148L * per_sm);
+  if (pad)
+    DGFS_CUDA(cudaFuncSetAttribute(fno::fno_tc_kernel<NC, EPI>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)pad));
+  fno::fno_tc_kernel<NC, EPI><<<grid, 128, pad, st>>>(a);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
 template <int N, int K>
 static int fno_forward(dgfs_fno_s* h, const void* f, int f_double,
                        const int32_t* src_slots, int src_base, int B,
-                       cudaStream_t st) {
+                       cudaStream_t st, bool store_y = true) {
   using namespace fno;
   const long R = (long)B * h->n;
   const long nm = (long)K * K * K;
@@ -1636,14 +1658,30 @@ static int fno_forward(dgfs_fno_s* h, const void* f, int f_double,
         h->Vh[l], nullptr, h->p16 + h->L.W[l], h->Uh, nullptr, B, (int)nm);
     DGFS_CUDA(cudaGetLastError());
     if ((rc = fno_idft3<N, K, 1>(h, h->Uh, h->tG, h->U, B, st))) return rc;
-    fno_dense_fwd_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(
-        h->v[l], h->p16, h->L.D[l], h->L.d[l], h->U, h->y[l], h->v[l + 1], R,
-        l < 3 ? 1 : 0);
+    if (h->use_tc) {
+      TcArgs ta{};
+      ta.x = h->v[l]; ta.w16 = h->p16; ta.offW = h->L.D[l]; ta.offb = h->L.d[l];
+      ta.U = h->U; ta.y = store_y ? h->y[l] : nullptr; ta.v = h->v[l + 1];
+      ta.R = R; ta.act = l < 3 ? 1 : 0; ta.err = h->err;
+      if ((rc = fno_tc<WD, 0>(h, ta, st))) return rc;
+    } else {
+      fno_dense_fwd_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(
+          h->v[l], h->p16, h->L.D[l], h->L.d[l], h->U, h->y[l], h->v[l + 1], R,
+          l < 3 ? 1 : 0);
+      DGFS_CUDA(cudaGetLastError());
+    }
+  }
+  if (h->use_tc) {
+    TcArgs ta{};
+    ta.x = h->v[4]; ta.w16 = h->p16; ta.offW = h->L.Q1; ta.offb = h->L.q1;
+    ta.offq2 = h->L.q2; ta.offq2b = h->L.q2b; ta.out = h->out; ta.R = R;
+    ta.err = h->err;
+    if ((rc = fno_tc<PJ, 1>(h, ta, st))) return rc;
+  } else {
+    fno_proj_fwd_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(
+        h->v[4], h->p16, h->L, h->out, R);
     DGFS_CUDA(cudaGetLastError());
   }
-  fno_proj_fwd_kernel<<<(unsigned)((R + 255) / 256), 256, 0, st>>>(
-      h->v[4], h->p16, h->L, h->out, R);
-  DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
 }
 
@@ -1726,7 +1764,7 @@ static int fno_eval_t(dgfs_fno_s* h, const void* f, int f_double, void* Q,
     const int B = std::min(h->maxB, nevals - off);
     int rc;
     if ((rc = fno_forward<N, K>(h, f, f_double, src_slots ? src_slots + off : nullptr,
-                                src_base + off, B, st)))
+                                src_base + off, B, st, false)))
       return rc;
     fno::OutArgs oa{};
     oa.out = h->out; oa.qs = h->qs; oa.sQ = h->sQ; oa.c0 = h->c0; oa.cw = h->cw;
@@ -1798,5 +1836,21 @@ extern "C" int dgfs_fno_last_loss(dgfs_fno_handle h, double* host, int32_t B) {
   if (B < 1 || B > h->maxB) return fail(DGFS_ERR_INVALID, "bad batch size");
   DGFS_CUDA(cudaDeviceSynchronize());
   DGFS_CUDA(cudaMemcpy(host, h->loss, B * sizeof(double), cudaMemcpyDeviceToHost));
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_fno_set_tensor_cores(dgfs_fno_handle h, int32_t enable) {
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  h->use_tc = enable ? 1 : 0;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_fno_error(dgfs_fno_handle h, int32_t* out) {
+  if (!h || !out) return fail(DGFS_ERR_INVALID, "null argument");
+  DGFS_CUDA(cudaDeviceSynchronize());
+  int v = 0;
+  DGFS_CUDA(cudaMemcpy(&v, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+  DGFS_CUDA(cudaMemset(h->err, 0, sizeof(int)));
+  *out = v;
   return DGFS_OK;
 }

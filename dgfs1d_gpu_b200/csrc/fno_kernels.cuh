@@ -601,6 +601,216 @@ fno_loss_kernel(const float* out, const double* Qt, const double* qs, double sQ,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Dense layers on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// One CTA (4 warps) computes 128-row tiles of D[128 x NC] = A[128 x 32] B,
+// A = BF16 activations (row-major [R][32], i.e. K-major), B = BF16 weights
+// W[32][NC] staged once per CTA as B^T (K-major).  Operands sit in shared
+// memory in the canonical no-swizzle K-major layout: 8x8 core matrices of
+// 128 contiguous bytes, core (row group g, K chunk c) at (g*4 + c)*128, so the
+// leading-dimension offset (next K chunk) is 128 B and the stride-dimension
+// offset (next 8 rows) 512 B.  One elected thread issues two
+// tcgen05.mma.kind::f16 (K = 16 each) into a TMEM accumulator (FP32, NC
+// columns, lane = row), commits to an mbarrier, and every thread reads its
+// row back with tcgen05.ld for the fused epilogue:
+//   EPI 0 (dense):      y = D + d + U;  v = GELU(y) (act) or y;  y stored if asked
+//   EPI 1 (projection): out = sum_j q2[j] GELU(D_j + q1[j]) + q2b
+// The mbarrier wait is bounded: on timeout the CTA records an error code
+// and stops issuing work (still freeing its TMEM).
+// ---------------------------------------------------------------------------
+struct TcArgs {
+  const __nv_bfloat16* x;   // [R][32]
+  const __nv_bfloat16* w16; // parameters (BF16)
+  long offW, offb;          // weight [32][NC], bias [NC]
+  long offq2, offq2b;       // projection only
+  const float* U;           // dense: [R][32] spectral part
+  __nv_bfloat16* y;         // dense: pre-activation out (may be null)
+  __nv_bfloat16* v;         // dense: activation out
+  float* out;               // projection: [R]
+  long R;
+  int act;
+  int* err;
+};
+
+__device__ __forceinline__ uint32_t tc_smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
+}
+
+template <int NC, int EPI>
+__global__ void __launch_bounds__(128) fno_tc_kernel(TcArgs a) {
+  static_assert(NC == 32 || NC == 128, "NC");
+  __shared__ __align__(1024) uint8_t sA[128 * 64];
+  __shared__ __align__(1024) uint8_t sB[NC * 64];
+  __shared__ float ep[3 * NC + 1];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tslot;
+  __shared__ int abort_flag;
+  const int t = threadIdx.x, warp = t >> 5;
+  // weights as B^T [NC][32] in core-matrix layout; epilogue vectors
+  for (int e = t; e < NC * WD; e += 128) {
+    const int j = e / WD, k = e % WD;
+    const __nv_bfloat16 w = a.w16[a.offW + (long)k * NC + j];
+    *reinterpret_cast<__nv_bfloat16*>(
+        sB + ((j >> 3) * 4 + (k >> 3)) * 128 + (j & 7) * 16 + (k & 7) * 2) = w;
+  }
+  for (int j = t; j < NC; j += 128) {
+    ep[j] = bf(a.w16[a.offb + j]);
+    if (EPI == 1) ep[NC + j] = bf(a.w16[a.offq2 + j]);
+  }
+  if (EPI == 1 && t == 0) ep[2 * NC] = bf(a.w16[a.offq2b]);
+  if (t == 0) {
+    abort_flag = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(tc_smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 ::"r"(tc_smem_u32(&tslot)), "r"(NC));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tslot;
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                         ((uint32_t)(NC >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  const uint32_t aS = tc_smem_u32(sA), bS = tc_smem_u32(sB);
+  const uint32_t mb = tc_smem_u32(&mbar);
+  const long ntiles = (a.R + 127) / 128;
+  uint32_t phase = 0;
+  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long row = tile * 128 + t;
+    // A row -> 4 core-matrix rows of 16 B
+    uint4 q[4] = {};
+    if (row < a.R) {
+      const uint4* src = reinterpret_cast<const uint4*>(a.x + row * WD);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) q[c] = src[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      *reinterpret_cast<uint4*>(sA + ((t >> 3) * 4 + c) * 128 + (t & 7) * 16) = q[c];
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2) {
+        const uint64_t ad = tc_desc(aS + s2 * 256), bd = tc_desc(bS + s2 * 256);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(s2), "r"(0u), "r"(0u),
+              "r"(0u), "r"(0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                   ::"r"(mb) : "memory");
+    }
+    // bounded wait for the MMA's completion
+    {
+      uint32_t done = 0;
+      for (int it = 0; it < (1 << 22) && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done) : "r"(mb), "r"(phase) : "memory");
+      }
+      if (!done) abort_flag = 1;
+    }
+    phase ^= 1u;
+    __syncthreads();
+    if (abort_flag) {
+      if (t == 0) atomicExch(a.err, 1);
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    if (EPI == 0) {
+      uint32_t r[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, "
+          "%8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, "
+          "%23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+            "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+            "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+            "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+            "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]),
+            "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(lane_addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (row < a.R) {
+        const float4* Ur = reinterpret_cast<const float4*>(a.U + row * WD);
+        uint4 yo[4], vo[4];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const float4 u = Ur[c];
+          const float y0 = __uint_as_float(r[4 * c]) + ep[4 * c] + u.x;
+          const float y1 = __uint_as_float(r[4 * c + 1]) + ep[4 * c + 1] + u.y;
+          const float y2 = __uint_as_float(r[4 * c + 2]) + ep[4 * c + 2] + u.z;
+          const float y3 = __uint_as_float(r[4 * c + 3]) + ep[4 * c + 3] + u.w;
+          const __nv_bfloat162 ya = __floats2bfloat162_rn(y0, y1);
+          const __nv_bfloat162 yb = __floats2bfloat162_rn(y2, y3);
+          __nv_bfloat162 va = ya, vb = yb;
+          if (a.act) {
+            const float2 fa = __bfloat1622float2(ya), fb = __bfloat1622float2(yb);
+            va = __floats2bfloat162_rn(gelu(fa.x), gelu(fa.y));
+            vb = __floats2bfloat162_rn(gelu(fb.x), gelu(fb.y));
+          }
+          reinterpret_cast<__nv_bfloat162*>(&yo[c >> 1])[(c & 1) * 2] = ya;
+          reinterpret_cast<__nv_bfloat162*>(&yo[c >> 1])[(c & 1) * 2 + 1] = yb;
+          reinterpret_cast<__nv_bfloat162*>(&vo[c >> 1])[(c & 1) * 2] = va;
+          reinterpret_cast<__nv_bfloat162*>(&vo[c >> 1])[(c & 1) * 2 + 1] = vb;
+        }
+        uint4* vd = reinterpret_cast<uint4*>(a.v + row * WD);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) vd[c] = vo[c];
+        if (a.y) {
+          uint4* yd = reinterpret_cast<uint4*>(a.y + row * WD);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) yd[c] = yo[c];
+        }
+      }
+    } else {
+      float o = ep[2 * NC];
+#pragma unroll 1
+      for (int cc = 0; cc < NC / 32; ++cc) {
+        uint32_t r[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, "
+            "%8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, "
+            "%23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+              "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+              "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]),
+              "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(lane_addr + (uint32_t)(cc * 32)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int jj = cc * 32 + j;
+          o += ep[NC + jj] * gelu(__uint_as_float(r[j]) + ep[jj]);
+        }
+      }
+      if (row < a.R) a.out[row] = o;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+  }
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n"
+                 ::"r"(tmem), "r"(NC));
+}
+
 // Adam on the FP32 master parameters; refreshes the BF16 copy.
 __global__ void fno_adam_kernel(float* p, __nv_bfloat16* p16, const float* g,
                                 float* m, float* v, long n, float lr, float b1,

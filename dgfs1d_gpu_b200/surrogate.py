@@ -142,6 +142,16 @@ class FNOSurrogate:
             int(B), float(lr), int(max(self.step, 1)), int(bool(update)),
             _stream_ptr(stream)))
 
+    def set_tensor_cores(self, enable=True):
+        """Dense layers on tcgen05 tensor cores (default) or CUDA cores."""
+        nat.check(nat.lib().dgfs_fno_set_tensor_cores(self._h, int(bool(enable))))
+
+    def device_error(self):
+        """Error flag of the tensor-core kernels (0 = none); resets it."""
+        v = ctypes.c_int32(0)
+        nat.check(nat.lib().dgfs_fno_error(self._h, ctypes.byref(v)))
+        return v.value
+
     def last_loss(self, B):
         out = np.empty(B, dtype=np.float64)
         nat.check(nat.lib().dgfs_fno_last_loss(self._h, out.ctypes.data, int(B)))

@@ -309,6 +309,13 @@ int dgfs_fno_train_step(dgfs_fno_handle h, const double* f, const double* Qt,
                         void* stream);
 /* Per-sample losses of the last training step (synchronous copy). */
 int dgfs_fno_last_loss(dgfs_fno_handle h, double* host, int32_t B);
+/* Dense layers and projection on the tcgen05 tensor cores (default, 1) or on
+ * the CUDA cores (0; the reference implementation the tensor-core kernels
+ * are tested against). */
+int dgfs_fno_set_tensor_cores(dgfs_fno_handle h, int32_t enable);
+/* Device error flag of the tensor-core kernels (1: an MMA completion wait
+ * timed out and the kernel stopped); synchronous, resets the flag. */
+int dgfs_fno_error(dgfs_fno_handle h, int32_t* out);
 
 /* Library identification and error reporting. */
 const char* dgfs_version(void);

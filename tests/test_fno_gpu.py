@@ -104,3 +104,23 @@ def test_training_on_operator_pairs_lowers_the_loss(built):
     last = net.last_loss(8).mean()
     print(f'training loss {first:.3e} -> {last:.3e}')
     assert np.isfinite(last) and last < 0.5 * first, (first, last)
+
+
+def test_tensor_core_layers_match_cuda_core_layers(built):
+    """The tcgen05 dense/projection kernels against the CUDA-core kernels on
+    the same network and inputs (eval path, N=16 and N=32)."""
+    from dgfs1d_gpu_b200.surrogate import FNOSurrogate
+    for n_, l_ in ((16, 5.0), (32, 6.0)):
+        net = FNOSurrogate(n_, l_, q_scale=SQ, max_batch=4, seed=12)
+        f = torch.tensor(_maxwellians(n_, l_, 3, 41), device='cuda')
+        out = []
+        for tc in (True, False):
+            net.set_tensor_cores(tc)
+            Q = torch.zeros_like(f)
+            net.eval(f, Q)
+            torch.cuda.synchronize()
+            out.append(Q.cpu().numpy())
+        assert net.device_error() == 0
+        e = _rel(out[0], out[1])
+        print(f'N={n_}: tensor cores vs CUDA cores rel L2 {e:.2e}')
+        assert e < 2e-2, e
