@@ -1416,9 +1416,10 @@ struct dgfs_fno_s {
   __nv_bfloat16* y[4] = {};
   float2* Vh[4] = {};
   float2 *Uh = nullptr, *T1 = nullptr, *T2 = nullptr;
-  float* U = nullptr;
+  __nv_bfloat16* U = nullptr;        // spectral-path output (BF16)
   float* out = nullptr;
   double* qs = nullptr;
+  double* fpart = nullptr;           // [maxB][FCH][6] partial sums
   float *dout = nullptr, *dz = nullptr, *aw = nullptr, *dvA = nullptr,
         *dvB = nullptr, *dy = nullptr, *part = nullptr;
   float2 *gUh = nullptr, *gVh = nullptr;
@@ -1527,6 +1528,7 @@ extern "C" int dgfs_fno_create(const dgfs_fno_desc* d, dgfs_fno_handle* out) {
   A(&h->U, B * n * fno::WD);
   A(&h->out, B * n);
   A(&h->qs, B);
+  A(&h->fpart, B * fno::FCH * 6);
   A(&h->dout, B * n);
   A(&h->dz, B * n * fno::PJ);
   A(&h->aw, B * n * fno::PJ);
@@ -1609,9 +1611,10 @@ static int fno_dft3(dgfs_fno_s* h, const void* in, const float2* tab, float2* ou
   return fno_dft<N, K, 2, 0>(h->T2, out, tab, (long)B * K * K, WD, st);
 }
 
-// expand [B][K^3][WD] complex to the real part on the grid (OUT: 1 store, 2 add)
+// expand [B][K^3][WD] complex to the real part on the grid
+// (OUT: 2 FP32 add, 3 BF16 store)
 template <int N, int K, int OUT>
-static int fno_idft3(dgfs_fno_s* h, const float2* in, const float2* tab, float* out,
+static int fno_idft3(dgfs_fno_s* h, const float2* in, const float2* tab, void* out,
                      int B, cudaStream_t st) {
   constexpr int WD = fno::WD;
   int rc;
@@ -1649,15 +1652,18 @@ static int fno_forward(dgfs_fno_s* h, const void* f, int f_double,
   FeatArgs fa{};
   fa.f = f; fa.f_double = f_double; fa.src_slots = src_slots; fa.src_base = src_base;
   fa.c0 = h->c0; fa.cw = h->cw; fa.N = N; fa.w16 = h->p16; fa.L = h->L;
-  fa.x0 = h->x0; fa.v0 = h->v[0]; fa.qs = h->qs;
-  fno_features_kernel<512><<<B, 512, 0, st>>>(fa);
+  fa.x0 = h->x0; fa.v0 = h->v[0]; fa.qs = h->qs; fa.part = h->fpart;
+  const dim3 fg(FCH, B);
+  fno_features_kernel<0><<<fg, 256, 0, st>>>(fa);
+  fno_features_kernel<1><<<fg, 256, 0, st>>>(fa);
+  fno_features_kernel<2><<<fg, 256, 0, st>>>(fa);
   DGFS_CUDA(cudaGetLastError());
   for (int l = 0; l < 4; ++l) {
     if ((rc = fno_dft3<N, K, 0>(h, h->v[l], h->tF, h->Vh[l], B, st))) return rc;
     fno_mix_kernel<0><<<(unsigned)nm, dim3(32, 8), 0, st>>>(
         h->Vh[l], nullptr, h->p16 + h->L.W[l], h->Uh, nullptr, B, (int)nm);
     DGFS_CUDA(cudaGetLastError());
-    if ((rc = fno_idft3<N, K, 1>(h, h->Uh, h->tG, h->U, B, st))) return rc;
+    if ((rc = fno_idft3<N, K, 3>(h, h->Uh, h->tG, h->U, B, st))) return rc;
     if (h->use_tc) {
       TcArgs ta{};
       ta.x = h->v[l]; ta.w16 = h->p16; ta.offW = h->L.D[l]; ta.offb = h->L.d[l];
@@ -1772,7 +1778,9 @@ static int fno_eval_t(dgfs_fno_s* h, const void* f, int f_double, void* Q,
     for (int i = 0; i < 25; ++i) oa.Ginv[i] = h->Ginv[i];
     oa.Q = Q; oa.q_double = q_double;
     oa.dst_slots = dst_slots ? dst_slots + off : nullptr; oa.dst_base = dst_base + off;
-    fno::fno_output_kernel<512><<<B, 512, 0, st>>>(oa);
+    oa.part = h->fpart;
+    fno::fno_output_kernel<0><<<dim3(fno::FCH, B), 256, 0, st>>>(oa);
+    fno::fno_output_kernel<1><<<dim3(fno::FCH, B), 256, 0, st>>>(oa);
     DGFS_CUDA(cudaGetLastError());
   }
   return DGFS_OK;

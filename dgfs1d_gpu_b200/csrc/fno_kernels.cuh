@@ -85,6 +85,7 @@ struct FeatArgs {
   __nv_bfloat16* x0;  // [B][n][CIN]
   __nv_bfloat16* v0;  // [B][n][WD]
   double* qs;         // out [B] rho^2 sigma (output scale without sQ)
+  double* part;       // scratch [B][FCH][6] partial sums
 };
 
 template <int NT>
@@ -107,71 +108,129 @@ __device__ __forceinline__ void block_sum5(double* s, double* red) {
   __syncthreads();
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT) fno_features_kernel(FeatArgs a) {
-  __shared__ double red[8 + 5 * (NT / 32)];
-  __shared__ float wl[CIN * WD + WD];
-  const int b = blockIdx.x, t = threadIdx.x, N = a.N;
+// Features in three grid-wide passes over f, grid (CH chunks, B samples):
+//   pass 0: per-chunk partial moments  (sum f, f c, f |c|^2)      -> part[b][ch][0..4]
+//   pass 1: per-chunk partial sum g^2 (g = (f - M)/rho)            -> part[b][ch][5]
+//   pass 2: features x0 and lift v0; qs[b] = rho^2 sigma
+// Every CTA re-reduces the CH partials of its sample in a fixed order, so all
+// CTAs see identical rho, u, T, sigma.
+constexpr int FCH = 64;  // chunks per sample
+static_assert(CIN == 4, "the feature pass packs four BF16 values");
+
+__device__ __forceinline__ void feat_load(const FeatArgs& a, int b, long i,
+                                          double& fv, double& cx, double& cy,
+                                          double& cz) {
+  const int N = a.N;
   const long n = (long)N * N * N;
   const long fb = (long)(a.src_slots ? a.src_slots[b] : a.src_base + b) * n;
-  for (int i = t; i < CIN * WD + WD; i += NT) wl[i] = bf(a.w16[a.L.P + i]);
-  double s[5] = {0, 0, 0, 0, 0};
-  for (long i = t; i < n; i += NT) {
-    const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
-    const double fv = a.f_double ? static_cast<const double*>(a.f)[fb + i]
-                                 : (double)static_cast<const float*>(a.f)[fb + i];
-    const double cx = a.c0[x], cy = a.c0[y], cz = a.c0[z];
-    s[0] += fv; s[1] += fv * cx; s[2] += fv * cy; s[3] += fv * cz;
-    s[4] += fv * (cx * cx + cy * cy + cz * cz);
-  }
-  block_sum5<NT>(s, red);
-  double rho = red[0] * a.cw;
-  const double ux = red[1] * a.cw / rho, uy = red[2] * a.cw / rho,
-               uz = red[3] * a.cw / rho;
-  double T = (2.0 / 3.0) * (red[4] * a.cw / rho - (ux * ux + uy * uy + uz * uz));
+  const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
+  fv = a.f_double ? static_cast<const double*>(a.f)[fb + i]
+                  : (double)static_cast<const float*>(a.f)[fb + i];
+  cx = a.c0[x]; cy = a.c0[y]; cz = a.c0[z];
+}
+
+struct FeatState { double rho, ux, uy, uz, T, amp, irho; };
+
+__device__ __forceinline__ FeatState feat_state(const FeatArgs& a, int b) {
+  const double* P = a.part + (long)b * FCH * 6;
+  double m[5] = {0, 0, 0, 0, 0};
+  for (int c = 0; c < FCH; ++c)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) m[k] += P[c * 6 + k];
+  FeatState s;
+  double rho = m[0] * a.cw;
+  s.ux = m[1] * a.cw / rho; s.uy = m[2] * a.cw / rho; s.uz = m[3] * a.cw / rho;
+  double T = (2.0 / 3.0) * (m[4] * a.cw / rho - (s.ux * s.ux + s.uy * s.uy + s.uz * s.uz));
   if (!(rho > 1e-300)) rho = 1.0;
   if (!(T > 1e-6)) T = 1.0;
-  const double amp = rho / pow(M_PI * T, 1.5), irho = 1.0 / rho;
-  // sigma = rms of (f - M)/rho over the grid
-  double s2[5] = {0, 0, 0, 0, 0};
-  for (long i = t; i < n; i += NT) {
-    const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
-    const double fv = a.f_double ? static_cast<const double*>(a.f)[fb + i]
-                                 : (double)static_cast<const float*>(a.f)[fb + i];
-    const double dx = a.c0[x] - ux, dy = a.c0[y] - uy, dz = a.c0[z] - uz;
-    const double gv = (fv - amp * exp(-(dx * dx + dy * dy + dz * dz) / T)) * irho;
-    s2[0] += gv * gv;
-  }
-  block_sum5<NT>(s2, red);
-  const double sig = fmax(sqrt(red[0] / (double)n), 1e-300), isig = 1.0 / sig;
-  if (t == 0) a.qs[b] = rho * rho * sig;
-  for (long i = t; i < n; i += NT) {
-    const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
-    const double fv = a.f_double ? static_cast<const double*>(a.f)[fb + i]
-                                 : (double)static_cast<const float*>(a.f)[fb + i];
-    const double dx = a.c0[x] - ux, dy = a.c0[y] - uy, dz = a.c0[z] - uz;
-    const double r2 = (dx * dx + dy * dy + dz * dz) / T;
-    const double M = amp * exp(-r2);
-    const double g = (fv - M) * irho * isig, r = sqrt(r2);
-    const __nv_bfloat16 h[CIN] = {tobf((float)(fv * irho)), tobf((float)g),
-                                  tobf((float)(g * r)), tobf((float)(g * r2))};
-    const long pt = (long)b * n + i;
-    float xf[CIN];
-#pragma unroll
-    for (int k = 0; k < CIN; ++k) {
-      a.x0[pt * CIN + k] = h[k];
-      xf[k] = bf(h[k]);
+  s.rho = rho; s.T = T;
+  s.amp = rho / pow(M_PI * T, 1.5);
+  s.irho = 1.0 / rho;
+  return s;
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(256) fno_features_kernel(FeatArgs a) {
+  __shared__ double red[8 + 5 * 8];
+  __shared__ float wl[CIN * WD + WD];
+  __shared__ FeatState st;
+  __shared__ double sig_s;
+  const int ch = blockIdx.x, b = blockIdx.y, t = threadIdx.x, N = a.N;
+  const long n = (long)N * N * N, len = n / FCH, i0 = ch * len;
+  if (PASS >= 1) {
+    if (t == 0) st = feat_state(a, b);
+    if (PASS == 2 && t == 1) {
+      double s2 = 0;
+      const double* P = a.part + (long)b * FCH * 6;
+      for (int c = 0; c < FCH; ++c) s2 += P[c * 6 + 5];
+      sig_s = fmax(sqrt(s2 / (double)n), 1e-300);
     }
-    __nv_bfloat16* v = a.v0 + pt * WD;
+    if (PASS == 2)
+      for (int i = t; i < CIN * WD + WD; i += 256) wl[i] = bf(a.w16[a.L.P + i]);
+    __syncthreads();
+  }
+  if (PASS == 0) {
+    double s[5] = {0, 0, 0, 0, 0};
+    for (long i = i0 + t; i < i0 + len; i += 256) {
+      double fv, cx, cy, cz;
+      feat_load(a, b, i, fv, cx, cy, cz);
+      s[0] += fv; s[1] += fv * cx; s[2] += fv * cy; s[3] += fv * cz;
+      s[4] += fv * (cx * cx + cy * cy + cz * cz);
+    }
+    block_sum5<256>(s, red);
+    if (t < 5) a.part[((long)b * FCH + ch) * 6 + t] = red[t];
+  } else if (PASS == 1) {
+    const FeatState S = st;
+    double s[5] = {0, 0, 0, 0, 0};
+    for (long i = i0 + t; i < i0 + len; i += 256) {
+      double fv, cx, cy, cz;
+      feat_load(a, b, i, fv, cx, cy, cz);
+      const double dx = cx - S.ux, dy = cy - S.uy, dz = cz - S.uz;
+      const double g = (fv - S.amp * exp(-(dx * dx + dy * dy + dz * dz) / S.T)) * S.irho;
+      s[0] += g * g;
+    }
+    block_sum5<256>(s, red);
+    if (t == 0) a.part[((long)b * FCH + ch) * 6 + 5] = red[0];
+  } else {
+    const FeatState S = st;
+    const double isig = 1.0 / sig_s;
+    if (ch == 0 && t == 0) a.qs[b] = S.rho * S.rho * sig_s;
+    for (long i = i0 + t; i < i0 + len; i += 256) {
+      double fv, cx, cy, cz;
+      feat_load(a, b, i, fv, cx, cy, cz);
+      const double dx = cx - S.ux, dy = cy - S.uy, dz = cz - S.uz;
+      const double r2 = (dx * dx + dy * dy + dz * dz) / S.T;
+      const double g = (fv - S.amp * exp(-r2)) * S.irho * isig, r = sqrt(r2);
+      const __nv_bfloat16 h[CIN] = {tobf((float)(fv * S.irho)), tobf((float)g),
+                                    tobf((float)(g * r)), tobf((float)(g * r2))};
+      const long pt = (long)b * n + i;
+      float xf[CIN];
+      uint2 xs;
+      reinterpret_cast<__nv_bfloat16*>(&xs)[0] = h[0];
+      reinterpret_cast<__nv_bfloat16*>(&xs)[1] = h[1];
+      reinterpret_cast<__nv_bfloat16*>(&xs)[2] = h[2];
+      reinterpret_cast<__nv_bfloat16*>(&xs)[3] = h[3];
+      *reinterpret_cast<uint2*>(a.x0 + pt * CIN) = xs;
 #pragma unroll
-    for (int o = 0; o < WD; o += 2) {
-      float y0 = wl[CIN * WD + o], y1 = wl[CIN * WD + o + 1];
+      for (int k = 0; k < CIN; ++k) xf[k] = bf(h[k]);
+      uint4* v = reinterpret_cast<uint4*>(a.v0 + pt * WD);
 #pragma unroll
-      for (int k = 0; k < CIN; ++k) {
-        y0 += xf[k] * wl[k * WD + o];
-        y1 += xf[k] * wl[k * WD + o + 1];
+      for (int q = 0; q < WD / 8; ++q) {
+        uint4 pk;
+        __nv_bfloat162* p2 = reinterpret_cast<__nv_bfloat162*>(&pk);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int o = q * 8 + 2 * e;
+          float y0 = wl[CIN * WD + o], y1 = wl[CIN * WD + o + 1];
+#pragma unroll
+          for (int k = 0; k < CIN; ++k) {
+            y0 += xf[k] * wl[k * WD + o];
+            y1 += xf[k] * wl[k * WD + o + 1];
+          }
+          p2[e] = __floats2bfloat162_rn(y0, y1);
+        }
+        v[q] = pk;
       }
-      *reinterpret_cast<__nv_bfloat162*>(v + o) = __floats2bfloat162_rn(y0, y1);
     }
   }
 }
@@ -180,7 +239,8 @@ __global__ void __launch_bounds__(NT) fno_features_kernel(FeatArgs a) {
 // Truncated DFT along one axis: in [outer][LIN][inner] -> out [outer][LOUT][inner],
 // out[k] = sum_j T[k][j] in[j] with a complex table T [LOUT][LIN].
 // IN: 0 BF16 real, 1 FP32 real, 2 complex FP32.
-// OUT: 0 complex FP32, 1 Re -> FP32 store, 2 Re -> FP32 accumulate.
+// OUT: 0 complex FP32, 1 Re -> FP32 store, 2 Re -> FP32 accumulate,
+//      3 Re -> BF16 store.
 // One thread per (outer, inner) pencil; consecutive threads take consecutive
 // inner indices, so every load and store is coalesced.
 // ---------------------------------------------------------------------------
@@ -203,7 +263,7 @@ fno_dft_kernel(const void* in, void* out, const float2* table, long outer,
     else if (IN == 1) x[j] = make_float2(static_cast<const float*>(in)[idx], 0.f);
     else x[j] = static_cast<const float2*>(in)[idx];
   }
-#pragma unroll 2
+#pragma unroll 4
   for (int k = 0; k < LOUT; ++k) {
     float re = 0.f, im = 0.f;
 #pragma unroll
@@ -211,16 +271,17 @@ fno_dft_kernel(const void* in, void* out, const float2* table, long outer,
       const float2 w = tb[k * LIN + j];
       if (IN == 2) {
         re += w.x * x[j].x - w.y * x[j].y;
-        im += w.x * x[j].y + w.y * x[j].x;
+        if (OUT == 0) im += w.x * x[j].y + w.y * x[j].x;
       } else {
         re += w.x * x[j].x;
-        im += w.y * x[j].x;
+        if (OUT == 0) im += w.y * x[j].x;
       }
     }
     const long idx = (o * LOUT + k) * inner + i;
     if (OUT == 0) static_cast<float2*>(out)[idx] = make_float2(re, im);
     else if (OUT == 1) static_cast<float*>(out)[idx] = re;
-    else static_cast<float*>(out)[idx] += re;
+    else if (OUT == 2) static_cast<float*>(out)[idx] += re;
+    else static_cast<__nv_bfloat16*>(out)[idx] = tobf(re);
   }
 }
 
@@ -290,7 +351,7 @@ fno_mix_kernel(const float2* in, const float2* in2, const __nv_bfloat16* W,
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 fno_dense_fwd_kernel(const __nv_bfloat16* x, const __nv_bfloat16* w16, long offD,
-                     long offd, const float* U, __nv_bfloat16* y,
+                     long offd, const __nv_bfloat16* U, __nv_bfloat16* y,
                      __nv_bfloat16* v, long R, int act) {
   __shared__ float Ds[WD * WD + WD];
   for (int i = threadIdx.x; i < WD * WD; i += blockDim.x) Ds[i] = bf(w16[offD + i]);
@@ -311,10 +372,10 @@ fno_dense_fwd_kernel(const __nv_bfloat16* x, const __nv_bfloat16* w16, long offD
       xi[q * 8 + 2 * k + 1] = f.y;
     }
   }
-  const float* Ur = U + r * WD;
+  const __nv_bfloat16* Ur = U + r * WD;
 #pragma unroll 4
   for (int o = 0; o < WD; o += 2) {
-    float a0 = Ds[WD * WD + o] + Ur[o], a1 = Ds[WD * WD + o + 1] + Ur[o + 1];
+    float a0 = Ds[WD * WD + o] + bf(Ur[o]), a1 = Ds[WD * WD + o + 1] + bf(Ur[o + 1]);
 #pragma unroll
     for (int i = 0; i < WD; ++i) {
       a0 += xi[i] * Ds[i * WD + o];
@@ -535,38 +596,53 @@ struct OutArgs {
   const float* out; const double* qs; double sQ;
   const double* c0; double cw; int N; double Ginv[25];
   void* Q; int q_double; const int32_t* dst_slots; int dst_base;
+  double* part;  // scratch [B][FCH][6]
 };
 
-template <int NT>
-__global__ void __launch_bounds__(NT) fno_output_kernel(OutArgs a) {
-  __shared__ double red[8 + 5 * (NT / 32)];
-  const int b = blockIdx.x, t = threadIdx.x, N = a.N;
-  const long n = (long)N * N * N;
+// Two grid-wide passes, grid (FCH chunks, B samples): partial moments of the
+// raw output (FP64), then every CTA reduces them in a fixed order, forms the
+// multipliers and writes its chunk.
+template <int PASS>
+__global__ void __launch_bounds__(256) fno_output_kernel(OutArgs a) {
+  __shared__ double red[8 + 5 * 8];
+  __shared__ double lam_s[5];
+  const int ch = blockIdx.x, b = blockIdx.y, t = threadIdx.x, N = a.N;
+  const long n = (long)N * N * N, len = n / FCH, i0 = ch * len;
   const double sc = a.qs[b] * a.sQ;
   const float* o = a.out + (long)b * n;
-  double s[5] = {0, 0, 0, 0, 0};
-  for (long i = t; i < n; i += NT) {
-    const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
-    const double q = sc * o[i] * a.cw;
-    const double cx = a.c0[x], cy = a.c0[y], cz = a.c0[z];
-    s[0] += q; s[1] += q * cx; s[2] += q * cy; s[3] += q * cz;
-    s[4] += q * (cx * cx + cy * cy + cz * cz);
+  if (PASS == 0) {
+    double s[5] = {0, 0, 0, 0, 0};
+    for (long i = i0 + t; i < i0 + len; i += 256) {
+      const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
+      const double q = sc * o[i] * a.cw;
+      const double cx = a.c0[x], cy = a.c0[y], cz = a.c0[z];
+      s[0] += q; s[1] += q * cx; s[2] += q * cy; s[3] += q * cz;
+      s[4] += q * (cx * cx + cy * cy + cz * cz);
+    }
+    block_sum5<256>(s, red);
+    if (t < 5) a.part[((long)b * FCH + ch) * 6 + t] = red[t];
+    return;
   }
-  block_sum5<NT>(s, red);
-  double lam[5];
+  if (t < 5) {
+    double m[5] = {0, 0, 0, 0, 0};
+    const double* P = a.part + (long)b * FCH * 6;
+    for (int c = 0; c < FCH; ++c)
 #pragma unroll
-  for (int j = 0; j < 5; ++j) {
+      for (int k = 0; k < 5; ++k) m[k] += P[c * 6 + k];
     double l = 0;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) l += a.Ginv[j * 5 + k] * red[k];
-    lam[j] = l;
+    for (int k = 0; k < 5; ++k) l += a.Ginv[t * 5 + k] * m[k];
+    lam_s[t] = l;
   }
+  __syncthreads();
+  const double l0 = lam_s[0], l1 = lam_s[1], l2 = lam_s[2], l3 = lam_s[3],
+               l4 = lam_s[4];
   const long qb = (long)(a.dst_slots ? a.dst_slots[b] : a.dst_base + b) * n;
-  for (long i = t; i < n; i += NT) {
+  for (long i = i0 + t; i < i0 + len; i += 256) {
     const int x = (int)(i / (N * N)), y = (int)((i / N) % N), z = (int)(i % N);
     const double cx = a.c0[x], cy = a.c0[y], cz = a.c0[z];
-    const double q = sc * o[i] - (lam[0] + lam[1] * cx + lam[2] * cy + lam[3] * cz +
-                                  lam[4] * (cx * cx + cy * cy + cz * cz));
+    const double q = sc * o[i] - (l0 + l1 * cx + l2 * cy + l3 * cz +
+                                  l4 * (cx * cx + cy * cy + cz * cz));
     if (a.q_double) static_cast<double*>(a.Q)[qb + i] += q;
     else static_cast<float*>(a.Q)[qb + i] += (float)q;
   }
@@ -624,7 +700,7 @@ struct TcArgs {
   const __nv_bfloat16* w16; // parameters (BF16)
   long offW, offb;          // weight [32][NC], bias [NC]
   long offq2, offq2b;       // projection only
-  const float* U;           // dense: [R][32] spectral part
+  const __nv_bfloat16* U;   // dense: [R][32] spectral part (BF16)
   __nv_bfloat16* y;         // dense: pre-activation out (may be null)
   __nv_bfloat16* v;         // dense: activation out
   float* out;               // projection: [R]
@@ -746,11 +822,16 @@ __global__ void __launch_bounds__(128) fno_tc_kernel(TcArgs a) {
           : "r"(lane_addr));
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
       if (row < a.R) {
-        const float4* Ur = reinterpret_cast<const float4*>(a.U + row * WD);
+        const uint4* Ur = reinterpret_cast<const uint4*>(a.U + row * WD);
+        uint4 ub[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ub[c] = Ur[c];
         uint4 yo[4], vo[4];
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-          const float4 u = Ur[c];
+          const __nv_bfloat162* u2 = reinterpret_cast<const __nv_bfloat162*>(&ub[c >> 1]) + (c & 1) * 2;
+          const float2 ua = __bfloat1622float2(u2[0]), ub2 = __bfloat1622float2(u2[1]);
+          const float4 u = make_float4(ua.x, ua.y, ub2.x, ub2.y);
           const float y0 = __uint_as_float(r[4 * c]) + ep[4 * c] + u.x;
           const float y1 = __uint_as_float(r[4 * c + 1]) + ep[4 * c + 1] + u.y;
           const float y2 = __uint_as_float(r[4 * c + 2]) + ep[4 * c + 2] + u.z;

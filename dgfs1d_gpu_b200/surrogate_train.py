@@ -8,9 +8,12 @@
 * ``SurrogateBoltzmann``: the Boltzmann-operator hook of ``DGFSABstd1D``.
   The surrogate replaces Q(f, f) except that every k-th call evaluates the
   plain operator as well; the plain result is used at those calls, and the
-  relative L2 residual |Q_sur - Q_plain| / |Q_plain| judges the surrogate:
+  relative L2 residual |Q_pred - Q_plain| / |Q_plain| judges the prediction:
   above ``tol`` the plain operator serves every call until a later check
-  passes.
+  passes.  With ``correct=True`` the prediction between checks is the
+  surrogate plus the defect d = Q_plain - Q_sur measured at the last check
+  (the residual then judges Q_sur + d_previous); a steady state of the
+  coupled scheme is then a steady state of the plain one.
 * ``run_to_steady``: steps a solver until the relative change of its FP64
   bulk moments per step falls below a tolerance.
 """
@@ -67,16 +70,23 @@ def harvest(solver, nsteps, every):
 
 
 def train(net, f, Q, steps, batch=24, lr=2e-3, lr_final=1e-5, seed=0,
-          time_budget=None, log_every=100):
-    """Adam on random mini-batches; returns [(step, mean loss)]."""
+          time_budget=None, log_every=100, tail=0, tail_frac=0.5):
+    """Adam on random mini-batches; returns [(step, mean loss)].
+
+    With ``tail`` > 0 a fraction ``tail_frac`` of every batch is drawn from
+    the last ``tail`` rows (e.g. states harvested along the target run)."""
     g = torch.Generator(device='cpu')
     g.manual_seed(int(seed))
     n = f.shape[0]
+    nt = int(round(batch * tail_frac)) if tail > 0 else 0
     hist, t0 = [], time.time()
     fb = torch.empty((batch, f.shape[1]), dtype=torch.float64, device=f.device)
     qb = torch.empty_like(fb)
     for s in range(steps):
-        idx = torch.randint(0, n, (batch,), generator=g).to(f.device)
+        idx = torch.randint(0, n, (batch,), generator=g)
+        if nt:
+            idx[:nt] = n - tail + torch.randint(0, tail, (nt,), generator=g)
+        idx = idx.to(f.device)
         torch.index_select(f, 0, idx, out=fb)
         torch.index_select(Q, 0, idx, out=qb)
         lr_s = lr_final + 0.5 * (lr - lr_final) * (1 + math.cos(math.pi * s / steps))
@@ -100,14 +110,17 @@ def residuals(net, op, f, batch=24):
 class SurrogateBoltzmann:
     """Boltzmann-operator hook for DGFSABstd1D (see the module docstring)."""
 
-    def __init__(self, solver, net, k=10, tol=1e-3):
+    def __init__(self, solver, net, k=10, tol=1e-3, correct=False):
         self.solver, self.net, self.k, self.tol = solver, net, int(k), float(tol)
+        self.correct = bool(correct)
         self.calls = 0
         self.fallback = False
         self.checks = []        # (call, residual)
         self.plain_calls = 0
         self._qp = torch.zeros_like(solver.u)
         self._qs = torch.zeros_like(solver.u)
+        self._d = torch.zeros_like(solver.u) if correct else None
+        self._have_d = False
 
     def __call__(self, t, u_in, u_out):
         s = self.solver
@@ -118,9 +131,13 @@ class SurrogateBoltzmann:
             self._qs.zero_()
             s.sm.fs_batch(u_in, self._qp, s.src, s.dst)
             self.net.eval(u_in, self._qs, src=s.src, dst=s.dst)
-            res = float(torch.linalg.norm(self._qs - self._qp)
+            pred = self._qs + self._d if (self.correct and self._have_d) else self._qs
+            res = float(torch.linalg.norm(pred - self._qp)
                         / torch.linalg.norm(self._qp))
             self.checks.append((self.calls, res))
+            if self.correct:
+                torch.sub(self._qp, self._qs, out=self._d)
+                self._have_d = True
             self.fallback = res > self.tol
             self.plain_calls += 1
             u_out += self._qp
@@ -129,13 +146,16 @@ class SurrogateBoltzmann:
             s.sm.fs_batch(u_in, u_out, s.src, s.dst)
         else:
             self.net.eval(u_in, u_out, src=s.src, dst=s.dst)
+            if self.correct:
+                u_out += self._d
 
     def stats(self):
         res = [r for _, r in self.checks]
         return dict(calls=self.calls, plain_calls=self.plain_calls,
                     checks=len(res),
+                    residual_first=res[0] if res else None,
                     residual_median=float(np.median(res)) if res else None,
-                    residual_max=float(np.max(res)) if res else None,
+                    residual_last=res[-1] if res else None,
                     fallback_fraction=self.plain_calls / max(self.calls, 1))
 
 

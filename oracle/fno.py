@@ -7,7 +7,7 @@ module is its defining restatement: the network, the loss and the exact
 gradients in float64 NumPy.  Features: [f/rho, g, g r, g r^2] with
 g = (f - M)/(rho sigma), sigma = rms((f - M)/rho), r = |c - u|/sqrt(T);
 output scale rho^2 sigma q_scale.  With ``emulate_bf16`` the activations that the
-GPU stores in BF16 (features, v_l, y_l) are rounded the same way, so that the
+GPU stores in BF16 (features, v_l, y_l, the spectral output U) are rounded the same way, so that the
 two agree to FP32-accumulation differences; without it the module is a plain
 float64 network, which ``tests/test_fno_oracle.py`` pins against central
 finite differences.
@@ -134,7 +134,7 @@ class FNO:
             V = self.dft(v[l], self.F)
             Vh.append(V)
             Uh = np.einsum('bmi,mio->bmo', V.reshape(B, K ** 3, WD), self.W(l))
-            U = self.idft(Uh.reshape(B, K, K, K, WD), G).real
+            U = self._r(self.idft(Uh.reshape(B, K, K, K, WD), G).real)
             yl = self._r(v[l] @ w[f'D{l}'].reshape(WD, WD) + w[f'd{l}'] + U)
             y.append(yl)
             v.append(self._r(gelu(yl)) if l < 3 else yl)
