@@ -155,6 +155,41 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def surrogate_line(torch, prm, fd, op32, op64, timed, args):
+    from dgfs1d_gpu_b200.surrogate import FNOSurrogate
+    from dgfs1d_gpu_b200 import surrogate_train as st
+    import time as _t
+    net = FNOSurrogate(32, prm['L'], q_scale=1.0, max_batch=24, seed=5)
+    t0 = _t.time()
+    fm = st.perturbed_maxwellians(prm['c0'], 4096, 20261203)
+    # Couette-like states: the bench family with other seeds
+    from dgfs1d_gpu_b200.workloads import couette_distributions
+    fc = torch.tensor(np.concatenate([couette_distributions(prm['c0'], 24, seed=s)
+                                      for s in range(64)]), device='cuda')
+    f_tr = torch.cat([fm, fc])
+    q_tr = st.operator_pairs(op32, f_tr)
+    hist = st.train(net, f_tr, q_tr, 100000, batch=24, lr=2e-3,
+                    time_budget=args.surrogate_train_s, log_every=500,
+                    tail=fc.shape[0], tail_frac=0.5)
+    train_s = _t.time() - t0
+    del fm, fc, f_tr, q_tr
+    Qs = torch.zeros_like(fd)
+    net.eval(fd, Qs)
+    Q64 = torch.zeros_like(fd)
+    op64.eval(fd, Q64)
+    torch.cuda.synchronize()
+    err = float(torch.linalg.norm(Qs - Q64) / torch.linalg.norm(Q64))
+    Q = torch.zeros_like(fd)
+    ms = timed(lambda: net.eval(fd, Q), max(3, args.steps // 4), 3)
+    return {'value': fd.shape[0] / (ms * 1e-3), 'unit': UNIT, 'ms_per_step': ms,
+            'err_vs_fp64_rel_l2': err, 'dtype': 'bf16 (FP32 accumulate)',
+            'train_seconds': train_s, 'train_steps': hist[-1][0],
+            'train_loss_last': hist[-1][1],
+            'train_pairs': '4096 perturbed Maxwellians + 1536 Couette-like states',
+            'tensor_cores': 'tcgen05.mma kind::f16 (dense layers, projection)',
+            'error_flag': net.device_error()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -162,6 +197,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='native', choices=['native', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-surrogate', action='store_true')
+    ap.add_argument('--surrogate-train-s', type=float, default=40.0)
     ap.add_argument('--kernel-only', action='store_true',
                     help='run only warm-up + timed FP32 evaluations (for ncu '
                          'launch lists); prints ms per step')
@@ -278,6 +315,12 @@ def main():
 
     fma_peak = fp32_fma_peak(torch)
 
+    # learned surrogate (FNO, BF16 tensor-core dense layers): trained here for
+    # a bounded time on operator pairs, then timed and compared with FP64
+    sur = None
+    if not args.no_surrogate:
+        sur = surrogate_line(torch, prm, fd, op32, op64, timed, args)
+
     # uneven multi-problem batch: 6 VHS problems (N=16/24/32) + 2 VSS
     # mixtures, one CUDA graph launch per stage vs the same launches issued
     # one after another on one stream
@@ -312,23 +355,34 @@ def main():
         peak_src = 'measured' if 'hbm_gbs' in peaks else 'fallback'
         n = 32 ** 3
         Nrho, Mu = 16, 6
-        # terms kernel, per launch: read F_g (n complex FP32) per eval and
-        # b1w (Nrho*n FP32) once, write H (Nrho*n complex FP32) per eval
-        alg_bytes = E * (n * 8 + Nrho * n * 8) + Nrho * n * 4
-        # algorithmic flops of the terms kernel per eval: 2*Mu*Nrho inverse
-        # and Nrho forward 3-D FFTs (5 n log2 n each) + pointwise combine
+        # terms kernel, per launch: per eval read F_g (n complex FP32) and the
+        # Nyquist-plane transforms (Nrho*Mu*3*N^2 complex FP32), write the
+        # packed radial-pair spectra H (Nrho/2 * n complex FP32); b1w
+        # (Nrho*n FP32) once
+        alg_bytes = E * (n * 8 + Nrho * Mu * 3 * 32 * 32 * 8 + Nrho // 2 * n * 8) \
+            + Nrho * n * 4
+        # flops per eval as executed: Mu*Nrho packed inverse and Nrho/2
+        # packed forward 3-D FFTs (5 n log2 n each) + the pointwise combine
+        # (~40 flops per point and term)
         fft = 5 * n * np.log2(n)
-        alg_flops = E * ((2 * Mu * Nrho + Nrho) * fft + 2 * Mu * Nrho * n * 30)
+        alg_flops = E * ((Mu * Nrho + Nrho // 2) * fft + Mu * Nrho * n * 40)
         evals = E * world
+        # DRAM bytes per launch of the terms kernel from the committed ncu
+        # summary (dram__bytes_read.sum + dram__bytes_write.sum, one capture)
         traffic = None
-        tp = os.path.join(ROOT, 'profiles', 'vhs_terms_fp32_traffic.json')
+        tp = os.path.join(ROOT, 'profiles', 'vhs_terms_fp32_n32_24pts.md')
         if os.path.exists(tp):
-            traffic = json.load(open(tp)).get('bytes_per_launch_24_evals')
+            import re
+            txt = open(tp).read()
+            rd = re.search(r'dram__bytes_read\.sum \| ([0-9.]+) MB', txt)
+            wr = re.search(r'dram__bytes_write\.sum \| ([0-9.]+) MB', txt)
+            if rd and wr:
+                traffic = (float(rd.group(1)) + float(wr.group(1))) * 1e6
         cores = os.cpu_count() or 1
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             rate, ns, dt = cpu_oracle_rate(prm, f, budget_s=12.0,
-                                           max_evals=3)
+                                           max_evals=48)
             cpu = {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'port',
                    'sample': f'{ns} single-point evals ({dt:.1f} s) of the '
                              'NumPy/SciPy oracle of this workload '
@@ -370,11 +424,12 @@ def main():
                                   'terms', 'epilogue'],
                                  [round(float(x), 4) for x in stage])),
             'uneven_batch': batch,
+            'surrogate': sur,
             'autotune_terms_ms': {str(k): round(v, 4) for k, v in tune.items()},
             'terms_cluster': op32.variant,
             'cpu_baseline': cpu,
             'clocks': clk.summary(),
-            'gpu_launches': 5 * args.steps,
+            'gpu_launches': 6 * args.steps,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

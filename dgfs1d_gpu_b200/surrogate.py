@@ -177,3 +177,27 @@ class FNOSurrogate:
             self.close()
         except Exception:
             pass
+
+
+def _main():
+    """``python -m dgfs1d_gpu_b200.surrogate [repeats]``: build an N=32
+    surrogate (untrained weights) and evaluate it on the 24 benchmark points
+    `repeats` times -- the launch sequence that profiles of the surrogate
+    kernels capture."""
+    import sys
+    from . import build
+    from .workloads import couette_distributions, vhs_mesh_params
+    build.build()
+    reps = int(sys.argv[1]) if len(sys.argv) > 1 else 2
+    prm = vhs_mesh_params(32, 12, 16, 6.0, True)
+    net = FNOSurrogate(32, prm['L'], q_scale=1.0, max_batch=24, seed=1)
+    f = torch.tensor(couette_distributions(prm['c0'], 24), device='cuda')
+    Q = torch.zeros_like(f)
+    for _ in range(reps):
+        net.eval(f, Q)
+    torch.cuda.synchronize()
+    print('surrogate evaluations done:', reps, 'error flag', net.device_error())
+
+
+if __name__ == '__main__':
+    _main()
