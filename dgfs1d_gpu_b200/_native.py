@@ -39,7 +39,7 @@ class VssDesc(ctypes.Structure):
         ('L', ctypes.c_double), ('qz', _c_dp), ('qw', _c_dp), ('sz', _c_dp),
         ('sw', ctypes.c_double), ('szpre', _c_dp), ('masses', _c_dp),
         ('gamma', _c_dp), ('eta', _c_dp), ('prefac', _c_dp),
-        ('max_evals', ctypes.c_int32),
+        ('max_evals', ctypes.c_int32), ('precision', ctypes.c_int32),
     ]
 
 

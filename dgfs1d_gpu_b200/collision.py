@@ -143,13 +143,18 @@ class VHSOperator:
 
 
 class VSSOperator:
-    """Batched binary-mixture VSS Q_pq(f_p, f_q) (``vss``), FP64.
+    """Batched binary-mixture VSS Q_pq(f_p, f_q) (``vss``).
 
     gamma, eta, prefac: (nspcs, nspcs) arrays (pair pq at [p, q]).
+    precision: 'fp64' (the reference's) or 'fp32' (FP32 transforms of
+    f - M; Maxwellian parts, radial sum, final transform and loss in FP64).
     """
 
     def __init__(self, N, L, qz, qw, sz, sw, szpre, masses, gamma, eta,
-                 prefac, max_evals=64):
+                 prefac, max_evals=64, precision='fp64'):
+        if precision not in _PREC:
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        self.precision = precision
         self.N, self.n = int(N), int(N) ** 3
         ns = len(masses)
         self.nspcs = ns
@@ -164,6 +169,7 @@ class VSSOperator:
         d.masses, d.gamma, d.eta, d.prefac = _dptr(m_), _dptr(g_), _dptr(e_), \
             _dptr(p_)
         d.max_evals = int(max_evals)
+        d.precision = _PREC[precision]
         h = ctypes.c_void_p()
         nat.check(nat.lib().dgfs_vss_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h

@@ -1071,14 +1071,29 @@ struct VssPair {
   double2* b = nullptr;    // [Nrho][M][n]
   double2* c = nullptr;    // [n]
   double2* ph = nullptr;   // [Nrho][M][2][3][N]
+  float2* b32 = nullptr;   // FP32 mode: FP32 copies of b and ph
+  float2* ph32 = nullptr;
   double prefac = 0;
 };
 
 struct dgfs_vss_s {
   int N = 0, Nrho = 0, M = 0, nspcs = 0, n = 0, max_evals = 0;
+  int precision = DGFS_PREC_FP64;
   double* w = nullptr;     // [Nrho] w_r s_w / n
   VssPair pair[16];
   double2* F[2] = {nullptr, nullptr};  // [E][n] spectra of the two inputs
+  // FP32 mode scratch (Maxwellian split)
+  double* c0 = nullptr;                // [N]
+  double* b2dummy = nullptr;           // [n] unused real loss kernel
+  float2* Fg[2] = {nullptr, nullptr};  // [E][n]
+  double2* mhat[2] = {nullptr, nullptr};
+  double* mom[2] = {nullptr, nullptr};
+  double* ReLf = nullptr;              // [E][n]
+  float2* uv = nullptr;                // [E][T][2][3][N]
+  double2* hh = nullptr;               // [E][T][3][N]
+  double2* GM = nullptr;               // [E][n]
+  float2* H = nullptr;                 // [E][Nrho][n]
+  double cw = 0;
 };
 
 static void free_vss(dgfs_vss_s* h) {
@@ -1086,11 +1101,21 @@ static void free_vss(dgfs_vss_s* h) {
     if (p.b) cudaFree(p.b);
     if (p.c) cudaFree(p.c);
     if (p.ph) cudaFree(p.ph);
+    if (p.b32) cudaFree(p.b32);
+    if (p.ph32) cudaFree(p.ph32);
   }
-  if (h->w) cudaFree(h->w);
-  for (auto* f : h->F)
-    if (f) cudaFree(f);
+  void* ptrs[] = {h->w, h->F[0], h->F[1], h->c0, h->b2dummy, h->Fg[0], h->Fg[1],
+                  h->mhat[0], h->mhat[1], h->mom[0], h->mom[1], h->ReLf, h->uv,
+                  h->hh, h->GM, h->H};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
   delete h;
+}
+
+// FP32 copies of a pair's weights and phases
+__global__ void vss_to_fp32_kernel(const double2* in, float2* out, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_float2((float)in[i].x, (float)in[i].y);
 }
 
 template <int N> struct VssClusters;
@@ -1098,6 +1123,12 @@ template <> struct VssClusters<8> { static constexpr int c = 1; };
 template <> struct VssClusters<16> { static constexpr int c = 2; };
 template <> struct VssClusters<24> { static constexpr int c = 6; };
 template <> struct VssClusters<32> { static constexpr int c = 16; };
+// FP32 terms kernel: four FP32 slabs per CTA
+template <int N> struct VssClusters32;
+template <> struct VssClusters32<8> { static constexpr int c = 1; };
+template <> struct VssClusters32<16> { static constexpr int c = 2; };
+template <> struct VssClusters32<24> { static constexpr int c = 3; };
+template <> struct VssClusters32<32> { static constexpr int c = 8; };
 
 template <int N>
 static int vss_setup_pair(dgfs_vss_s* h, const dgfs_vss_desc* d, int p, int q,
@@ -1174,9 +1205,12 @@ extern "C" int dgfs_vss_create(const dgfs_vss_desc* d, dgfs_vss_handle* out) {
   if (d->N != 8 && d->N != 16 && d->N != 24 && d->N != 32)
     return fail(DGFS_ERR_UNSUPPORTED, "VSS: N must be 8, 16, 24 or 32");
   if (int rc = ensure_twiddles()) return rc;
+  if (d->precision != DGFS_PREC_FP64 && d->precision != DGFS_PREC_FP32)
+    return fail(DGFS_ERR_INVALID, "unknown precision");
   auto* h = new dgfs_vss_s();
   h->N = d->N; h->n = d->N * d->N * d->N; h->Nrho = d->Nrho; h->M = d->M;
   h->nspcs = d->nspcs; h->max_evals = d->max_evals;
+  h->precision = d->precision;
   std::vector<double> w(d->Nrho);
   for (int r = 0; r < d->Nrho; ++r) w[r] = d->qw[r] * d->sw / h->n;
   int rc = upload(&h->w, w);
@@ -1195,6 +1229,35 @@ extern "C" int dgfs_vss_create(const dgfs_vss_desc* d, dgfs_vss_handle* out) {
       e1 = cudaMalloc(&h->F[1], sizeof(double2) * (size_t)h->max_evals * h->n);
     if (e1 != cudaSuccess)
       rc = fail(DGFS_ERR_CUDA, std::string("allocation: ") + cudaGetErrorString(e1));
+  }
+  if (!rc && h->precision == DGFS_PREC_FP32) {
+    const size_t E = h->max_evals, n = h->n, N = h->N, T = (size_t)h->Nrho * h->M;
+    cudaError_t e1 = cudaSuccess;
+    auto A = [&](auto** q, size_t cnt) {
+      if (e1 == cudaSuccess) e1 = cudaMalloc((void**)q, cnt * sizeof(**q));
+    };
+    for (int s2 = 0; s2 < 2; ++s2) {
+      A(&h->Fg[s2], E * n); A(&h->mhat[s2], E * 3 * N); A(&h->mom[s2], E * 5);
+    }
+    A(&h->ReLf, E * n); A(&h->uv, E * T * 6 * N); A(&h->hh, E * T * 3 * N);
+    A(&h->GM, E * n); A(&h->H, E * h->Nrho * n); A(&h->b2dummy, n);
+    for (int pq = 0; pq < h->nspcs * h->nspcs; ++pq) {
+      A(&h->pair[pq].b32, T * n); A(&h->pair[pq].ph32, T * 6 * N);
+    }
+    if (e1 == cudaSuccess) {
+      for (int pq = 0; pq < h->nspcs * h->nspcs; ++pq) {
+        vss_to_fp32_kernel<<<(unsigned)((T * n + 255) / 256), 256>>>(
+            h->pair[pq].b, h->pair[pq].b32, T * n);
+        vss_to_fp32_kernel<<<(unsigned)((T * 6 * N + 255) / 256), 256>>>(
+            h->pair[pq].ph, h->pair[pq].ph32, T * 6 * N);
+      }
+      e1 = cudaDeviceSynchronize();
+    }
+    std::vector<double> c0(N);
+    for (size_t i = 0; i < N; ++i) c0[i] = -d->L + d->L / N + i * (2.0 * d->L / N);
+    h->cw = std::pow(2.0 * d->L / N, 3);
+    if (e1 == cudaSuccess) rc = upload(&h->c0, c0);
+    else rc = fail(DGFS_ERR_CUDA, std::string("FP32 scratch: ") + cudaGetErrorString(e1));
   }
   if (rc) { free_vss(h); return rc; }
   *out = h;
@@ -1215,6 +1278,55 @@ static int vss_run(dgfs_vss_s* h, int p, int q, const void* fp, const void* fq,
   using G = Geo<N, C>;
   int rc;
   const VssPair& P = h->pair[p * h->nspcs + q];
+  if (h->precision == DGFS_PREC_FP32) {
+    constexpr int CPRO = VhsClusters<N>::cpro;
+    constexpr int CEPI = VhsClusters<N>::cepi;
+    constexpr int C3 = VssClusters32<N>::c;
+    using GPRO = Geo<N, CPRO>;
+    using GEPI = Geo<N, CEPI>;
+    using G3 = Geo<N, C3>;
+    const int T = h->Nrho * h->M;
+    // prologues: F_g, Maxwellian spectra of f_p and f_q; the f_q pass also
+    // leaves the loss Re IFFT(c G) (complex loss kernel)
+    for (int s2 = 0; s2 < 2; ++s2) {
+      VhsPrologueArgs a{};
+      a.f = s2 == 0 ? fp : fq; a.f_double = f_double; a.src_slots = ss; a.src_base = sb;
+      a.c0 = h->c0; a.b2 = h->b2dummy; a.b2c = P.c; a.cw = h->cw; a.split = 1;
+      a.Fg = h->Fg[s2]; a.ReLf = h->ReLf; a.mhat = h->mhat[s2]; a.moments = h->mom[s2];
+      a.Fny = nullptr;
+      const size_t smem = 2 * slab_bytes(N, CPRO, sizeof(double2)) +
+                          3 * N * sizeof(double2) + 8 * sizeof(double);
+      if ((rc = launch_cluster(vhs_prologue_kernel<N, CPRO>, dim3(CPRO, nevals),
+                               dim3(GPRO::NT), CPRO, smem, st, a)))
+        return rc;
+    }
+    VssTablesArgs ta{};
+    ta.mhat_p = h->mhat[0]; ta.mhat_q = h->mhat[1]; ta.ph = P.ph; ta.uv = h->uv;
+    ta.hh = h->hh; ta.T = T; ta.nevals = nevals;
+    if ((rc = launch_plain(vss_tables_kernel<N>, dim3((nevals * T * 3 + 127) / 128),
+                           dim3(128), 0, st, ta)))
+      return rc;
+    VssGainArgs ga{};
+    ga.hh = h->hh; ga.b = P.b; ga.w = h->w; ga.GM = h->GM; ga.Nrho = h->Nrho; ga.M = h->M;
+    if ((rc = launch_plain(vss_maxwell_gain_kernel<N>,
+                           dim3((h->n + 255) / 256, nevals), dim3(256), 0, st, ga)))
+      return rc;
+    VssTerms32Args tt{};
+    tt.Fgp = h->Fg[0]; tt.Fgq = h->Fg[1]; tt.ph = P.ph32; tt.uv = h->uv; tt.b = P.b32;
+    tt.w = h->w; tt.H = h->H; tt.Nrho = h->Nrho; tt.M = h->M;
+    const size_t smem3 = 4 * slab_bytes(N, C3, sizeof(float2)) + 12 * N * sizeof(float2);
+    if ((rc = launch_cluster(vss_terms32_kernel<N, C3>, dim3(C3, h->Nrho, nevals),
+                             dim3(G3::NT), C3, smem3, st, tt)))
+      return rc;
+    VhsEpilogueArgs ea{};
+    ea.H = h->H; ea.h_double = 0; ea.GM = h->GM; ea.ReLf = h->ReLf; ea.f = fp;
+    ea.f_double = f_double; ea.src_slots = ss; ea.src_base = sb; ea.Q = Q;
+    ea.q_double = q_double; ea.dst_slots = ds; ea.dst_base = db;
+    ea.prefac = P.prefac; ea.Nrho = h->Nrho; ea.project = 0; ea.c0 = h->c0; ea.cw = h->cw;
+    const size_t smemE = 2 * slab_bytes(N, CEPI, sizeof(double2));
+    return launch_cluster(vhs_epilogue_kernel<N, CEPI>, dim3(CEPI, nevals),
+                          dim3(GEPI::NT), CEPI, smemE, st, ea);
+  }
   for (int s = 0; s < 2; ++s) {
     Fft3Args fa{};
     fa.f = s == 0 ? fp : fq; fa.f_double = f_double; fa.slots = ss; fa.base = sb;

@@ -42,6 +42,8 @@ struct VhsPrologueArgs {
   int src_base;               // slot(i) = src_slots ? src_slots[i] : src_base+i
   const double* c0;           // [N] velocity grid (x, y and z)
   const double* b2;           // [n] loss kernel b2(l)
+  const double2* b2c;         // [n] complex loss kernel (used instead of b2
+                              // when set: the VSS c_pq)
   double cw;                  // velocity cell volume
   int split;                  // 1: Maxwellian split (FP32 mode)
   void* Fg;                   // out [nevals][n] complex (float2 if split else double2)
@@ -246,16 +248,22 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
       g.x = (float)(Fv.x - mm.x);
       g.y = (float)(Fv.y - mm.y);
       static_cast<float2*>(a.Fg)[gbase + j] = g;
-      float2* ny = a.Fny + (size_t)e * 3 * N * N;
-      if (lx == N / 2) ny[ly * N + lz] = g;
-      if (ly == N / 2) ny[N * N + lx * N + lz] = g;
-      if (lz == N / 2) ny[2 * N * N + lx * N + ly] = g;
+      if (a.Fny) {
+        float2* ny = a.Fny + (size_t)e * 3 * N * N;
+        if (lx == N / 2) ny[ly * N + lz] = g;
+        if (ly == N / 2) ny[N * N + lx * N + lz] = g;
+        if (lz == N / 2) ny[2 * N * N + lx * N + ly] = g;
+      }
     } else {
       static_cast<double2*>(a.Fg)[gbase + j] = Fv;
     }
-    const double b = a.b2[(size_t)rank * G::P * N * N + j];
-    Fv.x *= b;
-    Fv.y *= b;
+    if (a.b2c) {
+      Fv = cmul(Fv, a.b2c[(size_t)rank * G::P * N * N + j]);
+    } else {
+      const double b = a.b2[(size_t)rank * G::P * N * N + j];
+      Fv.x *= b;
+      Fv.y *= b;
+    }
     A[si] = Fv;
   }
   if (a.split && rank == 0)

@@ -377,4 +377,230 @@ vss_pair_kernel(VssPairArgs a) {
   if (pending) cluster_wait();
 }
 
+// ---------------------------------------------------------------------------
+// FP32 mode (no counterpart in the reference, which is FP64 only): the
+// Maxwellian split of the VHS operator carried over to a pair.  With
+// f_p = M_p + g_p, f_q = M_q + g_q (M from FP64 moments, separable),
+//   IFFT(t1) = u_M + X_u,  IFFT(t2) = v_M + X_v,
+//   u_M = prod_a IFFT1(e^{+i a_a mq'} mhat_p,a),  v_M likewise with q, -mp',
+//   X_u = IFFT3(e^{+i a mq'} F_gp),  X_v = IFFT3(e^{-i a mp'} F_gq)  (FP32),
+// and the product splits into u_M v_M, whose 3-D transform is the product of
+// the 1-D FP64 transforms H_a = FFT1(u_M,a v_M,a) (vss_maxwell_gain_kernel),
+// and the remainder u_M X_v + X_u (v_M + X_v), transformed in FP32
+// (vss_terms32_kernel, one cluster per (point, radial point), summed over
+// the directions in shared memory).  The radial sum, the final transform
+// and the loss f_p Re IFFT(c G) run in FP64 (prologue and epilogue kernels
+// of the VHS operator, with the complex loss kernel c).
+// ---------------------------------------------------------------------------
+struct VssTablesArgs {
+  const double2* mhat_p;   // [E][3][N]
+  const double2* mhat_q;   // [E][3][N]
+  const double2* ph;       // [T][2][3][N]
+  float2* uv;              // out [E][T][2][3][N]: u_M,a and v_M,a (FP32)
+  double2* hh;             // out [E][T][3][N]: FFT1(u_M,a v_M,a)
+  int T, nevals;
+};
+
+template <int N>
+__global__ void vss_tables_kernel(VssTablesArgs a) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= a.nevals * a.T * 3) return;
+  const int ax = gid % 3, term = (gid / 3) % a.T, e = gid / (3 * a.T);
+  const double2* mp = a.mhat_p + (size_t)e * 3 * N + ax * N;
+  const double2* mq = a.mhat_q + (size_t)e * 3 * N + ax * N;
+  const double2* pu = a.ph + ((size_t)term * 6 + ax) * N;
+  const double2* pv = a.ph + ((size_t)term * 6 + 3 + ax) * N;
+  double2 u[N], v[N];
+#pragma unroll
+  for (int l = 0; l < N; ++l) {
+    u[l] = cmul(mp[l], pu[l]);
+    v[l] = cmul(mq[l], pv[l]);
+  }
+  fft<double, N, +1>(u);
+  fft<double, N, +1>(v);
+  float2* uv = a.uv + ((size_t)e * a.T + term) * 6 * N;
+#pragma unroll
+  for (int l = 0; l < N; ++l) {
+    uv[ax * N + l] = make_float2((float)u[l].x, (float)u[l].y);
+    uv[(3 + ax) * N + l] = make_float2((float)v[l].x, (float)v[l].y);
+    u[l] = cmul(u[l], v[l]);
+  }
+  fft<double, N, -1>(u);
+  double2* hh = a.hh + (((size_t)e * a.T + term) * 3 + ax) * N;
+#pragma unroll
+  for (int l = 0; l < N; ++l) hh[l] = u[l];
+}
+
+// GM[e][l] = sum_r w_r sum_m b_rm(l) prod_a H_a,rm(l_a)   (FP64)
+// grid (ceil(n/256), E), one thread per wavenumber l.
+struct VssGainArgs {
+  const double2* hh;       // [E][T][3][N]
+  const double2* b;        // [T][n]
+  const double* w;         // [Nrho]
+  double2* GM;             // out [E][n]
+  int Nrho, M;
+};
+
+template <int N>
+__global__ void __launch_bounds__(256) vss_maxwell_gain_kernel(VssGainArgs a) {
+  constexpr int n = N * N * N;
+  const int l = blockIdx.x * 256 + threadIdx.x, e = blockIdx.y;
+  if (l >= n) return;
+  const int lx = l / (N * N), ly = (l / N) % N, lz = l % N;
+  const int T = a.Nrho * a.M;
+  const double2* hh = a.hh + (size_t)e * T * 3 * N;
+  double2 G = make_double2(0, 0);
+  for (int r = 0; r < a.Nrho; ++r) {
+    double2 acc = make_double2(0, 0);
+    for (int m = 0; m < a.M; ++m) {
+      const int term = r * a.M + m;
+      const double2* h = hh + (size_t)term * 3 * N;
+      const double2 x = cmul(cmul(h[lx], h[N + ly]), h[2 * N + lz]);
+      const double2 p = cmul(x, a.b[(size_t)term * n + l]);
+      acc.x += p.x;
+      acc.y += p.y;
+    }
+    G.x += a.w[r] * acc.x;
+    G.y += a.w[r] * acc.y;
+  }
+  a.GM[(size_t)e * n + l] = G;
+}
+
+struct VssTerms32Args {
+  const float2* Fgp;       // [E][n] F_gp
+  const float2* Fgq;       // [E][n] F_gq
+  const float2* ph;        // [T][2][3][N] FP32 phase factors
+  const float2* uv;        // [E][T][2][3][N] u_M,a, v_M,a
+  const float2* b;         // [T][n] FP32 weights
+  const double* w;         // [Nrho]
+  float2* H;               // out [E][Nrho][n]
+  int Nrho, M;
+};
+
+// z-pass of an inverse transform: rows of F (global, FP32) times the phase.
+template <int N, int C>
+__device__ __forceinline__ void vss32_zpass(float2* A, const float2* F,
+                                            const float2* tb, int t,
+                                            unsigned rank) {
+  using G = Geo<N, C>;
+  const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
+  const float2 bxy = cmul(tb[lx], tb[N + ly]);
+  const float2* row = F + ((size_t)lx * N + ly) * N;
+  float2 v[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = cmul(row[k], cmul(bxy, tb[2 * N + k]));
+  fft<float, N, +1>(v);
+  const int base = pl * G::PLANE + ly * G::ROW;
+#pragma unroll
+  for (int k = 0; k < N; ++k) A[base + k] = v[k];
+}
+
+template <int N, int C>
+__global__ void __launch_bounds__(Geo<N, C>::NT, 1)
+vss_terms32_kernel(VssTerms32Args a) {
+  using G = Geo<N, C>;
+  using T = float2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);   // X-slab work buffer
+  T* Rb = A + G::SLAB;                     // Y-slab receive buffer
+  T* U = Rb + G::SLAB;                     // Y-slab: X_u pencils
+  T* Qh = U + G::SLAB;                     // X-slab spectral accumulator
+  T* tab = Qh + G::SLAB;                   // [12N]: phases p, q | u_M | v_M
+  const int t = threadIdx.x;
+  const unsigned rank = cluster_rank();
+  const int r = blockIdx.y, e = blockIdx.z;
+  const int yl = t / N, zz = t % N, yy = rank * G::P + yl;
+  const int ybase = yl * G::PLANE + zz;
+  const T* Fp = a.Fgp + (size_t)e * G::n;
+  const T* Fq = a.Fgq + (size_t)e * G::n;
+  const int Tt = a.Nrho * a.M;
+  bool pending = false;
+  auto exchange_cols = [&](const T* v) {
+    if (pending) cluster_wait();
+    push_cols_to_yslab<float, N, C>(Rb, t, rank, v);
+    cluster_arrive();
+    cluster_wait();
+  };
+  auto release_receive = [&]() {
+    cluster_arrive();
+    pending = true;
+  };
+  auto inverse = [&](const T* F, const T* tb, T* v) {
+    vss32_zpass<N, C>(A, F, tb, t, rank);
+    __syncthreads();
+    slab_col_load_fft<float, N, C, +1>(A, t, v);
+    exchange_cols(v);
+    yslab_load_pencil<float, N, C>(Rb, t, v);
+    release_receive();
+    fft<float, N, +1>(v);
+  };
+  for (int j = t; j < G::SLAB; j += G::NT) Qh[j] = T{0.f, 0.f};
+#pragma unroll 1
+  for (int m = 0; m < a.M; ++m) {
+    const int term = r * a.M + m;
+    __syncthreads();
+    for (int i = t; i < 6 * N; i += G::NT) {
+      tab[i] = a.ph[(size_t)term * 6 * N + i];
+      tab[6 * N + i] = a.uv[((size_t)e * Tt + term) * 6 * N + i];
+    }
+    __syncthreads();
+    T v[N];
+    inverse(Fp, tab, v);                       // X_u
+#pragma unroll
+    for (int x = 0; x < N; ++x) U[ybase + x * G::ROW] = v[x];
+    inverse(Fq, tab + 3 * N, v);               // X_v
+    {
+      const T* ut = tab + 6 * N;
+      const T* vt = tab + 9 * N;
+      const T uyz = cmul(ut[N + yy], ut[2 * N + zz]);
+      const T vyz = cmul(vt[N + yy], vt[2 * N + zz]);
+#pragma unroll
+      for (int x = 0; x < N; ++x) {
+        const T uM = cmul(ut[x], uyz), vM = cmul(vt[x], vyz);
+        const T Xu = U[ybase + x * G::ROW], Xv = v[x];
+        const T a1 = cmul(uM, Xv);
+        const T a2 = cmul(Xu, make_float2(vM.x + Xv.x, vM.y + Xv.y));
+        v[x] = make_float2(a1.x + a2.x, a1.y + a2.y);
+      }
+    }
+    fft<float, N, -1>(v);                      // forward: x pass
+    if (pending) cluster_wait();
+    push_pencils_to_xslab<float, N, C>(A, t, rank, v);
+    cluster_arrive();
+    cluster_wait();
+    pending = false;
+    {
+      T w2[N];
+      slab_col_load_fft<float, N, C, -1>(A, t, w2);
+      const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+      for (int k = 0; k < N; ++k) A[base + k * G::ROW] = w2[k];
+    }
+    __syncthreads();
+    {
+      const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
+      const int base = pl * G::PLANE + ly * G::ROW;
+      T w2[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) w2[k] = A[base + k];
+      fft<float, N, -1>(w2);
+      const T* brow = a.b + (size_t)term * G::n + ((size_t)lx * N + ly) * N;
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        const T pr = cmul(w2[k], brow[k]);
+        Qh[base + k].x += pr.x;
+        Qh[base + k].y += pr.y;
+      }
+    }
+  }
+  __syncthreads();
+  const float wr = (float)a.w[r];
+  T* H = a.H + ((size_t)e * a.Nrho + r) * G::n + (size_t)rank * G::P * N * N;
+  for (int j = t; j < G::P * N * N; j += G::NT) {
+    const T q = Qh[slab_index<N, C>(j)];
+    H[j] = make_float2(wr * q.x, wr * q.y);
+  }
+  if (pending) cluster_wait();
+}
+
 }  // namespace dgfs

@@ -4,7 +4,9 @@ N in {16, 24, 32, 16, 24, 32}, Ne*K spatial points in {12, 24, 40, 12, 24,
 Nrho = N/2, plus two binary-mixture VSS problems (N=24, Ne=6, K=3, masses
 1:2, mole fractions 0.5/0.5, alpha=1.4, omega=0.81, full 12-point sphere,
 Mpre=192), with seeded perturbed (bi-)Maxwellians (VSS temperatures 1 and
-1.2, 2% uniform noise)."""
+1.2, 2% uniform noise).  All problems run in the given precision; the VHS
+problems add the FP64 conservation projection (a single VSS pair conserves
+only the mass of its species, so the mixtures are not projected)."""
 import math
 
 import numpy as np
@@ -64,7 +66,7 @@ def build_c3(precision='fp32', device='cuda', seed=20261203, project=True):
         eta = np.full((2, 2), alpha - 1)
         pre = np.full((2, 2), 0.1)
         op = VSSOperator(N, L, qz, qw, sz, 4 * np.pi / M, szpre, masses, gam,
-                         eta, pre, max_evals=pts)
+                         eta, pre, max_evals=pts, precision=precision)
         fd = [torch.tensor(x, device=device) for x in fs]
         Qd = [torch.zeros_like(x) for x in fd]
 

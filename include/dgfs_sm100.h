@@ -130,7 +130,7 @@ int dgfs_fma_peak(double* tflops, void* stream);
  * pre-integration rule szpre (Mpre points), nondimensional masses, and per
  * ordered pair pq = p*nspcs + q: gamma = 2(1-omega), eta = alpha - 1 and the
  * prefactor (bi/scattering.py:66-89).  The weights b_pq and c_pq
- * (precompute_bc_pq, vss.mako:51-93) are built on the GPU at create.  FP64.
+ * (precompute_bc_pq, vss.mako:51-93) are built on the GPU at create.
  */
 typedef struct dgfs_vss_s* dgfs_vss_handle;
 typedef struct {
@@ -150,6 +150,11 @@ typedef struct {
   const double* eta;       /* [nspcs*nspcs] host */
   const double* prefac;    /* [nspcs*nspcs] host */
   int32_t max_evals;
+  int32_t precision;       /* DGFS_PREC_FP64 (reference) or DGFS_PREC_FP32:
+                              FP32 transforms of f - M with the Maxwellian
+                              parts and the radial sum, final transform and
+                              loss in FP64 (no counterpart in the reference,
+                              which is FP64 only) */
 } dgfs_vss_desc;
 
 int dgfs_vss_create(const dgfs_vss_desc* desc, dgfs_vss_handle* out);

@@ -10,6 +10,7 @@ from oracle import mesh as om
 
 pytestmark = pytest.mark.gpu
 G = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+FP32_TOL = 1e-5   # relative L2, FP32 mode (Maxwellian split)
 FP64_TOL = 1e-11
 
 
@@ -51,8 +52,9 @@ def test_vss_matches_reference_kernel_golden(built, pq):
         assert _rel(got[s], ref[s]) < FP64_TOL, (pq, s)
 
 
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
 @pytest.mark.parametrize('N', [16, 24])
-def test_vss_matches_oracle(built, N):
+def test_vss_matches_oracle(built, N, precision):
     from dgfs1d_gpu_b200.collision import VSSOperator
     masses = [1.0, 2.0]
     vm = om.VelocityMeshBi(Nv=N, M=6, masses=masses, Nrho=6, dev=5.0)
@@ -68,8 +70,9 @@ def test_vss_matches_oracle(built, N):
     eta = np.full((2, 2), alpha - 1)
     pre = np.array([[0.1, 0.11], [0.12, 0.13]])
     op = VSSOperator(N, vm.L, vm.qz, vm.qw, vm.sz, vm.sw, szpre, masses, gam,
-                     eta, pre, max_evals=2)
+                     eta, pre, max_evals=2, precision=precision)
     fd = [torch.tensor(x[None], device='cuda') for x in f]
+    tol = FP64_TOL if precision == 'fp64' else FP32_TOL
     for p, q in ((0, 1), (1, 1)):
         tab = oc.VSSTables(N, vm.L, vm.qz, vm.qw, vm.sz, vm.sw, szpre,
                            gam[p, q], eta[p, q], masses[q] / (masses[p] + masses[q]))
@@ -77,4 +80,5 @@ def test_vss_matches_oracle(built, N):
         Q = torch.zeros_like(fd[p])
         op.eval(p, q, fd[p], fd[q], Q)
         torch.cuda.synchronize()
-        assert _rel(Q.cpu().numpy()[0], ref) < FP64_TOL, (N, p, q)
+        err = _rel(Q.cpu().numpy()[0], ref)
+        assert err < tol, (N, p, q, precision, err)
