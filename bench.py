@@ -190,6 +190,29 @@ def surrogate_line(torch, prm, fd, op32, op64, timed, args):
             'error_flag': net.device_error()}
 
 
+def solver_line(torch, timed, args):
+    """The whole dgfsStd1D step on the batched FP32 Couette configuration
+    (ssp-rk3: three RHS stages of 24 points each), eager and as one CUDA
+    graph per step."""
+    from dgfs1d_gpu_b200.config import Config
+    from dgfs1d_gpu_b200.configs import couette_std_ini
+    from dgfs1d_gpu_b200.std.solver import DGFSStd1D
+    ini = couette_std_ini(Ne=8, K=3, Nv=32, Nrho=16, M=12, dev=6.0,
+                          scheme='ssp-rk3', dt=2e-4, nsteps=200,
+                          precision_mode='fp32', sphere='full')
+    sol = DGFSStd1D(Config(ini))
+    n = max(3, args.steps // 10)
+    ms_eager = timed(sol.step, n, 3)
+    sol.capture_step()
+    ms_graph = timed(sol.step, n, 3)
+    evals = 3 * 24
+    return {'workload': 'dgfsStd1D Couette, N=32, M=12, Nrho=16, Ne=8, K=3, '
+                        'ssp-rk3, FP32 operator',
+            'ms_per_step_graph': ms_graph, 'ms_per_step_eager': ms_eager,
+            'evals_per_s_graph': evals / (ms_graph * 1e-3),
+            'graph_launches_per_step': 1}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -317,6 +340,7 @@ def main():
 
     # learned surrogate (FNO, BF16 tensor-core dense layers): trained here for
     # a bounded time on operator pairs, then timed and compared with FP64
+    solver = solver_line(torch, timed, args)
     sur = None
     if not args.no_surrogate:
         sur = surrogate_line(torch, prm, fd, op32, op64, timed, args)
@@ -425,6 +449,7 @@ def main():
                                  [round(float(x), 4) for x in stage])),
             'uneven_batch': batch,
             'surrogate': sur,
+            'solver_step': solver,
             'autotune_terms_ms': {str(k): round(v, 4) for k, v in tune.items()},
             'terms_cluster': op32.variant,
             'cpu_baseline': cpu,

@@ -79,8 +79,31 @@ class DGFSStd1D:
         self.dg.advect(u_in, u_out)
         self.sm.fs_batch(u_in, u_out, self.src, self.dst)
 
-    def step(self):
+    def capture_step(self):
+        """Capture one time step (every RHS stage -- advection, boundary
+        conditions, collision operator -- and every stage update) as one CUDA
+        graph; later calls of ``step`` replay it.  A warm-up step runs first
+        and is undone, so the solution is unchanged."""
+        u0 = self.u.clone()
         self.odes.integrate(self.t, self.dt, self.u)
+        torch.cuda.synchronize()
+        self.u.copy_(u0)
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(device=self.device)
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self.odes.integrate(self.t, self.dt, self.u)
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        self._graph = g
+        return g
+
+    def step(self):
+        if getattr(self, '_graph', None) is not None:
+            self._graph.replay()
+        else:
+            self.odes.integrate(self.t, self.dt, self.u)
         self.t += self.dt
         self.nacptsteps += 1
         n = self.nacptsteps
