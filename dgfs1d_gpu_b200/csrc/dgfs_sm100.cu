@@ -1705,14 +1705,17 @@ extern "C" int dgfs_fno_get_grads(dgfs_fno_handle h, float* host) {
 template <int LIN, int LOUT, int IN, int OUT>
 static int fno_dft(const void* in, void* out, const float2* table, long outer,
                    int inner, cudaStream_t st) {
-  const long tot = outer * inner;
+  const long tot = outer * (inner / 2);
   fno::fno_dft_kernel<LIN, LOUT, IN, OUT>
       <<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, out, table, outer, inner);
   DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
 }
 
-// forward DFT of a real field [B][n][WD] (IN: 0 BF16, 1 FP32) into [B][K^3][WD]
+// forward DFT of a real field [B][n][WD] (IN: 0 BF16, 1 FP32) into [B][K^3][WD]:
+// one pass per axis (the y and z passes read 32 complex values per pencil,
+// which keeps every thread busy; a fused y/z kernel idles 60% of its
+// threads in the y pass and measured slower)
 template <int N, int K, int IN>
 static int fno_dft3(dgfs_fno_s* h, const void* in, const float2* tab, float2* out,
                     int B, cudaStream_t st) {
@@ -1723,15 +1726,19 @@ static int fno_dft3(dgfs_fno_s* h, const void* in, const float2* tab, float2* ou
   return fno_dft<N, K, 2, 0>(h->T2, out, tab, (long)B * K * K, WD, st);
 }
 
-// expand [B][K^3][WD] complex to the real part on the grid
-// (OUT: 2 FP32 add, 3 BF16 store)
+// expand [B][K^3][WD] complex to the real part on the grid: fused z/y
+// passes, then the x pass (OUT: 2 FP32 add, 3 BF16 store)
 template <int N, int K, int OUT>
 static int fno_idft3(dgfs_fno_s* h, const float2* in, const float2* tab, void* out,
                      int B, cudaStream_t st) {
   constexpr int WD = fno::WD;
-  int rc;
-  if ((rc = fno_dft<K, N, 2, 0>(in, h->T2, tab, (long)B * K * K, WD, st))) return rc;
-  if ((rc = fno_dft<K, N, 2, 0>(h->T2, h->T1, tab, (long)B * K, N * WD, st))) return rc;
+  const size_t smem = (size_t)(K * K * fno::DCG + K * N * fno::DCG + N * K) * sizeof(float2);
+  if (smem > 48 * 1024)
+    DGFS_CUDA(cudaFuncSetAttribute(fno::fno_dft_zy_inv_kernel<N, K>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fno::fno_dft_zy_inv_kernel<N, K><<<dim3(WD / fno::DCG, K, B), 256, smem, st>>>(
+      in, h->T1, tab);
+  DGFS_CUDA(cudaGetLastError());
   return fno_dft<K, N, 2, OUT>(h->T1, out, tab, B, N * N * WD, st);
 }
 

@@ -241,8 +241,9 @@ __global__ void __launch_bounds__(256) fno_features_kernel(FeatArgs a) {
 // IN: 0 BF16 real, 1 FP32 real, 2 complex FP32.
 // OUT: 0 complex FP32, 1 Re -> FP32 store, 2 Re -> FP32 accumulate,
 //      3 Re -> BF16 store.
-// One thread per (outer, inner) pencil; consecutive threads take consecutive
-// inner indices, so every load and store is coalesced.
+// One thread per two adjacent (outer, inner) pencils (inner is even):
+// consecutive threads take consecutive inner pairs, so loads and stores are
+// coalesced and every table entry read from shared memory serves two pencils.
 // ---------------------------------------------------------------------------
 template <int LIN, int LOUT, int IN, int OUT>
 __global__ void __launch_bounds__(256)
@@ -251,37 +252,129 @@ fno_dft_kernel(const void* in, void* out, const float2* table, long outer,
   __shared__ float2 tb[LOUT * LIN];
   for (int i = threadIdx.x; i < LOUT * LIN; i += blockDim.x) tb[i] = table[i];
   __syncthreads();
+  const int half = inner / 2;
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= outer * inner) return;
-  const long o = gid / inner;
-  const int i = (int)(gid % inner);
-  float2 x[LIN];
+  if (gid >= outer * half) return;
+  const long o = gid / half;
+  const int i = 2 * (int)(gid % half);
+  float2 x0[LIN], x1[LIN];
 #pragma unroll
   for (int j = 0; j < LIN; ++j) {
     const long idx = (o * LIN + j) * inner + i;
-    if (IN == 0) x[j] = make_float2(bf(static_cast<const __nv_bfloat16*>(in)[idx]), 0.f);
-    else if (IN == 1) x[j] = make_float2(static_cast<const float*>(in)[idx], 0.f);
-    else x[j] = static_cast<const float2*>(in)[idx];
+    if (IN == 0) {
+      const float2 v = __bfloat1622float2(
+          *reinterpret_cast<const __nv_bfloat162*>(static_cast<const __nv_bfloat16*>(in) + idx));
+      x0[j] = make_float2(v.x, 0.f);
+      x1[j] = make_float2(v.y, 0.f);
+    } else if (IN == 1) {
+      const float2 v = *reinterpret_cast<const float2*>(static_cast<const float*>(in) + idx);
+      x0[j] = make_float2(v.x, 0.f);
+      x1[j] = make_float2(v.y, 0.f);
+    } else {
+      const float4 v = *reinterpret_cast<const float4*>(static_cast<const float2*>(in) + idx);
+      x0[j] = make_float2(v.x, v.y);
+      x1[j] = make_float2(v.z, v.w);
+    }
   }
-#pragma unroll 4
+#pragma unroll 2
   for (int k = 0; k < LOUT; ++k) {
-    float re = 0.f, im = 0.f;
+    float r0 = 0.f, i0 = 0.f, r1 = 0.f, i1 = 0.f;
 #pragma unroll
     for (int j = 0; j < LIN; ++j) {
       const float2 w = tb[k * LIN + j];
       if (IN == 2) {
-        re += w.x * x[j].x - w.y * x[j].y;
-        if (OUT == 0) im += w.x * x[j].y + w.y * x[j].x;
+        r0 += w.x * x0[j].x - w.y * x0[j].y;
+        r1 += w.x * x1[j].x - w.y * x1[j].y;
+        if (OUT == 0) {
+          i0 += w.x * x0[j].y + w.y * x0[j].x;
+          i1 += w.x * x1[j].y + w.y * x1[j].x;
+        }
       } else {
-        re += w.x * x[j].x;
-        if (OUT == 0) im += w.y * x[j].x;
+        r0 += w.x * x0[j].x;
+        r1 += w.x * x1[j].x;
+        if (OUT == 0) {
+          i0 += w.y * x0[j].x;
+          i1 += w.y * x1[j].x;
+        }
       }
     }
     const long idx = (o * LOUT + k) * inner + i;
-    if (OUT == 0) static_cast<float2*>(out)[idx] = make_float2(re, im);
-    else if (OUT == 1) static_cast<float*>(out)[idx] = re;
-    else if (OUT == 2) static_cast<float*>(out)[idx] += re;
-    else static_cast<__nv_bfloat16*>(out)[idx] = tobf(re);
+    if (OUT == 0) {
+      *reinterpret_cast<float4*>(static_cast<float2*>(out) + idx) = make_float4(r0, i0, r1, i1);
+    } else if (OUT == 1) {
+      *reinterpret_cast<float2*>(static_cast<float*>(out) + idx) = make_float2(r0, r1);
+    } else if (OUT == 2) {
+      float2* q = reinterpret_cast<float2*>(static_cast<float*>(out) + idx);
+      const float2 c = *q;
+      *q = make_float2(c.x + r0, c.y + r1);
+    } else {
+      *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(out) + idx) =
+          __floats2bfloat162_rn(r0, r1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused inverse z and y passes.  One CTA per (sample b, x-mode kx, group of
+// DCG channels); the (ky, z) intermediate of the group stays in shared
+// memory between the two passes:
+//   in U [B][K][K][K][WD] -> out T1 [B][K][N][N][WD],
+//   out[y][z] = sum_ky sum_kz G[y][ky] G[z][kz] in[ky][kz],  G: [N][K].
+// ---------------------------------------------------------------------------
+constexpr int DCG = 8;  // channels per CTA
+
+template <int N, int K>
+__global__ void __launch_bounds__(256)
+fno_dft_zy_inv_kernel(const float2* in, float2* out, const float2* table) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* S1 = reinterpret_cast<float2*>(smem_raw);  // [K][K][DCG]
+  float2* S2 = S1 + K * K * DCG;                      // [K][N][DCG]
+  float2* tb = S2 + K * N * DCG;                      // [N][K]
+  const int cg = blockIdx.x, kx = blockIdx.y, b = blockIdx.z, t = threadIdx.x;
+  for (int i = t; i < N * K; i += 256) tb[i] = table[i];
+  const long ibase = ((long)b * K + kx) * K * K * WD + cg * DCG;
+  for (int e = t; e < K * K * DCG; e += 256) {
+    const int c = e % DCG, kk = e / DCG;
+    S1[e] = in[ibase + (long)kk * WD + c];
+  }
+  __syncthreads();
+  // z expand: thread per (ky, c)
+  for (int w = t; w < K * DCG; w += 256) {
+    const int ky = w / DCG, c = w % DCG;
+    float2 x[K];
+#pragma unroll
+    for (int kz = 0; kz < K; ++kz) x[kz] = S1[(ky * K + kz) * DCG + c];
+#pragma unroll 4
+    for (int z = 0; z < N; ++z) {
+      float re = 0.f, im = 0.f;
+#pragma unroll
+      for (int kz = 0; kz < K; ++kz) {
+        const float2 g = tb[z * K + kz];
+        re += g.x * x[kz].x - g.y * x[kz].y;
+        im += g.x * x[kz].y + g.y * x[kz].x;
+      }
+      S2[(ky * N + z) * DCG + c] = make_float2(re, im);
+    }
+  }
+  __syncthreads();
+  // y expand: thread per (z, c)
+  const long obase = ((long)b * K + kx) * N * N * WD + cg * DCG;
+  for (int w = t; w < N * DCG; w += 256) {
+    const int z = w / DCG, c = w % DCG;
+    float2 x[K];
+#pragma unroll
+    for (int ky = 0; ky < K; ++ky) x[ky] = S2[(ky * N + z) * DCG + c];
+#pragma unroll 4
+    for (int y = 0; y < N; ++y) {
+      float re = 0.f, im = 0.f;
+#pragma unroll
+      for (int ky = 0; ky < K; ++ky) {
+        const float2 g = tb[y * K + ky];
+        re += g.x * x[ky].x - g.y * x[ky].y;
+        im += g.x * x[ky].y + g.y * x[ky].x;
+      }
+      out[obase + ((long)y * N + z) * WD + c] = make_float2(re, im);
+    }
   }
 }
 
