@@ -36,6 +36,20 @@ def make_inputs(rank=0):
     return prm, f
 
 
+def max_over_ranks(torch, dist, value, world, device):
+    """The maximum of a per-rank float over all ranks (the job's time)."""
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, ms_max):
+    """Whole-job throughput: every rank's units over the slowest rank's time
+    (weak scaling: each rank evaluates its own points)."""
+    return units_per_rank * world / (ms_max * 1e-3)
+
+
 def cpu_oracle_rate(prm, f, budget_s=12.0, max_evals=4):
     """Evals/s of the oracle (CPU checker) on this host's cores, bounded."""
     from oracle.collision import VHSTables, vhs_gll_fs
@@ -275,10 +289,7 @@ def main():
             e.synchronize()
             tot += s.elapsed_time(e)
         barrier()
-        t = torch.tensor([tot], device='cuda', dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()) / steps  # ms per step, max over ranks
+        return max_over_ranks(torch, dist, tot, world, 'cuda') / steps
 
     if args.kernel_only:
         ms = timed(lambda: op32.eval(fd, Q), args.steps, args.warmup)
@@ -413,7 +424,7 @@ def main():
                              f'(complex128, scipy.fft workers={cores})'}
         line = {
             'metric': METRIC,
-            'value': evals / (ms32 * 1e-3),
+            'value': job_rate(E, world, ms32),
             'unit': UNIT,
             'n_gpus': world,
             'steps': args.steps,
