@@ -204,6 +204,30 @@ def surrogate_line(torch, prm, fd, op32, op64, timed, args):
             'error_flag': net.device_error()}
 
 
+def stress_line(torch, timed, args):
+    """The stress-size operator: hard spheres (omega = 0.5), N=48^3 on
+    [-8,8]^3, full-sphere M=32 design, Nrho=24, 96 points (Ne=32, K=3), FP32
+    mode, seeded Couette-like distributions."""
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    from dgfs1d_gpu_b200.workloads import couette_distributions, vhs_mesh_params
+    prm = vhs_mesh_params(48, 32, 24, 8.0, True, omega=0.5)
+    f = torch.tensor(couette_distributions(prm['c0'], 96, seed=7), device='cuda')
+    op = VHSOperator(**prm, precision='fp32', max_evals=96)
+    op.set_projection(True)
+    Q = torch.zeros_like(f)
+    ms = timed(lambda: op.eval(f, Q), 5, 3)
+    Q.zero_()
+    op.eval(f, Q)
+    torch.cuda.synchronize()
+    ok = bool(torch.isfinite(Q).all())
+    op.close()
+    del f, Q
+    return {'workload': 'HS, N=48, L=8, M=32 full sphere, Nrho=24, 96 points, '
+                        'FP32 + FP64 projection',
+            'value': 96 / (ms * 1e-3), 'unit': UNIT, 'ms_per_step': ms,
+            'finite': ok}
+
+
 def solver_line(torch, timed, args):
     """The whole dgfsStd1D step on the batched FP32 Couette configuration
     (ssp-rk3: three RHS stages of 24 points each), eager and as one CUDA
@@ -352,6 +376,7 @@ def main():
     # learned surrogate (FNO, BF16 tensor-core dense layers): trained here for
     # a bounded time on operator pairs, then timed and compared with FP64
     solver = solver_line(torch, timed, args)
+    stress = stress_line(torch, timed, args)
     sur = None
     if not args.no_surrogate:
         sur = surrogate_line(torch, prm, fd, op32, op64, timed, args)
@@ -461,6 +486,7 @@ def main():
             'uneven_batch': batch,
             'surrogate': sur,
             'solver_step': solver,
+            'stress_n48': stress,
             'autotune_terms_ms': {str(k): round(v, 4) for k, v in tune.items()},
             'terms_cluster': op32.variant,
             'cpu_baseline': cpu,

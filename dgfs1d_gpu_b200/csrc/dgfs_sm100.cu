@@ -164,7 +164,7 @@ static int c64_of(int N) {
     case 16: return 2;
     case 24: return 4;
     case 32: return 8;
-    default: return 0;
+    default: return 0;  // N=48: no FP64 terms kernel (three FP64 slabs do not fit)
   }
 }
 static int c32_of(int N) {
@@ -173,6 +173,7 @@ static int c32_of(int N) {
     case 16: return 1;
     case 24: return 3;
     case 32: return 4;
+    case 48: return 16;
     default: return 0;
   }
 }
@@ -185,6 +186,9 @@ template <> struct VhsClusters<8> { static constexpr int c64 = 1, c32 = 1, cpro 
 template <> struct VhsClusters<16> { static constexpr int c64 = 2, c32 = 1, cpro = 2, cepi = 2; };
 template <> struct VhsClusters<24> { static constexpr int c64 = 4, c32 = 3, cpro = 4, cepi = 4; };
 template <> struct VhsClusters<32> { static constexpr int c64 = 8, c32 = 4, cpro = 8, cepi = 16; };
+// N=48 (FP32 mode only): 16-CTA clusters of 3 planes; the two FP64 slabs of
+// the prologue take 226 KB of the 227 KB a CTA may use
+template <> struct VhsClusters<48> { static constexpr int c64 = 0, c32 = 16, cpro = 16, cepi = 16; };
 
 static size_t slab_bytes(int N, int C, size_t elem) {
   return (size_t)(N / C) * N * (N + 1) * elem;
@@ -224,10 +228,14 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_desc* d, dgfs_vhs_handle* out) {
     return fail(DGFS_ERR_INVALID, "qz, qw, sz and c0 are required");
   if (d->precision != DGFS_PREC_FP64 && d->precision != DGFS_PREC_FP32)
     return fail(DGFS_ERR_INVALID, "unknown precision");
-  if (c64_of(d->N) == 0 || c32_of(d->N) == 0)
+  if (c32_of(d->N) == 0)
     return fail(DGFS_ERR_UNSUPPORTED,
                 "velocity grid N=" + std::to_string(d->N) +
-                    " is not compiled in (supported: 8, 16, 24, 32)");
+                    " is not compiled in (supported: 8, 16, 24, 32, 48)");
+  if (d->precision == DGFS_PREC_FP64 && c64_of(d->N) == 0)
+    return fail(DGFS_ERR_UNSUPPORTED,
+                "velocity grid N=" + std::to_string(d->N) +
+                    " is compiled for the FP32 mode only");
   if (int rc = ensure_twiddles()) return rc;
 
   const int N = d->N, n = N * N * N, Nrho = d->Nrho, M = d->M;
@@ -410,6 +418,7 @@ template <> struct Terms32Variants<8> { static constexpr int v[2] = {1, 2}; };
 template <> struct Terms32Variants<16> { static constexpr int v[2] = {1, 2}; };
 template <> struct Terms32Variants<24> { static constexpr int v[3] = {3, 4, 6}; };
 template <> struct Terms32Variants<32> { static constexpr int v[2] = {4, 8}; };
+template <> struct Terms32Variants<48> { static constexpr int v[1] = {16}; };
 
 template <int N>
 static int launch_terms32(int c, const VhsTermsArgs& a, int nevals, int Nrho,
@@ -424,6 +433,8 @@ static int launch_terms32(int c, const VhsTermsArgs& a, int nevals, int Nrho,
   } else if constexpr (N == 32) {
     if (c == 4) return launch_terms32_c<N, 4>(a, nevals, Nrho, st);
     if (c == 8) return launch_terms32_c<N, 8>(a, nevals, Nrho, st);
+  } else if constexpr (N == 48) {
+    if (c == 16) return launch_terms32_c<N, 16>(a, nevals, Nrho, st);
   }
   return fail(DGFS_ERR_UNSUPPORTED, "terms kernel cluster size not compiled in");
 }
@@ -433,7 +444,8 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                    int q_double, const int32_t* src_slots, int src_base,
                    const int32_t* dst_slots, int dst_base, int nevals,
                    cudaStream_t st) {
-  constexpr int C64 = VhsClusters<N>::c64;
+  constexpr int C64 = VhsClusters<N>::c64 > 0 ? VhsClusters<N>::c64 : 1;
+  constexpr bool HAS64 = VhsClusters<N>::c64 > 0;
   constexpr int C32 = VhsClusters<N>::c32;
   constexpr int CPRO = VhsClusters<N>::cpro;
   constexpr int CEPI = VhsClusters<N>::cepi;
@@ -512,15 +524,19 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     DGFS_CUDA(cudaStreamWaitEvent(st, h->join_aux, 0));
   } else {
     mark(); mark();  // no tables / Maxwellian-gain stages in FP64 mode
-    VhsTermsArgs a{};
-    a.Fg = h->Fg; a.ph = h->ph; a.uv = nullptr; a.mult = h->mult;
-    a.b1w = h->b1w64; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
-    const size_t smem = 3 * slab_bytes(N, C64, sizeof(double2)) +
-                        9 * N * sizeof(double2);
-    if ((rc = launch_cluster(vhs_terms_kernel<double, N, C64, false>,
-                             dim3(C64, h->Nrho, nevals), dim3(G64::NT), C64,
-                             smem, st, a)))
-      return rc;
+    if constexpr (HAS64) {
+      VhsTermsArgs a{};
+      a.Fg = h->Fg; a.ph = h->ph; a.uv = nullptr; a.mult = h->mult;
+      a.b1w = h->b1w64; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
+      const size_t smem = 3 * slab_bytes(N, C64, sizeof(double2)) +
+                          9 * N * sizeof(double2);
+      if ((rc = launch_cluster(vhs_terms_kernel<double, N, C64, false>,
+                               dim3(C64, h->Nrho, nevals), dim3(G64::NT), C64,
+                               smem, st, a)))
+        return rc;
+    } else {
+      return fail(DGFS_ERR_UNSUPPORTED, "no FP64 terms kernel at this N");
+    }
     mark();
   }
   // epilogue
@@ -569,6 +585,7 @@ extern "C" int dgfs_vhs_eval(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
       case 16: rc = vhs_run<16>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
       case 24: rc = vhs_run<24>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
       case 32: rc = vhs_run<32>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 48: rc = vhs_run<48>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
       default: return fail(DGFS_ERR_UNSUPPORTED, "N not compiled in");
     }
     if (rc) return rc;
@@ -1489,6 +1506,7 @@ extern "C" int dgfs_vhs_variants(int32_t N, int32_t* out, int32_t max) {
     case 16: v = Terms32Variants<16>::v; n = 2; break;
     case 24: v = Terms32Variants<24>::v; n = 3; break;
     case 32: v = Terms32Variants<32>::v; n = 2; break;
+    case 48: v = Terms32Variants<48>::v; n = 1; break;
     default: return fail(DGFS_ERR_UNSUPPORTED, "N not compiled in");
   }
   for (int i = 0; i < n && i < max; ++i) out[i] = v[i];

@@ -799,12 +799,15 @@ __device__ __forceinline__ void fp32_issue_rho_copy(float2* rbuf,
   const uint32_t sx = s0 + 8u * N * N;
   const float2* rx = rho + (size_t)rank * P * N;
   for (int c = t; c < P * N / 2; c += G::NT) cp_async16(sx + 16u * c, rx + 2 * c);
-  // rz[x][rank P .. rank P + P): N segments of P complex
+  // rz[x][rank P .. rank P + P): N segments of P complex, copied element by
+  // element (8 bytes) because P may be odd (N=48 with 16 planes: P=3), which
+  // leaves the segments only 8-byte aligned
   const uint32_t szz = sx + 8u * P * N;
   const float2* rz = rho + 2 * N * N + rank * P;
-  for (int c = t; c < N * P / 2; c += G::NT) {
-    const int x = c / (P / 2), j = c % (P / 2);
-    cp_async16(szz + 16u * c, rz + (size_t)x * N + 2 * j);
+  for (int c = t; c < N * P; c += G::NT) {
+    const int x = c / P, j = c % P;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
+                 :: "r"(szz + 8u * c), "l"(rz + (size_t)x * N + j) : "memory");
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }

@@ -186,3 +186,23 @@ def test_fp32_cluster_variants_match_oracle(lib, case):
             assert err < FP32_TOL, f'N={N} cluster {c}: rel L2 {err:.3e}'
     times = op.autotune(fd, torch.zeros_like(fd), reps=2)
     assert set(times) == set(variants) and op.variant in variants
+
+
+def test_n48_fp32_matches_oracle(lib):
+    """N=48 (FP32 mode only; 16-CTA clusters) against the oracle, hard
+    spheres (omega = 0.5) on [-8, 8]^3, with a reduced sphere/radial rule so
+    that the oracle finishes in seconds."""
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    vm, prefac, gamma, f = vhs_case(48, 6, 4, 8.0, False, omega=0.5, nslots=2)
+    tab = vhs_tables(vm, gamma)
+    op = VHSOperator(**op_kwargs(vm, prefac, gamma), precision='fp32',
+                     max_evals=2)
+    fd = torch.tensor(f, dtype=torch.float64, device='cuda')
+    Q = torch.zeros_like(fd)
+    op.eval(fd, Q)
+    torch.cuda.synchronize()
+    for s in range(2):
+        err = _rel(Q.cpu().numpy()[s], vhs_gll_fs(tab, prefac, f[s]))
+        assert err < FP32_TOL, f'N=48 slot {s}: rel L2 {err:.3e}'
+    with pytest.raises(Exception):
+        VHSOperator(**op_kwargs(vm, prefac, gamma), precision='fp64', max_evals=1)
