@@ -18,6 +18,7 @@ bulk moments per step.
    above a 1e-3 residual) runs to steady state, in two modes: the surrogate
    alone between checks, and the surrogate plus the defect measured at the
    last check.
+5. For context, the solver with the fused FP32 operator (no surrogate).
 
 ``python -m dgfs1d_gpu_b200.surrogate_couette [--quick]`` prints one JSON
 report (``--quick``: N = 16 and short budgets, for tests).
@@ -37,11 +38,11 @@ from . import surrogate_train as st
 
 
 def make_solver(N, Nrho, M, dev, Ne=8, K=3, dt=1e-3, scheme='imex-lm-bdf2',
-                sphere='full'):
+                sphere='full', precision_mode=None):
     ini = couette_astd_ini(scheme=scheme, penalty='boltz-bgk-direct-gll',
                            Ne=Ne, K=K, Nv=N, Nrho=Nrho, M=M, dev=dev, dt=dt,
                            nsteps=10 ** 7, ic='maxwellian', noise=0.0,
-                           sphere=sphere)
+                           sphere=sphere, precision_mode=precision_mode)
     return DGFSABstd1D(Config(ini))
 
 
@@ -56,14 +57,14 @@ def _rel_profile_diff(a, b):
 
 def experiment(N=32, Nrho=16, M=12, dev=6.0, dt=1e-3, sphere='full',
                steady_tol=1e-8,
-               max_steps=20000, n_maxwellian=20000, harvest_steps=3000,
-               harvest_every=10, train_steps=20000, train_time=180.0, k=10,
-               tol=1e-3, seed=20261203):
+               max_steps=40000, n_maxwellian=20000, harvest_steps=3000,
+               harvest_every=10, train_steps=40000, train_time=300.0, k=10,
+               tol=1e-3, seed=20261203, check_every=10):
     out = dict(config=dict(N=N, Nrho=Nrho, M=M, L=dev, Ne=8, K=3, dt=dt,
                            scheme='imex-lm-bdf2', steady_tol=steady_tol, k=k,
                            tol=tol))
     plain = make_solver(N, Nrho, M, dev, dt=dt, sphere=sphere)
-    rp = st.run_to_steady(plain, steady_tol, max_steps)
+    rp = st.run_to_steady(plain, steady_tol, max_steps, check_every)
     pxy_p, qx_p = _profiles(rp['moments'])
     out['plain'] = dict(steps=rp['steps'], wall_s=rp['wall_s'],
                         residual=rp['residual'])
@@ -101,7 +102,7 @@ def experiment(N=32, Nrho=16, M=12, dev=6.0, dt=1e-3, sphere='full',
         sol = make_solver(N, Nrho, M, dev, dt=dt, sphere=sphere)
         hook = st.SurrogateBoltzmann(sol, net, k=k, tol=tol, correct=correct)
         sol.boltzmann = hook
-        rs = st.run_to_steady(sol, steady_tol, max_steps)
+        rs = st.run_to_steady(sol, steady_tol, max_steps, check_every)
         pxy, qx = _profiles(rs['moments'])
         out[mode] = dict(steps=rs['steps'], wall_s=rs['wall_s'],
                          residual=rs['residual'],
@@ -109,6 +110,16 @@ def experiment(N=32, Nrho=16, M=12, dev=6.0, dt=1e-3, sphere='full',
                          shear_stress_rel_diff=_rel_profile_diff(pxy, pxy_p),
                          heat_flux_rel_diff=_rel_profile_diff(qx, qx_p),
                          **hook.stats())
+    # context: the same solver with the fused FP32 operator in place of the
+    # FP64 one (no surrogate)
+    f32 = make_solver(N, Nrho, M, dev, dt=dt, sphere=sphere, precision_mode='fp32')
+    rf = st.run_to_steady(f32, steady_tol, max_steps, check_every)
+    pxy, qx = _profiles(rf['moments'])
+    out['fp32-fused-operator'] = dict(
+        steps=rf['steps'], wall_s=rf['wall_s'], residual=rf['residual'],
+        speedup_vs_plain=rp['wall_s'] / rf['wall_s'],
+        shear_stress_rel_diff=_rel_profile_diff(pxy, pxy_p),
+        heat_flux_rel_diff=_rel_profile_diff(qx, qx_p))
     return out
 
 
@@ -120,7 +131,7 @@ def main():
     build.build()
     if args.quick:
         rep = experiment(N=16, Nrho=8, M=6, dev=5.0, dt=2e-3, sphere='auto',
-                         steady_tol=1e-6,
+                         steady_tol=1e-6, check_every=1,
                          max_steps=3000, n_maxwellian=512, harvest_steps=200,
                          harvest_every=10, train_steps=400, train_time=30.0)
     else:
