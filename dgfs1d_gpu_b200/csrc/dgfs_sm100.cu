@@ -407,7 +407,8 @@ static int launch_terms32_c(const VhsTermsArgs& a, int nevals, int Nrho,
   // three slabs, two table slots, the staged plane transforms of one term
   const size_t smem = 3 * slab_bytes(N, C, sizeof(float2)) +
                       2 * (9 * N + 4) * sizeof(float2) +
-                      (size_t)(N * N + 2 * G::P * N) * sizeof(float2);
+                      (size_t)((TermsRyStaged<C>::value ? N * N : 0) +
+                               2 * G::P * N) * sizeof(float2);
   return launch_cluster(vhs_terms_fp32_kernel<N, C>,
                         dim3(C, (Nrho + 1) / 2, nevals), dim3(G::NT), C, smem,
                         st, a);

@@ -783,20 +783,28 @@ vhs_nyq_planes_kernel(VhsTermsArgs a) {
   }
 }
 
+// Whether the terms kernel stages r_y (N*N complex) in shared memory.  With
+// 8 or more CTAs per cluster it reads r_y through L1 instead, which leaves
+// room for two CTAs per SM.
+template <int C> struct TermsRyStaged { static constexpr bool value = C < 8; };
+
 // Stage this CTA's share of the plane transforms of one term into smem:
-// rY = ry[x][z] (all), rX = rx[y][z] (own y), rZ = rz[x][y] (own y) as [x][yl].
+// rY = ry[x][z] (all; only if staged), rX = rx[y][z] (own y),
+// rZ = rz[x][y] (own y) as [x][yl].
 template <int N, int C>
 __device__ __forceinline__ void fp32_issue_rho_copy(float2* rbuf,
                                                     const float2* rho, int t,
                                                     unsigned rank) {
   using G = Geo<N, C>;
   constexpr int P = G::P;
+  constexpr bool RYS = TermsRyStaged<C>::value;
   const uint32_t s0 = smem_u32(rbuf);
   // ry: N*N complex = N*N/2 chunks of 16 B
-  for (int c = t; c < N * N / 2; c += G::NT)
-    cp_async16(s0 + 16u * c, rho + N * N + 2 * c);
+  if (RYS)
+    for (int c = t; c < N * N / 2; c += G::NT)
+      cp_async16(s0 + 16u * c, rho + N * N + 2 * c);
   // rx rows y in [rank P, rank P + P): P*N complex
-  const uint32_t sx = s0 + 8u * N * N;
+  const uint32_t sx = s0 + (RYS ? 8u * N * N : 0u);
   const float2* rx = rho + (size_t)rank * P * N;
   for (int c = t; c < P * N / 2; c += G::NT) cp_async16(sx + 16u * c, rx + 2 * c);
   // rz[x][rank P .. rank P + P): N segments of P complex, copied element by
@@ -822,9 +830,9 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
   T* A = reinterpret_cast<T*>(smem_raw);
   T* R0 = A + G::SLAB;          // receive buffer b at R0 + b*SLAB
   T* tab = R0 + 2 * G::SLAB;    // [2][TB]
-  T* rbuf = tab + 2 * TB;       // ry [N*N] | rx [P*N] | rz [N*P]
-  const T* rY = rbuf;
-  const T* rX = rbuf + N * N;
+  constexpr bool RYS = TermsRyStaged<C>::value;
+  T* rbuf = tab + 2 * TB;       // (ry [N*N]) | rx [P*N] | rz [N*P]
+  const T* rX = rbuf + (RYS ? N * N : 0);
   const T* rZ = rX + G::P * N;
   const int t = threadIdx.x;
   const unsigned rank = cluster_rank();
@@ -914,6 +922,7 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
     const T uyz = cmul(ut[N + yy], ut[2 * N + zz]);
     const T vyz = cmul(vt[N + yy], vt[2 * N + zz]);
     const T rx = rX[yl * N + zz];
+    const T* rY = RYS ? rbuf : rho_of(k) + N * N;
     const bool hi = k >= Mu;
 #pragma unroll
     for (int x = 0; x < N; ++x) {
