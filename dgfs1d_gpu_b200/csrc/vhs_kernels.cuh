@@ -980,6 +980,285 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Split-pencil variant of the FP32 terms kernel: two threads (adjacent lanes
+// h = 0, 1) share every pencil, each holding N/2 values, so a CTA runs twice
+// the warps for the same shared memory (registers per thread roughly halve).
+// An N-point transform is one radix-2 step across the pair (register
+// exchange by shuffles) around N/2-point register transforms:
+//   DIT (input samples 2m+h, output X[h N/2 + m]):  E/O transforms, then
+//       X[k] = E[k] + W^k O[k], X[k + N/2] = E[k] - W^k O[k];
+//   DIF (input x[h N/2 + m], output X[2m + h]):  a = x[m] + x[m + N/2],
+//       b = (x[m] - x[m + N/2]) W^m, then the N/2-point transforms.
+// Same algorithm, data layout and pipeline as vhs_terms_fp32_kernel.
+// ---------------------------------------------------------------------------
+template <int N, int SIGN>
+__device__ __forceinline__ void fft_pair_dit(float2* v, int h) {
+  constexpr int H = N / 2;
+  fft<float, H, SIGN>(v);
+#pragma unroll
+  for (int k = 0; k < H; ++k) {
+    const float2 w = h ? twiddle_mul<float, N, SIGN>(v[k], k) : v[k];
+    float2 o;
+    o.x = __shfl_xor_sync(0xffffffffu, w.x, 1);
+    o.y = __shfl_xor_sync(0xffffffffu, w.y, 1);
+    // h = 0 holds E, receives W O;  h = 1 holds W O, receives E
+    v[k] = h ? make_float2(o.x - w.x, o.y - w.y) : make_float2(w.x + o.x, w.y + o.y);
+  }
+}
+
+template <int N, int SIGN>
+__device__ __forceinline__ void fft_pair_dif(float2* v, int h) {
+  constexpr int H = N / 2;
+#pragma unroll
+  for (int k = 0; k < H; ++k) {
+    float2 o;
+    o.x = __shfl_xor_sync(0xffffffffu, v[k].x, 1);
+    o.y = __shfl_xor_sync(0xffffffffu, v[k].y, 1);
+    // h = 0 holds x[k], receives x[k + H];  h = 1 the reverse
+    const float2 a = make_float2(v[k].x + o.x, v[k].y + o.y);
+    const float2 b = make_float2(o.x - v[k].x, o.y - v[k].y);
+    v[k] = h ? twiddle_mul<float, N, SIGN>(b, k) : a;
+  }
+  fft<float, H, SIGN>(v);
+}
+
+template <int N, int C>
+struct GeoS {
+  using G = Geo<N, C>;
+  static constexpr int NT = 2 * G::NT;  // two threads per pencil
+};
+
+template <int N, int C>
+__device__ __forceinline__ void fp32s_zpass(float2* A, const float2* tb, int pp,
+                                            int h, unsigned rank) {
+  using G = Geo<N, C>;
+  constexpr int H = N / 2;
+  const int pl = pp / N, ly = pp % N, lx = rank * G::P + pl;
+  const float2 bxy = cmul(tb[lx], tb[N + ly]);
+  const float2* nu = tb + 9 * N;
+  float2 fxy = make_float2(1.f, 0.f);
+  if (lx == N / 2) fxy = nu[0];
+  if (ly == N / 2) fxy = cmul(fxy, nu[1]);
+  const float2 gb = cmul(nyq_main(fxy), bxy);
+  const float2 gbz = cmul(nyq_main(cmul(fxy, nu[2])), bxy);
+  const int base = pl * G::PLANE + ly * G::ROW;
+  float2 v[H];
+#pragma unroll
+  for (int m = 0; m < H; ++m) {
+    const int k = 2 * m + h;
+    const float2 bz = tb[2 * N + k];
+    const float2 g = (k == N / 2) ? gbz : gb;
+    const float mm = g.x * bz.x - g.y * bz.y;
+    const float2 f = A[base + k];
+    v[m] = make_float2(f.x * mm, f.y * mm);
+  }
+  fft_pair_dit<N, +1>(v, h);
+#pragma unroll
+  for (int m = 0; m < H; ++m) A[base + h * H + m] = v[m];
+}
+
+template <int N, int C>
+__global__ void __launch_bounds__(GeoS<N, C>::NT,
+                                  (512 / GeoS<N, C>::NT) > 0 ? 512 / GeoS<N, C>::NT : 1)
+vhs_terms_fp32s_kernel(VhsTermsArgs a) {
+  using G = Geo<N, C>;
+  using T = float2;
+  constexpr int H = N / 2;
+  constexpr int NT = GeoS<N, C>::NT;
+  constexpr int TB = 9 * N + 4;
+  constexpr bool RYS = TermsRyStaged<C>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);
+  T* R0 = A + G::SLAB;
+  T* tab = R0 + 2 * G::SLAB;
+  T* rbuf = tab + 2 * TB;
+  const T* rX = rbuf + (RYS ? N * N : 0);
+  const T* rZ = rX + G::P * N;
+  const int t = threadIdx.x, pp = t >> 1, h = t & 1;
+  const unsigned rank = cluster_rank();
+  const int pair = blockIdx.y, e = blockIdx.z;
+  const int Mu = a.Mu;
+  const int p0 = 2 * pair;
+  const int npass = (p0 + 1 < a.Nrho ? 2 : 1) * Mu;
+  const T* Fg = static_cast<const T*>(a.Fg) + (size_t)e * G::n +
+                (size_t)rank * G::P * N * N;
+  const T* phb = static_cast<const T*>(a.ph);
+  const T* uvb = static_cast<const T*>(a.uv);
+  const T* nyb = static_cast<const T*>(a.nyq);
+  const T* rhob = static_cast<const T*>(a.rho);
+  auto term = [&](int k) { return (p0 + k / Mu) * Mu + k % Mu; };
+  auto load_tables = [&](int k) {
+    T* dst = tab + (k & 1) * TB;
+    const int pq = term(k);
+    const T* ph = phb + (size_t)pq * 3 * N;
+    const T* uv = uvb + ((size_t)e * a.Nrho * Mu + pq) * 6 * N;
+    for (int i = t; i < 3 * N; i += NT) dst[i] = ph[i];
+    for (int i = t; i < 6 * N; i += NT) dst[3 * N + i] = uv[i];
+    if (t < 3) dst[9 * N + t] = nyb[(size_t)pq * 3 + t];
+  };
+  auto rho_of = [&](int k) {
+    return rhob + ((size_t)e * a.Nrho * Mu + term(k)) * 3 * N * N;
+  };
+  // the copy helpers stride by the one-thread-per-pencil count; thread
+  // pairs split the work by running them on the even threads' indices
+  auto slab_copy = [&]() {
+    const uint32_t a0 = smem_u32(A);
+    constexpr int TOT = G::P * N * N;
+#pragma unroll 4
+    for (int j = t; j < TOT; j += NT) {
+      const uint32_t dst = a0 + (uint32_t)slab_index<N, C>(j) * 8u;
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
+                   :: "r"(dst), "l"(Fg + j) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  auto rho_copy = [&](const T* rho) {
+    constexpr int P = G::P;
+    const uint32_t s0 = smem_u32(rbuf);
+    if (RYS)
+      for (int c = t; c < N * N / 2; c += NT) cp_async16(s0 + 16u * c, rho + N * N + 2 * c);
+    const uint32_t sx = s0 + (RYS ? 8u * N * N : 0u);
+    const T* rx = rho + (size_t)rank * P * N;
+    for (int c = t; c < P * N / 2; c += NT) cp_async16(sx + 16u * c, rx + 2 * c);
+    const uint32_t szz = sx + 8u * P * N;
+    const T* rz = rho + 2 * N * N + rank * P;
+    for (int c = t; c < N * P; c += NT) {
+      const int x = c / P, j = c % P;
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
+                   :: "r"(szz + 8u * c), "l"(rz + (size_t)x * N + j) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  load_tables(0);
+  uint32_t rbase[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) rbase[c] = mapa_u32(smem_u32(R0), (uint32_t)c);
+
+  const int yl = pp / N, zz = pp % N, yy = rank * G::P + yl;
+  const float sy = (yy & 1) ? -1.f : 1.f, sz = (zz & 1) ? -1.f : 1.f;
+  T S[H];   // x = h*H + m
+#pragma unroll
+  for (int m = 0; m < H; ++m) S[m] = make_float2(0.f, 0.f);
+
+  slab_copy();
+  cp_async_wait_all();
+  __syncthreads();
+  fp32s_zpass<N, C>(A, tab, pp, h, rank);
+  __syncthreads();
+#pragma unroll 1
+  for (int k = 0; k < npass; ++k) {
+    T v[H];
+    {
+      const int base = (pp / N) * G::PLANE + (pp % N);
+#pragma unroll
+      for (int m = 0; m < H; ++m) v[m] = A[base + (2 * m + h) * G::ROW];
+    }
+    __syncthreads();
+    rho_copy(rho_of(k));
+    if (k + 1 < npass) {
+      load_tables(k + 1);
+      slab_copy();
+    }
+    fft_pair_dit<N, +1>(v, h);
+    {
+      const int lx = rank * G::P + pp / N, z = pp % N;
+      const uint32_t off = (uint32_t)((k & 1) * G::SLAB + lx * G::ROW + z) * 8u;
+#pragma unroll
+      for (int m = 0; m < H; ++m) {
+        const int y = h * H + m, c = y / G::P, j = y % G::P;
+        st_cluster(rbase[c] + off + (uint32_t)(j * G::PLANE) * 8u, v[m]);
+      }
+    }
+    cluster_arrive();
+    cp_async_wait_all();
+    __syncthreads();
+    if (k + 1 < npass) {
+      fp32s_zpass<N, C>(A, tab + ((k + 1) & 1) * TB, pp, h, rank);
+      __syncthreads();
+    }
+    cluster_wait();
+    {
+      const T* Rk = R0 + (k & 1) * G::SLAB;
+      const int base = yl * G::PLANE + zz;
+#pragma unroll
+      for (int m = 0; m < H; ++m) v[m] = Rk[base + (2 * m + h) * G::ROW];
+    }
+    fft_pair_dit<N, +1>(v, h);
+    const T* tb = tab + (k & 1) * TB;
+    const T* ut = tb + 3 * N;
+    const T* vt = tb + 6 * N;
+    const T uyz = cmul(ut[N + yy], ut[2 * N + zz]);
+    const T vyz = cmul(vt[N + yy], vt[2 * N + zz]);
+    const T rx = rX[yl * N + zz];
+    const T* rY = RYS ? rbuf : rho_of(k) + N * N;
+    const bool hi = k >= Mu;
+#pragma unroll
+    for (int m = 0; m < H; ++m) {
+      const int x = h * H + m;
+      const T um = cmul(ut[x], uyz), vm = cmul(vt[x], vyz);
+      const float Ax = um.x + vm.x, Ay = um.y + vm.y;
+      const float Bx = um.x - vm.x, By = um.y - vm.y;
+      const T ry = rY[x * N + zz], rz = rZ[x * G::P + yl];
+      const float xs = (m & 1) ? -1.f : 1.f;   // (-1)^x, H even
+      const float sR = xs * rx.x + sy * ry.x + sz * rz.x;
+      const float cI = xs * rx.y + sy * ry.y + sz * rz.y;
+      const float Cm = v[m].x, sm = v[m].y;
+      const float hh = Cm * (Ax + Cm) + sm * (Bx - sm) + sR * (By + sR) -
+                       cI * (Ay + cI);
+      if (hi) S[m].y += hh;
+      else S[m].x += hh;
+    }
+  }
+
+  // forward FFT of S = S_p0 + i S_p1: x pass (DIF: outputs lx = 2m + h),
+  // exchange into X-slabs, y pass, z pass
+  fft_pair_dif<N, -1>(S, h);
+  {
+    const uint32_t a0 = smem_u32(A);
+    const uint32_t off = (uint32_t)(yy * G::ROW + zz) * 8u;
+#pragma unroll
+    for (int m = 0; m < H; ++m) {
+      const int lx = 2 * m + h, c = lx / G::P, j = lx % G::P;
+      st_cluster(mapa_u32(a0, (uint32_t)c) + off + (uint32_t)(j * G::PLANE) * 8u, S[m]);
+    }
+  }
+  cluster_arrive();
+  cluster_wait();
+  {
+    T w[H];
+    const int base = (pp / N) * G::PLANE + (pp % N);
+#pragma unroll
+    for (int m = 0; m < H; ++m) w[m] = A[base + (2 * m + h) * G::ROW];
+    fft_pair_dit<N, -1>(w, h);
+    __syncthreads();   // all column reads done before the in-place writes
+#pragma unroll
+    for (int m = 0; m < H; ++m) A[base + (h * H + m) * G::ROW] = w[m];
+  }
+  __syncthreads();
+  {
+    T w[H];
+    const int base = (pp / N) * G::PLANE + (pp % N) * G::ROW;
+#pragma unroll
+    for (int m = 0; m < H; ++m) w[m] = A[base + 2 * m + h];
+    fft_pair_dit<N, -1>(w, h);
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < H; ++m) A[base + h * H + m] = w[m];
+  }
+  __syncthreads();
+  const size_t off = (size_t)rank * G::P * N * N;
+  const float* b1a = static_cast<const float*>(a.b1w) + (size_t)p0 * G::n + off;
+  const float* b1b = (p0 + 1 < a.Nrho) ? b1a + G::n : nullptr;
+  const int npairs = (a.Nrho + 1) / 2;
+  T* Hout = static_cast<T*>(a.H) + ((size_t)e * npairs + pair) * G::n + off;
+  for (int j = t; j < G::P * N * N; j += NT) {
+    const T hv = A[slab_index<N, C>(j)];
+    const float w0 = b1a[j], w1 = b1b ? b1b[j] : 0.f;
+    Hout[j] = make_float2(hv.x * w0 + hv.y * w1, hv.y * w0 - hv.x * w1);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Epilogue: one cluster (FP64) per eval.
 // ---------------------------------------------------------------------------
 template <int N, int C>
