@@ -228,6 +228,24 @@ def stress_line(torch, timed, args):
             'finite': ok}
 
 
+def stress_solver_line(torch, timed, args):
+    """Steps of the stress configuration's solver: Mach-1.5 normal shock of
+    hard spheres, N=48^3 on [-8,8]^3, M=32, Nrho=24, Ne=32, K=3 (96 points),
+    inlet boundaries, lse-rk45 (5 RHS stages per step), FP32 operator, one
+    CUDA graph per step."""
+    from dgfs1d_gpu_b200.config import Config
+    from dgfs1d_gpu_b200.configs import normal_shock_std_ini
+    from dgfs1d_gpu_b200.std.solver import DGFSStd1D
+    sol = DGFSStd1D(Config(normal_shock_std_ini()))
+    sol.capture_step()
+    ms = timed(sol.step, 3, 1)
+    ok = bool(torch.isfinite(sol.u).all())
+    return {'workload': 'normal shock Mach 1.5, HS, N=48, M=32, Nrho=24, '
+                        'Ne=32, K=3, lse-rk45, FP32 operator, graph per step',
+            'ms_per_step': ms, 'evals_per_s': 5 * 96 / (ms * 1e-3),
+            'projected_s_for_500_steps': 500 * ms * 1e-3, 'finite': ok}
+
+
 def solver_line(torch, timed, args):
     """The whole dgfsStd1D step on the batched FP32 Couette configuration
     (ssp-rk3: three RHS stages of 24 points each), eager and as one CUDA
@@ -377,6 +395,7 @@ def main():
     # a bounded time on operator pairs, then timed and compared with FP64
     solver = solver_line(torch, timed, args)
     stress = stress_line(torch, timed, args)
+    stress_solver = stress_solver_line(torch, timed, args)
     sur = None
     if not args.no_surrogate:
         sur = surrogate_line(torch, prm, fd, op32, op64, timed, args)
@@ -487,6 +506,7 @@ def main():
             'surrogate': sur,
             'solver_step': solver,
             'stress_n48': stress,
+            'stress_solver_n48': stress_solver,
             'autotune_terms_ms': {str(k): round(v, 4) for k, v in tune.items()},
             'terms_cluster': op32.variant,
             'cpu_baseline': cpu,

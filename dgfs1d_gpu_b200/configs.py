@@ -185,3 +185,97 @@ omega = 0.81
 muRef = 2.117e-5
 Tref = 273
 """.format(penalty)
+
+
+def normal_shock_std_ini(Mach=1.5, Ne=32, K=3, Nv=48, Nrho=24, M=32, dev=8.0,
+                         omega=0.5, scheme='lse-rk45', dt=None, nsteps=500,
+                         half_width=20.0, ramp=2.0, noise=0.005,
+                         seed=20261203, precision_mode='fp32', sphere='full',
+                         basis='nodal-sem-gll'):
+    """Normal shock of a monatomic hard-sphere gas: Rankine-Hugoniot states
+    at Mach `Mach` (gamma = 5/3), joined by a tanh ramp of width `ramp` mean
+    free paths on x in [-half_width, half_width] mean free paths (the mean
+    free path is the reference length H0, Kn = 1), with inlet boundaries at
+    both ends and (1 + noise U[-1, 1]) seeded noise."""
+    g = 5.0 / 3.0
+    T0, molarMass0 = 273., 39.96e-3
+    H0 = 1e-3
+    rho1 = rho0_for_knudsen(1.0, H0=H0, omega=omega)
+    R = R0 / molarMass0
+    u1 = Mach * math.sqrt(g * R * T0)
+    r = (g + 1) * Mach ** 2 / ((g - 1) * Mach ** 2 + 2)
+    tr = ((2 * g * Mach ** 2 - (g - 1)) * ((g - 1) * Mach ** 2 + 2)
+          / ((g + 1) ** 2 * Mach ** 2))
+    rho2, T2, u2 = rho1 * r, T0 * tr, u1 / r
+    u0 = math.sqrt(2 * R0 / molarMass0 * T0)
+    if dt is None:
+        # advective CFL of the nodal DG scheme on the finest node spacing
+        dx = 2 * half_width / Ne / (K * K)
+        dt = 0.5 * dx / (dev + u1 / u0)
+    pm = f'precision-mode = {precision_mode}\n' if precision_mode else ''
+    return f"""
+[config]
+precision = double
+[mesh]
+xlo = {-half_width * H0!r}
+xhi = {half_width * H0!r}
+Ne = {Ne}
+H0 = {H0}
+[basis]
+kind = {basis}
+K = {K}
+Nqr = {K}
+[non-dim]
+T0 = {T0}
+rho0 = {rho1!r}
+molarMass0 = {molarMass0}
+[velocity-mesh]
+Nv = {Nv}
+Nrho = {Nrho}
+dev = {dev}
+cmax = 0
+Tmax = {T0}
+[spherical-design-rule]
+ssrule = womersley
+M = {M}
+sphere = {sphere}
+[scattering-model]
+type = vhs-gll
+omega = {omega}
+dRef = 4.17e-10
+Tref = 273
+muRef = 2.117e-5
+{pm}
+[time-integrator]
+scheme = {scheme}
+controller = none
+tstart = 0.0
+tend = {dt * nsteps!r}
+dt = {dt!r}
+[soln-ics]
+type = normal-shock
+rho1 = {rho1!r}
+T1 = {T0}
+ux1 = {u1!r}
+rho2 = {rho2!r}
+T2 = {T2!r}
+ux2 = {u2!r}
+x0 = 0.0
+width = {ramp * H0!r}
+noise = {noise}
+seed = {seed}
+[soln-bcs-xlo]
+type = dgfs-inlet
+rho = {rho1!r}
+T = {T0}
+ux = {u1!r}
+uy = 0
+uz = 0
+[soln-bcs-xhi]
+type = dgfs-inlet
+rho = {rho2!r}
+T = {T2!r}
+ux = {u2!r}
+uy = 0
+uz = 0
+"""

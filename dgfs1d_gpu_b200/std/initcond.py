@@ -4,6 +4,10 @@
 the velocity grid, nondimensional).  ``maxwellian-noise`` (no counterpart in
 the reference) multiplies the Maxwellian by (1 + amp U[-1, 1]), i.i.d. per
 phase-space point from a seeded generator (keys ``noise``, ``seed``).
+``normal-shock`` (no counterpart in the reference) joins an upstream and a
+downstream Maxwellian by a tanh ramp in x (keys ``rho1 T1 ux1 rho2 T2 ux2``,
+dimensional like ``maxwellian``; ``x0``, ``width`` in mesh units; optional
+``noise``, ``seed``).
 """
 import numpy as np
 
@@ -79,3 +83,38 @@ class DGFSBKWInitConditionStd(DGFSInitConditionStd):
 def get_initcond(cfg, vm, name, **kwargs):
     cls = subclass_where(DGFSInitConditionStd, model=cfg.lookup(name, 'type'))
     return cls(cfg, vm, name, **kwargs)
+
+
+class DGFSNormalShockInitConditionStd(DGFSInitConditionStd):
+    model = 'normal-shock'
+
+    def load_parameters(self, name):
+        vm, cfg = self.vm, self.cfg
+        u0 = vm.u0()
+        self._states = []
+        for k in ('1', '2'):
+            rho = cfg.lookupfloat(name, 'rho' + k) / vm.rho0()
+            T = cfg.lookupfloat(name, 'T' + k) / vm.T0()
+            ux = cfg.lookupfloat(name, 'ux' + k) / u0
+            self._states.append((rho, T, ux))
+        self._x0 = cfg.lookupfloat(name, 'x0') / vm.H0()
+        self._w = cfg.lookupfloat(name, 'width') / vm.H0()
+        self._amp = cfg.lookupordefault(name, 'noise', 0.0)
+        self._seed = cfg.lookupordefault(name, 'seed', 20261203)
+
+    def perform_precomputation(self):
+        cv = self.vm.cv()
+        self._M = []
+        for rho, T, ux in self._states:
+            u = np.array([ux, 0.0, 0.0]).reshape(3, 1)
+            self._M.append(rho / (np.pi * T) ** 1.5
+                           * np.exp(-np.sum((cv - u) ** 2, axis=0) / T))
+        self._init_vals = self._M[0]
+
+    def apply_init_vals(self, usol, Nq, Ne, xsol=None):
+        w = 0.5 * (1 + np.tanh((np.asarray(xsol) - self._x0) / self._w))
+        usol[:, :, :] = ((1 - w)[:, :, None] * self._M[0][None, None, :]
+                         + w[:, :, None] * self._M[1][None, None, :])
+        if self._amp:
+            rng = np.random.default_rng(self._seed)
+            usol *= 1 + self._amp * rng.uniform(-1, 1, usol.shape)

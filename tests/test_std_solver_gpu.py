@@ -118,3 +118,23 @@ def test_graph_captured_step_equals_eager_steps(scheme, precision_mode):
     torch.cuda.synchronize()
     assert torch.equal(a.u, b.u)
     assert torch.isfinite(a.u).all()
+
+
+def test_normal_shock_inlet_lse_rk45_graph_steps():
+    """The stress configuration's set-up on a small grid: Rankine-Hugoniot
+    states at Mach 1.5 joined by a tanh ramp, inlet boundaries at both ends,
+    lse-rk45, FP32 operator, hard spheres; graph-captured steps equal eager
+    steps bit for bit and keep the inflow/outflow densities."""
+    from dgfs1d_gpu_b200.configs import normal_shock_std_ini
+    ini = normal_shock_std_ini(Nv=16, Nrho=8, M=6, Ne=8, dev=8.0,
+                               sphere='auto', nsteps=4)
+    a, b = _solver(ini), _solver(ini)
+    b.capture_step()
+    for _ in range(4):
+        a.step()
+        b.step()
+    torch.cuda.synchronize()
+    assert torch.equal(a.u, b.u) and torch.isfinite(a.u).all()
+    m = a.dg.moments(a.u).cpu().numpy()
+    rho_l, rho_r = m[0, 0, 0], m[-1, -1, 0]
+    assert abs(rho_l - 1.0) < 2e-2 and abs(rho_r - 1.714) < 3e-2, (rho_l, rho_r)
