@@ -199,17 +199,26 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
         for (int k = 0; k < 5; ++k) a.moments[(size_t)e * 5 + k] = mom[k];
     }
     __syncthreads();
-    // 1-D Maxwellian factors and their spectra (direct DFT, table twiddles)
+    // 1-D Maxwellian factors (3N values, each computed once; staged in the
+    // receive slab past the moment partials, which peers read only below
+    // offset 5 NT + 5) and their spectra (direct DFT, table twiddles)
+    double* mv = red + 6 * G::NT + 8;
     for (int i = t; i < 3 * N; i += G::NT) {
-      const int ax = i / N, k = i % N;
+      const int ax = i / N, j = i % N;
       const double rho = mom[0], Tm = mom[4], u = mom[1 + ax];
       const double amp = (ax == 0) ? rho / pow(M_PI * Tm, 1.5) : 1.0;
+      const double d = a.c0[j] - u;
+      mv[i] = amp * exp(-d * d / Tm);
+    }
+    __syncthreads();
+    for (int i = t; i < 3 * N; i += G::NT) {
+      const int ax = i / N, k = i % N;
       double re = 0, im = 0;
+#pragma unroll 8
       for (int j = 0; j < N; ++j) {
-        const double d = a.c0[j] - u;
-        const double m = amp * exp(-d * d / Tm);
         constexpr int off = tw_offset(N);
         const double2 w = c_tw64[off + (j * k) % N];
+        const double m = mv[ax * N + j];
         re += m * w.x;
         im += m * w.y;
       }
@@ -236,6 +245,7 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
   // F = FFT(f)/n; write F (FP64) or F_g = F - mhat (FP32); then A <- b2 F
   const double inv_n = 1.0 / (double)G::n;
   const size_t gbase = (size_t)e * G::n + (size_t)rank * G::P * N * N;
+#pragma unroll 4
   for (int j = t; j < G::P * N * N; j += G::NT) {
     const int si = slab_index<N, C>(j);
     T Fv = A[si];
@@ -716,6 +726,7 @@ vhs_nyq_planes_kernel(VhsTermsArgs a) {
   const int P = tt / N, i = tt % N;
   const int Mu = a.Mu;
   const float2* Fny = static_cast<const float2*>(a.Fny) + (size_t)e * 3 * N * N;
+#pragma unroll 4
   for (int j = t; j < 3 * N * N; j += 6 * N)
     Fp[(j / N) * ROW + j % N] = Fny[j];
   for (int j = t; j < 2 * (3 * N + 3); j += 6 * N) {
@@ -1290,6 +1301,7 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
         acc[u][1] = T{0, 0};
       }
     }
+#pragma unroll 2
     for (int p = 0; p < a.Nrho; ++p) {
       const size_t hb = ((size_t)e * a.Nrho + p) * G::n + off;
       if (a.h_double) {
