@@ -400,7 +400,7 @@ extern "C" const double* dgfs_vhs_last_moments(dgfs_vhs_handle h) {
 
 // FP32 terms kernel at cluster size C (each C must divide N and fit three
 // slabs in shared memory).
-template <int N, int C>
+template <int N, int C, bool ASYNC_TAB = false>
 static int launch_terms32_c(const VhsTermsArgs& a, int nevals, int Nrho,
                             cudaStream_t st) {
   using G = Geo<N, C>;
@@ -409,7 +409,7 @@ static int launch_terms32_c(const VhsTermsArgs& a, int nevals, int Nrho,
                       2 * (9 * N + 4) * sizeof(float2) +
                       (size_t)((TermsRyStaged<C>::value ? N * N : 0) +
                                2 * G::P * N) * sizeof(float2);
-  return launch_cluster(vhs_terms_fp32_kernel<N, C>,
+  return launch_cluster(vhs_terms_fp32_kernel<N, C, ASYNC_TAB>,
                         dim3(C, (Nrho + 1) / 2, nevals), dim3(G::NT), C, smem,
                         st, a);
 }
@@ -429,12 +429,13 @@ static int launch_terms32s_c(const VhsTermsArgs& a, int nevals, int Nrho,
 }
 
 // Variant codes: the cluster size C for the one-thread-per-pencil kernel,
-// 100 + C for the split-pencil kernel.
+// 100 + C for the split-pencil kernel, 200 + C for the one-thread kernel with
+// asynchronous table loads.
 template <int N> struct Terms32Variants;
 template <> struct Terms32Variants<8> { static constexpr int v[2] = {1, 2}; };
 template <> struct Terms32Variants<16> { static constexpr int v[2] = {1, 2}; };
 template <> struct Terms32Variants<24> { static constexpr int v[3] = {3, 4, 6}; };
-template <> struct Terms32Variants<32> { static constexpr int v[4] = {4, 8, 104, 108}; };
+template <> struct Terms32Variants<32> { static constexpr int v[5] = {4, 8, 104, 108, 204}; };
 template <> struct Terms32Variants<48> { static constexpr int v[1] = {16}; };
 
 template <int N>
@@ -452,6 +453,7 @@ static int launch_terms32(int c, const VhsTermsArgs& a, int nevals, int Nrho,
     if (c == 8) return launch_terms32_c<N, 8>(a, nevals, Nrho, st);
     if (c == 104) return launch_terms32s_c<N, 4>(a, nevals, Nrho, st);
     if (c == 108) return launch_terms32s_c<N, 8>(a, nevals, Nrho, st);
+    if (c == 204) return launch_terms32_c<N, 4, true>(a, nevals, Nrho, st);
   } else if constexpr (N == 48) {
     if (c == 16) return launch_terms32_c<N, 16>(a, nevals, Nrho, st);
   }
@@ -1524,7 +1526,7 @@ extern "C" int dgfs_vhs_variants(int32_t N, int32_t* out, int32_t max) {
     case 8: v = Terms32Variants<8>::v; n = 2; break;
     case 16: v = Terms32Variants<16>::v; n = 2; break;
     case 24: v = Terms32Variants<24>::v; n = 3; break;
-    case 32: v = Terms32Variants<32>::v; n = 4; break;
+    case 32: v = Terms32Variants<32>::v; n = 5; break;
     case 48: v = Terms32Variants<48>::v; n = 1; break;
     default: return fail(DGFS_ERR_UNSUPPORTED, "N not compiled in");
   }

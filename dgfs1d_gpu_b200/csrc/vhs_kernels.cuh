@@ -831,7 +831,7 @@ __device__ __forceinline__ void fp32_issue_rho_copy(float2* rbuf,
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
-template <int N, int C>
+template <int N, int C, bool ASYNC_TAB = false>
 __global__ void __launch_bounds__(Geo<N, C>::NT, 1)
 vhs_terms_fp32_kernel(VhsTermsArgs a) {
   using G = Geo<N, C>;
@@ -859,14 +859,30 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
   const T* rhob = static_cast<const T*>(a.rho);
   // term k -> (p, q) = (p0 + k / Mu, k % Mu); tables index p*Mu + q
   auto term = [&](int k) { return (p0 + k / Mu) * Mu + k % Mu; };
+  // ASYNC_TAB: the tables go through cp.async (they join the next commit
+  // group) instead of a register round trip
   auto load_tables = [&](int k) {
     T* dst = tab + (k & 1) * TB;
     const int pq = term(k);
     const T* ph = phb + (size_t)pq * 3 * N;
     const T* uv = uvb + ((size_t)e * a.Nrho * Mu + pq) * 6 * N;
-    for (int i = t; i < 3 * N; i += G::NT) dst[i] = ph[i];
-    for (int i = t; i < 6 * N; i += G::NT) dst[3 * N + i] = uv[i];
-    if (t < 3) dst[9 * N + t] = nyb[(size_t)pq * 3 + t];
+    if (ASYNC_TAB) {
+      const uint32_t d0 = smem_u32(dst);
+      for (int i = t; i < 3 * N; i += G::NT)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
+                     :: "r"(d0 + 8u * i), "l"(ph + i) : "memory");
+      for (int i = t; i < 6 * N; i += G::NT)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
+                     :: "r"(d0 + 8u * (3 * N + i)), "l"(uv + i) : "memory");
+      if (t < 3)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
+                     :: "r"(d0 + 8u * (9 * N + t)), "l"(nyb + (size_t)pq * 3 + t)
+                     : "memory");
+    } else {
+      for (int i = t; i < 3 * N; i += G::NT) dst[i] = ph[i];
+      for (int i = t; i < 6 * N; i += G::NT) dst[3 * N + i] = uv[i];
+      if (t < 3) dst[9 * N + t] = nyb[(size_t)pq * 3 + t];
+    }
   };
   auto rho_of = [&](int k) {
     return rhob + ((size_t)e * a.Nrho * Mu + term(k)) * 3 * N * N;
