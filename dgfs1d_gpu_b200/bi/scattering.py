@@ -3,6 +3,8 @@
 ``vss`` keeps the constructor, parameters and ``fs(idx, d_f1, d_f2, d_Q,
 elem, upt, uptout)`` of dgfs1D/bi/scattering.py:47-321 (idx = 'pq'; Q_pq is
 accumulated into d_Q).  Precomputation of the pair weights runs on the GPU.
+``[scattering-model] precision-mode = fp64|fp32`` selects the operator's
+arithmetic (default: fp64 for double, fp32 for float configurations).
 """
 import itertools as it
 from math import gamma
@@ -65,10 +67,13 @@ class DGFSBiVSSScatteringModel(DGFSScatteringModelBi):
 
     def perform_precomputation(self):
         vm = self.vm
+        default = 'fp64' if self.cfg.dtype == np.float64 else 'fp32'
+        prec = self.cfg.lookupordefault('scattering-model', 'precision-mode',
+                                        default)
         self._op = VSSOperator(vm.Nv(), vm.L(), vm.qz(), vm.qw(), vm.sz(),
                                vm.sw(), self._szpre, vm.masses(), self._gamma,
                                self._eta, self._prefactor,
-                               max_evals=self._max_evals)
+                               max_evals=self._max_evals, precision=prec)
 
     @property
     def operator(self):

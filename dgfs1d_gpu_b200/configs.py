@@ -88,8 +88,10 @@ uz = 0
 def couette_bi_ini(Ne=3, K=3, Nv=8, Nrho=4, M=6, Mpre=12, dev=5.0,
                    scheme='euler', dt=0.0005, nsteps=3, uwall=0.1,
                    noise=0.02, seed=20261203, compat=0,
-                   masses=(39.96e-3, 83.77e-3)):
-    """Binary Couette (examples/bi/couette/dgfs1D.ini parameters, small)."""
+                   masses=(39.96e-3, 83.77e-3), precision_mode=None):
+    """Binary Couette (examples/bi/couette/dgfs1D.ini parameters, small).
+    ``precision_mode`` ('fp64'/'fp32') sets [scattering-model] precision-mode."""
+    pm = '' if precision_mode is None else f'precision-mode = {precision_mode}'
     T0, m0 = 273., masses[0]
     u0 = math.sqrt(2 * R0 / m0 * T0)
     rho0 = 0.00011140244750324529
@@ -126,6 +128,7 @@ M = {M}
 type = vss
 ssrulepre = womersley
 Mpre = {Mpre}
+{pm}
 alpha00 = 1.4
 omega00 = 0.81
 dRef00 = 4.11e-10

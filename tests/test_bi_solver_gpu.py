@@ -59,3 +59,22 @@ def test_bi_steps_match_oracle(scheme, compat):
         t += s.dt
     for p in range(2):
         assert _rel(got[p], us[p]) < 1e-11, (scheme, p)
+
+
+def test_bi_fp32_precision_mode_tracks_fp64():
+    """[scattering-model] precision-mode = fp32 selects the FP32 VSS operator;
+    a few steps stay within FP32 accuracy of the FP64 plugin."""
+    from dgfs1d_gpu_b200 import build
+    build.build()
+    from dgfs1d_gpu_b200.bi.solver import DGFSBi1D
+    out = {}
+    for pm in ('fp64', 'fp32'):
+        s = DGFSBi1D(Config(couette_bi_ini(scheme='ssp-rk2', nsteps=3,
+                                           precision_mode=pm)))
+        assert s.sm.operator.precision == pm
+        s.run(3)
+        torch.cuda.synchronize()
+        out[pm] = [u.cpu().numpy() for u in s.us]
+    for p in range(2):
+        assert np.all(np.isfinite(out['fp32'][p]))
+        assert _rel(out['fp32'][p], out['fp64'][p]) < 1e-5, p
