@@ -33,11 +33,33 @@ constexpr int WD = 32;   // width
 constexpr int PJ = 128;  // projection width
 constexpr int CIN = 4;   // input features
 
+// erf by Abramowitz & Stegun, Handbook of Mathematical Functions, 7.1.28:
+// erf(x) = 1 - (1 + a1 x + ... + a6 x^6)^-16 for x >= 0, |error| <= 3e-7
+// (about 2e-6 evaluated in FP32), odd extension.  Six FMAs, four squarings
+// and one approximate reciprocal: GELU is the hot scalar of the projection
+// (128 per grid point).
+__device__ __forceinline__ float erf_as(float x) {
+  const float ax = fabsf(x);
+  float p = fmaf(ax, 4.30638e-5f, 2.765672e-4f);
+  p = fmaf(ax, p, 1.520143e-4f);
+  p = fmaf(ax, p, 9.2705272e-3f);
+  p = fmaf(ax, p, 4.22820123e-2f);
+  p = fmaf(ax, p, 7.05230784e-2f);
+  p = fmaf(ax, p, 1.f);
+  p *= p;
+  p *= p;
+  p *= p;
+  p *= p;
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(p));
+  return copysignf(1.f - r, x);
+}
 __device__ __forceinline__ float gelu(float x) {
-  return 0.5f * x * (1.f + erff(x * 0.70710678118654752f));
+  const float h = 0.5f * x;
+  return fmaf(h, erf_as(x * 0.70710678118654752f), h);
 }
 __device__ __forceinline__ float gelu_d(float x) {
-  return 0.5f * (1.f + erff(x * 0.70710678118654752f)) +
+  return 0.5f * (1.f + erf_as(x * 0.70710678118654752f)) +
          x * 0.39894228040143268f * expf(-0.5f * x * x);
 }
 __device__ __forceinline__ float bf(const __nv_bfloat16 v) {
@@ -117,6 +139,22 @@ __device__ __forceinline__ void block_sum5(double* s, double* red) {
 constexpr int FCH = 64;  // chunks per sample
 static_assert(CIN == 4, "the feature pass packs four BF16 values");
 
+// Totals of the FCH partial records [FCH][6] of one sample, by one warp:
+// lane l adds chunks l and l + 32, then an xor-shuffle tree.  Every step adds
+// the same two operands on both lanes of a pair, so all lanes (and all CTAs
+// reading the same partials) end with bitwise identical totals.
+static_assert(FCH == 64, "reduce_parts assumes 64 chunks");
+__device__ __forceinline__ void reduce_parts(const double* P, double* m) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double v = P[lane * 6 + k] + P[(lane + 32) * 6 + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    m[k] = v;
+  }
+}
+
 __device__ __forceinline__ void feat_load(const FeatArgs& a, int b, long i,
                                           double& fv, double& cx, double& cy,
                                           double& cz) {
@@ -131,12 +169,9 @@ __device__ __forceinline__ void feat_load(const FeatArgs& a, int b, long i,
 
 struct FeatState { double rho, ux, uy, uz, T, amp, irho; };
 
-__device__ __forceinline__ FeatState feat_state(const FeatArgs& a, int b) {
-  const double* P = a.part + (long)b * FCH * 6;
-  double m[5] = {0, 0, 0, 0, 0};
-  for (int c = 0; c < FCH; ++c)
-#pragma unroll
-    for (int k = 0; k < 5; ++k) m[k] += P[c * 6 + k];
+// State of one sample from the totals m of its partial records.
+__device__ __forceinline__ FeatState feat_state(const FeatArgs& a,
+                                                const double* m) {
   FeatState s;
   double rho = m[0] * a.cw;
   s.ux = m[1] * a.cw / rho; s.uy = m[2] * a.cw / rho; s.uz = m[3] * a.cw / rho;
@@ -158,12 +193,13 @@ __global__ void __launch_bounds__(256) fno_features_kernel(FeatArgs a) {
   const int ch = blockIdx.x, b = blockIdx.y, t = threadIdx.x, N = a.N;
   const long n = (long)N * N * N, len = n / FCH, i0 = ch * len;
   if (PASS >= 1) {
-    if (t == 0) st = feat_state(a, b);
-    if (PASS == 2 && t == 1) {
-      double s2 = 0;
-      const double* P = a.part + (long)b * FCH * 6;
-      for (int c = 0; c < FCH; ++c) s2 += P[c * 6 + 5];
-      sig_s = fmax(sqrt(s2 / (double)n), 1e-300);
+    if (t < 32) {
+      double m[6];
+      reduce_parts(a.part + (long)b * FCH * 6, m);
+      if (t == 0) {
+        st = feat_state(a, m);
+        if (PASS == 2) sig_s = fmax(sqrt(m[5] / (double)n), 1e-300);
+      }
     }
     if (PASS == 2)
       for (int i = t; i < CIN * WD + WD; i += 256) wl[i] = bf(a.w16[a.L.P + i]);
@@ -716,16 +752,15 @@ __global__ void __launch_bounds__(256) fno_output_kernel(OutArgs a) {
     if (t < 5) a.part[((long)b * FCH + ch) * 6 + t] = red[t];
     return;
   }
-  if (t < 5) {
-    double m[5] = {0, 0, 0, 0, 0};
-    const double* P = a.part + (long)b * FCH * 6;
-    for (int c = 0; c < FCH; ++c)
+  if (t < 32) {
+    double m[6];
+    reduce_parts(a.part + (long)b * FCH * 6, m);
+    if (t < 5) {
+      double l = 0;
 #pragma unroll
-      for (int k = 0; k < 5; ++k) m[k] += P[c * 6 + k];
-    double l = 0;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) l += a.Ginv[t * 5 + k] * m[k];
-    lam_s[t] = l;
+      for (int k = 0; k < 5; ++k) l += a.Ginv[t * 5 + k] * m[k];
+      lam_s[t] = l;
+    }
   }
   __syncthreads();
   const double l0 = lam_s[0], l1 = lam_s[1], l2 = lam_s[2], l3 = lam_s[3],
