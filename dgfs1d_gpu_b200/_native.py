@@ -110,6 +110,7 @@ _SIGNATURES = [
     ('dgfs_fno_last_loss', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_fno_set_tensor_cores', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ('dgfs_fno_set_fused', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_fno_error', ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ('dgfs_vhs_destroy', ctypes.c_int, [ctypes.c_void_p]),
     ('dgfs_vhs_profile', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),

@@ -1577,6 +1577,8 @@ struct dgfs_fno_s {
   double* loss = nullptr;
   int* err = nullptr;                // device error flag (bounded waits)
   int use_tc = 1;                    // dense layers on tcgen05 tensor cores
+  int use_fused = 1;                 // eval: fused spectral passes
+  float2 *Yp = nullptr, *Sp = nullptr;  // eval: yz spectra, x-mixed spectra
   std::vector<void*> owned;
 };
 
@@ -1607,6 +1609,8 @@ extern "C" int dgfs_fno_create(const dgfs_fno_desc* d, dgfs_fno_handle* out) {
     return fail(DGFS_ERR_INVALID, "FNO max_batch must be in [1, 32]");
   if (!(d->L > 0) || !(d->q_scale > 0))
     return fail(DGFS_ERR_INVALID, "FNO needs L > 0 and q_scale > 0");
+  // the fused evaluation kernels use the register FFTs' twiddle tables
+  if (int rc = ensure_twiddles()) return rc;
   auto* h = new dgfs_fno_s();
   h->N = d->N; h->K = d->modes; h->maxB = d->max_batch;
   h->n = (long)h->N * h->N * h->N;
@@ -1674,6 +1678,8 @@ extern "C" int dgfs_fno_create(const dgfs_fno_desc* d, dgfs_fno_handle* out) {
   A(&h->Uh, B * nm * fno::WD);
   A(&h->gUh, B * nm * fno::WD);
   A(&h->gVh, B * nm * fno::WD);
+  A(&h->Yp, B * N * K * K * fno::WD);
+  A(&h->Sp, B * N * K * K * fno::WD);
   A(&h->T1, B * K * N * N * fno::WD);
   A(&h->T2, B * K * K * N * fno::WD);
   A(&h->U, B * n * fno::WD);
@@ -1849,6 +1855,55 @@ static int fno_forward(dgfs_fno_s* h, const void* f, int f_double,
   return DGFS_OK;
 }
 
+// Inference forward with the fused spectral passes (see fno_kernels.cuh):
+// per layer one x-mix launch and one yz-inverse + dense launch, and one
+// yz-forward launch for the next layer's spectra.
+template <int N, int K>
+static int fno_forward_fused(dgfs_fno_s* h, const void* f, int f_double,
+                             const int32_t* src_slots, int src_base, int B,
+                             cudaStream_t st) {
+  using namespace fno;
+  const long R = (long)B * h->n;
+  FeatArgs fa{};
+  fa.f = f; fa.f_double = f_double; fa.src_slots = src_slots; fa.src_base = src_base;
+  fa.c0 = h->c0; fa.cw = h->cw; fa.N = N; fa.w16 = h->p16; fa.L = h->L;
+  fa.x0 = h->x0; fa.v0 = h->v[0]; fa.qs = h->qs; fa.part = h->fpart;
+  const dim3 fg(FCH, B);
+  fno_features_kernel<0><<<fg, 256, 0, st>>>(fa);
+  fno_features_kernel<1><<<fg, 256, 0, st>>>(fa);
+  fno_features_kernel<2><<<fg, 256, 0, st>>>(fa);
+  DGFS_CUDA(cudaGetLastError());
+  const int fsm = N * K * WD * (int)sizeof(float2);
+  const int xsm = 2 * XM_SB * K * WD * (int)sizeof(float2);
+  const int ism = YzInvGeo<N, K>::SMEM;
+  DGFS_CUDA(cudaFuncSetAttribute(fno_yzfwd_kernel<N, K>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
+  DGFS_CUDA(cudaFuncSetAttribute(fno_xmix_kernel<N, K>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, xsm));
+  DGFS_CUDA(cudaFuncSetAttribute(fno_yzinv_dense_kernel<N, K>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, ism));
+  const dim3 pg(N, B);
+  fno_yzfwd_kernel<N, K><<<pg, 256, fsm, st>>>(h->v[0], h->Yp);
+  DGFS_CUDA(cudaGetLastError());
+  for (int l = 0; l < 4; ++l) {
+    fno_xmix_kernel<N, K><<<dim3(K * K, (B + XM_SB - 1) / XM_SB), K * 32, xsm, st>>>(
+        h->Yp, h->p16 + h->L.W[l], h->Sp, B);
+    YzInvArgs ya{};
+    ya.S = h->Sp; ya.v = h->v[l]; ya.w16 = h->p16; ya.offD = h->L.D[l];
+    ya.offd = h->L.d[l]; ya.vout = h->v[l + 1]; ya.act = l < 3 ? 1 : 0;
+    ya.err = h->err;
+    fno_yzinv_dense_kernel<N, K><<<dim3(N * YzInvGeo<N, K>::ZP, B),
+                                   YzInvGeo<N, K>::NT, ism, st>>>(ya);
+    if (l < 3) fno_yzfwd_kernel<N, K><<<pg, 256, fsm, st>>>(h->v[l + 1], h->Yp);
+    DGFS_CUDA(cudaGetLastError());
+  }
+  TcArgs ta{};
+  ta.x = h->v[4]; ta.w16 = h->p16; ta.offW = h->L.Q1; ta.offb = h->L.q1;
+  ta.offq2 = h->L.q2; ta.offq2b = h->L.q2b; ta.out = h->out; ta.R = R;
+  ta.err = h->err;
+  return fno_tc<PJ, 1>(h, ta, st);
+}
+
 template <int KA, int KB>
 static int fno_wgrad(dgfs_fno_s* h, const __nv_bfloat16* A, const float* Bm,
                      long R, long off, cudaStream_t st) {
@@ -1927,8 +1982,10 @@ static int fno_eval_t(dgfs_fno_s* h, const void* f, int f_double, void* Q,
   for (int off = 0; off < nevals; off += h->maxB) {
     const int B = std::min(h->maxB, nevals - off);
     int rc;
-    if ((rc = fno_forward<N, K>(h, f, f_double, src_slots ? src_slots + off : nullptr,
-                                src_base + off, B, st, false)))
+    const int32_t* ss = src_slots ? src_slots + off : nullptr;
+    if ((rc = (h->use_fused && h->use_tc)
+                  ? fno_forward_fused<N, K>(h, f, f_double, ss, src_base + off, B, st)
+                  : fno_forward<N, K>(h, f, f_double, ss, src_base + off, B, st, false)))
       return rc;
     fno::OutArgs oa{};
     oa.out = h->out; oa.qs = h->qs; oa.sQ = h->sQ; oa.c0 = h->c0; oa.cw = h->cw;
@@ -2008,6 +2065,12 @@ extern "C" int dgfs_fno_last_loss(dgfs_fno_handle h, double* host, int32_t B) {
 extern "C" int dgfs_fno_set_tensor_cores(dgfs_fno_handle h, int32_t enable) {
   if (!h) return fail(DGFS_ERR_INVALID, "null handle");
   h->use_tc = enable ? 1 : 0;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_fno_set_fused(dgfs_fno_handle h, int32_t enable) {
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  h->use_fused = enable ? 1 : 0;
   return DGFS_OK;
 }
 

@@ -1,6 +1,6 @@
 // Fourier-neural-operator surrogate of Q(f,f): forward, backward and Adam.
 //
-// Network (width WD = 32, projection width PJ = 128, GELU):
+// Network (width WD = 32, projection width PJ = 128, GELU in the tanh form):
 //   features  x0 = [f/rho, g, g r, g r^2],  g = (f - M)/(rho sigma),
 //             r = |c - u|/sqrt(T), sigma = rms((f - M)/rho) per sample
 //             (M: local Maxwellian; g r^k let the lift form the local loss
@@ -33,34 +33,25 @@ constexpr int WD = 32;   // width
 constexpr int PJ = 128;  // projection width
 constexpr int CIN = 4;   // input features
 
-// erf by Abramowitz & Stegun, Handbook of Mathematical Functions, 7.1.28:
-// erf(x) = 1 - (1 + a1 x + ... + a6 x^6)^-16 for x >= 0, |error| <= 3e-7
-// (about 2e-6 evaluated in FP32), odd extension.  Six FMAs, four squarings
-// and one approximate reciprocal: GELU is the hot scalar of the projection
-// (128 per grid point).
-__device__ __forceinline__ float erf_as(float x) {
-  const float ax = fabsf(x);
-  float p = fmaf(ax, 4.30638e-5f, 2.765672e-4f);
-  p = fmaf(ax, p, 1.520143e-4f);
-  p = fmaf(ax, p, 9.2705272e-3f);
-  p = fmaf(ax, p, 4.22820123e-2f);
-  p = fmaf(ax, p, 7.05230784e-2f);
-  p = fmaf(ax, p, 1.f);
-  p *= p;
-  p *= p;
-  p *= p;
-  p *= p;
+// GELU in the tanh form, GELU(x) = x/2 (1 + tanh(c (x + a x^3))),
+// c = sqrt(2/pi), a = 0.044715 (Hendrycks & Gimpel), with the hardware tanh
+// approximation (tanh.approx.f32, relative error below 2^-10.9): one MUFU and
+// five FP32 operations.  GELU is the hot scalar of the projection (128 per
+// grid point) and of the dense layers' epilogues.
+__device__ __forceinline__ float tanh_fast(float u) {
   float r;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(p));
-  return copysignf(1.f - r, x);
+  asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(u));
+  return r;
 }
 __device__ __forceinline__ float gelu(float x) {
   const float h = 0.5f * x;
-  return fmaf(h, erf_as(x * 0.70710678118654752f), h);
+  return fmaf(h, tanh_fast(x * fmaf(0.0356774081f, x * x, 0.7978845608f)), h);
 }
 __device__ __forceinline__ float gelu_d(float x) {
-  return 0.5f * (1.f + erf_as(x * 0.70710678118654752f)) +
-         x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float x2 = x * x;
+  const float t = tanh_fast(x * fmaf(0.0356774081f, x2, 0.7978845608f));
+  return 0.5f * (1.f + t) +
+         0.5f * x * (1.f - t * t) * fmaf(0.1070322244f, x2, 0.7978845608f);
 }
 __device__ __forceinline__ float bf(const __nv_bfloat16 v) {
   return __bfloat162float(v);
@@ -1018,6 +1009,359 @@ __global__ void __launch_bounds__(128) fno_tc_kernel(TcArgs a) {
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n"
                  ::"r"(tmem), "r"(NC));
+}
+
+// ---------------------------------------------------------------------------
+// Evaluation path with fused spectral passes (inference; training keeps the
+// per-axis passes above, whose intermediates its backward pass reuses).
+// With Y[b][x][ky][kz][c] = the yz spectra of v_l (complex FP32):
+//   fno_xmix_kernel        one CTA per (ky, kz): FFT over x, keep K modes, mix
+//                          with W_l, inverse FFT over x (1/N)
+//                          -> S[b][x][ky][kz][c]
+//   fno_yzinv_dense_kernel one CTA per z-slab of a (b, x) plane: U = Re IDFT_yz(S) (BF16),
+//                          y_l = v_l D_l + d_l + U on tcgen05,
+//                          v_{l+1} = GELU(y_l) (or y_l for the last layer)
+//   fno_yzfwd_kernel       one CTA per plane: Y = DFT_yz(v_{l+1})
+// Every truncated transform is a zero-padded N-point register FFT (modes
+// k = 0..K/2-1 sit in bins 0..K/2-1, k = -K/2..-1 in bins N-K/2..N-1); two
+// real pencils share one complex FFT.  Same values as the per-axis DFT passes
+// up to FP32 rounding; U, y_l and v_{l+1} are rounded to BF16 at the same
+// points.
+// ---------------------------------------------------------------------------
+template <int N, int K>
+__host__ __device__ constexpr int fbin(int kk) {
+  return kk < K / 2 ? kk : N - K + kk;
+}
+
+constexpr int XM_SB = 8;  // samples per chunk in fno_xmix_kernel
+
+// Grid (K*K, ceil(B / XM_SB)): blockIdx.x = ky K + kz, blockIdx.y = chunk of
+// XM_SB samples.  Several CTAs share an SM, so one's loads overlap another's
+// transforms; the W column is loaded after the forward transforms so that the
+// two register sets are not live together.
+template <int N, int K>
+__global__ void __launch_bounds__(K * 32)
+fno_xmix_kernel(const float2* __restrict__ Y, const __nv_bfloat16* __restrict__ W,
+                float2* __restrict__ S, int B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* Vs = reinterpret_cast<float2*>(smem_raw);  // [XM_SB][K][WD]
+  float2* Us = Vs + XM_SB * K * WD;                   // [XM_SB][K][WD]
+  const int kyz = blockIdx.x, ky = kyz / K, kz = kyz % K;
+  const int b0 = blockIdx.y * XM_SB, nb = min(XM_SB, B - b0);
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  const long xs = (long)K * K * WD;  // stride between x planes
+  if (w < nb) {  // forward FFT over x, one warp per sample, lane = channel
+    const float2* src = Y + ((long)(b0 + w) * N * K * K + kyz) * WD + lane;
+    float2 v[N];
+#pragma unroll
+    for (int x = 0; x < N; ++x) v[x] = src[x * xs];
+    fft<float, N, -1>(v);
+#pragma unroll
+    for (int kk = 0; kk < K; ++kk) Vs[(w * K + kk) * WD + lane] = v[fbin<N, K>(kk)];
+  }
+  __syncthreads();
+  {  // mix: thread (kx = w, o = lane) with the column W[m][.][o] in registers,
+     // m = (kx K + ky) K + kz
+    float2 wc[WD];
+    const long m = ((long)w * K + ky) * K + kz;
+    const __nv_bfloat162* wm = reinterpret_cast<const __nv_bfloat162*>(W) + m * WD * WD;
+#pragma unroll
+    for (int i = 0; i < WD; ++i) wc[i] = __bfloat1622float2(wm[i * WD + lane]);
+    for (int s = 0; s < nb; ++s) {
+      const float2* vr = Vs + (s * K + w) * WD;
+      float re = 0.f, im = 0.f;
+#pragma unroll
+      for (int i = 0; i < WD; ++i) {
+        const float2 x = vr[i];
+        re = fmaf(x.x, wc[i].x, re);
+        re = fmaf(-x.y, wc[i].y, re);
+        im = fmaf(x.x, wc[i].y, im);
+        im = fmaf(x.y, wc[i].x, im);
+      }
+      Us[(s * K + w) * WD + lane] = make_float2(re, im);
+    }
+  }
+  __syncthreads();
+  if (w < nb) {  // inverse FFT over x
+    float2 v[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) v[j] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int kk = 0; kk < K; ++kk) v[fbin<N, K>(kk)] = Us[(w * K + kk) * WD + lane];
+    fft<float, N, +1>(v);
+    float2* dst = S + ((long)(b0 + w) * N * K * K + kyz) * WD + lane;
+    constexpr float inv = 1.f / N;
+#pragma unroll
+    for (int x = 0; x < N; ++x) dst[x * xs] = make_float2(v[x].x * inv, v[x].y * inv);
+  }
+}
+
+// yz spectra of one (b, x) plane of a BF16 field [B][N][N][N][WD].
+template <int N, int K>
+__global__ void __launch_bounds__(256)
+fno_yzfwd_kernel(const __nv_bfloat16* __restrict__ v, float2* __restrict__ Y) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* T2 = reinterpret_cast<float2*>(smem_raw);  // [N y][K kz][WD]
+  const int x = blockIdx.x, b = blockIdx.y, t = threadIdx.x;
+  const long plane = (long)b * N + x;
+  const __nv_bfloat16* vp = v + plane * N * N * WD;
+  // z pass: pencil (y, channel pair cp); the two channels are the real and
+  // imaginary parts of one FFT, separated by Hermitian symmetry
+  for (int p = t; p < N * (WD / 2); p += 256) {
+    const int y = p / (WD / 2), cp = p % (WD / 2);
+    float2 c[N];
+#pragma unroll
+    for (int z = 0; z < N; ++z)
+      c[z] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(
+          vp + ((long)y * N + z) * WD + 2 * cp));
+    fft<float, N, -1>(c);
+#pragma unroll
+    for (int kk = 0; kk < K; ++kk) {
+      const int k = fbin<N, K>(kk), nk = (N - k) % N;
+      const float2 C = c[k], Cn = c[nk];
+      // channel 2cp: (C + conj Cn)/2; channel 2cp+1: (C - conj Cn)/(2i)
+      *reinterpret_cast<float4*>(T2 + (y * K + kk) * WD + 2 * cp) =
+          make_float4(0.5f * (C.x + Cn.x), 0.5f * (C.y - Cn.y),
+                      0.5f * (C.y + Cn.y), -0.5f * (C.x - Cn.x));
+    }
+  }
+  __syncthreads();
+  // y pass: pencil (kz, channel)
+  for (int p = t; p < K * WD; p += 256) {
+    const int kk = p / WD, ch = p % WD;
+    float2 c[N];
+#pragma unroll
+    for (int y = 0; y < N; ++y) c[y] = T2[(y * K + kk) * WD + ch];
+    fft<float, N, -1>(c);
+    float2* dst = Y + (plane * K * K + kk) * WD + ch;
+#pragma unroll
+    for (int ky = 0; ky < K; ++ky) dst[(long)ky * K * WD] = c[fbin<N, K>(ky)];
+  }
+}
+
+struct YzInvArgs {
+  const float2* S;           // [B][N][K][K][WD]
+  const __nv_bfloat16* v;    // v_l [B][N^3][WD]
+  const __nv_bfloat16* w16;  // BF16 parameters
+  long offD, offd;           // D_l [WD][WD], d_l [WD]
+  __nv_bfloat16* vout;       // v_{l+1} [B][N^3][WD]
+  int act;                   // GELU (layers 0..2) or identity (last layer)
+  int* err;                  // device error flag
+};
+
+// One CTA of fno_yzinv_dense_kernel takes a z-slab of a (b, x) plane: all y
+// and NZ = N/ZP consecutive z values; its rows (points) are r = y NZ + zl.
+// Two slabs per plane keep the shared memory under half an SM, so two CTAs
+// share an SM and one's loads overlap the other's transforms.
+template <int N, int K>
+struct YzInvGeo {
+  static constexpr int ZP = 2;                    // z-slabs per plane
+  static constexpr int NZ = N / ZP;               // z values per CTA
+  static constexpr int ROWS = N * NZ;             // points per CTA
+  static constexpr int TILES = ROWS / 128;        // 128-row MMA tiles
+  static constexpr int NT = 256;                  // threads
+  static constexpr int NCOL = TILES * WD;         // TMEM columns
+  static constexpr int A_BYTES = ROWS * WD * 2;   // BF16 rows (then U)
+  static constexpr int T_BYTES = K * NZ * WD * 8; // [K][NZ][WD] complex
+  static constexpr int SMEM = A_BYTES + T_BYTES + WD * WD * 2 + WD * 4 + 64;
+  static_assert(ROWS % 128 == 0, "slab must be whole 128-row tiles");
+  static_assert(NCOL >= 32 && (NCOL & (NCOL - 1)) == 0, "TMEM allocation");
+  static_assert(NT % 128 == 0, "epilogue warps cover the four TMEM lane quadrants");
+};
+
+// kz -> z inverse of one (ky, channel) pencil, keeping the slab's z values.
+template <int N, int K, int Z0, int NZ>
+__device__ __forceinline__ void yzinv_zpass(const float2* src, float2* T, int ky,
+                                            int ch) {
+  constexpr float inv = 1.f / N;
+  float2 c[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) c[j] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int kz = 0; kz < K; ++kz) c[fbin<N, K>(kz)] = src[kz * WD];
+  fft<float, N, +1>(c);
+#pragma unroll
+  for (int zl = 0; zl < NZ; ++zl)
+    T[(ky * NZ + zl) * WD + ch] = make_float2(c[Z0 + zl].x * inv, c[Z0 + zl].y * inv);
+}
+
+// Grid (N ZP, B): blockIdx.x = x ZP + slab.  The rows' BF16 activations load
+// asynchronously while the CUDA cores run the kz -> z pass; the dense MMAs
+// are issued next, and U overwrites their A operand only after the MMA
+// completion barrier; the epilogue adds U to the accumulator.
+template <int N, int K>
+__global__ void __launch_bounds__(YzInvGeo<N, K>::NT, 2)
+fno_yzinv_dense_kernel(YzInvArgs a) {
+  using G = YzInvGeo<N, K>;
+  constexpr int NT = G::NT, NZ = G::NZ;
+  // (the no-swizzle operand layout needs 16-byte alignment only)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint8_t* sA = smem_raw;
+  __nv_bfloat16* Us = reinterpret_cast<__nv_bfloat16*>(smem_raw);  // [ROWS][WD]
+  float2* T = reinterpret_cast<float2*>(smem_raw + G::A_BYTES);     // [K][NZ][WD]
+  uint8_t* sB = smem_raw + G::A_BYTES + G::T_BYTES;
+  float* ep = reinterpret_cast<float*>(sB + WD * WD * 2);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(ep + WD);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  int* abort_flag = reinterpret_cast<int*>(tslot + 1);
+  const int x = blockIdx.x / G::ZP, zh = blockIdx.x % G::ZP, z0 = zh * NZ;
+  const int b = blockIdx.y, t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const long plane = (long)b * N + x;
+  // A operand: the slab's rows as 128-row tiles in the canonical no-swizzle
+  // K-major layout (core (row group g, K chunk c) at g*512 + c*128)
+  {
+    const uint32_t a0 = tc_smem_u32(sA);
+    const __nv_bfloat16* vp = a.v + plane * N * N * WD;
+    for (int c = t; c < G::ROWS * 4; c += NT) {
+      const int r = c >> 2, q = c & 3, tile = r >> 7, rr = r & 127;
+      const int y = r / NZ, zl = r % NZ;
+      cp_async16(a0 + (uint32_t)(tile * 8192 + ((rr >> 3) * 4 + q) * 128 + (rr & 7) * 16),
+                 vp + ((long)y * N + z0 + zl) * WD + q * 8);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+  for (int e = t; e < WD * WD; e += NT) {  // D^T [o][i]
+    const int j = e / WD, k = e % WD;
+    *reinterpret_cast<__nv_bfloat16*>(sB + ((j >> 3) * 4 + (k >> 3)) * 128 +
+                                      (j & 7) * 16 + (k & 7) * 2) =
+        a.w16[a.offD + (long)k * WD + j];
+  }
+  if (t < WD) ep[t] = bf(a.w16[a.offd + t]);
+  if (t == 0) {
+    *abort_flag = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(tc_smem_u32(mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 ::"r"(tc_smem_u32(tslot)), "r"(G::NCOL));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  // kz -> z: pencil (ky, channel), while the A operand loads
+  for (int p = t; p < K * WD; p += NT) {
+    const int ky = p / WD, ch = p % WD;
+    const float2* src = a.S + (plane * K + ky) * K * WD + ch;
+    if (zh == 0) yzinv_zpass<N, K, 0, NZ>(src, T, ky, ch);
+    else yzinv_zpass<N, K, NZ, NZ>(src, T, ky, ch);
+  }
+  cp_async_wait_all();
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t mb = tc_smem_u32(mbar);
+  if (t == 0) {
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                           ((uint32_t)(WD >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    const uint32_t aS = tc_smem_u32(sA), bS = tc_smem_u32(sB);
+    for (int tile = 0; tile < G::TILES; ++tile) {
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2) {
+        const uint64_t ad = tc_desc(aS + tile * 8192 + s2 * 256);
+        const uint64_t bd = tc_desc(bS + s2 * 256);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            ::"r"(tmem + (uint32_t)(tile * WD)), "l"(ad), "l"(bd), "r"(idesc), "r"(s2),
+              "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                 ::"r"(mb) : "memory");
+  }
+  // the MMAs have read the A operand before U overwrites it (bounded wait)
+  {
+    uint32_t done = 0;
+    for (int it = 0; it < (1 << 22) && !done; ++it) {
+      asm volatile(
+          "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+          "selp.b32 %0, 1, 0, P1;\n\t}\n"
+          : "=r"(done) : "r"(mb), "r"(0u) : "memory");
+    }
+    if (!done) *abort_flag = 1;
+  }
+  __syncthreads();
+  const bool ok = *abort_flag == 0;
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  // ky -> y, real part: pencil (zl, channel pair); c = sym(a) + i sym(b) with
+  // sym(a)(k) = (a(k) + conj a(-k))/2, so that IFFT(c) = Re IFFT(a) + i Re IFFT(b)
+  if (ok) {
+    constexpr float inv = 1.f / N;
+    for (int p = t; p < NZ * (WD / 2); p += NT) {
+      const int zl = p / (WD / 2), cp = p % (WD / 2);
+      float2 c[N];
+#pragma unroll
+      for (int j = 0; j < N; ++j) c[j] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int ky = 0; ky < K; ++ky) {
+        const float4 ab = *reinterpret_cast<const float4*>(T + (ky * NZ + zl) * WD + 2 * cp);
+        const int k = fbin<N, K>(ky), nk = (N - k) % N;
+        c[k].x += 0.5f * (ab.x - ab.w);
+        c[k].y += 0.5f * (ab.y + ab.z);
+        c[nk].x += 0.5f * (ab.x + ab.w);
+        c[nk].y += 0.5f * (ab.z - ab.y);
+      }
+      fft<float, N, +1>(c);
+#pragma unroll
+      for (int y = 0; y < N; ++y)
+        *reinterpret_cast<__nv_bfloat162*>(Us + (long)(y * NZ + zl) * WD + 2 * cp) =
+            __floats2bfloat162_rn(c[y].x * inv, c[y].y * inv);
+    }
+  }
+  __syncthreads();
+  // epilogue: warp w reads TMEM lane quadrant w % 4 of tiles w/4, w/4 + NT/128, ...
+  if (ok) {
+    const int q = warp & 3;
+    for (int tile = warp >> 2; tile < G::TILES; tile += NT / 128) {
+      const int r = tile * 128 + q * 32 + lane;
+      const long pt = (long)(r / NZ) * N + z0 + r % NZ;
+      uint32_t rg[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, "
+          "%8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, "
+          "%23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+          : "=r"(rg[0]), "=r"(rg[1]), "=r"(rg[2]), "=r"(rg[3]), "=r"(rg[4]), "=r"(rg[5]),
+            "=r"(rg[6]), "=r"(rg[7]), "=r"(rg[8]), "=r"(rg[9]), "=r"(rg[10]), "=r"(rg[11]),
+            "=r"(rg[12]), "=r"(rg[13]), "=r"(rg[14]), "=r"(rg[15]), "=r"(rg[16]),
+            "=r"(rg[17]), "=r"(rg[18]), "=r"(rg[19]), "=r"(rg[20]), "=r"(rg[21]),
+            "=r"(rg[22]), "=r"(rg[23]), "=r"(rg[24]), "=r"(rg[25]), "=r"(rg[26]),
+            "=r"(rg[27]), "=r"(rg[28]), "=r"(rg[29]), "=r"(rg[30]), "=r"(rg[31])
+          : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tile * WD)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      const uint4* Ur = reinterpret_cast<const uint4*>(Us + (long)r * WD);
+      uint4 vo[4];
+#pragma unroll
+      for (int c4 = 0; c4 < 4; ++c4) {
+        const uint4 u = Ur[c4];
+        const __nv_bfloat162* u2 = reinterpret_cast<const __nv_bfloat162*>(&u);
+        __nv_bfloat162* o2 = reinterpret_cast<__nv_bfloat162*>(&vo[c4]);
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const int j = c4 * 8 + 2 * h;
+          const float2 uf = __bfloat1622float2(u2[h]);
+          const __nv_bfloat162 yy = __floats2bfloat162_rn(
+              __uint_as_float(rg[j]) + ep[j] + uf.x,
+              __uint_as_float(rg[j + 1]) + ep[j + 1] + uf.y);
+          if (a.act) {
+            const float2 yf = __bfloat1622float2(yy);
+            o2[h] = __floats2bfloat162_rn(gelu(yf.x), gelu(yf.y));
+          } else {
+            o2[h] = yy;
+          }
+        }
+      }
+      uint4* vd = reinterpret_cast<uint4*>(a.vout + (plane * N * N + pt) * WD);
+#pragma unroll
+      for (int c4 = 0; c4 < 4; ++c4) vd[c4] = vo[c4];
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n"
+                 ::"r"(tmem), "r"(G::NCOL));
+  if (!ok && t == 0) atomicExch(a.err, 1);
 }
 
 // Adam on the FP32 master parameters; refreshes the BF16 copy.

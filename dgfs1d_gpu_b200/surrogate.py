@@ -7,7 +7,8 @@ FP64 conservation projection of the output; backward and Adam for training).
 
 Network: features [f/rho, g, g r, g r^2] (g = (f - M)/(rho sigma),
 sigma = rms((f - M)/rho), r = |c - u|/sqrt(T), M the local Maxwellian) ->
-lift (4 -> 32) -> 4 Fourier layers (width 32, K modes per velocity axis, GELU)
+lift (4 -> 32) -> 4 Fourier layers (width 32, K modes per velocity axis, GELU
+in the tanh form)
 -> 32 -> 128 -> 1, output scaled by rho^2 sigma q_scale (near equilibrium Q is
 nearly linear in f - M, so inputs and target are O(1)), then projected so
 that mass, momentum and energy are conserved exactly.  BF16 weights and activations, FP32
@@ -145,6 +146,11 @@ class FNOSurrogate:
     def set_tensor_cores(self, enable=True):
         """Dense layers on tcgen05 tensor cores (default) or CUDA cores."""
         nat.check(nat.lib().dgfs_fno_set_tensor_cores(self._h, int(bool(enable))))
+
+    def set_fused(self, enable=True):
+        """Evaluation with the fused spectral kernels (default) or with the
+        per-axis DFT passes that training uses."""
+        nat.check(nat.lib().dgfs_fno_set_fused(self._h, int(bool(enable))))
 
     def device_error(self):
         """Error flag of the tensor-core kernels (0 = none); resets it."""

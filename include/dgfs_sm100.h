@@ -318,6 +318,11 @@ int dgfs_fno_last_loss(dgfs_fno_handle h, double* host, int32_t B);
  * the CUDA cores (0; the reference implementation the tensor-core kernels
  * are tested against). */
 int dgfs_fno_set_tensor_cores(dgfs_fno_handle h, int32_t enable);
+/* Evaluation with the fused spectral kernels (default, 1: per layer an x-mix
+ * launch and a yz-inverse + tensor-core dense launch, yz spectra by register
+ * FFTs) or with the per-axis DFT passes that training uses (0).  The fused
+ * path needs the tensor cores; with them disabled eval uses the passes. */
+int dgfs_fno_set_fused(dgfs_fno_handle h, int32_t enable);
 /* Device error flag of the tensor-core kernels (1: an MMA completion wait
  * timed out and the kernel stopped); synchronous, resets the flag. */
 int dgfs_fno_error(dgfs_fno_handle h, int32_t* out);

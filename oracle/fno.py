@@ -60,14 +60,17 @@ def tables(N, K):
     return np.exp(-2j * np.pi * np.outer(modes(K), x) / N)
 
 
+# GELU in the tanh form (Hendrycks & Gimpel): x/2 (1 + tanh(c (x + a x^3)))
+_GC, _GA = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(x):
-    from scipy.special import erf
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    return 0.5 * x * (1.0 + np.tanh(_GC * (x + _GA * x ** 3)))
 
 
 def gelu_d(x):
-    from scipy.special import erf
-    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2 * np.pi)
+    t = np.tanh(_GC * (x + _GA * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * _GC * (1.0 + 3.0 * _GA * x * x)
 
 
 class FNO:

@@ -124,3 +124,31 @@ def test_tensor_core_layers_match_cuda_core_layers(built):
         e = _rel(out[0], out[1])
         print(f'N={n_}: tensor cores vs CUDA cores rel L2 {e:.2e}')
         assert e < 2e-2, e
+
+
+def test_fused_eval_matches_per_axis_passes(built):
+    """The fused evaluation kernels (register-FFT spectral passes, yz inverse
+    fused with the tensor-core dense layer) against the per-axis DFT passes
+    that training uses, on the same network and inputs (N=16 and N=32)."""
+    from dgfs1d_gpu_b200.surrogate import FNOSurrogate, layout
+    for n_, l_ in ((16, 5.0), (32, 6.0)):
+        net = FNOSurrogate(n_, l_, q_scale=SQ, max_batch=4, seed=13)
+        # spectral weights scaled up so that the spectral path dominates the
+        # layers (at initialisation it is a small correction)
+        w = net.params()
+        for l in range(4):
+            o, sz = layout(net.K)[f'W{l}']
+            w[o:o + sz] *= 30.0
+        net.set_params(w)
+        f = torch.tensor(_maxwellians(n_, l_, 3, 43), device='cuda')
+        out = []
+        for fused in (True, False):
+            net.set_fused(fused)
+            Q = torch.zeros_like(f)
+            net.eval(f, Q)
+            torch.cuda.synchronize()
+            out.append(Q.cpu().numpy())
+        assert net.device_error() == 0
+        e = _rel(out[0], out[1])
+        print(f'N={n_}: fused vs per-axis passes rel L2 {e:.2e}')
+        assert e < 1e-2, e
