@@ -1874,7 +1874,7 @@ static int fno_forward_fused(dgfs_fno_s* h, const void* f, int f_double,
   fno_features_kernel<2><<<fg, 256, 0, st>>>(fa);
   DGFS_CUDA(cudaGetLastError());
   const int fsm = N * K * WD * (int)sizeof(float2);
-  const int xsm = 2 * XM_SB * K * WD * (int)sizeof(float2);
+  const int xsm = 2 * K * K * WD * (int)sizeof(float2);
   const int ism = YzInvGeo<N, K>::SMEM;
   DGFS_CUDA(cudaFuncSetAttribute(fno_yzfwd_kernel<N, K>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, fsm));
@@ -1886,7 +1886,7 @@ static int fno_forward_fused(dgfs_fno_s* h, const void* f, int f_double,
   fno_yzfwd_kernel<N, K><<<pg, 256, fsm, st>>>(h->v[0], h->Yp);
   DGFS_CUDA(cudaGetLastError());
   for (int l = 0; l < 4; ++l) {
-    fno_xmix_kernel<N, K><<<dim3(K * K, (B + XM_SB - 1) / XM_SB), K * 32, xsm, st>>>(
+    fno_xmix_kernel<N, K><<<dim3(K * K, (B + K - 1) / K), K * 32, xsm, st>>>(
         h->Yp, h->p16 + h->L.W[l], h->Sp, B);
     YzInvArgs ya{};
     ya.S = h->Sp; ya.v = h->v[l]; ya.w16 = h->p16; ya.offD = h->L.D[l];

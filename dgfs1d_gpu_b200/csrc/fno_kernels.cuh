@@ -1033,21 +1033,21 @@ __host__ __device__ constexpr int fbin(int kk) {
   return kk < K / 2 ? kk : N - K + kk;
 }
 
-constexpr int XM_SB = 8;  // samples per chunk in fno_xmix_kernel
 
-// Grid (K*K, ceil(B / XM_SB)): blockIdx.x = ky K + kz, blockIdx.y = chunk of
-// XM_SB samples.  Several CTAs share an SM, so one's loads overlap another's
-// transforms; the W column is loaded after the forward transforms so that the
-// two register sets are not live together.
+// Grid (K*K, ceil(B / K)): blockIdx.x = ky K + kz, blockIdx.y = chunk of K
+// samples (one per warp in the transforms; thread (kx, o) in the mix).  Two
+// CTAs share an SM, so one's loads overlap the other's transforms; the W
+// column is loaded after the forward transforms so that the two register sets
+// are not live together.
 template <int N, int K>
 __global__ void __launch_bounds__(K * 32)
 fno_xmix_kernel(const float2* __restrict__ Y, const __nv_bfloat16* __restrict__ W,
                 float2* __restrict__ S, int B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* Vs = reinterpret_cast<float2*>(smem_raw);  // [XM_SB][K][WD]
-  float2* Us = Vs + XM_SB * K * WD;                   // [XM_SB][K][WD]
+  float2* Vs = reinterpret_cast<float2*>(smem_raw);  // [K samples][K][WD]
+  float2* Us = Vs + K * K * WD;                       // [K samples][K][WD]
   const int kyz = blockIdx.x, ky = kyz / K, kz = kyz % K;
-  const int b0 = blockIdx.y * XM_SB, nb = min(XM_SB, B - b0);
+  const int b0 = blockIdx.y * K, nb = min(K, B - b0);
   const int t = threadIdx.x, w = t >> 5, lane = t & 31;
   const long xs = (long)K * K * WD;  // stride between x planes
   if (w < nb) {  // forward FFT over x, one warp per sample, lane = channel
@@ -1067,18 +1067,27 @@ fno_xmix_kernel(const float2* __restrict__ Y, const __nv_bfloat16* __restrict__ 
     const __nv_bfloat162* wm = reinterpret_cast<const __nv_bfloat162*>(W) + m * WD * WD;
 #pragma unroll
     for (int i = 0; i < WD; ++i) wc[i] = __bfloat1622float2(wm[i * WD + lane]);
-    for (int s = 0; s < nb; ++s) {
-      const float2* vr = Vs + (s * K + w) * WD;
-      float re = 0.f, im = 0.f;
+    // two samples per pass, two input channels per 16-byte load (the second
+    // sample's row stays inside Vs when nb is odd: s + 1 < K)
+    for (int s = 0; s < nb; s += 2) {
+      const float4* v0 = reinterpret_cast<const float4*>(Vs + (s * K + w) * WD);
+      const float4* v1 = reinterpret_cast<const float4*>(Vs + ((s + 1) * K + w) * WD);
+      float r0 = 0.f, i0 = 0.f, r1 = 0.f, i1 = 0.f;
 #pragma unroll
-      for (int i = 0; i < WD; ++i) {
-        const float2 x = vr[i];
-        re = fmaf(x.x, wc[i].x, re);
-        re = fmaf(-x.y, wc[i].y, re);
-        im = fmaf(x.x, wc[i].y, im);
-        im = fmaf(x.y, wc[i].x, im);
+      for (int q = 0; q < WD / 2; ++q) {
+        const float4 a = v0[q], c = v1[q];
+        const float2 wa = wc[2 * q], wb = wc[2 * q + 1];
+        r0 = fmaf(a.x, wa.x, r0); r0 = fmaf(-a.y, wa.y, r0);
+        i0 = fmaf(a.x, wa.y, i0); i0 = fmaf(a.y, wa.x, i0);
+        r0 = fmaf(a.z, wb.x, r0); r0 = fmaf(-a.w, wb.y, r0);
+        i0 = fmaf(a.z, wb.y, i0); i0 = fmaf(a.w, wb.x, i0);
+        r1 = fmaf(c.x, wa.x, r1); r1 = fmaf(-c.y, wa.y, r1);
+        i1 = fmaf(c.x, wa.y, i1); i1 = fmaf(c.y, wa.x, i1);
+        r1 = fmaf(c.z, wb.x, r1); r1 = fmaf(-c.w, wb.y, r1);
+        i1 = fmaf(c.z, wb.y, i1); i1 = fmaf(c.w, wb.x, i1);
       }
-      Us[(s * K + w) * WD + lane] = make_float2(re, im);
+      Us[(s * K + w) * WD + lane] = make_float2(r0, i0);
+      if (s + 1 < nb) Us[((s + 1) * K + w) * WD + lane] = make_float2(r1, i1);
     }
   }
   __syncthreads();

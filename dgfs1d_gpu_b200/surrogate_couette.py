@@ -14,11 +14,12 @@ bulk moments per step.
    harvested along a plain run, each with Q from the plain operator.
 3. The FNO surrogate is trained on the GPU with the library's kernels (half
    of every batch drawn from the harvested states).
-4. The surrogate-assisted solver (plain operator every k = 10 calls, fallback
-   above a 1e-3 residual) runs to steady state, in two modes: the surrogate
-   alone between checks, and the surrogate plus the defect measured at the
-   last check.
-5. For context, the solver with the fused FP32 operator (no surrogate).
+4. The solver with the fused FP32 operator (no surrogate).
+5. The surrogate-assisted solver (plain operator every k = 10 calls, fallback
+   above a 1e-3 residual) runs to steady state, in three modes: the surrogate
+   alone between checks, the surrogate plus the defect measured at the last
+   check, and the latter with the fused FP32 operator as the plain operator
+   (checks and fallback).
 
 ``python -m dgfs1d_gpu_b200.surrogate_couette [--quick]`` prints one JSON
 report (``--quick``: N = 16 and short budgets, for tests).
@@ -98,20 +99,8 @@ def experiment(N=32, Nrho=16, M=12, dev=6.0, dt=1e-3, sphere='full',
         np.median(st.residuals(net, op, fm_test)))
     out['residual_steady_couette_median'] = float(
         np.median(st.residuals(net, op, plain.u.reshape(-1, plain.u.shape[-1]))))
-    for mode, correct in (('surrogate', False), ('surrogate+defect', True)):
-        sol = make_solver(N, Nrho, M, dev, dt=dt, sphere=sphere)
-        hook = st.SurrogateBoltzmann(sol, net, k=k, tol=tol, correct=correct)
-        sol.boltzmann = hook
-        rs = st.run_to_steady(sol, steady_tol, max_steps, check_every)
-        pxy, qx = _profiles(rs['moments'])
-        out[mode] = dict(steps=rs['steps'], wall_s=rs['wall_s'],
-                         residual=rs['residual'],
-                         speedup_vs_plain=rp['wall_s'] / rs['wall_s'],
-                         shear_stress_rel_diff=_rel_profile_diff(pxy, pxy_p),
-                         heat_flux_rel_diff=_rel_profile_diff(qx, qx_p),
-                         **hook.stats())
-    # context: the same solver with the fused FP32 operator in place of the
-    # FP64 one (no surrogate)
+    # the solver with the fused FP32 operator in place of the FP64 one (no
+    # surrogate)
     f32 = make_solver(N, Nrho, M, dev, dt=dt, sphere=sphere, precision_mode='fp32')
     rf = st.run_to_steady(f32, steady_tol, max_steps, check_every)
     pxy, qx = _profiles(rf['moments'])
@@ -120,6 +109,25 @@ def experiment(N=32, Nrho=16, M=12, dev=6.0, dt=1e-3, sphere='full',
         speedup_vs_plain=rp['wall_s'] / rf['wall_s'],
         shear_stress_rel_diff=_rel_profile_diff(pxy, pxy_p),
         heat_flux_rel_diff=_rel_profile_diff(qx, qx_p))
+    del f32
+    # surrogate-assisted runs: the plain operator (FP64, or the fused FP32
+    # operator) checks every k-th call and serves as the fallback
+    for mode, correct, prec in (('surrogate', False, None),
+                                ('surrogate+defect', True, None),
+                                ('surrogate+defect, fp32 checks', True, 'fp32')):
+        sol = make_solver(N, Nrho, M, dev, dt=dt, sphere=sphere, precision_mode=prec)
+        hook = st.SurrogateBoltzmann(sol, net, k=k, tol=tol, correct=correct)
+        sol.boltzmann = hook
+        rs = st.run_to_steady(sol, steady_tol, max_steps, check_every)
+        pxy, qx = _profiles(rs['moments'])
+        out[mode] = dict(steps=rs['steps'], wall_s=rs['wall_s'],
+                         residual=rs['residual'],
+                         speedup_vs_plain=rp['wall_s'] / rs['wall_s'],
+                         speedup_vs_fp32_plain=rf['wall_s'] / rs['wall_s'],
+                         shear_stress_rel_diff=_rel_profile_diff(pxy, pxy_p),
+                         heat_flux_rel_diff=_rel_profile_diff(qx, qx_p),
+                         **hook.stats())
+        del sol, hook
     return out
 
 
