@@ -179,15 +179,14 @@ static int c32_of(int N) {
 }
 template <int N> struct VhsClusters;
 // c64: FP64 terms kernel; c32: FP32 terms kernel (default); cpro / cepi:
-// prologue / epilogue (FP64, two slabs).  At N=32 a 16-CTA epilogue cluster
-// needs 68 KB per CTA, so three CTAs share an SM and a 24-point batch runs in
-// one wave; the prologue's moment/Maxwellian set-up is faster at 8 CTAs.
+// prologue / epilogue (FP64, one slab per CTA).  At N=32 an 8-CTA prologue
+// cluster needs 75 KB per CTA and a 16-CTA epilogue cluster 34 KB, so two
+// (four) CTAs share an SM and a 24-point batch runs in one wave of each.
 template <> struct VhsClusters<8> { static constexpr int c64 = 1, c32 = 1, cpro = 1, cepi = 1; };
 template <> struct VhsClusters<16> { static constexpr int c64 = 2, c32 = 1, cpro = 2, cepi = 2; };
 template <> struct VhsClusters<24> { static constexpr int c64 = 4, c32 = 3, cpro = 4, cepi = 4; };
 template <> struct VhsClusters<32> { static constexpr int c64 = 8, c32 = 4, cpro = 8, cepi = 16; };
-// N=48 (FP32 mode only): 16-CTA clusters of 3 planes; the two FP64 slabs of
-// the prologue take 226 KB of the 227 KB a CTA may use
+// N=48 (FP32 mode only): 16-CTA clusters of 3 planes
 template <> struct VhsClusters<48> { static constexpr int c64 = 0, c32 = 16, cpro = 16, cepi = 16; };
 
 static size_t slab_bytes(int N, int C, size_t elem) {
@@ -488,8 +487,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     a.c0 = h->c0; a.b2 = h->b2; a.cw = h->cw; a.split = fp32 ? 1 : 0;
     a.Fg = h->Fg; a.ReLf = h->ReLf; a.mhat = h->mhat; a.moments = h->moments;
     a.Fny = h->Fny;
-    const size_t smem = 2 * slab_bytes(N, CPRO, sizeof(double2)) +
-                        3 * N * sizeof(double2) + 8 * sizeof(double);
+    const size_t smem = prologue_smem<N, CPRO>();
     if ((rc = launch_cluster(vhs_prologue_kernel<N, CPRO>, dim3(CPRO, nevals),
                              dim3(GPRO::NT), CPRO, smem, st, a)))
       return rc;
@@ -571,7 +569,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     a.Nrho = fp32 ? (h->Nrho + 1) / 2 : h->Nrho;  // FP32: packed radial pairs
     a.project = h->project; a.c0 = h->c0; a.cw = h->cw;
     for (int i = 0; i < 25; ++i) a.Ginv[i] = h->Ginv[i];
-    const size_t smem = 2 * slab_bytes(N, CEPI, sizeof(double2));
+    const size_t smem = slab_bytes(N, CEPI, sizeof(double2));
     if ((rc = launch_cluster(vhs_epilogue_kernel<N, CEPI>, dim3(CEPI, nevals),
                              dim3(GEPI::NT), CEPI, smem, st, a)))
       return rc;
@@ -1332,8 +1330,7 @@ static int vss_run(dgfs_vss_s* h, int p, int q, const void* fp, const void* fq,
       a.c0 = h->c0; a.b2 = h->b2dummy; a.b2c = P.c; a.cw = h->cw; a.split = 1;
       a.Fg = h->Fg[s2]; a.ReLf = h->ReLf; a.mhat = h->mhat[s2]; a.moments = h->mom[s2];
       a.Fny = nullptr;
-      const size_t smem = 2 * slab_bytes(N, CPRO, sizeof(double2)) +
-                          3 * N * sizeof(double2) + 8 * sizeof(double);
+      const size_t smem = prologue_smem<N, CPRO>();
       if ((rc = launch_cluster(vhs_prologue_kernel<N, CPRO>, dim3(CPRO, nevals),
                                dim3(GPRO::NT), CPRO, smem, st, a)))
         return rc;
@@ -1361,7 +1358,7 @@ static int vss_run(dgfs_vss_s* h, int p, int q, const void* fp, const void* fq,
     ea.f_double = f_double; ea.src_slots = ss; ea.src_base = sb; ea.Q = Q;
     ea.q_double = q_double; ea.dst_slots = ds; ea.dst_base = db;
     ea.prefac = P.prefac; ea.Nrho = h->Nrho; ea.project = 0; ea.c0 = h->c0; ea.cw = h->cw;
-    const size_t smemE = 2 * slab_bytes(N, CEPI, sizeof(double2));
+    const size_t smemE = slab_bytes(N, CEPI, sizeof(double2));
     return launch_cluster(vhs_epilogue_kernel<N, CEPI>, dim3(CEPI, nevals),
                           dim3(GEPI::NT), CEPI, smemE, st, ea);
   }

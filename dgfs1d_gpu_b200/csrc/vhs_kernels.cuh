@@ -126,21 +126,30 @@ __device__ __forceinline__ double load_real(const void* p, int is_double,
 }
 
 // ---------------------------------------------------------------------------
-// Prologue: one cluster (C CTAs, FP64) per eval.
+// Prologue: one cluster (C CTAs, FP64) per eval.  One slab per CTA serves
+// both transforms (the exchange of the inverse transform waits for every CTA
+// to have read its slab), which keeps a 24-point batch in one wave at N=32.
 // ---------------------------------------------------------------------------
+// Shared memory: the slab, the moment partials [5][NT] + [5] and the 1-D
+// Maxwellian factors [3N] (doubles), the Maxwellian spectra [3][N] (complex)
+// and the moments [8].
 template <int N, int C>
-__global__ void __launch_bounds__(Geo<N, C>::NT, 1)
+constexpr size_t prologue_smem() {
+  return (size_t)Geo<N, C>::SLAB * sizeof(double2) +
+         (size_t)(6 * Geo<N, C>::NT + 8 + 3 * N) * sizeof(double) +
+         (size_t)3 * N * sizeof(double2) + 8 * sizeof(double);
+}
+
+template <int N, int C>
+__global__ void __launch_bounds__(Geo<N, C>::NT)
 vhs_prologue_kernel(VhsPrologueArgs a) {
   using G = Geo<N, C>;
   using T = double2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* A = reinterpret_cast<T*>(smem_raw);
-  T* Rb = A + G::SLAB;
-  T* mh = Rb + G::SLAB;                                    // [3][N]
-  double* mom = reinterpret_cast<double*>(mh + 3 * N);     // [8]
-  // moment partials [5][NT] + [5] borrow the receive slab, unused until the
-  // loss transform (peers write it only two cluster barriers later)
-  double* red = reinterpret_cast<double*>(Rb);
+  double* red = reinterpret_cast<double*>(A + G::SLAB);     // [6 NT + 8 + 3N]
+  T* mh = reinterpret_cast<T*>(red + 6 * G::NT + 8 + 3 * N); // [3][N]
+  double* mom = reinterpret_cast<double*>(mh + 3 * N);      // [8]
 
   const int t = threadIdx.x;
   const unsigned rank = cluster_rank();
@@ -199,9 +208,9 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
         for (int k = 0; k < 5; ++k) a.moments[(size_t)e * 5 + k] = mom[k];
     }
     __syncthreads();
-    // 1-D Maxwellian factors (3N values, each computed once; staged in the
-    // receive slab past the moment partials, which peers read only below
-    // offset 5 NT + 5) and their spectra (direct DFT, table twiddles)
+    // 1-D Maxwellian factors (3N values, each computed once; past the moment
+    // partials, which peers read only below offset 5 NT + 5) and their
+    // spectra (direct DFT, table twiddles)
     double* mv = red + 6 * G::NT + 8;
     for (int i = t; i < 3 * N; i += G::NT) {
       const int ax = i / N, j = i % N;
@@ -279,16 +288,18 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
   if (a.split && rank == 0)
     for (int i = t; i < 3 * N; i += G::NT) a.mhat[(size_t)e * 3 * N + i] = mh[i];
   __syncthreads();
-  // loss: Re IFFT(b2 F)
+  // loss: Re IFFT(b2 F); the Y-slab exchange reuses the slab once every CTA
+  // of the cluster has read its own
   slab_row_pass<double, N, C, +1>(A, t);
   __syncthreads();
   {
     T w[N];
     slab_col_load_fft<double, N, C, +1>(A, t, w);
-    push_cols_to_yslab<double, N, C>(Rb, t, rank, w);
+    cluster_sync_all();
+    push_cols_to_yslab<double, N, C>(A, t, rank, w);
   }
   cluster_sync_all();
-  yslab_load_pencil<double, N, C>(Rb, t, v);
+  yslab_load_pencil<double, N, C>(A, t, v);
   fft<double, N, +1>(v);
 #pragma unroll
   for (int x = 0; x < N; ++x)
@@ -1295,7 +1306,6 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   using T = double2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* A = reinterpret_cast<T*>(smem_raw);
-  T* Rb = A + G::SLAB;
   const int t = threadIdx.x;
   const unsigned rank = cluster_rank();
   const int e = blockIdx.y;
@@ -1361,11 +1371,12 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   {
     T w[N];
     slab_col_load_fft<double, N, C, +1>(A, t, w);
-    push_cols_to_yslab<double, N, C>(Rb, t, rank, w);
+    cluster_sync_all();  // every CTA has read its slab: exchange into it
+    push_cols_to_yslab<double, N, C>(A, t, rank, w);
   }
   cluster_sync_all();
   T v[N];
-  yslab_load_pencil<double, N, C>(Rb, t, v);
+  yslab_load_pencil<double, N, C>(A, t, v);
   fft<double, N, +1>(v);
   const int yl = t / N, z = t % N, y = rank * G::P + yl;
   const size_t fb = (size_t)slot_of(a.src_slots, a.src_base, e) * G::n;
