@@ -179,7 +179,7 @@ static int c32_of(int N) {
 }
 template <int N> struct VhsClusters;
 // c64: FP64 terms kernel; c32: FP32 terms kernel (default); cpro / cepi:
-// prologue / epilogue (FP64, one slab per CTA).  At N=32 an 8-CTA prologue
+// prologue / epilogue (FP64, one slab per CTA up to N=32).  At N=32 an 8-CTA prologue
 // cluster needs 75 KB per CTA and a 16-CTA epilogue cluster 34 KB, so two
 // (four) CTAs share an SM and a 24-point batch runs in one wave of each.
 template <> struct VhsClusters<8> { static constexpr int c64 = 1, c32 = 1, cpro = 1, cepi = 1; };
@@ -569,7 +569,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     a.Nrho = fp32 ? (h->Nrho + 1) / 2 : h->Nrho;  // FP32: packed radial pairs
     a.project = h->project; a.c0 = h->c0; a.cw = h->cw;
     for (int i = 0; i < 25; ++i) a.Ginv[i] = h->Ginv[i];
-    const size_t smem = slab_bytes(N, CEPI, sizeof(double2));
+    const size_t smem = epilogue_smem<N, CEPI>();
     if ((rc = launch_cluster(vhs_epilogue_kernel<N, CEPI>, dim3(CEPI, nevals),
                              dim3(GEPI::NT), CEPI, smem, st, a)))
       return rc;
@@ -1358,7 +1358,7 @@ static int vss_run(dgfs_vss_s* h, int p, int q, const void* fp, const void* fq,
     ea.f_double = f_double; ea.src_slots = ss; ea.src_base = sb; ea.Q = Q;
     ea.q_double = q_double; ea.dst_slots = ds; ea.dst_base = db;
     ea.prefac = P.prefac; ea.Nrho = h->Nrho; ea.project = 0; ea.c0 = h->c0; ea.cw = h->cw;
-    const size_t smemE = slab_bytes(N, CEPI, sizeof(double2));
+    const size_t smemE = epilogue_smem<N, CEPI>();
     return launch_cluster(vhs_epilogue_kernel<N, CEPI>, dim3(CEPI, nevals),
                           dim3(GEPI::NT), CEPI, smemE, st, ea);
   }

@@ -126,18 +126,32 @@ __device__ __forceinline__ double load_real(const void* p, int is_double,
 }
 
 // ---------------------------------------------------------------------------
-// Prologue: one cluster (C CTAs, FP64) per eval.  One slab per CTA serves
-// both transforms (the exchange of the inverse transform waits for every CTA
-// to have read its slab), which keeps a 24-point batch in one wave at N=32.
+// Prologue: one cluster (C CTAs, FP64) per eval.  Up to N=32 one slab per CTA
+// serves both transforms (the exchange of the inverse transform waits for
+// every CTA to have read its slab), which keeps a 24-point batch in one wave.
 // ---------------------------------------------------------------------------
-// Shared memory: the slab, the moment partials [5][NT] + [5] and the 1-D
-// Maxwellian factors [3N] (doubles), the Maxwellian spectra [3][N] (complex)
-// and the moments [8].
+// Whether the prologue and epilogue keep one slab per CTA (exchange after a
+// cluster barrier) or a separate receive slab.  One slab pays off where it
+// lets more CTAs share an SM (N <= 32); at N=48 registers allow one CTA per
+// SM either way and the second slab saves the barrier.
+template <int N> struct OneSlab { static constexpr bool value = N <= 32; };
+
+// Shared memory: the slab(s), the moment partials [5][NT] + [5] and the 1-D
+// Maxwellian factors [3N] (doubles; with two slabs they borrow the receive
+// slab, which peers write only two cluster barriers later), the Maxwellian
+// spectra [3][N] (complex) and the moments [8].
 template <int N, int C>
 constexpr size_t prologue_smem() {
-  return (size_t)Geo<N, C>::SLAB * sizeof(double2) +
-         (size_t)(6 * Geo<N, C>::NT + 8 + 3 * N) * sizeof(double) +
-         (size_t)3 * N * sizeof(double2) + 8 * sizeof(double);
+  return OneSlab<N>::value
+             ? (size_t)Geo<N, C>::SLAB * sizeof(double2) +
+                   (size_t)(6 * Geo<N, C>::NT + 8 + 3 * N) * sizeof(double) +
+                   (size_t)3 * N * sizeof(double2) + 8 * sizeof(double)
+             : (size_t)2 * Geo<N, C>::SLAB * sizeof(double2) +
+                   (size_t)3 * N * sizeof(double2) + 8 * sizeof(double);
+}
+template <int N, int C>
+constexpr size_t epilogue_smem() {
+  return (size_t)(OneSlab<N>::value ? 1 : 2) * Geo<N, C>::SLAB * sizeof(double2);
 }
 
 template <int N, int C>
@@ -146,9 +160,13 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
   using G = Geo<N, C>;
   using T = double2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr bool OS = OneSlab<N>::value;
   T* A = reinterpret_cast<T*>(smem_raw);
-  double* red = reinterpret_cast<double*>(A + G::SLAB);     // [6 NT + 8 + 3N]
-  T* mh = reinterpret_cast<T*>(red + 6 * G::NT + 8 + 3 * N); // [3][N]
+  T* Rb = OS ? A : A + G::SLAB;                             // Y-slab receive
+  double* red = OS ? reinterpret_cast<double*>(A + G::SLAB)  // [6 NT + 8 + 3N]
+                   : reinterpret_cast<double*>(Rb);
+  T* mh = OS ? reinterpret_cast<T*>(red + 6 * G::NT + 8 + 3 * N)
+             : A + 2 * G::SLAB;                              // [3][N]
   double* mom = reinterpret_cast<double*>(mh + 3 * N);      // [8]
 
   const int t = threadIdx.x;
@@ -295,11 +313,11 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
   {
     T w[N];
     slab_col_load_fft<double, N, C, +1>(A, t, w);
-    cluster_sync_all();
-    push_cols_to_yslab<double, N, C>(A, t, rank, w);
+    if (OS) cluster_sync_all();
+    push_cols_to_yslab<double, N, C>(Rb, t, rank, w);
   }
   cluster_sync_all();
-  yslab_load_pencil<double, N, C>(A, t, v);
+  yslab_load_pencil<double, N, C>(Rb, t, v);
   fft<double, N, +1>(v);
 #pragma unroll
   for (int x = 0; x < N; ++x)
@@ -1305,7 +1323,9 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   using G = Geo<N, C>;
   using T = double2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr bool OS = OneSlab<N>::value;
   T* A = reinterpret_cast<T*>(smem_raw);
+  T* Rb = OS ? A : A + G::SLAB;  // Y-slab receive
   const int t = threadIdx.x;
   const unsigned rank = cluster_rank();
   const int e = blockIdx.y;
@@ -1371,12 +1391,12 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   {
     T w[N];
     slab_col_load_fft<double, N, C, +1>(A, t, w);
-    cluster_sync_all();  // every CTA has read its slab: exchange into it
-    push_cols_to_yslab<double, N, C>(A, t, rank, w);
+    if (OS) cluster_sync_all();  // every CTA has read its slab: exchange into it
+    push_cols_to_yslab<double, N, C>(Rb, t, rank, w);
   }
   cluster_sync_all();
   T v[N];
-  yslab_load_pencil<double, N, C>(A, t, v);
+  yslab_load_pencil<double, N, C>(Rb, t, v);
   fft<double, N, +1>(v);
   const int yl = t / N, z = t % N, y = rank * G::P + yl;
   const size_t fb = (size_t)slot_of(a.src_slots, a.src_base, e) * G::n;
