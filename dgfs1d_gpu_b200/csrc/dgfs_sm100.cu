@@ -526,7 +526,10 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     if ((rc = launch_terms32<N>(c, a, nevals, h->Nrho, h->hi))) return rc;
     if (h->profile) cudaEventRecord(h->ev[evi++], h->hi);
     DGFS_CUDA(cudaEventRecord(h->join_hi, h->hi));
-    // aux (after the tables): Maxwellian gain, behind the terms kernel
+    // aux (after the tables, and not before the terms kernel is launched, so
+    // that it does not take SMs from the Nyquist-plane kernel): Maxwellian
+    // gain, behind the terms kernel on the SMs its clusters leave free
+    DGFS_CUDA(cudaStreamWaitEvent(h->aux, h->fork1, 0));
     VhsGainArgs g{};
     g.hh = h->hh; g.mult = h->mult; g.b1w = h->b1w64; g.GM = h->GM;
     g.Mu = h->Mu; g.Nrho = h->Nrho;

@@ -414,10 +414,20 @@ vhs_maxwell_gain_kernel(VhsGainArgs a) {
   for (int pc = 0; pc < a.Nrho; pc += a.pch) {
     const int np = min(a.pch, a.Nrho - pc);
     __syncthreads();
-    for (int i = t; i < np * Mu * 2 * N; i += GG::NT) {
-      const int pq = i / (2 * N), r = i % (2 * N);
-      const int pp = pc + pq / Mu, q = pq % Mu;
-      hyz[i] = a.hh[(((size_t)e * a.Nrho + pp) * Mu + q) * 3 * N + N + r];
+    // the y and z tables of the chunk: asynchronous 16-byte copies, all in
+    // flight at once (a load-store loop would expose one L2 round trip per
+    // element per thread)
+    {
+      const uint32_t h0 = (uint32_t)__cvta_generic_to_shared(hyz);
+      for (int i = t; i < np * Mu * 2 * N; i += GG::NT) {
+        const int pq = i / (2 * N), r = i % (2 * N);
+        const int pp = pc + pq / Mu, q = pq % Mu;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n"
+                     :: "r"(h0 + 16u * (uint32_t)i),
+                        "l"(a.hh + (((size_t)e * a.Nrho + pp) * Mu + q) * 3 * N + N + r)
+                     : "memory");
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
     for (int i = t; i < np * Mu; i += GG::NT) {
       const int pp = pc + i / Mu, q = i % Mu;
@@ -425,6 +435,7 @@ vhs_maxwell_gain_kernel(VhsGainArgs a) {
       const double m = (double)a.mult[q];
       hxs[i] = make_double2(m * h.x, m * h.y);
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     for (int j = 0; j < np; ++j) {
       const int p = pc + j;
