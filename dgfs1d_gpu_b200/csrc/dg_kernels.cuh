@@ -29,7 +29,7 @@ struct DgAdvectArgs {
   const double* c0;         // [N] velocity grid; c_x of v = c0[v / (N*N)]
   const double* invjac;     // [Ne]
   const double* f0[2];      // [Nv] boundary Maxwellians (left, right)
-  const double* nden;       // [2] wall densities (from dg_wall_density_kernel)
+  const double* nden;       // [2] wall densities (from dg_wall_final_kernel)
   int bc[2];                // boundary kinds (left, right)
   double bc_ux[2];          // wall x-velocities
   double nl[2];             // outward normals (-1, +1)
@@ -50,19 +50,24 @@ __device__ __forceinline__ void st(void* p, int dbl, size_t i, double v) {
 
 // Wall densities n_w = -sum_{out} (c-u_w).n f cw / sum_{in} (c-u_w).n f0 cw
 // (updateBC of dgfs-wall-diffuse.mako with the two gpuarray.sum of
-// std/bc.py:63-76).  One block per boundary; deterministic order.
-__global__ void __launch_bounds__(1024) dg_wall_density_kernel(DgAdvectArgs a,
-                                                               double cw,
-                                                               double* nden) {
-  const int side = blockIdx.x;
-  __shared__ double rn[1024], rd[1024];
-  const int t = threadIdx.x;
+// std/bc.py:63-76), in a deterministic order.
+// Grid (kWallCh chunks of the velocity grid, 2 sides): partial sums
+// [2][kWallCh][2]; then one thread per side adds them in a fixed order (one
+// CTA per side would leave the reduction latency-bound on two SMs).
+constexpr int kWallCh = 32;
+__global__ void __launch_bounds__(256) dg_wall_partial_kernel(DgAdvectArgs a,
+                                                              double cw,
+                                                              double* part) {
+  const int ch = blockIdx.x, side = blockIdx.y, t = threadIdx.x;
+  __shared__ double rn[256], rd[256];
   double sn = 0, sd = 0;
   if (a.bc[side] == kBcWall) {
     const int e = side == 0 ? 0 : a.Ne - 1;
     const double* tw = side == 0 ? a.trL : a.trR;
     const double nl = a.nl[side], ux = a.bc_ux[side];
-    for (int v = t; v < a.Nv; v += blockDim.x) {
+    const int len = (a.Nv + kWallCh - 1) / kWallCh;
+    const int v1 = min(a.Nv, (ch + 1) * len);
+    for (int v = ch * len + t; v < v1; v += 256) {
       double ul = 0;
       for (int k = 0; k < a.K; ++k)
         ul += tw[k] * ld(a.u, a.f_double, ((size_t)k * a.Ne + e) * a.Nv + v);
@@ -74,11 +79,26 @@ __global__ void __launch_bounds__(1024) dg_wall_density_kernel(DgAdvectArgs a,
   rn[t] = sn;
   rd[t] = sd;
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (t < s) { rn[t] += rn[t + s]; rd[t] += rd[t + s]; }
+  for (int s2 = 128; s2 > 0; s2 >>= 1) {
+    if (t < s2) { rn[t] += rn[t + s2]; rd[t] += rd[t + s2]; }
     __syncthreads();
   }
-  if (t == 0) nden[side] = (a.bc[side] == kBcWall) ? -(rn[0] / rd[0]) : 0.0;
+  if (t == 0) {
+    part[(side * kWallCh + ch) * 2] = rn[0];
+    part[(side * kWallCh + ch) * 2 + 1] = rd[0];
+  }
+}
+
+__global__ void dg_wall_final_kernel(DgAdvectArgs a, const double* part,
+                                     double* nden) {
+  const int side = threadIdx.x;
+  if (side >= 2) return;
+  double rn = 0, rd = 0;
+  for (int c = 0; c < kWallCh; ++c) {
+    rn += part[(side * kWallCh + c) * 2];
+    rd += part[(side * kWallCh + c) * 2 + 1];
+  }
+  nden[side] = (a.bc[side] == kBcWall) ? -(rn / rd) : 0.0;
 }
 
 __device__ __forceinline__ double dg_ghost(const DgAdvectArgs& a, int side,
@@ -339,6 +359,45 @@ __global__ void __launch_bounds__(256) penalty_moments_kernel(PenaltyMomentArgs 
   if (t < 5) a.U[(size_t)p * 5 + t] = red[t][0];
 }
 
+// The same moments over many CTAs: grid (kPmCh chunks, npts), partial sums
+// [npts][kPmCh][5], then a fixed-order sum per (point, moment).
+constexpr int kPmCh = 16;
+__global__ void __launch_bounds__(256)
+penalty_moments_part_kernel(PenaltyMomentArgs a, double* part) {
+  const int ch = blockIdx.x, p = blockIdx.y, t = threadIdx.x;
+  __shared__ double red[5][256];
+  const int NN = a.N * a.N;
+  const int len = (a.Nv + kPmCh - 1) / kPmCh, v1 = min(a.Nv, (ch + 1) * len);
+  double s[5] = {0, 0, 0, 0, 0};
+  for (int v = ch * len + t; v < v1; v += 256) {
+    const double fv = ld(a.f, a.f_double, (size_t)p * a.Nv + v) * a.cw;
+    const double cx = a.c0[v / NN], cy = a.c0[(v / a.N) % a.N], cz = a.c0[v % a.N];
+    s[0] += fv;
+    s[1] += fv * cx;
+    s[2] += fv * cy;
+    s[3] += fv * cz;
+    s[4] += fv * (cx * cx + cy * cy + cz * cz);
+  }
+  for (int k = 0; k < 5; ++k) red[k][t] = s[k];
+  __syncthreads();
+  for (int st2 = 128; st2 > 0; st2 >>= 1) {
+    if (t < st2)
+      for (int k = 0; k < 5; ++k) red[k][t] += red[k][t + st2];
+    __syncthreads();
+  }
+  if (t < 5) part[((size_t)p * kPmCh + ch) * 5 + t] = red[t][0];
+}
+
+__global__ void penalty_moments_final_kernel(const double* part, double* U,
+                                             int npts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts * 5) return;
+  const int p = i / 5, k = i % 5;
+  double s = 0;
+  for (int c = 0; c < kPmCh; ++c) s += part[((size_t)p * kPmCh + c) * 5 + k];
+  U[i] = s;
+}
+
 struct PenaltyImplicitArgs {
   const double* U;        // [npts][5] moments at the new level
   const void* rhs;        // [npts][Nv] explicit combination
@@ -354,45 +413,73 @@ struct PenaltyImplicitArgs {
   size_t total;           // npts * Nv
 };
 
+// Per-point state of the penalty model: rho, u, T, the Maxwellian's
+// amplitude rho/(pi T)^1.5 and nu = prefac rho T^(1-omega) (the powers once
+// per point, not per velocity).
+struct PenaltyPoint { double ux, uy, uz, T, amp, nu; };
+__device__ __forceinline__ PenaltyPoint penalty_point(const double* U,
+                                                      double prefac,
+                                                      double omega) {
+  PenaltyPoint s;
+  const double T = (U[4] - (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]) /
+                   (1.5 * U[0]);
+  s.ux = U[1] / U[0]; s.uy = U[2] / U[0]; s.uz = U[3] / U[0];
+  s.T = T;
+  s.amp = U[0] / pow(M_PI * T, 1.5);
+  s.nu = prefac * U[0] * pow(T, 1. - omega);
+  return s;
+}
+
+// Grid (chunks of the velocity grid, npts): the point's state is formed once
+// per CTA in shared memory.
+constexpr int kPenaltyEpt = 8;  // velocities per thread
+__device__ __forceinline__ double penalty_maxwellian(const PenaltyPoint& s,
+                                                     const double* c0, int N,
+                                                     int v) {
+  const int NN = N * N;
+  const double dx = c0[v / NN] - s.ux;
+  const double dy = c0[(v / N) % N] - s.uy;
+  const double dz = c0[v % N] - s.uz;
+  return s.amp * exp(-(dx * dx + dy * dy + dz * dz) / s.T);
+}
+
 // f = (rhs + cdt nu M) / (adiv + cdt nu), optionally P = nu (M - f).
-__global__ void penalty_implicit_kernel(PenaltyImplicitArgs a) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.total;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const size_t p = i / a.Nv;
-    const int v = (int)(i % a.Nv);
-    const double* U = a.U + p * 5;
-    const double T = (U[4] - (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]) /
-                     (1.5 * U[0]);
-    const int NN = a.N * a.N;
-    const double dx = a.c0[v / NN] - U[1] / U[0];
-    const double dy = a.c0[(v / a.N) % a.N] - U[2] / U[0];
-    const double dz = a.c0[v % a.N] - U[3] / U[0];
-    const double M = U[0] / pow(M_PI * T, 1.5) * exp(-(dx * dx + dy * dy + dz * dz) / T);
-    const double nu = a.prefac * U[0] * pow(T, 1. - a.omega);
-    const double r = ld(a.rhs, a.f_double, i);
-    const double fn = (r + a.cdt * nu * M) / (a.adiv + a.cdt * nu);
+__global__ void __launch_bounds__(256) penalty_implicit_kernel(PenaltyImplicitArgs a) {
+  __shared__ PenaltyPoint sp;
+  const size_t p = blockIdx.y;
+  if (threadIdx.x == 0) sp = penalty_point(a.U + p * 5, a.prefac, a.omega);
+  __syncthreads();
+  const PenaltyPoint s = sp;
+  const int v0 = blockIdx.x * 256 * kPenaltyEpt + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < kPenaltyEpt; ++r) {
+    const int v = v0 + r * 256;
+    if (v >= a.Nv) break;
+    const size_t i = p * a.Nv + v;
+    const double M = penalty_maxwellian(s, a.c0, a.N, v);
+    const double rr = ld(a.rhs, a.f_double, i);
+    const double fn = (rr + a.cdt * s.nu * M) / (a.adiv + a.cdt * s.nu);
     st(a.f, a.f_double, i, fn);
-    if (a.P) st(a.P, a.f_double, i, nu * (M - fn));
+    if (a.P) st(a.P, a.f_double, i, s.nu * (M - fn));
     if (a.Mout) st(a.Mout, a.f_double, i, M);
   }
 }
 
 // P = nu (M(U) - f) for the current f and its moments U (collide).
-__global__ void penalty_collide_kernel(PenaltyImplicitArgs a) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.total;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const size_t p = i / a.Nv;
-    const int v = (int)(i % a.Nv);
-    const double* U = a.U + p * 5;
-    const double T = (U[4] - (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]) /
-                     (1.5 * U[0]);
-    const int NN = a.N * a.N;
-    const double dx = a.c0[v / NN] - U[1] / U[0];
-    const double dy = a.c0[(v / a.N) % a.N] - U[2] / U[0];
-    const double dz = a.c0[v % a.N] - U[3] / U[0];
-    const double M = U[0] / pow(M_PI * T, 1.5) * exp(-(dx * dx + dy * dy + dz * dz) / T);
-    const double nu = a.prefac * U[0] * pow(T, 1. - a.omega);
-    st(a.P, a.f_double, i, nu * (M - ld(a.f, a.f_double, i)));
+__global__ void __launch_bounds__(256) penalty_collide_kernel(PenaltyImplicitArgs a) {
+  __shared__ PenaltyPoint sp;
+  const size_t p = blockIdx.y;
+  if (threadIdx.x == 0) sp = penalty_point(a.U + p * 5, a.prefac, a.omega);
+  __syncthreads();
+  const PenaltyPoint s = sp;
+  const int v0 = blockIdx.x * 256 * kPenaltyEpt + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < kPenaltyEpt; ++r) {
+    const int v = v0 + r * 256;
+    if (v >= a.Nv) break;
+    const size_t i = p * a.Nv + v;
+    const double M = penalty_maxwellian(s, a.c0, a.N, v);
+    st(a.P, a.f_double, i, s.nu * (M - ld(a.f, a.f_double, i)));
     if (a.Mout) st(a.Mout, a.f_double, i, M);
   }
 }

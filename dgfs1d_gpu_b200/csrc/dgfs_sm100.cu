@@ -938,10 +938,14 @@ struct dgfs_dg_s {
   double* im = nullptr;
   double* part = nullptr;  // residual partials
   double* part_h = nullptr;
+  double* wpart = nullptr;  // wall-density partials [2][kWallCh][2]
+  double* mpart = nullptr;  // penalty-moment partials [mpts][kPmCh][5]
+  int mpts = 0;
 };
 
 static void free_dg(dgfs_dg_s* h) {
-  void* ptrs[] = {h->c0, h->invjac, h->f0[0], h->f0[1], h->nden, h->im, h->part};
+  void* ptrs[] = {h->c0, h->invjac, h->f0[0], h->f0[1], h->nden, h->im, h->part,
+                  h->wpart, h->mpart};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->part_h) cudaFreeHost(h->part_h);
@@ -994,6 +998,10 @@ extern "C" int dgfs_dg_create(const dgfs_dg_desc* d, dgfs_dg_handle* out) {
   cudaError_t e1 = cudaMalloc(&h->nden, 2 * sizeof(double));
   if (e1 == cudaSuccess) e1 = cudaMalloc(&h->part, 2 * 1024 * sizeof(double));
   if (e1 == cudaSuccess) e1 = cudaMallocHost(&h->part_h, 2 * 1024 * sizeof(double));
+  if (e1 == cudaSuccess) e1 = cudaMalloc(&h->wpart, 2 * kWallCh * 2 * sizeof(double));
+  h->mpts = std::max(K, d->Nqr) * Ne;
+  if (e1 == cudaSuccess)
+    e1 = cudaMalloc(&h->mpart, (size_t)h->mpts * kPmCh * 5 * sizeof(double));
   if (e1 != cudaSuccess) {
     free_dg(h);
     return fail(DGFS_ERR_CUDA, std::string("allocation: ") + cudaGetErrorString(e1));
@@ -1019,7 +1027,8 @@ extern "C" int dgfs_dg_advect(dgfs_dg_handle h, const void* u, void* ux,
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   DgAdvectArgs a = h->base;
   a.u = u; a.ux = ux; a.f_double = dtype == DGFS_F64;
-  dg_wall_density_kernel<<<2, 1024, 0, st>>>(a, h->cw, h->nden);
+  dg_wall_partial_kernel<<<dim3(kWallCh, 2), 256, 0, st>>>(a, h->cw, h->wpart);
+  dg_wall_final_kernel<<<1, 32, 0, st>>>(a, h->wpart, h->nden);
   DGFS_CUDA(cudaGetLastError());
   const dim3 grid((a.Nv + 255) / 256), block(256);
   switch (a.K) {
@@ -1462,13 +1471,6 @@ extern "C" int dgfs_vhs_set_projection(dgfs_vhs_handle h, int32_t enable) {
 // ---------------------------------------------------------------------------
 // Penalty model (IMEX) entry points
 // ---------------------------------------------------------------------------
-static unsigned grid_for_total(size_t total) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (unsigned)std::min<size_t>((total + 255) / 256, (size_t)sms * 16);
-}
-
 extern "C" int dgfs_penalty_moments(dgfs_dg_handle h, const void* f,
                                     int32_t dtype, int32_t npts, double* U,
                                     void* stream) {
@@ -1477,7 +1479,14 @@ extern "C" int dgfs_penalty_moments(dgfs_dg_handle h, const void* f,
   PenaltyMomentArgs a{};
   a.f = f; a.f_double = dtype == DGFS_F64; a.Nv = h->base.Nv; a.N = h->base.N;
   a.c0 = h->c0; a.cw = h->cw; a.U = U;
-  penalty_moments_kernel<<<npts, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (npts <= h->mpts) {
+    penalty_moments_part_kernel<<<dim3(kPmCh, npts), 256, 0, st>>>(a, h->mpart);
+    penalty_moments_final_kernel<<<(npts * 5 + 127) / 128, 128, 0, st>>>(
+        h->mpart, U, npts);
+  } else {
+    penalty_moments_kernel<<<npts, 256, 0, st>>>(a);
+  }
   DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
 }
@@ -1494,8 +1503,8 @@ extern "C" int dgfs_penalty_implicit(dgfs_dg_handle h, const double* U,
   a.c0 = h->c0; a.adiv = adiv; a.cdt = cdt; a.prefac = prefac; a.omega = omega;
   a.total = (size_t)npts * h->base.Nv;
   if (a.total == 0) return DGFS_OK;
-  penalty_implicit_kernel<<<grid_for_total(a.total), 256, 0,
-                            static_cast<cudaStream_t>(stream)>>>(a);
+  const dim3 pgrid((h->base.Nv + 256 * kPenaltyEpt - 1) / (256 * kPenaltyEpt), npts);
+  penalty_implicit_kernel<<<pgrid, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
   DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
 }
@@ -1511,8 +1520,8 @@ extern "C" int dgfs_penalty_collide(dgfs_dg_handle h, const double* U,
   a.c0 = h->c0; a.prefac = prefac; a.omega = omega;
   a.total = (size_t)npts * h->base.Nv;
   if (a.total == 0) return DGFS_OK;
-  penalty_collide_kernel<<<grid_for_total(a.total), 256, 0,
-                           static_cast<cudaStream_t>(stream)>>>(a);
+  const dim3 pgrid((h->base.Nv + 256 * kPenaltyEpt - 1) / (256 * kPenaltyEpt), npts);
+  penalty_collide_kernel<<<pgrid, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
   DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
 }
