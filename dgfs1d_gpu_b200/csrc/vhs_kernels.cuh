@@ -381,7 +381,7 @@ __global__ void vhs_tables_kernel(VhsTablesArgs a) {
 // grid (N [lx], nevals), block N*NYB threads: thread (ly0 = t/N, lz = t%N)
 // owns the points (lx, ly0 + NYB*k, lz), k < KY.  The 1-D factors of a chunk
 // of a.pch radial points are staged in shared memory at once (m_q folded into
-// hx), hx*hz is formed once per (p, q) and reused for the KY points, and the
+// hx), hx*hy is formed once per (p, q, ly) in place of the y table, and the
 // b1 weights of the next p are loaded while the current one is summed.
 // ---------------------------------------------------------------------------
 template <int N>
@@ -437,6 +437,13 @@ vhs_maxwell_gain_kernel(VhsGainArgs a) {
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
+    // fold hx (with m_q) into the y table once per (p, q, ly): hxy = hx hy
+    for (int i = t; i < np * Mu * N; i += GG::NT) {
+      const int pq = i / N, ly = i % N;
+      double2* y = hyz + (size_t)pq * 2 * N + ly;
+      *y = cmul(hxs[pq], *y);
+    }
+    __syncthreads();
     for (int j = 0; j < np; ++j) {
       const int p = pc + j;
       double wn[GG::KY];
@@ -451,13 +458,13 @@ vhs_maxwell_gain_kernel(VhsGainArgs a) {
       for (int k = 0; k < GG::KY; ++k) acc[k] = make_double2(0, 0);
       const double2* hj = hyz + (size_t)j * Mu * 2 * N;
       for (int q = 0; q < Mu; ++q) {
-        const double2 hxz = cmul(hxs[j * Mu + q], hj[q * 2 * N + N + lz]);
+        const double2 hz = hj[q * 2 * N + N + lz];
 #pragma unroll
         for (int k = 0; k < GG::KY; ++k) {
           const int ly = min(ly0 + GG::NYB * k, N - 1);
-          const double2 hy = hj[q * 2 * N + ly];
-          acc[k].x += hxz.x * hy.x - hxz.y * hy.y;
-          acc[k].y += hxz.x * hy.y + hxz.y * hy.x;
+          const double2 hxy = hj[q * 2 * N + ly];
+          acc[k].x += hxy.x * hz.x - hxy.y * hz.y;
+          acc[k].y += hxy.x * hz.y + hxy.y * hz.x;
         }
       }
 #pragma unroll
