@@ -152,6 +152,22 @@ _SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
       ctypes.c_double, ctypes.c_void_p]),
+    ('dgfs_penalty_moments_n', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
+    ('dgfs_penalty_model_relax', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+      ctypes.c_double, ctypes.c_void_p]),
+    ('dgfs_penalty_model_implicit', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+      ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+    ('dgfs_penalty_model_collide', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
     ('dgfs_axnpby', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_double,
       ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),

@@ -1,8 +1,11 @@
 """Penalised IMEX time integrators (``[time-integrator] scheme``).
 
 Keys and coefficients of dgfs1D/astd/integrator.py: ``bdf-111`` / ``bdf-222``
-(BGK penalty, explicit DG advection; :281-400) and ``imex-lm-bdf1`` /
-``imex-lm-bdf2`` (explicit L + Q - P, implicit P(f^{n+1}); :623-792).
+(penalty model only, explicit DG advection; :281-400) and ``imex-lm-bdf1`` /
+``imex-lm-bdf2`` (explicit L + Q - P, implicit P(f^{n+1}); :623-792).  The
+moment update is the linear combination of the scheme followed by the
+penalty model's implicit relaxation of its non-conserved moments (the
+updateMoment{BDF,LM} kernels of the model).
 Differences from the reference, all in start-up or dead code: start-up
 states come from first-order substeps of the same family (the reference
 uses ARS-222/443 substeps); the explicit part of a new IMEX-LM level uses
@@ -45,7 +48,7 @@ class DGFSIntegratorAstd:
         return torch.zeros(self.shape, dtype=self.dtype, device=self.device)
 
     def _zm(self):
-        return torch.zeros((self.npts, 5), dtype=torch.float64,
+        return torch.zeros((self.npts, self._sm.nalph), dtype=torch.float64,
                            device=self.device)
 
     def _mom(self, x):
@@ -64,6 +67,7 @@ class Bdf111IntegratorAstd(DGFSIntegratorAstd):
         LU0 = self._mom(L0)
         U = self._zm()
         _lin(U, [(1.0, U0), (dt, LU0)])
+        self._sm.relax(U, 1.0, dt)
         rhs = self._z()
         _lin(rhs, [(1.0, f), (dt, L0)])
         self._sm.implicit(U, rhs, f, 1.0, dt)
@@ -95,6 +99,7 @@ class Bdf222IntegratorAstd(DGFSIntegratorAstd):
         U = self._zm()
         _lin(U, [(-a1 / a3, h0['U']), (g1 * dt / a3, h0['LU']),
                  (-a2 / a3, h1['U']), (g2 * dt / a3, h1['LU'])])
+        self._sm.relax(U, a3, self.B * dt)
         rhs = self._z()
         _lin(rhs, [(-a1, h0['F']), (g1 * dt, h0['L']), (-a2, h1['F']),
                    (g2 * dt, h1['L'])])
@@ -152,6 +157,7 @@ class IMEXLMIntegratorAstd(DGFSIntegratorAstd):
         _lin(rhs, [p for i in range(s) for p in (
             (-A[s - i - 1], hs[i]['F']), (dt * B[s - i - 1], hs[i]['L']),
             (dt * C[s - i], hs[i]['P']))])
+        self._sm.relax(U, 1.0, C[0] * dt)
         P = self._z()
         self._sm.implicit(U, rhs, f, 1.0, C[0] * dt, P=P)
         E = self._z()

@@ -335,71 +335,70 @@ struct PenaltyMomentArgs {
   double* U;              // [npts][5]
 };
 
-__global__ void __launch_bounds__(256) penalty_moments_kernel(PenaltyMomentArgs a) {
-  const int p = blockIdx.x, t = threadIdx.x;
-  __shared__ double red[5][256];
-  const int NN = a.N * a.N;
-  double s[5] = {0, 0, 0, 0, 0};
-  for (int v = t; v < a.Nv; v += blockDim.x) {
-    const double fv = ld(a.f, a.f_double, (size_t)p * a.Nv + v) * a.cw;
-    const double cx = a.c0[v / NN], cy = a.c0[(v / a.N) % a.N], cz = a.c0[v % a.N];
-    s[0] += fv;
-    s[1] += fv * cx;
-    s[2] += fv * cy;
-    s[3] += fv * cz;
-    s[4] += fv * (cx * cx + cy * cy + cz * cz);
-  }
-  for (int k = 0; k < 5; ++k) red[k][t] = s[k];
-  __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if (t < st)
-      for (int k = 0; k < 5; ++k) red[k][t] += red[k][t + st];
-    __syncthreads();
-  }
-  if (t < 5) a.U[(size_t)p * 5 + t] = red[t][0];
-}
 
 // The same moments over many CTAs: grid (kPmCh chunks, npts), partial sums
-// [npts][kPmCh][5], then a fixed-order sum per (point, moment).
+// [npts][kPmCh][NA], then a fixed-order sum per (point, moment).  NA = 5
+// (BGK), 11 (ES-BGK: + c_x^2, c_y^2, c_z^2, c_x c_y, c_y c_z, c_z c_x) or
+// 14 (Shakov: + |c|^2 c), the rows of astd/scattering.py:155-162, 306-316,
+// 375-388.
 constexpr int kPmCh = 16;
+constexpr int kPmMaxNa = 14;
+template <int NA>
 __global__ void __launch_bounds__(256)
 penalty_moments_part_kernel(PenaltyMomentArgs a, double* part) {
   const int ch = blockIdx.x, p = blockIdx.y, t = threadIdx.x;
-  __shared__ double red[5][256];
+  __shared__ double red[NA][256];
   const int NN = a.N * a.N;
   const int len = (a.Nv + kPmCh - 1) / kPmCh, v1 = min(a.Nv, (ch + 1) * len);
-  double s[5] = {0, 0, 0, 0, 0};
+  double s[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) s[k] = 0;
   for (int v = ch * len + t; v < v1; v += 256) {
     const double fv = ld(a.f, a.f_double, (size_t)p * a.Nv + v) * a.cw;
     const double cx = a.c0[v / NN], cy = a.c0[(v / a.N) % a.N], cz = a.c0[v % a.N];
+    const double c2 = cx * cx + cy * cy + cz * cz;
     s[0] += fv;
     s[1] += fv * cx;
     s[2] += fv * cy;
     s[3] += fv * cz;
-    s[4] += fv * (cx * cx + cy * cy + cz * cz);
+    s[4] += fv * c2;
+    if (NA > 5) {
+      s[5] += fv * cx * cx;
+      s[6] += fv * cy * cy;
+      s[7] += fv * cz * cz;
+      s[8] += fv * cx * cy;
+      s[9] += fv * cy * cz;
+      s[10] += fv * cz * cx;
+    }
+    if (NA > 11) {
+      s[11] += fv * c2 * cx;
+      s[12] += fv * c2 * cy;
+      s[13] += fv * c2 * cz;
+    }
   }
-  for (int k = 0; k < 5; ++k) red[k][t] = s[k];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) red[k][t] = s[k];
   __syncthreads();
   for (int st2 = 128; st2 > 0; st2 >>= 1) {
     if (t < st2)
-      for (int k = 0; k < 5; ++k) red[k][t] += red[k][t + st2];
+      for (int k = 0; k < NA; ++k) red[k][t] += red[k][t + st2];
     __syncthreads();
   }
-  if (t < 5) part[((size_t)p * kPmCh + ch) * 5 + t] = red[t][0];
+  if (t < NA) part[((size_t)p * kPmCh + ch) * NA + t] = red[t][0];
 }
 
 __global__ void penalty_moments_final_kernel(const double* part, double* U,
-                                             int npts) {
+                                             int npts, int na) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= npts * 5) return;
-  const int p = i / 5, k = i % 5;
+  if (i >= npts * na) return;
+  const int p = i / na, k = i % na;
   double s = 0;
-  for (int c = 0; c < kPmCh; ++c) s += part[((size_t)p * kPmCh + c) * 5 + k];
+  for (int c = 0; c < kPmCh; ++c) s += part[((size_t)p * kPmCh + c) * na + k];
   U[i] = s;
 }
 
 struct PenaltyImplicitArgs {
-  const double* U;        // [npts][5] moments at the new level
+  const double* U;        // [npts][NA] moments at the new level
   const void* rhs;        // [npts][Nv] explicit combination
   void* f;                // out [npts][Nv] new distribution
   void* P;                // out (or null) nu (M - f)
@@ -410,44 +409,102 @@ struct PenaltyImplicitArgs {
   double adiv;            // denominator constant (a_q for BDF, 1 for LM)
   double cdt;             // implicit weight times dt (b dt, c0 dt)
   double prefac, omega;
+  double Pr;              // Prandtl number (ES-BGK, Shakov)
   size_t total;           // npts * Nv
 };
 
-// Per-point state of the penalty model: rho, u, T, the Maxwellian's
-// amplitude rho/(pi T)^1.5 and nu = prefac rho T^(1-omega) (the powers once
-// per point, not per velocity).
-struct PenaltyPoint { double ux, uy, uz, T, amp, nu; };
+// Penalty models: 0 BGK (Maxwellian), 1 ES-BGK (anisotropic Gaussian),
+// 2 Shakov (Maxwellian times the heat-flux polynomial).  U holds each point's
+// NA = 5 / 11 / 14 raw moments (see penalty_moments_part_kernel).
+constexpr int kPenBGK = 0, kPenESBGK = 1, kPenShakov = 2;
+template <int KIND> struct PenaltyNa;
+template <> struct PenaltyNa<kPenBGK> { static constexpr int value = 5; };
+template <> struct PenaltyNa<kPenESBGK> { static constexpr int value = 11; };
+template <> struct PenaltyNa<kPenShakov> { static constexpr int value = 14; };
+
+// Per-point state, formed once per CTA: u, T, nu = prefac rho T^(1-omega)
+// (the powers once per point, not per velocity) and the Gaussian's
+// parameters: amp and, for ES-BGK, the inverse of the temperature tensor
+// T_ij = T/Pr delta_ij + 2 (1 - 1/Pr)(P_ij/rho - u_i u_j)
+// (esbgk-direct-gll.mako:157-254); for Shakov, the peculiar heat flux
+// scaled by 2 (1 - Pr)/(5 rho T^2) (shakov-direct-gll.mako:193-278).
+struct PenaltyPoint {
+  double ux, uy, uz, T, amp, nu;
+  double Ai[6];  // ES-BGK: inverse tensor xx, yy, zz, xy, yz, zx
+  double qc[3];  // Shakov: scaled heat flux
+};
+template <int KIND>
 __device__ __forceinline__ PenaltyPoint penalty_point(const double* U,
                                                       double prefac,
-                                                      double omega) {
+                                                      double omega, double Pr) {
   PenaltyPoint s;
-  const double T = (U[4] - (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]) /
-                   (1.5 * U[0]);
-  s.ux = U[1] / U[0]; s.uy = U[2] / U[0]; s.uz = U[3] / U[0];
+  const double rho = U[0];
+  const double T = (U[4] - (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / rho) /
+                   (1.5 * rho);
+  s.ux = U[1] / rho; s.uy = U[2] / rho; s.uz = U[3] / rho;
   s.T = T;
-  s.amp = U[0] / pow(M_PI * T, 1.5);
-  s.nu = prefac * U[0] * pow(T, 1. - omega);
+  s.nu = prefac * rho * pow(T, 1. - omega);
+  s.amp = rho / pow(M_PI * T, 1.5);
+  if (KIND == kPenESBGK) {
+    const double lam = 1. / Pr, mu = 2. * (1. - 1. / Pr);
+    const double a = lam * T + mu * (U[5] / rho - s.ux * s.ux);
+    const double b = lam * T + mu * (U[6] / rho - s.uy * s.uy);
+    const double c = lam * T + mu * (U[7] / rho - s.uz * s.uz);
+    const double d = mu * (U[8] / rho - s.ux * s.uy);
+    const double e = mu * (U[9] / rho - s.uy * s.uz);
+    const double f = mu * (U[10] / rho - s.uz * s.ux);
+    const double det = -c * d * d + 2 * d * e * f - a * e * e - b * f * f + a * b * c;
+    s.Ai[0] = (b * c - e * e) / det;
+    s.Ai[1] = (a * c - f * f) / det;
+    s.Ai[2] = (a * b - d * d) / det;
+    s.Ai[3] = (e * f - c * d) / det;
+    s.Ai[4] = (d * f - a * e) / det;
+    s.Ai[5] = (d * e - f * b) / det;
+    s.amp = rho / (pow(M_PI, 1.5) * sqrt(det));
+  } else if (KIND == kPenShakov) {
+    const double u2 = s.ux * s.ux + s.uy * s.uy + s.uz * s.uz;
+    const double u[3] = {s.ux, s.uy, s.uz};
+    const int row[3][3] = {{5, 8, 10}, {8, 6, 9}, {10, 9, 7}};
+    const double sc = 2. * (1. - Pr) / 5. / (rho * T * T);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      s.qc[i] = sc * (U[11 + i] - 2. * (U[row[i][0]] * s.ux + U[row[i][1]] * s.uy +
+                                       U[row[i][2]] * s.uz) +
+                      rho * u[i] * u2 - 1.5 * u[i] * rho * T);
+  }
   return s;
 }
 
-// Grid (chunks of the velocity grid, npts): the point's state is formed once
-// per CTA in shared memory.
 constexpr int kPenaltyEpt = 8;  // velocities per thread
-__device__ __forceinline__ double penalty_maxwellian(const PenaltyPoint& s,
-                                                     const double* c0, int N,
-                                                     int v) {
+template <int KIND>
+__device__ __forceinline__ double penalty_gaussian(const PenaltyPoint& s,
+                                                   const double* c0, int N,
+                                                   int v) {
   const int NN = N * N;
   const double dx = c0[v / NN] - s.ux;
   const double dy = c0[(v / N) % N] - s.uy;
   const double dz = c0[v % N] - s.uz;
-  return s.amp * exp(-(dx * dx + dy * dy + dz * dz) / s.T);
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  if (KIND == kPenESBGK) {
+    const double q = s.Ai[0] * dx * dx + s.Ai[1] * dy * dy + s.Ai[2] * dz * dz +
+                     2. * (s.Ai[3] * dx * dy + s.Ai[4] * dy * dz + s.Ai[5] * dz * dx);
+    return s.amp * exp(-q);
+  }
+  const double M = s.amp * exp(-d2 / s.T);
+  if (KIND == kPenShakov)
+    return M * (1. + (s.qc[0] * dx + s.qc[1] * dy + s.qc[2] * dz) *
+                         (2. * d2 / s.T - 5.));
+  return M;
 }
 
-// f = (rhs + cdt nu M) / (adiv + cdt nu), optionally P = nu (M - f).
+// f = (rhs + cdt nu G) / (adiv + cdt nu), optionally P = nu (G - f) and G;
+// grid (chunks of the velocity grid, npts).
+template <int KIND>
 __global__ void __launch_bounds__(256) penalty_implicit_kernel(PenaltyImplicitArgs a) {
   __shared__ PenaltyPoint sp;
+  constexpr int NA = PenaltyNa<KIND>::value;
   const size_t p = blockIdx.y;
-  if (threadIdx.x == 0) sp = penalty_point(a.U + p * 5, a.prefac, a.omega);
+  if (threadIdx.x == 0) sp = penalty_point<KIND>(a.U + p * NA, a.prefac, a.omega, a.Pr);
   __syncthreads();
   const PenaltyPoint s = sp;
   const int v0 = blockIdx.x * 256 * kPenaltyEpt + threadIdx.x;
@@ -456,7 +513,7 @@ __global__ void __launch_bounds__(256) penalty_implicit_kernel(PenaltyImplicitAr
     const int v = v0 + r * 256;
     if (v >= a.Nv) break;
     const size_t i = p * a.Nv + v;
-    const double M = penalty_maxwellian(s, a.c0, a.N, v);
+    const double M = penalty_gaussian<KIND>(s, a.c0, a.N, v);
     const double rr = ld(a.rhs, a.f_double, i);
     const double fn = (rr + a.cdt * s.nu * M) / (a.adiv + a.cdt * s.nu);
     st(a.f, a.f_double, i, fn);
@@ -465,11 +522,13 @@ __global__ void __launch_bounds__(256) penalty_implicit_kernel(PenaltyImplicitAr
   }
 }
 
-// P = nu (M(U) - f) for the current f and its moments U (collide).
+// P = nu (G(U) - f) for the current f and its moments U (collide).
+template <int KIND>
 __global__ void __launch_bounds__(256) penalty_collide_kernel(PenaltyImplicitArgs a) {
   __shared__ PenaltyPoint sp;
+  constexpr int NA = PenaltyNa<KIND>::value;
   const size_t p = blockIdx.y;
-  if (threadIdx.x == 0) sp = penalty_point(a.U + p * 5, a.prefac, a.omega);
+  if (threadIdx.x == 0) sp = penalty_point<KIND>(a.U + p * NA, a.prefac, a.omega, a.Pr);
   __syncthreads();
   const PenaltyPoint s = sp;
   const int v0 = blockIdx.x * 256 * kPenaltyEpt + threadIdx.x;
@@ -478,9 +537,58 @@ __global__ void __launch_bounds__(256) penalty_collide_kernel(PenaltyImplicitArg
     const int v = v0 + r * 256;
     if (v >= a.Nv) break;
     const size_t i = p * a.Nv + v;
-    const double M = penalty_maxwellian(s, a.c0, a.N, v);
+    const double M = penalty_gaussian<KIND>(s, a.c0, a.N, v);
     st(a.P, a.f_double, i, s.nu * (M - ld(a.f, a.f_double, i)));
     if (a.Mout) st(a.Mout, a.f_double, i, M);
+  }
+}
+
+// Implicit relaxation of the non-conserved moments after the linear
+// combination of a BDF / IMEX-LM moment update (updateMom{q}_BDF and _LM of
+// esbgk-direct-gll.mako :16-81, :480-540 and shakov-direct-gll.mako :18-120,
+// :549-645, with adiv = a_q, cdt = b dt for BDF and adiv = 1, cdt = c_0 dt
+// for LM): with nu = prefac rho T^(1-omega) from the updated conserved
+// moments, the stresses relax as (adiv U + k tau)/(adiv + k), tau_ii =
+// rho T/2 + (rho u_i)^2/rho, tau_ij = (rho u_i)(rho u_j)/rho, k = cdt nu/Pr
+// (ES-BGK) or cdt nu (Shakov); the Shakov heat flux as (adiv U + cdt nu
+// tau_q)/(adiv + Pr cdt nu) with the relaxed stresses.  One thread per point.
+template <int KIND>
+__global__ void penalty_relax_kernel(double* Uall, int npts, double adiv,
+                                     double cdt, double prefac, double omega,
+                                     double Pr) {
+  constexpr int NA = PenaltyNa<KIND>::value;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  double* U = Uall + (size_t)p * NA;
+  const double rho = U[0];
+  const double T = (U[4] - (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / rho) /
+                   (1.5 * rho);
+  const double nu = prefac * rho * pow(T, 1. - omega);
+  const double k = KIND == kPenESBGK ? cdt / Pr * nu : cdt * nu;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const double tau = 0.5 * rho * T + U[1 + i] * U[1 + i] / rho;
+    U[5 + i] = (adiv * U[5 + i] + k * tau) / (adiv + k);
+  }
+  const int oi[3] = {1, 2, 3}, oj[3] = {2, 3, 1};
+#pragma unroll
+  for (int n = 0; n < 3; ++n) {
+    const double tau = U[oi[n]] * U[oj[n]] / rho;
+    U[8 + n] = (adiv * U[8 + n] + k * tau) / (adiv + k);
+  }
+  if (KIND == kPenShakov) {
+    const int row[3][3] = {{5, 8, 10}, {8, 6, 9}, {10, 9, 7}};
+    const double m2 = (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / (rho * rho);
+    const double kq = cdt * nu;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double ru = U[1 + i];
+      const double tq = (1. - Pr) * (-2. * (U[row[i][0]] * U[1] + U[row[i][1]] * U[2] +
+                                            U[row[i][2]] * U[3]) / rho +
+                                     ru * m2 - 1.5 * ru * T) +
+                        (ru * m2 + 2.5 * ru * T);
+      U[11 + i] = (adiv * U[11 + i] + kq * tq) / (adiv + Pr * kq);
+    }
   }
 }
 

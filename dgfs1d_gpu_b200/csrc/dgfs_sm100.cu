@@ -939,7 +939,7 @@ struct dgfs_dg_s {
   double* part = nullptr;  // residual partials
   double* part_h = nullptr;
   double* wpart = nullptr;  // wall-density partials [2][kWallCh][2]
-  double* mpart = nullptr;  // penalty-moment partials [mpts][kPmCh][5]
+  double* mpart = nullptr;  // penalty-moment partials [mpts][kPmCh][<= 14]
   int mpts = 0;
 };
 
@@ -1001,7 +1001,7 @@ extern "C" int dgfs_dg_create(const dgfs_dg_desc* d, dgfs_dg_handle* out) {
   if (e1 == cudaSuccess) e1 = cudaMalloc(&h->wpart, 2 * kWallCh * 2 * sizeof(double));
   h->mpts = std::max(K, d->Nqr) * Ne;
   if (e1 == cudaSuccess)
-    e1 = cudaMalloc(&h->mpart, (size_t)h->mpts * kPmCh * 5 * sizeof(double));
+    e1 = cudaMalloc(&h->mpart, (size_t)h->mpts * kPmCh * kPmMaxNa * sizeof(double));
   if (e1 != cudaSuccess) {
     free_dg(h);
     return fail(DGFS_ERR_CUDA, std::string("allocation: ") + cudaGetErrorString(e1));
@@ -1471,22 +1471,70 @@ extern "C" int dgfs_vhs_set_projection(dgfs_vhs_handle h, int32_t enable) {
 // ---------------------------------------------------------------------------
 // Penalty model (IMEX) entry points
 // ---------------------------------------------------------------------------
+// Penalty-model moments: NA = 5 (BGK), 11 (ES-BGK) or 14 (Shakov) per
+// point, in chunks of the handle's partial-sum capacity.
+static int penalty_moments_n(dgfs_dg_s* h, const void* f, int32_t dtype,
+                             int32_t npts, int32_t na, double* U,
+                             cudaStream_t st) {
+  if (!h || !f || !U || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
+  if (na != 5 && na != 11 && na != 14)
+    return fail(DGFS_ERR_INVALID, "moments per point must be 5, 11 or 14");
+  const size_t elem = dtype == DGFS_F64 ? sizeof(double) : sizeof(float);
+  for (int off = 0; off < npts; off += h->mpts) {
+    const int cnt = std::min(h->mpts, npts - off);
+    PenaltyMomentArgs a{};
+    a.f = static_cast<const char*>(f) + (size_t)off * h->base.Nv * elem;
+    a.f_double = dtype == DGFS_F64; a.Nv = h->base.Nv; a.N = h->base.N;
+    a.c0 = h->c0; a.cw = h->cw; a.U = U + (size_t)off * na;
+    const dim3 grid(kPmCh, cnt);
+    if (na == 5) penalty_moments_part_kernel<5><<<grid, 256, 0, st>>>(a, h->mpart);
+    else if (na == 11) penalty_moments_part_kernel<11><<<grid, 256, 0, st>>>(a, h->mpart);
+    else penalty_moments_part_kernel<14><<<grid, 256, 0, st>>>(a, h->mpart);
+    penalty_moments_final_kernel<<<(cnt * na + 127) / 128, 128, 0, st>>>(
+        h->mpart, a.U, cnt, na);
+  }
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
 extern "C" int dgfs_penalty_moments(dgfs_dg_handle h, const void* f,
                                     int32_t dtype, int32_t npts, double* U,
                                     void* stream) {
-  if (!h || !f || !U || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
-  if (npts == 0) return DGFS_OK;
-  PenaltyMomentArgs a{};
-  a.f = f; a.f_double = dtype == DGFS_F64; a.Nv = h->base.Nv; a.N = h->base.N;
-  a.c0 = h->c0; a.cw = h->cw; a.U = U;
+  return penalty_moments_n(h, f, dtype, npts, 5, U, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int dgfs_penalty_moments_n(dgfs_dg_handle h, const void* f,
+                                      int32_t dtype, int32_t npts, int32_t nalph,
+                                      double* U, void* stream) {
+  return penalty_moments_n(h, f, dtype, npts, nalph, U,
+                           static_cast<cudaStream_t>(stream));
+}
+
+static int penalty_kind_ok(int32_t kind) {
+  return kind == kPenBGK || kind == kPenESBGK || kind == kPenShakov;
+}
+
+extern "C" int dgfs_penalty_model_implicit(dgfs_dg_handle h, int32_t kind,
+                                           const double* U, const void* rhs,
+                                           void* f, void* P, void* M,
+                                           int32_t dtype, int32_t npts,
+                                           double adiv, double cdt,
+                                           double prefac, double omega,
+                                           double Pr, void* stream) {
+  if (!h || !U || !rhs || !f || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
+  if (!penalty_kind_ok(kind)) return fail(DGFS_ERR_INVALID, "unknown penalty model");
+  PenaltyImplicitArgs a{};
+  a.U = U; a.rhs = rhs; a.f = f; a.P = P; a.Mout = M;
+  a.f_double = dtype == DGFS_F64; a.Nv = h->base.Nv; a.N = h->base.N;
+  a.c0 = h->c0; a.adiv = adiv; a.cdt = cdt; a.prefac = prefac; a.omega = omega;
+  a.Pr = Pr;
+  a.total = (size_t)npts * h->base.Nv;
+  if (a.total == 0) return DGFS_OK;
+  const dim3 pgrid((h->base.Nv + 256 * kPenaltyEpt - 1) / (256 * kPenaltyEpt), npts);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (npts <= h->mpts) {
-    penalty_moments_part_kernel<<<dim3(kPmCh, npts), 256, 0, st>>>(a, h->mpart);
-    penalty_moments_final_kernel<<<(npts * 5 + 127) / 128, 128, 0, st>>>(
-        h->mpart, U, npts);
-  } else {
-    penalty_moments_kernel<<<npts, 256, 0, st>>>(a);
-  }
+  if (kind == kPenBGK) penalty_implicit_kernel<kPenBGK><<<pgrid, 256, 0, st>>>(a);
+  else if (kind == kPenESBGK) penalty_implicit_kernel<kPenESBGK><<<pgrid, 256, 0, st>>>(a);
+  else penalty_implicit_kernel<kPenShakov><<<pgrid, 256, 0, st>>>(a);
   DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
 }
@@ -1496,15 +1544,29 @@ extern "C" int dgfs_penalty_implicit(dgfs_dg_handle h, const double* U,
                                      void* M, int32_t dtype, int32_t npts,
                                      double adiv, double cdt, double prefac,
                                      double omega, void* stream) {
-  if (!h || !U || !rhs || !f || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
+  return dgfs_penalty_model_implicit(h, kPenBGK, U, rhs, f, P, M, dtype, npts,
+                                     adiv, cdt, prefac, omega, 1.0, stream);
+}
+
+extern "C" int dgfs_penalty_model_collide(dgfs_dg_handle h, int32_t kind,
+                                          const double* U, const void* f,
+                                          void* P, void* M, int32_t dtype,
+                                          int32_t npts, double prefac,
+                                          double omega, double Pr,
+                                          void* stream) {
+  if (!h || !U || !f || !P || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
+  if (!penalty_kind_ok(kind)) return fail(DGFS_ERR_INVALID, "unknown penalty model");
   PenaltyImplicitArgs a{};
-  a.U = U; a.rhs = rhs; a.f = f; a.P = P; a.Mout = M;
+  a.U = U; a.f = const_cast<void*>(f); a.P = P; a.Mout = M;
   a.f_double = dtype == DGFS_F64; a.Nv = h->base.Nv; a.N = h->base.N;
-  a.c0 = h->c0; a.adiv = adiv; a.cdt = cdt; a.prefac = prefac; a.omega = omega;
+  a.c0 = h->c0; a.prefac = prefac; a.omega = omega; a.Pr = Pr;
   a.total = (size_t)npts * h->base.Nv;
   if (a.total == 0) return DGFS_OK;
   const dim3 pgrid((h->base.Nv + 256 * kPenaltyEpt - 1) / (256 * kPenaltyEpt), npts);
-  penalty_implicit_kernel<<<pgrid, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (kind == kPenBGK) penalty_collide_kernel<kPenBGK><<<pgrid, 256, 0, st>>>(a);
+  else if (kind == kPenESBGK) penalty_collide_kernel<kPenESBGK><<<pgrid, 256, 0, st>>>(a);
+  else penalty_collide_kernel<kPenShakov><<<pgrid, 256, 0, st>>>(a);
   DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
 }
@@ -1513,15 +1575,23 @@ extern "C" int dgfs_penalty_collide(dgfs_dg_handle h, const double* U,
                                     const void* f, void* P, void* M,
                                     int32_t dtype, int32_t npts, double prefac,
                                     double omega, void* stream) {
-  if (!h || !U || !f || !P || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
-  PenaltyImplicitArgs a{};
-  a.U = U; a.f = const_cast<void*>(f); a.P = P; a.Mout = M;
-  a.f_double = dtype == DGFS_F64; a.Nv = h->base.Nv; a.N = h->base.N;
-  a.c0 = h->c0; a.prefac = prefac; a.omega = omega;
-  a.total = (size_t)npts * h->base.Nv;
-  if (a.total == 0) return DGFS_OK;
-  const dim3 pgrid((h->base.Nv + 256 * kPenaltyEpt - 1) / (256 * kPenaltyEpt), npts);
-  penalty_collide_kernel<<<pgrid, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  return dgfs_penalty_model_collide(h, kPenBGK, U, f, P, M, dtype, npts,
+                                    prefac, omega, 1.0, stream);
+}
+
+extern "C" int dgfs_penalty_model_relax(dgfs_dg_handle h, int32_t kind,
+                                        double* U, int32_t npts, double adiv,
+                                        double cdt, double prefac, double omega,
+                                        double Pr, void* stream) {
+  if (!h || !U || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
+  if (!penalty_kind_ok(kind)) return fail(DGFS_ERR_INVALID, "unknown penalty model");
+  if (kind == kPenBGK || npts == 0) return DGFS_OK;  // nothing to relax
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned grid = (unsigned)((npts + 127) / 128);
+  if (kind == kPenESBGK)
+    penalty_relax_kernel<kPenESBGK><<<grid, 128, 0, st>>>(U, npts, adiv, cdt, prefac, omega, Pr);
+  else
+    penalty_relax_kernel<kPenShakov><<<grid, 128, 0, st>>>(U, npts, adiv, cdt, prefac, omega, Pr);
   DGFS_CUDA(cudaGetLastError());
   return DGFS_OK;
 }

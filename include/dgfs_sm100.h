@@ -246,6 +246,38 @@ int dgfs_penalty_collide(dgfs_dg_handle h, const double* U, const void* f,
                          void* P, void* M, int32_t dtype, int32_t npts,
                          double prefac, double omega, void* stream);
 
+/*
+ * ES-BGK and Shakov penalty models (astd/scattering.py:280-400,
+ * astd/kernels/scattering/esbgk-direct-gll.mako, shakov-direct-gll.mako;
+ * the boltz-* variants use the same kernels).  kind: 0 BGK (5 moments per
+ * point), 1 ES-BGK (11: + sum f c_i c_j cw), 2 Shakov (14: + sum f |c|^2 c
+ * cw), in the row order of the reference's moment matrices.  The Gaussian is
+ * built from the moments inside the kernels (momentNorm + cmaxwellian).
+ */
+/* U[npts][nalph] = moments of f, nalph = 5, 11 or 14. */
+int dgfs_penalty_moments_n(dgfs_dg_handle h, const void* f, int32_t dtype,
+                           int32_t npts, int32_t nalph, double* U,
+                           void* stream);
+/* After the linear combination of a BDF / IMEX-LM moment update: the
+ * implicit relaxation of the stresses (and the Shakov heat flux) towards the
+ * model's targets (updateMom{q}_BDF: adiv = a_q, cdt = b dt; updateMom{q}_LM:
+ * adiv = 1, cdt = c_0 dt).  A no-op for BGK. */
+int dgfs_penalty_model_relax(dgfs_dg_handle h, int32_t kind, double* U,
+                             int32_t npts, double adiv, double cdt,
+                             double prefac, double omega, double Pr,
+                             void* stream);
+/* dgfs_penalty_implicit / _collide with the model's Gaussian G(U). */
+int dgfs_penalty_model_implicit(dgfs_dg_handle h, int32_t kind,
+                                const double* U, const void* rhs, void* f,
+                                void* P, void* M, int32_t dtype, int32_t npts,
+                                double adiv, double cdt, double prefac,
+                                double omega, double Pr, void* stream);
+int dgfs_penalty_model_collide(dgfs_dg_handle h, int32_t kind,
+                               const double* U, const void* f, void* P,
+                               void* M, int32_t dtype, int32_t npts,
+                               double prefac, double omega, double Pr,
+                               void* stream);
+
 /* x0 <- a0 x0 + sum_i as[i] xs[i] over n elements, 1..4 terms, with the
  * a0 == 0 (x0 not read) and a0 == 1 branches of dgfs1D/axnpby.py:10-44. */
 int dgfs_axnpby(void* x0, int64_t n, int32_t dtype, double a0, int32_t nterms,

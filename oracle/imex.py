@@ -9,6 +9,12 @@ schemes restate dgfs1D/astd/integrator.py (bdf-111 :281-322, bdf-222
 first-order substeps of the same family (the reference uses ARS-222/443
 substeps); ``imex-lm-*`` does not stop after its first step (astd/
 integrator.py:732 exits the process there).
+
+The ES-BGK and Shakov penalty models restate esbgk-direct-gll.mako (momentNorm
+:157-217, cmaxwellian :220-254, updateMom{q}_BDF :16-81, updateMom{q}_LM
+:480-540) and shakov-direct-gll.mako (momentNorm :193-235, cmaxwellian
+:237-278, updateMom{q}_BDF :18-120, updateMom{q}_LM :549-645); their
+distribution updates and collide are the BGK ones with the model's Gaussian.
 """
 import numpy as np
 
@@ -47,6 +53,143 @@ def implicit(U, rhs, cv, adiv, cdt, prefac, omega):
     return (rhs.reshape(M.shape) + cdt * n * M) / (adiv + cdt * n)
 
 
+def moment_rows(cv, nalph):
+    """Rows (1, c, |c|^2, c_x^2, c_y^2, c_z^2, c_x c_y, c_y c_z, c_z c_x,
+    |c|^2 c) of the penalty models' moment matrix, the first nalph
+    (astd/scattering.py:155-162, 306-316, 375-388)."""
+    c2 = np.sum(cv * cv, axis=0)
+    rows = [np.ones(cv.shape[1]), cv[0], cv[1], cv[2], c2, cv[0] ** 2,
+            cv[1] ** 2, cv[2] ** 2, cv[0] * cv[1], cv[1] * cv[2],
+            cv[2] * cv[0], c2 * cv[0], c2 * cv[1], c2 * cv[2]]
+    return np.vstack(rows[:nalph])
+
+
+def moments_n(f, cv, cw, nalph):
+    return f.reshape(-1, cv.shape[1]) @ (moment_rows(cv, nalph) * cw).T
+
+
+# stress pairs (i, j) of moments 8, 9, 10 and the stress rows entering the
+# heat-flux components: x (5, 8, 10), y (8, 6, 9), z (10, 9, 7)
+_OFF = [(1, 2), (2, 3), (3, 1)]
+_QROW = [(5, 8, 10), (8, 6, 9), (10, 9, 7)]
+
+
+class BGKModel:
+    nalph = 5
+
+    def __init__(self, Pr=1.0):
+        self.Pr = Pr
+
+    def gaussian(self, U, cv):
+        return maxwellian(U[:, :5], cv)
+
+    def relax(self, U, adiv, cdt, prefac, omega):
+        return U.copy()
+
+
+class ESBGKModel(BGKModel):
+    """Anisotropic Gaussian with T_ij = T/Pr delta_ij + 2(1 - 1/Pr)(P_ij/rho
+    - u_i u_j); the stress moments relax with rate nu/Pr."""
+    nalph = 11
+
+    def __init__(self, Pr=2. / 3.):
+        self.Pr = Pr
+
+    def gaussian(self, U, cv):
+        rho = U[:, 0]
+        u = U[:, 1:4] / rho[:, None]
+        T = U[:, 4] / (1.5 * rho) - np.sum(u * u, axis=1) / 1.5
+        lam, mu = 1. / self.Pr, 2. * (1. - 1. / self.Pr)
+        A = np.zeros((U.shape[0], 3, 3))
+        for i in range(3):
+            A[:, i, i] = lam * T + mu * (U[:, 5 + i] / rho - u[:, i] ** 2)
+        for k, (i, j) in enumerate(_OFF):
+            v = mu * (U[:, 8 + k] / rho - u[:, i - 1] * u[:, j - 1])
+            A[:, i - 1, j - 1] = A[:, j - 1, i - 1] = v
+        det = np.linalg.det(A)
+        Ainv = np.linalg.inv(A)
+        d = cv[None, :, :] - u[:, :, None]            # (npts, 3, nv)
+        q = np.einsum('pin,pij,pjn->pn', d, Ainv, d)
+        return rho[:, None] / (np.pi ** 1.5 * np.sqrt(det)[:, None]) * np.exp(-q)
+
+    def relax(self, U, adiv, cdt, prefac, omega):
+        V = U.copy()
+        rho, T = U[:, 0], temperature(U[:, :5])
+        k = cdt / self.Pr * prefac * rho * T ** (1. - omega)
+        for s in (5, 6, 7):
+            tau = 0.5 * rho * T + U[:, s - 4] ** 2 / rho
+            V[:, s] = (adiv * U[:, s] + k * tau) / (adiv + k)
+        for n, (i, j) in enumerate(_OFF):
+            tau = U[:, i] * U[:, j] / rho
+            V[:, 8 + n] = (adiv * U[:, 8 + n] + k * tau) / (adiv + k)
+        return V
+
+
+class ShakovModel(BGKModel):
+    """Maxwellian times 1 + 2(1 - Pr)/5 (q.d)/(rho T^2) (2|d|^2/T - 5) with
+    the peculiar heat flux q; stresses relax with rate nu, the heat flux with
+    rate Pr nu."""
+    nalph = 14
+
+    def __init__(self, Pr=2. / 3.):
+        self.Pr = Pr
+
+    def heat_flux(self, U):
+        rho = U[:, 0]
+        u = U[:, 1:4] / rho[:, None]
+        T = U[:, 4] / (1.5 * rho) - np.sum(u * u, axis=1) / 1.5
+        u2 = np.sum(u * u, axis=1)
+        q = np.empty((U.shape[0], 3))
+        for i, (a, b, c) in enumerate(_QROW):
+            q[:, i] = (U[:, 11 + i] - 2 * (U[:, a] * u[:, 0] + U[:, b] * u[:, 1]
+                                           + U[:, c] * u[:, 2])
+                       + rho * u[:, i] * u2 - 1.5 * u[:, i] * rho * T)
+        return rho, u, T, q
+
+    def gaussian(self, U, cv):
+        rho, u, T, q = self.heat_flux(U)
+        d = cv[None, :, :] - u[:, :, None]
+        d2 = np.sum(d * d, axis=1)
+        M = rho[:, None] / (np.pi * T[:, None]) ** 1.5 * np.exp(-d2 / T[:, None])
+        qd = np.einsum('pi,pin->pn', q, d)
+        return M * (1. + 2. * (1. - self.Pr) / 5. * qd
+                    / (rho * T * T)[:, None] * (2. * d2 / T[:, None] - 5.))
+
+    def relax(self, U, adiv, cdt, prefac, omega):
+        V = U.copy()
+        rho, T = U[:, 0], temperature(U[:, :5])
+        nu_ = prefac * rho * T ** (1. - omega)
+        k = cdt * nu_
+        for s in (5, 6, 7):
+            tau = 0.5 * rho * T + U[:, s - 4] ** 2 / rho
+            V[:, s] = (adiv * U[:, s] + k * tau) / (adiv + k)
+        for n, (i, j) in enumerate(_OFF):
+            tau = U[:, i] * U[:, j] / rho
+            V[:, 8 + n] = (adiv * U[:, 8 + n] + k * tau) / (adiv + k)
+        m2 = np.sum(U[:, 1:4] ** 2, axis=1) / rho ** 2
+        Pr = self.Pr
+        for i, (a, b, c) in enumerate(_QROW):
+            ru = U[:, 1 + i]
+            tq = ((1. - Pr) * (-2. * (V[:, a] * U[:, 1] + V[:, b] * U[:, 2]
+                                      + V[:, c] * U[:, 3]) / rho
+                               + ru * m2 - 1.5 * ru * T)
+                  + (ru * m2 + 2.5 * ru * T))
+            V[:, 11 + i] = (adiv * U[:, 11 + i] + k * tq) / (adiv + Pr * k)
+        return V
+
+
+def model_collide(model, U, f, cv, prefac, omega):
+    M = model.gaussian(U, cv)
+    return nu(U[:, :5], prefac, omega)[:, None] * (M - f.reshape(M.shape))
+
+
+def model_implicit(model, U, rhs, cv, adiv, cdt, prefac, omega):
+    """f = (rhs + cdt nu G(U))/(adiv + cdt nu) with the model's Gaussian."""
+    M = model.gaussian(U, cv)
+    n = nu(U[:, :5], prefac, omega)[:, None]
+    return (rhs.reshape(M.shape) + cdt * n * M) / (adiv + cdt * n)
+
+
 class IMEX:
     """Penalised schemes on (K, Ne, Nv) arrays.
 
@@ -54,17 +197,18 @@ class IMEX:
     """
 
     def __init__(self, kind, explicit, boltz, cv, cw, prefac, omega, dt,
-                 f0, nsub=10):
+                 f0, nsub=10, model=None):
         self.kind, self.cv, self.cw = kind, cv, cw
         self.prefac, self.omega, self.dt = prefac, omega, dt
         self.explicit, self.boltz = explicit, boltz
+        self.model = model if model is not None else BGKModel()
         self.shape = f0.shape
         self.step_no = 0
         if kind in ('bdf-222', 'imex-lm-bdf2'):
             f = f0.copy()
             sub = 'bdf-111' if kind == 'bdf-222' else 'imex-lm-bdf1'
             helper = IMEX(sub, explicit, boltz, cv, cw, prefac, omega,
-                          dt / nsub, f0)
+                          dt / nsub, f0, model=self.model)
             for _ in range(nsub):
                 f = helper.step(f)
             self.start = f
@@ -76,11 +220,22 @@ class IMEX:
             self.hist = [self._state(f0)]
 
     def _mom(self, x):
-        return moments5(x, self.cv, self.cw)
+        return moments_n(x, self.cv, self.cw, self.model.nalph)
+
+    def _implicit(self, U, rhs, adiv, cdt):
+        return model_implicit(self.model, U, rhs, self.cv, adiv, cdt,
+                              self.prefac, self.omega).reshape(self.shape)
+
+    def _collide(self, U, f):
+        return model_collide(self.model, U, f, self.cv, self.prefac,
+                             self.omega).reshape(self.shape)
+
+    def _relax(self, U, adiv, cdt):
+        return self.model.relax(U, adiv, cdt, self.prefac, self.omega)
 
     def _state(self, f):
         U = self._mom(f)
-        P = collide(U, f, self.cv, self.prefac, self.omega).reshape(self.shape)
+        P = self._collide(U, f)
         E = self.explicit(f) + self.boltz(f) - P
         return dict(F=f.copy(), U=U, P=P, LM=self._mom(P), L=E,
                     LU=self._mom(E))
@@ -95,10 +250,9 @@ class IMEX:
             U0 = self._mom(f)
             L0 = self.explicit(f)
             LU0 = self._mom(L0)
-            U = -((-1.) * U0 + (-1.) * dt * LU0) / 1.
+            U = self._relax(-((-1.) * U0 + (-1.) * dt * LU0) / 1., 1., dt)
             rhs = -((-1.) * f + (-1.) * dt * L0)
-            return implicit(U, rhs, self.cv, 1., dt, self.prefac,
-                            self.omega).reshape(self.shape)
+            return self._implicit(U, rhs, 1., dt)
         if k == 'bdf-222':
             a1, a2, a3 = 1. / 3., -4. / 3., 1.
             g1, g2 = -2. / 3., 4. / 3.
@@ -109,10 +263,10 @@ class IMEX:
             h0, h1 = self.hist
             U = -(a1 * h0['U'] + (-g1) * dt * h0['LU'] + a2 * h1['U']
                   + (-g2) * dt * h1['LU']) / a3
+            U = self._relax(U, a3, b * dt)
             rhs = -(a1 * h0['F'] + (-g1) * dt * h0['L'] + a2 * h1['F']
                     + (-g2) * dt * h1['L'])
-            fn = implicit(U, rhs, self.cv, a3, b * dt, self.prefac,
-                          self.omega).reshape(self.shape)
+            fn = self._implicit(U, rhs, a3, b * dt)
             self.hist = [h1, self._bdf_state(fn)]
             self.step_no += 1
             return fn
@@ -130,9 +284,9 @@ class IMEX:
                     + dt * C[s - i] * hs[i]['LM'] for i in range(s))
             rhs = sum(-A[s - i - 1] * hs[i]['F'] + dt * B[s - i - 1] * hs[i]['L']
                       + dt * C[s - i] * hs[i]['P'] for i in range(s))
-            fn = implicit(U, rhs, self.cv, 1., C[0] * dt, self.prefac,
-                          self.omega).reshape(self.shape)
-            P = collide(U, fn, self.cv, self.prefac, self.omega).reshape(self.shape)
+            U = self._relax(U, 1., C[0] * dt)
+            fn = self._implicit(U, rhs, 1., C[0] * dt)
+            P = self._collide(U, fn)
             E = self.explicit(fn) + self.boltz(fn) - P
             new = dict(F=fn.copy(), U=U, P=P, LM=self._mom(P), L=E,
                        LU=self._mom(E))

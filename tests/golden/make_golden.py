@@ -4,6 +4,7 @@ Run in a container where the reference checkout exists (``$DGFS_REF``,
 default /root/reference)::
 
     python tests/golden/make_golden.py
+    python tests/golden/make_golden.py penalty-models   # only the ES-BGK/Shakov files
 
 What runs from the reference:
   * its pure-Python setup code, imported directly with stand-ins for the
@@ -596,6 +597,86 @@ def golden_penalty(R, Nv=8, npts=6, omega=0.81, prefac=3.7):
     return out
 
 
+def golden_penalty_model(name, nalph, Nv=8, npts=6, omega=0.81, prefac=3.7,
+                         Pr=2. / 3.):
+    """The ES-BGK / Shakov penalty kernels (astd esbgk-direct-gll.mako,
+    shakov-direct-gll.mako) on seeded data: moment normalisation + Gaussian,
+    collide, the BDF2 and IMEX-LM2 moment and distribution updates, called
+    the way the reference's integrators call them."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    vsize = Nv ** 3
+    src = render_template(
+        'dgfs1D/astd/kernels/scattering/%s.mako' % name, vsize=vsize,
+        nalph=nalph, omega=omega, Pr=Pr, dtype='double', nbdf=[1, 2],
+        nars=[1, 2])
+    K = RefModule(src, tag=name.split('-')[0])
+    rng = np.random.default_rng(SEED + 13 + nalph)
+    L = 5.0
+    c0 = np.linspace(-L + L / Nv, L - L / Nv, Nv)
+    g = np.meshgrid(c0, c0, c0, indexing='ij')
+    cv = np.stack([x.ravel() for x in g])
+    cw = (2 * L / Nv) ** 3
+    f = np.stack([_maxwellian_noise(cv, rng, rho=rng.uniform(0.5, 2))
+                  for _ in range(npts)]).ravel()
+    c2 = np.sum(cv * cv, axis=0)
+    rows = [np.ones(vsize), cv[0], cv[1], cv[2], c2, cv[0] ** 2, cv[1] ** 2,
+            cv[2] ** 2, cv[0] * cv[1], cv[1] * cv[2], cv[2] * cv[0],
+            c2 * cv[0], c2 * cv[1], c2 * cv[2]][:nalph]
+    phi = np.vstack(rows) * cw
+    U = np.ascontiguousarray((f.reshape(npts, vsize) @ phi.T).ravel())
+    blk = 256
+    lda = npts * vsize
+    gg = grid_for(lda, blk)
+    gm = grid_for(npts, blk)
+    cx, cy, cz = (np.ascontiguousarray(cv[i]) for i in range(3))
+
+    def gauss(Ux):
+        nU = Ux.copy()
+        K.launch('momentNorm', gm, blk, npts, nU)
+        Mx = np.zeros(lda)
+        K.launch('cmaxwellian', gg, blk, lda, cx, cy, cz, Mx, nU)
+        return Mx, nU
+    M, normU = gauss(U)
+    Q = np.zeros(lda)
+    K.launch('collide', gg, blk, prefac, lda, M, U, f, Q)
+    out = dict(Nv=Nv, npts=npts, omega=omega, prefac=prefac, Pr=Pr,
+               nalph=nalph, cv=cv, cw=cw, f=f, U=U, normU=normU, M=M, Q=Q)
+    dt = 0.01
+    L0 = rng.normal(size=lda) * 1e-3
+    L1 = rng.normal(size=lda) * 1e-3
+    f1 = f * (1 + 0.01 * rng.uniform(-1, 1, lda))
+    LU0 = rng.normal(size=npts * nalph) * 1e-3
+    LU1 = rng.normal(size=npts * nalph) * 1e-3
+    U1 = U * (1 + 0.01 * rng.uniform(-1, 1, U.shape))
+    Un = np.zeros(npts * nalph)
+    # bdf-222 coefficients, called as Bdf222IntegratorAstd does
+    a1, a2, a3, g1, g2, b = 1. / 3., -4. / 3., 1., -2. / 3., 4. / 3., 2. / 3.
+    K.launch('updateMom2_BDF', gm, blk, prefac, npts, dt, a1, U, -g1, LU0,
+             a2, U1, -g2, LU1, a3, Un, b)
+    Mn, _ = gauss(Un)
+    fn = np.zeros(lda)
+    K.launch('updateDistribution2_BDF', gg, blk, prefac, lda, dt, a1, f, -g1,
+             L0, a2, f1, -g2, L1, b, Mn, a3, Un, fn)
+    out.update(dt=dt, L0=L0, L1=L1, f1=f1, LU0=LU0, LU1=LU1, U1=U1,
+               Un_bdf2=Un, Mn_bdf2=Mn, fn_bdf2=fn)
+    # imex-lm-bdf2 coefficients (A, B, C of IMEXLM_BDF2_IntegratorAstd)
+    A, B, C = [-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]
+    LM0 = rng.normal(size=npts * nalph) * 1e-4
+    LM1 = rng.normal(size=npts * nalph) * 1e-4
+    P0 = rng.normal(size=lda) * 1e-4
+    P1 = rng.normal(size=lda) * 1e-4
+    U2 = np.zeros(npts * nalph)
+    K.launch('updateMom2_LM', gm, blk, prefac, npts, dt, *A, *B, *C, LU0, LU1,
+             LM0, LM1, U, U1, U2)
+    M2, _ = gauss(U2)
+    f2 = np.zeros(lda)
+    K.launch('updateDistribution2_LM', gg, blk, prefac, lda, dt, *A, *B, *C,
+             L0, L1, P0, P1, M2, f, f1, f2, U, U1, U2)
+    out.update(LM0=LM0, LM1=LM1, P0=P0, P1=P1, U2_lm2=U2, M2_lm2=M2,
+               f2_lm2=f2)
+    return out
+
+
 def golden_setup(R):
     """Velocity meshes, rules and DG bases from the reference setup code."""
     out = {}
@@ -651,10 +732,22 @@ def main():
             **golden_dg(R, kind))
     np.savez_compressed(os.path.join(HERE, 'penalty_N8.npz'),
                         **golden_penalty(R))
+    penalty_models()
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith('.npz'):
             print(fn, os.path.getsize(os.path.join(HERE, fn)), 'bytes')
 
 
+def penalty_models():
+    for name, nalph, tag in (('esbgk-direct-gll', 11, 'esbgk'),
+                             ('shakov-direct-gll', 14, 'shakov')):
+        np.savez_compressed(os.path.join(HERE, 'penalty_%s_N8.npz' % tag),
+                            **golden_penalty_model(name, nalph))
+
+
 if __name__ == '__main__':
-    main()
+    import sys
+    if sys.argv[1:] == ['penalty-models']:
+        penalty_models()
+    else:
+        main()

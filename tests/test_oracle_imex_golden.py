@@ -1,9 +1,12 @@
-"""The IMEX oracle's kernels against the reference's bgk-direct-gll.mako."""
+"""The IMEX oracle's kernels against the reference's bgk-direct-gll.mako,
+esbgk-direct-gll.mako and shakov-direct-gll.mako."""
 import os
 
 import numpy as np
+import pytest
 
 from oracle import imex as oim
+from oracle import imex as oi
 
 G = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
 
@@ -54,3 +57,43 @@ def test_penalty_kernels_match_reference():
     nu2 = oim.nu(U2, pre, om)[:, None]
     f2 = (rhs.reshape(M.shape) + C[0] * dt * nu2 * M) / (1.0 + C[0] * dt * nu2)
     assert _rel(f2, g['f2_lm2']) < 1e-13
+
+
+@pytest.mark.parametrize('tag', ['esbgk', 'shakov'])
+def test_esbgk_shakov_oracle_matches_reference(tag):
+    """The oracle's ES-BGK / Shakov penalty models against the reference's
+    own kernels (esbgk-direct-gll.mako, shakov-direct-gll.mako compiled for
+    the CPU): moments, moment normalisation + Gaussian, collide, and the BDF2
+    and IMEX-LM2 moment and distribution updates."""
+    z = np.load(os.path.join(G, 'penalty_%s_N8.npz' % tag))
+    model = {'esbgk': oi.ESBGKModel, 'shakov': oi.ShakovModel}[tag](float(z['Pr']))
+    na, npts, cv, cw = int(z['nalph']), int(z['npts']), z['cv'], float(z['cw'])
+    pf, om, dt = float(z['prefac']), float(z['omega']), float(z['dt'])
+    f = z['f'].reshape(npts, -1)
+
+    def rel(a, b):
+        return float(np.abs(np.ravel(a) - np.ravel(b)).max() / np.abs(np.ravel(b)).max())
+    U = oi.moments_n(f, cv, cw, na)
+    assert rel(U, z['U']) < 1e-13
+    assert rel(model.gaussian(U, cv), z['M']) < 1e-13
+    assert rel(oi.model_collide(model, U, f, cv, pf, om), z['Q']) < 1e-12
+    sh = lambda k: z[k].reshape(npts, -1)
+    a1, a2, a3, g1, g2, b = 1. / 3., -4. / 3., 1., -2. / 3., 4. / 3., 2. / 3.
+    Ul = -(a1 * U + (-g1) * dt * sh('LU0') + a2 * sh('U1') + (-g2) * dt * sh('LU1')) / a3
+    Un = model.relax(Ul, a3, b * dt, pf, om)
+    assert rel(Un, z['Un_bdf2']) < 1e-13
+    assert rel(model.gaussian(Un, cv), z['Mn_bdf2']) < 1e-13
+    rhs = -(a1 * f + (-g1) * dt * sh('L0') + a2 * sh('f1') + (-g2) * dt * sh('L1'))
+    fn = oi.model_implicit(model, Un, rhs, cv, a3, b * dt, pf, om)
+    assert rel(fn, z['fn_bdf2']) < 1e-13
+    A, B, C = [-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]
+    Us, LUs, LMs = [U, sh('U1')], [sh('LU0'), sh('LU1')], [sh('LM0'), sh('LM1')]
+    Ul = sum(-A[1 - i] * Us[i] + dt * B[1 - i] * LUs[i] + dt * C[2 - i] * LMs[i]
+             for i in range(2))
+    U2 = model.relax(Ul, 1.0, C[0] * dt, pf, om)
+    assert rel(U2, z['U2_lm2']) < 1e-13
+    Fs, Ls, Ps = [f, sh('f1')], [sh('L0'), sh('L1')], [sh('P0'), sh('P1')]
+    rhs = sum(-A[1 - i] * Fs[i] + dt * B[1 - i] * Ls[i] + dt * C[2 - i] * Ps[i]
+              for i in range(2))
+    f2 = oi.model_implicit(model, U2, rhs, cv, 1.0, C[0] * dt, pf, om)
+    assert rel(f2, z['f2_lm2']) < 1e-13
