@@ -2,13 +2,15 @@
 
 Keys and coefficients of dgfs1D/astd/integrator.py: ``bdf-111`` / ``bdf-222``
 (penalty model only, explicit DG advection; :281-400) and ``imex-lm-bdf1`` /
-``imex-lm-bdf2`` (explicit L + Q - P, implicit P(f^{n+1}); :623-792).  The
+``imex-lm-bdf2`` and the other ``imex-lm-*`` schemes (cn2, ad2, sg2, bdf3,
+ad3, tvb3, bdf4, tvb4, shu3, shu4; explicit L + Q - P, implicit P(f^{n+1});
+:623-907).  The
 moment update is the linear combination of the scheme followed by the
 penalty model's implicit relaxation of its non-conserved moments (the
 updateMoment{BDF,LM} kernels of the model).
-Differences from the reference, all in start-up or dead code: start-up
-states come from first-order substeps of the same family (the reference
-uses ARS-222/443 substeps); the explicit part of a new IMEX-LM level uses
+Differences from the reference, all in start-up or dead code: the s - 1
+start-up levels come from first-order substeps of the same family (the
+reference uses ARS-222/443 substeps); the explicit part of a new IMEX-LM level uses
 that level's penalty P(f^{n+1}) (the reference's two-stage path would use
 the previous level's after its circular shift, but exits the process after
 its first step, astd/integrator.py:732, so it never gets there).
@@ -116,19 +118,22 @@ class IMEXLMIntegratorAstd(DGFSIntegratorAstd):
         super().__init__(explicit, sm, shape, dtype, t=t, dt=dt, f0=f0,
                          explicitQ=explicitQ, **kwargs)
         s = len(self.A)
-        self.hist = []
+        self.hist = [self._state(t, f0)]
+        self.starts = []
         if s > 1:
+            # levels 1 .. s-1 by nsub first-order substeps each, continuing
             f = f0.clone()
             sub = IMEXLMBdf1IntegratorAstd(explicit, sm, shape, dtype, t=t,
                                            dt=dt / self.nsub, f0=f,
                                            explicitQ=explicitQ,
                                            device=self.device)
-            for i in range(self.nsub):
-                sub.integrate(t + i * dt / self.nsub, dt / self.nsub, i, f)
-            self.start = f
-            self.hist = [self._state(t, f0), self._state(t + dt, f)]
-        else:
-            self.hist = [self._state(t, f0)]
+            k = 0
+            for lvl in range(1, s):
+                for _ in range(self.nsub):
+                    sub.integrate(t + k * dt / self.nsub, dt / self.nsub, k, f)
+                    k += 1
+                self.starts.append(f.clone())
+                self.hist.append(self._state(t + lvl * dt, f))
 
     def _state(self, t, f):
         U = self._mom(f)
@@ -146,7 +151,7 @@ class IMEXLMIntegratorAstd(DGFSIntegratorAstd):
         A, B, C = self.A, self.B, self.C
         s = len(A)
         if nacptsteps < s - 1:
-            f.copy_(self.start)
+            f.copy_(self.starts[nacptsteps])
             return
         hs = self.hist
         U = self._zm()
@@ -178,3 +183,45 @@ class IMEXLMBdf1IntegratorAstd(IMEXLMIntegratorAstd):
 class IMEXLMBdf2IntegratorAstd(IMEXLMIntegratorAstd):
     intg_kind = 'imex-lm-bdf2'
     A, B, C = [-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]
+
+
+# The remaining IMEX linear multistep schemes of astd/integrator.py:751-907
+# (coefficient tables kept as the reference defines them: A, B of length s,
+# C of length s + 1).
+_LM_SCHEMES = {
+    'imex-lm-cn2': ([-1., 0.], [1.5, -0.5], [0.5, 0.5, 0.]),
+    'imex-lm-ad2': ([-1., 0.], [1.5, -0.5], [9. / 16., 3. / 8., 1. / 16.]),
+    'imex-lm-sg2': ([-3. / 4., 0., -1. / 4.], [3. / 2., 0., 0.],
+                    [1., 0., 0., 1. / 2.]),
+    'imex-lm-bdf3': ([-18. / 11., 9. / 11., -2. / 11.],
+                     [18. / 11., -18. / 11., 6. / 11.], [6. / 11., 0., 0., 0.]),
+    'imex-lm-ad3': ([-1., 0., 0.], [23. / 12., -4. / 3., 5. / 12.],
+                    [4661. / 10000., 15551. / 30000., 1949. / 30000.,
+                     -1483. / 30000.]),
+    'imex-lm-tvb3': ([-3909. / 2048., 1367. / 1024., -873. / 2048.],
+                     [18463. / 12288., -1271. / 768., 8233. / 12288.],
+                     [1089. / 2048., -1139. / 12288., -367. / 6144.,
+                      1699. / 12288.]),
+    'imex-lm-bdf4': ([-48. / 25., 36. / 25., -16. / 25., 3. / 25.],
+                     [48. / 25., -72. / 25., 48. / 25., -12. / 25.],
+                     [12. / 25., 0., 0., 0., 0.]),
+    'imex-lm-tvb4': ([-21531. / 8192., 22753. / 8192., -12245. / 8192.,
+                      2831. / 8192.],
+                     [13261. / 8192., -75029. / 24576., 54799. / 24576.,
+                      -15245. / 24576.],
+                     [4207. / 8192., -3567. / 8192., 697. / 24576.,
+                      4315. / 24576., -41. / 384.]),
+    'imex-lm-shu3': ([-16. / 27, 0., 0., -11. / 27.], [16. / 9., 0., 0., 4. / 9.],
+                     [9035. / 19683., 13541. / 19683., 1127. / 2187.,
+                      7927. / 19683., 3094. / 19683.]),
+    'imex-lm-shu4': ([-137. / 400., 0., 0., -959. / 5000., -8781. / 94000.,
+                      -87487 / 235000.],
+                     [976903. / 470000., 0., 0., 136757. / 117500.,
+                      266997. / 470000., 0.],
+                     [237. / 500., 7547. / 10000., 299. / 400., 4513. / 5875.,
+                      118099. / 235000., 174527. / 470000., 90349. / 470000.]),
+}
+for _kind, (_A, _B, _C) in _LM_SCHEMES.items():
+    globals()['IMEXLM_%s_IntegratorAstd' % _kind.split('-')[-1].upper()] = type(
+        'IMEXLM_%s_IntegratorAstd' % _kind.split('-')[-1].upper(),
+        (IMEXLMIntegratorAstd,), dict(intg_kind=_kind, A=_A, B=_B, C=_C))

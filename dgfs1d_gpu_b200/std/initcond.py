@@ -1,7 +1,7 @@
 """Initial-condition plugins (``[soln-ics] type``) of the single-species solver.
 
-``maxwellian`` and ``bkw`` restate dgfs1D/std/initcond.py:36-141 (values on
-the velocity grid, nondimensional).  ``maxwellian-noise`` (no counterpart in
+``maxwellian``, ``bkw`` and ``sod-shock-tube`` restate dgfs1D/std/
+initcond.py:36-141, 320-383 (values on the velocity grid, nondimensional).  ``maxwellian-noise`` (no counterpart in
 the reference) multiplies the Maxwellian by (1 + amp U[-1, 1]), i.i.d. per
 phase-space point from a seeded generator (keys ``noise``, ``seed``).
 ``normal-shock`` (no counterpart in the reference) joins an upstream and a
@@ -118,3 +118,43 @@ class DGFSNormalShockInitConditionStd(DGFSInitConditionStd):
         if self._amp:
             rng = np.random.default_rng(self._seed)
             usol *= 1 + self._amp * rng.uniform(-1, 1, usol.shape)
+
+
+class DGFSSodShockTubeInitConditionStd(DGFSInitConditionStd):
+    """Sod shock tube (std/initcond.py:320-383): the left half of the
+    elements holds the Maxwellian (rho-left, T-left, ux-left), the right half
+    (rho-right, T-right, ux-right), dimensional as ``maxwellian``; Ne must be
+    even, and each Maxwellian's density must be resolved by the grid."""
+    model = 'sod-shock-tube'
+
+    def load_parameters(self, name):
+        vm, cfg = self.vm, self.cfg
+        self._states = []
+        for side in ('left', 'right'):
+            rho = cfg.lookupfloat(name, 'rho-' + side) / vm.rho0()
+            T = cfg.lookupfloat(name, 'T-' + side) / vm.T0()
+            ux = cfg.lookupordefault(name, 'ux-' + side, 0.) / vm.u0()
+            self._states.append((rho, T, ux))
+
+    def perform_precomputation(self):
+        cv, cw = self.vm.cv(), self.vm.cw()
+        self._M = []
+        for rho, T, ux in self._states:
+            u = np.array([ux, 0.0, 0.0]).reshape(3, 1)
+            M = rho / (np.pi * T) ** 1.5 * np.exp(-np.sum((cv - u) ** 2, axis=0) / T)
+            if not np.allclose(rho, np.sum(M) * cw, atol=1e-5):
+                raise ValueError('Bulk properties not conserved! Check Nv, dev')
+            self._M.append(M)
+        self._init_vals = self._M[0]
+
+    def get_init_vals(self):
+        raise ValueError('this model depends on spatial coordinates!')
+
+    def unondim(self):
+        raise ValueError('this model depends on spatial coordinates!')
+
+    def apply_init_vals(self, usol, Nq, Ne, xsol=None):
+        if Ne % 2:
+            raise ValueError('Not implemented')
+        usol[:, :Ne // 2, :] = self._M[0][None, None, :]
+        usol[:, Ne // 2:, :] = self._M[1][None, None, :]

@@ -190,6 +190,38 @@ def model_implicit(model, U, rhs, cv, adiv, cdt, prefac, omega):
     return (rhs.reshape(M.shape) + cdt * n * M) / (adiv + cdt * n)
 
 
+# (A, B, C) of the IMEX linear multistep schemes, astd/integrator.py:736-907
+LM_COEF = {
+    'imex-lm-bdf1': ([-1.], [1.], [1., 0.]),
+    'imex-lm-bdf2': ([-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]),
+    'imex-lm-cn2': ([-1., 0.], [1.5, -0.5], [0.5, 0.5, 0.]),
+    'imex-lm-ad2': ([-1., 0.], [1.5, -0.5], [9. / 16., 3. / 8., 1. / 16.]),
+    'imex-lm-sg2': ([-3. / 4., 0., -1. / 4.], [3. / 2., 0., 0.], [1., 0., 0., 1. / 2.]),
+    'imex-lm-bdf3': ([-18. / 11., 9. / 11., -2. / 11.], [18. / 11., -18. / 11., 6. / 11.],
+                     [6. / 11., 0., 0., 0.]),
+    'imex-lm-ad3': ([-1., 0., 0.], [23. / 12., -4. / 3., 5. / 12.],
+                    [4661. / 10000., 15551. / 30000., 1949. / 30000., -1483. / 30000.]),
+    'imex-lm-tvb3': ([-3909. / 2048., 1367. / 1024., -873. / 2048.],
+                     [18463. / 12288., -1271. / 768., 8233. / 12288.],
+                     [1089. / 2048., -1139. / 12288., -367. / 6144., 1699. / 12288.]),
+    'imex-lm-bdf4': ([-48. / 25., 36. / 25., -16. / 25., 3. / 25.],
+                     [48. / 25., -72. / 25., 48. / 25., -12. / 25.],
+                     [12. / 25., 0., 0., 0., 0.]),
+    'imex-lm-tvb4': ([-21531. / 8192., 22753. / 8192., -12245. / 8192., 2831. / 8192.],
+                     [13261. / 8192., -75029. / 24576., 54799. / 24576., -15245. / 24576.],
+                     [4207. / 8192., -3567. / 8192., 697. / 24576., 4315. / 24576.,
+                      -41. / 384.]),
+    'imex-lm-shu3': ([-16. / 27, 0., 0., -11. / 27.], [16. / 9., 0., 0., 4. / 9.],
+                     [9035. / 19683., 13541. / 19683., 1127. / 2187., 7927. / 19683.,
+                      3094. / 19683.]),
+    'imex-lm-shu4': ([-137. / 400., 0., 0., -959. / 5000., -8781. / 94000.,
+                      -87487 / 235000.],
+                     [976903. / 470000., 0., 0., 136757. / 117500., 266997. / 470000., 0.],
+                     [237. / 500., 7547. / 10000., 299. / 400., 4513. / 5875.,
+                      118099. / 235000., 174527. / 470000., 90349. / 470000.]),
+}
+
+
 class IMEX:
     """Penalised schemes on (K, Ne, Nv) arrays.
 
@@ -204,20 +236,27 @@ class IMEX:
         self.model = model if model is not None else BGKModel()
         self.shape = f0.shape
         self.step_no = 0
-        if kind in ('bdf-222', 'imex-lm-bdf2'):
+        self.starts = []
+        if kind == 'bdf-222':
             f = f0.copy()
-            sub = 'bdf-111' if kind == 'bdf-222' else 'imex-lm-bdf1'
-            helper = IMEX(sub, explicit, boltz, cv, cw, prefac, omega,
+            helper = IMEX('bdf-111', explicit, boltz, cv, cw, prefac, omega,
                           dt / nsub, f0, model=self.model)
             for _ in range(nsub):
                 f = helper.step(f)
-            self.start = f
-            if kind == 'imex-lm-bdf2':
-                self.hist = [self._state(f0), self._state(f)]
-            else:
-                self.hist = [self._bdf_state(f0), self._bdf_state(f)]
-        elif kind == 'imex-lm-bdf1':
+            self.starts = [f]
+            self.hist = [self._bdf_state(f0), self._bdf_state(f)]
+        elif kind in LM_COEF:
+            s = len(LM_COEF[kind][0])
             self.hist = [self._state(f0)]
+            if s > 1:
+                f = f0.copy()
+                helper = IMEX('imex-lm-bdf1', explicit, boltz, cv, cw, prefac,
+                              omega, dt / nsub, f0, model=self.model)
+                for _ in range(1, s):
+                    for _ in range(nsub):
+                        f = helper.step(f)
+                    self.starts.append(f.copy())
+                    self.hist.append(self._state(f))
 
     def _mom(self, x):
         return moments_n(x, self.cv, self.cw, self.model.nalph)
@@ -259,7 +298,7 @@ class IMEX:
             b = 2. / 3.
             if self.step_no == 0:
                 self.step_no += 1
-                return self.start.copy()
+                return self.starts[0].copy()
             h0, h1 = self.hist
             U = -(a1 * h0['U'] + (-g1) * dt * h0['LU'] + a2 * h1['U']
                   + (-g2) * dt * h1['LU']) / a3
@@ -270,15 +309,12 @@ class IMEX:
             self.hist = [h1, self._bdf_state(fn)]
             self.step_no += 1
             return fn
-        if k in ('imex-lm-bdf1', 'imex-lm-bdf2'):
-            if k == 'imex-lm-bdf1':
-                A, B, C = [-1.], [1.], [1., 0.]
-            else:
-                A, B, C = [-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]
+        if k in LM_COEF:
+            A, B, C = LM_COEF[k]
             s = len(A)
             if s > 1 and self.step_no < s - 1:
                 self.step_no += 1
-                return self.start.copy()
+                return self.starts[self.step_no - 1].copy()
             hs = self.hist
             U = sum(-A[s - i - 1] * hs[i]['U'] + dt * B[s - i - 1] * hs[i]['LU']
                     + dt * C[s - i] * hs[i]['LM'] for i in range(s))
