@@ -152,6 +152,11 @@ _SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
       ctypes.c_double, ctypes.c_void_p]),
+    ('dgfs_dg_set_limiter', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_void_p]),
+    ('dgfs_dg_limit', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     ('dgfs_penalty_moments_n', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
       ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),

@@ -74,6 +74,10 @@ class DGFSABstd1D:
                          t=ti, dt=self.dt, f0=self.u, explicitQ=self.explicitQ,
                          device=self.device)
         self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, self.xsol)
+        # linear slope limiter after every step (abstd.py:459, 476)
+        self.limiter = int(cfg.lookupordefault('time-integrator', 'limiter', 0))
+        if self.limiter:
+            self.dg.set_limiter(basis, mesh.invjac, self.xsol)
 
     def explicit(self, t, u_in, u_out):
         self.dg.advect(u_in, u_out)
@@ -87,6 +91,8 @@ class DGFSABstd1D:
 
     def step(self):
         self.odes.integrate(self.t, self.dt, self.nacptsteps, self.u)
+        if self.limiter:
+            self.dg.limit(self.u)
         self.t += self.dt
         self.nacptsteps += 1
 

@@ -48,6 +48,16 @@ class Basis:
         self.faceOp = _filter(self.Bqf.T)          # (Nqf, K) face traces
         self.derivOp = _filter(self.derivMat)      # ux = derivOp . u
         self.invMassOp = _filter(self.invMassMat)
+        # slope-limiter operators (dgfs1D/basis.py:289-301): projections onto
+        # the Legendre mode 0 (cell average) and modes 0-1 (linear part, then
+        # differentiated), as the nodal values of each element
+        Vo = legendre_orthonormal(self.K, self.z).T
+        invV = np.linalg.inv(Vo)
+        A0, A1 = Vo.copy(), Vo.copy()
+        A0[:, 1:] = 0.0
+        A1[:, 2:] = 0.0
+        self.cellAvgOp = _filter(A0 @ invV)
+        self.drLinOp = _filter(self.derivMat @ (A1 @ invV))
 
     def mode_sources(self):
         """For nodal bases: the coefficient slot feeding each (m, r) term.

@@ -48,6 +48,67 @@ __device__ __forceinline__ void st(void* p, int dbl, size_t i, double v) {
   else static_cast<float*>(p)[i] = (float)v;
 }
 
+// Linear slope limiter of dgfsABstd1D (``[time-integrator] limiter = 1``,
+// abstd.py:403-415 with limitLin of astd/kernels/limiters.mako:17-76), in
+// place, one thread per velocity point walking the interior elements.  The
+// cell averages (row 0 of the cell-average operator) and the linear slopes
+// (row 0 of the differentiated linear projection, times invjac) come from the
+// unlimited solution: a window of three averages is formed before an element
+// is written.  An element is limited when its end values differ from the
+// minmod-limited linear reconstruction by more than tol; it then becomes
+// avg + dx_k minmod(slope, (avg_R - avg)/h, (avg - avg_L)/h).
+struct DgLimitArgs {
+  void* u;
+  int f_double;
+  int K, Ne, Nv;
+  const double* wavg;   // [K]
+  const double* wdr;    // [K]
+  const double* invjac; // [Ne]
+  const double* dx;     // [K][Ne] node position minus element centre
+  const double* h;      // [Ne] element length
+  double tol;
+};
+
+__device__ __forceinline__ double minmod3(double a, double b, double c) {
+  const int sa = (a > 0) - (a < 0), sb = (b > 0) - (b < 0), sc = (c > 0) - (c < 0);
+  const int m = (sa + sb + sc) / 3;
+  return (m == 1 || m == -1) ? m * fmin(fmin(fabs(a), fabs(b)), fabs(c)) : 0.;
+}
+
+__global__ void __launch_bounds__(256) dg_limit_kernel(DgLimitArgs a) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= a.Nv || a.Ne < 3) return;
+  const int K = a.K, Ne = a.Ne;
+  auto U = [&](int k, int e) {
+    return ld(a.u, a.f_double, ((size_t)k * Ne + e) * a.Nv + v);
+  };
+  auto avg = [&](int e) {
+    double s = 0;
+    for (int k = 0; k < K; ++k) s += a.wavg[k] * U(k, e);
+    return s;
+  };
+  double aL = avg(0), ac = avg(1);
+  for (int e = 1; e < Ne - 1; ++e) {
+    const double aR = avg(e + 1);
+    const double u0 = U(0, e), uK = U(K - 1, e);
+    const bool lim =
+        fabs(ac - minmod3(ac - u0, aR - ac, ac - aL) - u0) +
+            fabs(ac + minmod3(uK - ac, aR - ac, ac - aL) - uK) > a.tol;
+    if (lim) {
+      double sl = 0;
+      for (int k = 0; k < K; ++k) sl += a.wdr[k] * U(k, e);
+      sl *= a.invjac[e];
+      const double he = a.h[e];
+      const double m = minmod3(sl, (aR - ac) / he, (ac - aL) / he);
+      for (int k = 0; k < K; ++k)
+        st(a.u, a.f_double, ((size_t)k * Ne + e) * a.Nv + v,
+           ac + a.dx[k * Ne + e] * m);
+    }
+    aL = ac;
+    ac = aR;
+  }
+}
+
 // Wall densities n_w = -sum_{out} (c-u_w).n f cw / sum_{in} (c-u_w).n f0 cw
 // (updateBC of dgfs-wall-diffuse.mako with the two gpuarray.sum of
 // std/bc.py:63-76), in a deterministic order.

@@ -939,13 +939,14 @@ struct dgfs_dg_s {
   double* part = nullptr;  // residual partials
   double* part_h = nullptr;
   double* wpart = nullptr;  // wall-density partials [2][kWallCh][2]
+  double* lim = nullptr;    // limiter tables: wavg [K] | wdr [K] | dx [K][Ne] | h [Ne]
   double* mpart = nullptr;  // penalty-moment partials [mpts][kPmCh][<= 14]
   int mpts = 0;
 };
 
 static void free_dg(dgfs_dg_s* h) {
   void* ptrs[] = {h->c0, h->invjac, h->f0[0], h->f0[1], h->nden, h->im, h->part,
-                  h->wpart, h->mpart};
+                  h->wpart, h->mpart, h->lim};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->part_h) cudaFreeHost(h->part_h);
@@ -1471,6 +1472,40 @@ extern "C" int dgfs_vhs_set_projection(dgfs_vhs_handle h, int32_t enable) {
 // ---------------------------------------------------------------------------
 // Penalty model (IMEX) entry points
 // ---------------------------------------------------------------------------
+// Linear slope limiter: tables (host, FP64) then in-place application.
+extern "C" int dgfs_dg_set_limiter(dgfs_dg_handle h, const double* wavg,
+                                   const double* wdr, const double* dx,
+                                   const double* hs) {
+  if (!h || !wavg || !wdr || !dx || !hs) return fail(DGFS_ERR_INVALID, "null argument");
+  const int K = h->base.K, Ne = h->base.Ne;
+  std::vector<double> t;
+  t.insert(t.end(), wavg, wavg + K);
+  t.insert(t.end(), wdr, wdr + K);
+  t.insert(t.end(), dx, dx + (size_t)K * Ne);
+  t.insert(t.end(), hs, hs + Ne);
+  if (h->lim) {
+    cudaFree(h->lim);
+    h->lim = nullptr;
+  }
+  return upload(&h->lim, t);
+}
+
+extern "C" int dgfs_dg_limit(dgfs_dg_handle h, void* u, int32_t dtype,
+                             void* stream) {
+  if (!h || !u) return fail(DGFS_ERR_INVALID, "null argument");
+  if (!h->lim) return fail(DGFS_ERR_INVALID, "limiter tables not set");
+  if (dtype != DGFS_F32 && dtype != DGFS_F64)
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  const int K = h->base.K, Ne = h->base.Ne;
+  DgLimitArgs a{};
+  a.u = u; a.f_double = dtype == DGFS_F64; a.K = K; a.Ne = Ne; a.Nv = h->base.Nv;
+  a.wavg = h->lim; a.wdr = h->lim + K; a.dx = h->lim + 2 * K;
+  a.h = h->lim + 2 * K + (size_t)K * Ne; a.invjac = h->invjac; a.tol = 1e-6;
+  dg_limit_kernel<<<(a.Nv + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
 // Penalty-model moments: NA = 5 (BGK), 11 (ES-BGK) or 14 (Shakov) per
 // point, in chunks of the handle's partial-sum capacity.
 static int penalty_moments_n(dgfs_dg_s* h, const void* f, int32_t dtype,

@@ -48,6 +48,25 @@ class DGOperator:
         if not np.array_equal(basis.invMassOp, np.eye(K)):
             raise NotImplementedError('non-identity inverse mass operator')
 
+    def set_limiter(self, basis, invjac, xsol):
+        """Tables of the linear slope limiter (abstd.py:403-415): row 0 of the
+        basis' cell-average and differentiated linear-projection operators,
+        the node offsets from each element centre and the element lengths,
+        formed as limiters.mako forms them (h = 2/invjac, x0 = x_0 + h/2)."""
+        inv = np.ravel(invjac).astype(np.float64)
+        hs = (1. / inv) * 2
+        xs = np.asarray(xsol, dtype=np.float64)
+        dx = np.ascontiguousarray(xs - (xs[0:1, :] + hs[None, :] / 2))
+        tabs = [np.ascontiguousarray(basis.cellAvgOp[0], dtype=np.float64),
+                np.ascontiguousarray(basis.drLinOp[0], dtype=np.float64),
+                dx, np.ascontiguousarray(hs)]
+        nat.check(nat.lib().dgfs_dg_set_limiter(self._h, *[_dp(t) for t in tabs]))
+
+    def limit(self, u, stream=None):
+        """Apply the linear slope limiter to u (K, Ne, N^3) in place."""
+        nat.check(nat.lib().dgfs_dg_limit(self._h, ctypes.c_void_p(u.data_ptr()),
+                                          _DT[u.dtype], _stream_ptr(stream)))
+
     def advect(self, u, ux, stream=None):
         nat.check(nat.lib().dgfs_dg_advect(
             self._h, ctypes.c_void_p(u.data_ptr()),

@@ -224,6 +224,16 @@ int dgfs_dg_moments(dgfs_dg_handle h, const void* coeff, int32_t dtype,
 int dgfs_dg_residual(dgfs_dg_handle h, const void* x, const void* y, int64_t n,
                      int32_t dtype, double* out2, void* stream);
 
+/* Linear slope limiter of dgfsABstd1D ([time-integrator] limiter = 1;
+ * abstd.py:403-415, astd/kernels/limiters.mako:17-76), applied in place to a
+ * (K, Ne, N^3) solution.  Tables: wavg[K] and wdr[K] are row 0 of the basis'
+ * cell-average operator and of its differentiated linear projection
+ * (basis.py:289-301), dx[K][Ne] the node positions minus the element centre,
+ * hs[Ne] the element lengths. */
+int dgfs_dg_set_limiter(dgfs_dg_handle h, const double* wavg, const double* wdr,
+                        const double* dx, const double* hs);
+int dgfs_dg_limit(dgfs_dg_handle h, void* u, int32_t dtype, void* stream);
+
 /*
  * Penalty (BGK-type) model of the penalised IMEX schemes, FP64 arithmetic
  * (dgfs1D/astd/scattering.py:44-284, astd/kernels/scattering/

@@ -64,6 +64,17 @@ class NodalBasis:
             V.append(Vm)
             sig.append(np.intersect1d(nnzU, nnzV))
         self.U, self.V, self.sigModes = U, V, sig
+        # slope-limiter operators (basis.py:289-301): projection onto the
+        # Legendre mode 0 (cell average) and modes 0-1 (linear part),
+        # differentiated with the nodal derivative
+        Vo = ortho_basis_at(K, z).T
+        invV = np.linalg.inv(Vo)
+        A0 = Vo.copy()
+        A0[:, 1:] = 0
+        A1 = Vo.copy()
+        A1[:, 2:] = 0
+        self.cellAvgOp = filter_tol(A0 @ invV)
+        self.drLinOp = filter_tol(D.T @ (A1 @ invV))
         # the operators as the kernels apply them (C = A . B, filtered)
         self.bwdFaceOp = filter_tol(self.Bqf.T)      # (Nqf, K)
         self.derivOp = filter_tol(D.T)               # (K, K): ux = D^T u
@@ -340,3 +351,36 @@ def bi_integrate(kind, rhs, t, dt, us, compat=False):
                 us[p][...] = r0[p]
     else:
         raise ValueError(kind)
+
+
+def _minmod(a, b, c):
+    """minmod of limiters.mako:11-15: the smallest magnitude when the three
+    signs agree (and none is zero), else 0."""
+    sa, sb, sc = np.sign(a), np.sign(b), np.sign(c)
+    m = np.trunc((sa + sb + sc) / 3.)
+    return np.where(np.abs(m) == 1,
+                    m * np.minimum(np.minimum(np.abs(a), np.abs(b)), np.abs(c)),
+                    0.)
+
+
+def limit_linear(basis, invjac, xsol, u, tol=1e-6):
+    """The linear slope limiter applied after every step of dgfsABstd1D with
+    ``[time-integrator] limiter = 1`` (abstd.py:403-415, limitLin of
+    astd/kernels/limiters.mako:17-76): in every interior element whose end
+    values differ from the minmod-limited linear reconstruction by more than
+    tol, the solution becomes the cell average plus the minmod of its linear
+    slope and the two one-sided average differences (divided by h)."""
+    K, Ne = u.shape[0], u.shape[1]
+    uavg = np.einsum('kj,jev->kev', basis.cellAvgOp, u)
+    ulx = np.einsum('kj,jev->kev', basis.drLinOp, u) * np.asarray(invjac).reshape(1, Ne, 1)
+    out = u.copy()
+    for e in range(1, Ne - 1):
+        h = (1. / np.asarray(invjac).ravel()[e]) * 2
+        x0 = xsol[0, e] + h / 2
+        a, aR, aL = uavg[0, e], uavg[0, min(e + 1, Ne - 1)], uavg[0, max(e - 1, 0)]
+        lim = (np.abs(a - _minmod(a - u[0, e], aR - a, a - aL) - u[0, e])
+               + np.abs(a + _minmod(u[K - 1, e] - a, aR - a, a - aL) - u[K - 1, e])) > tol
+        slope = _minmod(ulx[0, e], (aR - a) / h, (a - aL) / h)
+        for k in range(K):
+            out[k, e] = np.where(lim, a + (xsol[k, e] - x0) * slope, u[k, e])
+    return out

@@ -43,6 +43,11 @@ typedef struct { double x, y; } cufftDoubleComplex;
 typedef struct { float x, y; } cufftComplex;
 using std::sin; using std::cos; using std::pow; using std::sqrt; using std::fabs;
 using std::exp;
+// CUDA's overloaded min/max for double and int operands
+static inline double min(double a, double b) { return a < b ? a : b; }
+static inline double max(double a, double b) { return a > b ? a : b; }
+static inline int min(int a, int b) { return a < b ? a : b; }
+static inline int max(int a, int b) { return a > b ? a : b; }
 '''
 
 

@@ -5,6 +5,7 @@ default /root/reference)::
 
     python tests/golden/make_golden.py
     python tests/golden/make_golden.py penalty-models   # only the ES-BGK/Shakov files
+    python tests/golden/make_golden.py limiter          # only the slope-limiter file
 
 What runs from the reference:
   * its pure-Python setup code, imported directly with stand-ins for the
@@ -677,6 +678,51 @@ def golden_penalty_model(name, nalph, Nv=8, npts=6, omega=0.81, prefac=3.7,
     return out
 
 
+def golden_limiter(R, K=3, Ne=8, Nv=4):
+    """The linear slope limiter of dgfsABstd1D (``[time-integrator] limiter =
+    1``): the reference basis' cell-average and linear-derivative operators
+    (basis.py:289-301, captured by letting get_mm_kernel return its matrix)
+    and its limitLin kernel (astd/kernels/limiters.mako:17-76) on a seeded
+    step profile."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    ini = STD_INI.format(basis='nodal-sem-gll', Nv=Nv, Nrho=2, M=6, dev=5.0)
+    ini = ini.replace('Ne = 4', 'Ne = %d' % Ne).replace('K = 3', 'K = %d' % K)
+    cfg = R.Dictionary(ini)
+    old = R.basis.get_mm_kernel
+    R.basis.get_mm_kernel = lambda m, *a, **k: np.array(m, dtype=float)
+    try:
+        b = R.basis.NodalSemGLL(cfg)
+    finally:
+        R.basis.get_mm_kernel = old
+    # the gimmik kernels drop entries below 1e-15 (util.py:16-26)
+    import dgfs1D.util as rutil
+    Aavg = rutil.filter_tol(b.computeCellAvgKern.copy())
+    Adr = rutil.filter_tol(b.extractDrLinKern.copy())
+    xlo, xhi = 0.0, 1.0   # nondimensional mesh (xhi - xlo = H0)
+    x = np.linspace(xlo, xhi, Ne + 1)
+    jac = 0.5 * np.diff(x)
+    invjac = (1.0 / jac).reshape(Ne, 1)
+    xsol = np.array([0.5 * (x[j] + x[j + 1]) + jac[j] * b.z for j in range(Ne)]).T
+    vsize = Nv ** 3
+    rng = np.random.default_rng(SEED + 29)
+    prof = 1.0 + 0.5 * np.tanh((xsol - 0.5) / 0.05)
+    amp = rng.uniform(0.5, 1.5, vsize)
+    u = (prof[:, :, None] * amp[None, None, :]
+         * (1 + 0.05 * rng.uniform(-1, 1, (K, Ne, vsize)))).ravel()
+    U = u.reshape(K, Ne, vsize)
+    uavg = np.einsum('kj,jev->kev', Aavg, U).ravel()
+    ulx = (np.einsum('kj,jev->kev', Adr, U) * invjac[None, :, 0, None]).ravel()
+    src = render_template('dgfs1D/astd/kernels/limiters.mako', K=K, Ne=Ne,
+                          vsize=vsize, nalph=5, dtype='double', invjac=invjac,
+                          xsol=xsol, Dr=b.derivMat)
+    Km = RefModule(src, tag='limiters')
+    ulim = np.zeros(K * Ne * vsize)
+    Km.launch('limitLin', grid_for(vsize, 128), 128, u, ulx, uavg, ulim)
+    return dict(K=K, Ne=Ne, Nv=Nv, z=b.z, Aavg=Aavg, Adr=Adr,
+                derivMat=b.derivMat, invjac=invjac.ravel(), xsol=xsol, u=u,
+                uavg=uavg, ulx=ulx, ulim=ulim)
+
+
 def golden_setup(R):
     """Velocity meshes, rules and DG bases from the reference setup code."""
     out = {}
@@ -733,9 +779,15 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'penalty_N8.npz'),
                         **golden_penalty(R))
     penalty_models()
+    np.savez_compressed(os.path.join(HERE, 'limiter_N4.npz'), **golden_limiter(R))
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith('.npz'):
             print(fn, os.path.getsize(os.path.join(HERE, fn)), 'bytes')
+
+
+def limiter():
+    R = _import_reference()
+    np.savez_compressed(os.path.join(HERE, 'limiter_N4.npz'), **golden_limiter(R))
 
 
 def penalty_models():
@@ -749,5 +801,7 @@ if __name__ == '__main__':
     import sys
     if sys.argv[1:] == ['penalty-models']:
         penalty_models()
+    elif sys.argv[1:] == ['limiter']:
+        limiter()
     else:
         main()
