@@ -282,3 +282,80 @@ ux = {u2!r}
 uy = 0
 uz = 0
 """
+
+
+def sod_astd_ini(Ne=8, K=3, Nv=32, Nrho=6, M=6, dev=7.0, dt=1e-3, nsteps=10,
+                 scheme='imex-lm-bdf1', penalty='boltz-shakov-direct-gll',
+                 limiter=1, sphere='auto'):
+    """Sod shock tube of nitrogen-like gas on [-5, 5] (mean free paths) for
+    dgfsABstd1D: the set-up of the reference's abstd sod example (the keys
+    and physical values it uses: inlet walls at the two states, VHS
+    omega = 0.77 Boltzmann operator, Shakov penalty, IMEX-LM BDF1, slope
+    limiter), at a chosen resolution."""
+    T0, rho0, m0 = 278.746, 125e-9, 28.96278e-3
+    return f"""
+[config]
+precision = double
+[mesh]
+xlo = -5
+xhi = 5
+Ne = {Ne}
+H0 = 1
+[basis]
+kind = nodal-sem-gll
+K = {K}
+Nq = {K}
+Nqr = 16
+[non-dim]
+T0 = {T0}
+rho0 = {rho0}
+molarMass0 = {m0}
+[velocity-mesh]
+Nv = {Nv}
+Nrho = {Nrho}
+dev = {dev}
+cmax = 0
+Tmax = 348.4
+[spherical-design-rule]
+ssrule = womersley
+M = {M}
+sphere = {sphere}
+[penalized-scattering-model]
+type = {penalty}
+omega = 0.81
+muRef = 2.117e-5
+Tref = 273
+[scattering-model]
+type = vhs-gll
+omega = 0.77
+muRef = 1.7175337355197123e-05
+dRef = 4.19e-10
+Tref = 273
+[time-integrator]
+scheme = {scheme}
+controller = none
+tstart = 0.0
+tend = {dt * nsteps!r}
+dt = {dt!r}
+limiter = {limiter}
+[soln-ics]
+type = sod-shock-tube
+rho-left = 1000e-9
+T-left = 348.432
+rho-right = 125e-9
+T-right = 278.746
+[soln-bcs-xlo]
+type = dgfs-inlet
+T = 348.432
+ux = 0
+uy = 0
+uz = 0
+rho = 1000e-9
+[soln-bcs-xhi]
+type = dgfs-inlet
+T = 278.746
+ux = 0
+uy = 0
+uz = 0
+rho = 125e-9
+"""
