@@ -137,6 +137,10 @@ _SIGNATURES = [
     ('dgfs_dg_moments', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
       ctypes.c_void_p]),
+    ('dgfs_dg_moments_bi', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32,
+      ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_void_p]),
     ('dgfs_dg_residual', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
       ctypes.c_int32, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),

@@ -13,11 +13,14 @@ import torch
 
 from ..basis import get_basis
 from ..dg import DGOperator
+from ..distribution import (DGFSDistributionWriter, read_distribution,
+                            remaining_steps)
 from ..mesh import Mesh
 from ..plugins import subclass_where
 from ..std.bc import get_bc
 from ..std.initcond import get_initcond
 from ..std.moments import DGFSMomWriterStd
+from ..std.residual import DGFSResidualStd
 from ..std.scattering import DGFSScatteringModelStd
 from ..velocitymesh import DGFSVelocityMeshStd
 from .integrator import DGFSIntegratorAstd
@@ -25,7 +28,7 @@ from .scattering import DGFSScatteringModelAstd
 
 
 class DGFSABstd1D:
-    def __init__(self, cfg, device='cuda', boltzmann=None):
+    def __init__(self, cfg, device='cuda', boltzmann=None, restart=None):
         self.cfg = cfg
         self.device = torch.device(device)
         self.dtype = torch.float64
@@ -64,6 +67,10 @@ class DGFSABstd1D:
         get_initcond(cfg, vm, 'soln-ics').apply_init_vals(usol, basis.Nq, Ne,
                                                           self.xsol)
         self.u = torch.tensor(usol, dtype=self.dtype, device=self.device)
+        if restart is not None:       # abstd.py:243-253
+            arrs, ti = read_distribution(restart, ['coeff'], K, Ne, Nv)
+            self.u.copy_(torch.from_numpy(arrs['coeff'].reshape(K, Ne, Nv)))
+            self.nsteps = remaining_steps(ti, tf, self.dt)
         self.t = ti
         self.nacptsteps = 0
         # the Boltzmann operator may be replaced (e.g. by a surrogate)
@@ -73,7 +80,11 @@ class DGFSABstd1D:
         self.odes = icls(self.explicit, self.psm, (K, Ne, Nv), self.dtype,
                          t=ti, dt=self.dt, f0=self.u, explicitQ=self.explicitQ,
                          device=self.device)
-        self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, self.xsol)
+        self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, self.xsol,
+                                        tcurr=self.t, coeff=self.u)
+        self.distribution = DGFSDistributionWriter(ti, (K, Ne, Nv), cfg)
+        self.residual = DGFSResidualStd(cfg, self.dg)
+        self.uprev = self.u.clone()
         # linear slope limiter after every step (abstd.py:459, 476)
         self.limiter = int(cfg.lookupordefault('time-integrator', 'limiter', 0))
         if self.limiter:
@@ -95,6 +106,11 @@ class DGFSABstd1D:
             self.dg.limit(self.u)
         self.t += self.dt
         self.nacptsteps += 1
+        # post-processing of abstd.py:480-486
+        self.residual(self.t, self.nacptsteps, self.u, self.uprev)
+        self.moments(self.dt, self.t, self.u)
+        self.distribution(self.dt, self.t, self.u)
+        self.uprev.copy_(self.u)
 
     def run(self, nsteps=None):
         for _ in range(self.nsteps if nsteps is None else nsteps):

@@ -11,17 +11,20 @@ import torch
 
 from ..basis import get_basis
 from ..dg import DGOperator
+from ..distribution import (DGFSDistributionWriter, read_distribution,
+                            remaining_steps)
 from ..mesh import Mesh
 from ..plugins import subclass_where
 from ..velocitymesh import DGFSVelocityMeshBi
 from .bc import get_bc
 from .initcond import get_initcond
 from .integrator import DGFSIntegratorBi
+from .moments import DGFSMomWriterBi, DGFSResidualBi
 from .scattering import DGFSScatteringModelBi
 
 
 class DGFSBi1D:
-    def __init__(self, cfg, device='cuda'):
+    def __init__(self, cfg, device='cuda', restart=None):
         self.cfg = cfg
         self.device = torch.device(device)
         self.dtype = torch.float64 if cfg.dtype == np.float64 else torch.float32
@@ -60,11 +63,24 @@ class DGFSBi1D:
             usol = np.empty((basis.Nq, Ne, Nv))
             ic.apply_init_vals(p, usol, basis.Nq, Ne, self.xsol)
             self.us.append(torch.tensor(usol, dtype=self.dtype, device=self.device))
+        if restart is not None:       # bi.py:223-236
+            names = ['coeff%d' % p for p in range(ns)]
+            arrs, ti = read_distribution(restart, names, K, Ne, Nv)
+            for u, n in zip(self.us, names):
+                u.copy_(torch.from_numpy(arrs[n].reshape(K, Ne, Nv)))
+            self.nsteps = remaining_steps(ti, tf, self.dt)
         icls = subclass_where(DGFSIntegratorBi,
                               intg_kind=cfg.lookup('time-integrator', 'scheme'))
         self.odes = icls(self.rhs, (K, Ne, Nv), self.dtype, ns,
                          device=self.device, cfg=cfg)
         self.t = ti
+        self.nacptsteps = 0
+        self.uprevs = [u.clone() for u in self.us]
+        self.moments = DGFSMomWriterBi(cfg, vm, self.dgs[0], basis, self.xsol,
+                                       tcurr=ti, coeffs=self.us)
+        self.residual = DGFSResidualBi(cfg, self.dgs)
+        self.distribution = DGFSDistributionWriter(ti, (K, Ne, Nv), cfg,
+                                                   nspcs=ns)
 
     def rhs(self, p, t, us, out):
         self.dgs[p].advect(us[p], out)
@@ -72,8 +88,21 @@ class DGFSBi1D:
             self.sm.fs_batch(p, q, us[p], us[q], out, self.src, self.dst)
 
     def step(self):
+        """One step and the post-processing of bi.py:360-381: residual,
+        moments, then the copy of the solution for the next residual."""
         self.odes.integrate(self.t, self.dt, self.us)
         self.t += self.dt
+        self.nacptsteps += 1
+        self.residual(self.t, self.nacptsteps, self.uprevs, self.us)
+        self.moments(self.dt, self.t, self.us)
+        self.distribution(self.dt, self.t, self.us)
+        for a, b in zip(self.uprevs, self.us):
+            a.copy_(b)
+
+    def bulk_moments(self):
+        """(Nqr, Ne, 7 nspcs) dimensional mixture moments of the current
+        solution (rho, U:x, U:y, T, Q:x, p, nden per species)."""
+        return self.moments.compute(self.us)
 
     def run(self, nsteps=None):
         for _ in range(self.nsteps if nsteps is None else nsteps):

@@ -348,6 +348,133 @@ __global__ void __launch_bounds__(256) std_moments_kernel(MomentArgs a) {
   }
 }
 
+// Moments of a multi-species solution (dgfs1D/bi/moments.py:11-113), FP64,
+// nondimensional, [Nqr][Ne][nspcs][5] = rho, ux, uy, T, qx per species.
+// Species temperatures use the species' own velocity, heat fluxes the
+// mass-weighted mixture velocity; u_z is taken as zero in both, as there.
+// A species whose density summed over all points is below 1e-10 keeps its
+// density, gets zero velocity and temperature and is left out of the
+// mixture velocity (bi/moments.py:43-45).  Two launches: pass 1 per (r, e,
+// species) writes rho, ux, uy; pass 2 per (r, e) reads every point's
+// densities for the global test, then writes T and qx.
+constexpr int kMaxSpecies = 4;
+constexpr double kMinSpeciesDensity = 1e-10;
+
+struct BiMomentArgs {
+  const void* coeff[kMaxSpecies];   // (K, Ne, Nv) per species
+  double mass[kMaxSpecies];         // nondimensional molecular masses
+  int f_double, nspcs;
+  int K, Ne, Nv, N, Nqr;
+  const double* im;                 // [K][Nqr]
+  const double* c0;                 // [N]
+  double cw;
+  double* out;                      // [Nqr][Ne][nspcs][5]
+};
+
+__device__ __forceinline__ double bi_sol(const BiMomentArgs& a, int p, int r,
+                                         int e, int v) {
+  double s = 0;
+  for (int k = 0; k < a.K; ++k)
+    s += a.im[k * a.Nqr + r] *
+         ld(a.coeff[p], a.f_double, ((size_t)k * a.Ne + e) * a.Nv + v);
+  return s;
+}
+
+// Tree sum of n per-thread values over a 256-thread block; result in red[i][0].
+__device__ __forceinline__ void block_sum256(double (*red)[256], int n) {
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int i = 0; i < n; ++i) red[i][threadIdx.x] += red[i][threadIdx.x + s];
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) bi_moments_pass1_kernel(BiMomentArgs a) {
+  const int r = blockIdx.x, e = blockIdx.y, p = blockIdx.z, t = threadIdx.x;
+  __shared__ double red[3][256];
+  const int NN = a.N * a.N;
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int v = t; v < a.Nv; v += 256) {
+    const double f = bi_sol(a, p, r, e, v);
+    s0 += f;
+    s1 += f * a.c0[v / NN];
+    s2 += f * a.c0[(v / a.N) % a.N];
+  }
+  red[0][t] = s0; red[1][t] = s1; red[2][t] = s2;
+  block_sum256(red, 3);
+  if (t == 0) {
+    const double mcw = a.mass[p] * a.cw;
+    const double rho = red[0][0] * mcw;
+    double* o = a.out + (((size_t)r * a.Ne + e) * a.nspcs + p) * 5;
+    o[0] = rho;
+    o[1] = red[1][0] * mcw / rho;
+    o[2] = red[2][0] * mcw / rho;
+    o[3] = 0;
+    o[4] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(256) bi_moments_pass2_kernel(BiMomentArgs a) {
+  const int r = blockIdx.x, e = blockIdx.y, t = threadIdx.x;
+  __shared__ double red[2 * kMaxSpecies][256];
+  __shared__ int keep[kMaxSpecies];
+  __shared__ double ut[2];
+  const int npts = a.Nqr * a.Ne, ns = a.nspcs;
+  // global densities per species (each block sums in the same order)
+  for (int p = 0; p < ns; ++p) {
+    double s = 0;
+    for (int i = t; i < npts; i += 256) s += a.out[((size_t)i * ns + p) * 5];
+    red[p][t] = s;
+  }
+  block_sum256(red, ns);
+  if (t == 0) {
+    const double* o = a.out + ((size_t)r * a.Ne + e) * ns * 5;
+    double rho = 0, mx = 0, my = 0;
+    for (int p = 0; p < ns; ++p) {
+      keep[p] = !(red[p][0] < kMinSpeciesDensity);
+      if (keep[p]) {
+        rho += o[p * 5];
+        mx += o[p * 5] * o[p * 5 + 1];
+        my += o[p * 5] * o[p * 5 + 2];
+      }
+    }
+    ut[0] = mx / rho;
+    ut[1] = my / rho;
+  }
+  __syncthreads();
+  const int NN = a.N * a.N;
+  double* o = a.out + ((size_t)r * a.Ne + e) * ns * 5;
+  for (int p = 0; p < ns; ++p) {
+    const double ux = keep[p] ? o[p * 5 + 1] : 0.0, uy = keep[p] ? o[p * 5 + 2] : 0.0;
+    double sT = 0, sq = 0;
+    for (int v = t; v < a.Nv; v += 256) {
+      const double f = bi_sol(a, p, r, e, v);
+      const double cx = a.c0[v / NN], cy = a.c0[(v / a.N) % a.N], cz = a.c0[v % a.N];
+      const double px = cx - ux, py = cy - uy;
+      sT += f * (px * px + py * py + cz * cz);
+      const double qx = cx - ut[0], qy = cy - ut[1];
+      sq += f * (qx * qx + qy * qy + cz * cz) * qx;
+    }
+    red[2 * p][t] = sT;
+    red[2 * p + 1][t] = sq;
+  }
+  block_sum256(red, 2 * ns);
+  if (t == 0) {
+    for (int p = 0; p < ns; ++p) {
+      const double m = a.mass[p], mcw = m * a.cw;
+      if (keep[p]) {
+        o[p * 5 + 3] = red[2 * p][0] * (2.0 / 3.0 * mcw * m) / o[p * 5];
+      } else {
+        o[p * 5 + 1] = 0;
+        o[p * 5 + 2] = 0;
+        o[p * 5 + 3] = 0;
+      }
+      o[p * 5 + 4] = m * red[2 * p + 1][0] * mcw;
+    }
+  }
+}
+
 // sum (x - y)^2 and sum y^2 in FP64 (residual of std/residual.py:15-29)
 __global__ void __launch_bounds__(512) residual_kernel(const void* x,
                                                        const void* y, int dbl,

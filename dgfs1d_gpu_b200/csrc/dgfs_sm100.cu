@@ -1067,6 +1067,32 @@ extern "C" int dgfs_dg_moments(dgfs_dg_handle h, const void* coeff,
   return DGFS_OK;
 }
 
+extern "C" int dgfs_dg_moments_bi(dgfs_dg_handle h, const void* const* coeffs,
+                                  int32_t nspcs, const double* masses,
+                                  int32_t dtype, double* out, void* stream) {
+  if (!h || !coeffs || !masses || !out) return fail(DGFS_ERR_INVALID, "null argument");
+  if (nspcs < 1 || nspcs > kMaxSpecies)
+    return fail(DGFS_ERR_INVALID, "need 1 <= nspcs <= 4");
+  if (dtype != DGFS_F32 && dtype != DGFS_F64)
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  BiMomentArgs m{};
+  for (int p = 0; p < nspcs; ++p) {
+    if (!coeffs[p]) return fail(DGFS_ERR_INVALID, "null species solution");
+    if (!(masses[p] > 0)) return fail(DGFS_ERR_INVALID, "species mass must be > 0");
+    m.coeff[p] = coeffs[p];
+    m.mass[p] = masses[p];
+  }
+  m.f_double = dtype == DGFS_F64; m.nspcs = nspcs;
+  m.K = h->base.K; m.Ne = h->base.Ne; m.Nv = h->base.Nv; m.N = h->base.N;
+  m.Nqr = h->Nqr; m.im = h->im; m.c0 = h->c0; m.cw = h->cw; m.out = out;
+  auto st = static_cast<cudaStream_t>(stream);
+  bi_moments_pass1_kernel<<<dim3(h->Nqr, h->base.Ne, nspcs), 256, 0, st>>>(m);
+  DGFS_CUDA(cudaGetLastError());
+  bi_moments_pass2_kernel<<<dim3(h->Nqr, h->base.Ne), 256, 0, st>>>(m);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
 extern "C" int dgfs_axnpby(void* x0, int64_t n, int32_t dtype, double a0,
                            int32_t nterms, const void* const* xs,
                            const double* as, void* stream) {

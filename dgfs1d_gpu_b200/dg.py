@@ -87,6 +87,20 @@ class DGOperator:
             ctypes.c_void_p(out.data_ptr()), _stream_ptr(stream)))
         return out
 
+    def moments_bi(self, coeffs, masses, out=None, stream=None):
+        """(Nqr, Ne, nspcs, 5) FP64 nondimensional mixture moments rho, Ux,
+        Uy, T, Qx of the species solutions ``coeffs`` (device tensor)."""
+        ns = len(coeffs)
+        if out is None:
+            out = torch.empty((self.Nqr, self.Ne, ns, 5), dtype=torch.float64,
+                              device=coeffs[0].device)
+        ptrs = (ctypes.c_void_p * ns)(*[c.data_ptr() for c in coeffs])
+        ms = (ctypes.c_double * ns)(*[float(m) for m in masses])
+        nat.check(nat.lib().dgfs_dg_moments_bi(
+            self._h, ptrs, ns, ms, _DT[coeffs[0].dtype],
+            ctypes.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+        return out
+
     def residual(self, x, y, stream=None):
         out = (ctypes.c_double * 2)()
         nat.check(nat.lib().dgfs_dg_residual(

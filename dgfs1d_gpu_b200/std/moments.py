@@ -23,7 +23,8 @@ def dimensional(nd, vm):
 
 
 class DGFSMomWriterStd:
-    def __init__(self, cfg, vm, dg, basis, xcoeff, sect='dgfsmomwriter'):
+    def __init__(self, cfg, vm, dg, basis, xcoeff, tcurr=None, coeff=None,
+                 sect='dgfsmomwriter'):
         self.cfg, self.vm, self.dg = cfg, vm, dg
         self.enabled = cfg.has_section(sect)
         if self.enabled:
@@ -36,11 +37,15 @@ class DGFSMomWriterStd:
         Nqr = im.shape[1]
         self.xsol = (im.T @ xcoeff.reshape(basis.K, -1)).reshape(Nqr, -1) \
             * vm.H0()
-        self.tout_next = None
+        self.tout_next = tcurr
+        if tcurr is not None and coeff is not None:
+            self(1e-10, tcurr, coeff)       # the initial state (moments.py:191)
 
     def compute(self, coeff):
         """(Nqr, Ne, 10) dimensional moments (host numpy)."""
         nd = self.dg.moments(coeff).cpu().numpy()
+        if np.sum(nd[..., 0]) < 1e-10:      # moments.py:35-37 writes zeros
+            return np.zeros_like(nd)
         return dimensional(nd, self.vm)
 
     def __call__(self, dt, tcurr, coeff):

@@ -14,6 +14,8 @@ import torch
 
 from ..basis import get_basis
 from ..dg import DGOperator
+from ..distribution import (DGFSDistributionWriter, read_distribution,
+                            remaining_steps)
 from ..mesh import Mesh
 from ..plugins import subclass_where
 from ..velocitymesh import DGFSVelocityMeshStd
@@ -21,11 +23,12 @@ from .bc import get_bc
 from .initcond import get_initcond
 from .integrator import DGFSIntegratorStd
 from .moments import DGFSMomWriterStd
+from .residual import DGFSResidualStd
 from .scattering import DGFSScatteringModelStd
 
 
 class DGFSStd1D:
-    def __init__(self, cfg, device='cuda'):
+    def __init__(self, cfg, device='cuda', restart=None):
         self.cfg = cfg
         self.device = torch.device(device)
         self.dtype = torch.float64 if cfg.dtype == np.float64 else torch.float32
@@ -64,6 +67,10 @@ class DGFSStd1D:
         ic = get_initcond(cfg, vm, 'soln-ics')
         ic.apply_init_vals(usol, basis.Nq, Ne, self.xsol)
         self.u = torch.tensor(usol, dtype=self.dtype, device=self.device)
+        if restart is not None:       # std.py:234-244
+            arrs, ti = read_distribution(restart, ['coeff'], K, Ne, Nv)
+            self.u.copy_(torch.from_numpy(arrs['coeff'].reshape(K, Ne, Nv)))
+            self.nsteps = remaining_steps(ti, tf, self.dt)
         self.uprev = self.u.clone()
         scheme = cfg.lookup('time-integrator', 'scheme')
         icls = subclass_where(DGFSIntegratorStd, intg_kind=scheme)
@@ -71,9 +78,25 @@ class DGFSStd1D:
         self.t = ti
         self.nacptsteps = 0
         xcoeff = self.xsol  # nodal: forward transform is the identity
-        self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, xcoeff)
-        self.res_nsteps = cfg.lookupordefault('dgfsresidual', 'nsteps', -1)
-        self.residuals = []
+        self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, xcoeff,
+                                        tcurr=self.t, coeff=self.u)
+        self.distribution = DGFSDistributionWriter(ti, (K, Ne, Nv), cfg)
+        self.residual = DGFSResidualStd(cfg, self.dg)
+        # linear slope limiter after every step (std.py:369-400)
+        self.limiter = int(cfg.lookupordefault('time-integrator', 'limiter', 0))
+        if self.limiter:
+            self.dg.set_limiter(basis, mesh.invjac, self.xsol)
+
+    @property
+    def residuals(self):
+        """[(t, residual)] recorded at step 1 and every [dgfsresidual]
+        nsteps."""
+        return self.residual.history
+
+    def _advance(self):
+        self.odes.integrate(self.t, self.dt, self.u)
+        if self.limiter:
+            self.dg.limit(self.u)
 
     def rhs(self, t, u_in, u_out):
         self.dg.advect(u_in, u_out)
@@ -85,7 +108,7 @@ class DGFSStd1D:
         graph; later calls of ``step`` replay it.  A warm-up step runs first
         and is undone, so the solution is unchanged."""
         u0 = self.u.clone()
-        self.odes.integrate(self.t, self.dt, self.u)
+        self._advance()
         torch.cuda.synchronize()
         self.u.copy_(u0)
         g = torch.cuda.CUDAGraph()
@@ -93,7 +116,7 @@ class DGFSStd1D:
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
             with torch.cuda.graph(g, stream=s):
-                self.odes.integrate(self.t, self.dt, self.u)
+                self._advance()
         torch.cuda.current_stream().wait_stream(s)
         torch.cuda.synchronize()
         self._graph = g
@@ -103,14 +126,12 @@ class DGFSStd1D:
         if getattr(self, '_graph', None) is not None:
             self._graph.replay()
         else:
-            self.odes.integrate(self.t, self.dt, self.u)
+            self._advance()
         self.t += self.dt
         self.nacptsteps += 1
-        n = self.nacptsteps
-        if self.res_nsteps > 0 and (n % self.res_nsteps == 0 or n == 1):
-            a, b = self.dg.residual(self.u, self.uprev)
-            self.residuals.append((self.t, math.sqrt(a / b)))
+        self.residual(self.t, self.nacptsteps, self.u, self.uprev)
         self.moments(self.dt, self.t, self.u)
+        self.distribution(self.dt, self.t, self.u)
         self.uprev.copy_(self.u)
 
     def run(self, nsteps=None):

@@ -219,6 +219,18 @@ int dgfs_dg_wall_density(dgfs_dg_handle h, double* out2);
 int dgfs_dg_moments(dgfs_dg_handle h, const void* coeff, int32_t dtype,
                     double* out, void* stream);
 
+/* Moments of a mixture of nspcs <= 4 species sharing the grid of h
+ * (replaces DGFSMomWriterBi._compute_moments_1D, bi/moments.py:11-113,
+ * before its dimensional scaling): coeffs[p] is species p's solution
+ * (K, Ne, N^3), masses[p] its nondimensional mass (host array); out (device)
+ * receives out[((r*Ne + e)*nspcs + p)*5 + i] for i = rho, Ux, Uy, T, Qx.
+ * T uses the species velocity, Qx the mixture velocity; a species whose
+ * density summed over all points is below 1e-10 keeps rho, has zero U and T
+ * and is left out of the mixture velocity, as in the reference. */
+int dgfs_dg_moments_bi(dgfs_dg_handle h, const void* const* coeffs,
+                       int32_t nspcs, const double* masses, int32_t dtype,
+                       double* out, void* stream);
+
 /* Residual sums (|x-y|^2, |y|^2) in FP64 (std/residual.py:15-29); waits for
  * the stream and writes the two sums to host memory out2. */
 int dgfs_dg_residual(dgfs_dg_handle h, const void* x, const void* y, int64_t n,

@@ -255,6 +255,8 @@ def moments(basis, coeff, cv, cw, T0=1.0, rho0=1.0, u0=1.0, R0=8.3144598,
     mcw = cw
     out = np.zeros(soln.shape[:2] + (10,))
     out[:, :, 0] = np.einsum('...j->...', soln) * mcw
+    if np.sum(out[:, :, 0]) < 1e-10:      # :35-37 writes zeros
+        return np.zeros_like(out)
     out[:, :, 1] = np.einsum('rej,j->re', soln, cv[0]) * mcw / out[:, :, 0]
     out[:, :, 2] = np.einsum('rej,j->re', soln, cv[1]) * mcw / out[:, :, 0]
     Nqr = soln.shape[0]
@@ -273,6 +275,55 @@ def moments(basis, coeff, cv, cw, T0=1.0, rho0=1.0, u0=1.0, R0=8.3144598,
                                 0.5 * rho0 * u0 ** 3, 0.5 * rho0 * u0 ** 2,
                                 0.5 * rho0 * u0 ** 2, 0.5 * rho0 * u0 ** 2])
     out[:, :, 9] = (R0 / molarMass0) * out[:, :, 0] * out[:, :, 3]
+    return out
+
+
+def moments_bi(basis, coeffs, cv, cw, masses, T0=1.0, rho0=1.0, u0=1.0,
+               R0=8.3144598, NA=6.0221409e+23, molarMass0=1.0):
+    """Mixture moments of bi/moments.py:11-113 at the reconstruction points.
+
+    Returns (Nqr, Ne, 7 * nspcs): per species rho, Ux, Uy, T, Qx, p, nden,
+    dimensional.  T uses the species velocity, Qx the mixture velocity of
+    the species kept (u_z taken as zero in both); a species whose density
+    summed over all points is below 1e-10 keeps rho and has zero U and T
+    (:43-45).
+    """
+    ns = len(coeffs)
+    im = basis.interpMat
+    soln = [np.einsum('mr,mej->rej', im, c) for c in coeffs]
+    Nqr, Ne, Nv = soln[0].shape
+    out = np.zeros((Nqr, Ne, 7 * ns))
+    tot = np.zeros((Nqr, Ne, 3))
+
+    def pec(ux, uy):
+        cx = cv[0].reshape(1, 1, Nv) - ux.reshape(Nqr, Ne, 1)
+        cy = cv[1].reshape(1, 1, Nv) - uy.reshape(Nqr, Ne, 1)
+        cz = cv[2].reshape(1, 1, Nv) - np.zeros((Nqr, Ne, 1))
+        return cx, cx * cx + cy * cy + cz * cz
+
+    for p in range(ns):
+        m, o, f = masses[p], 7 * p, soln[p]
+        mcw = m * cw
+        out[:, :, o] = np.sum(f, axis=-1) * mcw
+        if np.sum(out[:, :, o]) < 1e-10:
+            continue
+        out[:, :, o + 1] = np.tensordot(f, cv[0], axes=(-1, 0)) * mcw / out[:, :, o]
+        out[:, :, o + 2] = np.tensordot(f, cv[1], axes=(-1, 0)) * mcw / out[:, :, o]
+        _, c2 = pec(out[:, :, o + 1], out[:, :, o + 2])
+        out[:, :, o + 3] = np.sum(f * c2, axis=-1) * (2. / 3. * mcw * m) / out[:, :, o]
+        tot[:, :, 0] += out[:, :, o]
+        tot[:, :, 1] += out[:, :, o] * out[:, :, o + 1]
+        tot[:, :, 2] += out[:, :, o] * out[:, :, o + 2]
+    tot[:, :, 1] /= tot[:, :, 0]
+    tot[:, :, 2] /= tot[:, :, 0]
+    cx, c2 = pec(tot[:, :, 1], tot[:, :, 2])
+    for p in range(ns):
+        m, o, f = masses[p], 7 * p, soln[p]
+        mcw = m * cw
+        out[:, :, o + 4] = m * np.sum(f * c2 * cx, axis=-1) * mcw
+        out[:, :, o:o + 5] *= np.array([rho0, u0, u0, T0, 0.5 * rho0 * u0 ** 3])
+        out[:, :, o + 5] = (m * R0 / molarMass0) * out[:, :, o] * out[:, :, o + 3]
+        out[:, :, o + 6] = (NA / m / molarMass0) * out[:, :, o]
     return out
 
 

@@ -6,6 +6,7 @@ default /root/reference)::
     python tests/golden/make_golden.py
     python tests/golden/make_golden.py penalty-models   # only the ES-BGK/Shakov files
     python tests/golden/make_golden.py limiter          # only the slope-limiter file
+    python tests/golden/make_golden.py moments          # only the moment-writer file
 
 What runs from the reference:
   * its pure-Python setup code, imported directly with stand-ins for the
@@ -723,6 +724,80 @@ def golden_limiter(R, K=3, Ne=8, Nv=4):
                 uavg=uavg, ulx=ulx, ulim=ulim)
 
 
+def golden_moments(R, Nv=8, Ne=4, K=3):
+    """Bulk moments of the reference's writers: DGFSMomWriterStd and
+    DGFSMomWriterBi ``_compute_moments_1D`` (std/moments.py:11-70,
+    bi/moments.py:11-113) on seeded drifting Maxwellians, including a mixture
+    whose second species is absent (the below-1e-10 branch)."""
+    import warnings
+    from dgfs1D.std.moments import DGFSMomWriterStd
+    from dgfs1D.bi.moments import DGFSMomWriterBi
+    rng = np.random.default_rng(SEED + 31)
+    out = {}
+
+    class _Dev:               # what .get() returns, as a GPUArray would
+        def __init__(self, a):
+            self.a = a
+
+        def get(self):
+            return self.a
+
+    def drift(cv, rho, ux, uy, T, mass=1.0):
+        c2 = ((cv[0] - ux) ** 2 + (cv[1] - uy) ** 2 + cv[2] ** 2)
+        return rho * (mass / (np.pi * T)) ** 1.5 * np.exp(-mass * c2 / T)
+
+    def field(cv, K, Ne, mass, rho, T):
+        f = np.empty((K, Ne, cv.shape[1]))
+        for k in range(K):
+            for e in range(Ne):
+                f[k, e] = drift(cv, rho * rng.uniform(0.8, 1.2),
+                                rng.uniform(-0.3, 0.3), rng.uniform(-0.3, 0.3),
+                                T * rng.uniform(0.8, 1.2), mass)
+        return f * (1 + 0.02 * rng.uniform(-1, 1, f.shape))
+
+    cfg = R.Dictionary(STD_INI.format(basis='nodal-sem-gll', Nv=Nv, Nrho=2,
+                                      M=6, dev=5.0).replace('Ne = 4', 'Ne = %d' % Ne))
+    old = R.basis.get_mm_kernel
+    R.basis.get_mm_kernel = lambda m, *a, **k: None
+    try:
+        b = R.basis.NodalSemGLL(cfg)
+    finally:
+        R.basis.get_mm_kernel = old
+    vm = R.vstd.DGFSVelocityMeshStd(cfg)
+    f = field(vm.cv(), K, Ne, 1.0, 1.0, 1.0)
+    w = object.__new__(DGFSMomWriterStd)
+    w.vm, w.im = vm, b.interpMat
+    w._bulksoln = np.zeros((b.interpMat.shape[1], Ne, 10))
+    w._compute_moments_1D(_Dev(f.ravel()))
+    out.update(std_f=f, std_mom=w._bulksoln.copy(), std_cw=vm.cw(),
+               std_cv=vm.cv(), std_T0=vm.T0(), std_rho0=vm.rho0(),
+               std_u0=vm.u0(), std_molarMass0=vm.molarMass0(),
+               interpMat=b.interpMat)
+    cfg = R.Dictionary(BI_INI.format(Nv=Nv, Nrho=2, M=6, Mpre=12, dev=5.0)
+                       .replace('Ne = 2', 'Ne = %d' % Ne))
+    vm = R.vbi.DGFSVelocityMeshBi(cfg)
+    ms = vm.masses()
+    for tag, absent in (('mix', False), ('absent', True)):
+        fs = [field(vm.cv(), K, Ne, ms[0], 0.5, 1.0),
+              field(vm.cv(), K, Ne, ms[1], 0.5, 1.2)]
+        if absent:
+            fs[1][:] = 0.0
+        w = object.__new__(DGFSMomWriterBi)
+        w.vm, w.im = vm, b.interpMat
+        Nqr = b.interpMat.shape[1]
+        w._bulksoln = np.zeros((Nqr, Ne, 7 * 2))
+        w._bulksolntot = np.zeros((Nqr, Ne, 4))
+        with warnings.catch_warnings():
+            warnings.simplefilter('ignore')
+            w._compute_moments_1D([_Dev(x.ravel()) for x in fs])
+        out['bi_%s_f0' % tag], out['bi_%s_f1' % tag] = fs
+        out['bi_%s_mom' % tag] = w._bulksoln.copy()
+    out.update(bi_cw=vm.cw(), bi_cv=vm.cv(), bi_masses=np.array(ms),
+               bi_T0=vm.T0(), bi_rho0=vm.rho0(), bi_u0=vm.u0(),
+               bi_molarMass0=vm.molarMass0(), bi_R0=vm.R0, bi_NA=vm.NA)
+    return out
+
+
 def golden_setup(R):
     """Velocity meshes, rules and DG bases from the reference setup code."""
     out = {}
@@ -780,6 +855,7 @@ def main():
                         **golden_penalty(R))
     penalty_models()
     np.savez_compressed(os.path.join(HERE, 'limiter_N4.npz'), **golden_limiter(R))
+    np.savez_compressed(os.path.join(HERE, 'moments_N8.npz'), **golden_moments(R))
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith('.npz'):
             print(fn, os.path.getsize(os.path.join(HERE, fn)), 'bytes')
@@ -788,6 +864,11 @@ def main():
 def limiter():
     R = _import_reference()
     np.savez_compressed(os.path.join(HERE, 'limiter_N4.npz'), **golden_limiter(R))
+
+
+def moments():
+    R = _import_reference()
+    np.savez_compressed(os.path.join(HERE, 'moments_N8.npz'), **golden_moments(R))
 
 
 def penalty_models():
@@ -803,5 +884,7 @@ if __name__ == '__main__':
         penalty_models()
     elif sys.argv[1:] == ['limiter']:
         limiter()
+    elif sys.argv[1:] == ['moments']:
+        moments()
     else:
         main()

@@ -1,0 +1,67 @@
+"""Checkpoint files of the distribution writer (CPU): the datasets and
+attributes of std/distribution.py and bi/distribution.py, the file-name
+pattern, and the K / Ne / Nv checks of a restart."""
+import numpy as np
+import pytest
+
+from dgfs1d_gpu_b200.config import Config
+from dgfs1d_gpu_b200.distribution import (DGFSDistributionWriter,
+                                          read_distribution, remaining_steps,
+                                          write_distribution)
+
+
+class _T:
+    """Stands in for a device tensor (the writer calls .detach().cpu())."""
+
+    def __init__(self, a):
+        self.a = a
+
+    def detach(self):
+        return self
+
+    def cpu(self):
+        return self
+
+    def numpy(self):
+        return self.a
+
+
+def test_round_trip_and_checks(tmp_path):
+    rng = np.random.default_rng(5)
+    a, b = rng.standard_normal(3 * 4 * 8), rng.standard_normal(3 * 4 * 8)
+    p = str(tmp_path / 'x.npz_rank=0')
+    write_distribution(p, {'coeff0': a, 'coeff1': b}, 0.125, 3, 4, 8)
+    got, t = read_distribution(p, ['coeff0', 'coeff1'], 3, 4, 8)
+    assert t == 0.125
+    assert np.array_equal(got['coeff0'], a) and np.array_equal(got['coeff1'], b)
+    for K, Ne, Nv, what in ((2, 4, 8, 'K'), (3, 5, 8, 'Ne'), (3, 4, 9, 'N')):
+        with pytest.raises(ValueError, match='Inconsistent distribution ' + what):
+            read_distribution(p, ['coeff0'], K, Ne, Nv)
+    with pytest.raises(KeyError):
+        read_distribution(p, ['coeff'], 3, 4, 8)
+
+
+def test_writer_schedule_and_names(tmp_path):
+    cfg = Config('[dgfsdistwriter]\nbasedir = %s\nbasename = d-{t:.3f}\n'
+                 'dt-out = 0.5\n' % tmp_path)
+    w = DGFSDistributionWriter(0.0, (3, 2, 8), cfg)
+    u = _T(np.arange(48.0))
+    assert w(0.25, 0.25, u) is None                 # not an output time
+    p = w(0.25, 0.5, u)
+    assert p.endswith('d-0.500.npz_rank=0')
+    got, t = read_distribution(p, ['coeff'], 3, 2, 8)
+    assert t == 0.5 and np.array_equal(got['coeff'], np.arange(48.0))
+    assert w(0.25, 0.75, u) is None and w(0.25, 1.0, u) is not None
+    wb = DGFSDistributionWriter(0.0, (3, 2, 8), cfg, nspcs=2)
+    p = wb(0.5, 0.5, [u, _T(2 * np.arange(48.0))])
+    got, _ = read_distribution(p, ['coeff0', 'coeff1'], 3, 2, 8)
+    assert np.array_equal(got['coeff1'], 2 * np.arange(48.0))
+    off = DGFSDistributionWriter(0.0, (3, 2, 8), Config('[x]\na = 1\n'))
+    assert off(0.5, 0.5, u) is None
+
+
+def test_remaining_steps():
+    assert remaining_steps(0.0, 1.0, 0.25) == 4
+    assert remaining_steps(0.5, 1.0, 0.25) == 2
+    assert remaining_steps(0.1 + 0.2, 0.3, 0.1) == 0
+    assert remaining_steps(1.0, 1.0, 0.1) == 0

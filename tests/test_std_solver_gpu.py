@@ -43,8 +43,9 @@ def test_rhs_matches_reference_kernel_golden(kind):
     assert _rel(out.cpu().numpy(), g['rhs_q']) < 1e-11
 
 
-def _oracle_run(s, nsteps, scheme):
-    """Integrate the same problem with the oracle (CPU)."""
+def _oracle_run(s, nsteps, scheme, limit=False):
+    """Integrate the same problem with the oracle (CPU); with ``limit`` the
+    slope limiter follows every step (std.py:400)."""
     vm = s.vm
     ovm = om.VelocityMeshStd(Nv=vm.Nv(), M=vm.M(), Nrho=vm.Nrho(), dev=vm.dev(),
                              rho0=vm.rho0(), full_sphere=vm.sphere_mode() == 'full')
@@ -67,6 +68,8 @@ def _oracle_run(s, nsteps, scheme):
     t = 0.0
     for _ in range(nsteps):
         odg.integrate(scheme, rhs, t, s.dt, u)
+        if limit:
+            u[...] = odg.limit_linear(b, invjac, s.xsol, u)
         t += s.dt
     return b, cv, cw, u
 
@@ -138,3 +141,91 @@ def test_normal_shock_inlet_lse_rk45_graph_steps():
     m = a.dg.moments(a.u).cpu().numpy()
     rho_l, rho_r = m[0, 0, 0], m[-1, -1, 0]
     assert abs(rho_l - 1.0) < 2e-2 and abs(rho_r - 1.714) < 3e-2, (rho_l, rho_r)
+
+
+def test_std_limiter_matches_oracle():
+    """dgfsStd1D with ``[time-integrator] limiter = 1``: every step followed
+    by the linear slope limiter (std.py:369-400), eager and graph-captured,
+    against the oracle."""
+    ini = couette_std_ini(Nv=8, Nrho=4, Ne=6, scheme='ssp-rk2', nsteps=3,
+                          noise=0.2)
+    ini = ini.replace('[time-integrator]\n', '[time-integrator]\nlimiter = 1\n', 1)
+    s = _solver(ini)
+    assert s.limiter == 1
+    u0 = s.u.clone()
+    b, cv, cw, uref = _oracle_run(s, 3, 'ssp-rk2', limit=True)
+    un = u0.cpu().numpy()
+    assert np.abs(odg.limit_linear(b, s.mesh.invjac, s.xsol, un) - un).max() > 0
+    s.u.copy_(u0)
+    s.run(3)
+    torch.cuda.synchronize()
+    assert _rel(s.u.cpu().numpy(), uref) < 1e-12
+    s2 = _solver(ini)
+    s2.capture_step()
+    s2.run(3)
+    torch.cuda.synchronize()
+    assert _rel(s2.u.cpu().numpy(), uref) < 1e-12
+
+
+def test_std_residual_is_the_reference_norm():
+    """[dgfsresidual] nsteps = 1: sqrt(|u^n - u^{n+1}|^2 / |u^{n+1}|^2), the
+    normalisation the std driver's call residual(t, n, u, u_prev) gives."""
+    ini = couette_std_ini(Nv=8, Nrho=4, nsteps=3) + '\n[dgfsresidual]\nnsteps = 1\n'
+    s = _solver(ini)
+    want = []
+    for _ in range(3):
+        prev = s.u.double().cpu().numpy().copy()
+        s.step()
+        cur = s.u.double().cpu().numpy()
+        want.append(np.linalg.norm(prev - cur) / np.linalg.norm(cur))
+    got = [r for _, r in s.residuals]
+    assert len(got) == 3
+    assert np.allclose(got, want, rtol=1e-12)
+
+
+@pytest.mark.parametrize('driver', ['std', 'astd', 'bi'])
+def test_restart_from_distribution_file(tmp_path, driver):
+    """[dgfsdistwriter] checkpoints (datasets coeff / coeff<p> with time, K,
+    Ne, Nv) and a restart from one continue the run as if uninterrupted;
+    a checkpoint of another grid is refused."""
+    from dgfs1d_gpu_b200 import build
+    build.build()
+    from dgfs1d_gpu_b200.configs import couette_astd_ini, couette_bi_ini
+    if driver == 'std':
+        from dgfs1d_gpu_b200.std.solver import DGFSStd1D as S
+        ini = couette_std_ini(Nv=8, Nrho=4, scheme='ssp-rk3', nsteps=4)
+        names = ['coeff']
+    elif driver == 'astd':
+        from dgfs1d_gpu_b200.astd.solver import DGFSABstd1D as S
+        ini = couette_astd_ini(scheme='bdf-111', penalty='bgk-direct-gll',
+                               Nv=8, Nrho=4, nsteps=4)
+        names = ['coeff']
+    else:
+        from dgfs1d_gpu_b200.bi.solver import DGFSBi1D as S
+        ini = couette_bi_ini(scheme='ssp-rk2', nsteps=4)
+        names = ['coeff0', 'coeff1']
+    dt = Config(ini).lookupfloat('time-integrator', 'dt')
+    ini_w = ini + ('\n[dgfsdistwriter]\nbasedir = %s\nbasename = dist-{t:.6f}\n'
+                   'dt-out = %.17g\n' % (tmp_path, 2 * dt))
+    full = S(Config(ini))
+    full.run(4)
+    a = S(Config(ini_w))
+    a.run(2)
+    files = sorted(p.name for p in tmp_path.iterdir())
+    assert len(files) == 1 and files[0].endswith('_rank=0'), files
+    from dgfs1d_gpu_b200.distribution import read_distribution
+    K, Ne = a.basis.K, a.mesh.Ne
+    Nv = a.vm.vsize()
+    arrs, t = read_distribution(str(tmp_path / files[0]), names, K, Ne, Nv)
+    assert abs(t - 2 * dt) < 1e-15 and sorted(arrs) == names
+    b = S(Config(ini), restart=str(tmp_path / files[0]))
+    assert abs(b.t - 2 * dt) < 1e-15 and b.nsteps == 2
+    b.run()
+    torch.cuda.synchronize()
+    ends = [full.u] if driver != 'bi' else full.us
+    got = [b.u] if driver != 'bi' else b.us
+    for x, y in zip(got, ends):
+        assert _rel(x.cpu().numpy(), y.cpu().numpy()) < 1e-14
+    with pytest.raises(ValueError, match='Inconsistent distribution'):
+        S(Config(ini.replace('Ne = %d' % Ne, 'Ne = %d' % (Ne + 1), 1)),
+          restart=str(tmp_path / files[0]))
