@@ -1,7 +1,8 @@
 """Penalised IMEX time integrators (``[time-integrator] scheme``).
 
 Keys and coefficients of dgfs1D/astd/integrator.py: ``bdf-111`` / ``bdf-222``
-(penalty model only, explicit DG advection; :281-400) and ``imex-lm-bdf1`` /
+(penalty model only, explicit DG advection; :281-400), ``boltz-ars-111``
+(explicit Boltzmann operator and penalty, :491-552) and ``imex-lm-bdf1`` /
 ``imex-lm-bdf2`` and the other ``imex-lm-*`` schemes (cn2, ad2, sg2, bdf3,
 ad3, tvb3, bdf4, tvb4, shu3, shu4; explicit L + Q - P, implicit P(f^{n+1});
 :623-907).  The
@@ -67,6 +68,31 @@ class Bdf111IntegratorAstd(DGFSIntegratorAstd):
         L0 = self._z()
         self._explicit(t, f, L0)
         LU0 = self._mom(L0)
+        U = self._zm()
+        _lin(U, [(1.0, U0), (dt, LU0)])
+        self._sm.relax(U, 1.0, dt)
+        rhs = self._z()
+        _lin(rhs, [(1.0, f), (dt, L0)])
+        self._sm.implicit(U, rhs, f, 1.0, dt)
+
+
+class BoltzARS111IntegratorAstd(DGFSIntegratorAstd):
+    """First-order ARS scheme of the penalised Boltzmann equation
+    (astd/integrator.py:491-552): the moments advance with the advection
+    only; f advances with the explicit L + Q(f) - P(f), P = nu (M(U^n) - f),
+    and the implicit penalty at the new moments."""
+    intg_kind = 'boltz-ars-111'
+
+    def integrate(self, t, dt, nacptsteps, f):
+        U0 = self._mom(f)
+        P0 = self._z()
+        self._sm.collide(t, U0, f, P0)
+        L0 = self._z()
+        self._explicit(t, f, L0)
+        LU0 = self._mom(L0)
+        if self._Q is not None:
+            self._Q(t, f, L0)             # accumulates Q(f)
+        axnpby(L0, 1.0, -1.0, P0)
         U = self._zm()
         _lin(U, [(1.0, U0), (dt, LU0)])
         self._sm.relax(U, 1.0, dt)

@@ -50,8 +50,8 @@ class DGFSABstd1D:
         x = mesh.xmesh
         self.xsol = np.array([0.5 * (x[j] + x[j + 1]) + mesh.jac[j] * basis.z
                               for j in range(Ne)]).T
-        bcl = get_bc(cfg, 'soln-bcs-xlo', x[0], -1., vm)
-        bcr = get_bc(cfg, 'soln-bcs-xhi', x[-1], 1., vm)
+        self.bcl = bcl = get_bc(cfg, 'soln-bcs-xlo', x[0], -1., vm)
+        self.bcr = bcr = get_bc(cfg, 'soln-bcs-xhi', x[-1], 1., vm)
         self.dg = DGOperator(basis, mesh.invjac, vm.c0(), vm.cw(),
                              [(bcl.type, bcl.f0, bcl.ux),
                               (bcr.type, bcr.f0, bcr.ux)])
@@ -91,6 +91,8 @@ class DGFSABstd1D:
             self.dg.set_limiter(basis, mesh.invjac, self.xsol)
 
     def explicit(self, t, u_in, u_out):
+        for side, bc in enumerate((self.bcl, self.bcr)):
+            bc.at_time(t, self.dg, side)
         self.dg.advect(u_in, u_out)
 
     def explicitQ(self, t, u_in, u_out):

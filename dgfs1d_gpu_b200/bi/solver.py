@@ -44,8 +44,8 @@ class DGFSBi1D:
         x = mesh.xmesh
         self.xsol = np.array([0.5 * (x[j] + x[j + 1]) + mesh.jac[j] * basis.z
                               for j in range(Ne)]).T
-        bcl = get_bc(cfg, 'soln-bcs-xlo', x[0], -1., vm)
-        bcr = get_bc(cfg, 'soln-bcs-xhi', x[-1], 1., vm)
+        self.bcl = bcl = get_bc(cfg, 'soln-bcs-xlo', x[0], -1., vm)
+        self.bcr = bcr = get_bc(cfg, 'soln-bcs-xhi', x[-1], 1., vm)
         self.dgs = [DGOperator(basis, mesh.invjac, vm.c0(), vm.cw(),
                                [(bcl.type, bcl.f0[p], bcl.ux),
                                 (bcr.type, bcr.f0[p], bcr.ux)])
@@ -83,6 +83,8 @@ class DGFSBi1D:
                                                    nspcs=ns)
 
     def rhs(self, p, t, us, out):
+        for side, bc in enumerate((self.bcl, self.bcr)):
+            bc.at_time(t, self.dgs[p], side, p)
         self.dgs[p].advect(us[p], out)
         for q in range(self.nspcs):
             self.sm.fs_batch(p, q, us[p], us[q], out, self.src, self.dst)

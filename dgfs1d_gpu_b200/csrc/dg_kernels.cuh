@@ -17,9 +17,11 @@ namespace dgfs {
 constexpr int kDgMaxK = 8;
 
 // boundary kinds
-constexpr int kBcCopy = 0;     // dgfs-periodic on one rank: ghost = interior
+constexpr int kBcCopy = 0;     // dgfs-periodic / dgfs-cyclic on one rank: ghost = interior
 constexpr int kBcWall = 1;     // dgfs-wall-diffuse
-constexpr int kBcInlet = 2;    // dgfs-inlet
+constexpr int kBcInlet = 2;    // dgfs-inlet, dgfs-inlet-nondim (incoming test (c_x - u_x) n)
+constexpr int kBcVanish = 3;   // dgfs-vanish
+constexpr int kBcWallExpr = 4; // dgfs-wall-expr-diffuse (wall state set per call)
 
 struct DgAdvectArgs {
   const void* u;            // (K, Ne, Nv) in
@@ -33,6 +35,7 @@ struct DgAdvectArgs {
   int bc[2];                // boundary kinds (left, right)
   double bc_ux[2];          // wall x-velocities
   double nl[2];             // outward normals (-1, +1)
+  double ws[2][5];          // kBcWallExpr: ux, uy, uz, T, mass of the wall
   double trL[kDgMaxK];      // left-face trace weights  (row 0 of Bqf^T)
   double trR[kDgMaxK];      // right-face trace weights (row Nqf-1 of Bqf^T)
   double D[kDgMaxK * kDgMaxK];  // derivOp (K x K): ux = D u
@@ -109,6 +112,17 @@ __global__ void __launch_bounds__(256) dg_limit_kernel(DgLimitArgs a) {
   }
 }
 
+// Unnormalised wall Maxwellian exp(-m |c - u_w|^2 / T_w) of a wall whose
+// state is set per call (dgfs-wall-expr-diffuse.mako, bi: with the mass m).
+__device__ __forceinline__ double wall_expr_maxwellian(const DgAdvectArgs& a,
+                                                      int side, int v) {
+  const int N = a.N;
+  const double* w = a.ws[side];
+  const double dx = a.c0[v / (N * N)] - w[0], dy = a.c0[(v / N) % N] - w[1],
+               dz = a.c0[v % N] - w[2];
+  return exp(-w[4] * (dx * dx + dy * dy + dz * dz) / w[3]);
+}
+
 // Wall densities n_w = -sum_{out} (c-u_w).n f cw / sum_{in} (c-u_w).n f0 cw
 // (updateBC of dgfs-wall-diffuse.mako with the two gpuarray.sum of
 // std/bc.py:63-76), in a deterministic order.
@@ -122,10 +136,12 @@ __global__ void __launch_bounds__(256) dg_wall_partial_kernel(DgAdvectArgs a,
   const int ch = blockIdx.x, side = blockIdx.y, t = threadIdx.x;
   __shared__ double rn[256], rd[256];
   double sn = 0, sd = 0;
-  if (a.bc[side] == kBcWall) {
+  const int kind = a.bc[side];
+  if (kind == kBcWall || kind == kBcWallExpr) {
     const int e = side == 0 ? 0 : a.Ne - 1;
     const double* tw = side == 0 ? a.trL : a.trR;
-    const double nl = a.nl[side], ux = a.bc_ux[side];
+    const double nl = a.nl[side];
+    const double ux = kind == kBcWall ? a.bc_ux[side] : a.ws[side][0];
     const int len = (a.Nv + kWallCh - 1) / kWallCh;
     const int v1 = min(a.Nv, (ch + 1) * len);
     for (int v = ch * len + t; v < v1; v += 256) {
@@ -134,7 +150,7 @@ __global__ void __launch_bounds__(256) dg_wall_partial_kernel(DgAdvectArgs a,
         ul += tw[k] * ld(a.u, a.f_double, ((size_t)k * a.Ne + e) * a.Nv + v);
       const double fac = (a.c0[v / (a.N * a.N)] - ux) * nl;
       if (fac >= 0.) sn += fac * ul * cw;
-      else sd += fac * a.f0[side][v] * cw;
+      else sd += fac * (kind == kBcWall ? a.f0[side][v] : wall_expr_maxwellian(a, side, v)) * cw;
     }
   }
   rn[t] = sn;
@@ -159,7 +175,7 @@ __global__ void dg_wall_final_kernel(DgAdvectArgs a, const double* part,
     rn += part[(side * kWallCh + c) * 2];
     rd += part[(side * kWallCh + c) * 2 + 1];
   }
-  nden[side] = (a.bc[side] == kBcWall) ? -(rn / rd) : 0.0;
+  nden[side] = (a.bc[side] == kBcWall || a.bc[side] == kBcWallExpr) ? -(rn / rd) : 0.0;
 }
 
 __device__ __forceinline__ double dg_ghost(const DgAdvectArgs& a, int side,
@@ -170,8 +186,16 @@ __device__ __forceinline__ double dg_ghost(const DgAdvectArgs& a, int side,
     return fac < 0 ? a.f0[side][v] * a.nden[side] : ul;
   }
   if (kind == kBcInlet) {
-    const double fac = cx * a.nl[side];
+    const double fac = (cx - a.bc_ux[side]) * a.nl[side];
     return fac < 0 ? a.f0[side][v] : ul;
+  }
+  if (kind == kBcWallExpr) {
+    const double fac = (cx - a.ws[side][0]) * a.nl[side];
+    return fac < 0 ? wall_expr_maxwellian(a, side, v) * a.nden[side] : ul;
+  }
+  if (kind == kBcVanish) {
+    const double fac = cx * a.nl[side];
+    return fac >= 0 ? 0.0 : ul;
   }
   return ul;
 }

@@ -962,9 +962,9 @@ extern "C" int dgfs_dg_create(const dgfs_dg_desc* d, dgfs_dg_handle* out) {
       !d->c0 || !d->im)
     return fail(DGFS_ERR_INVALID, "missing operator arrays");
   for (int s = 0; s < 2; ++s) {
-    if (d->bc_kind[s] < kBcCopy || d->bc_kind[s] > kBcInlet)
+    if (d->bc_kind[s] < kBcCopy || d->bc_kind[s] > kBcWallExpr)
       return fail(DGFS_ERR_INVALID, "unknown boundary kind");
-    if (d->bc_kind[s] != kBcCopy && !d->bc_f0[s])
+    if ((d->bc_kind[s] == kBcWall || d->bc_kind[s] == kBcInlet) && !d->bc_f0[s])
       return fail(DGFS_ERR_INVALID, "wall/inlet boundary needs its Maxwellian");
   }
   const int K = d->K, Ne = d->Ne, N = d->N, Nv = N * N * N;
@@ -980,6 +980,8 @@ extern "C" int dgfs_dg_create(const dgfs_dg_desc* d, dgfs_dg_handle* out) {
     a.bc[s] = d->bc_kind[s];
     a.bc_ux[s] = d->bc_ux[s];
     a.nl[s] = s == 0 ? -1.0 : 1.0;
+    a.ws[s][0] = a.ws[s][1] = a.ws[s][2] = 0.0;
+    a.ws[s][3] = a.ws[s][4] = 1.0;
   }
   h->Nqr = d->Nqr;
   h->cw = d->cw;
@@ -1043,6 +1045,20 @@ extern "C" int dgfs_dg_advect(dgfs_dg_handle h, const void* u, void* ux,
     default: dg_advect_kernel<8><<<grid, block, 0, st>>>(a); break;
   }
   DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_set_wall_state(dgfs_dg_handle h, int32_t side,
+                                      double ux, double uy, double uz,
+                                      double T, double mass) {
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  if (side < 0 || side > 1) return fail(DGFS_ERR_INVALID, "side must be 0 or 1");
+  if (h->base.bc[side] != kBcWallExpr)
+    return fail(DGFS_ERR_INVALID, "boundary is not a dgfs-wall-expr-diffuse wall");
+  if (!(T > 0) || !(mass > 0))
+    return fail(DGFS_ERR_INVALID, "wall temperature and mass must be > 0");
+  double* w = h->base.ws[side];
+  w[0] = ux; w[1] = uy; w[2] = uz; w[3] = T; w[4] = mass;
   return DGFS_OK;
 }
 

@@ -7,7 +7,9 @@ import torch
 from . import _native as nat
 from .collision import _DT, _stream_ptr
 
-BC_KIND = {'dgfs-periodic': 0, 'dgfs-wall-diffuse': 1, 'dgfs-inlet': 2}
+BC_KIND = {'dgfs-periodic': 0, 'dgfs-cyclic': 0, 'dgfs-wall-diffuse': 1,
+           'dgfs-inlet': 2, 'dgfs-inlet-nondim': 2, 'dgfs-vanish': 3,
+           'dgfs-wall-expr-diffuse': 4}
 
 
 def _dp(a):
@@ -71,6 +73,13 @@ class DGOperator:
         nat.check(nat.lib().dgfs_dg_advect(
             self._h, ctypes.c_void_p(u.data_ptr()),
             ctypes.c_void_p(ux.data_ptr()), _DT[u.dtype], _stream_ptr(stream)))
+
+    def set_wall_state(self, side, ux, uy, uz, T, mass=1.0):
+        """Velocity and temperature (nondimensional) of a
+        ``dgfs-wall-expr-diffuse`` boundary for the following advect calls."""
+        nat.check(nat.lib().dgfs_dg_set_wall_state(
+            self._h, int(side), float(ux), float(uy), float(uz), float(T),
+            float(mass)))
 
     def wall_density(self):
         out = (ctypes.c_double * 2)()

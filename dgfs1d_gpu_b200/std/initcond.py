@@ -4,6 +4,10 @@
 initcond.py:36-141, 320-383 (values on the velocity grid, nondimensional).  ``maxwellian-noise`` (no counterpart in
 the reference) multiplies the Maxwellian by (1 + amp U[-1, 1]), i.i.d. per
 phase-space point from a seeded generator (keys ``noise``, ``seed``).
+``maxwellian-expr`` / ``maxwellian-expr-nondim`` and ``sod-shock-tube-nondim``
+(initcond.py:144-238, 282-300, 385-434) evaluate their keys as expressions
+of the nondimensional solution-point coordinate ``x`` and the values of the
+``[non-dim]`` and ``[mesh]`` sections.
 ``normal-shock`` (no counterpart in the reference) joins an upstream and a
 downstream Maxwellian by a tanh ramp in x (keys ``rho1 T1 ux1 rho2 T2 ux2``,
 dimensional like ``maxwellian``; ``x0``, ``width`` in mesh units; optional
@@ -11,6 +15,7 @@ dimensional like ``maxwellian``; ``x0``, ``width`` in mesh units; optional
 """
 import numpy as np
 
+from ..config import npeval
 from ..plugins import subclass_where
 
 
@@ -158,3 +163,107 @@ class DGFSSodShockTubeInitConditionStd(DGFSInitConditionStd):
             raise ValueError('Not implemented')
         usol[:, :Ne // 2, :] = self._M[0][None, None, :]
         usol[:, Ne // 2:, :] = self._M[1][None, None, :]
+
+
+def _maxwellian(cv, rho, ux, uy, uz, T):
+    """rho / (pi T)^1.5 exp(-|c - u|^2 / T) for every point of the (...,)
+    shaped state arrays, on the velocity grid cv (3, Nv): shape (..., Nv)."""
+    rho, ux, uy, uz, T = np.broadcast_arrays(*[np.asarray(a, dtype=np.float64)
+                                              for a in (rho, ux, uy, uz, T)])
+    out = np.empty(rho.shape + (cv.shape[1],))
+    flat = out.reshape(-1, cv.shape[1])
+    for i, (r, a, b, c, t) in enumerate(zip(rho.ravel(), ux.ravel(), uy.ravel(),
+                                            uz.ravel(), T.ravel())):
+        c2 = (cv[0] - a) ** 2 + (cv[1] - b) ** 2 + (cv[2] - c) ** 2
+        flat[i] = r / (np.pi * t) ** 1.5 * np.exp(-c2 / t)
+    return out
+
+
+def _expr_vars(cfg, xsol):
+    v = {}
+    v.update(cfg.section_values('non-dim', np.float64))
+    v.update(cfg.section_values('mesh', np.float64))
+    v['x'] = xsol
+    return v
+
+
+class DGFSMaxwellianExprInitConditionStd(DGFSInitConditionStd):
+    """Maxwellian whose rho, ux, uy, uz, T are expressions of x
+    (initcond.py:144-238), dimensional (scaled by rho0, u0, T0)."""
+    model = 'maxwellian-expr'
+    _scaled = True
+
+    def load_parameters(self, name):
+        self._exprs = {k: self.cfg.lookupexpr(name, k)
+                       for k in ('rho', 'ux', 'uy', 'uz', 'T')}
+
+    def perform_precomputation(self):
+        pass
+
+    def get_init_vals(self):
+        raise ValueError('this model depends on spatial coordinates!')
+
+    def unondim(self):
+        raise ValueError('this model depends on spatial coordinates!')
+
+    def states(self, xsol):
+        vm = self.vm
+        v = _expr_vars(self.cfg, xsol)
+        sc = dict(rho=vm.rho0(), ux=vm.u0(), uy=vm.u0(), uz=vm.u0(), T=vm.T0())
+        out = {}
+        for k, e in self._exprs.items():
+            val = np.asarray(npeval(e, v), dtype=np.float64)
+            out[k] = val / sc[k] if self._scaled else val
+        return out
+
+    def apply_init_vals(self, usol, Nq, Ne, xsol=None):
+        st = self.states(xsol)
+        shape = (Nq, Ne)
+        st = {k: np.broadcast_to(v, shape) for k, v in st.items()}
+        usol[...] = _maxwellian(self.vm.cv(), st['rho'], st['ux'], st['uy'],
+                                st['uz'], st['T'])
+
+
+class DGFSMaxwellianExprNonDimInitConditionStd(
+        DGFSMaxwellianExprInitConditionStd):
+    """``maxwellian-expr`` with nondimensional values (initcond.py:282-300)."""
+    model = 'maxwellian-expr-nondim'
+    _scaled = False
+
+
+class DGFSSodShockNonDimTubeInitConditionStd(DGFSInitConditionStd):
+    """Nondimensional Sod tube (initcond.py:385-434): rho-, T-, ux-left/right
+    are expressions of x; points with x <= xMid take the left state; every
+    Maxwellian's density must be resolved by the grid (atol 1e-5)."""
+    model = 'sod-shock-tube-nondim'
+
+    def load_parameters(self, name):
+        cfg = self.cfg
+        self._exprs = {'%s-%s' % (k, s): cfg.lookupexpr(name, '%s-%s' % (k, s))
+                       for k in ('rho', 'T', 'ux') for s in ('left', 'right')}
+        self._xmid = cfg.lookupfloat(name, 'xMid')
+
+    def perform_precomputation(self):
+        pass
+
+    def get_init_vals(self):
+        raise ValueError('this model depends on spatial coordinates!')
+
+    def unondim(self):
+        raise ValueError('this model depends on spatial coordinates!')
+
+    def apply_init_vals(self, usol, Nq, Ne, xsol=None):
+        v = _expr_vars(self.cfg, xsol)
+        val = {k: np.broadcast_to(np.asarray(npeval(e, v), dtype=np.float64),
+                                  (Nq, Ne)).ravel()
+               for k, e in self._exprs.items()}
+        x = np.asarray(xsol).ravel()
+        flat = usol.reshape(-1, usol.shape[-1])
+        cv, cw = self.vm.cv(), self.vm.cw()
+        for side, sel in (('left', x <= self._xmid), ('right', x > self._xmid)):
+            rho = val['rho-' + side][sel]
+            M = _maxwellian(cv, rho, val['ux-' + side][sel], 0.0, 0.0,
+                            val['T-' + side][sel])
+            if not np.allclose(rho, M.sum(axis=-1) * cw, atol=1e-5):
+                raise ValueError('Bulk properties not conserved! Check Nv, dev')
+            flat[sel, :] = M

@@ -22,6 +22,7 @@ from ..velocitymesh import DGFSVelocityMeshStd
 from .bc import get_bc
 from .initcond import get_initcond
 from .integrator import DGFSIntegratorStd
+from .distributionslice import DGFSDistributionSliceStd
 from .moments import DGFSMomWriterStd
 from .residual import DGFSResidualStd
 from .scattering import DGFSScatteringModelStd
@@ -81,6 +82,11 @@ class DGFSStd1D:
         self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, xcoeff,
                                         tcurr=self.t, coeff=self.u)
         self.distribution = DGFSDistributionWriter(ti, (K, Ne, Nv), cfg)
+        if cfg.has_section('dgfsdistslicewriter'):
+            self.distributionslice = DGFSDistributionSliceStd(
+                ti, (K, Ne, Nv), basis.interpMat, vm, cfg)
+        else:
+            self.distributionslice = lambda *a: None
         self.residual = DGFSResidualStd(cfg, self.dg)
         # linear slope limiter after every step (std.py:369-400)
         self.limiter = int(cfg.lookupordefault('time-integrator', 'limiter', 0))
@@ -99,6 +105,8 @@ class DGFSStd1D:
             self.dg.limit(self.u)
 
     def rhs(self, t, u_in, u_out):
+        for side, bc in enumerate((self.bcl, self.bcr)):
+            bc.at_time(t, self.dg, side)
         self.dg.advect(u_in, u_out)
         self.sm.fs_batch(u_in, u_out, self.src, self.dst)
 
@@ -106,7 +114,11 @@ class DGFSStd1D:
         """Capture one time step (every RHS stage -- advection, boundary
         conditions, collision operator -- and every stage update) as one CUDA
         graph; later calls of ``step`` replay it.  A warm-up step runs first
-        and is undone, so the solution is unchanged."""
+        and is undone, so the solution is unchanged.  A boundary whose state
+        depends on time (dgfs-wall-expr-diffuse) cannot be captured."""
+        if self.bcl.time_dependent or self.bcr.time_dependent:
+            raise ValueError('a time-dependent boundary condition cannot be '
+                             'captured in a CUDA graph')
         u0 = self.u.clone()
         self._advance()
         torch.cuda.synchronize()
@@ -132,6 +144,7 @@ class DGFSStd1D:
         self.residual(self.t, self.nacptsteps, self.u, self.uprev)
         self.moments(self.dt, self.t, self.u)
         self.distribution(self.dt, self.t, self.u)
+        self.distributionslice(self.dt, self.t, self.u)
         self.uprev.copy_(self.u)
 
     def run(self, nsteps=None):

@@ -178,8 +178,12 @@ int dgfs_vss_eval(dgfs_vss_handle h, int32_t p, int32_t q, const void* f_p,
  * mul_by_adv, totalFlux and mul_by_invjac (std.mako:92-190).  trL/trR are
  * rows 0 and Nqf-1 of Bqf^T, D the derivative operator (ux = D u), gLD/gRD
  * the lifting vectors, im the K x Nqr interpolation to the moment points.
- * Boundary kinds: 0 dgfs-periodic (one rank: ghost = interior trace),
- * 1 dgfs-wall-diffuse, 2 dgfs-inlet; bc_f0 the wall/inlet Maxwellian.
+ * Boundary kinds: 0 dgfs-periodic / dgfs-cyclic (one rank: ghost = interior
+ * trace), 1 dgfs-wall-diffuse, 2 dgfs-inlet / dgfs-inlet-nondim (incoming
+ * where (c_x - bc_ux) n < 0; bc_ux = 0 for dgfs-inlet), 3 dgfs-vanish,
+ * 4 dgfs-wall-expr-diffuse (state set by dgfs_dg_set_wall_state);
+ * bc_f0 the wall/inlet Maxwellian (kinds 1 and 2).
+ * (std/bc.py:25-327, std/kernels/bcs/*.mako, bi/bc.py)
  */
 typedef struct dgfs_dg_s* dgfs_dg_handle;
 typedef struct {
@@ -211,6 +215,16 @@ int dgfs_dg_destroy(dgfs_dg_handle h);
 int dgfs_dg_advect(dgfs_dg_handle h, const void* u, void* ux, int32_t dtype,
                    void* stream);
 int dgfs_dg_wall_density(dgfs_dg_handle h, double* out2);
+
+/* State of a dgfs-wall-expr-diffuse wall for the following dgfs_dg_advect
+ * calls: nondimensional velocity, temperature, and the species mass in the
+ * exponent of its Maxwellian exp(-mass |c - u|^2 / T) (1 for one species).
+ * Replaces the ux/uy/uz/T expressions of t rendered into
+ * dgfs-wall-expr-diffuse.mako (std/bc.py:136-199, bi/bc.py:122-205): the
+ * caller evaluates them at the stage time.  Host-side only; a CUDA graph
+ * keeps the state it was captured with. */
+int dgfs_dg_set_wall_state(dgfs_dg_handle h, int32_t side, double ux,
+                           double uy, double uz, double T, double mass);
 
 /* Bulk moments (FP64) at the Nqr reconstruction points of each element,
  * nondimensional, out[(r*Ne + e)*10 + i] for i = rho, Ux, Uy, T, Qx, Qy,

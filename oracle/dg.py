@@ -117,10 +117,12 @@ class WallDiffuseBC:
 
 
 class InletBC:
-    """Inlet: incoming from a fixed Maxwellian (dgfs-inlet.mako)."""
+    """Inlet: incoming from a fixed Maxwellian (dgfs-inlet.mako); with
+    ``shift`` = u_x the incoming test is (c_x - u_x) n < 0
+    (dgfs-inlet-nondim.mako)."""
 
-    def __init__(self, cv, rho, T, u, nl):
-        self.cx, self.nl = cv[0], nl
+    def __init__(self, cv, rho, T, u, nl, shift=0.0):
+        self.cx, self.nl, self.shift = cv[0], nl, shift
         self.f0 = (rho / (np.pi * T) ** 1.5) * np.exp(
             -np.sum((cv - np.reshape(u, (3, 1))) ** 2, axis=0) / T)
 
@@ -128,8 +130,50 @@ class InletBC:
         pass
 
     def apply(self, ul):
-        fac = self.cx * self.nl
+        fac = (self.cx - self.shift) * self.nl
         return (fac < 0) * self.f0 + (fac >= 0) * ul
+
+
+class VanishBC:
+    """dgfs-vanish.mako: ghost 0 where c_x n >= 0, the trace elsewhere."""
+
+    def __init__(self, cv, nl):
+        self.cx, self.nl = cv[0], nl
+
+    def update(self, ul):
+        pass
+
+    def apply(self, ul):
+        fac = self.cx * self.nl
+        return (fac >= 0) * 0.0 + (fac < 0) * ul
+
+
+class WallExprBC:
+    """dgfs-wall-expr-diffuse.mako (std and bi): diffuse wall with state
+    (ux, uy, uz, T) = state(t) (nondimensional) and the unnormalised
+    Maxwellian exp(-m |c - u|^2 / T); set ``t`` before each right-hand side."""
+
+    def __init__(self, cv, cw, nl, state, mass=1.0):
+        self.cv, self.cw, self.nl, self.state, self.mass = cv, cw, nl, state, mass
+        self.t = 0.0
+
+    def _mx(self):
+        ux, uy, uz, T = self.state(self.t)
+        cv = self.cv
+        c2 = (cv[0] - ux) ** 2 + (cv[1] - uy) ** 2 + (cv[2] - uz) ** 2
+        return ux, np.exp(-self.mass * c2 / T)
+
+    def update(self, ul):
+        ux, mx = self._mx()
+        fac = (self.cv[0] - ux) * self.nl
+        num = (fac >= 0.) * (fac * ul * self.cw)
+        den = (fac < 0.) * (fac * mx * self.cw)
+        self.nden = -(np.sum(num) / np.sum(den))
+
+    def apply(self, ul):
+        ux, mx = self._mx()
+        fac = (self.cv[0] - ux) * self.nl
+        return (fac < 0) * (mx * self.nden) + (fac >= 0) * ul
 
 
 class PeriodicBC:

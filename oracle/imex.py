@@ -5,7 +5,7 @@ dgfs1D/astd/kernels/scattering/bgk-direct-gll.mako (cmaxwellian :118-153,
 collide :157-181, updateMom{q}_BDF :16-42, updateDistribution{q}_BDF
 :46-78, updateMom{q}_LM :327-351, updateDistribution{q}_LM :354-405); the
 schemes restate dgfs1D/astd/integrator.py (bdf-111 :281-322, bdf-222
-:325-400, IMEX-LM :623-792).  Start-up steps of the multi-step schemes use
+:325-400, boltz-ars-111 :491-552, IMEX-LM :623-792).  Start-up steps of the multi-step schemes use
 first-order substeps of the same family (the reference uses ARS-222/443
 substeps); ``imex-lm-*`` does not stop after its first step (astd/
 integrator.py:732 exits the process there).
@@ -285,6 +285,17 @@ class IMEX:
 
     def step(self, f):
         dt, k = self.dt, self.kind
+        if k == 'boltz-ars-111':
+            # integrator.py:491-552: moments of the advection only, then the
+            # explicit part L + Q - P (P = nu (M(U0) - f)) in the update of f
+            U0 = self._mom(f)
+            P0 = self._collide(U0, f)
+            L0 = self.explicit(f)
+            LU0 = self._mom(L0)
+            L0 = L0 + self.boltz(f) - P0
+            U = self._relax(-((-1.) * U0 + (-1.) * dt * LU0) / 1., 1., dt)
+            rhs = -((-1.) * f + (-1.) * dt * L0)
+            return self._implicit(U, rhs, 1., dt)
         if k == 'bdf-111':
             U0 = self._mom(f)
             L0 = self.explicit(f)

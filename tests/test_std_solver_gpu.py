@@ -229,3 +229,84 @@ def test_restart_from_distribution_file(tmp_path, driver):
     with pytest.raises(ValueError, match='Inconsistent distribution'):
         S(Config(ini.replace('Ne = %d' % Ne, 'Ne = %d' % (Ne + 1), 1)),
           restart=str(tmp_path / files[0]))
+
+
+def test_std_driver_writes_velocity_slice(tmp_path):
+    """[dgfsdistslicewriter] in the single-species driver: the slice of the
+    device solution written every dt-out equals the interpolated host copy."""
+    ini = couette_std_ini(Nv=8, Nrho=4, nsteps=2)
+    dt = Config(ini).lookupfloat('time-integrator', 'dt')
+    ini += ('\n[dgfsdistslicewriter]\nbasedir = %s\nbasename = sl-{t:.6f}\n'
+            'dt-out = %.17g\nNe-out = 1\nNqr-out = 2\nNvy-out = 3\nNvz-out = 4\n'
+            % (tmp_path, dt))
+    s = _solver(ini)
+    s.run(2)
+    torch.cuda.synchronize()
+    files = sorted(tmp_path.iterdir())
+    assert len(files) == 2
+    N = s.vm.Nv()
+    sol = np.einsum('mr,mej->rej', s.basis.interpMat,
+                    s.u.cpu().numpy())[2, 1].reshape(N, N, N)[:, 3, 4]
+    data = np.loadtxt(files[-1])
+    assert np.allclose(data[:, 1], sol, rtol=1e-14, atol=0)
+    assert np.allclose(data[:, 0], s.vm.cv()[0].reshape(N, N, N)[:, 3, 4])
+
+
+def _custom_ini(ics, bcs, **kw):
+    return couette_std_ini(**kw).split('[soln-ics]')[0] + ics + bcs
+
+
+@pytest.mark.parametrize('case', ['inlet-vanish', 'cyclic-wallexpr'])
+def test_std_expression_ics_and_boundaries_match_oracle(case):
+    """maxwellian-expr-nondim / sod-shock-tube-nondim initial conditions and
+    the dgfs-inlet-nondim, dgfs-vanish, dgfs-cyclic and time-dependent
+    dgfs-wall-expr-diffuse boundaries in the native right-hand side, against
+    the oracle over three ssp-rk2 steps (FP64)."""
+    import math
+    if case == 'inlet-vanish':
+        ics = ('[soln-ics]\ntype = maxwellian-expr-nondim\n'
+               'rho = 1 + 0.1*sin(2*pi*x)\nux = 0.05*cos(pi*x)\nuy = 0.02\n'
+               'uz = 0\nT = 1 + 0.05*x\n')
+        bcs = ('[soln-bcs-xlo]\ntype = dgfs-inlet-nondim\nrho = 1.1\nux = 0.2\n'
+               'T = 0.95\n[soln-bcs-xhi]\ntype = dgfs-vanish\n')
+    else:
+        ics = ('[soln-ics]\ntype = sod-shock-tube-nondim\nxMid = 0.5\n'
+               'rho-left = 1\nT-left = 1\nux-left = 0\n'
+               'rho-right = 0.5\nT-right = 0.9\nux-right = 0.05*x\n')
+        bcs = ('[soln-bcs-xlo]\ntype = dgfs-cyclic\n'
+               '[soln-bcs-xhi]\ntype = dgfs-wall-expr-diffuse\nT = 300\nux = 0\n'
+               'uy = 60*sin(2000*t)\nuz = 0\n')
+    ini = _custom_ini(ics, bcs, Nv=16, Nrho=4, scheme='ssp-rk2', nsteps=3)
+    s = _solver(ini)
+    vm = s.vm
+    u0 = s.u.cpu().numpy().copy()
+    s.run(3)
+    torch.cuda.synchronize()
+    got = s.u.cpu().numpy()
+    cv, cw = vm.cv(), vm.cw()
+    if case == 'inlet-vanish':
+        bcl = odg.InletBC(cv, 1.1, 0.95, [0.2, 0, 0], -1., shift=0.2)
+        bcr = odg.VanishBC(cv, 1.)
+    else:
+        bcl = odg.PeriodicBC()
+        st = lambda t: (0.0, 60 * math.sin(2000 * t) / vm.u0(), 0.0, 300 / vm.T0())
+        bcr = odg.WallExprBC(cv, cw, 1., st)
+    ovm = om.VelocityMeshStd(Nv=vm.Nv(), M=vm.M(), Nrho=vm.Nrho(), dev=vm.dev(),
+                             rho0=vm.rho0(), full_sphere=vm.sphere_mode() == 'full')
+    tab = oc.VHSTables(vm.Nv(), vm.L(), vm.qz(), vm.qw(), vm.sz(), vm.sw(),
+                       s.sm._gamma, sphere_factor=vm.sphere_factor())
+    b = odg.NodalBasis(s.basis.basis_kind, s.basis.K, s.basis.interpMat.shape[1])
+    collide = odg.collide_fs(b, lambda f, g: oc.vhs_gll_fs(tab, s.sm.prefac, f))
+    assert np.array_equal(ovm.cv, cv)
+
+    def rhs(t, x):
+        bcr.t = t
+        return odg.dg_rhs(b, s.mesh.invjac, cv[0], bcl, bcr, x, collide=collide)
+    u, t = u0.copy(), 0.0
+    for _ in range(3):
+        odg.integrate('ssp-rk2', rhs, t, s.dt, u)
+        t += s.dt
+    assert _rel(got, u) < 1e-11
+    if case == 'cyclic-wallexpr':
+        with pytest.raises(ValueError, match='time-dependent'):
+            s.capture_step()
