@@ -56,6 +56,7 @@ class DGFSABstd1D:
                              [(bcl.type, bcl.f0, bcl.ux),
                               (bcr.type, bcr.f0, bcr.ux)])
         self.psm.bind(self.dg)
+        self._configure_dg(cfg)
         src, dst = [], []
         for m, a in basis.mode_sources():
             for e in range(Ne):
@@ -102,10 +103,17 @@ class DGFSABstd1D:
         else:
             self.sm.fs_batch(u_in, u_out, self.src, self.dst)
 
+    positivity = False      # positivity limiter after the slope limiter
+
+    def _configure_dg(self, cfg):
+        """Hook for variants of the spatial discretisation."""
+
     def step(self):
         self.odes.integrate(self.t, self.dt, self.nacptsteps, self.u)
         if self.limiter:
             self.dg.limit(self.u)
+            if self.positivity:
+                self.dg.limit_positivity(self.u)
         self.t += self.dt
         self.nacptsteps += 1
         # post-processing of abstd.py:480-486
@@ -121,3 +129,19 @@ class DGFSABstd1D:
 
     def bulk_moments(self):
         return self.moments.compute(self.u)
+
+
+class DGFSABUstd1D(DGFSABstd1D):
+    """Upwind summation-by-parts variant (``dgfsABUstd1D``, dgfs1D/astd/
+    abstdu.py:37-530): the same penalised IMEX driver with the advection
+    volume term split by the sign of c_x (basis operators Dp, Dm with
+    ``[basis] sigma``, default -1, read as an integer as there), periodic
+    traces when the right boundary is ``dgfs-cyclic`` (one rank), and, with
+    ``[time-integrator] limiter = 1``, the positivity limiter after the slope
+    limiter (abstdu.py:509-510)."""
+    positivity = True
+
+    def _configure_dg(self, cfg):
+        sigma = cfg.lookupordefault('basis', 'sigma', -1)
+        dpos, dneg = self.basis.upwind_ops(sigma)
+        self.dg.set_upwind(dpos, dneg, swap=self.bcr.type == 'dgfs-cyclic')

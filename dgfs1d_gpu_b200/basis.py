@@ -59,6 +59,22 @@ class Basis:
         self.cellAvgOp = _filter(A0 @ invV)
         self.drLinOp = _filter(self.derivMat @ (A1 @ invV))
 
+    def upwind_ops(self, sigma=-1):
+        """Applied volume operators of the upwind summation-by-parts
+        discretisation (dgfs1D/basis.py:304-312): (Dm^T, Dp^T) with
+        Dp/m = D +- S P^-1 / 2, D = derivMat^T, P = diag(w) and S = sigma q q^T,
+        q the last column of the QR factor of the Legendre Vandermonde.  The
+        first is used where c_x > 0, the second where c_x < 0."""
+        V = legendre_orthonormal(self.K, self.z).T
+        Q, _ = np.linalg.qr(V)
+        sig = np.zeros(self.K)
+        sig[-1] = sigma
+        S = Q @ np.diag(sig) @ Q.T
+        invP = np.diag(1.0 / self.w)
+        D = self.derivMat.T
+        Dp, Dm = D + 0.5 * S @ invP, D - 0.5 * S @ invP
+        return _filter(Dm.T), _filter(Dp.T)
+
     def mode_sources(self):
         """For nodal bases: the coefficient slot feeding each (m, r) term.
 

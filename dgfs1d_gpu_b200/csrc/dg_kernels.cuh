@@ -40,6 +40,12 @@ struct DgAdvectArgs {
   double trR[kDgMaxK];      // right-face trace weights (row Nqf-1 of Bqf^T)
   double D[kDgMaxK * kDgMaxK];  // derivOp (K x K): ux = D u
   double gLD[kDgMaxK], gRD[kDgMaxK];
+  // upwind summation-by-parts volume term (dgfsABUstd1D): D is applied where
+  // c_x > 0 and D2 where c_x < 0; swap: the ghosts take the trace at the
+  // opposite end of the domain (one-rank dgfs-cyclic right boundary)
+  double D2[kDgMaxK * kDgMaxK];
+  int upwind;
+  int swap;
 };
 
 __device__ __forceinline__ double ld(const void* p, int dbl, size_t i) {
@@ -109,6 +115,31 @@ __global__ void __launch_bounds__(256) dg_limit_kernel(DgLimitArgs a) {
     }
     aL = ac;
     ac = aR;
+  }
+}
+
+// Positivity limiter of dgfsABUstd1D (abstdu.py:432-441, limitPos of
+// astd/kernels/limiters.mako:198-227), in place, every element: with the cell
+// average a and the smallest nodal value m, u_k <- a + theta (u_k - a),
+// theta = min(1, |(a - 1e-13) / (a - m)|), the ratio rounded to single
+// precision as the reference's fabsf rounds it.
+__global__ void __launch_bounds__(256) dg_limit_pos_kernel(DgLimitArgs a) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= a.Nv) return;
+  const int K = a.K, Ne = a.Ne;
+  for (int e = 0; e < Ne; ++e) {
+    double avg = 0, m = 1e10;
+    for (int k = 0; k < K; ++k) {
+      const double x = ld(a.u, a.f_double, ((size_t)k * Ne + e) * a.Nv + v);
+      avg += a.wavg[k] * x;
+      m = fmin(m, x);
+    }
+    const float ratio = (float)((avg - 1e-13) / (avg - m));
+    const double theta = fmin(1.0, (double)fabsf(ratio));
+    for (int k = 0; k < K; ++k) {
+      const size_t i = ((size_t)k * Ne + e) * a.Nv + v;
+      st(a.u, a.f_double, i, avg + theta * (ld(a.u, a.f_double, i) - avg));
+    }
   }
 }
 
@@ -226,9 +257,21 @@ __global__ void __launch_bounds__(256) dg_advect_kernel(DgAdvectArgs a) {
     for (int k = 0; k < K; ++k) s += a.trR[k] * w[k];
     return s;
   };
+  // the volume operator of this velocity (upwind: split by the sign of c_x)
+  const double* Dv = (a.upwind && cx < 0) ? a.D2 : a.D;
+  // traces at the two ends of the domain, for the swapped (periodic) ghosts
+  double uEnd0 = 0, uEnd1 = 0;
+  if (a.swap) {
+    double ul[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      ul[k] = ld(a.u, a.f_double, ((size_t)k * Ne + Ne - 1) * Nv + v);
+    uEnd1 = tr(ul);
+    uEnd0 = tl(ue);
+  }
   // face 0: ghost on the left, element 0 on the right
   double uRf = tl(ue);
-  double uLf = dg_ghost(a, 0, v, cx, uRf);
+  double uLf = dg_ghost(a, 0, v, cx, a.swap ? uEnd1 : uRf);
   double jR = ac * (uLf - uRf) + hc * (uLf - uRf);
   for (int e = 0; e < Ne; ++e) {
     // face e+1
@@ -240,7 +283,7 @@ __global__ void __launch_bounds__(256) dg_advect_kernel(DgAdvectArgs a) {
         un[k] = ld(a.u, a.f_double, ((size_t)k * Ne + e + 1) * Nv + v);
       uR1 = tl(un);
     } else {
-      uR1 = dg_ghost(a, 1, v, cx, uL1);
+      uR1 = dg_ghost(a, 1, v, cx, a.swap ? uEnd0 : uL1);
     }
     const double jd = ac * (uL1 - uR1);
     const double jL1 = jd + hc * (uR1 - uL1);
@@ -249,7 +292,7 @@ __global__ void __launch_bounds__(256) dg_advect_kernel(DgAdvectArgs a) {
     for (int k = 0; k < K; ++k) {
       double d = 0;
 #pragma unroll
-      for (int m = 0; m < K; ++m) d += a.D[k * K + m] * ue[m];
+      for (int m = 0; m < K; ++m) d += Dv[k * K + m] * ue[m];
       double r = d * (-cx);
       r += -jL1 * a.gRD[k] + jR * a.gLD[k];
       st(a.ux, a.f_double, ((size_t)k * Ne + e) * Nv + v, r * ij);

@@ -1532,6 +1532,37 @@ extern "C" int dgfs_dg_set_limiter(dgfs_dg_handle h, const double* wavg,
   return upload(&h->lim, t);
 }
 
+extern "C" int dgfs_dg_limit_positivity(dgfs_dg_handle h, void* u,
+                                        int32_t dtype, void* stream) {
+  if (!h || !u) return fail(DGFS_ERR_INVALID, "null argument");
+  if (!h->lim) return fail(DGFS_ERR_INVALID, "limiter tables not set");
+  if (dtype != DGFS_F32 && dtype != DGFS_F64)
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  DgLimitArgs a{};
+  a.u = u; a.f_double = dtype == DGFS_F64; a.K = h->base.K; a.Ne = h->base.Ne;
+  a.Nv = h->base.Nv; a.wavg = h->lim;
+  dg_limit_pos_kernel<<<(a.Nv + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_dg_set_upwind(dgfs_dg_handle h, const double* Dpos,
+                                  const double* Dneg, int32_t swap) {
+  if (!h || !Dpos || !Dneg) return fail(DGFS_ERR_INVALID, "null argument");
+  DgAdvectArgs& a = h->base;
+  if (swap && (a.bc[0] == kBcWall || a.bc[1] == kBcWall ||
+               a.bc[0] == kBcWallExpr || a.bc[1] == kBcWallExpr))
+    return fail(DGFS_ERR_UNSUPPORTED, "swapped (periodic) traces with a wall boundary");
+  const int K = a.K;
+  for (int i = 0; i < K * K; ++i) {
+    a.D[i] = Dpos[i];
+    a.D2[i] = Dneg[i];
+  }
+  a.upwind = 1;
+  a.swap = swap ? 1 : 0;
+  return DGFS_OK;
+}
+
 extern "C" int dgfs_dg_limit(dgfs_dg_handle h, void* u, int32_t dtype,
                              void* stream) {
   if (!h || !u) return fail(DGFS_ERR_INVALID, "null argument");

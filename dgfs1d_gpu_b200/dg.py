@@ -74,6 +74,23 @@ class DGOperator:
             self._h, ctypes.c_void_p(u.data_ptr()),
             ctypes.c_void_p(ux.data_ptr()), _DT[u.dtype], _stream_ptr(stream)))
 
+    def set_upwind(self, dpos, dneg, swap=False):
+        """Use the upwind summation-by-parts volume term: dpos where c_x > 0,
+        dneg where c_x < 0 (K x K); ``swap`` makes the boundaries periodic
+        (each ghost takes the trace at the other end)."""
+        self._keep['upw'] = [np.ascontiguousarray(dpos, dtype=np.float64),
+                             np.ascontiguousarray(dneg, dtype=np.float64)]
+        a, b = self._keep['upw']
+        nat.check(nat.lib().dgfs_dg_set_upwind(self._h, _dp(a), _dp(b),
+                                               int(bool(swap))))
+
+    def limit_positivity(self, u, stream=None):
+        """Positivity limiter (limitPos) on u (K, Ne, N^3), in place; needs
+        set_limiter's tables."""
+        nat.check(nat.lib().dgfs_dg_limit_positivity(
+            self._h, ctypes.c_void_p(u.data_ptr()), _DT[u.dtype],
+            _stream_ptr(stream)))
+
     def set_wall_state(self, side, ux, uy, uz, T, mass=1.0):
         """Velocity and temperature (nondimensional) of a
         ``dgfs-wall-expr-diffuse`` boundary for the following advect calls."""

@@ -260,6 +260,23 @@ int dgfs_dg_set_limiter(dgfs_dg_handle h, const double* wavg, const double* wdr,
                         const double* dx, const double* hs);
 int dgfs_dg_limit(dgfs_dg_handle h, void* u, int32_t dtype, void* stream);
 
+/* Positivity limiter of dgfsABUstd1D (abstdu.py:432-441, limitPos of
+ * astd/kernels/limiters.mako:198-227), in place on every element: u_k <-
+ * a + theta (u_k - a), a the cell average, theta = min(1, |(a - 1e-13) /
+ * (a - min_k u_k)|) rounded to single precision as there.  Needs the tables
+ * of dgfs_dg_set_limiter. */
+int dgfs_dg_limit_positivity(dgfs_dg_handle h, void* u, int32_t dtype,
+                             void* stream);
+
+/* Switch h's advection to the upwind summation-by-parts volume term of
+ * dgfsABUstd1D (abstdu.py:355-383, upwind.mako): Dpos (K x K, row-major,
+ * applied as ux = -c_x Dpos u) where c_x > 0 -- the reference's Dm^T -- and
+ * Dneg (Dp^T) where c_x < 0; the face fluxes are unchanged.  swap != 0 gives
+ * the ghost at each end the trace at the other end (abstdu.py:330-331, a
+ * one-rank dgfs-cyclic right boundary); not with wall boundaries. */
+int dgfs_dg_set_upwind(dgfs_dg_handle h, const double* Dpos, const double* Dneg,
+                       int32_t swap);
+
 /*
  * Penalty (BGK-type) model of the penalised IMEX schemes, FP64 arithmetic
  * (dgfs1D/astd/scattering.py:44-284, astd/kernels/scattering/

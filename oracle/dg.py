@@ -220,6 +220,71 @@ def dg_rhs(basis, invjac, cx, bcl, bcr, u_in, collide=None):
     return np.einsum('km,mev->kev', basis.invMassOp, ux)
 
 
+def upwind_ops(basis, sigma=-1):
+    """Upwind summation-by-parts operators of basis.py:304-312 as applied
+    (Dp^T, Dm^T): S = sigma q q^T with q the last column of the QR of the
+    Legendre Vandermonde, P = diag(w), Dp/m = D -/+ ... = D +- S P^-1 / 2,
+    D = derivMat^T."""
+    K = basis.K
+    V = ortho_basis_at(K, basis.z).T
+    Vo, _ = np.linalg.qr(V)
+    sig = np.zeros(K)
+    sig[-1] = sigma
+    S = Vo @ np.diag(sig) @ Vo.T
+    invP = np.diag(1.0 / basis.w)
+    D = basis.derivMat.T
+    Dp, Dm = D + 0.5 * S @ invP, D - 0.5 * S @ invP
+    return filter_tol(Dp.T), filter_tol(Dm.T)
+
+
+def dg_rhs_upwind(basis, invjac, cx, bcl, bcr, u_in, sigma=-1, swap=False,
+                  collide=None):
+    """Explicit right-hand side of dgfsABUstd1D (abstdu.py:295-383): the
+    upwind fluxes jL = (uR - uL) min(c, 0), jR = -(uR - uL) max(c, 0) (equal
+    to the central-upwind fluxes of dg_rhs), the split volume term
+    -(Dm^T max(c,0) u + Dp^T min(c,0) u), lifting, invjac; ``swap`` gives
+    each end's boundary the other end's trace (one-rank dgfs-cyclic)."""
+    K, Ne, Nv = u_in.shape
+    DpT, DmT = upwind_ops(basis, sigma)
+    usolF = np.einsum('qk,kev->qev', basis.bwdFaceOp, u_in).reshape(-1, Nv)
+    mapL, mapR = face_maps(Ne, basis.Nqf)
+    uL = usolF[mapL].copy()
+    uR = usolF[mapR].copy()
+    bcL, bcR = uL[0].copy(), uR[Ne].copy()
+    if swap:
+        bcL, bcR = bcR, bcL
+    bcl.update(bcL)
+    uL[0] = bcl.apply(bcL)
+    bcr.update(bcR)
+    uR[Ne] = bcr.apply(bcR)
+    diff = uR - uL
+    jL = diff * np.minimum(cx, 0.0)
+    jR = -diff * np.maximum(cx, 0.0)
+    f = np.where(cx > 0, cx, 0.0) * u_in
+    g = np.where(cx < 0, cx, 0.0) * u_in
+    ux = -(np.einsum('km,mev->kev', DmT, f) + np.einsum('km,mev->kev', DpT, g))
+    for k in range(K):
+        for e in range(Ne):
+            ux[k, e] += -jL[e + 1] * basis.gRD[k] + jR[e] * basis.gLD[k]
+    ux = ux * invjac.reshape(1, Ne, 1)
+    if collide is not None:
+        collide(u_in, ux)
+    return np.einsum('km,mev->kev', basis.invMassOp, ux)
+
+
+def limit_positivity(basis, u):
+    """limitPos of limiters.mako:198-227 (every element): u_k <- a + theta
+    (u_k - a), theta = min(1, |(a - 1e-13)/(a - min u)|) rounded to single
+    precision (the kernel's fabsf)."""
+    K, Ne, Nv = u.shape
+    avg = np.einsum('j,jev->ev', basis.cellAvgOp[0], u)
+    mn = np.minimum(1e10, u.min(axis=0))
+    with np.errstate(divide='ignore', invalid='ignore'):
+        ratio = ((avg - 1e-13) / (avg - mn)).astype(np.float32)
+    theta = np.minimum(1.0, np.abs(ratio).astype(np.float64))
+    return avg[None] + theta[None] * (u - avg[None])
+
+
 def collide_fs(basis, fs):
     """The collision loop of std.py:349-356 with fs(f, g) -> increment."""
     def collide(u_in, ux):

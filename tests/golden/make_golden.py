@@ -7,6 +7,7 @@ default /root/reference)::
     python tests/golden/make_golden.py penalty-models   # only the ES-BGK/Shakov files
     python tests/golden/make_golden.py limiter          # only the slope-limiter file
     python tests/golden/make_golden.py moments          # only the moment-writer file
+    python tests/golden/make_golden.py upwind           # only the upwind (abstdu) file
 
 What runs from the reference:
   * its pure-Python setup code, imported directly with stand-ins for the
@@ -724,6 +725,114 @@ def golden_limiter(R, K=3, Ne=8, Nv=4):
                 uavg=uavg, ulx=ulx, ulim=ulim)
 
 
+def golden_upwind(R, Nv=8, Ne=5, K=3):
+    """The explicit right-hand side of dgfsABUstd1D (abstdu.py:295-383): the
+    reference basis' upwind operators Dp, Dm (basis.py:304-312, captured by
+    letting get_mm_kernel return its matrix), its std.mako and upwind.mako
+    kernels and boundary kernels, composed as explicit() composes them; two
+    boundary set-ups (one-rank dgfs-cyclic on both ends, whose traces are
+    swapped, and dgfs-inlet-nondim / dgfs-vanish); and the positivity limiter
+    limitPos of limiters.mako on data with negative values."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    import dgfs1D.util as util
+    ini = STD_INI.format(basis='nodal-sem-gll', Nv=Nv, Nrho=2, M=6, dev=5.0)
+    ini = ini.replace('Ne = 4', 'Ne = %d' % Ne).replace('K = 3', 'K = %d' % K)
+    cfg = R.Dictionary(ini)
+    vm = R.vstd.DGFSVelocityMeshStd(cfg)
+    old = R.basis.get_mm_kernel
+    R.basis.get_mm_kernel = lambda m, *a, **k: np.array(m, dtype=float)
+    try:
+        b = R.basis.NodalSemGLL(cfg)
+    finally:
+        R.basis.get_mm_kernel = old
+    Dp, Dm = np.array(b.DpKern), np.array(b.DmKern)
+    Nqf, vsize = b.Nqf, vm.vsize()
+    xmesh = np.linspace(0., 1., Ne + 1)
+    h = np.diff(xmesh).reshape(-1, 1)
+    jac, invjac = h / 2., 2. / h
+    mapL, mapR = np.arange(Ne + 1) + (Nqf - 1) * Ne - 1, np.arange(Ne + 1)
+    mapL[0], mapR[-1] = 0, Ne * Nqf - 1
+    xsol = np.array([0.5 * (xmesh[j] + xmesh[j + 1]) + jac[j] * b.z
+                     for j in range(Ne)]).T
+    args = dict(K=K, Ne=Ne, Nq=K, vsize=vsize, dtype='double', mapL=mapL,
+                mapR=mapR, offsetL=0, offsetR=len(mapR) - 1, invjac=invjac,
+                gRD=b.gRD, gLD=b.gLD, xsol=xsol)
+    SK = RefModule(render_template('dgfs1D/std/kernels/std.mako', **args), tag='std_u')
+    UK = RefModule(render_template('dgfs1D/astd/kernels/upwind.mako', **args), tag='upwind')
+    LK = RefModule(render_template('dgfs1D/astd/kernels/limiters.mako', nalph=5,
+                                   Dr=b.derivMat, **args), tag='limiters_u')
+    blk = 128
+    gv = grid_for(vsize, blk)
+    filt = util.filter_tol
+
+    def mm(A, B):
+        return np.ascontiguousarray(
+            (filt(np.array(A, dtype=np.float64)) @ B.reshape(A.shape[1], -1)).ravel())
+
+    cvx = np.ascontiguousarray(vm.cv()[0])
+    rng = np.random.default_rng(SEED + 37)
+    u = np.stack([_maxwellian_noise(vm.cv(), rng, rho=rng.uniform(0.5, 1.5))
+                  for _ in range(K * Ne)]).reshape(K, Ne, vsize)
+    u = np.ascontiguousarray(u.ravel())
+    inlet = dict(rho=1.1, ux=0.2, T=0.95)
+    uin = np.array([inlet['ux'], 0, 0]).reshape(3, 1)
+    f_in = (inlet['rho'] / (np.pi * inlet['T']) ** 1.5) * np.exp(
+        -np.sum((vm.cv() - uin) ** 2, axis=0) / inlet['T'])
+    bmods = {}
+    for kind, nl in (('dgfs-cyclic', -1.), ('dgfs-cyclic', 1.),
+                     ('dgfs-inlet-nondim', -1.), ('dgfs-vanish', 1.)):
+        src = render_template('dgfs1D/std/kernels/bcs/%s.mako' % kind, dtype='double',
+                              vsize=vsize, cw=vm.cw(), nl=nl, x=0.0, u=inlet['ux'])
+        bmods[kind, nl] = RefModule(src, tag='%s%d' % (kind.replace('-', '_'), nl > 0))
+    out = {}
+    for case, (kl, kr) in (('cyclic', ('dgfs-cyclic', 'dgfs-cyclic')),
+                           ('inlet_vanish', ('dgfs-inlet-nondim', 'dgfs-vanish'))):
+        usolF = mm(b._Bqf.T, u)
+        uL, uR = np.zeros((Ne + 1) * vsize), np.zeros((Ne + 1) * vsize)
+        SK.launch('extract_left', gv, blk, usolF, uL)
+        SK.launch('extract_right', gv, blk, usolF, uR)
+        bcL, bcR, bcT = np.zeros(vsize), np.zeros(vsize), np.zeros(vsize)
+        SK.launch('transfer_bc_left', gv, blk, uL, bcL)
+        SK.launch('transfer_bc_right', gv, blk, uR, bcR)
+        if kr == 'dgfs-cyclic':          # abstdu.py:330-331 on one rank
+            bcT[:] = bcL
+            bcL[:] = bcR
+            bcR[:] = bcT
+        for kind, nl, bcv, ins in ((kl, -1., bcL, 'insert_bc_left'),
+                                   (kr, 1., bcR, 'insert_bc_right')):
+            BK = bmods[kind, nl]
+            if kind == 'dgfs-cyclic':
+                BK.launch('applyBC', gv, blk, bcv, bcT, cvx)
+            elif kind == 'dgfs-inlet-nondim':
+                BK.launch('applyBC', gv, blk, bcv, bcT, cvx, f_in, 0.0)
+            else:
+                BK.launch('applyBC', gv, blk, bcv, bcT, cvx, 0.0)
+            SK.launch(ins, gv, blk, bcT, uL if nl < 0 else uR)
+        jL, jR = np.zeros_like(uL), np.zeros_like(uR)
+        UK.launch('uflux', gv, blk, uL, uR, cvx, jL, jR)
+        f, g = np.zeros_like(u), np.zeros_like(u)
+        UK.launch('splitFlux', grid_for(K * Ne * vsize, blk), blk, cvx, u, f, g)
+        ux = mm(Dm, f)
+        f = mm(Dp, g)
+        ux = -(ux + f)
+        SK.launch('totalFlux', gv, blk, ux, cvx, jL, jR)
+        SK.launch('mul_by_invjac', gv, blk, ux)
+        out['rhs_' + case] = mm(b._B.T, ux)
+    # positivity limiter on data with negative values
+    w = u.copy().reshape(K, Ne, vsize)
+    w[0, :, ::7] -= 0.02
+    w[-1, :, 3::11] -= 0.05
+    w = np.ascontiguousarray(w.ravel())
+    uavg = mm(b.computeCellAvgKern, w)
+    ulim = np.zeros_like(w)
+    LK.launch('limitPos', gv, blk, w.copy(), uavg, ulim)
+    out.update(u=u, K=K, Ne=Ne, Nv=Nv, Dp=Dp, Dm=Dm, cv=vm.cv(), cw=vm.cw(),
+               invjac=invjac.ravel(), inlet=np.array([inlet['rho'], inlet['ux'],
+                                                     inlet['T']]),
+               wpos=w, wpos_lim=ulim)
+    return out
+
+
 def golden_moments(R, Nv=8, Ne=4, K=3):
     """Bulk moments of the reference's writers: DGFSMomWriterStd and
     DGFSMomWriterBi ``_compute_moments_1D`` (std/moments.py:11-70,
@@ -856,6 +965,7 @@ def main():
     penalty_models()
     np.savez_compressed(os.path.join(HERE, 'limiter_N4.npz'), **golden_limiter(R))
     np.savez_compressed(os.path.join(HERE, 'moments_N8.npz'), **golden_moments(R))
+    np.savez_compressed(os.path.join(HERE, 'upwind_N8.npz'), **golden_upwind(R))
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith('.npz'):
             print(fn, os.path.getsize(os.path.join(HERE, fn)), 'bytes')
@@ -864,6 +974,11 @@ def main():
 def limiter():
     R = _import_reference()
     np.savez_compressed(os.path.join(HERE, 'limiter_N4.npz'), **golden_limiter(R))
+
+
+def upwind():
+    R = _import_reference()
+    np.savez_compressed(os.path.join(HERE, 'upwind_N8.npz'), **golden_upwind(R))
 
 
 def moments():
@@ -886,5 +1001,7 @@ if __name__ == '__main__':
         limiter()
     elif sys.argv[1:] == ['moments']:
         moments()
+    elif sys.argv[1:] == ['upwind']:
+        upwind()
     else:
         main()
