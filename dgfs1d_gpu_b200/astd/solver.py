@@ -145,3 +145,15 @@ class DGFSABUstd1D(DGFSABstd1D):
         sigma = cfg.lookupordefault('basis', 'sigma', -1)
         dpos, dneg = self.basis.upwind_ops(sigma)
         self.dg.set_upwind(dpos, dneg, swap=self.bcr.type == 'dgfs-cyclic')
+
+
+class DGFSABE2std1D(DGFSABstd1D):
+    """Entropy-stable variant (``dgfsABE2std1D``, dgfs1D/astd/abstde2.py): the
+    advection volume term is the two-point form -2 c_x sum_l Dr[k][l]
+    aveL(u_k, u_l) with the logarithmic mean (eDeriv of
+    astd/kernels/limiters.mako:162-195); with ``[time-integrator] limiter =
+    1`` the positivity limiter follows the slope limiter (abstde2.py:492-493)."""
+    positivity = True
+
+    def _configure_dg(self, cfg):
+        self.dg.set_entropy_stable(self.basis.derivMat)

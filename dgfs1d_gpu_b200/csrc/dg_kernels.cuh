@@ -40,13 +40,28 @@ struct DgAdvectArgs {
   double trR[kDgMaxK];      // right-face trace weights (row Nqf-1 of Bqf^T)
   double D[kDgMaxK * kDgMaxK];  // derivOp (K x K): ux = D u
   double gLD[kDgMaxK], gRD[kDgMaxK];
-  // upwind summation-by-parts volume term (dgfsABUstd1D): D is applied where
-  // c_x > 0 and D2 where c_x < 0; swap: the ghosts take the trace at the
-  // opposite end of the domain (one-rank dgfs-cyclic right boundary)
+  // volume term: upwind = 0: -c_x D u; 1: upwind summation-by-parts
+  // (dgfsABUstd1D), D applied where c_x > 0 and D2 where c_x < 0;
+  // 2: entropy-stable two-point form (dgfsABE2std1D),
+  // -2 c_x sum_l D[k][l] aveL(u_k, u_l) with the logarithmic mean aveL.
+  // swap: the ghosts take the trace at the opposite end of the domain
+  // (one-rank dgfs-cyclic right boundary of dgfsABUstd1D)
   double D2[kDgMaxK * kDgMaxK];
   int upwind;
   int swap;
 };
+
+// Logarithmic mean (a + b) / 2 / (log(xi) / (2 f)), xi = |a / b|,
+// f = (xi - 1)/(xi + 1), with the series 1 + u/3 + u^2/5 + u^3/7 (u = f^2)
+// for u < 1e-2 and the 1e-20 guards of aveL in astd/kernels/limiters.mako:163-170.
+__device__ __forceinline__ double log_mean(double a, double b) {
+  const double xi = fabs(a / (b + 1e-20));
+  const double f = (xi - 1) / (xi + 1);
+  const double u = f * f;
+  return 0.5 * (a + b) /
+         (u < 1e-2 ? (1 + u / 3 + u * u / 5 + u * u * u / 7)
+                   : log(xi + 1e-20) / 2. / (f + 1e-20));
+}
 
 __device__ __forceinline__ double ld(const void* p, int dbl, size_t i) {
   return dbl ? static_cast<const double*>(p)[i]
@@ -258,7 +273,7 @@ __global__ void __launch_bounds__(256) dg_advect_kernel(DgAdvectArgs a) {
     return s;
   };
   // the volume operator of this velocity (upwind: split by the sign of c_x)
-  const double* Dv = (a.upwind && cx < 0) ? a.D2 : a.D;
+  const double* Dv = (a.upwind == 1 && cx < 0) ? a.D2 : a.D;
   // traces at the two ends of the domain, for the swapped (periodic) ghosts
   double uEnd0 = 0, uEnd1 = 0;
   if (a.swap) {
@@ -290,10 +305,18 @@ __global__ void __launch_bounds__(256) dg_advect_kernel(DgAdvectArgs a) {
     const double ij = a.invjac[e];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      double d = 0;
+      double r;
+      if (a.upwind == 2) {
+        r = 0;
 #pragma unroll
-      for (int m = 0; m < K; ++m) d += Dv[k * K + m] * ue[m];
-      double r = d * (-cx);
+        for (int m = 0; m < K; ++m)
+          r += -2 * Dv[k * K + m] * cx * log_mean(ue[k], ue[m]);
+      } else {
+        double d = 0;
+#pragma unroll
+        for (int m = 0; m < K; ++m) d += Dv[k * K + m] * ue[m];
+        r = d * (-cx);
+      }
       r += -jL1 * a.gRD[k] + jR * a.gLD[k];
       st(a.ux, a.f_double, ((size_t)k * Ne + e) * Nv + v, r * ij);
     }

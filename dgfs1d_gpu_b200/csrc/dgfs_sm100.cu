@@ -1563,6 +1563,15 @@ extern "C" int dgfs_dg_set_upwind(dgfs_dg_handle h, const double* Dpos,
   return DGFS_OK;
 }
 
+extern "C" int dgfs_dg_set_entropy_stable(dgfs_dg_handle h, const double* Dr) {
+  if (!h || !Dr) return fail(DGFS_ERR_INVALID, "null argument");
+  DgAdvectArgs& a = h->base;
+  for (int i = 0; i < a.K * a.K; ++i) a.D[i] = Dr[i];
+  a.upwind = 2;
+  a.swap = 0;
+  return DGFS_OK;
+}
+
 extern "C" int dgfs_dg_limit(dgfs_dg_handle h, void* u, int32_t dtype,
                              void* stream) {
   if (!h || !u) return fail(DGFS_ERR_INVALID, "null argument");

@@ -84,6 +84,12 @@ class DGOperator:
         nat.check(nat.lib().dgfs_dg_set_upwind(self._h, _dp(a), _dp(b),
                                                int(bool(swap))))
 
+    def set_entropy_stable(self, Dr):
+        """Use the entropy-stable two-point volume term with the derivative
+        matrix Dr (K x K, the basis' derivMat)."""
+        self._keep['es'] = np.ascontiguousarray(Dr, dtype=np.float64)
+        nat.check(nat.lib().dgfs_dg_set_entropy_stable(self._h, _dp(self._keep['es'])))
+
     def limit_positivity(self, u, stream=None):
         """Positivity limiter (limitPos) on u (K, Ne, N^3), in place; needs
         set_limiter's tables."""

@@ -277,6 +277,12 @@ int dgfs_dg_limit_positivity(dgfs_dg_handle h, void* u, int32_t dtype,
 int dgfs_dg_set_upwind(dgfs_dg_handle h, const double* Dpos, const double* Dneg,
                        int32_t swap);
 
+/* Switch h's advection to the entropy-stable volume term of dgfsABE2std1D
+ * (abstde2.py:363-367, eDeriv of astd/kernels/limiters.mako:162-195):
+ * ux_k = -2 c_x sum_l Dr[k][l] aveL(u_k, u_l), aveL the logarithmic mean, Dr
+ * (K x K, row-major) the basis' derivMat; the face fluxes are unchanged. */
+int dgfs_dg_set_entropy_stable(dgfs_dg_handle h, const double* Dr);
+
 /*
  * Penalty (BGK-type) model of the penalised IMEX schemes, FP64 arithmetic
  * (dgfs1D/astd/scattering.py:44-284, astd/kernels/scattering/

@@ -272,6 +272,50 @@ def dg_rhs_upwind(basis, invjac, cx, bcl, bcr, u_in, sigma=-1, swap=False,
     return np.einsum('km,mev->kev', basis.invMassOp, ux)
 
 
+def log_mean(a, b):
+    """aveL of astd/kernels/limiters.mako:163-170 (elementwise)."""
+    xi = np.abs(a / (b + 1e-20))
+    f = (xi - 1) / (xi + 1)
+    u = f * f
+    with np.errstate(divide='ignore', invalid='ignore'):
+        den = np.where(u < 1e-2, 1 + u / 3 + u * u / 5 + u * u * u / 7,
+                       np.log(xi + 1e-20) / 2. / (f + 1e-20))
+    return 0.5 * (a + b) / den
+
+
+def dg_rhs_entropy(basis, invjac, cx, bcl, bcr, u_in, collide=None):
+    """Explicit right-hand side of dgfsABE2std1D (abstde2.py:340-380): the
+    fluxes, lifting and invjac of dg_rhs with the entropy-stable volume term
+    -2 c_x sum_l Dr[k][l] aveL(u_k, u_l) (eDeriv, limiters.mako:173-195)."""
+    K, Ne, Nv = u_in.shape
+    usolF = np.einsum('qk,kev->qev', basis.bwdFaceOp, u_in).reshape(-1, Nv)
+    mapL, mapR = face_maps(Ne, basis.Nqf)
+    uL = usolF[mapL].copy()
+    uR = usolF[mapR].copy()
+    bcL, bcR = uL[0].copy(), uR[Ne].copy()
+    bcl.update(bcL)
+    uL[0] = bcl.apply(bcL)
+    bcr.update(bcR)
+    uR[Ne] = bcr.apply(bcR)
+    ac = 0.5 * np.abs(cx)
+    jL = ac * (uL - uR)
+    jR = jL.copy()
+    jL = jL + 0.5 * cx * (uR - uL)
+    jR = jR + 0.5 * cx * (uL - uR)
+    Dr = basis.derivMat
+    ux = np.zeros_like(u_in)
+    for k in range(K):
+        for l in range(K):
+            ux[k] += -2 * Dr[k, l] * cx * log_mean(u_in[k], u_in[l])
+    for k in range(K):
+        for e in range(Ne):
+            ux[k, e] += -jL[e + 1] * basis.gRD[k] + jR[e] * basis.gLD[k]
+    ux = ux * invjac.reshape(1, Ne, 1)
+    if collide is not None:
+        collide(u_in, ux)
+    return np.einsum('km,mev->kev', basis.invMassOp, ux)
+
+
 def limit_positivity(basis, u):
     """limitPos of limiters.mako:198-227 (every element): u_k <- a + theta
     (u_k - a), theta = min(1, |(a - 1e-13)/(a - min u)|) rounded to single

@@ -8,6 +8,7 @@ default /root/reference)::
     python tests/golden/make_golden.py limiter          # only the slope-limiter file
     python tests/golden/make_golden.py moments          # only the moment-writer file
     python tests/golden/make_golden.py upwind           # only the upwind (abstdu) file
+    python tests/golden/make_golden.py entropy          # only the entropy-stable (abstde2) file
 
 What runs from the reference:
   * its pure-Python setup code, imported directly with stand-ins for the
@@ -833,6 +834,80 @@ def golden_upwind(R, Nv=8, Ne=5, K=3):
     return out
 
 
+def golden_entropy(R, Nv=8, Ne=4, K=3):
+    """The explicit right-hand side of dgfsABE2std1D (abstde2.py:340-380):
+    the entropy-stable volume term eDeriv of limiters.mako (logarithmic mean)
+    with the std.mako fluxes, lifting and invjac, and diffuse walls, composed
+    as explicit() composes them, on data whose nodal values differ enough to
+    take both branches of the logarithmic mean."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    import dgfs1D.util as util
+    ini = STD_INI.format(basis='nodal-sem-gll', Nv=Nv, Nrho=2, M=6, dev=5.0)
+    ini = ini.replace('Ne = 4', 'Ne = %d' % Ne).replace('K = 3', 'K = %d' % K)
+    cfg = R.Dictionary(ini)
+    vm = R.vstd.DGFSVelocityMeshStd(cfg)
+    b = R.basis.NodalSemGLL(cfg)
+    Nqf, vsize = b.Nqf, vm.vsize()
+    xmesh = np.linspace(0., 1., Ne + 1)
+    h = np.diff(xmesh).reshape(-1, 1)
+    jac, invjac = h / 2., 2. / h
+    mapL, mapR = np.arange(Ne + 1) + (Nqf - 1) * Ne - 1, np.arange(Ne + 1)
+    mapL[0], mapR[-1] = 0, Ne * Nqf - 1
+    xsol = np.array([0.5 * (xmesh[j] + xmesh[j + 1]) + jac[j] * b.z
+                     for j in range(Ne)]).T
+    args = dict(K=K, Ne=Ne, Nq=K, vsize=vsize, dtype='double', mapL=mapL,
+                mapR=mapR, offsetL=0, offsetR=len(mapR) - 1, invjac=invjac,
+                gRD=b.gRD, gLD=b.gLD, xsol=xsol)
+    SK = RefModule(render_template('dgfs1D/std/kernels/std.mako', **args), tag='std_e')
+    LK = RefModule(render_template('dgfs1D/astd/kernels/limiters.mako', nalph=5,
+                                   Dr=b.derivMat, **args), tag='limiters_e')
+    blk = 128
+    gv = grid_for(vsize, blk)
+    filt = util.filter_tol
+
+    def mm(A, B):
+        return np.ascontiguousarray(
+            (filt(np.array(A, dtype=np.float64)) @ B.reshape(A.shape[1], -1)).ravel())
+
+    cvx = np.ascontiguousarray(vm.cv()[0])
+    rng = np.random.default_rng(SEED + 41)
+    u = np.stack([_maxwellian_noise(vm.cv(), rng, rho=rng.uniform(0.3, 2.0))
+                  for _ in range(K * Ne)]).reshape(K, Ne, vsize)
+    u = np.ascontiguousarray(u.ravel())
+    walls = {}
+    for side, nl, uy in (('L', -1., -0.1), ('R', 1., 0.1)):
+        u_w = np.array([0., uy, 0.]).reshape(3, 1)
+        f0 = (1.0 / np.pi ** 1.5) * np.exp(-np.sum((vm.cv() - u_w) ** 2, axis=0))
+        bsrc = render_template('dgfs1D/std/kernels/bcs/dgfs-wall-diffuse.mako',
+                               dtype='double', vsize=vsize, cw=vm.cw(), ux=0.0,
+                               nl=nl, x=0.0)
+        walls[side] = (RefModule(bsrc, tag='wall_e' + side), f0)
+    usolF = mm(b._Bqf.T, u)
+    uL, uR = np.zeros((Ne + 1) * vsize), np.zeros((Ne + 1) * vsize)
+    SK.launch('extract_left', gv, blk, usolF, uL)
+    SK.launch('extract_right', gv, blk, usolF, uR)
+    bcL, bcR, bcT = np.zeros(vsize), np.zeros(vsize), np.zeros(vsize)
+    SK.launch('transfer_bc_left', gv, blk, uL, bcL)
+    SK.launch('transfer_bc_right', gv, blk, uR, bcR)
+    for side, bcv, ins in (('L', bcL, 'insert_bc_left'), ('R', bcR, 'insert_bc_right')):
+        BK, f0 = walls[side]
+        num, den = np.zeros(vsize), np.zeros(vsize)
+        BK.launch('updateBC', gv, blk, bcv, cvx, f0, num, den, 0.0)
+        nden = np.array([-(np.sum(num) / np.sum(den))])
+        BK.launch('applyBC', gv, blk, bcv, bcT, cvx, f0, nden, 0.0)
+        SK.launch(ins, gv, blk, bcT, uL if side == 'L' else uR)
+    jL, jR = np.zeros_like(uL), np.zeros_like(uR)
+    SK.launch('flux', gv, blk, uL, uR, cvx, jL, jR)
+    ux = np.zeros_like(u)
+    LK.launch('eDeriv', gv, blk, cvx, u, ux)
+    SK.launch('totalFlux', gv, blk, ux, cvx, jL, jR)
+    SK.launch('mul_by_invjac', gv, blk, ux)
+    rhs = mm(b._B.T, ux)
+    return dict(u=u, rhs=rhs, K=K, Ne=Ne, Nv=Nv, cv=vm.cv(), cw=vm.cw(),
+                invjac=invjac.ravel(), derivMat=b.derivMat,
+                f0L=walls['L'][1], f0R=walls['R'][1])
+
+
 def golden_moments(R, Nv=8, Ne=4, K=3):
     """Bulk moments of the reference's writers: DGFSMomWriterStd and
     DGFSMomWriterBi ``_compute_moments_1D`` (std/moments.py:11-70,
@@ -966,6 +1041,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'limiter_N4.npz'), **golden_limiter(R))
     np.savez_compressed(os.path.join(HERE, 'moments_N8.npz'), **golden_moments(R))
     np.savez_compressed(os.path.join(HERE, 'upwind_N8.npz'), **golden_upwind(R))
+    np.savez_compressed(os.path.join(HERE, 'entropy_N8.npz'), **golden_entropy(R))
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith('.npz'):
             print(fn, os.path.getsize(os.path.join(HERE, fn)), 'bytes')
@@ -979,6 +1055,11 @@ def limiter():
 def upwind():
     R = _import_reference()
     np.savez_compressed(os.path.join(HERE, 'upwind_N8.npz'), **golden_upwind(R))
+
+
+def entropy():
+    R = _import_reference()
+    np.savez_compressed(os.path.join(HERE, 'entropy_N8.npz'), **golden_entropy(R))
 
 
 def moments():
@@ -1003,5 +1084,7 @@ if __name__ == '__main__':
         moments()
     elif sys.argv[1:] == ['upwind']:
         upwind()
+    elif sys.argv[1:] == ['entropy']:
+        entropy()
     else:
         main()

@@ -57,3 +57,22 @@ def test_positivity_limiter_matches_reference_kernel():
     ref = z['wpos_lim'].reshape(got.shape)
     assert np.abs(got - ref).max() <= 1e-14 * np.abs(ref).max()
     assert np.abs(ref - w).max() > 0            # the limiter acted
+
+
+def test_entropy_stable_rhs_matches_reference_kernels():
+    z = np.load(os.path.join(G, 'entropy_N8.npz'))
+    K, Ne, Nv = int(z['K']), int(z['Ne']), int(z['Nv'])
+    b = odg.NodalBasis('nodal-sem-gll', K, K)
+    assert np.allclose(b.derivMat, z['derivMat'], rtol=0, atol=1e-13)
+    cv, cw = z['cv'], float(z['cw'])
+    bcl = odg.WallDiffuseBC(cv, cw, 1.0, [0, -0.1, 0], -1.)
+    bcr = odg.WallDiffuseBC(cv, cw, 1.0, [0, 0.1, 0], 1.)
+    bcl.f0, bcr.f0 = z['f0L'], z['f0R']
+    u = z['u'].reshape(K, Ne, Nv ** 3)
+    got = odg.dg_rhs_entropy(b, z['invjac'], cv[0], bcl, bcr, u)
+    ref = z['rhs'].reshape(got.shape)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    # both branches of the logarithmic mean occur
+    xi = np.abs(u[0] / u[1])
+    fu = ((xi - 1) / (xi + 1)) ** 2
+    assert (fu < 1e-2).any() and (fu >= 1e-2).any()
