@@ -65,3 +65,21 @@ def test_remaining_steps():
     assert remaining_steps(0.5, 1.0, 0.25) == 2
     assert remaining_steps(0.1 + 0.2, 0.3, 0.1) == 0
     assert remaining_steps(1.0, 1.0, 0.1) == 0
+
+
+def test_command_line_parsing(tmp_path):
+    """``python -m dgfs1d_gpu_b200 <driver> run|restart ini [dist] -v s::k v``
+    (the reference's console-script interface) parses and applies overrides."""
+    from dgfs1d_gpu_b200.__main__ import parse
+    from dgfs1d_gpu_b200.configs import couette_std_ini
+    ini = tmp_path / 'c.ini'
+    ini.write_text(couette_std_ini())
+    a = parse(['dgfsStd1D', 'run', str(ini), '-v', 'mesh::Ne', '6',
+               '-v', 'time-integrator::scheme', 'ssp-rk2'])
+    cfg = Config.load(a.inp, defaults=Config.overrides(a.v))
+    assert cfg.lookupint('mesh', 'Ne') == 6
+    assert cfg.lookup('time-integrator', 'scheme') == 'ssp-rk2'
+    b = parse(['dgfsABUstd1D', 'restart', str(ini), 'd.npz_rank=0'])
+    assert b.cmd == 'restart' and b.dist == ['d.npz_rank=0']
+    with pytest.raises(SystemExit):
+        parse(['dgfsNope1D', 'run', str(ini)])

@@ -108,3 +108,32 @@ def test_boundary_states():
         cfg3 = _ini('[soln-ics]\ntype = maxwellian\nrho = 1\nT = 273\nux = 0\nuy = 0\nuz = 0\n',
                     '[soln-bcs-xlo]\ntype = %s\n' % kind)
         assert get_bc(cfg3, 'soln-bcs-xlo', 0.0, -1., vm).type == kind
+
+
+def test_bi_maxwellian_expr():
+    from dgfs1d_gpu_b200.bi.initcond import get_initcond as get_bi
+    from dgfs1d_gpu_b200.configs import couette_bi_ini
+    from dgfs1d_gpu_b200.velocitymesh import DGFSVelocityMeshBi
+    base = couette_bi_ini(Nv=24, Nrho=4).split('[soln-ics]')[0]
+    cfg0 = Config(base + '[soln-ics]\ntype = maxwellian\nnden1 = 1\nnden2 = 1\n'
+                  'T = 273\nux = 0\nuy = 0\nuz = 0\n')
+    vm = DGFSVelocityMeshBi(cfg0)
+    n0, u0, T0 = float(vm.n0()), float(vm.u0()), float(vm.T0())
+    ics = ('[soln-ics]\ntype = maxwellian-expr\nnden1 = %r*(1 + 0.1*x)\n'
+           'nden2 = %r*0.5\nux = 0\nuy = %r*0.05*sin(pi*x)\nuz = 0\n'
+           'T = %r*(1 + 0.02*x)\n' % (n0, n0, u0, T0))
+    cfg = Config(base + ics)
+    ic = get_bi(cfg, vm, 'soln-ics')
+    xs = _xsol()
+    for p, m in enumerate(vm.masses()):
+        u = np.empty((3, 4, vm.vsize()))
+        ic.apply_init_vals(p, u, 3, 4, xs)
+        for q in range(3):
+            for e in range(4):
+                x = xs[q, e]
+                nd = (1 + 0.1 * x) if p == 0 else 0.5
+                T = 1 + 0.02 * x
+                c2 = np.sum((vm.cv() - np.array([0, 0.05 * math.sin(math.pi * x), 0])
+                             .reshape(3, 1)) ** 2, axis=0)
+                ref = nd * (m / np.pi / T) ** 1.5 * np.exp(-m * c2 / T)
+                assert np.allclose(u[q, e], ref, rtol=1e-12, atol=0)

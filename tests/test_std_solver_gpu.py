@@ -310,3 +310,30 @@ def test_std_expression_ics_and_boundaries_match_oracle(case):
     if case == 'cyclic-wallexpr':
         with pytest.raises(ValueError, match='time-dependent'):
             s.capture_step()
+
+
+def test_command_line_run_and_restart(tmp_path, capsys):
+    """``python -m dgfs1d_gpu_b200 dgfsStd1D run|restart``: a run that writes
+    moments and a checkpoint, then a restart from that checkpoint that ends
+    where the uninterrupted run ends."""
+    from dgfs1d_gpu_b200 import build
+    build.build()
+    from dgfs1d_gpu_b200.__main__ import main
+    ini = couette_std_ini(Nv=8, Nrho=4, nsteps=4)
+    dt = Config(ini).lookupfloat('time-integrator', 'dt')
+    ini += ('\n[dgfsmomwriter]\nbasedir = %s\nbasename = m-{t:.6f}\ndt-out = %.17g\n'
+            '[dgfsdistwriter]\nbasedir = %s\nbasename = d-{t:.6f}\ndt-out = %.17g\n'
+            % (tmp_path, 2 * dt, tmp_path, 2 * dt))
+    p = tmp_path / 'run.ini'
+    p.write_text(ini)
+    s = main(['dgfsStd1D', 'run', str(p)])
+    out = capsys.readouterr().out
+    assert 'Nsteps 4' in out and 'elapsed time' in out
+    names = sorted(x.name for x in tmp_path.iterdir())
+    assert sum(n.startswith('m-') for n in names) == 3       # t = 0, 2dt, 4dt
+    dist = sorted(n for n in names if n.startswith('d-'))
+    assert len(dist) == 2
+    r = main(['dgfsStd1D', 'restart', str(p), str(tmp_path / dist[0]),
+              '-v', 'dgfsdistwriter::basename', 'r-{t:.6f}'])
+    assert r.nsteps == 2
+    assert _rel(r.u.cpu().numpy(), s.u.cpu().numpy()) < 1e-14
