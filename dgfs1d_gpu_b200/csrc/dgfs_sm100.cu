@@ -164,7 +164,8 @@ static int c64_of(int N) {
     case 16: return 2;
     case 24: return 4;
     case 32: return 8;
-    default: return 0;  // N=48: no FP64 terms kernel (three FP64 slabs do not fit)
+    case 48: return 16;  // FP64 sums in global memory (vhs_terms_fp64g_kernel)
+    default: return 0;
   }
 }
 static int c32_of(int N) {
@@ -186,8 +187,9 @@ template <> struct VhsClusters<8> { static constexpr int c64 = 1, c32 = 1, cpro 
 template <> struct VhsClusters<16> { static constexpr int c64 = 2, c32 = 1, cpro = 2, cepi = 2; };
 template <> struct VhsClusters<24> { static constexpr int c64 = 4, c32 = 3, cpro = 4, cepi = 4; };
 template <> struct VhsClusters<32> { static constexpr int c64 = 8, c32 = 4, cpro = 8, cepi = 16; };
-// N=48 (FP32 mode only): 16-CTA clusters of 3 planes
-template <> struct VhsClusters<48> { static constexpr int c64 = 0, c32 = 16, cpro = 16, cepi = 16; };
+// N=48: 16-CTA clusters of 3 planes; the FP64 terms kernel keeps its running
+// sums in global memory (three FP64 slabs would need 331 KB per CTA)
+template <> struct VhsClusters<48> { static constexpr int c64 = 16, c32 = 16, cpro = 16, cepi = 16; };
 
 static size_t slab_bytes(int N, int C, size_t elem) {
   return (size_t)(N / C) * N * (N + 1) * elem;
@@ -550,12 +552,23 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
       VhsTermsArgs a{};
       a.Fg = h->Fg; a.ph = h->ph; a.uv = nullptr; a.mult = h->mult;
       a.b1w = h->b1w64; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
-      const size_t smem = 3 * slab_bytes(N, C64, sizeof(double2)) +
-                          9 * N * sizeof(double2);
-      if ((rc = launch_cluster(vhs_terms_kernel<double, N, C64, false>,
-                               dim3(C64, h->Nrho, nevals), dim3(G64::NT), C64,
-                               smem, st, a)))
-        return rc;
+      constexpr size_t kSmemMax = 232448;  // 227 KB per CTA
+      constexpr size_t smem3 = 3 * (size_t)G64::SLAB * sizeof(double2) +
+                               9 * N * sizeof(double2);
+      if constexpr (smem3 <= kSmemMax) {
+        if ((rc = launch_cluster(vhs_terms_kernel<double, N, C64, false>,
+                                 dim3(C64, h->Nrho, nevals), dim3(G64::NT), C64,
+                                 smem3, st, a)))
+          return rc;
+      } else {
+        constexpr size_t smem2 = 2 * (size_t)G64::SLAB * sizeof(double2) +
+                                 3 * N * sizeof(double2);
+        static_assert(smem2 <= kSmemMax, "FP64 terms slabs exceed shared memory");
+        if ((rc = launch_cluster(vhs_terms_fp64g_kernel<N, C64>,
+                                 dim3(C64, h->Nrho, nevals), dim3(G64::NT), C64,
+                                 smem2, st, a)))
+          return rc;
+      }
     } else {
       return fail(DGFS_ERR_UNSUPPORTED, "no FP64 terms kernel at this N");
     }

@@ -652,6 +652,120 @@ vhs_terms_kernel(VhsTermsArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// FP64 terms for grids whose three FP64 slabs do not fit in shared memory
+// (N = 48: 16-CTA clusters of three planes; the transform slab A and the
+// receive slab take 225.8 KB of the 227 KB).  Same algorithm as
+// vhs_terms_kernel<double, N, C, false>, but each thread's running sum
+// S_p(x, y, z) over the sphere directions lives in global memory at
+// Sg[x * NT + t] (coalesced across the CTA) inside this CTA's own block of H,
+// which the CTA reads back once before the final transform and overwrites
+// with the output only after the cluster barrier that follows.
+// ---------------------------------------------------------------------------
+template <int N, int C>
+__global__ void __launch_bounds__(Geo<N, C>::NT, 1)
+vhs_terms_fp64g_kernel(VhsTermsArgs a) {
+  using G = Geo<N, C>;
+  using R = double;
+  using T = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);
+  T* Rb = A + G::SLAB;
+  T* tab = Rb + G::SLAB;            // [3][N] phase
+  const int t = threadIdx.x;
+  const unsigned rank = cluster_rank();
+  const int p = blockIdx.y, e = blockIdx.z;
+  const T* Fg = static_cast<const T*>(a.Fg) + (size_t)e * G::n;
+  const T* ph = static_cast<const T*>(a.ph);
+  T* H = static_cast<T*>(a.H) + ((size_t)e * a.Nrho + p) * G::n +
+         (size_t)rank * G::P * N * N;
+  T* Sg = H;                        // running sums, then the output block
+  for (int x = 0; x < N; ++x) Sg[(size_t)x * G::NT + t] = T{0, 0};
+
+  bool first = true;
+  for (int q = 0; q < a.Mu; ++q) {
+    __syncthreads();  // previous term's table readers are done
+    for (int i = t; i < 3 * N; i += G::NT)
+      tab[i] = ph[((size_t)p * a.Mu + q) * 3 * N + i];
+    __syncthreads();
+    const R mq = a.mult[q];
+#pragma unroll 1
+    for (int s = 0; s < 2; ++s) {
+      // z-pass: multiplier cos/sin of a(l), inverse FFT along z
+      {
+        const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
+        const T bxy = cmul(tab[lx], tab[N + ly]);
+        T v[N];
+        const T* row = Fg + ((size_t)lx * N + ly) * N;
+#pragma unroll
+        for (int k = 0; k < N; ++k) v[k] = row[k];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const T ph3 = cmul(bxy, tab[2 * N + k]);
+          const R m = s == 0 ? ph3.x : ph3.y;
+          v[k].x *= m;
+          v[k].y *= m;
+        }
+        fft<R, N, +1>(v);
+        const int base = pl * G::PLANE + ly * G::ROW;
+#pragma unroll
+        for (int k = 0; k < N; ++k) A[base + k] = v[k];
+      }
+      __syncthreads();
+      {
+        T v[N];
+        slab_col_load_fft<R, N, C, +1>(A, t, v);
+        if (!first) cluster_wait();  // receive buffers are free
+        push_cols_to_yslab<R, N, C>(Rb, t, rank, v);
+      }
+      first = false;
+      cluster_arrive();
+      cluster_wait();
+      T v[N];
+      yslab_load_pencil<R, N, C>(Rb, t, v);
+      cluster_arrive();  // done reading the receive buffer
+      fft<R, N, +1>(v);
+#pragma unroll
+      for (int x = 0; x < N; ++x) {
+        const T h = cmul(v[x], v[x]);
+        T sv = Sg[(size_t)x * G::NT + t];
+        sv.x += mq * h.x;
+        sv.y += mq * h.y;
+        Sg[(size_t)x * G::NT + t] = sv;
+      }
+    }
+  }
+
+  // forward FFT of S_p: x-pass, exchange into X-slabs, y-pass, z-pass
+  T v[N];
+#pragma unroll
+  for (int x = 0; x < N; ++x) v[x] = Sg[(size_t)x * G::NT + t];
+  fft<R, N, -1>(v);
+  if (!first) cluster_wait();
+  push_pencils_to_xslab<R, N, C>(A, t, rank, v);
+  cluster_arrive();
+  cluster_wait();
+  {
+    T w[N];
+    slab_col_load_fft<R, N, C, -1>(A, t, w);
+    const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+    for (int k = 0; k < N; ++k) A[base + k * G::ROW] = w[k];
+  }
+  __syncthreads();
+  slab_row_pass<R, N, C, -1>(A, t);
+  __syncthreads();
+  const R* b1w = static_cast<const R*>(a.b1w) + (size_t)p * G::n +
+                 (size_t)rank * G::P * N * N;
+  for (int j = t; j < G::P * N * N; j += G::NT) {
+    T hv = A[slab_index<N, C>(j)];
+    const R w = b1w[j];
+    hv.x *= w;
+    hv.y *= w;
+    H[j] = hv;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Terms, FP32 Maxwellian-split path with packed real transforms.
 //
 // g = f - M is real, so F_g is Hermitian.  With the phase a(l) = kappa.l the
