@@ -86,6 +86,23 @@ def read_distribution(path, names, K, Ne, Nv):
     return out, time
 
 
+def read_dataset(path, name='coeff'):
+    """(flat array, {time, K, Ne, Nv}) of one dataset, without checks."""
+    with open(path, 'rb') as fh:
+        magic = fh.read(8)
+    if magic == b'\x89HDF\r\n\x1a\n':
+        h5 = _h5py()
+        if h5 is None:
+            raise RuntimeError('%s is an HDF5 file and h5py is not available'
+                               % path)
+        with h5.File(path, 'r') as f:
+            d = f[name]
+            return np.asarray(d[:]), {a: d.attrs[a] for a in ATTRS}
+    with np.load(path) as z:
+        return (np.asarray(z[name]),
+                {a: z['%s.%s' % (name, a)][()] for a in ATTRS})
+
+
 def remaining_steps(t, tf, dt):
     """Steps of size dt left from t to tf (the drivers loop while t < tf)."""
     import math

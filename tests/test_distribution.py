@@ -83,3 +83,41 @@ def test_command_line_parsing(tmp_path):
     assert b.cmd == 'restart' and b.dist == ['d.npz_rank=0']
     with pytest.raises(SystemExit):
         parse(['dgfsNope1D', 'run', str(ini)])
+
+
+def test_grid_convergence_error(tmp_path):
+    """dgfsStdError1D on two checkpoints (Ne and 2 Ne elements): zero for a
+    polynomial the nodal basis holds exactly, the restated L1 norm for a
+    non-polynomial profile, and the element-count check."""
+    from dgfs1d_gpu_b200.error import compute_error
+    from dgfs1d_gpu_b200.quadrature import gauss_lobatto_jacobi, lagrange_at
+    K, Nv = 3, 5
+    z, w = gauss_lobatto_jacobi(K)
+
+    def field(Ne, fn):
+        x = np.linspace(0, 1, Ne + 1)
+        xs = np.array([0.5 * (x[j] + x[j + 1]) + 0.5 * (x[j + 1] - x[j]) * z
+                       for j in range(Ne)]).T                   # (K, Ne)
+        amp = np.arange(1, Nv + 1, dtype=float)
+        return fn(xs)[:, :, None] * amp[None, None, :]
+
+    def save(name, u):
+        p = str(tmp_path / name)
+        write_distribution(p, {'coeff': u.ravel()}, 0.0, K, u.shape[1], Nv)
+        return p
+    quad = lambda x: 1 + x - 2 * x ** 2
+    assert compute_error(save('a', field(4, quad)), save('b', field(8, quad))) < 1e-15
+    f = lambda x: np.sin(3 * x)
+    u1, u2 = field(4, f), field(8, f)
+    err = compute_error(save('c', u1), save('d', u2))
+    # restated: coarse interpolant at the fine nodes vs the fine values
+    r2 = np.concatenate((-np.flip(z * 0.5 + 0.5), z * 0.5 + 0.5))
+    im = lagrange_at(z, r2)
+    ref = 0.0
+    for j in range(4):
+        fine = np.concatenate((u2[:, 2 * j], u2[:, 2 * j + 1]), axis=0)  # (2K, Nv)
+        d = np.abs(im @ u1[:, j] - fine)
+        ref += 0.5 * (w @ d[:K]).sum() + 0.5 * (w @ d[K:]).sum()
+    assert err > 0 and abs(err - ref / 8 / Nv) < 1e-15
+    with pytest.raises(ValueError, match='2 \\*'):
+        compute_error(save('e', u1), save('f', field(12, f)))
