@@ -1,7 +1,7 @@
 """Penalised IMEX time integrators (``[time-integrator] scheme``).
 
-Keys and coefficients of dgfs1D/astd/integrator.py: ``bdf-111`` / ``bdf-222``
-(penalty model only, explicit DG advection; :281-400), ``boltz-ars-111``
+Keys and coefficients of dgfs1D/astd/integrator.py: ``bdf-111`` / ``bdf-222`` /
+``bdf-333`` (penalty model only, explicit DG advection; :281-488), ``boltz-ars-111``
 (explicit Boltzmann operator and penalty, :491-552) and ``imex-lm-bdf1`` /
 ``imex-lm-bdf2`` and the other ``imex-lm-*`` schemes (cn2, ad2, sg2, bdf3,
 ad3, tvb3, bdf4, tvb4, shu3, shu4; explicit L + Q - P, implicit P(f^{n+1});
@@ -101,11 +101,15 @@ class BoltzARS111IntegratorAstd(DGFSIntegratorAstd):
         self._sm.implicit(U, rhs, f, 1.0, dt)
 
 
-class Bdf222IntegratorAstd(DGFSIntegratorAstd):
-    intg_kind = 'bdf-222'
-    A = [1. / 3., -4. / 3., 1.]
-    G = [-2. / 3., 4. / 3.]
-    B = 2. / 3.
+class BdfIntegratorAstd(DGFSIntegratorAstd):
+    """k-level BDF penalty schemes (astd/integrator.py:325-488): with levels
+    n-k+1 .. n, U = sum_i (-A_i U_i + G_i dt LU_i) / A_k relaxed with
+    (A_k, B dt), then f = (sum_i (-A_i f_i + G_i dt L_i) + B dt nu M(U)) /
+    (A_k + B dt nu).  Levels 1 .. k-1 come from nsub first-order substeps
+    each, one level per step (the reference uses ARS-222 substeps and, for
+    bdf-333, computes two levels in its first step)."""
+    intg_kind = None
+    A = G = B = None
 
     def _state(self, t, f):
         L = self._z()
@@ -113,26 +117,41 @@ class Bdf222IntegratorAstd(DGFSIntegratorAstd):
         return dict(F=f.clone(), U=self._mom(f), L=L, LU=self._mom(L))
 
     def integrate(self, t, dt, nacptsteps, f):
-        a1, a2, a3 = self.A
-        g1, g2 = self.G
-        if nacptsteps == 0:
-            f0 = f.clone()
+        A, G, B = self.A, self.G, self.B
+        k = len(G)
+        if nacptsteps < k - 1:
+            if nacptsteps == 0:
+                self.hist = [self._state(t, f)]
             sub = Bdf111IntegratorAstd(self._explicit, self._sm, self.shape,
                                        self.dtype, device=self.device)
             for i in range(self.nsub):
                 sub.integrate(t + i * dt / self.nsub, dt / self.nsub, i, f)
-            self.hist = [self._state(t, f0), self._state(t + dt, f)]
+            self.hist.append(self._state(t + dt, f))
             return
-        h0, h1 = self.hist
+        hs = self.hist
         U = self._zm()
-        _lin(U, [(-a1 / a3, h0['U']), (g1 * dt / a3, h0['LU']),
-                 (-a2 / a3, h1['U']), (g2 * dt / a3, h1['LU'])])
-        self._sm.relax(U, a3, self.B * dt)
+        _lin(U, [p for i in range(k) for p in (
+            (-A[i] / A[k], hs[i]['U']), (G[i] * dt / A[k], hs[i]['LU']))])
+        self._sm.relax(U, A[k], B * dt)
         rhs = self._z()
-        _lin(rhs, [(-a1, h0['F']), (g1 * dt, h0['L']), (-a2, h1['F']),
-                   (g2 * dt, h1['L'])])
-        self._sm.implicit(U, rhs, f, a3, self.B * dt)
-        self.hist = [h1, self._state(t + dt, f)]
+        _lin(rhs, [p for i in range(k) for p in (
+            (-A[i], hs[i]['F']), (G[i] * dt, hs[i]['L']))])
+        self._sm.implicit(U, rhs, f, A[k], B * dt)
+        self.hist = hs[1:] + [self._state(t + dt, f)]
+
+
+class Bdf222IntegratorAstd(BdfIntegratorAstd):
+    intg_kind = 'bdf-222'
+    A = [1. / 3., -4. / 3., 1.]
+    G = [-2. / 3., 4. / 3.]
+    B = 2. / 3.
+
+
+class Bdf333IntegratorAstd(BdfIntegratorAstd):
+    intg_kind = 'bdf-333'
+    A = [-2. / 11., 9. / 11., -18. / 11., 1.]
+    G = [6. / 11., -18. / 11., 18. / 11.]
+    B = 6. / 11.
 
 
 class IMEXLMIntegratorAstd(DGFSIntegratorAstd):

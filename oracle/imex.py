@@ -5,7 +5,7 @@ dgfs1D/astd/kernels/scattering/bgk-direct-gll.mako (cmaxwellian :118-153,
 collide :157-181, updateMom{q}_BDF :16-42, updateDistribution{q}_BDF
 :46-78, updateMom{q}_LM :327-351, updateDistribution{q}_LM :354-405); the
 schemes restate dgfs1D/astd/integrator.py (bdf-111 :281-322, bdf-222
-:325-400, boltz-ars-111 :491-552, IMEX-LM :623-792).  Start-up steps of the multi-step schemes use
+:325-400, bdf-333 :401-488, boltz-ars-111 :491-552, IMEX-LM :623-792).  Start-up steps of the multi-step schemes use
 first-order substeps of the same family (the reference uses ARS-222/443
 substeps); ``imex-lm-*`` does not stop after its first step (astd/
 integrator.py:732 exits the process there).
@@ -191,6 +191,12 @@ def model_implicit(model, U, rhs, cv, adiv, cdt, prefac, omega):
 
 
 # (A, B, C) of the IMEX linear multistep schemes, astd/integrator.py:736-907
+BDF_COEF = {
+    'bdf-222': ([1. / 3., -4. / 3., 1.], [-2. / 3., 4. / 3.], 2. / 3.),
+    'bdf-333': ([-2. / 11., 9. / 11., -18. / 11., 1.], [6. / 11., -18. / 11., 18. / 11.],
+                6. / 11.),
+}
+
 LM_COEF = {
     'imex-lm-bdf1': ([-1.], [1.], [1., 0.]),
     'imex-lm-bdf2': ([-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]),
@@ -237,14 +243,17 @@ class IMEX:
         self.shape = f0.shape
         self.step_no = 0
         self.starts = []
-        if kind == 'bdf-222':
+        if kind in BDF_COEF:
+            k = len(BDF_COEF[kind][1])
             f = f0.copy()
             helper = IMEX('bdf-111', explicit, boltz, cv, cw, prefac, omega,
                           dt / nsub, f0, model=self.model)
-            for _ in range(nsub):
-                f = helper.step(f)
-            self.starts = [f]
-            self.hist = [self._bdf_state(f0), self._bdf_state(f)]
+            self.hist = [self._bdf_state(f0)]
+            for _ in range(k - 1):
+                for _ in range(nsub):
+                    f = helper.step(f)
+                self.starts.append(f.copy())
+                self.hist.append(self._bdf_state(f))
         elif kind in LM_COEF:
             s = len(LM_COEF[kind][0])
             self.hist = [self._state(f0)]
@@ -303,21 +312,21 @@ class IMEX:
             U = self._relax(-((-1.) * U0 + (-1.) * dt * LU0) / 1., 1., dt)
             rhs = -((-1.) * f + (-1.) * dt * L0)
             return self._implicit(U, rhs, 1., dt)
-        if k == 'bdf-222':
-            a1, a2, a3 = 1. / 3., -4. / 3., 1.
-            g1, g2 = -2. / 3., 4. / 3.
-            b = 2. / 3.
-            if self.step_no == 0:
+        if k in BDF_COEF:
+            # integrator.py:325-488 (updateMom{q}_BDF, updateDistribution{q}_BDF)
+            A, G, b = BDF_COEF[k]
+            q = len(G)
+            if self.step_no < q - 1:
                 self.step_no += 1
-                return self.starts[0].copy()
-            h0, h1 = self.hist
-            U = -(a1 * h0['U'] + (-g1) * dt * h0['LU'] + a2 * h1['U']
-                  + (-g2) * dt * h1['LU']) / a3
-            U = self._relax(U, a3, b * dt)
-            rhs = -(a1 * h0['F'] + (-g1) * dt * h0['L'] + a2 * h1['F']
-                    + (-g2) * dt * h1['L'])
-            fn = self._implicit(U, rhs, a3, b * dt)
-            self.hist = [h1, self._bdf_state(fn)]
+                return self.starts[self.step_no - 1].copy()
+            hs = self.hist
+            U = -sum(A[i] * hs[i]['U'] + (-G[i]) * dt * hs[i]['LU']
+                     for i in range(q)) / A[q]
+            U = self._relax(U, A[q], b * dt)
+            rhs = -sum(A[i] * hs[i]['F'] + (-G[i]) * dt * hs[i]['L']
+                       for i in range(q))
+            fn = self._implicit(U, rhs, A[q], b * dt)
+            self.hist = hs[1:] + [self._bdf_state(fn)]
             self.step_no += 1
             return fn
         if k in LM_COEF:
