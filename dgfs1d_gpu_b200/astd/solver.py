@@ -16,6 +16,7 @@ from ..dg import DGOperator
 from ..distribution import (DGFSDistributionWriter, read_distribution,
                             remaining_steps)
 from ..mesh import Mesh
+from ..nancheck import DGFSNaNCheck
 from ..plugins import subclass_where
 from ..std.bc import get_bc
 from ..std.initcond import get_initcond
@@ -84,6 +85,7 @@ class DGFSABstd1D:
         self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, self.xsol,
                                         tcurr=self.t, coeff=self.u)
         self.distribution = DGFSDistributionWriter(ti, (K, Ne, Nv), cfg)
+        self.nancheck = DGFSNaNCheck(cfg)
         self.residual = DGFSResidualStd(cfg, self.dg)
         self.uprev = self.u.clone()
         # linear slope limiter after every step (abstd.py:459, 476)
@@ -120,6 +122,7 @@ class DGFSABstd1D:
         self.residual(self.t, self.nacptsteps, self.u, self.uprev)
         self.moments(self.dt, self.t, self.u)
         self.distribution(self.dt, self.t, self.u)
+        self.nancheck(self.t, self.nacptsteps, [self.u])
         self.uprev.copy_(self.u)
 
     def run(self, nsteps=None):

@@ -14,6 +14,7 @@ from ..dg import DGOperator
 from ..distribution import (DGFSDistributionWriter, read_distribution,
                             remaining_steps)
 from ..mesh import Mesh
+from ..nancheck import DGFSNaNCheck
 from ..plugins import subclass_where
 from ..velocitymesh import DGFSVelocityMeshBi
 from .bc import get_bc
@@ -81,6 +82,7 @@ class DGFSBi1D:
         self.residual = DGFSResidualBi(cfg, self.dgs)
         self.distribution = DGFSDistributionWriter(ti, (K, Ne, Nv), cfg,
                                                    nspcs=ns)
+        self.nancheck = DGFSNaNCheck(cfg)
 
     def rhs(self, p, t, us, out):
         for side, bc in enumerate((self.bcl, self.bcr)):
@@ -98,6 +100,7 @@ class DGFSBi1D:
         self.residual(self.t, self.nacptsteps, self.uprevs, self.us)
         self.moments(self.dt, self.t, self.us)
         self.distribution(self.dt, self.t, self.us)
+        self.nancheck(self.t, self.nacptsteps, self.us)
         for a, b in zip(self.uprevs, self.us):
             a.copy_(b)
 

@@ -17,6 +17,7 @@ from ..dg import DGOperator
 from ..distribution import (DGFSDistributionWriter, read_distribution,
                             remaining_steps)
 from ..mesh import Mesh
+from ..nancheck import DGFSNaNCheck
 from ..plugins import subclass_where
 from ..velocitymesh import DGFSVelocityMeshStd
 from .bc import get_bc
@@ -82,6 +83,7 @@ class DGFSStd1D:
         self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, xcoeff,
                                         tcurr=self.t, coeff=self.u)
         self.distribution = DGFSDistributionWriter(ti, (K, Ne, Nv), cfg)
+        self.nancheck = DGFSNaNCheck(cfg)
         if cfg.has_section('dgfsdistslicewriter'):
             self.distributionslice = DGFSDistributionSliceStd(
                 ti, (K, Ne, Nv), basis.interpMat, vm, cfg)
@@ -144,6 +146,7 @@ class DGFSStd1D:
         self.residual(self.t, self.nacptsteps, self.u, self.uprev)
         self.moments(self.dt, self.t, self.u)
         self.distribution(self.dt, self.t, self.u)
+        self.nancheck(self.t, self.nacptsteps, [self.u])
         self.distributionslice(self.dt, self.t, self.u)
         self.uprev.copy_(self.u)
 

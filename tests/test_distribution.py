@@ -121,3 +121,17 @@ def test_grid_convergence_error(tmp_path):
     assert err > 0 and abs(err - ref / 8 / Nv) < 1e-15
     with pytest.raises(ValueError, match='2 \\*'):
         compute_error(save('e', u1), save('f', field(12, f)))
+
+
+def test_nan_check():
+    """[dgfsnancheck] nsteps: a NaN in any solution array raises at the
+    checked steps only (CPU tensors; the drivers pass their device arrays)."""
+    import torch
+    from dgfs1d_gpu_b200.nancheck import DGFSNaNCheck
+    chk = DGFSNaNCheck(Config('[dgfsnancheck]\nnsteps = 2\n'))
+    good, bad = torch.ones(4), torch.tensor([1.0, float('nan')])
+    chk(0.1, 1, [good, bad])                       # not a checked step
+    chk(0.2, 2, [good])
+    with pytest.raises(RuntimeError, match='NaNs detected at t = 0.2'):
+        chk(0.2, 2, [good, bad])
+    DGFSNaNCheck(Config('[x]\na = 1\n'))(0.0, 2, [bad])   # section absent: off
