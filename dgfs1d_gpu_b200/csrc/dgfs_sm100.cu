@@ -9,6 +9,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/dgfs_sm100.h"
 #include "fft_reg.cuh"
 #include "cluster_slab.cuh"
@@ -17,6 +19,13 @@
 #include "vss_kernels.cuh"
 
 using namespace dgfs;
+
+// NVTX range over an entry point (host side: the launches it issues), for
+// nsys / ncu --nvtx; free when no tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 // ---------------------------------------------------------------------------
 // errors
@@ -600,6 +609,7 @@ extern "C" int dgfs_vhs_eval(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
                              const int32_t* src_slots, int32_t src_base,
                              const int32_t* dst_slots, int32_t dst_base,
                              int32_t nevals, void* stream) {
+  NvtxRange nvtx_range("dgfs_vhs_eval");
   if (!h) return fail(DGFS_ERR_INVALID, "null handle");
   if (nevals < 0) return fail(DGFS_ERR_INVALID, "negative nevals");
   if (nevals == 0) return DGFS_OK;
@@ -1036,6 +1046,7 @@ extern "C" int dgfs_dg_destroy(dgfs_dg_handle h) {
 
 extern "C" int dgfs_dg_advect(dgfs_dg_handle h, const void* u, void* ux,
                               int32_t dtype, void* stream) {
+  NvtxRange nvtx_range("dgfs_dg_advect");
   if (!h || !u || !ux) return fail(DGFS_ERR_INVALID, "null argument");
   if (dtype != DGFS_F32 && dtype != DGFS_F64)
     return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
@@ -1455,6 +1466,7 @@ extern "C" int dgfs_vss_eval(dgfs_vss_handle h, int32_t p, int32_t q,
                              const int32_t* src_slots, int32_t src_base,
                              const int32_t* dst_slots, int32_t dst_base,
                              int32_t nevals, void* stream) {
+  NvtxRange nvtx_range("dgfs_vss_eval");
   if (!h) return fail(DGFS_ERR_INVALID, "null handle");
   if (p < 0 || q < 0 || p >= h->nspcs || q >= h->nspcs)
     return fail(DGFS_ERR_INVALID, "species index out of range");
@@ -2214,6 +2226,7 @@ extern "C" int dgfs_fno_eval(dgfs_fno_handle h, const void* f, int32_t f_dtype,
                              void* Q, int32_t q_dtype, const int32_t* src_slots,
                              int32_t src_base, const int32_t* dst_slots,
                              int32_t dst_base, int32_t nevals, void* stream) {
+  NvtxRange nvtx_range("dgfs_fno_eval");
   if (!h) return fail(DGFS_ERR_INVALID, "null handle");
   if (nevals < 0 || src_base < 0 || dst_base < 0)
     return fail(DGFS_ERR_INVALID, "negative count or slot base");
