@@ -3,7 +3,7 @@
     python -m dgfs1d_gpu_b200 dgfsStd1D run cfg.ini [-v mesh::Ne 8 ...]
     python -m dgfs1d_gpu_b200 dgfsStd1D restart cfg.ini dist.npz_rank=0 [-v ...]
 
-Drivers: dgfsStd1D, dgfsBi1D, dgfsABstd1D, dgfsABUstd1D, dgfsABE2std1D
+Drivers: dgfsStd1D, dgfsBi1D, dgfsAstd1D, dgfsABstd1D, dgfsABUstd1D, dgfsABE2std1D
 (setup.py:91-107 of the reference; each there is ``<driver> run|restart``,
 dgfs1D/initialize.py:7-50).  ``-v section::key value`` overrides an INI
 value.  One rank: ``restart`` takes one distribution file.  The run marches
@@ -19,6 +19,7 @@ from .config import Config
 DRIVERS = {
     'dgfsStd1D': ('std.solver', 'DGFSStd1D'),
     'dgfsBi1D': ('bi.solver', 'DGFSBi1D'),
+    'dgfsAstd1D': ('astd.solver', 'DGFSAstd1D'),
     'dgfsABstd1D': ('astd.solver', 'DGFSABstd1D'),
     'dgfsABUstd1D': ('astd.solver', 'DGFSABUstd1D'),
     'dgfsABE2std1D': ('astd.solver', 'DGFSABE2std1D'),

@@ -39,12 +39,7 @@ class DGFSABstd1D:
         K = basis.K
         self.vm = vm = DGFSVelocityMeshStd(cfg)
         Nv = vm.vsize()
-        smcls = subclass_where(DGFSScatteringModelStd, scattering_model=cfg.lookup(
-            'scattering-model', 'type'))
-        self.sm = smcls(cfg, vm, Ne=Ne, max_evals=K * Ne)
-        pcls = subclass_where(DGFSScatteringModelAstd, scattering_model=cfg.lookup(
-            'penalized-scattering-model', 'type'))
-        self.psm = pcls(cfg, vm, Ne=Ne, eps=self.sm.prefac)
+        self._make_models(cfg, vm, Ne, K)
         ti, dt, tf = cfg.lookupfloats('time-integrator', ('tstart', 'dt', 'tend'))
         self.nsteps = int(math.ceil((tf - ti) / dt))
         self.dt = (tf - ti) / self.nsteps
@@ -80,7 +75,8 @@ class DGFSABstd1D:
         icls = subclass_where(DGFSIntegratorAstd,
                               intg_kind=cfg.lookup('time-integrator', 'scheme'))
         self.odes = icls(self.explicit, self.psm, (K, Ne, Nv), self.dtype,
-                         t=ti, dt=self.dt, f0=self.u, explicitQ=self.explicitQ,
+                         t=ti, dt=self.dt, f0=self.u,
+                         explicitQ=self.explicitQ if self.sm is not None else None,
                          device=self.device)
         self.moments = DGFSMomWriterStd(cfg, vm, self.dg, basis, self.xsol,
                                         tcurr=self.t, coeff=self.u)
@@ -106,6 +102,16 @@ class DGFSABstd1D:
             self.sm.fs_batch(u_in, u_out, self.src, self.dst)
 
     positivity = False      # positivity limiter after the slope limiter
+
+    def _make_models(self, cfg, vm, Ne, K):
+        """The Boltzmann model of ``[scattering-model]`` (explicit) and the
+        penalty model of ``[penalized-scattering-model]`` (abstd.py:80-91)."""
+        smcls = subclass_where(DGFSScatteringModelStd, scattering_model=cfg.lookup(
+            'scattering-model', 'type'))
+        self.sm = smcls(cfg, vm, Ne=Ne, max_evals=K * Ne)
+        pcls = subclass_where(DGFSScatteringModelAstd, scattering_model=cfg.lookup(
+            'penalized-scattering-model', 'type'))
+        self.psm = pcls(cfg, vm, Ne=Ne, eps=self.sm.prefac)
 
     def _configure_dg(self, cfg):
         """Hook for variants of the spatial discretisation."""
@@ -160,3 +166,16 @@ class DGFSABE2std1D(DGFSABstd1D):
 
     def _configure_dg(self, cfg):
         self.dg.set_entropy_stable(self.basis.derivMat)
+
+
+class DGFSAstd1D(DGFSABstd1D):
+    """Linear kinetic models (``dgfsAstd1D``, dgfs1D/astd/astd.py): the model
+    of ``[scattering-model]`` is itself a penalty model (bgk-, esbgk-,
+    shakov-direct-gll) solved by the same IMEX schemes, with no Boltzmann
+    operator (astd.py:82-86, 388-390)."""
+
+    def _make_models(self, cfg, vm, Ne, K):
+        pcls = subclass_where(DGFSScatteringModelAstd, scattering_model=cfg.lookup(
+            'scattering-model', 'type'))
+        self.sm = None
+        self.psm = pcls(cfg, vm, Ne=Ne)
