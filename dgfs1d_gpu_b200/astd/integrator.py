@@ -76,6 +76,147 @@ class Bdf111IntegratorAstd(DGFSIntegratorAstd):
         self._sm.implicit(U, rhs, f, 1.0, dt)
 
 
+class _StageIMEXIntegratorAstd(DGFSIntegratorAstd):
+    """Penalty-only IMEX Runge-Kutta schemes of the linear kinetic driver
+    (dgfsAstd1D) with the BGK model: ARS (astd/integrator.py:56-179) and SSPL
+    (:182-278) with the updateMom{q}_ARS / updateDistribution{q}_ARS /
+    updateDistributionWeight{q}_SSPL arithmetic of bgk-direct-gll.mako:202-326.
+    With stage moments U_j, stage solutions F_j, L_j the advection of a stage
+    and P_j = nu(U_j) (M(U_j) - F_j):
+      U_q = U_0 + dt sum_j _a_qj LU_j
+      F_q = (F_0 + dt sum_j _a_qj L_j + dt sum_{j<q} a_qj P_j
+             + a_qq dt nu_q M_q) / (1 + a_qq dt nu_q).
+    Not built with a Boltzmann operator (in the Boltzmann drivers the
+    reference's ARS stage overwrites Q(f) before using it) nor for the
+    ES-BGK / Shakov models."""
+
+    def __init__(self, explicit, sm, shape, dtype, explicitQ=None, **kwargs):
+        super().__init__(explicit, sm, shape, dtype, explicitQ=explicitQ, **kwargs)
+        if explicitQ is not None:
+            raise NotImplementedError('%s with a Boltzmann operator' % self.intg_kind)
+        if sm.kind != 0:
+            raise NotImplementedError('%s with the %s model' % (
+                self.intg_kind, sm.scattering_model))
+
+    def _stage(self, t, dt, F0, Ls, Ps, q_expl, q_impl, U):
+        """F_q from the explicit weights over Ls, implicit weights over the
+        earlier stages' penalties Ps and the implicit weight of stage q."""
+        rhs = self._z()
+        _lin(rhs, [(1.0, F0)] + [(dt * a, L) for a, L in zip(q_expl, Ls)]
+             + [(dt * a, P) for a, P in zip(q_impl, Ps)])
+        f = self._z()
+        self._sm.implicit(U, rhs, f, 1.0, self._aqq * dt)
+        return f
+
+    def _penalty(self, t, U, f):
+        P = self._z()
+        self._sm.collide(t, U, f, P)
+        return P
+
+
+class ARSIntegratorAstd(_StageIMEXIntegratorAstd):
+    intg_kind = None
+    _A = A = None
+
+    def integrate(self, t, dt, nacptsteps, f):
+        ns = len(self.A) - 1
+        F0 = f.clone()
+        U0 = self._mom(F0)
+        Fs, Us, Ls, LUs, Ps = [F0], [U0], [], [], []
+        for i in range(ns):
+            L = self._z()
+            self._explicit(t, Fs[i], L)
+            Ls.append(L)
+            LUs.append(self._mom(L))
+            ex = self._A[i + 1][0:i + 1]
+            U = self._zm()
+            _lin(U, [(1.0, U0)] + [(dt * a, LU) for a, LU in zip(ex, LUs)])
+            Us.append(U)
+            self._aqq = self.A[i + 1][i + 1]
+            Fq = self._stage(t, dt, F0, Ls, Ps, ex, self.A[i + 1][1:i + 1], U)
+            Fs.append(Fq)
+            if i + 1 < ns:
+                Ps.append(self._penalty(t, U, Fq))
+        f.copy_(Fs[-1])
+
+
+class ARS111IntegratorAstd(ARSIntegratorAstd):
+    intg_kind = 'ars-111'
+    _A = [[0., 0.], [1., 0.]]
+    A = [[0., 0.], [0., 1.]]
+
+
+class ARS222IntegratorAstd(ARSIntegratorAstd):
+    intg_kind = 'ars-222'
+    _g = 1. - (2. ** 0.5) / 2.
+    _d = 1. - 1. / (2. * _g)
+    _A = [[0., 0., 0.], [_g, 0., 0.], [_d, 1 - _d, 0.]]
+    A = [[0., 0., 0.], [0., _g, 0.], [0., 1 - _g, _g]]
+
+
+class ARS443IntegratorAstd(ARSIntegratorAstd):
+    intg_kind = 'ars-443'
+    _A = [[0., 0., 0., 0., 0.], [1. / 2., 0., 0., 0., 0.],
+          [11. / 18., 1. / 18., 0., 0., 0.], [5. / 6., -5. / 6., 1. / 2., 0., 0.],
+          [1. / 4., 7. / 4., 3. / 4., -7. / 4., 0.]]
+    A = [[0., 0., 0., 0., 0.], [0., 1. / 2., 0., 0., 0.], [0., 1. / 6., 1. / 2., 0., 0.],
+         [0., -1. / 2., 1. / 2., 1. / 2., 0.], [0., 3. / 2., -3. / 2., 1. / 2., 1. / 2.]]
+
+
+class SSPLIntegratorAstd(_StageIMEXIntegratorAstd):
+    """SSP L-stable schemes: the first stage is implicit only, stage q uses
+    row q-1 of the tables (a_qj = A[q-1][j-1]), and the new solution is the
+    weighted sum F_0 + dt sum_j (_w_j L_j + w_j P_j) over all stages."""
+    intg_kind = None
+    _A = A = _w = w = None
+
+    def integrate(self, t, dt, nacptsteps, f):
+        ns = len(self.A)
+        F0 = f.clone()
+        U0 = self._mom(F0)
+        U1 = U0.clone()
+        self._aqq = self.A[0][0]
+        F1 = self._stage(t, dt, F0, [], [], [], [], U1)
+        Fs, Us, Ls, LUs, Ps = [F0, F1], [U0, U1], [], [], [self._penalty(t, U1, F1)]
+        for i in range(1, ns):
+            L = self._z()
+            self._explicit(t, Fs[i], L)
+            Ls.append(L)
+            LUs.append(self._mom(L))
+            ex = self._A[i][0:i]
+            U = self._zm()
+            _lin(U, [(1.0, U0)] + [(dt * a, LU) for a, LU in zip(ex, LUs)])
+            Us.append(U)
+            self._aqq = self.A[i][i]
+            Fq = self._stage(t, dt, F0, Ls, Ps, ex, self.A[i][0:i], U)
+            Fs.append(Fq)
+            Ps.append(self._penalty(t, U, Fq))
+        L = self._z()
+        self._explicit(t, Fs[ns], L)
+        Ls.append(L)
+        _lin(f, [(1.0, F0)] + [(dt * a, x) for a, x in zip(self._w, Ls)]
+             + [(dt * a, P) for a, P in zip(self.w, Ps)])
+
+
+class SSPL222IntegratorAstd(SSPLIntegratorAstd):
+    intg_kind = 'sspl-222'
+    _g = 1. - (2. ** 0.5) / 2.
+    _A = [[0., 0.], [1., 0.]]
+    A = [[_g, 0.], [1 - 2 * _g, _g]]
+    _w = [0.5, 0.5]
+    w = [0.5, 0.5]
+
+
+class SSPL443IntegratorAstd(SSPLIntegratorAstd):
+    intg_kind = 'sspl-443'
+    _al, _be, _et = 0.24169426078821, 0.06042356519705, 0.12915286960590
+    _A = [[0., 0., 0., 0.], [0., 0., 0., 0.], [0., 1., 0., 0.], [0., 1. / 4., 1. / 4., 0.]]
+    A = [[_al, 0., 0., 0.], [-_al, _al, 0., 0.], [0., 1. - _al, _al, 0.],
+         [_be, _et, 1. / 2. - _be - _et - _al, _al]]
+    _w = [0., 1. / 6., 1. / 6., 2. / 3.]
+    w = [0., 1. / 6., 1. / 6., 2. / 3.]
+
+
 class BoltzARS111IntegratorAstd(DGFSIntegratorAstd):
     """First-order ARS scheme of the penalised Boltzmann equation
     (astd/integrator.py:491-552): the moments advance with the advection

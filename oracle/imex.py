@@ -4,7 +4,8 @@ Test infrastructure only (see ``oracle/__init__.py``).  Kernels restate
 dgfs1D/astd/kernels/scattering/bgk-direct-gll.mako (cmaxwellian :118-153,
 collide :157-181, updateMom{q}_BDF :16-42, updateDistribution{q}_BDF
 :46-78, updateMom{q}_LM :327-351, updateDistribution{q}_LM :354-405); the
-schemes restate dgfs1D/astd/integrator.py (bdf-111 :281-322, bdf-222
+schemes restate dgfs1D/astd/integrator.py (ARS :56-179 and SSPL :182-278
+for the BGK model without Boltzmann operator, bdf-111 :281-322, bdf-222
 :325-400, bdf-333 :401-488, boltz-ars-111 :491-552, IMEX-LM :623-792).  Start-up steps of the multi-step schemes use
 first-order substeps of the same family (the reference uses ARS-222/443
 substeps); ``imex-lm-*`` does not stop after its first step (astd/
@@ -197,6 +198,31 @@ BDF_COEF = {
                 6. / 11.),
 }
 
+# ARS (astd/integrator.py:117-179) and SSPL (:240-278) tables: (_A, A) and,
+# for SSPL, the weights (_w, w)
+_g2 = 1. - (2. ** 0.5) / 2.
+_d2 = 1. - 1. / (2. * _g2)
+ARS_COEF = {
+    'ars-111': ([[0., 0.], [1., 0.]], [[0., 0.], [0., 1.]]),
+    'ars-222': ([[0., 0., 0.], [_g2, 0., 0.], [_d2, 1 - _d2, 0.]],
+                [[0., 0., 0.], [0., _g2, 0.], [0., 1 - _g2, _g2]]),
+    'ars-443': ([[0., 0., 0., 0., 0.], [1. / 2., 0., 0., 0., 0.],
+                 [11. / 18., 1. / 18., 0., 0., 0.], [5. / 6., -5. / 6., 1. / 2., 0., 0.],
+                 [1. / 4., 7. / 4., 3. / 4., -7. / 4., 0.]],
+                [[0., 0., 0., 0., 0.], [0., 1. / 2., 0., 0., 0.], [0., 1. / 6., 1. / 2., 0., 0.],
+                 [0., -1. / 2., 1. / 2., 1. / 2., 0.], [0., 3. / 2., -3. / 2., 1. / 2., 1. / 2.]]),
+}
+_al, _be, _et = 0.24169426078821, 0.06042356519705, 0.12915286960590
+SSPL_COEF = {
+    'sspl-222': ([[0., 0.], [1., 0.]], [[_g2, 0.], [1 - 2 * _g2, _g2]],
+                 [0.5, 0.5], [0.5, 0.5]),
+    'sspl-443': ([[0., 0., 0., 0.], [0., 0., 0., 0.], [0., 1., 0., 0.],
+                  [0., 1. / 4., 1. / 4., 0.]],
+                 [[_al, 0., 0., 0.], [-_al, _al, 0., 0.], [0., 1. - _al, _al, 0.],
+                  [_be, _et, 1. / 2. - _be - _et - _al, _al]],
+                 [0., 1. / 6., 1. / 6., 2. / 3.], [0., 1. / 6., 1. / 6., 2. / 3.]),
+}
+
 LM_COEF = {
     'imex-lm-bdf1': ([-1.], [1.], [1., 0.]),
     'imex-lm-bdf2': ([-4. / 3., 1. / 3.], [4. / 3., -2. / 3.], [2. / 3., 0., 0.]),
@@ -292,8 +318,52 @@ class IMEX:
         L = self.explicit(f)
         return dict(F=f.copy(), U=self._mom(f), L=L, LU=self._mom(L))
 
+    def _ars_stage(self, F0, Ls, Ps, ex, im, aqq, U):
+        # updateDistribution{q}_ARS (bgk-direct-gll.mako:233-279): the
+        # explicit sum over the stage advections, the implicit sum over the
+        # earlier stages' penalties and the implicit last stage
+        dt = self.dt
+        rhs = F0 + sum(a * dt * L for a, L in zip(ex, Ls)) + \
+            sum(a * dt * P for a, P in zip(im, Ps))
+        return self._implicit(U, rhs, 1., aqq * dt)
+
     def step(self, f):
         dt, k = self.dt, self.kind
+        if k in ARS_COEF:
+            # ARSabcIntegratorAstd._integrate (astd/integrator.py:56-114)
+            _A, A = ARS_COEF[k]
+            ns = len(A) - 1
+            U0 = self._mom(f)
+            Fs, Ls, LUs, Ps = [f], [], [], []
+            for i in range(ns):
+                Ls.append(self.explicit(Fs[i]))
+                LUs.append(self._mom(Ls[i]))
+                ex = _A[i + 1][:i + 1]
+                U = U0 + sum(dt * a * LU for a, LU in zip(ex, LUs))
+                Fq = self._ars_stage(f, Ls, Ps, ex, A[i + 1][1:i + 1],
+                                     A[i + 1][i + 1], U)
+                Fs.append(Fq)
+                Ps.append(self._collide(U, Fq))
+            return Fs[-1]
+        if k in SSPL_COEF:
+            # SSPLabcIntegratorAstd._integrate (astd/integrator.py:182-228)
+            _A, A, _w, w = SSPL_COEF[k]
+            ns = len(A)
+            U0 = self._mom(f)
+            F1 = self._ars_stage(f, [], [], [], [], A[0][0], U0)
+            Fs, Ls, LUs, Ps = [f, F1], [], [], [self._collide(U0, F1)]
+            for i in range(1, ns):
+                Ls.append(self.explicit(Fs[i]))
+                LUs.append(self._mom(Ls[-1]))
+                ex = _A[i][:i]
+                U = U0 + sum(dt * a * LU for a, LU in zip(ex, LUs))
+                Fq = self._ars_stage(f, Ls, Ps, ex, A[i][:i], A[i][i], U)
+                Fs.append(Fq)
+                Ps.append(self._collide(U, Fq))
+            Ls.append(self.explicit(Fs[ns]))
+            # updateDistributionWeight{q}_SSPL (bgk-direct-gll.mako:282-326)
+            return f + sum(a * dt * L for a, L in zip(_w, Ls)) + \
+                sum(a * dt * P for a, P in zip(w, Ps))
         if k == 'boltz-ars-111':
             # integrator.py:491-552: moments of the advection only, then the
             # explicit part L + Q - P (P = nu (M(U0) - f)) in the update of f

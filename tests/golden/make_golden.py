@@ -8,6 +8,7 @@ default /root/reference)::
     python tests/golden/make_golden.py limiter          # only the slope-limiter file
     python tests/golden/make_golden.py moments          # only the moment-writer file
     python tests/golden/make_golden.py upwind           # only the upwind (abstdu) file
+    python tests/golden/make_golden.py penalty          # only the BGK penalty-kernel file
     python tests/golden/make_golden.py entropy          # only the entropy-stable (abstde2) file
 
 What runs from the reference:
@@ -598,6 +599,28 @@ def golden_penalty(R, Nv=8, npts=6, omega=0.81, prefac=3.7):
     K.launch('updateDistribution2_LM', gg, blk, prefac, lda, dt, *A, *B, *C,
              L0, L1, P0, P1, M2, f, f1, f2, U, U1, U2)
     out.update(LM0=LM0, LM1=LM1, P0=P0, P1=P1, U2_lm2=U2, f2_lm2=f2)
+    # one ARS stage (q = 2, ars-222 coefficients) and the SSPL weighting
+    # (q = 2, sspl-222 weights), as ARSabcIntegratorAstd / SSPLabcIntegratorAstd
+    # call updateMom2_ARS, updateDistribution2_ARS, updateDistributionWeight2_SSPL
+    gam = 1. - (2. ** 0.5) / 2.
+    dl = 1. - 1. / (2. * gam)
+    _a, a = [dl, 1 - dl], [1 - gam, gam]
+    U2a = np.zeros(npts * 5)
+    K.launch('updateMom2_ARS', gm, blk, prefac, npts, dt, *_a, *a, LU0, LU1,
+             U, U1, U2a)
+    M1 = np.zeros(lda)
+    K.launch('cmaxwellian', gg, blk, lda, cx, cy, cz, M1, U1)
+    M2a = np.zeros(lda)
+    K.launch('cmaxwellian', gg, blk, lda, cx, cy, cz, M2a, U2a)
+    f2a = np.zeros(lda)
+    K.launch('updateDistribution2_ARS', gg, blk, prefac, lda, dt, *_a, *a,
+             L0, L1, U, U1, U2a, M1, M2a, f, f1, f2a)
+    f2s = f1 * (1 + 0.01 * rng.uniform(-1, 1, lda))
+    f3 = np.zeros(lda)
+    K.launch('updateDistributionWeight2_SSPL', gg, blk, prefac, lda, dt,
+             0.5, 0.5, 0.5, 0.5, L0, L1, U, U1, U2a, M1, M2a, f, f1, f2s, f3)
+    out.update(ars_a=np.array(_a), ars_A=np.array(a), U2_ars=U2a, M1_ars=M1,
+               M2_ars=M2a, f2_ars=f2a, f2_sspl=f2s, f3_sspl=f3)
     return out
 
 
@@ -1052,6 +1075,11 @@ def limiter():
     np.savez_compressed(os.path.join(HERE, 'limiter_N4.npz'), **golden_limiter(R))
 
 
+def penalty():
+    R = _import_reference()
+    np.savez_compressed(os.path.join(HERE, 'penalty_N8.npz'), **golden_penalty(R))
+
+
 def upwind():
     R = _import_reference()
     np.savez_compressed(os.path.join(HERE, 'upwind_N8.npz'), **golden_upwind(R))
@@ -1084,6 +1112,8 @@ if __name__ == '__main__':
         moments()
     elif sys.argv[1:] == ['upwind']:
         upwind()
+    elif sys.argv[1:] == ['penalty']:
+        penalty()
     elif sys.argv[1:] == ['entropy']:
         entropy()
     else:

@@ -59,6 +59,33 @@ def test_penalty_kernels_match_reference():
     assert _rel(f2, g['f2_lm2']) < 1e-13
 
 
+def test_ars_sspl_stage_matches_reference():
+    """One ARS stage and the SSPL weighting of the oracle (the arithmetic of
+    IMEX._ars_stage and the SSPL weighted sum) against the reference's
+    updateMom2_ARS, updateDistribution2_ARS and updateDistributionWeight2_SSPL
+    kernels on the golden data."""
+    g = np.load(os.path.join(G, 'penalty_N8.npz'))
+    npts, cv = int(g['npts']), g['cv']
+    pre, om, dt = float(g['prefac']), float(g['omega']), float(g['dt'])
+    _a, a = list(g['ars_a']), list(g['ars_A'])
+    U0, U1 = g['U'].reshape(npts, 5), g['U1'].reshape(npts, 5)
+    LU0, LU1 = g['LU0'].reshape(npts, 5), g['LU1'].reshape(npts, 5)
+    U2 = U0 + dt * _a[0] * LU0 + dt * _a[1] * LU1
+    assert _rel(U2, g['U2_ars']) < 1e-14
+    assert _rel(oim.maxwellian(U1, cv), g['M1_ars']) < 1e-13
+    assert _rel(oim.maxwellian(U2, cv), g['M2_ars']) < 1e-13
+    f0, f1 = g['f'].reshape(npts, -1), g['f1'].reshape(npts, -1)
+    L0, L1 = g['L0'].reshape(npts, -1), g['L1'].reshape(npts, -1)
+    P1 = oim.collide(U1, f1, cv, pre, om)
+    rhs = f0 + _a[0] * dt * L0 + _a[1] * dt * L1 + a[0] * dt * P1
+    f2 = oim.implicit(U2, rhs, cv, 1.0, a[1] * dt, pre, om)
+    assert _rel(f2, g['f2_ars']) < 1e-13
+    f2s = g['f2_sspl'].reshape(npts, -1)
+    P2 = oim.collide(U2, f2s, cv, pre, om)
+    f3 = f0 + 0.5 * dt * L0 + 0.5 * dt * L1 + 0.5 * dt * P1 + 0.5 * dt * P2
+    assert _rel(f3, g['f3_sspl']) < 1e-13
+
+
 @pytest.mark.parametrize('tag', ['esbgk', 'shakov'])
 def test_esbgk_shakov_oracle_matches_reference(tag):
     """The oracle's ES-BGK / Shakov penalty models against the reference's
