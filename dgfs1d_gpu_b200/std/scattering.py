@@ -137,3 +137,90 @@ class DGFSVHSScatteringModelStd(DGFSVHSGLLScatteringModelStd):
                 not torch.equal(d_arr_in1, d_arr_in2):
             raise NotImplementedError('bilinear Q(f, g) with g != f')
         super().fs(d_arr_in1, d_arr_in1, d_arr_out, elem, modein, modeout)
+
+
+class DGFSBGKDirectGLLScatteringModelStd(DGFSScatteringModelStd):
+    """Explicit BGK relaxation ``bgk-direct-gll`` of dgfsStd1D
+    (std/scattering.py:1186-1371, std/kernels/scattering/bgk-direct-gll.mako):
+    at every point Q += prefac rho T^(1-omega) (M[rho, u, T] - f) with rho, u,
+    T the moments of f there, prefac = t0 p0 / visc from ``[scattering-model]``
+    omega, muRef, Tref (Pr = 1).  Runs on the native BGK penalty kernels
+    (moments and collide over all points at once); the driver binds its DG
+    handle (``bind``) for the grid tables."""
+    scattering_model = 'bgk-direct-gll'
+
+    def __init__(self, cfg, velocitymesh, **kwargs):
+        self._Ne = kwargs.get('Ne')
+        self._dg = None
+        super().__init__(cfg, velocitymesh, **kwargs)
+
+    def load_parameters(self):
+        cfg, vm = self.cfg, self.vm
+        omega = cfg.lookupfloat('scattering-model', 'omega')
+        muRef = cfg.lookupfloat('scattering-model', 'muRef')
+        Tref = cfg.lookupfloat('scattering-model', 'Tref')
+        t0 = vm.H0() / vm.u0()
+        visc = muRef * ((vm.T0() / Tref) ** omega)
+        p0 = vm.n0() * vm.R0 / vm.NA * vm.T0()
+        self._prefactor = float(t0 * 1.0 * p0 / visc)
+        self._omega = float(omega)
+
+    def perform_precomputation(self):
+        pass
+
+    def bind(self, dg):
+        self._dg = dg
+
+    def _relax(self, f, Q, stream=None):
+        """Q += nu (M - f) for the points (rows of N^3) of f."""
+        import ctypes
+        from .. import _native as nat
+        from ..collision import _DT, _stream_ptr
+        if self._dg is None:
+            raise RuntimeError('bgk-direct-gll: bind(dg) first')
+        Nv = self.vm.vsize()
+        npts = f.numel() // Nv
+        U = torch.zeros((npts, 5), dtype=torch.float64, device=f.device)
+        P = torch.empty_like(f)
+        sp = _stream_ptr(stream)
+        nat.check(nat.lib().dgfs_penalty_moments_n(
+            self._dg._h, ctypes.c_void_p(f.data_ptr()), _DT[f.dtype], npts, 5,
+            ctypes.c_void_p(U.data_ptr()), sp))
+        nat.check(nat.lib().dgfs_penalty_model_collide(
+            self._dg._h, 0, ctypes.c_void_p(U.data_ptr()),
+            ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(P.data_ptr()),
+            ctypes.c_void_p(0), _DT[f.dtype], npts, self._prefactor,
+            self._omega, 1.0, sp))
+        from ..dg import axnpby
+        axnpby(Q, 1.0, 1.0, P, stream=stream)
+
+    def fs_batch(self, d_f, d_Q, src, dst, stream=None):
+        """Q[dst[i]] += relaxation of f[src[i]]; the nodal bases pair every
+        point with itself (src == dst).  The slot lists are inspected on the
+        host once per pair of lists (the first call, before any graph
+        capture)."""
+        Nv = self.vm.vsize()
+        f = d_f.reshape(-1, Nv)
+        Q = d_Q.reshape(-1, Nv)
+        key = (src.data_ptr(), dst.data_ptr(), src.numel(), f.shape[0])
+        cache = self.__dict__.setdefault('_slots', {})
+        if key not in cache:
+            s_h, d_h = src.cpu(), dst.cpu()
+            if not torch.equal(s_h, d_h):
+                raise NotImplementedError('bgk-direct-gll needs src == dst slots')
+            cache[key] = torch.equal(s_h.long(), torch.arange(f.shape[0]))
+        if cache[key]:
+            self._relax(f, Q, stream)
+        else:
+            idx = src.long()
+            fq = f.index_select(0, idx).contiguous()
+            Qq = torch.zeros_like(fq)
+            self._relax(fq, Qq, stream)
+            Q.index_add_(0, idx, Qq)
+
+    def fs(self, d_arr_in, d_arr_in2, d_arr_out, elem, modein, modeout):
+        Nv, Ne = self.vm.vsize(), self._Ne
+        f = d_arr_in.reshape(-1, Nv)[modein * Ne + elem].reshape(1, Nv).contiguous()
+        P = torch.zeros_like(f)
+        self._relax(f, P)
+        d_arr_out.reshape(-1, Nv)[modeout * Ne + elem] += P[0]

@@ -56,6 +56,8 @@ class DGFSStd1D:
         self.dg = DGOperator(basis, mesh.invjac, vm.c0(), vm.cw(),
                              [(self.bcl.type, self.bcl.f0, self.bcl.ux),
                               (self.bcr.type, self.bcr.f0, self.bcr.ux)])
+        if hasattr(self.sm, 'bind'):          # relaxation models use its tables
+            self.sm.bind(self.dg)
         # collision sources: Q at mode m, element e from coefficient a
         src, dst = [], []
         for m, a in basis.mode_sources():

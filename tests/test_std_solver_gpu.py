@@ -337,3 +337,41 @@ def test_command_line_run_and_restart(tmp_path, capsys):
               '-v', 'dgfsdistwriter::basename', 'r-{t:.6f}'])
     assert r.nsteps == 2
     assert _rel(r.u.cpu().numpy(), s.u.cpu().numpy()) < 1e-14
+
+
+def test_std_bgk_direct_relaxation_matches_oracle():
+    """dgfsStd1D with ``[scattering-model] type = bgk-direct-gll`` (explicit BGK
+    relaxation at every point) over three ssp-rk2 steps, eager and
+    graph-captured, against the oracle."""
+    from oracle import imex as oim
+    ini = couette_std_ini(Nv=8, Nrho=4, scheme='ssp-rk2', nsteps=3)
+    ini = ini.replace('type = vhs-gll', 'type = bgk-direct-gll')
+    s = _solver(ini)
+    assert s.sm.scattering_model == 'bgk-direct-gll'
+    u0 = s.u.cpu().numpy().copy()
+    s.run(3)
+    torch.cuda.synchronize()
+    got = s.u.cpu().numpy()
+    vm = s.vm
+    b = odg.NodalBasis(s.basis.basis_kind, s.basis.K, s.basis.interpMat.shape[1])
+    cv, cw = vm.cv(), vm.cw()
+    bcl = odg.WallDiffuseBC(cv, cw, 1.0, [0, 0, 0], -1.)
+    bcr = odg.WallDiffuseBC(cv, cw, 1.0, [0, 0, 0], 1.)
+    bcl.f0, bcr.f0 = s.bcl.f0, s.bcr.f0
+    pre, om = s.sm.prefac, s.sm.omega
+
+    def fs(f, g):
+        U = oim.moments5(f[None], cv, cw)
+        return oim.collide(U, f, cv, pre, om).ravel()
+    collide = odg.collide_fs(b, fs)
+    u, t = u0.copy(), 0.0
+    for _ in range(3):
+        odg.integrate('ssp-rk2', lambda tt, x: odg.dg_rhs(
+            b, s.mesh.invjac, cv[0], bcl, bcr, x, collide=collide), t, s.dt, u)
+        t += s.dt
+    assert _rel(got, u) < 1e-12
+    s2 = _solver(ini)
+    s2.capture_step()
+    s2.run(3)
+    torch.cuda.synchronize()
+    assert _rel(s2.u.cpu().numpy(), got) < 1e-14
