@@ -9,13 +9,16 @@ The operator runs in the native library (FP64 parity mode or the FP32
 Maxwellian-split mode, ``[scattering-model] precision-mode = fp64|fp32``,
 default: fp64 for precision=double, fp32 for precision=float).
 """
+import ctypes
 from abc import ABCMeta, abstractmethod
 from math import gamma
 
 import numpy as np
 import torch
 
-from ..collision import VHSOperator
+from .. import _native as nat
+from ..collision import _DT, VHSOperator, _stream_ptr
+from ..dg import axnpby
 
 
 class DGFSScatteringModelStd(metaclass=ABCMeta):
@@ -173,9 +176,6 @@ class DGFSBGKDirectGLLScatteringModelStd(DGFSScatteringModelStd):
 
     def _relax(self, f, Q, stream=None):
         """Q += nu (M - f) for the points (rows of N^3) of f."""
-        import ctypes
-        from .. import _native as nat
-        from ..collision import _DT, _stream_ptr
         if self._dg is None:
             raise RuntimeError('bgk-direct-gll: bind(dg) first')
         Nv = self.vm.vsize()
@@ -191,7 +191,6 @@ class DGFSBGKDirectGLLScatteringModelStd(DGFSScatteringModelStd):
             ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(P.data_ptr()),
             ctypes.c_void_p(0), _DT[f.dtype], npts, self._prefactor,
             self._omega, 1.0, sp))
-        from ..dg import axnpby
         axnpby(Q, 1.0, 1.0, P, stream=stream)
 
     def fs_batch(self, d_f, d_Q, src, dst, stream=None):
