@@ -147,10 +147,11 @@ class DGFSBGKDirectGLLScatteringModelStd(DGFSScatteringModelStd):
     (std/scattering.py:1186-1371, std/kernels/scattering/bgk-direct-gll.mako):
     at every point Q += prefac rho T^(1-omega) (M[rho, u, T] - f) with rho, u,
     T the moments of f there, prefac = t0 p0 / visc from ``[scattering-model]``
-    omega, muRef, Tref (Pr = 1).  Runs on the native BGK penalty kernels
-    (moments and collide over all points at once); the driver binds its DG
-    handle (``bind``) for the grid tables."""
+    omega, muRef, Tref (Pr = 1).  Runs on the native penalty kernels (moments
+    and collide over all points at once); the driver binds its DG handle
+    (``bind``) for the grid tables."""
     scattering_model = 'bgk-direct-gll'
+    kind, nalph = 0, 5      # native penalty model: BGK, 5 moments
 
     def __init__(self, cfg, velocitymesh, **kwargs):
         self._Ne = kwargs.get('Ne')
@@ -167,6 +168,10 @@ class DGFSBGKDirectGLLScatteringModelStd(DGFSScatteringModelStd):
         p0 = vm.n0() * vm.R0 / vm.NA * vm.T0()
         self._prefactor = float(t0 * 1.0 * p0 / visc)
         self._omega = float(omega)
+        self._Pr = self._load_Pr()
+
+    def _load_Pr(self):
+        return 1.0
 
     def perform_precomputation(self):
         pass
@@ -180,17 +185,17 @@ class DGFSBGKDirectGLLScatteringModelStd(DGFSScatteringModelStd):
             raise RuntimeError('bgk-direct-gll: bind(dg) first')
         Nv = self.vm.vsize()
         npts = f.numel() // Nv
-        U = torch.zeros((npts, 5), dtype=torch.float64, device=f.device)
+        U = torch.zeros((npts, self.nalph), dtype=torch.float64, device=f.device)
         P = torch.empty_like(f)
         sp = _stream_ptr(stream)
         nat.check(nat.lib().dgfs_penalty_moments_n(
-            self._dg._h, ctypes.c_void_p(f.data_ptr()), _DT[f.dtype], npts, 5,
-            ctypes.c_void_p(U.data_ptr()), sp))
+            self._dg._h, ctypes.c_void_p(f.data_ptr()), _DT[f.dtype], npts,
+            self.nalph, ctypes.c_void_p(U.data_ptr()), sp))
         nat.check(nat.lib().dgfs_penalty_model_collide(
-            self._dg._h, 0, ctypes.c_void_p(U.data_ptr()),
+            self._dg._h, self.kind, ctypes.c_void_p(U.data_ptr()),
             ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(P.data_ptr()),
             ctypes.c_void_p(0), _DT[f.dtype], npts, self._prefactor,
-            self._omega, 1.0, sp))
+            self._omega, self._Pr, sp))
         axnpby(Q, 1.0, 1.0, P, stream=stream)
 
     def fs_batch(self, d_f, d_Q, src, dst, stream=None):
@@ -223,3 +228,18 @@ class DGFSBGKDirectGLLScatteringModelStd(DGFSScatteringModelStd):
         P = torch.zeros_like(f)
         self._relax(f, P)
         d_arr_out.reshape(-1, Nv)[modeout * Ne + elem] += P[0]
+
+
+class DGFSShakovDirectGLLScatteringModelStd(DGFSBGKDirectGLLScatteringModelStd):
+    """Explicit Shakov relaxation ``shakov-direct-gll`` of dgfsStd1D
+    (std/scattering.py:1638-1846, std/kernels/scattering/shakov-direct-gll.mako):
+    Q += prefac rho T^(1-omega) (M (1 + 4 (1 - Pr)/5 (q.c')/(rho T^2)
+    (|c'|^2/T - 5/2)) - f), c' = c - u, q = sum f |c'|^2 c' cw, prefac =
+    t0 p0 / visc and Pr from ``[scattering-model]`` (default 2/3) -- the
+    Shakov collide of the penalty kernels, whose heat flux is formed from the
+    raw moments."""
+    scattering_model = 'shakov-direct-gll'
+    kind, nalph = 2, 14
+
+    def _load_Pr(self):
+        return float(self.cfg.lookupordefault('scattering-model', 'Pr', 2. / 3.))

@@ -8,6 +8,7 @@ default /root/reference)::
     python tests/golden/make_golden.py limiter          # only the slope-limiter file
     python tests/golden/make_golden.py moments          # only the moment-writer file
     python tests/golden/make_golden.py upwind           # only the upwind (abstdu) file
+    python tests/golden/make_golden.py std-relax        # only the dgfsStd1D relaxation file
     python tests/golden/make_golden.py penalty          # only the BGK penalty-kernel file
     python tests/golden/make_golden.py entropy          # only the entropy-stable (abstde2) file
 
@@ -931,6 +932,60 @@ def golden_entropy(R, Nv=8, Ne=4, K=3):
                 f0L=walls['L'][1], f0R=walls['R'][1])
 
 
+def golden_std_relax(R, Nv=8, omega=0.81, prefac=3.7, Pr=2. / 3.):
+    """The explicit relaxation fs of dgfsStd1D's bgk-direct-gll and
+    shakov-direct-gll (std/scattering.py:1320-1371, 1764-1846): the kernels of
+    std/kernels/scattering/{bgk,shakov}-direct-gll.mako driven in fs's order
+    on one point, with NumPy sums in place of the block reductions of sum_."""
+    from oracle.ref_build import RefModule, grid_for, render_template
+    vsize = Nv ** 3
+    L = 5.0
+    c0 = np.linspace(-L + L / Nv, L - L / Nv, Nv)
+    g = np.meshgrid(c0, c0, c0, indexing='ij')
+    cv = np.stack([x.ravel() for x in g])
+    cw = (2 * L / Nv) ** 3
+    cx, cy, cz = (np.ascontiguousarray(cv[i]) for i in range(3))
+    rng = np.random.default_rng(SEED + 43)
+    u = np.array([0.1, -0.05, 0.02]).reshape(3, 1)
+    f = 1.1 / (np.pi * 0.9) ** 1.5 * np.exp(-np.sum((cv - u) ** 2, axis=0) / 0.9)
+    f = np.ascontiguousarray(f * (1 + 0.05 * rng.uniform(-1, 1, vsize)))
+    blk = 128
+    gv = grid_for(vsize, blk)
+    one = lambda v: np.array([float(v)])
+    out = dict(f=f, cv=cv, cw=cw, omega=omega, prefac=prefac, Pr=Pr, Nv=Nv)
+    for name in ('bgk', 'shakov'):
+        src = render_template('dgfs1D/std/kernels/scattering/%s-direct-gll.mako' % name,
+                              cw=cw, vsize=vsize, prefac=prefac, nalph=5,
+                              nalphSk=8, omega=omega, Pr=Pr, block_size=256,
+                              Ne=1, dtype='double')
+        K = RefModule(src, tag='std_%s_direct' % name)
+        floc = np.zeros(vsize)
+        K.launch('flocKern', gv, blk, 0, 0, f, floc)
+        m10, m11, m12 = np.zeros(vsize), np.zeros(vsize), np.zeros(vsize)
+        K.launch('mom1', gv, blk, cx, cy, cz, floc, m10, m11, m12)
+        moms = [one(np.sum(floc)), one(np.sum(m10)), one(np.sum(m11)),
+                one(np.sum(m12))]
+        K.launch('mom01Norm', 1, 1, *moms)
+        Q = np.zeros(vsize)
+        if name == 'bgk':
+            m2 = np.zeros(vsize)
+            K.launch('mom2', gv, blk, cx, cy, cz, floc, m2, *moms)
+            moms.append(one(np.sum(m2)))
+            K.launch('equiDistInit', 1, 1, *moms)
+            fe = np.zeros(vsize)
+            K.launch('output', gv, blk, 0, 0, 0, *moms, fe, floc, Q, cx, cy, cz)
+        else:
+            m2, q1, q2, q3 = (np.zeros(vsize) for _ in range(4))
+            K.launch('mom23Sk', gv, blk, cx, cy, cz, floc, *moms, m2, q1, q2, q3)
+            sk = moms + [one(np.sum(x)) for x in (m2, q1, q2, q3)]
+            K.launch('mom23SkNorm', 1, 1, *sk)
+            feSk = np.zeros(vsize)
+            K.launch('equiSkDistCompute', gv, blk, cx, cy, cz, feSk, *sk)
+            K.launch('output', gv, blk, 0, 0, 0, sk[0], sk[4], feSk, floc, Q)
+        out['Q_' + name] = Q
+    return out
+
+
 def golden_moments(R, Nv=8, Ne=4, K=3):
     """Bulk moments of the reference's writers: DGFSMomWriterStd and
     DGFSMomWriterBi ``_compute_moments_1D`` (std/moments.py:11-70,
@@ -1065,6 +1120,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'moments_N8.npz'), **golden_moments(R))
     np.savez_compressed(os.path.join(HERE, 'upwind_N8.npz'), **golden_upwind(R))
     np.savez_compressed(os.path.join(HERE, 'entropy_N8.npz'), **golden_entropy(R))
+    np.savez_compressed(os.path.join(HERE, 'std_relax_N8.npz'), **golden_std_relax(R))
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith('.npz'):
             print(fn, os.path.getsize(os.path.join(HERE, fn)), 'bytes')
@@ -1078,6 +1134,11 @@ def limiter():
 def penalty():
     R = _import_reference()
     np.savez_compressed(os.path.join(HERE, 'penalty_N8.npz'), **golden_penalty(R))
+
+
+def std_relax():
+    R = _import_reference()
+    np.savez_compressed(os.path.join(HERE, 'std_relax_N8.npz'), **golden_std_relax(R))
 
 
 def upwind():
@@ -1112,6 +1173,8 @@ if __name__ == '__main__':
         moments()
     elif sys.argv[1:] == ['upwind']:
         upwind()
+    elif sys.argv[1:] == ['std-relax']:
+        std_relax()
     elif sys.argv[1:] == ['penalty']:
         penalty()
     elif sys.argv[1:] == ['entropy']:

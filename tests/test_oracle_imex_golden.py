@@ -124,3 +124,16 @@ def test_esbgk_shakov_oracle_matches_reference(tag):
               for i in range(2))
     f2 = oi.model_implicit(model, U2, rhs, cv, 1.0, C[0] * dt, pf, om)
     assert rel(f2, z['f2_lm2']) < 1e-13
+
+
+def test_std_direct_relaxation_matches_reference():
+    """dgfsStd1D's explicit bgk-direct-gll / shakov-direct-gll fs (the std
+    kernels, golden) equal the penalty models' collide of the oracle."""
+    g = np.load(os.path.join(G, 'std_relax_N8.npz'))
+    f, cv, cw = g['f'], g['cv'], float(g['cw'])
+    pre, om, Pr = float(g['prefac']), float(g['omega']), float(g['Pr'])
+    U5 = oim.moments5(f[None], cv, cw)
+    assert _rel(oim.collide(U5, f, cv, pre, om).ravel(), g['Q_bgk']) < 1e-12
+    U14 = oim.moments_n(f[None], cv, cw, 14)
+    Q = oim.model_collide(oim.ShakovModel(Pr), U14, f[None], cv, pre, om).ravel()
+    assert _rel(Q, g['Q_shakov']) < 1e-12

@@ -339,15 +339,16 @@ def test_command_line_run_and_restart(tmp_path, capsys):
     assert _rel(r.u.cpu().numpy(), s.u.cpu().numpy()) < 1e-14
 
 
-def test_std_bgk_direct_relaxation_matches_oracle():
-    """dgfsStd1D with ``[scattering-model] type = bgk-direct-gll`` (explicit BGK
-    relaxation at every point) over three ssp-rk2 steps, eager and
-    graph-captured, against the oracle."""
+@pytest.mark.parametrize('model', ['bgk-direct-gll', 'shakov-direct-gll'])
+def test_std_direct_relaxation_matches_oracle(model):
+    """dgfsStd1D with ``[scattering-model] type = bgk-direct-gll`` /
+    ``shakov-direct-gll`` (explicit relaxation at every point) over three
+    ssp-rk2 steps, eager and graph-captured, against the oracle."""
     from oracle import imex as oim
     ini = couette_std_ini(Nv=8, Nrho=4, scheme='ssp-rk2', nsteps=3)
-    ini = ini.replace('type = vhs-gll', 'type = bgk-direct-gll')
+    ini = ini.replace('type = vhs-gll', 'type = %s' % model)
     s = _solver(ini)
-    assert s.sm.scattering_model == 'bgk-direct-gll'
+    assert s.sm.scattering_model == model
     u0 = s.u.cpu().numpy().copy()
     s.run(3)
     torch.cuda.synchronize()
@@ -360,9 +361,11 @@ def test_std_bgk_direct_relaxation_matches_oracle():
     bcl.f0, bcr.f0 = s.bcl.f0, s.bcr.f0
     pre, om = s.sm.prefac, s.sm.omega
 
+    om_model = oim.BGKModel() if s.sm.kind == 0 else oim.ShakovModel(s.sm._Pr)
+
     def fs(f, g):
-        U = oim.moments5(f[None], cv, cw)
-        return oim.collide(U, f, cv, pre, om).ravel()
+        U = oim.moments_n(f[None], cv, cw, s.sm.nalph)
+        return oim.model_collide(om_model, U, f[None], cv, pre, om).ravel()
     collide = odg.collide_fs(b, fs)
     u, t = u0.copy(), 0.0
     for _ in range(3):
@@ -375,3 +378,32 @@ def test_std_bgk_direct_relaxation_matches_oracle():
     s2.run(3)
     torch.cuda.synchronize()
     assert _rel(s2.u.cpu().numpy(), got) < 1e-14
+
+
+@pytest.mark.parametrize('model', ['bgk', 'shakov'])
+def test_std_direct_relaxation_kernel_matches_reference(model):
+    """The native relaxation of one point (fs) against the golden output of
+    the reference's std {bgk,shakov}-direct-gll kernels."""
+    from dgfs1d_gpu_b200 import build
+    build.build()
+    from dgfs1d_gpu_b200.std.scattering import (
+        DGFSBGKDirectGLLScatteringModelStd, DGFSShakovDirectGLLScatteringModelStd)
+    from dgfs1d_gpu_b200.basis import get_basis
+    from dgfs1d_gpu_b200.dg import DGOperator
+    g = np.load(os.path.join(G, 'std_relax_N8.npz'))
+    N = int(g['Nv'])
+    cls = {'bgk': DGFSBGKDirectGLLScatteringModelStd,
+           'shakov': DGFSShakovDirectGLLScatteringModelStd}[model]
+    sm = object.__new__(cls)            # parameters from the golden case
+    sm._Ne, sm._prefactor, sm._omega = 1, float(g['prefac']), float(g['omega'])
+    sm._Pr = 1.0 if model == 'bgk' else float(g['Pr'])
+    sm.vm = type('VM', (), {'vsize': lambda self: N ** 3})()
+    b = get_basis(Config(couette_std_ini()))
+    dg = DGOperator(b, np.ones(1), g['cv'][2, :N], float(g['cw']),
+                    [('dgfs-periodic', None, 0.0), ('dgfs-periodic', None, 0.0)])
+    sm.bind(dg)
+    f = torch.tensor(g['f'].reshape(1, -1), device='cuda')
+    Q = torch.zeros_like(f)
+    sm.fs(f, f, Q, 0, 0, 0)
+    torch.cuda.synchronize()
+    assert _rel(Q.cpu().numpy().ravel(), g['Q_' + model]) < 1e-12
