@@ -136,6 +136,10 @@ _SIGNATURES = [
      [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ('dgfs_dg_limit_positivity', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    ('dgfs_std_esbgk_relax', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+      ctypes.c_void_p]),
     ('dgfs_dg_set_entropy_stable', ctypes.c_int,
      [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     ('dgfs_dg_set_upwind', ctypes.c_int,

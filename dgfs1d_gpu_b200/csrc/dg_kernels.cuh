@@ -565,6 +565,109 @@ __global__ void __launch_bounds__(256) bi_moments_pass2_kernel(BiMomentArgs a) {
   }
 }
 
+// Explicit ES-BGK relaxation of dgfsStd1D (esbgk-direct-gll, the fs of
+// std/scattering.py:1540-1637 with std/kernels/scattering/esbgk-direct-gll.mako):
+// per point rho = sum f cw, u = sum f c / sum f, T = sum f |c-u|^2 cw/(1.5 rho);
+// the covariance S_ij = sum (c-u)_i (c-u)_j ((1-1/Pr) f + (1/Pr) f_M) cw / rho
+// with the grid Maxwellian f_M = rho/(pi T)^1.5 exp(-|c-u|^2/T); then
+// Q += prefac rho / T^(omega-1) (f_ES - f), f_ES = rho/((2 pi)^1.5 sqrt(det S))
+// exp(-(c-u)^T S^-1 (c-u) / 2).  One block per point (FP64 sums).
+struct StdEsArgs {
+  const void* f;
+  void* Q;
+  int f_double;
+  int N, Nv;
+  const double* c0;
+  double cw, prefac, omega, Pr;
+};
+
+__global__ void __launch_bounds__(256) std_esbgk_relax_kernel(StdEsArgs a) {
+  const int pt = blockIdx.x, t = threadIdx.x;
+  __shared__ double red[6][256];
+  __shared__ double pv[12];  // rho, ux, uy, uz, T, det, A[6]
+  const int N = a.N, NN = N * N, Nv = a.Nv;
+  const size_t base = (size_t)pt * Nv;
+  auto fv = [&](int v) { return ld(a.f, a.f_double, base + v); };
+  auto cxyz = [&](int v, double& x, double& y, double& z) {
+    x = a.c0[v / NN]; y = a.c0[(v / N) % N]; z = a.c0[v % N];
+  };
+  // rho, u
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  for (int v = t; v < Nv; v += 256) {
+    double x, y, z;
+    cxyz(v, x, y, z);
+    const double f = fv(v);
+    s0 += f; s1 += f * x; s2 += f * y; s3 += f * z;
+  }
+  red[0][t] = s0; red[1][t] = s1; red[2][t] = s2; red[3][t] = s3;
+  block_sum256(red, 4);
+  if (t == 0) {
+    pv[1] = red[1][0] / red[0][0];
+    pv[2] = red[2][0] / red[0][0];
+    pv[3] = red[3][0] / red[0][0];
+    pv[0] = red[0][0] * a.cw;
+  }
+  __syncthreads();
+  const double rho = pv[0], ux = pv[1], uy = pv[2], uz = pv[3];
+  // T
+  double s4 = 0;
+  for (int v = t; v < Nv; v += 256) {
+    double x, y, z;
+    cxyz(v, x, y, z);
+    s4 += fv(v) * ((x - ux) * (x - ux) + (y - uy) * (y - uy) + (z - uz) * (z - uz));
+  }
+  __syncthreads();
+  red[0][t] = s4;
+  block_sum256(red, 1);
+  if (t == 0) pv[4] = red[0][0] * (a.cw / (1.5 * rho));
+  __syncthreads();
+  const double T = pv[4];
+  // covariance of (1 - 1/Pr) f + (1/Pr) f_M
+  const double wf = 1. - 1. / a.Pr, wm = 1. / a.Pr;
+  const double nm = rho / pow(M_PI * T, 1.5);
+  double m[6] = {0, 0, 0, 0, 0, 0};  // xx, yy, zz, xy, yz, zx
+  for (int v = t; v < Nv; v += 256) {
+    double x, y, z;
+    cxyz(v, x, y, z);
+    const double dx = x - ux, dy = y - uy, dz = z - uz;
+    const double fm = nm * exp(-(dx * dx + dy * dy + dz * dz) / T);
+    const double w = wf * fv(v) + wm * fm;
+    m[0] += dx * dx * w; m[1] += dy * dy * w; m[2] += dz * dz * w;
+    m[3] += dx * dy * w; m[4] += dy * dz * w; m[5] += dz * dx * w;
+  }
+  __syncthreads();
+  for (int i = 0; i < 6; ++i) red[i][t] = m[i];
+  block_sum256(red, 6);
+  if (t == 0) {
+    const double k = a.cw / rho;
+    const double m4 = red[0][0] * k, m5 = red[1][0] * k, m6 = red[2][0] * k,
+                 m7 = red[3][0] * k, m8 = red[4][0] * k, m9 = red[5][0] * k;
+    const double det = -m6 * m7 * m7 + 2 * m7 * m8 * m9 - m4 * m8 * m8 -
+                       m5 * m9 * m9 + m4 * m5 * m6;
+    pv[5] = det;
+    pv[6] = (m5 * m6 - m8 * m8) / det;   // 11
+    pv[7] = (m4 * m6 - m9 * m9) / det;   // 22
+    pv[8] = (m4 * m5 - m7 * m7) / det;   // 33
+    pv[9] = (m8 * m9 - m6 * m7) / det;   // 12
+    pv[10] = (m7 * m9 - m4 * m8) / det;  // 23
+    pv[11] = (m7 * m8 - m9 * m5) / det;  // 31
+  }
+  __syncthreads();
+  const double* A = pv + 6;
+  const double ne = rho / (pow(2 * M_PI, 1.5) * sqrt(pv[5]));
+  const double nu = a.prefac * (rho / pow(T, a.omega - 1.));
+  for (int v = t; v < Nv; v += 256) {
+    double x, y, z;
+    cxyz(v, x, y, z);
+    const double dx = x - ux, dy = y - uy, dz = z - uz;
+    const double q = A[0] * (dx * dx) + A[1] * (dy * dy) + A[2] * (dz * dz) +
+                     2 * A[3] * (dx * dy) + 2 * A[4] * (dy * dz) + 2 * A[5] * (dz * dx);
+    const double fes = ne * exp(-q / 2.);
+    const double r = ld(a.Q, a.f_double, base + v) + nu * (fes - fv(v));
+    st(a.Q, a.f_double, base + v, r);
+  }
+}
+
 // sum (x - y)^2 and sum y^2 in FP64 (residual of std/residual.py:15-29)
 __global__ void __launch_bounds__(512) residual_kernel(const void* x,
                                                        const void* y, int dbl,

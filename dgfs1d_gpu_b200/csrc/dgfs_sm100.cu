@@ -1557,6 +1557,23 @@ extern "C" int dgfs_dg_set_limiter(dgfs_dg_handle h, const double* wavg,
   return upload(&h->lim, t);
 }
 
+extern "C" int dgfs_std_esbgk_relax(dgfs_dg_handle h, const void* f, void* Q,
+                                    int32_t dtype, int32_t npts, double prefac,
+                                    double omega, double Pr, void* stream) {
+  if (!h || !f || !Q || npts < 0) return fail(DGFS_ERR_INVALID, "bad arguments");
+  if (dtype != DGFS_F32 && dtype != DGFS_F64)
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  if (!(Pr > 0)) return fail(DGFS_ERR_INVALID, "Pr must be > 0");
+  if (npts == 0) return DGFS_OK;
+  StdEsArgs a{};
+  a.f = f; a.Q = Q; a.f_double = dtype == DGFS_F64;
+  a.N = h->base.N; a.Nv = h->base.Nv; a.c0 = h->c0; a.cw = h->cw;
+  a.prefac = prefac; a.omega = omega; a.Pr = Pr;
+  std_esbgk_relax_kernel<<<npts, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+  DGFS_CUDA(cudaGetLastError());
+  return DGFS_OK;
+}
+
 extern "C" int dgfs_dg_limit_positivity(dgfs_dg_handle h, void* u,
                                         int32_t dtype, void* stream) {
   if (!h || !u) return fail(DGFS_ERR_INVALID, "null argument");

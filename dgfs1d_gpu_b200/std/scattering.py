@@ -243,3 +243,31 @@ class DGFSShakovDirectGLLScatteringModelStd(DGFSBGKDirectGLLScatteringModelStd):
 
     def _load_Pr(self):
         return float(self.cfg.lookupordefault('scattering-model', 'Pr', 2. / 3.))
+
+
+class DGFSESBGKDirectGLLScatteringModelStd(DGFSBGKDirectGLLScatteringModelStd):
+    """Explicit ES-BGK relaxation ``esbgk-direct-gll`` of dgfsStd1D
+    (std/scattering.py:1372-1637, std/kernels/scattering/esbgk-direct-gll.mako):
+    Q += prefac rho / T^(omega-1) (f_ES - f) with the Gaussian f_ES whose
+    covariance is the discrete second moment of (1-1/Pr) f + (1/Pr) f_M over
+    rho (f_M the grid Maxwellian), prefac = t0 Pr p0 / visc and Pr from
+    ``[scattering-model]`` (default 2/3).  One native kernel
+    (``dgfs_std_esbgk_relax``), one block per point."""
+    scattering_model = 'esbgk-direct-gll'
+    kind, nalph = 1, 11
+
+    def _load_Pr(self):
+        Pr = float(self.cfg.lookupordefault('scattering-model', 'Pr', 2. / 3.))
+        self._prefactor *= Pr            # t0 Pr p0 / visc
+        return Pr
+
+    def _relax(self, f, Q, stream=None):
+        if self._dg is None:
+            raise RuntimeError('esbgk-direct-gll: bind(dg) first')
+        if f.dtype != Q.dtype or not (f.is_contiguous() and Q.is_contiguous()):
+            raise ValueError('f and Q must be contiguous with the same dtype')
+        npts = f.numel() // self.vm.vsize()
+        nat.check(nat.lib().dgfs_std_esbgk_relax(
+            self._dg._h, ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(Q.data_ptr()),
+            _DT[f.dtype], npts, self._prefactor, self._omega, self._Pr,
+            _stream_ptr(stream)))

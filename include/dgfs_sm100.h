@@ -277,6 +277,16 @@ int dgfs_dg_limit_positivity(dgfs_dg_handle h, void* u, int32_t dtype,
 int dgfs_dg_set_upwind(dgfs_dg_handle h, const double* Dpos, const double* Dneg,
                        int32_t swap);
 
+/* Explicit ES-BGK relaxation of dgfsStd1D (esbgk-direct-gll, the fs of
+ * std/scattering.py:1540-1637 with std/kernels/scattering/esbgk-direct-gll.mako)
+ * on npts consecutive points of f (N^3 each, the grid of h): Q += prefac rho /
+ * T^(omega-1) (f_ES - f), f_ES the Gaussian whose covariance is the discrete
+ * second moment of (1-1/Pr) f + (1/Pr) f_M (f_M the grid Maxwellian of the
+ * point), normalised by rho.  f and Q have the same dtype. */
+int dgfs_std_esbgk_relax(dgfs_dg_handle h, const void* f, void* Q, int32_t dtype,
+                         int32_t npts, double prefac, double omega, double Pr,
+                         void* stream);
+
 /* Switch h's advection to the entropy-stable volume term of dgfsABE2std1D
  * (abstde2.py:363-367, eDeriv of astd/kernels/limiters.mako:162-195):
  * ux_k = -2 c_x sum_l Dr[k][l] aveL(u_k, u_l), aveL the logarithmic mean, Dr

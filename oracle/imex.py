@@ -420,3 +420,23 @@ class IMEX:
             self.step_no += 1
             return fn
         raise ValueError(k)
+
+
+def std_esbgk_relax(f, cv, cw, prefac, omega, Pr):
+    """Explicit ES-BGK relaxation of dgfsStd1D (esbgk-direct-gll fs,
+    std/scattering.py:1540-1637 with std/kernels/scattering/esbgk-direct-gll.mako):
+    Q = prefac rho / T^(omega-1) (f_ES - f), f_ES the Gaussian whose covariance
+    is the discrete second moment of (1-1/Pr) f + (1/Pr) f_M normalised by rho
+    (f_M the grid Maxwellian).  f: (Nv,)."""
+    s0 = f.sum()
+    u = np.array([(f * cv[i]).sum() / s0 for i in range(3)])
+    rho = s0 * cw
+    d = cv - u[:, None]
+    T = (f * (d * d).sum(axis=0)).sum() * (cw / (1.5 * rho))
+    fm = rho / (np.pi * T) ** 1.5 * np.exp(-(d * d).sum(axis=0) / T)
+    w = (1. - 1. / Pr) * f + (1. / Pr) * fm
+    S = np.array([[(d[i] * d[j] * w).sum() for j in range(3)] for i in range(3)]) * cw / rho
+    A = np.linalg.inv(S)
+    q = np.einsum('iv,ij,jv->v', d, A, d)
+    fes = rho / ((2 * np.pi) ** 1.5 * np.sqrt(np.linalg.det(S))) * np.exp(-q / 2.)
+    return prefac * (rho / T ** (omega - 1.)) * (fes - f)

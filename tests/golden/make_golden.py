@@ -933,9 +933,9 @@ def golden_entropy(R, Nv=8, Ne=4, K=3):
 
 
 def golden_std_relax(R, Nv=8, omega=0.81, prefac=3.7, Pr=2. / 3.):
-    """The explicit relaxation fs of dgfsStd1D's bgk-direct-gll and
-    shakov-direct-gll (std/scattering.py:1320-1371, 1764-1846): the kernels of
-    std/kernels/scattering/{bgk,shakov}-direct-gll.mako driven in fs's order
+    """The explicit relaxation fs of dgfsStd1D's bgk-, shakov- and
+    esbgk-direct-gll (std/scattering.py:1320-1371, 1764-1846, 1540-1637): the
+    kernels of std/kernels/scattering/*-direct-gll.mako driven in fs's order
     on one point, with NumPy sums in place of the block reductions of sum_."""
     from oracle.ref_build import RefModule, grid_for, render_template
     vsize = Nv ** 3
@@ -953,10 +953,10 @@ def golden_std_relax(R, Nv=8, omega=0.81, prefac=3.7, Pr=2. / 3.):
     gv = grid_for(vsize, blk)
     one = lambda v: np.array([float(v)])
     out = dict(f=f, cv=cv, cw=cw, omega=omega, prefac=prefac, Pr=Pr, Nv=Nv)
-    for name in ('bgk', 'shakov'):
+    for name in ('bgk', 'shakov', 'esbgk'):
         src = render_template('dgfs1D/std/kernels/scattering/%s-direct-gll.mako' % name,
                               cw=cw, vsize=vsize, prefac=prefac, nalph=5,
-                              nalphSk=8, omega=omega, Pr=Pr, block_size=256,
+                              nalphSk=8, nalphES=10, omega=omega, Pr=Pr, block_size=256,
                               Ne=1, dtype='double')
         K = RefModule(src, tag='std_%s_direct' % name)
         floc = np.zeros(vsize)
@@ -974,6 +974,20 @@ def golden_std_relax(R, Nv=8, omega=0.81, prefac=3.7, Pr=2. / 3.):
             K.launch('equiDistInit', 1, 1, *moms)
             fe = np.zeros(vsize)
             K.launch('output', gv, blk, 0, 0, 0, *moms, fe, floc, Q, cx, cy, cz)
+        elif name == 'esbgk':
+            m2 = np.zeros(vsize)
+            K.launch('mom2', gv, blk, cx, cy, cz, floc, m2, *moms)
+            moms.append(one(np.sum(m2)))
+            K.launch('equiDistInit', 1, 1, *moms)
+            fe = np.zeros(vsize)
+            K.launch('equiDistCompute', gv, blk, cx, cy, cz, fe, *moms)
+            es = [np.zeros(vsize) for _ in range(6)]
+            K.launch('mom2ES', gv, blk, cx, cy, cz, floc, fe, *moms[:4], *es)
+            momsES = [one(0.0) for _ in range(4)] + [one(np.sum(x)) for x in es]
+            K.launch('mom2ESNorm', 1, 1, *moms, *momsES)
+            feES = np.zeros(vsize)
+            K.launch('equiESDistCompute', gv, blk, cx, cy, cz, feES, *momsES)
+            K.launch('output', gv, blk, 0, 0, 0, moms[0], moms[4], feES, floc, Q)
         else:
             m2, q1, q2, q3 = (np.zeros(vsize) for _ in range(4))
             K.launch('mom23Sk', gv, blk, cx, cy, cz, floc, *moms, m2, q1, q2, q3)

@@ -137,3 +137,5 @@ def test_std_direct_relaxation_matches_reference():
     U14 = oim.moments_n(f[None], cv, cw, 14)
     Q = oim.model_collide(oim.ShakovModel(Pr), U14, f[None], cv, pre, om).ravel()
     assert _rel(Q, g['Q_shakov']) < 1e-12
+    # ES-BGK: the std form (discrete covariance of the grid Maxwellian mix)
+    assert _rel(oim.std_esbgk_relax(f, cv, cw, pre, om, Pr), g['Q_esbgk']) < 1e-12

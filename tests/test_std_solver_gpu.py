@@ -339,7 +339,8 @@ def test_command_line_run_and_restart(tmp_path, capsys):
     assert _rel(r.u.cpu().numpy(), s.u.cpu().numpy()) < 1e-14
 
 
-@pytest.mark.parametrize('model', ['bgk-direct-gll', 'shakov-direct-gll'])
+@pytest.mark.parametrize('model', ['bgk-direct-gll', 'shakov-direct-gll',
+                                   'esbgk-direct-gll'])
 def test_std_direct_relaxation_matches_oracle(model):
     """dgfsStd1D with ``[scattering-model] type = bgk-direct-gll`` /
     ``shakov-direct-gll`` (explicit relaxation at every point) over three
@@ -364,6 +365,8 @@ def test_std_direct_relaxation_matches_oracle(model):
     om_model = oim.BGKModel() if s.sm.kind == 0 else oim.ShakovModel(s.sm._Pr)
 
     def fs(f, g):
+        if s.sm.kind == 1:
+            return oim.std_esbgk_relax(f, cv, cw, pre, om, s.sm._Pr)
         U = oim.moments_n(f[None], cv, cw, s.sm.nalph)
         return oim.model_collide(om_model, U, f[None], cv, pre, om).ravel()
     collide = odg.collide_fs(b, fs)
@@ -380,20 +383,22 @@ def test_std_direct_relaxation_matches_oracle(model):
     assert _rel(s2.u.cpu().numpy(), got) < 1e-14
 
 
-@pytest.mark.parametrize('model', ['bgk', 'shakov'])
+@pytest.mark.parametrize('model', ['bgk', 'shakov', 'esbgk'])
 def test_std_direct_relaxation_kernel_matches_reference(model):
     """The native relaxation of one point (fs) against the golden output of
     the reference's std {bgk,shakov}-direct-gll kernels."""
     from dgfs1d_gpu_b200 import build
     build.build()
     from dgfs1d_gpu_b200.std.scattering import (
-        DGFSBGKDirectGLLScatteringModelStd, DGFSShakovDirectGLLScatteringModelStd)
+        DGFSBGKDirectGLLScatteringModelStd, DGFSESBGKDirectGLLScatteringModelStd,
+        DGFSShakovDirectGLLScatteringModelStd)
     from dgfs1d_gpu_b200.basis import get_basis
     from dgfs1d_gpu_b200.dg import DGOperator
     g = np.load(os.path.join(G, 'std_relax_N8.npz'))
     N = int(g['Nv'])
     cls = {'bgk': DGFSBGKDirectGLLScatteringModelStd,
-           'shakov': DGFSShakovDirectGLLScatteringModelStd}[model]
+           'shakov': DGFSShakovDirectGLLScatteringModelStd,
+           'esbgk': DGFSESBGKDirectGLLScatteringModelStd}[model]
     sm = object.__new__(cls)            # parameters from the golden case
     sm._Ne, sm._prefactor, sm._omega = 1, float(g['prefac']), float(g['omega'])
     sm._Pr = 1.0 if model == 'bgk' else float(g['Pr'])
