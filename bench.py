@@ -228,6 +228,23 @@ def stress_line(torch, timed, args):
             'finite': ok}
 
 
+def fp64_n48_line(torch, timed, args):
+    """The FP64 operator at N=48, the grid and rule of the reference's Lax
+    examples (M=6 half sphere, Nrho=6, on [-10, 10]^3), 24
+    points, seeded Couette-like distributions."""
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    from dgfs1d_gpu_b200.workloads import couette_distributions, vhs_mesh_params
+    prm = vhs_mesh_params(48, 6, 6, 10.0, False)
+    f = torch.tensor(couette_distributions(prm['c0'], 24, seed=9), device='cuda')
+    op = VHSOperator(**prm, precision='fp64', max_evals=24)
+    Q = torch.zeros_like(f)
+    ms = timed(lambda: op.eval(f, Q), 5, 3)
+    op.close()
+    del f, Q
+    return {'workload': 'VHS, N=48, M=6 half sphere, Nrho=6, 24 points, FP64',
+            'value': 24 / (ms * 1e-3), 'unit': UNIT, 'ms_per_step': ms}
+
+
 def stress_solver_line(torch, timed, args):
     """Steps of the stress configuration's solver: Mach-1.5 normal shock of
     hard spheres, N=48^3 on [-8,8]^3, M=32, Nrho=24, Ne=32, K=3 (96 points),
@@ -395,6 +412,7 @@ def main():
     # a bounded time on operator pairs, then timed and compared with FP64
     solver = solver_line(torch, timed, args)
     stress = stress_line(torch, timed, args)
+    fp64_n48 = fp64_n48_line(torch, timed, args)
     stress_solver = stress_solver_line(torch, timed, args)
     sur = None
     if not args.no_surrogate:
@@ -506,6 +524,7 @@ def main():
             'surrogate': sur,
             'solver_step': solver,
             'stress_n48': stress,
+            'fp64_n48': fp64_n48,
             'stress_solver_n48': stress_solver,
             'autotune_terms_ms': {str(k): round(v, 4) for k, v in tune.items()},
             'terms_cluster': op32.variant,
