@@ -24,7 +24,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(workload='vhs-couette-fp32-batched', N=32, M=12, Nrho=16,
-                L=6.0, points=24, Ne=8, K=3, omega=0.81, sphere='full-12pt')
+                L=6.0, points=24, Ne=8, K=3, omega=0.81, sphere='full-12pt',
+                parallelism='points sharded over ranks (weak)',
+                l2='flushed between timed steps (256 MB write)')
 METRIC = 'Q(f,f) evals/s at N=32^3 (FP32 fused, M=12, Nrho=16, 24 points)'
 UNIT = 'evals/s'
 
@@ -68,7 +70,8 @@ def cpu_oracle_rate(prm, f, budget_s=12.0, max_evals=4):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """nvidia-smi clock/throttle sampling (every 100 ms) over the bench's
+    timed regions."""
     Q = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
          'clocks_event_reasons.hw_slowdown,'
          'clocks_event_reasons.hw_thermal_slowdown,'
@@ -112,15 +115,26 @@ class ClockSampler:
     def summary(self):
         if not getattr(self, 'rows', None):
             return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
-        sm = [float(r[0]) for r in self.rows if r[0].replace('.', '').isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace('.', '').isdigit()]
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        rows = [r for r in self.rows if num(r[0]) is not None]
+        mx = [num(r[1]) for r in rows if num(r[1]) is not None]
+        pw = [num(r[2]) or 0.0 for r in rows]
+        # under load: power at least half of the run's maximum
+        hot = [r for r, p in zip(rows, pw) if pw and p >= 0.5 * max(pw)]
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
                  'sw_power_cap']
-        reasons = sorted({names[i] for r in self.rows for i in range(4)
+        reasons = sorted({names[i] for r in hot for i in range(4)
                           if r[4 + i].lower() == 'active'})
-        return {'sm_mhz': float(np.median(sm)) if sm else None,
+        return {'sm_mhz': float(np.median([num(r[0]) for r in hot]))
+                if hot else None,
                 'sm_max_mhz': max(mx) if mx else None,
-                'reasons': reasons, 'samples': len(self.rows)}
+                'reasons': reasons, 'samples': len(rows),
+                'samples_under_load': len(hot),
+                'power_w_max': max(pw) if pw else None}
 
 
 def fp32_fma_peak(torch):
@@ -135,34 +149,46 @@ def fp32_fma_peak(torch):
 
 
 def run_reference(args, rank, world):
-    """CPU oracle arm: rank 0 only, all host cores."""
+    """CPU oracle arm: rank 0 only, all host cores.  One step is a bounded
+    sample of the 24-point workload: 2 of its points, evaluated one after
+    another (the reference's serial per-point loop, std.py:352-356); the line
+    reports the measured time per step and the rate in evals/s."""
     if rank != 0:
         return
     prm, f = make_inputs(0)
     cores = os.cpu_count() or 1
-    rates = []
+    from oracle.collision import VHSTables, vhs_gll_fs
+    tab = VHSTables(prm['N'], prm['L'], prm['qz'], prm['qw'], prm['sz'],
+                    prm['sw'], prm['gamma'],
+                    sphere_factor=prm['sphere_factor'])
+    per_step = 2
+    k = 0
+
+    def step():
+        nonlocal k
+        for _ in range(per_step):
+            vhs_gll_fs(tab, prm['prefac'], f[k % len(f)])
+            k += 1
     for _ in range(args.warmup):
-        cpu_oracle_rate(prm, f, budget_s=2.0, max_evals=1)
-    t_all = 0.0
-    n_all = 0
+        step()
+    t0 = time.perf_counter()
     for _ in range(args.steps):
-        r, n, dt = cpu_oracle_rate(prm, f, budget_s=6.0, max_evals=2)
-        rates.append(r)
-        t_all += dt
-        n_all += n
-    value = n_all / t_all
+        step()
+    dt = time.perf_counter() - t0
+    value = args.steps * per_step / dt
     line = {
         'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT,
         'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
-        'ms_per_step': 1e3 * 24 / value, 'higher_is_better': True,
+        'ms_per_step': 1e3 * dt / args.steps, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
         'data': 'synthetic', 'config': dict(WORKLOAD),
         'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores,
                          'kind': 'port',
-                         'sample': f'{n_all} single-point evals of the NumPy/'
-                                   'SciPy oracle (reference algorithm, 3T+3 '
-                                   'FFTs per eval, complex128, '
-                                   f'scipy.fft workers={cores})'},
+                         'sample': f'each step = {per_step} of the 24 points, '
+                                   'one NumPy/SciPy oracle evaluation each '
+                                   '(reference algorithm, 3T+3 FFTs per eval, '
+                                   'complex128, scipy.fft '
+                                   f'workers={cores}); {args.steps} steps'},
         'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0,
                 'd2h_bytes_per_step': 0},
     }
@@ -204,10 +230,51 @@ def surrogate_line(torch, prm, fd, op32, op64, timed, args):
             'error_flag': net.device_error()}
 
 
+def _rel_l2(torch, a, b):
+    return float(torch.linalg.norm((a - b).double()) /
+                 torch.linalg.norm(b.double()))
+
+
+def _moment_errors(m32, m64):
+    """Per-field error of (Nqr, Ne, 10) moments: max over points of
+    |m32 - m64| / max |m64| for rho, U:y, T, Q:x, P:xy."""
+    from dgfs1d_gpu_b200.std.moments import FIELDS
+    out = {}
+    for name in ('rho', 'U:y', 'T', 'Q:x', 'P:xy'):
+        k = FIELDS.index(name)
+        scale = np.max(np.abs(m64[..., k]))
+        out[name] = float(np.max(np.abs(m32[..., k] - m64[..., k])) / scale) \
+            if scale > 0 else 0.0
+    return out
+
+
+def _solver_pair(torch, ini32, ini64):
+    from dgfs1d_gpu_b200.config import Config
+    from dgfs1d_gpu_b200.std.solver import DGFSStd1D
+    s32, s64 = DGFSStd1D(Config(ini32)), DGFSStd1D(Config(ini64))
+    if not torch.equal(s32.u, s64.u):
+        raise RuntimeError('FP32 and FP64 runs must start from the same state')
+    return s32, s64
+
+
+def _run_ms(torch, sol, nsteps):
+    """CUDA-event time of nsteps solver steps (graph replays), no L2 flush:
+    a solver run keeps its state resident."""
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(nsteps):
+        sol.step()
+    e.record()
+    e.synchronize()
+    return s.elapsed_time(e)
+
+
 def stress_line(torch, timed, args):
     """The stress-size operator: hard spheres (omega = 0.5), N=48^3 on
     [-8,8]^3, full-sphere M=32 design, Nrho=24, 96 points (Ne=32, K=3), FP32
-    mode, seeded Couette-like distributions."""
+    mode, seeded Couette-like distributions; error against the FP64 operator
+    on the same inputs (both with the conservation projection)."""
     from dgfs1d_gpu_b200.collision import VHSOperator
     from dgfs1d_gpu_b200.workloads import couette_distributions, vhs_mesh_params
     prm = vhs_mesh_params(48, 32, 24, 8.0, True, omega=0.5)
@@ -218,14 +285,26 @@ def stress_line(torch, timed, args):
     ms = timed(lambda: op.eval(f, Q), 5, 3)
     Q.zero_()
     op.eval(f, Q)
-    torch.cuda.synchronize()
-    ok = bool(torch.isfinite(Q).all())
     op.close()
-    del f, Q
-    return {'workload': 'HS, N=48, L=8, M=32 full sphere, Nrho=24, 96 points, '
-                        'FP32 + FP64 projection',
-            'value': 96 / (ms * 1e-3), 'unit': UNIT, 'ms_per_step': ms,
-            'finite': ok}
+    op64 = VHSOperator(**prm, precision='fp64', max_evals=16)
+    op64.set_projection(True)
+    Q64 = torch.zeros_like(f)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    op64.eval(f, Q64)
+    t1.record()
+    t1.synchronize()
+    err = _rel_l2(torch, Q, Q64)
+    op64.close()
+    out = {'workload': 'HS, N=48, L=8, M=32 full sphere, Nrho=24, 96 points, '
+                       'FP32 + FP64 projection',
+           'value': 96 / (ms * 1e-3), 'unit': UNIT, 'ms_per_step': ms,
+           'fp64_ms_per_step': t0.elapsed_time(t1),
+           'err_vs_fp64_rel_l2': err,
+           'finite': bool(torch.isfinite(Q).all())}
+    del f, Q, Q64
+    return out
 
 
 def fp64_n48_line(torch, timed, args):
@@ -242,48 +321,72 @@ def fp64_n48_line(torch, timed, args):
     op.close()
     del f, Q
     return {'workload': 'VHS, N=48, M=6 half sphere, Nrho=6, 24 points, FP64',
-            'value': 24 / (ms * 1e-3), 'unit': UNIT, 'ms_per_step': ms}
+            'value': 24 / (ms * 1e-3), 'unit': UNIT, 'ms_per_step': ms,
+            'err_vs_fp64_rel_l2': 0.0}
 
 
-def stress_solver_line(torch, timed, args):
+def stress_solver_line(torch, timed, args, nseg=2):
     """Steps of the stress configuration's solver: Mach-1.5 normal shock of
     hard spheres, N=48^3 on [-8,8]^3, M=32, Nrho=24, Ne=32, K=3 (96 points),
     inlet boundaries, lse-rk45 (5 RHS stages per step), FP32 operator, one
-    CUDA graph per step."""
-    from dgfs1d_gpu_b200.config import Config
+    CUDA graph per step; then an nseg-step segment of the same solver with
+    the FP32 and the FP64 operator from the same state, compared."""
     from dgfs1d_gpu_b200.configs import normal_shock_std_ini
-    from dgfs1d_gpu_b200.std.solver import DGFSStd1D
-    sol = DGFSStd1D(Config(normal_shock_std_ini()))
-    sol.capture_step()
-    ms = timed(sol.step, 3, 1)
-    ok = bool(torch.isfinite(sol.u).all())
-    return {'workload': 'normal shock Mach 1.5, HS, N=48, M=32, Nrho=24, '
-                        'Ne=32, K=3, lse-rk45, FP32 operator, graph per step',
-            'ms_per_step': ms, 'evals_per_s': 5 * 96 / (ms * 1e-3),
-            'projected_s_for_500_steps': 500 * ms * 1e-3, 'finite': ok}
+    s32, s64 = _solver_pair(torch, normal_shock_std_ini(precision_mode='fp32'),
+                            normal_shock_std_ini(precision_mode='fp64'))
+    s32.capture_step()
+    ms = timed(s32.step, 3, 1)
+    s32.u.copy_(s64.u)
+    ms32 = _run_ms(torch, s32, nseg)
+    ms64 = _run_ms(torch, s64, nseg)
+    err = _rel_l2(torch, s32.u, s64.u)
+    merr = _moment_errors(s32.bulk_moments(), s64.bulk_moments())
+    ok = bool(torch.isfinite(s32.u).all())
+    out = {'workload': 'normal shock Mach 1.5, HS, N=48, M=32, Nrho=24, '
+                       'Ne=32, K=3, lse-rk45, FP32 operator, graph per step',
+           'ms_per_step': ms, 'evals_per_s': 5 * 96 / (ms * 1e-3),
+           'projected_s_for_500_steps': 500 * ms * 1e-3,
+           'segment_steps': nseg, 'segment_ms_fp32': ms32,
+           'segment_ms_fp64_eager': ms64,
+           'err_vs_fp64_rel_l2': err, 'moment_err_vs_fp64': merr,
+           'finite': ok}
+    del s32, s64
+    return out
 
 
-def solver_line(torch, timed, args):
-    """The whole dgfsStd1D step on the batched FP32 Couette configuration
-    (ssp-rk3: three RHS stages of 24 points each), eager and as one CUDA
-    graph per step."""
-    from dgfs1d_gpu_b200.config import Config
-    from dgfs1d_gpu_b200.configs import couette_std_ini
-    from dgfs1d_gpu_b200.std.solver import DGFSStd1D
-    ini = couette_std_ini(Ne=8, K=3, Nv=32, Nrho=16, M=12, dev=6.0,
-                          scheme='ssp-rk3', dt=2e-4, nsteps=200,
-                          precision_mode='fp32', sphere='full')
-    sol = DGFSStd1D(Config(ini))
+def solver_line(torch, timed, args, nsteps=200):
+    """The batched FP32 Couette configuration as a run: dgfsStd1D, N=32,
+    M=12, Nrho=16, Ne=8, K=3, 200 ssp-rk3 steps (three RHS stages of 24
+    point evaluations each), one CUDA graph per step; the same 200 steps
+    with the plain FP64 operator from the same initial state, and the FP32
+    run's error against it."""
+    from dgfs1d_gpu_b200.configs import couette_c2_ini
+    s32, s64 = _solver_pair(torch, couette_c2_ini('fp32', nsteps),
+                            couette_c2_ini('fp64', nsteps))
     n = max(3, args.steps // 10)
-    ms_eager = timed(sol.step, n, 3)
-    sol.capture_step()
-    ms_graph = timed(sol.step, n, 3)
+    ms_eager = timed(s32.step, n, 3)
+    s32.u.copy_(s64.u)
+    s32.t, s32.nacptsteps = s64.t, 0
+    s32.capture_step()
+    s64.capture_step()
+    ms32 = _run_ms(torch, s32, nsteps)
+    ms64 = _run_ms(torch, s64, nsteps)
+    m32, m64 = s32.bulk_moments(), s64.bulk_moments()
     evals = 3 * 24
-    return {'workload': 'dgfsStd1D Couette, N=32, M=12, Nrho=16, Ne=8, K=3, '
-                        'ssp-rk3, FP32 operator',
-            'ms_per_step_graph': ms_graph, 'ms_per_step_eager': ms_eager,
-            'evals_per_s_graph': evals / (ms_graph * 1e-3),
-            'graph_launches_per_step': 1}
+    out = {'workload': 'dgfsStd1D Couette, N=32, M=12, Nrho=16, Ne=8, K=3, '
+                       'ssp-rk3, FP32 operator, u_y -0.1..0.1 and T 0.95..1.05 '
+                       'across x, 1% noise, dt=1.25e-4',
+           'steps': nsteps, 'ms_per_step_graph': ms32 / nsteps,
+           'ms_per_step_eager': ms_eager,
+           'fp64_ms_per_step_graph': ms64 / nsteps,
+           'run_s_fp32': ms32 * 1e-3, 'run_s_fp64': ms64 * 1e-3,
+           'speedup_fp32_vs_fp64': ms64 / ms32,
+           'evals_per_s_graph': evals * nsteps / (ms32 * 1e-3),
+           'graph_launches_per_step': 1,
+           'err_vs_fp64_rel_l2': _rel_l2(torch, s32.u, s64.u),
+           'moment_err_vs_fp64': _moment_errors(m32, m64)}
+    del s32, s64
+    return out
 
 
 def main():
@@ -356,13 +459,15 @@ def main():
             print(json.dumps({'kernel_only_ms_per_step': ms}), flush=True)
         return
 
+    # clocks sampled over the whole native run (every timed region below)
+    clk = ClockSampler(local).__enter__()
+
     # project autotuner: cluster size of the FP32 terms kernel, timed on this
     # very batch
     tune = op32.autotune(fd, Q, reps=3)
 
     # headline: FP32 fused operator, inputs resident in HBM
-    with ClockSampler(local) as clk:
-        ms32 = timed(lambda: op32.eval(fd, Q), args.steps, args.warmup)
+    ms32 = timed(lambda: op32.eval(fd, Q), args.steps, args.warmup)
     # plain FP64 path (same kernels, FP64 arithmetic, no split)
     ms64 = timed(lambda: op64.eval(fd, Q), max(3, args.steps // 2), 3)
 
@@ -372,7 +477,7 @@ def main():
     op32.eval(fd, Q32)
     op64.eval(fd, Q64)
     torch.cuda.synchronize()
-    err = float(torch.linalg.norm(Q32 - Q64) / torch.linalg.norm(Q64))
+    err = _rel_l2(torch, Q32, Q64)
 
     # end to end through the C ABI with host buffers: H2D f, eval, D2H Q
     fh = torch.tensor(f, dtype=torch.float64).pin_memory()
@@ -408,19 +513,20 @@ def main():
 
     fma_peak = fp32_fma_peak(torch)
 
-    # learned surrogate (FNO, BF16 tensor-core dense layers): trained here for
-    # a bounded time on operator pairs, then timed and compared with FP64
     solver = solver_line(torch, timed, args)
     stress = stress_line(torch, timed, args)
     fp64_n48 = fp64_n48_line(torch, timed, args)
     stress_solver = stress_solver_line(torch, timed, args)
+    # learned surrogate (FNO, BF16 tensor-core dense layers): trained here for
+    # a bounded time on operator pairs, then timed and compared with FP64
     sur = None
     if not args.no_surrogate:
         sur = surrogate_line(torch, prm, fd, op32, op64, timed, args)
 
     # uneven multi-problem batch: 6 VHS problems (N=16/24/32) + 2 VSS
     # mixtures, one CUDA graph launch per stage vs the same launches issued
-    # one after another on one stream
+    # one after another on one stream; error against the same problems in
+    # the FP64 mode
     from dgfs1d_gpu_b200.batch import StageGraph
     from dgfs1d_gpu_b200.workloads_c3 import build_c3
     probs = build_c3(precision='fp32')
@@ -434,15 +540,27 @@ def main():
         for p in probs:
             p['fn']()
     ms_serial = timed(serial, b_steps, 3)
+    serial()
+    probs64 = build_c3(precision='fp64')
+    for p in probs64:
+        p['fn']()
+    torch.cuda.synchronize()
+    b_err = {}
+    for a, b in zip(probs, probs64):
+        qa = a['Q'] if isinstance(a['Q'], list) else [a['Q']]
+        qb = b['Q'] if isinstance(b['Q'], list) else [b['Q']]
+        b_err[a['name']] = max(_rel_l2(torch, x, y) for x, y in zip(qa, qb))
     batch = {'value': b_evals * world / (ms_graph * 1e-3), 'unit': UNIT,
              'ms_per_stage': ms_graph, 'graph_launches_per_stage': 1,
              'serial_stream_ms_per_stage': ms_serial,
              'problems': [p['name'] for p in probs],
              'evals_per_stage': b_evals,
+             'err_vs_fp64_rel_l2': b_err,
              'note': 'VSS evals count each (p,q) pair at each point'}
-    del sg
+    del sg, probs, probs64
 
     barrier()
+    clk.__exit__(None, None, None)
     if rank == 0:
         peaks = {}
         pth = os.path.join(ROOT, 'MEASURED_PEAKS.json')
@@ -451,18 +569,19 @@ def main():
         hbm_peak = peaks.get('hbm_gbs', 6650.0)
         peak_src = 'measured' if 'hbm_gbs' in peaks else 'fallback'
         n = 32 ** 3
-        Nrho, Mu = 16, 6
-        # terms kernel, per launch: per eval read F_g (n complex FP32) and the
-        # Nyquist-plane transforms (Nrho*Mu*3*N^2 complex FP32), write the
-        # packed radial-pair spectra H (Nrho/2 * n complex FP32); b1w
-        # (Nrho*n FP32) once
-        alg_bytes = E * (n * 8 + Nrho * Mu * 3 * 32 * 32 * 8 + Nrho // 2 * n * 8) \
-            + Nrho * n * 4
-        # flops per eval as executed: Mu*Nrho packed inverse and Nrho/2
-        # packed forward 3-D FFTs (5 n log2 n each) + the pointwise combine
-        # (~40 flops per point and term)
+        Nrho, Mu, M = 16, 6, 12
+        T = M * Nrho
         fft = 5 * n * np.log2(n)
-        alg_flops = E * ((Mu * Nrho + Nrho // 2) * fft + Mu * Nrho * n * 40)
+        # minimal exact algorithm per evaluation (the unit of work):
+        # 2T + Nrho + 3 transforms of n points and ~20 flops per point and
+        # term of pointwise work: 1.116 GFLOP at this configuration
+        min_flops_eval = (2 * T + Nrho + 3) * fft + 20 * T * n
+        # flops per terms-kernel launch as executed: Mu*Nrho packed inverse
+        # and Nrho/2 packed forward 3-D FFTs, ~40 flops per point and term
+        exec_flops = E * ((Mu * Nrho + Nrho // 2) * fft + Mu * Nrho * n * 40)
+        # compulsory HBM bytes per evaluation of the fused operator: read f,
+        # read and write Q (FP64 arrays)
+        compulsory = 3 * n * 8
         evals = E * world
         # DRAM bytes per launch of the terms kernel from the committed ncu
         # summary (dram__bytes_read.sum + dram__bytes_write.sum, one capture)
@@ -484,9 +603,12 @@ def main():
                    'sample': f'{ns} single-point evals ({dt:.1f} s) of the '
                              'NumPy/SciPy oracle of this workload '
                              f'(complex128, scipy.fft workers={cores})'}
+        value = job_rate(E, world, ms32)
+        achieved = value / world * min_flops_eval / 1e12
+        clocks = clk.summary()
         line = {
             'metric': METRIC,
-            'value': job_rate(E, world, ms32),
+            'value': value,
             'unit': UNIT,
             'n_gpus': world,
             'steps': args.steps,
@@ -497,8 +619,7 @@ def main():
             'vs_baseline': None,
             'dtype': 'f32',
             'data': 'synthetic',
-            'config': dict(WORKLOAD, parallelism=f'points-sharded x{world}',
-                           l2='flushed between timed steps (256 MB write)'),
+            'config': dict(WORKLOAD),
             'fp64_plain': {'value': evals / (ms64 * 1e-3), 'unit': UNIT,
                            'ms_per_step': ms64},
             'speedup_fp32_vs_fp64': ms64 / ms32,
@@ -506,17 +627,30 @@ def main():
             'e2e': {'value': evals / (ms_e2e * 1e-3), 'unit': UNIT,
                     'h2d_bytes_per_step': int(fh.numel() * 8),
                     'd2h_bytes_per_step': int(qh.numel() * 8)},
-            'roofline': {'bound': 'hbm', 'kernel': f'vhs_terms_fp32_kernel<32,{op32.variant}>',
-                         'achieved': alg_bytes / (terms_ms * 1e-3) / 1e9,
-                         'peak': hbm_peak, 'unit': 'GB/s',
-                         'frac': alg_bytes / (terms_ms * 1e-3) / 1e9 / hbm_peak,
-                         'traffic': traffic, 'peak_source': peak_src,
-                         'launch_ms': terms_ms},
-            'roofline_fp32': {'bound': 'fp32-fma',
-                              'achieved': alg_flops / (terms_ms * 1e-3) / 1e12,
-                              'peak': fma_peak, 'unit': 'TFLOP/s',
-                              'frac': alg_flops / (terms_ms * 1e-3) / 1e12 / fma_peak,
-                              'peak_source': 'measured by dgfs_fma_peak'},
+            'roofline': {
+                'bound': 'fp32-fma',
+                'kernel': f'vhs_terms_fp32_kernel<32,{op32.variant}> '
+                          '(dominant) within the whole operator',
+                'achieved': achieved, 'peak': fma_peak, 'unit': 'TFLOP/s',
+                'frac': achieved / fma_peak,
+                'flops_per_eval_minimal_algorithm': min_flops_eval,
+                'frac_executed': exec_flops / (terms_ms * 1e-3) / 1e12 / fma_peak,
+                'executed_flops_per_terms_launch': exec_flops,
+                'launch_ms': terms_ms,
+                'peak_source': 'measured in this run by dgfs_fma_peak (own '
+                               'FP32 FMA kernel, every SM); MEASURED_PEAKS.json '
+                               'has no FP32 figure',
+                'peak_clock_sm_mhz': clocks.get('sm_mhz'),
+                'traffic': traffic,
+                'hbm': {'traffic_per_terms_launch': traffic,
+                        'achieved_gbs': (traffic / (terms_ms * 1e-3) / 1e9
+                                         if traffic else None),
+                        'peak_gbs': hbm_peak, 'peak_source': peak_src,
+                        'frac': (traffic / (terms_ms * 1e-3) / 1e9 / hbm_peak
+                                 if traffic else None),
+                        'compulsory_bytes_per_step': compulsory * E,
+                        'traffic_over_compulsory': (traffic / (compulsory * E)
+                                                    if traffic else None)}},
             'stage_ms': dict(zip(['prologue', 'tables', 'maxwell_gain',
                                   'terms', 'epilogue'],
                                  [round(float(x), 4) for x in stage])),
@@ -529,7 +663,7 @@ def main():
             'autotune_terms_ms': {str(k): round(v, 4) for k, v in tune.items()},
             'terms_cluster': op32.variant,
             'cpu_baseline': cpu,
-            'clocks': clk.summary(),
+            'clocks': clocks,
             'gpu_launches': 6 * args.steps,
         }
         print(json.dumps(line), flush=True)

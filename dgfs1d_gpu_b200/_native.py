@@ -88,6 +88,14 @@ _SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
       ctypes.c_void_p]),
+    ('dgfs_vhs_eval2', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
+    ('dgfs_vhs_fs2', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_void_p]),
     ('dgfs_vhs_last_moments', ctypes.c_void_p, [ctypes.c_void_p]),
     ('dgfs_vhs_set_projection', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_vhs_variants', ctypes.c_int,

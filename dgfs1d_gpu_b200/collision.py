@@ -66,11 +66,8 @@ class VHSOperator:
         self.Nrho, self.M = d.Nrho, d.M
         self.variant = 0          # 0: the library's default cluster size
 
-    def eval(self, f, Q, src=None, dst=None, src_base=0, dst_base=0,
-             nevals=None, stream=None):
-        """Q[dst(i)] += Q(f[src(i)]) for i < nevals (slot-major arrays)."""
-        _check_dist(f, 'f')
-        _check_dist(Q, 'Q')
+    def _nevals(self, f, Q, src, dst, src_base, dst_base, nevals):
+        """Check the arrays and slot ranges; return the evaluation count."""
         nf, nq = f.numel() // self.n, Q.numel() // self.n
         if f.numel() % self.n or Q.numel() % self.n:
             raise ValueError('array sizes must be multiples of N^3')
@@ -81,16 +78,42 @@ class VHSOperator:
             if sl is None:
                 if base < 0 or base + nevals > cnt:
                     raise IndexError(f'{name} slots out of range')
-            else:
-                if sl.dtype != torch.int32 or not sl.is_cuda or len(sl) < nevals:
-                    raise TypeError(f'{name} must be a CUDA int32 tensor of '
-                                    f'length >= nevals')
+            elif sl.dtype != torch.int32 or not sl.is_cuda or len(sl) < nevals:
+                raise TypeError(f'{name} must be a CUDA int32 tensor of '
+                                f'length >= nevals')
+        return int(nevals)
+
+    def eval(self, f, Q, src=None, dst=None, src_base=0, dst_base=0,
+             nevals=None, stream=None):
+        """Q[dst(i)] += Q(f[src(i)]) for i < nevals (slot-major arrays)."""
+        _check_dist(f, 'f')
+        _check_dist(Q, 'Q')
+        nevals = self._nevals(f, Q, src, dst, src_base, dst_base, nevals)
         nat.check(nat.lib().dgfs_vhs_eval(
             self._h, ctypes.c_void_p(f.data_ptr()), _DT[f.dtype],
             ctypes.c_void_p(Q.data_ptr()), _DT[Q.dtype],
             ctypes.c_void_p(src.data_ptr() if src is not None else 0), int(src_base),
             ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
-            int(nevals), _stream_ptr(stream)))
+            nevals, _stream_ptr(stream)))
+
+    def eval2(self, f, g, Q, src=None, dst=None, src_base=0, dst_base=0,
+              nevals=None, stream=None):
+        """Bilinear Q[dst(i)] += Q(f[src(i)], g[src(i)]) (``vhs``): gain of
+        the pair (f, g), loss f * Re IFFT(b2 FFT(g)/n); f and g have the same
+        dtype and shape.  Two (FP64) or three (FP32) passes of the Q(h, h)
+        pipeline."""
+        _check_dist(f, 'f')
+        _check_dist(g, 'g')
+        _check_dist(Q, 'Q')
+        if g.dtype != f.dtype or g.shape != f.shape:
+            raise TypeError('f and g must have the same dtype and shape')
+        nevals = self._nevals(f, Q, src, dst, src_base, dst_base, nevals)
+        nat.check(nat.lib().dgfs_vhs_eval2(
+            self._h, ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(g.data_ptr()),
+            _DT[f.dtype], ctypes.c_void_p(Q.data_ptr()), _DT[Q.dtype],
+            ctypes.c_void_p(src.data_ptr() if src is not None else 0), int(src_base),
+            ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
+            nevals, _stream_ptr(stream)))
 
     def variants(self):
         """Cluster sizes of the FP32 terms kernel compiled for this N."""

@@ -85,6 +85,33 @@ uz = 0
 """
 
 
+def couette_c2_ini(precision_mode='fp32', nsteps=200, Ne=8, K=3, Nv=32,
+                   Nrho=16, M=12, dev=6.0, scheme='ssp-rk3', noise=0.01,
+                   seed=20261203):
+    """The batched FP32 Couette configuration: Ne=8, K=3 (24 points),
+    N=32 on [-6, 6]^3, the full 12-point design, Nrho=16, ssp-rk3, diffuse
+    walls at T=1 with u_y = -+0.1; initial Maxwellian (nondimensional) with
+    u_y linear from -0.1 to 0.1 across the slab and T linear from 0.95 to
+    1.05, times (1 + 0.01 U[-1, 1]) seeded noise; dt = 0.001/Ne as for the
+    12-point configuration (whose 52 Euler steps use 0.001/4)."""
+    ini = couette_std_ini(Ne=Ne, K=K, Nv=Nv, Nrho=Nrho, M=M, dev=dev,
+                          scheme=scheme, dt=0.001 / Ne, nsteps=nsteps,
+                          precision_mode=precision_mode, sphere='full')
+    head, rest = ini.split('[soln-ics]', 1)
+    tail = rest[rest.index('[soln-bcs-xlo]'):]
+    ics = f"""[soln-ics]
+type = maxwellian-expr-nondim
+rho = 1.0
+ux = 0.0
+uy = -0.1 + 0.2*x
+uz = 0.0
+T = 0.95 + 0.1*x
+noise = {noise}
+seed = {seed}
+"""
+    return head + ics + tail
+
+
 def couette_bi_ini(Ne=3, K=3, Nv=8, Nrho=4, M=6, Mpre=12, dev=5.0,
                    scheme='euler', dt=0.0005, nsteps=3, uwall=0.1,
                    noise=0.02, seed=20261203, compat=0,

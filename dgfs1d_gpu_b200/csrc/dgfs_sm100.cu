@@ -470,11 +470,18 @@ static int launch_terms32(int c, const VhsTermsArgs& a, int nevals, int Nrho,
   return fail(DGFS_ERR_UNSUPPORTED, "terms kernel cluster size not compiled in");
 }
 
+// One component of the bilinear form: the pipeline transforms
+// alpha f + beta g and adds prefac (cg Re G - cl f Re Lf) (dgfs_vhs_eval2).
+struct VhsBilin {
+  const void* g;
+  double alpha, beta, cg, cl;
+};
+
 template <int N>
 static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                    int q_double, const int32_t* src_slots, int src_base,
                    const int32_t* dst_slots, int dst_base, int nevals,
-                   cudaStream_t st) {
+                   cudaStream_t st, const VhsBilin* bl = nullptr) {
   constexpr int C64 = VhsClusters<N>::c64 > 0 ? VhsClusters<N>::c64 : 1;
   constexpr bool HAS64 = VhsClusters<N>::c64 > 0;
   constexpr int C32 = VhsClusters<N>::c32;
@@ -498,6 +505,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     a.c0 = h->c0; a.b2 = h->b2; a.cw = h->cw; a.split = fp32 ? 1 : 0;
     a.Fg = h->Fg; a.ReLf = h->ReLf; a.mhat = h->mhat; a.moments = h->moments;
     a.Fny = h->Fny;
+    if (bl) { a.g = bl->g; a.alpha = bl->alpha; a.beta = bl->beta; }
     const size_t smem = prologue_smem<N, CPRO>();
     if ((rc = launch_cluster(vhs_prologue_kernel<N, CPRO>, dim3(CPRO, nevals),
                              dim3(GPRO::NT), CPRO, smem, st, a)))
@@ -594,6 +602,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     a.Nrho = fp32 ? (h->Nrho + 1) / 2 : h->Nrho;  // FP32: packed radial pairs
     a.project = h->project; a.c0 = h->c0; a.cw = h->cw;
     for (int i = 0; i < 25; ++i) a.Ginv[i] = h->Ginv[i];
+    if (bl) { a.bilinear = 1; a.cg = bl->cg; a.cl = bl->cl; }
     const size_t smem = epilogue_smem<N, CEPI>();
     if ((rc = launch_cluster(vhs_epilogue_kernel<N, CEPI>, dim3(CEPI, nevals),
                              dim3(GEPI::NT), CEPI, smem, st, a)))
@@ -604,12 +613,71 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
   return DGFS_OK;
 }
 
+static int vhs_eval_impl(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
+                         void* Q, int32_t q_dtype, const int32_t* src_slots,
+                         int32_t src_base, const int32_t* dst_slots,
+                         int32_t dst_base, int32_t nevals, void* stream,
+                         const VhsBilin* bl);
+
 extern "C" int dgfs_vhs_eval(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
                              void* Q, int32_t q_dtype,
                              const int32_t* src_slots, int32_t src_base,
                              const int32_t* dst_slots, int32_t dst_base,
                              int32_t nevals, void* stream) {
   NvtxRange nvtx_range("dgfs_vhs_eval");
+  return vhs_eval_impl(h, f, f_dtype, Q, q_dtype, src_slots, src_base,
+                       dst_slots, dst_base, nevals, stream, nullptr);
+}
+
+// Bilinear Q(f, g) of `vhs` (std/scattering.py:346-429): gain
+// B(f, g) = sum_pq FFT(IFFT(cos a F) IFFT(cos a G) + IFFT(sin a F) IFFT(sin a G))
+// (weighted by b1), loss f Re IFFT(b2 G).  B is symmetric and bilinear with
+// B(h, h) the gain of Q(h, h), so it is evaluated by polarisation through
+// the Q(h, h) pipeline, whose kernels are unchanged:
+//   FP64: B(f, g) = (B(f+g, f+g) - B(f-g, f-g)) / 4, and by linearity
+//         Re IFFT(b2 G) = (Lf(f+g) - Lf(f-g)) / 2  (two passes);
+//   FP32: B(f, g) = (B(f+g, f+g) - B(f, f) - B(g, g)) / 2, loss from the g
+//         pass (three passes: every transformed input stays close to a
+//         Maxwellian, which the split of the FP32 mode needs; f - g is
+//         not).
+// Each pass adds prefac (cg Re G_h - cl f Re Lf_h) into Q.
+extern "C" int dgfs_vhs_eval2(dgfs_vhs_handle h, const void* f, const void* g,
+                              int32_t f_dtype, void* Q, int32_t q_dtype,
+                              const int32_t* src_slots, int32_t src_base,
+                              const int32_t* dst_slots, int32_t dst_base,
+                              int32_t nevals, void* stream) {
+  NvtxRange nvtx_range("dgfs_vhs_eval2");
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  if (!g) return fail(DGFS_ERR_INVALID, "null g");
+  const bool fp32 = h->precision == DGFS_PREC_FP32;
+  const VhsBilin p64[2] = {{g, 1.0, 1.0, 0.25, 0.5},
+                           {g, 1.0, -1.0, -0.25, -0.5}};
+  const VhsBilin p32[3] = {{g, 1.0, 1.0, 0.5, 0.0},
+                           {g, 1.0, 0.0, -0.5, 0.0},
+                           {g, 0.0, 1.0, -0.5, 1.0}};
+  const VhsBilin* parts = fp32 ? p32 : p64;
+  const int np = fp32 ? 3 : 2;
+  for (int i = 0; i < np; ++i)
+    if (int rc = vhs_eval_impl(h, f, f_dtype, Q, q_dtype, src_slots, src_base,
+                               dst_slots, dst_base, nevals, stream, parts + i))
+      return rc;
+  return DGFS_OK;
+}
+
+extern "C" int dgfs_vhs_fs2(dgfs_vhs_handle h, const void* f, const void* g,
+                            void* Q, int32_t dtype, int32_t Ne, int32_t elem,
+                            int32_t modein, int32_t modeout, void* stream) {
+  if (Ne <= 0 || elem < 0 || elem >= Ne || modein < 0 || modeout < 0)
+    return fail(DGFS_ERR_INVALID, "bad Ne/elem/mode");
+  return dgfs_vhs_eval2(h, f, g, dtype, Q, dtype, nullptr, modein * Ne + elem,
+                        nullptr, modeout * Ne + elem, 1, stream);
+}
+
+static int vhs_eval_impl(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
+                         void* Q, int32_t q_dtype, const int32_t* src_slots,
+                         int32_t src_base, const int32_t* dst_slots,
+                         int32_t dst_base, int32_t nevals, void* stream,
+                         const VhsBilin* bl) {
   if (!h) return fail(DGFS_ERR_INVALID, "null handle");
   if (nevals < 0) return fail(DGFS_ERR_INVALID, "negative nevals");
   if (nevals == 0) return DGFS_OK;
@@ -626,11 +694,11 @@ extern "C" int dgfs_vhs_eval(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
     const int32_t* ds = dst_slots ? dst_slots + off : nullptr;
     int rc;
     switch (h->N) {
-      case 8: rc = vhs_run<8>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
-      case 16: rc = vhs_run<16>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
-      case 24: rc = vhs_run<24>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
-      case 32: rc = vhs_run<32>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
-      case 48: rc = vhs_run<48>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 8: rc = vhs_run<8>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
+      case 16: rc = vhs_run<16>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
+      case 24: rc = vhs_run<24>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
+      case 32: rc = vhs_run<32>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
+      case 48: rc = vhs_run<48>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
       default: return fail(DGFS_ERR_UNSUPPORTED, "N not compiled in");
     }
     if (rc) return rc;
@@ -730,10 +798,10 @@ extern "C" int dgfs_fma_peak(double* tflops, void* stream) {
 // ---------------------------------------------------------------------------
 // Allocation-free VHS evaluation.
 //
-// For callers that cannot allocate device memory -- code running while a
-// CUDA stream is being captured into a graph by someone else, hosts whose
-// memory is owned by a pool they must not grow, or plugins loaded into a
-// process that forbids cudaMalloc after start-up.  All scratch of the FP64
+// For callers that cannot allocate device memory -- services whose device
+// memory is a fixed pool carved out at start-up, plugins loaded into a
+// process that forbids cudaMalloc once it is serving, and time loops that
+// cannot afford cudaMalloc's implicit device synchronisation.  All scratch of the FP64
 // evaluation (tables and per-evaluation buffers) lives in one file-scope
 // device array of kNoallocBytes; every GPU that loads this library holds it
 // until the process exits.  The array is shared by every call: two calls

@@ -38,6 +38,9 @@ namespace dgfs {
 struct VhsPrologueArgs {
   const void* f;              // input distribution (float or double)
   int f_double;               // 1: f is double
+  const void* g;              // optional second input (same dtype as f): the
+                              // transformed input is then alpha f + beta g
+  double alpha, beta;
   const int32_t* src_slots;   // device slot list or null
   int src_base;               // slot(i) = src_slots ? src_slots[i] : src_base+i
   const double* c0;           // [N] velocity grid (x, y and z)
@@ -114,6 +117,10 @@ struct VhsEpilogueArgs {
   const double* c0;           // [N]
   double cw;
   double Ginv[25];
+  // bilinear component (polarisation of the gain, see dgfs_vhs_eval2):
+  // Q += prefac (cg Re G - cl f Re Lf) instead of prefac (Re G - f Re Lf)
+  int bilinear;
+  double cg, cl;
 };
 
 __device__ __forceinline__ int slot_of(const int32_t* slots, int base, int i) {
@@ -178,7 +185,10 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
   T v[N];
 #pragma unroll
   for (int x = 0; x < N; ++x) {
-    v[x].x = load_real(a.f, a.f_double, fbase + ((size_t)x * N + y) * N + z);
+    const size_t idx = fbase + ((size_t)x * N + y) * N + z;
+    v[x].x = a.g ? a.alpha * load_real(a.f, a.f_double, idx) +
+                       a.beta * load_real(a.g, a.f_double, idx)
+                 : load_real(a.f, a.f_double, idx);
     v[x].y = 0.0;
   }
 
@@ -1537,7 +1547,9 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   for (int x = 0; x < N; ++x) {
     const size_t idx = ((size_t)x * N + y) * N + z;
     const double fv = load_real(a.f, a.f_double, fb + idx);
-    v[x].y = a.prefac * (v[x].x - fv * a.ReLf[(size_t)e * G::n + idx]);
+    const double lf = a.ReLf[(size_t)e * G::n + idx];
+    v[x].y = a.bilinear ? a.prefac * (a.cg * v[x].x - a.cl * fv * lf)
+                        : a.prefac * (v[x].x - fv * lf);
   }
   double lam[5] = {0, 0, 0, 0, 0};
   if (a.project) {

@@ -3,7 +3,7 @@
 Interface of dgfs1D/sphericaldesign/__init__.py:82-105:
 ``get_sphquadrule('symmetric', rule='womersley', npts=M)`` returns an object
 with ``pts`` (M x 3).  The point sets are the published Womersley designs,
-bundled in ``data/womersley_symmetric.npz`` (see ``data/make_sphere_designs.py``);
+bundled in ``data/womersley_symmetric.npz`` (recipe: ``tests/golden/make_sphere_designs.py``);
 when several degrees share a point count the highest degree is chosen.
 """
 import os

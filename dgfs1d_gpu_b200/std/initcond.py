@@ -7,7 +7,9 @@ phase-space point from a seeded generator (keys ``noise``, ``seed``).
 ``maxwellian-expr`` / ``maxwellian-expr-nondim`` and ``sod-shock-tube-nondim``
 (initcond.py:144-238, 282-300, 385-434) evaluate their keys as expressions
 of the nondimensional solution-point coordinate ``x`` and the values of the
-``[non-dim]`` and ``[mesh]`` sections.
+``[non-dim]`` and ``[mesh]`` sections; the two Maxwellian-expression models
+also take the optional ``noise``/``seed`` keys of ``maxwellian-noise`` (no
+counterpart in the reference).
 ``normal-shock`` (no counterpart in the reference) joins an upstream and a
 downstream Maxwellian by a tanh ramp in x (keys ``rho1 T1 ux1 rho2 T2 ux2``,
 dimensional like ``maxwellian``; ``x0``, ``width`` in mesh units; optional
@@ -196,6 +198,8 @@ class DGFSMaxwellianExprInitConditionStd(DGFSInitConditionStd):
     def load_parameters(self, name):
         self._exprs = {k: self.cfg.lookupexpr(name, k)
                        for k in ('rho', 'ux', 'uy', 'uz', 'T')}
+        self._amp = float(self.cfg.lookupordefault(name, 'noise', 0.0))
+        self._seed = int(self.cfg.lookupordefault(name, 'seed', 20261203))
 
     def perform_precomputation(self):
         pass
@@ -222,6 +226,9 @@ class DGFSMaxwellianExprInitConditionStd(DGFSInitConditionStd):
         st = {k: np.broadcast_to(v, shape) for k, v in st.items()}
         usol[...] = _maxwellian(self.vm.cv(), st['rho'], st['ux'], st['uy'],
                                 st['uz'], st['T'])
+        if self._amp:
+            rng = np.random.default_rng(self._seed)
+            usol *= 1 + self._amp * rng.uniform(-1, 1, usol.shape)
 
 
 class DGFSMaxwellianExprNonDimInitConditionStd(

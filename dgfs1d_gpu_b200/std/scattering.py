@@ -128,18 +128,39 @@ class DGFSVHSGLLScatteringModelStd(DGFSScatteringModelStd):
 
 
 class DGFSVHSScatteringModelStd(DGFSVHSGLLScatteringModelStd):
-    """``vhs`` (std/scattering.py:317-429): the bilinear Q(f, g).
+    """``vhs`` (std/scattering.py:317-429): the bilinear Q(f, g), gain from
+    IFFT(cos a F) IFFT(cos a G) + IFFT(sin a F) IFFT(sin a G), loss
+    f IFFT(b2 G), with f and g read at the same slot of two arrays.
 
-    The drivers call it with g = V u and f = U^T u, which for the nodal
-    bases are the same coefficient (mode_sources); Q(f, f) is evaluated then.
+    Two arrays that are the same tensor are evaluated as Q(f, f) (one pass);
+    distinct arrays go through the native bilinear entry (two FP64 / three
+    FP32 passes), without comparing their contents on the host.
     """
     scattering_model = 'vhs'
 
-    def fs(self, d_arr_in1, d_arr_in2, d_arr_out, elem, modein, modeout):
-        if d_arr_in2 is not None and d_arr_in2 is not d_arr_in1 and \
-                not torch.equal(d_arr_in1, d_arr_in2):
-            raise NotImplementedError('bilinear Q(f, g) with g != f')
-        super().fs(d_arr_in1, d_arr_in1, d_arr_out, elem, modein, modeout)
+    @staticmethod
+    def _same(a, b):
+        return b is None or b is a or (
+            a.data_ptr() == b.data_ptr() and a.shape == b.shape
+            and a.dtype == b.dtype)
+
+    def fs(self, d_arr_in1, d_arr_in2, d_arr_out, elem, modein, modeout,
+           d_nu=None):
+        if self._same(d_arr_in1, d_arr_in2):
+            return super().fs(d_arr_in1, d_arr_in1, d_arr_out, elem, modein,
+                              modeout, d_nu=d_nu)
+        if d_nu is not None:
+            raise NotImplementedError('collision-frequency output (d_nu)')
+        Ne = self._Ne
+        self._op.eval2(d_arr_in1, d_arr_in2, d_arr_out,
+                       src_base=modein * Ne + elem,
+                       dst_base=modeout * Ne + elem, nevals=1)
+
+    def fs_batch(self, d_f, d_Q, src, dst, stream=None, d_g=None):
+        """Q[dst[i]] += Q(f[src[i]], g[src[i]]) for all i (g = f if absent)."""
+        if self._same(d_f, d_g):
+            return super().fs_batch(d_f, d_Q, src, dst, stream=stream)
+        self._op.eval2(d_f, d_g, d_Q, src=src, dst=dst, stream=stream)
 
 
 class DGFSBGKDirectGLLScatteringModelStd(DGFSScatteringModelStd):

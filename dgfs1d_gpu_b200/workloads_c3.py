@@ -77,5 +77,9 @@ def build_c3(precision='fp32', device='cuda', seed=20261203, project=True):
                 for q in range(2):
                     op.eval(p, q, fd[p], fd[q], Qd[p])
         problems.append(dict(name=f'vss{j}-N{N}-{pts}pts', op=op, f=fd, Q=Qd,
-                             nevals=4 * pts, fn=fn))
+                             nevals=4 * pts, fn=fn,
+                             params=dict(N=N, L=L, qz=qz, qw=qw, sz=sz,
+                                         sw=4 * np.pi / M, szpre=szpre,
+                                         masses=masses, gamma=gam, eta=eta,
+                                         prefac=pre)))
     return problems

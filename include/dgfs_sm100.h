@@ -90,6 +90,30 @@ int dgfs_vhs_fs(dgfs_vhs_handle h, const void* f, void* Q, int32_t dtype,
                 int32_t Ne, int32_t elem, int32_t modein, int32_t modeout,
                 void* stream);
 
+/* Bilinear Q(f, g), `vhs` in the reference (DGFSVHSScatteringModelStd.fs,
+ * std/scattering.py:346-429 with cosMul/sinMul/cplxMul/cplxMulAdd of
+ * vhs-gll.mako:260-397):  for i in [0, nevals):
+ *     Q[dst(i)] += prefac * (gain(f[src(i)], g[src(i)])
+ *                            - f[src(i)] * Re IFFT(b2 FFT(g[src(i)])/n))
+ * with the gain sum_pq FFT(IFFT(cos a F) IFFT(cos a G) + IFFT(sin a F)
+ * IFFT(sin a G)) weighted by b1 as in Q(f, f).  f and g are read at the same
+ * slot of two arrays of dtype f_dtype.  Evaluated by polarisation of the
+ * symmetric gain through the Q(h, h) pipeline: two passes in the FP64 mode,
+ * three in the FP32 mode (so twice / three times the cost of dgfs_vhs_eval).
+ * With g == f it equals dgfs_vhs_eval up to rounding. */
+int dgfs_vhs_eval2(dgfs_vhs_handle h, const void* f, const void* g,
+                   int32_t f_dtype, void* Q, int32_t q_dtype,
+                   const int32_t* src_slots, int32_t src_base,
+                   const int32_t* dst_slots, int32_t dst_base, int32_t nevals,
+                   void* stream);
+
+/* Reference-shaped bilinear evaluation: fs(d_arr_in1, d_arr_in2, d_arr_out,
+ * elem, modein, modeout) of std/scattering.py:346: f = d_arr_in1 and
+ * g = d_arr_in2, both read at slot modein*Ne + elem; dst = modeout*Ne + elem. */
+int dgfs_vhs_fs2(dgfs_vhs_handle h, const void* f, const void* g, void* Q,
+                 int32_t dtype, int32_t Ne, int32_t elem, int32_t modein,
+                 int32_t modeout, void* stream);
+
 /* Conservation projection (no counterpart in the reference, which has no
  * projection): when enabled, every evaluation subtracts from its increment
  * the minimal-L2 combination of (1, cx, cy, cz, |c|^2) that makes the five
@@ -353,9 +377,11 @@ int dgfs_axnpby(void* x0, int64_t n, int32_t dtype, double a0, int32_t nterms,
                 const void* const* xs, const double* as, void* stream);
 
 /* Allocation-free Q(f,f) in FP64, for callers that cannot allocate device
- * memory (code running inside someone else's stream capture, processes whose
- * device memory belongs to a pool they must not grow, plugins barred from
- * cudaMalloc after start-up).  No counterpart in the reference.  Same
+ * memory: services whose device memory is a fixed pool carved out at
+ * start-up (a cudaMalloc would fail or eat into the pool), plugins loaded
+ * into a host process that forbids cudaMalloc once it is serving, and time
+ * loops that cannot afford cudaMalloc's implicit device synchronisation.
+ * No counterpart in the reference.  Same
  * semantics as creating a DGFS_PREC_FP64 handle from `desc` and calling
  * dgfs_vhs_eval with double f and Q, but no handle is created and nothing is
  * allocated: tables and scratch live in one static 16 MiB device array that

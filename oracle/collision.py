@@ -76,15 +76,19 @@ def vhs_gll_fs(tab, prefac, f):
     fC = f.reshape(N, N, N).astype(np.complex128)
     FTf = _fwd(fC) / n
     a = tab.aa.reshape(Nrho, M, N, N, N)
-    t1 = np.cos(a) * FTf
-    t2 = np.sin(a) * FTf
-    t3 = _inv(t1)
-    t4 = _inv(t2)
-    t2 = t3 * t3 + t4 * t4
-    t1 = _fwd(t2)
-    intw = (tab.sphere_factor * tab.qw * tab.sw / n)[:, None, None, None]
-    QGh = np.sum(intw * tab.bb1.reshape(Nrho, N, N, N) * t1.sum(axis=1),
-                 axis=0)
+    intw = tab.sphere_factor * tab.qw * tab.sw / n
+    bb1 = tab.bb1.reshape(Nrho, N, N, N)
+    # the reference's batched plans run all Nrho*M terms at once; here one
+    # radial point at a time (same terms, bounded memory at N=48)
+    QGh = np.zeros((N, N, N), dtype=np.complex128)
+    for p in range(Nrho):
+        t1 = np.cos(a[p]) * FTf
+        t2 = np.sin(a[p]) * FTf
+        t3 = _inv(t1)
+        t4 = _inv(t2)
+        t2 = t3 * t3 + t4 * t4
+        t1 = _fwd(t2)
+        QGh += intw[p] * bb1[p] * t1.sum(axis=0)
     QG = _inv(QGh)
     fL = _inv(tab.bb2.reshape(N, N, N) * FTf)
     return (prefac * (QG.real - f.reshape(N, N, N) * fL.real)).ravel()
@@ -132,25 +136,22 @@ class VSSTables:
         self.b = np.empty((Nrho, M, self.n), dtype=np.complex128)
         self.c = np.zeros(self.n, dtype=np.complex128)
         self.qw, self.sw = np.asarray(qw), sw
+        szpre = np.asarray(szpre)
+        # Bpq[y, k] = (1 + sigma_y . sigma'_k)^eta, the kernel weight of the
+        # precompute loop (one launch per (x, y), a sum over k inside)
+        Bpq = np.power(1 + np.asarray(sz) @ szpre.T, eta)
+        lmat = np.stack([lx, ly, lz])
         for x in range(Nrho):
             fac = np.pi / L * qz[x]
             fac_b = swpre * pow(qz[x], gamma + 2)
             fac_c = qw[x] * sw * fac_b
+            Ld = fac * (szpre @ lmat)                       # [Mpre, n]
+            # sum_k Bpq[y,k] fac_b e^{-i mpq Ld_k}, sum_k Bpq[y,k] fac_c e^{-i Ld_k}
+            self.b[x] = fac_b * (Bpq @ np.exp(-1j * mpq * Ld))
+            self.c += fac_c * np.sum(Bpq @ np.exp(-1j * Ld), axis=0)
             for y in range(M):
                 self.aa[x, y] = fac * (sz[y, 0] * lx + sz[y, 1] * ly
                                        + sz[y, 2] * lz)
-                bs = np.zeros(self.n, dtype=np.complex128)
-                cs = np.zeros(self.n, dtype=np.complex128)
-                for k in range(Mpre):
-                    Bpq = pow(1 + sz[y, 0] * szpre[k, 0]
-                              + sz[y, 1] * szpre[k, 1]
-                              + sz[y, 2] * szpre[k, 2], eta)
-                    Ld = fac * ((szpre[k, 0] * lx) + (szpre[k, 1] * ly)
-                                + (szpre[k, 2] * lz))
-                    bs += Bpq * fac_b * (np.cos(mpq * Ld) - 1j * np.sin(mpq * Ld))
-                    cs += Bpq * fac_c * (np.cos(Ld) - 1j * np.sin(Ld))
-                self.b[x, y] = bs
-                self.c += cs
 
 
 def vss_fs(tab, prefac, mp, mq, f1, f2):

@@ -4,7 +4,7 @@ Test infrastructure only (see ``oracle/__init__.py``).  The reference's
 kernels are Mako templates of CUDA C (dgfs1D/std/kernels/scattering/
 vhs-gll.mako, dgfs1D/bi/kernels/scattering/vss.mako, dgfs1D/std/kernels/
 std.mako, ...).  This recipe renders a template from the reference checkout
-(``$DGFS_REF``, default /root/reference) with ``oracle.minimako``, prepends a
+(the directory named by ``$DGFS_REF``, which must be set) with ``oracle.minimako``, prepends a
 small prelude that makes the CUDA C compile as C++ (thread indices become
 globals set by generated launchers that loop over the grid), and compiles it
 with g++ into ``oracle/_ref/`` (git-ignored).  Nothing of the reference is
@@ -25,7 +25,7 @@ import numpy as np
 
 from .minimako import render
 
-REF = os.environ.get('DGFS_REF', '/root/reference')
+REF = os.environ.get('DGFS_REF')
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), '_ref')
 
 PRELUDE = r'''
@@ -52,6 +52,9 @@ static inline int max(int a, int b) { return a > b ? a : b; }
 
 
 def template_path(rel):
+    if not REF:
+        raise RuntimeError('set DGFS_REF to the reference checkout (the '
+                           'directory that holds dgfs1D/)')
     return os.path.join(REF, rel)
 
 

@@ -1,7 +1,7 @@
 """Generate the golden vectors of tests/golden from the reference itself.
 
-Run in a container where the reference checkout exists (``$DGFS_REF``,
-default /root/reference)::
+Run in a container where the reference checkout exists, with ``$DGFS_REF``
+set to it (the directory that holds dgfs1D/)::
 
     python tests/golden/make_golden.py
     python tests/golden/make_golden.py penalty-models   # only the ES-BGK/Shakov files
@@ -37,7 +37,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-REF = os.environ.get('DGFS_REF', '/root/reference')
+REF = os.environ.get('DGFS_REF')
 SEED = 20261203
 
 
@@ -98,6 +98,9 @@ def _install_stubs():
 
 
 def _import_reference():
+    if not REF:
+        raise SystemExit('set DGFS_REF to the reference checkout (the '
+                         'directory that holds dgfs1D/)')
     _install_stubs()
     sys.path.insert(0, REF)
     import dgfs1D.nputil as nputil

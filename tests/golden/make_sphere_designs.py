@@ -4,12 +4,14 @@ The DGFS spherical-quadrature loader (dgfs1D/sphericaldesign/__init__.py:43-105
 in the reference) reads Womersley's antipodally symmetric spherical designs,
 stored one point per line as ``womersley-ssDDD-mNNNNN.txt`` (DDD = design
 degree, NNNNN = point count).  This script converts those published point sets
-into ``womersley_symmetric.npz`` beside it, keyed ``ss<DDD>_m<NNNNN>``, so the
-package can load them on machines where the reference checkout is absent.
+into ``dgfs1d_gpu_b200/data/womersley_symmetric.npz``, keyed
+``ss<DDD>_m<NNNNN>``, so the package can load them on machines where the
+reference checkout is absent.
 
-Usage::
+Usage (the directory argument defaults to
+``$DGFS_REF/dgfs1D/sphericaldesign/symmetric``)::
 
-    python make_sphere_designs.py /path/to/dgfs1D/sphericaldesign/symmetric
+    python tests/golden/make_sphere_designs.py [/path/to/sphericaldesign/symmetric]
 """
 import os
 import re
@@ -29,12 +31,20 @@ def main(srcdir):
         if len(pts) != int(m.group(2)):
             raise ValueError(f'{name}: expected {m.group(2)} points')
         out['ss%03d_m%05d' % (int(m.group(1)), int(m.group(2)))] = pts
-    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)),
+    root = os.path.dirname(os.path.dirname(os.path.dirname(
+        os.path.abspath(__file__))))
+    dst = os.path.join(root, 'dgfs1d_gpu_b200', 'data',
                        'womersley_symmetric.npz')
     np.savez_compressed(dst, **out)
     print(f'wrote {len(out)} designs to {dst}')
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else
-         '/root/reference/dgfs1D/sphericaldesign/symmetric')
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    elif os.environ.get('DGFS_REF'):
+        main(os.path.join(os.environ['DGFS_REF'], 'dgfs1D', 'sphericaldesign',
+                          'symmetric'))
+    else:
+        raise SystemExit('give the directory of the symmetric designs, or set '
+                         'DGFS_REF to the reference checkout')

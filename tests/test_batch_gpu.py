@@ -2,8 +2,8 @@
 
 Six VHS problems (N = 16/24/32, 12-39 points) and two VSS mixtures (N=24)
 are captured as concurrent branches of one graph; a replay must give the
-same Q as the eager launches, bit for bit, and each VHS problem must match
-the oracle on sampled slots."""
+same Q as the eager launches, bit for bit, and every slot of every problem
+must match the oracle."""
 import numpy as np
 import pytest
 import torch
@@ -44,28 +44,55 @@ def test_graph_replay_equals_eager(problems):
     assert all(torch.isfinite(x).all() for a in graph for x in a)
 
 
-def test_vhs_problems_match_oracle(problems):
-    from oracle.collision import VHSTables, vhs_gll_fs
+def _projected(ref, prm):
+    """The minimal-L2 conservation correction the VHS problems apply."""
+    g = np.meshgrid(prm['c0'], prm['c0'], prm['c0'], indexing='ij')
+    cv = np.stack([x.ravel() for x in g])
+    phi = np.vstack([np.ones(cv.shape[1]), cv, np.sum(cv ** 2, axis=0)])
+    G = (phi * prm['cw']) @ phi.T
+    return ref - np.linalg.solve(G, (phi * prm['cw']) @ ref.T).T @ phi
+
+
+def test_every_slot_matches_oracle(problems):
+    """Every slot of every problem against the oracle: the six VHS problems
+    (FP32 mode with the FP64 conservation projection, applied to the
+    oracle's Q as well) and both VSS mixtures (each species' Q is the sum of
+    its two pair operators, Q_p = Q_p0(f_p, f_0) + Q_p1(f_p, f_1))."""
+    from oracle.collision import VHSTables, VSSTables, vhs_gll_fs, vss_fs
     for p in problems:
-        if not p['name'].startswith('vhs'):
-            continue
-        op = p['op']
-        prm = p['params']
-        tab = VHSTables(prm['N'], prm['L'], prm['qz'], prm['qw'], prm['sz'],
-                        prm['sw'], prm['gamma'],
-                        sphere_factor=prm['sphere_factor'])
-        f = p['f'].cpu().numpy()
         p['fn']()
-        torch.cuda.synchronize()
-        Q = p['Q'].cpu().numpy()
-        s = p['nevals'] - 1
-        ref = vhs_gll_fs(tab, prm['prefac'], f[s])
-        # the operators run with the conservation projection: apply the same
-        # minimal-L2 correction to the oracle's Q
-        g = np.meshgrid(prm['c0'], prm['c0'], prm['c0'], indexing='ij')
-        cv = np.stack([x.ravel() for x in g])
-        phi = np.vstack([np.ones(cv.shape[1]), cv, np.sum(cv ** 2, axis=0)])
-        G = (phi * prm['cw']) @ phi.T
-        ref = ref - np.linalg.solve(G, (phi * prm['cw']) @ ref) @ phi
-        err = np.linalg.norm(Q[s] - ref) / np.linalg.norm(ref)
-        assert err < 1e-5, f"{p['name']}: rel L2 {err:.3e}"
+    torch.cuda.synchronize()
+    vss_tabs = {}
+    for p in problems:
+        prm = p['params']
+        if p['name'].startswith('vhs'):
+            tab = VHSTables(prm['N'], prm['L'], prm['qz'], prm['qw'], prm['sz'],
+                            prm['sw'], prm['gamma'],
+                            sphere_factor=prm['sphere_factor'])
+            f = p['f'].cpu().numpy()
+            Q = p['Q'].cpu().numpy()
+            ref = np.stack([vhs_gll_fs(tab, prm['prefac'], x) for x in f])
+            ref = _projected(ref, prm)
+            for s in range(p['nevals']):
+                err = np.linalg.norm(Q[s] - ref[s]) / np.linalg.norm(ref[s])
+                assert err < 1e-5, f"{p['name']} slot {s}: rel L2 {err:.3e}"
+        else:
+            m = prm['masses']
+            fs = [x.cpu().numpy() for x in p['f']]
+            for sp in range(2):
+                Q = p['Q'][sp].cpu().numpy()
+                ref = np.zeros_like(Q)
+                for q in range(2):
+                    key = (prm['gamma'][sp, q], prm['eta'][sp, q],
+                           m[q] / (m[sp] + m[q]))
+                    if key not in vss_tabs:
+                        vss_tabs[key] = VSSTables(
+                            prm['N'], prm['L'], prm['qz'], prm['qw'], prm['sz'],
+                            prm['sw'], prm['szpre'], *key)
+                    ref += np.stack([vss_fs(vss_tabs[key], prm['prefac'][sp, q],
+                                            m[sp], m[q], fs[sp][s], fs[q][s])
+                                     for s in range(Q.shape[0])])
+                for s in range(Q.shape[0]):
+                    err = np.linalg.norm(Q[s] - ref[s]) / np.linalg.norm(ref[s])
+                    assert err < 1e-5, \
+                        f"{p['name']} species {sp} slot {s}: rel L2 {err:.3e}"

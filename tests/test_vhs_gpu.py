@@ -211,3 +211,153 @@ def test_n48_matches_oracle(lib, precision):
             err = _rel(Q.cpu().numpy()[s], refs[s])
             assert err < tol, f'N=48 {precision} variant {c} slot {s}: rel L2 {err:.3e}'
 
+
+
+@pytest.fixture(scope='module')
+def c5_case():
+    """The stress configuration's rule: hard spheres (omega = 0.5), N=48 on
+    [-8, 8]^3, the full 32-point spherical design, Nrho=24.  The oracle takes
+    about 6 s per point on 8 host cores (2307 transforms of 48^3)."""
+    vm, prefac, gamma, f = vhs_case(48, 32, 24, 8.0, True, omega=0.5, nslots=2)
+    tab = vhs_tables(vm, gamma)
+    refs = [vhs_gll_fs(tab, prefac, f[s]) for s in range(2)]
+    return vm, prefac, gamma, f, refs
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_n48_stress_rule_matches_oracle(lib, c5_case, precision):
+    """N=48 at the full stress rule (M=32 full sphere, Nrho=24): 16-CTA
+    clusters with three planes per CTA in both modes, 16 merged directions."""
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    vm, prefac, gamma, f, refs = c5_case
+    op = VHSOperator(**op_kwargs(vm, prefac, gamma), precision=precision,
+                     max_evals=2)
+    fd = torch.tensor(f, dtype=torch.float64, device='cuda')
+    Q = torch.zeros_like(fd)
+    op.eval(fd, Q)
+    torch.cuda.synchronize()
+    tol = FP64_TOL if precision == 'fp64' else FP32_TOL
+    for s in range(2):
+        err = _rel(Q.cpu().numpy()[s], refs[s])
+        assert err < tol, f'N=48 stress rule {precision} slot {s}: rel L2 {err:.3e}'
+    op.close()
+
+
+# -- bilinear Q(f, g) (``vhs``) ----------------------------------------------
+
+def _two_inputs(vm, nslots, seed=5):
+    """f: the Couette-like case distributions; g: Maxwellians of another
+    temperature and bulk velocity with their own 1% noise."""
+    from dgfs1d_gpu_b200.workloads import couette_distributions
+    c0 = vm.cv[2, :vm.Nv]
+    f = couette_distributions(c0, nslots, noise=0.01, seed=seed)
+    cv = vm.cv
+    rng = np.random.default_rng(seed + 1)
+    u = np.array([0.05, -0.08, 0.02])[:, None]
+    m = 1.1 / (np.pi * 1.2) ** 1.5 * np.exp(-np.sum((cv - u) ** 2, axis=0) / 1.2)
+    g = np.stack([m * (1 + 0.01 * rng.uniform(-1, 1, m.shape))
+                  for _ in range(nslots)])
+    return f, g
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_bilinear_matches_reference_kernel_golden(lib, precision):
+    """dgfs_vhs_eval2 vs the reference's own bilinear kernels
+    (cosMul/sinMul/cplxMul/cplxMulAdd, tests/golden/vhs_N8.npz Q_vhs)."""
+    import os
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    g = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'vhs_N8.npz'))
+    N = int(g['Nv'])
+    op = VHSOperator(N=N, L=float(g['L']), qz=g['qz'], qw=g['qw'], sz=g['sz'],
+                     sw=float(g['sw']), sphere_factor=2.0,
+                     gamma=float(g['gamma']), prefac=float(g['prefac']),
+                     cw=float(g['cw']), c0=g['cv'][2, :N], precision=precision,
+                     max_evals=4)
+    f = torch.tensor(g['f'], device='cuda').reshape(-1, N ** 3)
+    gg = torch.tensor(g['g'], device='cuda').reshape(-1, N ** 3)
+    Q = torch.zeros_like(f)
+    op.eval2(f, gg, Q)
+    torch.cuda.synchronize()
+    tol = FP64_TOL if precision == 'fp64' else FP32_TOL
+    ref = g['Q_vhs'].reshape(-1, N ** 3)
+    got = Q.cpu().numpy()
+    for s in range(ref.shape[0]):
+        assert _rel(got[s], ref[s]) < tol, s
+
+
+@pytest.mark.parametrize('case', [CASES[1], CASES[2]], ids=['N16', 'N32'])
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_bilinear_matches_oracle(lib, case, precision):
+    """Q(f, g) with g != f (another temperature and bulk velocity) against
+    the oracle's vhs_fs, slot lists and += included."""
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    from oracle.collision import vhs_fs
+    N, M, Nrho, dev, full = case
+    vm, prefac, gamma, _ = vhs_case(N, M, Nrho, dev, full, nslots=1)
+    f, g = _two_inputs(vm, 3)
+    tab = vhs_tables(vm, gamma)
+    op = VHSOperator(**op_kwargs(vm, prefac, gamma), precision=precision,
+                     max_evals=2)
+    fd, gd = torch.tensor(f, device='cuda'), torch.tensor(g, device='cuda')
+    Q0 = torch.randn_like(fd) * 1e-6
+    Q = Q0.clone()
+    src = torch.tensor([2, 0], dtype=torch.int32, device='cuda')
+    dst = torch.tensor([1, 2], dtype=torch.int32, device='cuda')
+    op.eval2(fd, gd, Q, src=src, dst=dst)
+    torch.cuda.synchronize()
+    tol = FP64_TOL if precision == 'fp64' else FP32_TOL
+    got = (Q - Q0).cpu().numpy()
+    for s, d in ((2, 1), (0, 2)):
+        ref = vhs_fs(tab, prefac, f[s], g[s])
+        assert _rel(got[d], ref) < tol, (precision, N, s)
+    assert torch.equal(Q[0], Q0[0])
+
+
+def test_bilinear_with_g_equal_f_is_q_ff(lib):
+    """Q(f, f) through the bilinear entry equals dgfs_vhs_eval (FP64)."""
+    from dgfs1d_gpu_b200.collision import VHSOperator
+    N, M, Nrho, dev, full = CASES[1]
+    vm, prefac, gamma, f = vhs_case(N, M, Nrho, dev, full, nslots=2)
+    op = VHSOperator(**op_kwargs(vm, prefac, gamma), precision='fp64',
+                     max_evals=2)
+    fd = torch.tensor(f, device='cuda')
+    Q1, Q2 = torch.zeros_like(fd), torch.zeros_like(fd)
+    op.eval(fd, Q1)
+    op.eval2(fd, fd.clone(), Q2)
+    torch.cuda.synchronize()
+    assert _rel(Q2.cpu().numpy(), Q1.cpu().numpy()) < 1e-12
+
+
+@pytest.mark.parametrize('precision', [None, 'fp32'])
+def test_vhs_plugin_fs_bilinear(lib, precision):
+    """The ``vhs`` plugin's fs(d_arr_in1, d_arr_in2, d_arr_out, elem, modein,
+    modeout) with two distinct arrays is Q(f, g) at slot modein*Ne + elem,
+    added into slot modeout*Ne + elem (std/scattering.py:346-429); with the
+    same array twice it is Q(f, f)."""
+    from dgfs1d_gpu_b200.config import Config
+    from dgfs1d_gpu_b200.configs import couette_std_ini
+    from dgfs1d_gpu_b200.std.solver import DGFSStd1D
+    from oracle.collision import VHSTables, vhs_fs, vhs_gll_fs
+    ini = couette_std_ini(Nv=16, Nrho=8, M=6, precision_mode=precision)
+    ini = ini.replace('type = vhs-gll', 'type = vhs')
+    s = DGFSStd1D(Config(ini))
+    assert s.sm.scattering_model == 'vhs'
+    vm, Ne = s.vm, s.mesh.Ne
+    u = s.u.reshape(-1, vm.vsize())
+    g = (u * (1 + 0.05 * torch.rand_like(u))).contiguous()
+    Q = torch.zeros_like(u)
+    s.sm.fs(u, g, Q, 2, 1, 0)          # elem 2, modein 1, modeout 0
+    s.sm.fs(u, u, Q, 3, 0, 2)          # the same array: Q(f, f)
+    torch.cuda.synchronize()
+    # double arrays: the sinc regulariser is the double one in both modes
+    tab = VHSTables(vm.Nv(), vm.L(), vm.qz(), vm.qw(), vm.sz(), vm.sw(),
+                    2 * (1 - s.sm.omega), sphere_factor=vm.sphere_factor())
+    uh, gh, Qh = u.cpu().numpy(), g.cpu().numpy(), Q.cpu().numpy()
+    tol = FP64_TOL if precision is None else FP32_TOL
+    ref1 = vhs_fs(tab, s.sm.prefac, uh[1 * Ne + 2], gh[1 * Ne + 2])
+    ref2 = vhs_gll_fs(tab, s.sm.prefac, uh[0 * Ne + 3])
+    assert _rel(Qh[0 * Ne + 2], ref1) < tol
+    assert _rel(Qh[2 * Ne + 3], ref2) < tol
+    mask = np.ones(len(Qh), bool)
+    mask[[2, 2 * Ne + 3]] = False
+    assert not Qh[mask].any()
