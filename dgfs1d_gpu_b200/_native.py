@@ -134,6 +134,11 @@ _SIGNATURES = [
       ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
       ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
       ctypes.c_int32, ctypes.c_void_p]),
+    ('dgfs_vss_eval_species', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),
+      ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_void_p]),
     ('dgfs_dg_create', ctypes.c_int,
      [ctypes.POINTER(DgDesc), ctypes.POINTER(ctypes.c_void_p)]),
     ('dgfs_dg_destroy', ctypes.c_int, [ctypes.c_void_p]),

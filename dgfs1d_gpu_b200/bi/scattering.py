@@ -88,3 +88,8 @@ class DGFSBiVSSScatteringModel(DGFSScatteringModelBi):
 
     def fs_batch(self, p, q, d_fp, d_fq, d_Qp, src, dst, stream=None):
         self._op.eval(p, q, d_fp, d_fq, d_Qp, src=src, dst=dst, stream=stream)
+
+    def fs_batch_species(self, p, d_fs, d_Qp, src, dst, stream=None):
+        """Q_p[dst] += sum_q Q_pq(f_p[src], f_q[src]): the partner loop of
+        bi.py:336-342 in one call."""
+        self._op.eval_species(p, d_fs, d_Qp, src=src, dst=dst, stream=stream)

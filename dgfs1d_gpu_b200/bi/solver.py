@@ -88,8 +88,7 @@ class DGFSBi1D:
         for side, bc in enumerate((self.bcl, self.bcr)):
             bc.at_time(t, self.dgs[p], side, p)
         self.dgs[p].advect(us[p], out)
-        for q in range(self.nspcs):
-            self.sm.fs_batch(p, q, us[p], us[q], out, self.src, self.dst)
+        self.sm.fs_batch_species(p, us, out, self.src, self.dst)
 
     def step(self):
         """One step and the post-processing of bi.py:360-381: residual,

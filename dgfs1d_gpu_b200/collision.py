@@ -220,6 +220,32 @@ class VSSOperator:
             ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
             int(nevals), _stream_ptr(stream)))
 
+    def eval_species(self, p, fs, Qp, src=None, dst=None, src_base=0,
+                     dst_base=0, nevals=None, stream=None):
+        """Q_p[dst(i)] += sum_q Q_pq(f_p[src(i)], f_q[src(i)]): every pair
+        of species p in one call (fs: one tensor per species)."""
+        if len(fs) != self.nspcs:
+            raise ValueError('fs must hold one array per species')
+        for i, t in enumerate(fs):
+            _check_dist(t, f'f[{i}]')
+            if t.dtype != fs[0].dtype or t.shape != fs[0].shape:
+                raise TypeError('the species arrays must share dtype and shape')
+        _check_dist(Qp, 'Q_p')
+        nf = fs[0].numel() // self.n
+        if nevals is None:
+            nevals = len(src) if src is not None else nf - src_base
+        for sl, base, cnt, name in ((src, src_base, nf, 'src'),
+                                    (dst, dst_base, Qp.numel() // self.n, 'dst')):
+            if sl is None and (base < 0 or base + nevals > cnt):
+                raise IndexError(f'{name} slots out of range')
+        ptrs = (ctypes.c_void_p * self.nspcs)(*[t.data_ptr() for t in fs])
+        nat.check(nat.lib().dgfs_vss_eval_species(
+            self._h, int(p), ptrs, _DT[fs[0].dtype],
+            ctypes.c_void_p(Qp.data_ptr()), _DT[Qp.dtype],
+            ctypes.c_void_p(src.data_ptr() if src is not None else 0), int(src_base),
+            ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
+            int(nevals), _stream_ptr(stream)))
+
     def close(self):
         if getattr(self, '_h', None):
             nat.lib().dgfs_vss_destroy(self._h)

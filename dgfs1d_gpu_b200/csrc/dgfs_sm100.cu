@@ -1265,18 +1265,25 @@ struct dgfs_vss_s {
   double* w = nullptr;     // [Nrho] w_r s_w / n
   VssPair pair[16];
   double2* F[2] = {nullptr, nullptr};  // [E][n] spectra of the two inputs
-  // FP32 mode scratch (Maxwellian split)
+  // FP32 mode scratch (Maxwellian split): per input slot s (the two inputs
+  // of a pair, or every species of dgfs_vss_eval_species) F_g, spectra and
+  // moments; per partner q of a species (slice q) the loss, tables, FP64
+  // Maxwellian gain and the FP32 terms
   double* c0 = nullptr;                // [N]
   double* b2dummy = nullptr;           // [n] unused real loss kernel
-  float2* Fg[2] = {nullptr, nullptr};  // [E][n]
-  double2* mhat[2] = {nullptr, nullptr};
-  double* mom[2] = {nullptr, nullptr};
-  double* ReLf = nullptr;              // [E][n]
-  float2* uv = nullptr;                // [E][T][2][3][N]
-  double2* hh = nullptr;               // [E][T][3][N]
-  double2* GM = nullptr;               // [E][n]
-  float2* H = nullptr;                 // [E][Nrho][n]
+  float2* Fg[4] = {};                  // [E][n]
+  double2* mhat[4] = {};               // [E][3][N]
+  double* mom[4] = {};                 // [E][5]
+  double* ReLf = nullptr;              // [nspcs][E][n]
+  float2* uv = nullptr;                // [nspcs][E][T][2][3][N]
+  double2* hh = nullptr;               // [nspcs][E][T][3][N]
+  double2* GM = nullptr;               // [nspcs][E][n]
+  float2* H = nullptr;                 // [nspcs][E][Nrho][n]
   double cw = 0;
+  // the FP64 Maxwellian gain of dgfs_vss_eval_species runs on `aux` (low
+  // priority) beside the FP32 terms kernel
+  cudaStream_t aux = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 static void free_vss(dgfs_vss_s* h) {
@@ -1287,11 +1294,16 @@ static void free_vss(dgfs_vss_s* h) {
     if (p.b32) cudaFree(p.b32);
     if (p.ph32) cudaFree(p.ph32);
   }
-  void* ptrs[] = {h->w, h->F[0], h->F[1], h->c0, h->b2dummy, h->Fg[0], h->Fg[1],
-                  h->mhat[0], h->mhat[1], h->mom[0], h->mom[1], h->ReLf, h->uv,
+  void* ptrs[] = {h->w, h->F[0], h->F[1], h->c0, h->b2dummy, h->ReLf, h->uv,
                   h->hh, h->GM, h->H};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  for (int s = 0; s < 4; ++s)
+    for (void* q : {(void*)h->Fg[s], (void*)h->mhat[s], (void*)h->mom[s]})
+      if (q) cudaFree(q);
+  if (h->fork) cudaEventDestroy(h->fork);
+  if (h->join) cudaEventDestroy(h->join);
+  if (h->aux) cudaStreamDestroy(h->aux);
   delete h;
 }
 
@@ -1419,11 +1431,21 @@ extern "C" int dgfs_vss_create(const dgfs_vss_desc* d, dgfs_vss_handle* out) {
     auto A = [&](auto** q, size_t cnt) {
       if (e1 == cudaSuccess) e1 = cudaMalloc((void**)q, cnt * sizeof(**q));
     };
-    for (int s2 = 0; s2 < 2; ++s2) {
+    const size_t ns = h->nspcs;
+    for (int s2 = 0; s2 < std::max(2, h->nspcs); ++s2) {
       A(&h->Fg[s2], E * n); A(&h->mhat[s2], E * 3 * N); A(&h->mom[s2], E * 5);
     }
-    A(&h->ReLf, E * n); A(&h->uv, E * T * 6 * N); A(&h->hh, E * T * 3 * N);
-    A(&h->GM, E * n); A(&h->H, E * h->Nrho * n); A(&h->b2dummy, n);
+    A(&h->ReLf, ns * E * n); A(&h->uv, ns * E * T * 6 * N);
+    A(&h->hh, ns * E * T * 3 * N); A(&h->GM, ns * E * n);
+    A(&h->H, ns * E * h->Nrho * n); A(&h->b2dummy, n);
+    if (e1 == cudaSuccess) {
+      int lo = 0, hi = 0;
+      e1 = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+      if (e1 == cudaSuccess)
+        e1 = cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, lo);
+      if (e1 == cudaSuccess) e1 = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+      if (e1 == cudaSuccess) e1 = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
+    }
     for (int pq = 0; pq < h->nspcs * h->nspcs; ++pq) {
       A(&h->pair[pq].b32, T * n); A(&h->pair[pq].ph32, T * 6 * N);
     }
@@ -1494,8 +1516,8 @@ static int vss_run(dgfs_vss_s* h, int p, int q, const void* fp, const void* fq,
                            dim3((h->n + 255) / 256, nevals), dim3(256), 0, st, ga)))
       return rc;
     VssTerms32Args tt{};
-    tt.Fgp = h->Fg[0]; tt.Fgq = h->Fg[1]; tt.ph = P.ph32; tt.uv = h->uv; tt.b = P.b32;
-    tt.w = h->w; tt.H = h->H; tt.Nrho = h->Nrho; tt.M = h->M;
+    tt.pr[0] = {h->Fg[0], h->Fg[1], P.ph32, h->uv, P.b32, h->H};
+    tt.w = h->w; tt.Nrho = h->Nrho; tt.M = h->M; tt.nevals = nevals;
     const size_t smem3 = 4 * slab_bytes(N, C3, sizeof(float2)) + 12 * N * sizeof(float2);
     if ((rc = launch_cluster(vss_terms32_kernel<N, C3>, dim3(C3, h->Nrho, nevals),
                              dim3(G3::NT), C3, smem3, st, tt)))
@@ -1526,6 +1548,139 @@ static int vss_run(dgfs_vss_s* h, int p, int q, const void* fp, const void* fq,
   const size_t smem = 4 * slab_bytes(N, C, sizeof(double2)) + 6 * N * sizeof(double2);
   return launch_cluster(vss_pair_kernel<N, C>, dim3(C, nevals), dim3(G::NT), C,
                         smem, st, a);
+}
+
+extern "C" int dgfs_vss_eval(dgfs_vss_handle h, int32_t p, int32_t q,
+                             const void* fp, const void* fq, int32_t f_dtype,
+                             void* Q, int32_t q_dtype, const int32_t* src_slots,
+                             int32_t src_base, const int32_t* dst_slots,
+                             int32_t dst_base, int32_t nevals, void* stream);
+
+// All pairs (p, q), q < nspcs, of one species p in FP32 mode:
+//   Q_p[dst] += sum_q Q_pq(f_p[src], f_q[src])
+// with one prologue per input species q (its F_g, Maxwellian spectra and
+// the loss of the pair, Re IFFT(c_pq F_q)), the 1-D tables per pair, the
+// FP64 Maxwellian gain per pair on the low-priority stream beside one FP32
+// terms launch over every pair, and one epilogue that sums the pairs'
+// spectra with their prefactors before a single inverse transform
+// (Re IFFT is linear: sum_q pref_pq Re IFFT(Ghat_pq) = Re IFFT(sum ...)).
+template <int N>
+static int vss_run_species(dgfs_vss_s* h, int p, const void* const* f,
+                           int f_double, void* Qp, int q_double,
+                           const int32_t* ss, int sb, const int32_t* ds,
+                           int db, int nevals, cudaStream_t st) {
+  constexpr int CPRO = VhsClusters<N>::cpro;
+  constexpr int CEPI = VhsClusters<N>::cepi;
+  constexpr int C3 = VssClusters32<N>::c;
+  using GPRO = Geo<N, CPRO>;
+  using GEPI = Geo<N, CEPI>;
+  using G3 = Geo<N, C3>;
+  const int ns = h->nspcs, T = h->Nrho * h->M;
+  const size_t E = h->max_evals, n = h->n;
+  auto ReLf = [&](int q) { return h->ReLf + q * E * n; };
+  auto uv = [&](int q) { return h->uv + q * E * T * 6 * N; };
+  auto hh = [&](int q) { return h->hh + q * E * T * 3 * N; };
+  auto GM = [&](int q) { return h->GM + q * E * n; };
+  auto H = [&](int q) { return h->H + q * E * h->Nrho * n; };
+  int rc;
+  for (int q = 0; q < ns; ++q) {
+    const VssPair& P = h->pair[p * ns + q];
+    VhsPrologueArgs a{};
+    a.f = f[q]; a.f_double = f_double; a.src_slots = ss; a.src_base = sb;
+    a.c0 = h->c0; a.b2 = h->b2dummy; a.b2c = P.c; a.cw = h->cw; a.split = 1;
+    a.Fg = h->Fg[q]; a.ReLf = ReLf(q); a.mhat = h->mhat[q]; a.moments = h->mom[q];
+    if ((rc = launch_cluster(vhs_prologue_kernel<N, CPRO>, dim3(CPRO, nevals),
+                             dim3(GPRO::NT), CPRO, prologue_smem<N, CPRO>(), st,
+                             a)))
+      return rc;
+  }
+  for (int q = 0; q < ns; ++q) {
+    VssTablesArgs ta{};
+    ta.mhat_p = h->mhat[p]; ta.mhat_q = h->mhat[q];
+    ta.ph = h->pair[p * ns + q].ph; ta.uv = uv(q); ta.hh = hh(q);
+    ta.T = T; ta.nevals = nevals;
+    if ((rc = launch_plain(vss_tables_kernel<N>, dim3((nevals * T * 3 + 127) / 128),
+                           dim3(128), 0, st, ta)))
+      return rc;
+  }
+  DGFS_CUDA(cudaEventRecord(h->fork, st));
+  DGFS_CUDA(cudaStreamWaitEvent(h->aux, h->fork, 0));
+  VssTerms32Args tt{};
+  for (int q = 0; q < ns; ++q) {
+    const VssPair& P = h->pair[p * ns + q];
+    tt.pr[q] = {h->Fg[p], h->Fg[q], P.ph32, uv(q), P.b32, H(q)};
+  }
+  tt.w = h->w; tt.Nrho = h->Nrho; tt.M = h->M; tt.nevals = nevals;
+  const size_t smem3 = 4 * slab_bytes(N, C3, sizeof(float2)) + 12 * N * sizeof(float2);
+  if ((rc = launch_cluster(vss_terms32_kernel<N, C3>, dim3(C3, h->Nrho, nevals * ns),
+                           dim3(G3::NT), C3, smem3, st, tt)))
+    return rc;
+  for (int q = 0; q < ns; ++q) {
+    VssGainArgs ga{};
+    ga.hh = hh(q); ga.b = h->pair[p * ns + q].b; ga.w = h->w; ga.GM = GM(q);
+    ga.Nrho = h->Nrho; ga.M = h->M;
+    if ((rc = launch_plain(vss_maxwell_gain_kernel<N>,
+                           dim3((h->n + 255) / 256, nevals), dim3(256), 0,
+                           h->aux, ga)))
+      return rc;
+  }
+  DGFS_CUDA(cudaEventRecord(h->join, h->aux));
+  DGFS_CUDA(cudaStreamWaitEvent(st, h->join, 0));
+  VhsEpilogueArgs ea{};
+  ea.f = f[p]; ea.f_double = f_double; ea.src_slots = ss; ea.src_base = sb;
+  ea.Q = Qp; ea.q_double = q_double; ea.dst_slots = ds; ea.dst_base = db;
+  ea.Nrho = h->Nrho; ea.project = 0; ea.c0 = h->c0; ea.cw = h->cw;
+  ea.nt = ns;
+  for (int q = 0; q < ns; ++q) {
+    ea.Ht[q] = H(q); ea.GMt[q] = GM(q); ea.ReLft[q] = ReLf(q);
+    ea.pref[q] = h->pair[p * ns + q].prefac;
+  }
+  return launch_cluster(vhs_epilogue_kernel<N, CEPI>, dim3(CEPI, nevals),
+                        dim3(GEPI::NT), CEPI, epilogue_smem<N, CEPI>(), st, ea);
+}
+
+extern "C" int dgfs_vss_eval_species(dgfs_vss_handle h, int32_t p,
+                                     const void* const* f, int32_t f_dtype,
+                                     void* Qp, int32_t q_dtype,
+                                     const int32_t* src_slots, int32_t src_base,
+                                     const int32_t* dst_slots, int32_t dst_base,
+                                     int32_t nevals, void* stream) {
+  NvtxRange nvtx_range("dgfs_vss_eval_species");
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  if (p < 0 || p >= h->nspcs) return fail(DGFS_ERR_INVALID, "species out of range");
+  if (!f || !Qp) return fail(DGFS_ERR_INVALID, "null f list or Q");
+  for (int q = 0; q < h->nspcs; ++q)
+    if (!f[q]) return fail(DGFS_ERR_INVALID, "null f in the species list");
+  if (nevals < 0 || src_base < 0 || dst_base < 0)
+    return fail(DGFS_ERR_INVALID, "negative nevals or slot base");
+  if ((f_dtype != DGFS_F32 && f_dtype != DGFS_F64) ||
+      (q_dtype != DGFS_F32 && q_dtype != DGFS_F64))
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  if (nevals == 0) return DGFS_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (h->precision != DGFS_PREC_FP32) {
+    // the FP64 mode (the reference's) evaluates the pairs one by one
+    for (int q = 0; q < h->nspcs; ++q)
+      if (int rc = dgfs_vss_eval(h, p, q, f[p], f[q], f_dtype, Qp, q_dtype,
+                                 src_slots, src_base, dst_slots, dst_base,
+                                 nevals, stream))
+        return rc;
+    return DGFS_OK;
+  }
+  for (int off = 0; off < nevals; off += h->max_evals) {
+    const int cnt = std::min(h->max_evals, nevals - off);
+    const int32_t* ss = src_slots ? src_slots + off : nullptr;
+    const int32_t* ds = dst_slots ? dst_slots + off : nullptr;
+    int rc;
+    switch (h->N) {
+      case 8: rc = vss_run_species<8>(h, p, f, f_dtype, Qp, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 16: rc = vss_run_species<16>(h, p, f, f_dtype, Qp, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      case 24: rc = vss_run_species<24>(h, p, f, f_dtype, Qp, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+      default: rc = vss_run_species<32>(h, p, f, f_dtype, Qp, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+    }
+    if (rc) return rc;
+  }
+  return DGFS_OK;
 }
 
 extern "C" int dgfs_vss_eval(dgfs_vss_handle h, int32_t p, int32_t q,

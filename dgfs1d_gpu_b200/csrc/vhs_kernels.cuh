@@ -53,6 +53,8 @@ struct VhsPrologueArgs {
   double* ReLf;               // out [nevals][n] Re IFFT(b2 F)
   double2* mhat;              // out [nevals][3][N] Maxwellian 1-D spectra (split)
   double* moments;            // out [nevals][5] rho, ux, uy, uz, T (split)
+                              // Fg, mhat and moments may be null (split):
+                              // the launch then only writes the loss
   float2* Fny;                // out (split) [nevals][3][N][N] Nyquist planes of
                               // F_g: [0][ly][lz] at lx=N/2, [1][lx][lz] at
                               // ly=N/2, [2][lx][ly] at lz=N/2
@@ -121,6 +123,14 @@ struct VhsEpilogueArgs {
   // Q += prefac (cg Re G - cl f Re Lf) instead of prefac (Re G - f Re Lf)
   int bilinear;
   double cg, cl;
+  // several pair operators into one output (the VSS species sum): when
+  // nt > 0, Ghat = sum_t pref[t] (GMt[t] + sum_p Ht[t][p]) and the loss is
+  // f sum_t pref[t] ReLft[t] (FP32 H); H, GM, ReLf and prefac are unused
+  int nt;
+  const void* Ht[4];
+  const double2* GMt[4];
+  const double* ReLft[4];
+  double pref[4];
 };
 
 __device__ __forceinline__ int slot_of(const int32_t* slots, int base, int i) {
@@ -232,7 +242,7 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
         rho = 0;
       }
       mom[0] = rho; mom[1] = ux; mom[2] = uy; mom[3] = uz; mom[4] = Tm;
-      if (rank == 0)
+      if (rank == 0 && a.moments)
         for (int k = 0; k < 5; ++k) a.moments[(size_t)e * 5 + k] = mom[k];
     }
     __syncthreads();
@@ -294,7 +304,7 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
       float2 g;
       g.x = (float)(Fv.x - mm.x);
       g.y = (float)(Fv.y - mm.y);
-      static_cast<float2*>(a.Fg)[gbase + j] = g;
+      if (a.Fg) static_cast<float2*>(a.Fg)[gbase + j] = g;
       if (a.Fny) {
         float2* ny = a.Fny + (size_t)e * 3 * N * N;
         if (lx == N / 2) ny[ly * N + lz] = g;
@@ -314,7 +324,8 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
     A[si] = Fv;
   }
   if (a.split && rank == 0)
-    for (int i = t; i < 3 * N; i += G::NT) a.mhat[(size_t)e * 3 * N + i] = mh[i];
+    if (a.mhat)
+      for (int i = t; i < 3 * N; i += G::NT) a.mhat[(size_t)e * 3 * N + i] = mh[i];
   __syncthreads();
   // loss: Re IFFT(b2 F); the Y-slab exchange reuses the slab once every CTA
   // of the cluster has read its own
@@ -1476,7 +1487,44 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   // UNR pairs per thread in flight per p so that the loads overlap
   constexpr int TOT2 = G::P * N * N / 2;
   constexpr int UNR = 8;
-  for (int b0 = t; b0 < TOT2; b0 += G::NT * UNR) {
+  for (int b0 = t; b0 < TOT2 && a.nt > 0; b0 += G::NT * UNR) {
+    T acc[UNR][2];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      acc[u][0] = T{0, 0};
+      acc[u][1] = T{0, 0};
+    }
+    for (int it = 0; it < a.nt; ++it) {
+      const double w = a.pref[it];
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const int j2 = b0 + u * G::NT;
+        if (j2 < TOT2) {
+          T g0 = a.GMt[it][(size_t)e * G::n + off + 2 * j2];
+          T g1 = a.GMt[it][(size_t)e * G::n + off + 2 * j2 + 1];
+          for (int p = 0; p < a.Nrho; ++p) {
+            const float4 h = reinterpret_cast<const float4*>(
+                static_cast<const float2*>(a.Ht[it]) +
+                ((size_t)e * a.Nrho + p) * G::n + off)[j2];
+            g0.x += (double)h.x; g0.y += (double)h.y;
+            g1.x += (double)h.z; g1.y += (double)h.w;
+          }
+          acc[u][0].x += w * g0.x; acc[u][0].y += w * g0.y;
+          acc[u][1].x += w * g1.x; acc[u][1].y += w * g1.y;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      const int j2 = b0 + u * G::NT;
+      if (j2 < TOT2) {
+        const int si = slab_index<N, C>(2 * j2);
+        A[si] = acc[u][0];
+        A[si + 1] = acc[u][1];
+      }
+    }
+  }
+  for (int b0 = t; b0 < TOT2 && a.nt == 0; b0 += G::NT * UNR) {
     T acc[UNR][2];
 #pragma unroll
     for (int u = 0; u < UNR; ++u) {
@@ -1547,6 +1595,13 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   for (int x = 0; x < N; ++x) {
     const size_t idx = ((size_t)x * N + y) * N + z;
     const double fv = load_real(a.f, a.f_double, fb + idx);
+    if (a.nt > 0) {
+      double lf = 0;
+      for (int it = 0; it < a.nt; ++it)
+        lf += a.pref[it] * a.ReLft[it][(size_t)e * G::n + idx];
+      v[x].y = v[x].x - fv * lf;
+      continue;
+    }
     const double lf = a.ReLf[(size_t)e * G::n + idx];
     v[x].y = a.bilinear ? a.prefac * (a.cg * v[x].x - a.cl * fv * lf)
                         : a.prefac * (v[x].x - fv * lf);

@@ -387,8 +387,8 @@ vss_pair_kernel(VssPairArgs a) {
 // and the product splits into u_M v_M, whose 3-D transform is the product of
 // the 1-D FP64 transforms H_a = FFT1(u_M,a v_M,a) (vss_maxwell_gain_kernel),
 // and the remainder u_M X_v + X_u (v_M + X_v), transformed in FP32
-// (vss_terms32_kernel, one cluster per (point, radial point), summed over
-// the directions in shared memory).  The radial sum, the final transform
+// (vss_terms32_kernel, one cluster per (pair, point, radial point), summed
+// over the directions in shared memory).  The radial sum, the final transform
 // and the loss f_p Re IFFT(c G) run in FP64 (prologue and epilogue kernels
 // of the VHS operator, with the complex loss kernel c).
 // ---------------------------------------------------------------------------
@@ -466,15 +466,20 @@ __global__ void __launch_bounds__(256) vss_maxwell_gain_kernel(VssGainArgs a) {
   a.GM[(size_t)e * n + l] = G;
 }
 
-struct VssTerms32Args {
+// Pointers of one species pair; a launch covers npair pairs, grid z =
+// npair * nevals (pair major).
+struct VssTerms32Pair {
   const float2* Fgp;       // [E][n] F_gp
   const float2* Fgq;       // [E][n] F_gq
   const float2* ph;        // [T][2][3][N] FP32 phase factors
   const float2* uv;        // [E][T][2][3][N] u_M,a, v_M,a
   const float2* b;         // [T][n] FP32 weights
-  const double* w;         // [Nrho]
   float2* H;               // out [E][Nrho][n]
-  int Nrho, M;
+};
+struct VssTerms32Args {
+  VssTerms32Pair pr[16];
+  const double* w;         // [Nrho]
+  int Nrho, M, nevals;
 };
 
 // z-pass of an inverse transform: rows of F (global, FP32) times the phase.
@@ -508,11 +513,12 @@ vss_terms32_kernel(VssTerms32Args a) {
   T* tab = Qh + G::SLAB;                   // [12N]: phases p, q | u_M | v_M
   const int t = threadIdx.x;
   const unsigned rank = cluster_rank();
-  const int r = blockIdx.y, e = blockIdx.z;
+  const int r = blockIdx.y, e = blockIdx.z % a.nevals;
+  const VssTerms32Pair& P = a.pr[blockIdx.z / a.nevals];
   const int yl = t / N, zz = t % N, yy = rank * G::P + yl;
   const int ybase = yl * G::PLANE + zz;
-  const T* Fp = a.Fgp + (size_t)e * G::n;
-  const T* Fq = a.Fgq + (size_t)e * G::n;
+  const T* Fp = P.Fgp + (size_t)e * G::n;
+  const T* Fq = P.Fgq + (size_t)e * G::n;
   const int Tt = a.Nrho * a.M;
   bool pending = false;
   auto exchange_cols = [&](const T* v) {
@@ -540,8 +546,8 @@ vss_terms32_kernel(VssTerms32Args a) {
     const int term = r * a.M + m;
     __syncthreads();
     for (int i = t; i < 6 * N; i += G::NT) {
-      tab[i] = a.ph[(size_t)term * 6 * N + i];
-      tab[6 * N + i] = a.uv[((size_t)e * Tt + term) * 6 * N + i];
+      tab[i] = P.ph[(size_t)term * 6 * N + i];
+      tab[6 * N + i] = P.uv[((size_t)e * Tt + term) * 6 * N + i];
     }
     __syncthreads();
     T v[N];
@@ -584,7 +590,7 @@ vss_terms32_kernel(VssTerms32Args a) {
 #pragma unroll
       for (int k = 0; k < N; ++k) w2[k] = A[base + k];
       fft<float, N, -1>(w2);
-      const T* brow = a.b + (size_t)term * G::n + ((size_t)lx * N + ly) * N;
+      const T* brow = P.b + (size_t)term * G::n + ((size_t)lx * N + ly) * N;
 #pragma unroll
       for (int k = 0; k < N; ++k) {
         const T pr = cmul(w2[k], brow[k]);
@@ -595,7 +601,7 @@ vss_terms32_kernel(VssTerms32Args a) {
   }
   __syncthreads();
   const float wr = (float)a.w[r];
-  T* H = a.H + ((size_t)e * a.Nrho + r) * G::n + (size_t)rank * G::P * N * N;
+  T* H = P.H + ((size_t)e * a.Nrho + r) * G::n + (size_t)rank * G::P * N * N;
   for (int j = t; j < G::P * N * N; j += G::NT) {
     const T q = Qh[slab_index<N, C>(j)];
     H[j] = make_float2(wr * q.x, wr * q.y);

@@ -74,8 +74,7 @@ def build_c3(precision='fp32', device='cuda', seed=20261203, project=True):
             for x in Qd:
                 x.zero_()
             for p in range(2):
-                for q in range(2):
-                    op.eval(p, q, fd[p], fd[q], Qd[p])
+                op.eval_species(p, fd, Qd[p])
         problems.append(dict(name=f'vss{j}-N{N}-{pts}pts', op=op, f=fd, Q=Qd,
                              nevals=4 * pts, fn=fn,
                              params=dict(N=N, L=L, qz=qz, qw=qw, sz=sz,

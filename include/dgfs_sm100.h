@@ -193,6 +193,19 @@ int dgfs_vss_eval(dgfs_vss_handle h, int32_t p, int32_t q, const void* f_p,
                   const int32_t* dst_slots, int32_t dst_base, int32_t nevals,
                   void* stream);
 
+/* Every pair of one species in one call (the species loop of the
+ * reference's mixture right-hand side, bi/bi.py:336-342, which calls fs once
+ * per partner q):  Q_p[dst(i)] += sum_q Q_pq(f_p[src(i)], f_q[src(i)]).
+ * f is a host array of nspcs device pointers (f[q] holds species q).  In
+ * the FP32 mode one launch per stage covers every pair (prologues once per
+ * input species, the FP64 Maxwellian gain beside the FP32 terms kernel, one
+ * epilogue summing the pairs); in the FP64 mode the pairs run one by one. */
+int dgfs_vss_eval_species(dgfs_vss_handle h, int32_t p, const void* const* f,
+                          int32_t f_dtype, void* Q_p, int32_t q_dtype,
+                          const int32_t* src_slots, int32_t src_base,
+                          const int32_t* dst_slots, int32_t dst_base,
+                          int32_t nevals, void* stream);
+
 /*
  * Nodal DG advection right-hand side of the single-species solver.
  * Replaces the kernels of the rhs() closure in dgfs1D/std/std.py:281-345:
