@@ -1318,7 +1318,7 @@ template <> struct VssClusters<8> { static constexpr int c = 1; };
 template <> struct VssClusters<16> { static constexpr int c = 2; };
 template <> struct VssClusters<24> { static constexpr int c = 6; };
 template <> struct VssClusters<32> { static constexpr int c = 16; };
-// FP32 terms kernel: four FP32 slabs per CTA
+// FP32 terms kernel: five FP32 slabs per CTA
 template <int N> struct VssClusters32;
 template <> struct VssClusters32<8> { static constexpr int c = 1; };
 template <> struct VssClusters32<16> { static constexpr int c = 2; };
@@ -1518,7 +1518,7 @@ static int vss_run(dgfs_vss_s* h, int p, int q, const void* fp, const void* fq,
     VssTerms32Args tt{};
     tt.pr[0] = {h->Fg[0], h->Fg[1], P.ph32, h->uv, P.b32, h->H};
     tt.w = h->w; tt.Nrho = h->Nrho; tt.M = h->M; tt.nevals = nevals;
-    const size_t smem3 = 4 * slab_bytes(N, C3, sizeof(float2)) + 12 * N * sizeof(float2);
+    const size_t smem3 = 5 * slab_bytes(N, C3, sizeof(float2)) + 24 * N * sizeof(float2);
     if ((rc = launch_cluster(vss_terms32_kernel<N, C3>, dim3(C3, h->Nrho, nevals),
                              dim3(G3::NT), C3, smem3, st, tt)))
       return rc;
@@ -1611,7 +1611,7 @@ static int vss_run_species(dgfs_vss_s* h, int p, const void* const* f,
     tt.pr[q] = {h->Fg[p], h->Fg[q], P.ph32, uv(q), P.b32, H(q)};
   }
   tt.w = h->w; tt.Nrho = h->Nrho; tt.M = h->M; tt.nevals = nevals;
-  const size_t smem3 = 4 * slab_bytes(N, C3, sizeof(float2)) + 12 * N * sizeof(float2);
+  const size_t smem3 = 5 * slab_bytes(N, C3, sizeof(float2)) + 24 * N * sizeof(float2);
   if ((rc = launch_cluster(vss_terms32_kernel<N, C3>, dim3(C3, h->Nrho, nevals * ns),
                            dim3(G3::NT), C3, smem3, st, tt)))
     return rc;

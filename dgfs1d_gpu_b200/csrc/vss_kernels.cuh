@@ -500,87 +500,138 @@ __device__ __forceinline__ void vss32_zpass(float2* A, const float2* F,
   for (int k = 0; k < N; ++k) A[base + k] = v[k];
 }
 
+// One cluster per (pair, point, radial point r); per direction m three
+// transforms, each with one cluster barrier (arrive after the stores into
+// the peers, wait before reading):
+//   T1 = IFFT3(phi_p F_gp) -> receive buffer R0 -> X_u (registers)
+//   T2 = IFFT3(phi_q F_gq) -> R1 -> X_v, combined with X_u into h
+//   T3 = FFT3(h) -> X-slab B -> b_rm (*) FFT(h) added into Qhat (shared)
+// The z-pass of T2 runs while T1's stores land, and the z-pass of T1 of the
+// next direction while T2's do.  Five slabs: A (z/y passes of T1 and T2),
+// B (T3), R0, R1, Qhat; the direction tables sit in a two-slot ring.
 template <int N, int C>
 __global__ void __launch_bounds__(Geo<N, C>::NT, 1)
 vss_terms32_kernel(VssTerms32Args a) {
   using G = Geo<N, C>;
   using T = float2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* A = reinterpret_cast<T*>(smem_raw);   // X-slab work buffer
-  T* Rb = A + G::SLAB;                     // Y-slab receive buffer
-  T* U = Rb + G::SLAB;                     // Y-slab: X_u pencils
-  T* Qh = U + G::SLAB;                     // X-slab spectral accumulator
-  T* tab = Qh + G::SLAB;                   // [12N]: phases p, q | u_M | v_M
+  T* A = reinterpret_cast<T*>(smem_raw);   // X-slab work buffer (inverse)
+  T* B = A + G::SLAB;                      // X-slab receive (forward)
+  T* R0 = B + G::SLAB;                     // Y-slab receive buffers R0, R1
+  T* Qh = R0 + 2 * G::SLAB;                // X-slab spectral accumulator
+  T* tab = Qh + G::SLAB;                   // [2][12N]: phases p, q | u_M | v_M
   const int t = threadIdx.x;
   const unsigned rank = cluster_rank();
   const int r = blockIdx.y, e = blockIdx.z % a.nevals;
   const VssTerms32Pair& P = a.pr[blockIdx.z / a.nevals];
   const int yl = t / N, zz = t % N, yy = rank * G::P + yl;
-  const int ybase = yl * G::PLANE + zz;
   const T* Fp = P.Fgp + (size_t)e * G::n;
   const T* Fq = P.Fgq + (size_t)e * G::n;
   const int Tt = a.Nrho * a.M;
-  bool pending = false;
-  auto exchange_cols = [&](const T* v) {
-    if (pending) cluster_wait();
-    push_cols_to_yslab<float, N, C>(Rb, t, rank, v);
-    cluster_arrive();
-    cluster_wait();
+  auto load_tables = [&](int m) {
+    T* dst = tab + (m & 1) * 12 * N;
+    const int term = r * a.M + m;
+    for (int i = t; i < 6 * N; i += G::NT) {
+      dst[i] = P.ph[(size_t)term * 6 * N + i];
+      dst[6 * N + i] = P.uv[((size_t)e * Tt + term) * 6 * N + i];
+    }
   };
-  auto release_receive = [&]() {
-    cluster_arrive();
-    pending = true;
+  uint32_t rb[C], bb[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    rb[c] = mapa_u32(smem_u32(R0), (uint32_t)c);
+    bb[c] = mapa_u32(smem_u32(B), (uint32_t)c);
+  }
+  // y-pass stores of an inverse transform into the peers' receive buffer buf
+  auto push_y = [&](int buf, const T* v) {
+    const int lx = rank * G::P + t / N, z = t % N;
+    const uint32_t off = (uint32_t)(buf * G::SLAB + lx * G::ROW + z) * 8u;
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+#pragma unroll
+      for (int j = 0; j < G::P; ++j)
+        st_cluster(rb[c] + off + (uint32_t)(j * G::PLANE) * 8u, v[c * G::P + j]);
   };
-  auto inverse = [&](const T* F, const T* tb, T* v) {
-    vss32_zpass<N, C>(A, F, tb, t, rank);
-    __syncthreads();
-    slab_col_load_fft<float, N, C, +1>(A, t, v);
-    exchange_cols(v);
-    yslab_load_pencil<float, N, C>(Rb, t, v);
-    release_receive();
-    fft<float, N, +1>(v);
+  auto col_load = [&](const T* S, T* v) {
+    const int base = (t / N) * G::PLANE + (t % N);
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = S[base + k * G::ROW];
   };
   for (int j = t; j < G::SLAB; j += G::NT) Qh[j] = T{0.f, 0.f};
+  load_tables(0);
+  __syncthreads();
+  vss32_zpass<N, C>(A, Fp, tab, t, rank);
+  __syncthreads();
 #pragma unroll 1
   for (int m = 0; m < a.M; ++m) {
+    const T* tb = tab + (m & 1) * 12 * N;
     const int term = r * a.M + m;
+    T v[N], Xu[N];
+    // T1: y-pass, stores into R0; the z-pass of T2 overlaps them
+    col_load(A, v);
+    __syncthreads();                 // A read; ring slot (m+1)&1 free
+    if (m + 1 < a.M) load_tables(m + 1);
+    fft<float, N, +1>(v);
+    push_y(0, v);
+    cluster_arrive();
+    vss32_zpass<N, C>(A, Fq, tb + 3 * N, t, rank);
     __syncthreads();
-    for (int i = t; i < 6 * N; i += G::NT) {
-      tab[i] = P.ph[(size_t)term * 6 * N + i];
-      tab[6 * N + i] = P.uv[((size_t)e * Tt + term) * 6 * N + i];
-    }
-    __syncthreads();
-    T v[N];
-    inverse(Fp, tab, v);                       // X_u
-#pragma unroll
-    for (int x = 0; x < N; ++x) U[ybase + x * G::ROW] = v[x];
-    inverse(Fq, tab + 3 * N, v);               // X_v
+    cluster_wait();
     {
-      const T* ut = tab + 6 * N;
-      const T* vt = tab + 9 * N;
+      const T* R = R0 + yl * G::PLANE + zz;
+#pragma unroll
+      for (int x = 0; x < N; ++x) Xu[x] = R[x * G::ROW];
+    }
+    fft<float, N, +1>(Xu);
+    // T2: y-pass, stores into R1; the z-pass of T1 of the next direction
+    // overlaps them
+    col_load(A, v);
+    __syncthreads();                 // A read; the tables of m+1 are stored
+    fft<float, N, +1>(v);
+    push_y(1, v);
+    cluster_arrive();
+    if (m + 1 < a.M) vss32_zpass<N, C>(A, Fp, tab + ((m + 1) & 1) * 12 * N, t, rank);
+    cluster_wait();
+    {
+      const T* R = R0 + G::SLAB + yl * G::PLANE + zz;
+#pragma unroll
+      for (int x = 0; x < N; ++x) v[x] = R[x * G::ROW];
+    }
+    fft<float, N, +1>(v);            // X_v
+    {
+      const T* ut = tb + 6 * N;
+      const T* vt = tb + 9 * N;
       const T uyz = cmul(ut[N + yy], ut[2 * N + zz]);
       const T vyz = cmul(vt[N + yy], vt[2 * N + zz]);
 #pragma unroll
       for (int x = 0; x < N; ++x) {
         const T uM = cmul(ut[x], uyz), vM = cmul(vt[x], vyz);
-        const T Xu = U[ybase + x * G::ROW], Xv = v[x];
+        const T Xv = v[x];
         const T a1 = cmul(uM, Xv);
-        const T a2 = cmul(Xu, make_float2(vM.x + Xv.x, vM.y + Xv.y));
+        const T a2 = cmul(Xu[x], make_float2(vM.x + Xv.x, vM.y + Xv.y));
         v[x] = make_float2(a1.x + a2.x, a1.y + a2.y);
       }
     }
-    fft<float, N, -1>(v);                      // forward: x pass
-    if (pending) cluster_wait();
-    push_pencils_to_xslab<float, N, C>(A, t, rank, v);
+    // T3: forward x-pass, stores into the peers' B, then y- and z-passes
+    // on B and the weighted accumulation into Qhat
+    fft<float, N, -1>(v);
+    {
+      const uint32_t off = (uint32_t)(yy * G::ROW + zz) * 8u;
+#pragma unroll
+      for (int c = 0; c < C; ++c)
+#pragma unroll
+        for (int j = 0; j < G::P; ++j)
+          st_cluster(bb[c] + off + (uint32_t)(j * G::PLANE) * 8u, v[c * G::P + j]);
+    }
     cluster_arrive();
     cluster_wait();
-    pending = false;
     {
       T w2[N];
-      slab_col_load_fft<float, N, C, -1>(A, t, w2);
+      col_load(B, w2);
+      fft<float, N, -1>(w2);
       const int base = (t / N) * G::PLANE + (t % N);
 #pragma unroll
-      for (int k = 0; k < N; ++k) A[base + k * G::ROW] = w2[k];
+      for (int k = 0; k < N; ++k) B[base + k * G::ROW] = w2[k];
     }
     __syncthreads();
     {
@@ -588,7 +639,7 @@ vss_terms32_kernel(VssTerms32Args a) {
       const int base = pl * G::PLANE + ly * G::ROW;
       T w2[N];
 #pragma unroll
-      for (int k = 0; k < N; ++k) w2[k] = A[base + k];
+      for (int k = 0; k < N; ++k) w2[k] = B[base + k];
       fft<float, N, -1>(w2);
       const T* brow = P.b + (size_t)term * G::n + ((size_t)lx * N + ly) * N;
 #pragma unroll
@@ -606,7 +657,6 @@ vss_terms32_kernel(VssTerms32Args a) {
     const T q = Qh[slab_index<N, C>(j)];
     H[j] = make_float2(wr * q.x, wr * q.y);
   }
-  if (pending) cluster_wait();
 }
 
 }  // namespace dgfs
