@@ -524,40 +524,55 @@ def main():
         sur = surrogate_line(torch, prm, fd, op32, op64, timed, args)
 
     # uneven multi-problem batch: 6 VHS problems (N=16/24/32) + 2 VSS
-    # mixtures, one CUDA graph launch per stage vs the same launches issued
-    # one after another on one stream; error against the same problems in
-    # the FP64 mode
+    # mixtures.  Merged: the problems that share an operator evaluated in
+    # one call per kernel (one group per N, one for the mixtures), the
+    # groups as concurrent branches of one CUDA graph per stage; against the
+    # per-problem calls issued one after another on one stream and against
+    # the per-problem graph; error against the same problems in FP64
     from dgfs1d_gpu_b200.batch import StageGraph
     from dgfs1d_gpu_b200.workloads_c3 import build_c3
-    probs = build_c3(precision='fp32')
-    sg = StageGraph([p['fn'] for p in probs])
-    sg.capture()
-    b_evals = sum(p['nevals'] for p in probs)
+    groups = build_c3(precision='fp32', merged=True)
+    members = [m for g in groups for m in g['members']]
+    b_evals = sum(g['nevals'] for g in groups)
     b_steps = max(3, args.steps // 4)
+    sg = StageGraph([g['fn'] for g in groups])
+    sg.capture()
     ms_graph = timed(sg.replay, b_steps, 3)
+    del sg
+    sg = None
+    probs = build_c3(precision='fp32')
 
     def serial():
         for p in probs:
             p['fn']()
     ms_serial = timed(serial, b_steps, 3)
-    serial()
+    sg1 = StageGraph([p['fn'] for p in probs])
+    sg1.capture()
+    ms_graph1 = timed(sg1.replay, b_steps, 3)
+    del sg1
+    for g in groups:
+        g['fn']()
     probs64 = build_c3(precision='fp64')
     for p in probs64:
         p['fn']()
     torch.cuda.synchronize()
     b_err = {}
-    for a, b in zip(probs, probs64):
+    for a, b in zip(members, probs64):
         qa = a['Q'] if isinstance(a['Q'], list) else [a['Q']]
         qb = b['Q'] if isinstance(b['Q'], list) else [b['Q']]
         b_err[a['name']] = max(_rel_l2(torch, x, y) for x, y in zip(qa, qb))
     batch = {'value': b_evals * world / (ms_graph * 1e-3), 'unit': UNIT,
              'ms_per_stage': ms_graph, 'graph_launches_per_stage': 1,
+             'groups': [g['name'] for g in groups],
              'serial_stream_ms_per_stage': ms_serial,
-             'problems': [p['name'] for p in probs],
+             'per_problem_graph_ms_per_stage': ms_graph1,
+             'speedup_vs_serial_stream': ms_serial / ms_graph,
+             'problems': [m['name'] for m in members],
              'evals_per_stage': b_evals,
              'err_vs_fp64_rel_l2': b_err,
-             'note': 'VSS evals count each (p,q) pair at each point'}
-    del sg, probs, probs64
+             'note': 'VSS evals count each (p,q) pair at each point; '
+                     'serial = one call per problem, one after another'}
+    del groups, probs, probs64
 
     barrier()
     clk.__exit__(None, None, None)

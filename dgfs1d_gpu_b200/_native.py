@@ -88,6 +88,10 @@ _SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
       ctypes.c_void_p]),
+    ('dgfs_vhs_eval_multi', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     ('dgfs_vhs_eval2', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
       ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
@@ -134,6 +138,10 @@ _SIGNATURES = [
       ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
       ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
       ctypes.c_int32, ctypes.c_void_p]),
+    ('dgfs_vss_eval_species_multi', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     ('dgfs_vss_eval_species', ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),
       ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,

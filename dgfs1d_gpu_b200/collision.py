@@ -96,6 +96,26 @@ class VHSOperator:
             ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
             nevals, _stream_ptr(stream)))
 
+    def eval_multi(self, f_list, q_list, dtype_f, dtype_q, src, dst,
+                   stream=None):
+        """Q(f, f) for points of several problems sharing this operator:
+        f_list, q_list are CUDA int64 tensors of array addresses (one per
+        evaluation), src/dst CUDA int32 slot tensors of the same length."""
+        n = len(src)
+        for t_, name in ((f_list, 'f_list'), (q_list, 'q_list')):
+            if t_.dtype != torch.int64 or not t_.is_cuda or len(t_) != n:
+                raise TypeError(f'{name} must be a CUDA int64 tensor of '
+                                'length nevals')
+        for t_, name in ((src, 'src'), (dst, 'dst')):
+            if t_.dtype != torch.int32 or not t_.is_cuda or len(t_) != n:
+                raise TypeError(f'{name} must be a CUDA int32 tensor of '
+                                'length nevals')
+        nat.check(nat.lib().dgfs_vhs_eval_multi(
+            self._h, ctypes.c_void_p(f_list.data_ptr()), _DT[dtype_f],
+            ctypes.c_void_p(q_list.data_ptr()), _DT[dtype_q],
+            ctypes.c_void_p(src.data_ptr()), 0,
+            ctypes.c_void_p(dst.data_ptr()), 0, n, _stream_ptr(stream)))
+
     def eval2(self, f, g, Q, src=None, dst=None, src_base=0, dst_base=0,
               nevals=None, stream=None):
         """Bilinear Q[dst(i)] += Q(f[src(i)], g[src(i)]) (``vhs``): gain of
@@ -245,6 +265,24 @@ class VSSOperator:
             ctypes.c_void_p(src.data_ptr() if src is not None else 0), int(src_base),
             ctypes.c_void_p(dst.data_ptr() if dst is not None else 0), int(dst_base),
             int(nevals), _stream_ptr(stream)))
+
+    def eval_species_multi(self, p, f_lists, q_list, dtype_f, dtype_q, src,
+                           dst, stream=None):
+        """eval_species for points of several mixtures sharing this
+        operator (FP32 mode): f_lists a CUDA int64 tensor [nspcs * nevals]
+        of input array addresses, q_list [nevals] of species-p outputs."""
+        n = len(src)
+        if f_lists.dtype != torch.int64 or not f_lists.is_cuda or \
+                len(f_lists) != self.nspcs * n:
+            raise TypeError('f_lists must be a CUDA int64 tensor of length '
+                            'nspcs * nevals')
+        if q_list.dtype != torch.int64 or not q_list.is_cuda or len(q_list) != n:
+            raise TypeError('q_list must be a CUDA int64 tensor of length nevals')
+        nat.check(nat.lib().dgfs_vss_eval_species_multi(
+            self._h, int(p), ctypes.c_void_p(f_lists.data_ptr()), _DT[dtype_f],
+            ctypes.c_void_p(q_list.data_ptr()), _DT[dtype_q],
+            ctypes.c_void_p(src.data_ptr()), 0, ctypes.c_void_p(dst.data_ptr()),
+            0, n, _stream_ptr(stream)))
 
     def close(self):
         if getattr(self, '_h', None):

@@ -481,7 +481,9 @@ template <int N>
 static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
                    int q_double, const int32_t* src_slots, int src_base,
                    const int32_t* dst_slots, int dst_base, int nevals,
-                   cudaStream_t st, const VhsBilin* bl = nullptr) {
+                   cudaStream_t st, const VhsBilin* bl = nullptr,
+                   const void* const* f_list = nullptr,
+                   void* const* q_list = nullptr) {
   constexpr int C64 = VhsClusters<N>::c64 > 0 ? VhsClusters<N>::c64 : 1;
   constexpr bool HAS64 = VhsClusters<N>::c64 > 0;
   constexpr int C32 = VhsClusters<N>::c32;
@@ -501,7 +503,8 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
   // prologue
   {
     VhsPrologueArgs a{};
-    a.f = f; a.f_double = f_double; a.src_slots = src_slots; a.src_base = src_base;
+    a.f = f; a.f_list = f_list; a.f_double = f_double;
+    a.src_slots = src_slots; a.src_base = src_base;
     a.c0 = h->c0; a.b2 = h->b2; a.cw = h->cw; a.split = fp32 ? 1 : 0;
     a.Fg = h->Fg; a.ReLf = h->ReLf; a.mhat = h->mhat; a.moments = h->moments;
     a.Fny = h->Fny;
@@ -595,9 +598,10 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
   {
     VhsEpilogueArgs a{};
     a.H = h->H; a.h_double = fp32 ? 0 : 1; a.GM = fp32 ? h->GM : nullptr;
-    a.ReLf = h->ReLf; a.f = f; a.f_double = f_double;
+    a.ReLf = h->ReLf; a.f = f; a.f_list = f_list; a.f_double = f_double;
     a.src_slots = src_slots; a.src_base = src_base;
-    a.Q = Q; a.q_double = q_double; a.dst_slots = dst_slots; a.dst_base = dst_base;
+    a.Q = Q; a.q_list = q_list; a.q_double = q_double;
+    a.dst_slots = dst_slots; a.dst_base = dst_base;
     a.prefac = h->prefac;
     a.Nrho = fp32 ? (h->Nrho + 1) / 2 : h->Nrho;  // FP32: packed radial pairs
     a.project = h->project; a.c0 = h->c0; a.cw = h->cw;
@@ -617,7 +621,8 @@ static int vhs_eval_impl(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
                          void* Q, int32_t q_dtype, const int32_t* src_slots,
                          int32_t src_base, const int32_t* dst_slots,
                          int32_t dst_base, int32_t nevals, void* stream,
-                         const VhsBilin* bl);
+                         const VhsBilin* bl, const void* const* f_list = nullptr,
+                         void* const* q_list = nullptr);
 
 extern "C" int dgfs_vhs_eval(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
                              void* Q, int32_t q_dtype,
@@ -673,15 +678,34 @@ extern "C" int dgfs_vhs_fs2(dgfs_vhs_handle h, const void* f, const void* g,
                         nullptr, modeout * Ne + elem, 1, stream);
 }
 
+// Q(f, f) for a list of (array, slot) pairs: f_list and q_list are device
+// arrays of nevals pointers, evaluation i reading slot src(i) of f_list[i]
+// and adding into slot dst(i) of q_list[i] -- points of several problems
+// that share one operator (same grid, rules and parameters) in one launch
+// sequence.
+extern "C" int dgfs_vhs_eval_multi(dgfs_vhs_handle h, const void* const* f_list,
+                                   int32_t f_dtype, void* const* q_list,
+                                   int32_t q_dtype, const int32_t* src_slots,
+                                   int32_t src_base, const int32_t* dst_slots,
+                                   int32_t dst_base, int32_t nevals,
+                                   void* stream) {
+  NvtxRange nvtx_range("dgfs_vhs_eval_multi");
+  if (!f_list || !q_list) return fail(DGFS_ERR_INVALID, "null array lists");
+  return vhs_eval_impl(h, nullptr, f_dtype, nullptr, q_dtype, src_slots,
+                       src_base, dst_slots, dst_base, nevals, stream, nullptr,
+                       f_list, q_list);
+}
+
 static int vhs_eval_impl(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
                          void* Q, int32_t q_dtype, const int32_t* src_slots,
                          int32_t src_base, const int32_t* dst_slots,
                          int32_t dst_base, int32_t nevals, void* stream,
-                         const VhsBilin* bl) {
+                         const VhsBilin* bl, const void* const* f_list,
+                         void* const* q_list) {
   if (!h) return fail(DGFS_ERR_INVALID, "null handle");
   if (nevals < 0) return fail(DGFS_ERR_INVALID, "negative nevals");
   if (nevals == 0) return DGFS_OK;
-  if (!f || !Q) return fail(DGFS_ERR_INVALID, "null f or Q");
+  if ((!f && !f_list) || (!Q && !q_list)) return fail(DGFS_ERR_INVALID, "null f or Q");
   if ((f_dtype != DGFS_F32 && f_dtype != DGFS_F64) ||
       (q_dtype != DGFS_F32 && q_dtype != DGFS_F64))
     return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
@@ -692,13 +716,15 @@ static int vhs_eval_impl(dgfs_vhs_handle h, const void* f, int32_t f_dtype,
     const int cnt = std::min(h->max_evals, nevals - off);
     const int32_t* ss = src_slots ? src_slots + off : nullptr;
     const int32_t* ds = dst_slots ? dst_slots + off : nullptr;
+    const void* const* fl = f_list ? f_list + off : nullptr;
+    void* const* ql = q_list ? q_list + off : nullptr;
     int rc;
     switch (h->N) {
-      case 8: rc = vhs_run<8>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
-      case 16: rc = vhs_run<16>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
-      case 24: rc = vhs_run<24>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
-      case 32: rc = vhs_run<32>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
-      case 48: rc = vhs_run<48>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl); break;
+      case 8: rc = vhs_run<8>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl, fl, ql); break;
+      case 16: rc = vhs_run<16>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl, fl, ql); break;
+      case 24: rc = vhs_run<24>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl, fl, ql); break;
+      case 32: rc = vhs_run<32>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl, fl, ql); break;
+      case 48: rc = vhs_run<48>(h, f, f_dtype, Q, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, bl, fl, ql); break;
       default: return fail(DGFS_ERR_UNSUPPORTED, "N not compiled in");
     }
     if (rc) return rc;
@@ -1568,7 +1594,9 @@ template <int N>
 static int vss_run_species(dgfs_vss_s* h, int p, const void* const* f,
                            int f_double, void* Qp, int q_double,
                            const int32_t* ss, int sb, const int32_t* ds,
-                           int db, int nevals, cudaStream_t st) {
+                           int db, int nevals, cudaStream_t st,
+                           const void* const* fl = nullptr, size_t fl_stride = 0,
+                           void* const* ql = nullptr) {
   constexpr int CPRO = VhsClusters<N>::cpro;
   constexpr int CEPI = VhsClusters<N>::cepi;
   constexpr int C3 = VssClusters32<N>::c;
@@ -1586,7 +1614,8 @@ static int vss_run_species(dgfs_vss_s* h, int p, const void* const* f,
   for (int q = 0; q < ns; ++q) {
     const VssPair& P = h->pair[p * ns + q];
     VhsPrologueArgs a{};
-    a.f = f[q]; a.f_double = f_double; a.src_slots = ss; a.src_base = sb;
+    a.f = fl ? nullptr : f[q]; a.f_list = fl ? fl + q * fl_stride : nullptr;
+    a.f_double = f_double; a.src_slots = ss; a.src_base = sb;
     a.c0 = h->c0; a.b2 = h->b2dummy; a.b2c = P.c; a.cw = h->cw; a.split = 1;
     a.Fg = h->Fg[q]; a.ReLf = ReLf(q); a.mhat = h->mhat[q]; a.moments = h->mom[q];
     if ((rc = launch_cluster(vhs_prologue_kernel<N, CPRO>, dim3(CPRO, nevals),
@@ -1627,8 +1656,10 @@ static int vss_run_species(dgfs_vss_s* h, int p, const void* const* f,
   DGFS_CUDA(cudaEventRecord(h->join, h->aux));
   DGFS_CUDA(cudaStreamWaitEvent(st, h->join, 0));
   VhsEpilogueArgs ea{};
-  ea.f = f[p]; ea.f_double = f_double; ea.src_slots = ss; ea.src_base = sb;
-  ea.Q = Qp; ea.q_double = q_double; ea.dst_slots = ds; ea.dst_base = db;
+  ea.f = fl ? nullptr : f[p]; ea.f_list = fl ? fl + p * fl_stride : nullptr;
+  ea.f_double = f_double; ea.src_slots = ss; ea.src_base = sb;
+  ea.Q = Qp; ea.q_list = ql; ea.q_double = q_double;
+  ea.dst_slots = ds; ea.dst_base = db;
   ea.Nrho = h->Nrho; ea.project = 0; ea.c0 = h->c0; ea.cw = h->cw;
   ea.nt = ns;
   for (int q = 0; q < ns; ++q) {
@@ -1677,6 +1708,50 @@ extern "C" int dgfs_vss_eval_species(dgfs_vss_handle h, int32_t p,
       case 16: rc = vss_run_species<16>(h, p, f, f_dtype, Qp, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
       case 24: rc = vss_run_species<24>(h, p, f, f_dtype, Qp, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
       default: rc = vss_run_species<32>(h, p, f, f_dtype, Qp, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st); break;
+    }
+    if (rc) return rc;
+  }
+  return DGFS_OK;
+}
+
+// Every pair of species p for a list of points of several mixtures that
+// share one operator (FP32 mode): f_lists is a device array [nspcs][nevals]
+// of input arrays (evaluation i of species q reads slot src(i) of
+// f_lists[q * nevals + i]), q_list a device array [nevals] of output arrays.
+extern "C" int dgfs_vss_eval_species_multi(dgfs_vss_handle h, int32_t p,
+                                           const void* const* f_lists,
+                                           int32_t f_dtype,
+                                           void* const* q_list, int32_t q_dtype,
+                                           const int32_t* src_slots,
+                                           int32_t src_base,
+                                           const int32_t* dst_slots,
+                                           int32_t dst_base, int32_t nevals,
+                                           void* stream) {
+  NvtxRange nvtx_range("dgfs_vss_eval_species_multi");
+  if (!h) return fail(DGFS_ERR_INVALID, "null handle");
+  if (h->precision != DGFS_PREC_FP32)
+    return fail(DGFS_ERR_UNSUPPORTED, "array lists need the FP32 mode");
+  if (p < 0 || p >= h->nspcs) return fail(DGFS_ERR_INVALID, "species out of range");
+  if (!f_lists || !q_list) return fail(DGFS_ERR_INVALID, "null array lists");
+  if (nevals < 0 || src_base < 0 || dst_base < 0)
+    return fail(DGFS_ERR_INVALID, "negative nevals or slot base");
+  if ((f_dtype != DGFS_F32 && f_dtype != DGFS_F64) ||
+      (q_dtype != DGFS_F32 && q_dtype != DGFS_F64))
+    return fail(DGFS_ERR_INVALID, "dtype must be DGFS_F32 or DGFS_F64");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const void* none[4] = {};
+  for (int off = 0; off < nevals; off += h->max_evals) {
+    const int cnt = std::min(h->max_evals, nevals - off);
+    const int32_t* ss = src_slots ? src_slots + off : nullptr;
+    const int32_t* ds = dst_slots ? dst_slots + off : nullptr;
+    const void* const* fl = f_lists + off;
+    void* const* ql = q_list + off;
+    int rc;
+    switch (h->N) {
+      case 8: rc = vss_run_species<8>(h, p, none, f_dtype, nullptr, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, fl, nevals, ql); break;
+      case 16: rc = vss_run_species<16>(h, p, none, f_dtype, nullptr, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, fl, nevals, ql); break;
+      case 24: rc = vss_run_species<24>(h, p, none, f_dtype, nullptr, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, fl, nevals, ql); break;
+      default: rc = vss_run_species<32>(h, p, none, f_dtype, nullptr, q_dtype, ss, src_base + off, ds, dst_base + off, cnt, st, fl, nevals, ql); break;
     }
     if (rc) return rc;
   }

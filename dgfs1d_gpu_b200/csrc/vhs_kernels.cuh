@@ -37,6 +37,8 @@ namespace dgfs {
 
 struct VhsPrologueArgs {
   const void* f;              // input distribution (float or double)
+  const void* const* f_list;  // or, if set, one input array per evaluation
+                              // (device array [nevals]; slots index into it)
   int f_double;               // 1: f is double
   const void* g;              // optional second input (same dtype as f): the
                               // transformed input is then alpha f + beta g
@@ -103,10 +105,12 @@ struct VhsEpilogueArgs {
   const double2* GM;          // [nevals][n] or null
   const double* ReLf;         // [nevals][n]
   const void* f;              // input distribution
+  const void* const* f_list;  // or one input array per evaluation
   int f_double;
   const int32_t* src_slots;
   int src_base;
   void* Q;                    // output distribution (+=)
+  void* const* q_list;        // or one output array per evaluation
   int q_double;
   const int32_t* dst_slots;
   int dst_base;
@@ -191,14 +195,15 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
   const int e = blockIdx.y;
   const int yl = t / N, z = t % N, y = rank * G::P + yl;
   const size_t fbase = (size_t)slot_of(a.src_slots, a.src_base, e) * G::n;
+  const void* fin = a.f_list ? a.f_list[e] : a.f;
 
   T v[N];
 #pragma unroll
   for (int x = 0; x < N; ++x) {
     const size_t idx = fbase + ((size_t)x * N + y) * N + z;
-    v[x].x = a.g ? a.alpha * load_real(a.f, a.f_double, idx) +
+    v[x].x = a.g ? a.alpha * load_real(fin, a.f_double, idx) +
                        a.beta * load_real(a.g, a.f_double, idx)
-                 : load_real(a.f, a.f_double, idx);
+                 : load_real(fin, a.f_double, idx);
     v[x].y = 0.0;
   }
 
@@ -1591,10 +1596,12 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
   const int yl = t / N, z = t % N, y = rank * G::P + yl;
   const size_t fb = (size_t)slot_of(a.src_slots, a.src_base, e) * G::n;
   const size_t qb = (size_t)slot_of(a.dst_slots, a.dst_base, e) * G::n;
+  const void* fin = a.f_list ? a.f_list[e] : a.f;
+  void* qout = a.q_list ? a.q_list[e] : a.Q;
 #pragma unroll
   for (int x = 0; x < N; ++x) {
     const size_t idx = ((size_t)x * N + y) * N + z;
-    const double fv = load_real(a.f, a.f_double, fb + idx);
+    const double fv = load_real(fin, a.f_double, fb + idx);
     if (a.nt > 0) {
       double lf = 0;
       for (int it = 0; it < a.nt; ++it)
@@ -1654,8 +1661,8 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
       qv -= lam[0] + lam[1] * cx + lam[2] * cy + lam[3] * cz +
             lam[4] * (cx * cx + cy * cy + cz * cz);
     }
-    if (a.q_double) static_cast<double*>(a.Q)[qb + idx] += qv;
-    else static_cast<float*>(a.Q)[qb + idx] += (float)qv;
+    if (a.q_double) static_cast<double*>(qout)[qb + idx] += qv;
+    else static_cast<float*>(qout)[qb + idx] += (float)qv;
   }
 }
 

@@ -21,8 +21,20 @@ VHS_PROBLEMS = [(16, 12, 6), (24, 24, 12), (32, 40, 12),
                 (16, 12, 6), (24, 24, 12), (32, 40, 12)]
 
 
-def build_c3(precision='fp32', device='cuda', seed=20261203, project=True):
-    """Return a list of (name, enqueue_fn, nevals, op) and the tensors."""
+def build_c3(precision='fp32', device='cuda', seed=20261203, project=True,
+             merged=False):
+    """The eight problems as dicts (name, op, f, Q, nevals, params, fn).
+
+    merged=True instead returns one dict per group of problems that share
+    an operator -- the VHS problems of equal N (equal grids and rules here)
+    and the two mixtures -- with one operator per group, ``fn`` evaluating
+    every member's points in one call per kernel, and the members' dicts
+    (without ops) under ``members``."""
+    if merged:
+        if precision != 'fp32':
+            raise ValueError('merged groups need the FP32 mode (the VSS array '
+                             'lists are FP32 only)')
+        return _build_merged(precision, device, seed, project)
     problems = []
     for i, (N, pts, M) in enumerate(VHS_PROBLEMS):
         full = M == 12
@@ -82,3 +94,46 @@ def build_c3(precision='fp32', device='cuda', seed=20261203, project=True):
                                          masses=masses, gamma=gam, eta=eta,
                                          prefac=pre)))
     return problems
+
+
+def _build_merged(precision, device, seed, project):
+    from .batch import merged_vhs, merged_vss
+    single = build_c3(precision, device, seed, project)
+    groups = []
+    vhs = [p for p in single if p['name'].startswith('vhs')]
+    for N in sorted({p['params']['N'] for p in vhs}):
+        members = [p for p in vhs if p['params']['N'] == N]
+        prm = members[0]['params']
+        tot = sum(p['nevals'] for p in members)
+        op = VHSOperator(**prm, precision=precision, max_evals=tot)
+        if project:
+            op.set_projection(True)
+        call = merged_vhs(op, [(p['f'], p['Q']) for p in members])
+
+        def fn(call=call, members=members):
+            for p in members:
+                p['Q'].zero_()
+            call()
+        groups.append(dict(name=f'vhs-N{N}-x{len(members)}', op=op, fn=fn,
+                           nevals=tot, members=members))
+    vss = [p for p in single if p['name'].startswith('vss')]
+    prm = vss[0]['params']
+    tot = sum(p['nevals'] // 4 for p in vss)
+    op = VSSOperator(prm['N'], prm['L'], prm['qz'], prm['qw'], prm['sz'],
+                     prm['sw'], prm['szpre'], prm['masses'], prm['gamma'],
+                     prm['eta'], prm['prefac'], max_evals=tot,
+                     precision=precision)
+    call = merged_vss(op, [(p['f'], p['Q']) for p in vss])
+
+    def fn(call=call, members=vss):
+        for p in members:
+            for x in p['Q']:
+                x.zero_()
+        call()
+    groups.append(dict(name=f'vss-N{prm["N"]}-x{len(vss)}', op=op, fn=fn,
+                       nevals=4 * tot, members=vss))
+    for p in single:          # the members' own operators are not needed
+        p['op'].close()
+        p.pop('op')
+        p.pop('fn')
+    return groups

@@ -83,6 +83,17 @@ int dgfs_vhs_eval(dgfs_vhs_handle h, const void* f, int32_t f_dtype, void* Q,
                   const int32_t* dst_slots, int32_t dst_base, int32_t nevals,
                   void* stream);
 
+/* Q(f, f) for points of several problems that share this handle's operator
+ * (same grid, rules and parameters) in one launch sequence: f_list and
+ * q_list are DEVICE arrays of nevals pointers; evaluation i reads slot
+ * src(i) of f_list[i] and adds into slot dst(i) of q_list[i].  No reference
+ * counterpart (the reference evaluates one point per call). */
+int dgfs_vhs_eval_multi(dgfs_vhs_handle h, const void* const* f_list,
+                        int32_t f_dtype, void* const* q_list, int32_t q_dtype,
+                        const int32_t* src_slots, int32_t src_base,
+                        const int32_t* dst_slots, int32_t dst_base,
+                        int32_t nevals, void* stream);
+
 /* Reference-shaped single evaluation: fs(d_f, d_g, d_Q, elem, modein,
  * modeout) of std/scattering.py:251 (d_g unused there as here):
  * src = modein*Ne + elem, dst = modeout*Ne + elem. */
@@ -205,6 +216,18 @@ int dgfs_vss_eval_species(dgfs_vss_handle h, int32_t p, const void* const* f,
                           const int32_t* src_slots, int32_t src_base,
                           const int32_t* dst_slots, int32_t dst_base,
                           int32_t nevals, void* stream);
+
+/* dgfs_vss_eval_species for points of several mixtures that share this
+ * handle's operator (FP32 mode only): f_lists is a DEVICE array
+ * [nspcs][nevals] of input arrays (evaluation i of species q reads slot
+ * src(i) of f_lists[q*nevals + i]), q_list a DEVICE array [nevals] of the
+ * species-p output arrays.  No reference counterpart. */
+int dgfs_vss_eval_species_multi(dgfs_vss_handle h, int32_t p,
+                                const void* const* f_lists, int32_t f_dtype,
+                                void* const* q_list, int32_t q_dtype,
+                                const int32_t* src_slots, int32_t src_base,
+                                const int32_t* dst_slots, int32_t dst_base,
+                                int32_t nevals, void* stream);
 
 /*
  * Nodal DG advection right-hand side of the single-species solver.

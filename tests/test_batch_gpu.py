@@ -11,17 +11,26 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope='module')
-def problems():
+@pytest.fixture(scope='module', params=[False, True], ids=['per-problem', 'merged'])
+def problems(request):
+    """Per problem (one operator and one call per problem), or merged (the
+    problems that share an operator evaluated in one call per kernel)."""
     from dgfs1d_gpu_b200 import build
     build.build()
     from dgfs1d_gpu_b200.workloads_c3 import build_c3
-    return build_c3(precision='fp32')
+    return build_c3(precision='fp32', merged=request.param)
+
+
+def _members(probs):
+    out = []
+    for p in probs:
+        out += p.get('members', [p])
+    return out
 
 
 def _snapshot(probs):
     out = []
-    for p in probs:
+    for p in _members(probs):
         qs = p['Q'] if isinstance(p['Q'], list) else [p['Q']]
         out.append([q.clone() for q in qs])
     return out
@@ -38,7 +47,7 @@ def test_graph_replay_equals_eager(problems):
         sg.replay()
     torch.cuda.synchronize()
     graph = _snapshot(problems)
-    for p, a, b in zip(problems, eager, graph):
+    for p, a, b in zip(_members(problems), eager, graph):
         for x, y in zip(a, b):
             assert torch.equal(x, y), p['name']
     assert all(torch.isfinite(x).all() for a in graph for x in a)
@@ -63,7 +72,7 @@ def test_every_slot_matches_oracle(problems):
         p['fn']()
     torch.cuda.synchronize()
     vss_tabs = {}
-    for p in problems:
+    for p in _members(problems):
         prm = p['params']
         if p['name'].startswith('vhs'):
             tab = VHSTables(prm['N'], prm['L'], prm['qz'], prm['qw'], prm['sz'],
