@@ -101,6 +101,8 @@ _SIGNATURES = [
       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
       ctypes.c_int32, ctypes.c_void_p]),
     ('dgfs_vhs_last_moments', ctypes.c_void_p, [ctypes.c_void_p]),
+    ('dgfs_vhs_device_error', ctypes.c_int,
+     [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ('dgfs_vhs_set_projection', ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ('dgfs_vhs_variants', ctypes.c_int,
      [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),

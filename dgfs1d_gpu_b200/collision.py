@@ -169,6 +169,13 @@ class VHSOperator:
         self.set_variant(min(times, key=times.get))
         return times
 
+    def device_error(self):
+        """Waits for the device; nonzero if a bounded wait of the handle's
+        kernels gave up since the last call (the flag is then cleared)."""
+        out = ctypes.c_int32(0)
+        nat.check(nat.lib().dgfs_vhs_device_error(self._h, ctypes.byref(out)))
+        return int(out.value)
+
     def set_projection(self, enable=True):
         """Toggle the FP64 conservation projection of every evaluation."""
         nat.check(nat.lib().dgfs_vhs_set_projection(self._h, int(bool(enable))))

@@ -146,5 +146,10 @@ __device__ __forceinline__ void st_cluster(uint32_t addr, double2 v) {
   asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};\n"
                :: "r"(addr), "d"(v.x), "d"(v.y) : "memory");
 }
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
 
 }  // namespace dgfs

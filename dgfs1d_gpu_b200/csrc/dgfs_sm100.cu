@@ -1,4 +1,6 @@
 // C ABI of the sm_100a DGFS collision operators (single translation unit).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -107,6 +109,32 @@ static int launch_cluster(K kernel, dim3 grid, dim3 block, int cluster,
   return DGFS_OK;
 }
 
+template <typename K, typename A, typename B>
+static int launch_cluster2(K kernel, dim3 grid, dim3 block, int cluster,
+                           size_t smem, cudaStream_t st, const A& args,
+                           const B& args2) {
+  DGFS_CUDA(cudaFuncSetAttribute(kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  if (cluster > 8)
+    DGFS_CUDA(cudaFuncSetAttribute(
+        kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  DGFS_CUDA(cudaLaunchKernelEx(&cfg, kernel, args, args2));
+  return DGFS_OK;
+}
+
 template <typename K, typename A>
 static int launch_plain(K kernel, dim3 grid, dim3 block, size_t smem,
                         cudaStream_t st, const A& args) {
@@ -150,6 +178,9 @@ struct dgfs_vhs_s {
   void* uv = nullptr;        // [E][Nrho][Mu][2][3][N] R
   double2* hh = nullptr;     // [E][Nrho][Mu][3][N]
   double2* GM = nullptr;     // [E][n]
+  int* err = nullptr;        // device error flag of the bounded waits
+  CUtensorMap fg_map;        // FP32: TMA map of Fg, box P x N x (N+2)
+  bool fg_map_ok = false;
   // optional per-kernel timing (events recorded between the launches)
   bool profile = false;
   cudaEvent_t ev[6] = {};
@@ -207,7 +238,7 @@ static size_t slab_bytes(int N, int C, size_t elem) {
 static void free_handle(dgfs_vhs_s* h) {
   void* ptrs[] = {h->c0, h->b2, h->b1w64, h->b1w32, h->ph, h->kappa, h->mult,
                   h->Fg, h->H, h->ReLf, h->mhat, h->moments, h->uv, h->hh,
-                  h->GM, h->nyq32, h->rho, h->Fny};
+                  h->GM, h->nyq32, h->rho, h->Fny, h->err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : h->ev)
@@ -361,6 +392,8 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_desc* d, dgfs_vhs_handle* out) {
   auto alloc = [&](void** p, size_t bytes) {
     if (ce_ == cudaSuccess) ce_ = cudaMalloc(p, bytes);
   };
+  alloc((void**)&h->err, sizeof(int));
+  if (ce_ == cudaSuccess) ce_ = cudaMemset(h->err, 0, sizeof(int));
   alloc(&h->Fg, E * n * ce);
   alloc(&h->H, E * Nrho * n * ce);
   alloc((void**)&h->ReLf, E * n * sizeof(double));
@@ -377,6 +410,30 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_desc* d, dgfs_vhs_handle* out) {
     free_handle(h);
     return fail(DGFS_ERR_CUDA,
                 std::string("scratch allocation: ") + cudaGetErrorString(ce_));
+  }
+  if (fp32) {
+    // TMA map of F_g for the TMA terms variant at the default cluster size
+    // (P = N / c32 planes per CTA): dims (lz, ly, lx, eval), 8-byte elements
+    // (one complex float), box (N+2, N, P, 1): the two elements past each
+    // row are out of bounds and arrive as zeros (the row padding)
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault,
+                                &q) == cudaSuccess && fn &&
+        q == cudaDriverEntryPointSuccess) {
+      const cuuint64_t dims[4] = {(cuuint64_t)N, (cuuint64_t)N, (cuuint64_t)N,
+                                  (cuuint64_t)E};
+      const cuuint64_t strides[3] = {(cuuint64_t)N * 8, (cuuint64_t)N * N * 8,
+                                     (cuuint64_t)n * 8};
+      const cuuint32_t box[4] = {(cuuint32_t)(N + 2), (cuuint32_t)N,
+                                 (cuuint32_t)(N / c32_of(N)), 1u};
+      const cuuint32_t estr[4] = {1, 1, 1, 1};
+      const CUresult r = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn)(
+          &h->fg_map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, h->Fg, dims, strides,
+          box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      h->fg_map_ok = r == CUDA_SUCCESS;
+    }
   }
   if (fp32) {
     int lo_prio = 0, hi_prio = 0;
@@ -408,20 +465,37 @@ extern "C" const double* dgfs_vhs_last_moments(dgfs_vhs_handle h) {
   return h ? h->moments : nullptr;
 }
 
+extern "C" int dgfs_vhs_device_error(dgfs_vhs_handle h, int32_t* out) {
+  if (!h || !out) return fail(DGFS_ERR_INVALID, "null argument");
+  int v = 0;
+  DGFS_CUDA(cudaMemcpy(&v, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (v) DGFS_CUDA(cudaMemset(h->err, 0, sizeof(int)));
+  *out = v;
+  return DGFS_OK;
+}
+
 // FP32 terms kernel at cluster size C (each C must divide N and fit three
 // slabs in shared memory).
-template <int N, int C, bool ASYNC_TAB = false>
+template <int N, int C, bool TMA = false>
 static int launch_terms32_c(const VhsTermsArgs& a, int nevals, int Nrho,
-                            cudaStream_t st) {
+                            cudaStream_t st, const CUtensorMap* map = nullptr) {
   using G = Geo<N, C>;
-  // three slabs, two table slots, the staged plane transforms of one term
-  const size_t smem = 3 * slab_bytes(N, C, sizeof(float2)) +
+  // three slabs (with TMA the transform slab has rows of N+2 elements and
+  // 128 bytes of alignment slack), two table slots, the staged plane
+  // transforms of one term (and the TMA mbarrier)
+  const size_t smem = (TMA ? (size_t)G::P * N * (N + 2) * sizeof(float2) + 128
+                           : slab_bytes(N, C, sizeof(float2))) +
+                      2 * slab_bytes(N, C, sizeof(float2)) +
                       2 * (9 * N + 4) * sizeof(float2) +
                       (size_t)((TermsRyStaged<C>::value ? N * N : 0) +
-                               2 * G::P * N) * sizeof(float2);
-  return launch_cluster(vhs_terms_fp32_kernel<N, C, ASYNC_TAB>,
-                        dim3(C, (Nrho + 1) / 2, nevals), dim3(G::NT), C, smem,
-                        st, a);
+                               2 * G::P * N) * sizeof(float2) +
+                      (TMA ? sizeof(uint64_t) : 0);
+  if (TMA && !map) return fail(DGFS_ERR_UNSUPPORTED, "no TMA map for this handle");
+  CUtensorMap none;
+  std::memset(&none, 0, sizeof(none));
+  return launch_cluster2(vhs_terms_fp32_kernel<N, C, TMA>,
+                         dim3(C, (Nrho + 1) / 2, nevals), dim3(G::NT), C, smem,
+                         st, a, map ? *map : none);
 }
 
 // Split-pencil terms kernel (two threads per pencil), same shared memory.
@@ -439,22 +513,24 @@ static int launch_terms32s_c(const VhsTermsArgs& a, int nevals, int Nrho,
 }
 
 // Variant codes: the cluster size C for the one-thread-per-pencil kernel,
-// 100 + C for the split-pencil kernel, 200 + C for the one-thread kernel with
-// asynchronous table loads.
+// 100 + C for the split-pencil kernel, 500 + C for the one-thread kernel
+// whose F_g slab and plane transforms arrive by TMA and bulk copies.
 template <int N> struct Terms32Variants;
-template <> struct Terms32Variants<8> { static constexpr int v[2] = {1, 2}; };
-template <> struct Terms32Variants<16> { static constexpr int v[2] = {1, 2}; };
-template <> struct Terms32Variants<24> { static constexpr int v[3] = {3, 4, 6}; };
-template <> struct Terms32Variants<32> { static constexpr int v[5] = {4, 8, 104, 108, 204}; };
-template <> struct Terms32Variants<48> { static constexpr int v[1] = {16}; };
+template <> struct Terms32Variants<8> { static constexpr int v[3] = {1, 2, 501}; };
+template <> struct Terms32Variants<16> { static constexpr int v[3] = {1, 2, 501}; };
+template <> struct Terms32Variants<24> { static constexpr int v[4] = {3, 4, 6, 503}; };
+template <> struct Terms32Variants<32> { static constexpr int v[5] = {4, 8, 104, 108, 504}; };
+template <> struct Terms32Variants<48> { static constexpr int v[2] = {16, 516}; };
 
 template <int N>
 static int launch_terms32(int c, const VhsTermsArgs& a, int nevals, int Nrho,
-                          cudaStream_t st) {
+                          cudaStream_t st, const CUtensorMap* map = nullptr) {
   if constexpr (N == 8 || N == 16) {
     if (c == 1) return launch_terms32_c<N, 1>(a, nevals, Nrho, st);
     if (c == 2) return launch_terms32_c<N, 2>(a, nevals, Nrho, st);
+    if (c == 501) return launch_terms32_c<N, 1, true>(a, nevals, Nrho, st, map);
   } else if constexpr (N == 24) {
+    if (c == 503) return launch_terms32_c<N, 3, true>(a, nevals, Nrho, st, map);
     if (c == 3) return launch_terms32_c<N, 3>(a, nevals, Nrho, st);
     if (c == 4) return launch_terms32_c<N, 4>(a, nevals, Nrho, st);
     if (c == 6) return launch_terms32_c<N, 6>(a, nevals, Nrho, st);
@@ -463,9 +539,10 @@ static int launch_terms32(int c, const VhsTermsArgs& a, int nevals, int Nrho,
     if (c == 8) return launch_terms32_c<N, 8>(a, nevals, Nrho, st);
     if (c == 104) return launch_terms32s_c<N, 4>(a, nevals, Nrho, st);
     if (c == 108) return launch_terms32s_c<N, 8>(a, nevals, Nrho, st);
-    if (c == 204) return launch_terms32_c<N, 4, true>(a, nevals, Nrho, st);
+    if (c == 504) return launch_terms32_c<N, 4, true>(a, nevals, Nrho, st, map);
   } else if constexpr (N == 48) {
     if (c == 16) return launch_terms32_c<N, 16>(a, nevals, Nrho, st);
+    if (c == 516) return launch_terms32_c<N, 16, true>(a, nevals, Nrho, st, map);
   }
   return fail(DGFS_ERR_UNSUPPORTED, "terms kernel cluster size not compiled in");
 }
@@ -532,7 +609,7 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     VhsTermsArgs a{};
     a.Fg = h->Fg; a.ph = h->ph; a.uv = h->uv; a.mult = h->mult;
     a.b1w = h->b1w32; a.H = h->H; a.Mu = h->Mu; a.Nrho = h->Nrho;
-    a.nyq = h->nyq32; a.rho = h->rho; a.Fny = h->Fny;
+    a.nyq = h->nyq32; a.rho = h->rho; a.Fny = h->Fny; a.err = h->err;
     const size_t psmem = (size_t)(9 * N * (N + 1) + 2 * (3 * N + 3)) * sizeof(float2);
     if ((rc = launch_plain(vhs_nyq_planes_kernel<N>,
                            dim3((h->Mu + 1) / 2, h->Nrho, nevals), dim3(6 * N),
@@ -544,8 +621,12 @@ static int vhs_run(dgfs_vhs_s* h, const void* f, int f_double, void* Q,
     DGFS_CUDA(cudaEventRecord(h->fork1, st));
     DGFS_CUDA(cudaStreamWaitEvent(h->hi, h->fork1, 0));
     if (h->profile) cudaEventRecord(h->ev[evi++], h->hi);
-    const int c = h->c32 ? h->c32 : C32;
-    if ((rc = launch_terms32<N>(c, a, nevals, h->Nrho, h->hi))) return rc;
+    // default: the TMA variant at the default cluster size, when its map
+    // could be made
+    const int c = h->c32 ? h->c32 : (h->fg_map_ok ? 500 + C32 : C32);
+    if ((rc = launch_terms32<N>(c, a, nevals, h->Nrho, h->hi,
+                                h->fg_map_ok ? &h->fg_map : nullptr)))
+      return rc;
     if (h->profile) cudaEventRecord(h->ev[evi++], h->hi);
     DGFS_CUDA(cudaEventRecord(h->join_hi, h->hi));
     // aux (after the tables, and not before the terms kernel is launched, so

@@ -30,6 +30,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cuda.h>
+
 #include "cluster_slab.cuh"
 #include "fft_reg.cuh"
 
@@ -75,6 +77,7 @@ struct VhsTermsArgs {
   void* rho;                  // FP32: [nevals][Nrho][Mu][3][N][N] plane transforms
   int Mu;
   int Nrho;
+  int* err;                   // device error flag (a bounded wait gave up)
 };
 
 struct VhsTablesArgs {
@@ -869,10 +872,11 @@ __device__ __forceinline__ float2 nyq_plane(float2 f) {
 // z-pass of the packed transform: multiply this thread's z-pencil
 // (lx, ly) by m(l) and inverse-transform it along z.
 // tb: [ph x,y,z (3N) | u (3N) | v (3N) | nu x,y,z (3)]
-template <int N, int C>
+template <int N, int C, int ROW = N + 1>
 __device__ __forceinline__ void fp32_zpass(float2* A, const float2* tb, int t,
                                            unsigned rank) {
   using G = Geo<N, C>;
+  constexpr int PLANE = N * ROW;
   const int pl = t / N, ly = t % N, lx = rank * G::P + pl;
   const float2 bxy = cmul(tb[lx], tb[N + ly]);
   const float2* nu = tb + 9 * N;
@@ -881,7 +885,7 @@ __device__ __forceinline__ void fp32_zpass(float2* A, const float2* tb, int t,
   if (ly == N / 2) fxy = cmul(fxy, nu[1]);
   const float2 gb = cmul(nyq_main(fxy), bxy);
   const float2 gbz = cmul(nyq_main(cmul(fxy, nu[2])), bxy);
-  const int base = pl * G::PLANE + ly * G::ROW;
+  const int base = pl * PLANE + ly * ROW;
   float2 v[N];
 #pragma unroll
   for (int k = 0; k < N; ++k) {
@@ -1018,20 +1022,39 @@ __device__ __forceinline__ void fp32_issue_rho_copy(float2* rbuf,
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
-template <int N, int C, bool ASYNC_TAB = false>
+// TMA selects how the F_g slab (once per transform) and the staged plane
+// transforms of a term reach shared memory:
+//   false: 8-byte cp.async per element into rows padded to N+1 elements;
+//   true:  one tiled TMA load of the CTA's P x N x (N+2) box of F_g (the two
+//          elements past the end of each row lie outside the tensor and are
+//          filled with zeros, which gives padded rows whose starts are
+//          16-byte aligned), and 1-D bulk copies of r_y and r_x, all
+//          completing on one mbarrier (bounded wait, error flag a.err); r_z
+//          (P-element pieces) stays on cp.async.  Rows of N+2 elements give
+//          the z-pass two-way bank conflicts, which N+1 avoids.
+template <int N, int C, bool TMA = false>
 __global__ void __launch_bounds__(Geo<N, C>::NT, 1)
-vhs_terms_fp32_kernel(VhsTermsArgs a) {
+vhs_terms_fp32_kernel(VhsTermsArgs a, const __grid_constant__ CUtensorMap tmap) {
   using G = Geo<N, C>;
   using T = float2;
   constexpr int TB = 9 * N + 4;  // ring slot: ph | u | v | nu (+1 pad)
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* A = reinterpret_cast<T*>(smem_raw);
-  T* R0 = A + G::SLAB;          // receive buffer b at R0 + b*SLAB
+  constexpr int RA = TMA ? N + 2 : G::ROW;   // row pitch of the A slab
+  constexpr int PA = N * RA;                 // its plane pitch
+  constexpr int SA = G::P * PA;              // its size
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // TMA writes need a 128-byte aligned destination: the launch adds 128
+  // bytes of slack and A starts at the next 128-byte boundary
+  T* A = reinterpret_cast<T*>(
+      TMA ? smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u) : smem_raw);
+  T* R0 = A + SA;               // receive buffer b at R0 + b*SLAB
   T* tab = R0 + 2 * G::SLAB;    // [2][TB]
   constexpr bool RYS = TermsRyStaged<C>::value;
   T* rbuf = tab + 2 * TB;       // (ry [N*N]) | rx [P*N] | rz [N*P]
   const T* rX = rbuf + (RYS ? N * N : 0);
   const T* rZ = rX + G::P * N;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(rbuf + (RYS ? N * N : 0) +
+                                               2 * G::P * N);
+  static_assert(((N + 2) * 8) % 16 == 0, "TMA rows must be 16-byte multiples");
   const int t = threadIdx.x;
   const unsigned rank = cluster_rank();
   const int pair = blockIdx.y, e = blockIdx.z;
@@ -1046,30 +1069,78 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
   const T* rhob = static_cast<const T*>(a.rho);
   // term k -> (p, q) = (p0 + k / Mu, k % Mu); tables index p*Mu + q
   auto term = [&](int k) { return (p0 + k / Mu) * Mu + k % Mu; };
-  // ASYNC_TAB: the tables go through cp.async (they join the next commit
-  // group) instead of a register round trip
   auto load_tables = [&](int k) {
     T* dst = tab + (k & 1) * TB;
     const int pq = term(k);
     const T* ph = phb + (size_t)pq * 3 * N;
     const T* uv = uvb + ((size_t)e * a.Nrho * Mu + pq) * 6 * N;
-    if (ASYNC_TAB) {
-      const uint32_t d0 = smem_u32(dst);
-      for (int i = t; i < 3 * N; i += G::NT)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
-                     :: "r"(d0 + 8u * i), "l"(ph + i) : "memory");
-      for (int i = t; i < 6 * N; i += G::NT)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
-                     :: "r"(d0 + 8u * (3 * N + i)), "l"(uv + i) : "memory");
-      if (t < 3)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
-                     :: "r"(d0 + 8u * (9 * N + t)), "l"(nyb + (size_t)pq * 3 + t)
-                     : "memory");
-    } else {
-      for (int i = t; i < 3 * N; i += G::NT) dst[i] = ph[i];
-      for (int i = t; i < 6 * N; i += G::NT) dst[3 * N + i] = uv[i];
-      if (t < 3) dst[9 * N + t] = nyb[(size_t)pq * 3 + t];
+    for (int i = t; i < 3 * N; i += G::NT) dst[i] = ph[i];
+    for (int i = t; i < 6 * N; i += G::NT) dst[3 * N + i] = uv[i];
+    if (t < 3) dst[9 * N + t] = nyb[(size_t)pq * 3 + t];
+  };
+  // TMA: thread 0 issues the copies of one stage (the slab of the next
+  // transform if `slab`, the r_y and r_x of term k if k >= 0) on mbar;
+  // every thread then waits for phase `ph` (bounded) before using them
+  constexpr uint32_t SLAB_BYTES = (uint32_t)(G::P * N * (N + 2) * sizeof(T));
+  constexpr uint32_t RY_BYTES = RYS ? (uint32_t)(N * N * sizeof(T)) : 0u;
+  constexpr uint32_t RX_BYTES = (uint32_t)(G::P * N * sizeof(T));
+  uint32_t tphase = 0;
+  bool tma_ok = true;
+  auto tma_issue = [&](bool slab, int k) {
+    if (t != 0) return;
+    const uint32_t mb = smem_u32(mbar);
+    const uint32_t bytes = (slab ? SLAB_BYTES : 0u) + (k >= 0 ? RY_BYTES + RX_BYTES : 0u);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+                 :: "r"(mb), "r"(bytes) : "memory");
+    if (slab)
+      asm volatile(
+          "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+          :: "r"(smem_u32(A)), "l"(&tmap), "r"(0), "r"(0), "r"((int)(rank * G::P)),
+             "r"(e), "r"(mb) : "memory");
+    if (k >= 0) {
+      const T* rho = rhob + ((size_t)e * a.Nrho * Mu + term(k)) * 3 * N * N;
+      if (RYS)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+            " [%0], [%1], %2, [%3];\n"
+            :: "r"(smem_u32(rbuf)), "l"(rho + N * N), "r"(RY_BYTES), "r"(mb)
+            : "memory");
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+          " [%0], [%1], %2, [%3];\n"
+          :: "r"(smem_u32(rbuf + (RYS ? N * N : 0))),
+             "l"(rho + (size_t)rank * G::P * N), "r"(RX_BYTES), "r"(mb)
+          : "memory");
     }
+  };
+  auto tma_wait = [&]() {
+    const uint32_t mb = smem_u32(mbar);
+    uint32_t done = 0;
+    uint64_t t0 = 0;
+    for (int it = 0; !done; ++it) {
+      asm volatile(
+          "{\n\t.reg .pred P1;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+          "selp.b32 %0, 1, 0, P1;\n\t}\n"
+          : "=r"(done) : "r"(mb), "r"(tphase) : "memory");
+      if (done) break;
+      if (it == 0) t0 = global_ns();
+      else if (global_ns() - t0 > 200000000ull) { tma_ok = false; break; }
+    }
+    tphase ^= 1u;
+  };
+  // r_z pieces (P elements per x) by 8-byte cp.async, one commit group
+  auto issue_rz = [&](int k) {
+    const uint32_t szz = smem_u32(rbuf + (RYS ? N * N : 0) + G::P * N);
+    const T* rz = rhob + ((size_t)e * a.Nrho * Mu + term(k)) * 3 * N * N +
+                  2 * N * N + rank * G::P;
+    for (int c = t; c < N * G::P; c += G::NT) {
+      const int x = c / G::P, j = c % G::P;
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
+                   :: "r"(szz + 8u * c), "l"(rz + (size_t)x * N + j) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
   auto rho_of = [&](int k) {
     return rhob + ((size_t)e * a.Nrho * Mu + term(k)) * 3 * N * N;
@@ -1085,24 +1156,42 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
 #pragma unroll
   for (int x = 0; x < N; ++x) S[x] = make_float2(0.f, 0.f);
 
-  fp32_issue_slab_copy<N, C>(A, Fg, t);
-  cp_async_wait_all();
-  __syncthreads();
-  fp32_zpass<N, C>(A, tab, t, rank);
+  if constexpr (TMA) {
+    if (t == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n"
+                   :: "r"(smem_u32(mbar)) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    tma_issue(true, -1);
+    tma_wait();
+    __syncthreads();
+  } else {
+    fp32_issue_slab_copy<N, C>(A, Fg, t);
+    cp_async_wait_all();
+    __syncthreads();
+  }
+  fp32_zpass<N, C, RA>(A, tab, t, rank);
   __syncthreads();
 #pragma unroll 1
   for (int k = 0; k < npass; ++k) {
     T v[N];
     {
-      const int base = (t / N) * G::PLANE + (t % N);
+      const int base = (t / N) * PA + (t % N);
 #pragma unroll
-      for (int y = 0; y < N; ++y) v[y] = A[base + y * G::ROW];
+      for (int y = 0; y < N; ++y) v[y] = A[base + y * RA];
     }
     __syncthreads();  // every thread has read A and used rbuf: refill both
-    fp32_issue_rho_copy<N, C>(rbuf, rho_of(k), t, rank);
-    if (k + 1 < npass) {
-      load_tables(k + 1);
-      fp32_issue_slab_copy<N, C>(A, Fg, t);
+    if constexpr (TMA) {
+      tma_issue(k + 1 < npass, k);
+      issue_rz(k);
+      if (k + 1 < npass) load_tables(k + 1);
+    } else {
+      fp32_issue_rho_copy<N, C>(rbuf, rho_of(k), t, rank);
+      if (k + 1 < npass) {
+        load_tables(k + 1);
+        fp32_issue_slab_copy<N, C>(A, Fg, t);
+      }
     }
     fft<float, N, +1>(v);
     {
@@ -1117,9 +1206,10 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
     }
     cluster_arrive();
     cp_async_wait_all();
+    if constexpr (TMA) tma_wait();
     __syncthreads();
     if (k + 1 < npass) {
-      fp32_zpass<N, C>(A, tab + ((k + 1) & 1) * TB, t, rank);
+      fp32_zpass<N, C, RA>(A, tab + ((k + 1) & 1) * TB, t, rank);
       __syncthreads();
     }
     cluster_wait();
@@ -1160,34 +1250,45 @@ vhs_terms_fp32_kernel(VhsTermsArgs a) {
   fft<float, N, -1>(S);
   {
     const uint32_t a0 = smem_u32(A);
-    const uint32_t off = (uint32_t)(yy * G::ROW + zz) * 8u;
+    const uint32_t off = (uint32_t)(yy * RA + zz) * 8u;
 #pragma unroll
     for (int c = 0; c < C; ++c) {
       const uint32_t ab = mapa_u32(a0, (uint32_t)c) + off;
 #pragma unroll
       for (int j = 0; j < G::P; ++j)
-        st_cluster(ab + (uint32_t)(j * G::PLANE) * 8u, S[c * G::P + j]);
+        st_cluster(ab + (uint32_t)(j * PA) * 8u, S[c * G::P + j]);
     }
   }
   cluster_arrive();
   cluster_wait();
   {
     T w[N];
-    slab_col_load_fft<float, N, C, -1>(A, t, w);
-    const int base = (t / N) * G::PLANE + (t % N);
+    const int base = (t / N) * PA + (t % N);
 #pragma unroll
-    for (int k = 0; k < N; ++k) A[base + k * G::ROW] = w[k];
+    for (int k = 0; k < N; ++k) w[k] = A[base + k * RA];
+    fft<float, N, -1>(w);
+#pragma unroll
+    for (int k = 0; k < N; ++k) A[base + k * RA] = w[k];
   }
   __syncthreads();
-  slab_row_pass<float, N, C, -1>(A, t);
+  {
+    T w[N];
+    const int base = (t / N) * PA + (t % N) * RA;
+#pragma unroll
+    for (int k = 0; k < N; ++k) w[k] = A[base + k];
+    fft<float, N, -1>(w);
+#pragma unroll
+    for (int k = 0; k < N; ++k) A[base + k] = w[k];
+  }
   __syncthreads();
   const size_t off = (size_t)rank * G::P * N * N;
   const float* b1a = static_cast<const float*>(a.b1w) + (size_t)p0 * G::n + off;
   const float* b1b = (p0 + 1 < a.Nrho) ? b1a + G::n : nullptr;
   const int npairs = (a.Nrho + 1) / 2;
   T* H = static_cast<T*>(a.H) + ((size_t)e * npairs + pair) * G::n + off;
+  if (TMA && !tma_ok && a.err && t == 0) atomicExch(a.err, 1);
   for (int j = t; j < G::P * N * N; j += G::NT) {
-    const T hv = A[slab_index<N, C>(j)];
+    const T hv = A[(j / (N * N)) * PA + ((j / N) % N) * RA + (j % N)];
     const float w0 = b1a[j], w1 = b1b ? b1b[j] : 0.f;
     H[j] = make_float2(hv.x * w0 + hv.y * w1, hv.y * w0 - hv.x * w1);
   }

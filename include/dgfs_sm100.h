@@ -139,6 +139,12 @@ int dgfs_vhs_set_projection(dgfs_vhs_handle h, int32_t enable);
 int dgfs_vhs_variants(int32_t N, int32_t* out, int32_t max);
 int dgfs_vhs_set_variant(dgfs_vhs_handle h, int32_t cluster);
 
+/* Device error flag of the handle's kernels (no reference counterpart):
+ * nonzero when a bounded wait (the TMA copies of the TMA terms variant)
+ * gave up, which leaves that evaluation's Q invalid.  Waits for the device,
+ * writes the flag to *out and clears it. */
+int dgfs_vhs_device_error(dgfs_vhs_handle h, int32_t* out);
+
 /* Per-eval local moments (rho, ux, uy, uz, T) of the last FP32 evaluation
  * batch, device pointer owned by the handle ([max_evals][5] doubles). */
 const double* dgfs_vhs_last_moments(dgfs_vhs_handle h);
