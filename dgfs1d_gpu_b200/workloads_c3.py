@@ -137,3 +137,18 @@ def _build_merged(precision, device, seed, project):
         p.pop('op')
         p.pop('fn')
     return groups
+
+
+if __name__ == '__main__':
+    # python -m dgfs1d_gpu_b200.workloads_c3 [vhs|vss|all] [stages]: run the
+    # stage of the chosen problems (FP32, one call per problem) a few times
+    import sys
+    which = sys.argv[1] if len(sys.argv) > 1 else 'all'
+    stages = int(sys.argv[2]) if len(sys.argv) > 2 else 3
+    probs = [p for p in build_c3(precision='fp32')
+             if which == 'all' or p['name'].startswith(which)]
+    for _ in range(stages):
+        for p in probs:
+            p['fn']()
+    torch.cuda.synchronize()
+    print('ran', stages, 'stages of', [p['name'] for p in probs])
