@@ -557,7 +557,11 @@ def main():
         p['fn']()
     torch.cuda.synchronize()
     b_err = {}
-    for a, b in zip(members, probs64):
+    # the merged groups list their members by group (grouped by N), not in
+    # the problems' own order: pair each with its FP64 twin by name
+    by_name = {p['name']: p for p in probs64}
+    for a in members:
+        b = by_name[a['name']]
         qa = a['Q'] if isinstance(a['Q'], list) else [a['Q']]
         qb = b['Q'] if isinstance(b['Q'], list) else [b['Q']]
         b_err[a['name']] = max(_rel_l2(torch, x, y) for x, y in zip(qa, qb))
