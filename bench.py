@@ -466,10 +466,20 @@ def main():
     # very batch
     tune = op32.autotune(fd, Q, reps=3)
 
-    # headline: FP32 fused operator, inputs resident in HBM
-    ms32 = timed(lambda: op32.eval(fd, Q), args.steps, args.warmup)
-    # plain FP64 path (same kernels, FP64 arithmetic, no split)
-    ms64 = timed(lambda: op64.eval(fd, Q), max(3, args.steps // 2), 3)
+    # headline: FP32 fused operator, inputs resident in HBM, one evaluation
+    # as one CUDA graph launch (its kernels and stream forks captured once);
+    # the plain FP64 path (same kernels, FP64 arithmetic, no split) the same
+    # way; the eager launch sequences beside them
+    from dgfs1d_gpu_b200.batch import StageGraph
+    g32 = StageGraph([lambda: op32.eval(fd, Q)])
+    g32.capture()
+    g64 = StageGraph([lambda: op64.eval(fd, Q)])
+    g64.capture()
+    ms32 = timed(g32.replay, args.steps, args.warmup)
+    ms64 = timed(g64.replay, max(3, args.steps // 2), 3)
+    ms32_eager = timed(lambda: op32.eval(fd, Q), args.steps, args.warmup)
+    ms64_eager = timed(lambda: op64.eval(fd, Q), max(3, args.steps // 2), 3)
+    del g32, g64
 
     # error of the FP32 mode vs the FP64 mode on this workload
     Q32 = torch.zeros_like(fd)
@@ -640,8 +650,12 @@ def main():
             'data': 'synthetic',
             'config': dict(WORKLOAD),
             'fp64_plain': {'value': evals / (ms64 * 1e-3), 'unit': UNIT,
-                           'ms_per_step': ms64},
+                           'ms_per_step': ms64,
+                           'ms_per_step_eager': ms64_eager},
             'speedup_fp32_vs_fp64': ms64 / ms32,
+            'ms_per_step_eager': ms32_eager,
+            'speedup_fp32_vs_fp64_eager': ms64_eager / ms32_eager,
+            'step': 'one 24-point evaluation as one CUDA graph launch',
             'err_fp32_vs_fp64_rel_l2': err,
             'e2e': {'value': evals / (ms_e2e * 1e-3), 'unit': UNIT,
                     'h2d_bytes_per_step': int(fh.numel() * 8),

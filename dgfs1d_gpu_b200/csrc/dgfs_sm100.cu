@@ -53,6 +53,18 @@ extern "C" const char* dgfs_version(void) { return "dgfs_sm100 0.1 (sm_100a)"; }
 // ---------------------------------------------------------------------------
 // twiddle tables (uploaded once per device)
 // ---------------------------------------------------------------------------
+// Host-to-device copies from pageable memory (cudaMemcpy, cudaMemcpyToSymbol)
+// and cudaMemset run on the legacy default stream, and the copies may still
+// be in flight when the call returns.  The handles' kernels run on the
+// caller's and the handles' own streams, which may be non-blocking and then
+// do not wait for the legacy stream: every create (and every upload of
+// constant tables) ends by waiting for that stream, so a kernel launched
+// right after it reads complete tables.
+static int settle_uploads() {
+  DGFS_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
+  return DGFS_OK;
+}
+
 static std::mutex g_tw_mu;
 static bool g_tw_done[64];
 
@@ -77,6 +89,7 @@ static int ensure_twiddles() {
   }
   DGFS_CUDA(cudaMemcpyToSymbol(c_tw64, t64.data(), sizeof(double2) * kTwTotal));
   DGFS_CUDA(cudaMemcpyToSymbol(c_tw32, t32.data(), sizeof(float2) * kTwTotal));
+  if (int rc = settle_uploads()) return rc;
   g_tw_done[dev] = true;
   return DGFS_OK;
 }
@@ -451,6 +464,7 @@ extern "C" int dgfs_vhs_create(const dgfs_vhs_desc* d, dgfs_vhs_handle* out) {
                                      cudaGetErrorString(e1));
     }
   }
+  if (int rc_s = settle_uploads()) { free_handle(h); return rc_s; }
   *out = h;
   return DGFS_OK;
 }
@@ -997,6 +1011,7 @@ static int noalloc_setup(unsigned char** out) {
       }
       DGFS_CUDA(cudaMemcpyToSymbol(c_tw64, t64, sizeof(t64)));
       DGFS_CUDA(cudaMemcpyToSymbol(c_tw32, t32, sizeof(t32)));
+      if (int rc = settle_uploads()) return rc;
       g_tw_done[dev] = true;
     }
     void* p = nullptr;
@@ -1210,6 +1225,7 @@ extern "C" int dgfs_dg_create(const dgfs_dg_desc* d, dgfs_dg_handle* out) {
   a.c0 = h->c0; a.invjac = h->invjac;
   a.f0[0] = h->f0[0]; a.f0[1] = h->f0[1];
   a.nden = h->nden;
+  if (int rc_s = settle_uploads()) { free_dg(h); return rc_s; }
   *out = h;
   return DGFS_OK;
 }
@@ -1572,6 +1588,7 @@ extern "C" int dgfs_vss_create(const dgfs_vss_desc* d, dgfs_vss_handle* out) {
     else rc = fail(DGFS_ERR_CUDA, std::string("FP32 scratch: ") + cudaGetErrorString(e1));
   }
   if (rc) { free_vss(h); return rc; }
+  if (int rc_s = settle_uploads()) { free_vss(h); return rc_s; }
   *out = h;
   return DGFS_OK;
 }
@@ -2326,6 +2343,7 @@ extern "C" int dgfs_fno_create(const dgfs_fno_desc* d, dgfs_fno_handle* out) {
     fno_free(h);
     return fail(DGFS_ERR_CUDA, std::string("FNO allocation: ") + cudaGetErrorString(e));
   }
+  if (int rc_s = settle_uploads()) { fno_free(h); return rc_s; }
   *out = h;
   return DGFS_OK;
 }

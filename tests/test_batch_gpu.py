@@ -49,7 +49,13 @@ def test_graph_replay_equals_eager(problems):
     graph = _snapshot(problems)
     for p, a, b in zip(_members(problems), eager, graph):
         for x, y in zip(a, b):
-            assert torch.equal(x, y), p['name']
+            if not torch.equal(x, y):
+                d = (x - y).abs().reshape(x.shape[0], -1).amax(1)
+                raise AssertionError(
+                    f"{p['name']}: graph replay differs from the eager launches "
+                    f"(max |diff| {float(d.max()):.3e} of max |Q| "
+                    f"{float(x.abs().max()):.3e}, slots "
+                    f"{torch.nonzero(d).flatten().tolist()})")
     assert all(torch.isfinite(x).all() for a in graph for x in a)
 
 
