@@ -489,19 +489,68 @@ def main():
     torch.cuda.synchronize()
     err = _rel_l2(torch, Q32, Q64)
 
-    # end to end through the C ABI with host buffers: H2D f, eval, D2H Q
+    # end to end through the C ABI with host buffers: every step copies its
+    # 24 distributions from pinned host memory to the device and its Q back.
+    # (1) one step at a time: H2D f, eval, D2H Q on one stream;
     fh = torch.tensor(f, dtype=torch.float64).pin_memory()
-    qh = torch.empty_like(fh).pin_memory()
-    fdev = torch.empty_like(fd)
-    qdev = torch.empty_like(fd)
+    qh = [torch.empty_like(fh).pin_memory() for _ in range(2)]
+    fdev = [torch.empty_like(fd) for _ in range(2)]
+    qdev = [torch.empty_like(fd) for _ in range(2)]
 
     def e2e_step():
-        fdev.copy_(fh, non_blocking=True)
-        qdev.zero_()
-        op32.eval(fdev, qdev)
-        qh.copy_(qdev, non_blocking=True)
+        fdev[0].copy_(fh, non_blocking=True)
+        qdev[0].zero_()
+        op32.eval(fdev[0], qdev[0])
+        qh[0].copy_(qdev[0], non_blocking=True)
 
-    ms_e2e = timed(e2e_step, args.steps, args.warmup)
+    ms_e2e_seq = timed(e2e_step, args.steps, args.warmup)
+
+    # (2) a stream of steps, as a solver feeding batches of points through
+    # the operator runs it: double-buffered device arrays on three streams,
+    # so that step i+1's H2D and step i-1's D2H overlap step i's evaluation;
+    # the 256 MB L2 flush precedes every evaluation on the compute stream
+    s_in, s_cmp, s_out = (torch.cuda.Stream() for _ in range(3))
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_cmp = [torch.cuda.Event() for _ in range(2)]
+    ev_out = [torch.cuda.Event() for _ in range(2)]
+
+    def e2e_stream(nsteps):
+        for i in range(nsteps):
+            b = i % 2
+            with torch.cuda.stream(s_in):
+                if i >= 2:
+                    s_in.wait_event(ev_cmp[b])    # step i-2 has read fdev[b]
+                fdev[b].copy_(fh, non_blocking=True)
+                ev_in[b].record(s_in)
+            with torch.cuda.stream(s_cmp):
+                s_cmp.wait_event(ev_in[b])
+                if i >= 2:
+                    s_cmp.wait_event(ev_out[b])   # qdev[b] of step i-2 is out
+                flush.fill_(1.0)
+                qdev[b].zero_()
+                op32.eval(fdev[b], qdev[b])
+                ev_cmp[b].record(s_cmp)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_cmp[b])
+                qh[b].copy_(qdev[b], non_blocking=True)
+                ev_out[b].record(s_out)
+
+    e2e_stream(args.warmup)
+    barrier()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(s_in)
+    e2e_stream(args.steps)
+    t_end.record(s_out)
+    t_end.synchronize()
+    barrier()
+    ms_e2e = max_over_ranks(torch, dist, t_start.elapsed_time(t_end), world,
+                            'cuda') / args.steps
+    # the streamed results equal the resident-input evaluation
+    Qchk = torch.zeros_like(fd)
+    op32.eval(fd, Qchk)
+    torch.cuda.synchronize()
+    e2e_match = bool(torch.equal(qh[(args.steps - 1) % 2].cuda(), Qchk))
 
     # per-kernel durations inside the timed region: CUDA events recorded by
     # the library on the launching stream between its kernels
@@ -659,7 +708,17 @@ def main():
             'err_fp32_vs_fp64_rel_l2': err,
             'e2e': {'value': evals / (ms_e2e * 1e-3), 'unit': UNIT,
                     'h2d_bytes_per_step': int(fh.numel() * 8),
-                    'd2h_bytes_per_step': int(qh.numel() * 8)},
+                    'd2h_bytes_per_step': int(qh[0].numel() * 8),
+                    'ms_per_step': ms_e2e,
+                    'mode': 'stream of steps through dgfs_vhs_eval: pinned '
+                            'host f -> device, evaluation, Q -> pinned host '
+                            'every step, double-buffered on three streams '
+                            '(H2D of step i+1 and D2H of step i-1 overlap '
+                            'step i), L2 flushed before every evaluation',
+                    'result_equals_resident_eval': e2e_match,
+                    'one_step_at_a_time': {
+                        'value': evals / (ms_e2e_seq * 1e-3), 'unit': UNIT,
+                        'ms_per_step': ms_e2e_seq}},
             'roofline': {
                 'bound': 'fp32-fma',
                 'kernel': f'vhs_terms_fp32_kernel<32,{op32.variant}> '
