@@ -227,7 +227,55 @@ def surrogate_line(torch, prm, fd, op32, op64, timed, args):
             'train_loss_last': hist[-1][1],
             'train_pairs': '4096 perturbed Maxwellians + 1536 Couette-like states',
             'tensor_cores': 'tcgen05.mma kind::f16 (dense layers, projection)',
-            'error_flag': net.device_error()}
+            'error_flag': net.device_error(), '_net': net}
+
+
+def couette_segment_line(torch, net, warm=300, nsteps=300, k=10, tol=1e-3):
+    """The learned part inside a run: the IMEX Couette solver (Kn 0.1,
+    diffuse walls u_y = -/+0.1, N=32, M=12, Nrho=16, Ne=8, K=3,
+    imex-lm-bdf2, dt=1e-3, the fused FP32 operator) advanced `warm` steps
+    from rest, then `nsteps` more steps three ways from that same state:
+    the plain operator (the method without the surrogate), the surrogate
+    plus the defect of its last check, and the surrogate alone between
+    checks (the plain operator checks every k-th call and serves every call
+    while a check is above tol).  Wall time of the segment and the shear
+    stress / heat flux profiles against the plain segment."""
+    import time as _t
+    from dgfs1d_gpu_b200.surrogate_couette import (make_solver, _profiles,
+                                                   _rel_profile_diff)
+    from dgfs1d_gpu_b200 import surrogate_train as st
+    out = {'workload': 'IMEX Couette Kn=0.1, N=32, M=12, Nrho=16, Ne=8, K=3, '
+                       'imex-lm-bdf2, dt=1e-3, FP32 operator; segment after '
+                       f'{warm} steps from rest', 'warm_steps': warm,
+           'steps': nsteps, 'k': k, 'tol': tol}
+    ref = None
+    for mode in ('plain', 'surrogate+defect', 'surrogate'):
+        sol = make_solver(32, 16, 12, 6.0, precision_mode='fp32')
+        for _ in range(warm):
+            sol.step()
+        hook = None
+        if mode != 'plain':
+            hook = st.SurrogateBoltzmann(sol, net, k=k, tol=tol,
+                                         correct=mode == 'surrogate+defect')
+            sol.boltzmann = hook
+        torch.cuda.synchronize()
+        t0 = _t.perf_counter()
+        for _ in range(nsteps):
+            sol.step()
+        torch.cuda.synchronize()
+        wall = _t.perf_counter() - t0
+        pxy, qx = _profiles(sol.bulk_moments())
+        rec = {'wall_s': wall, 'ms_per_step': 1e3 * wall / nsteps}
+        if ref is None:
+            ref = (wall, pxy, qx)
+        else:
+            rec.update(gain_vs_plain=ref[0] / wall,
+                       shear_stress_rel_diff=_rel_profile_diff(pxy, ref[1]),
+                       heat_flux_rel_diff=_rel_profile_diff(qx, ref[2]),
+                       **hook.stats())
+        out[mode] = rec
+        del sol, hook
+    return out
 
 
 def _rel_l2(torch, a, b):
@@ -581,6 +629,7 @@ def main():
     sur = None
     if not args.no_surrogate:
         sur = surrogate_line(torch, prm, fd, op32, op64, timed, args)
+        sur['couette_segment'] = couette_segment_line(torch, sur.pop('_net'))
 
     # uneven multi-problem batch: 6 VHS problems (N=16/24/32) + 2 VSS
     # mixtures.  Merged: the problems that share an operator evaluated in
