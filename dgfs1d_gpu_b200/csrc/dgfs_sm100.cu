@@ -534,7 +534,7 @@ template <> struct Terms32Variants<8> { static constexpr int v[3] = {1, 2, 501};
 template <> struct Terms32Variants<16> { static constexpr int v[3] = {1, 2, 501}; };
 template <> struct Terms32Variants<24> { static constexpr int v[4] = {3, 4, 6, 503}; };
 template <> struct Terms32Variants<32> { static constexpr int v[5] = {4, 8, 104, 108, 504}; };
-template <> struct Terms32Variants<48> { static constexpr int v[2] = {16, 516}; };
+template <> struct Terms32Variants<48> { static constexpr int v[3] = {16, 116, 516}; };
 
 template <int N>
 static int launch_terms32(int c, const VhsTermsArgs& a, int nevals, int Nrho,
@@ -556,6 +556,7 @@ static int launch_terms32(int c, const VhsTermsArgs& a, int nevals, int Nrho,
     if (c == 504) return launch_terms32_c<N, 4, true>(a, nevals, Nrho, st, map);
   } else if constexpr (N == 48) {
     if (c == 16) return launch_terms32_c<N, 16>(a, nevals, Nrho, st);
+    if (c == 116) return launch_terms32s_c<N, 16>(a, nevals, Nrho, st);
     if (c == 516) return launch_terms32_c<N, 16, true>(a, nevals, Nrho, st, map);
   }
   return fail(DGFS_ERR_UNSUPPORTED, "terms kernel cluster size not compiled in");
@@ -2157,11 +2158,11 @@ extern "C" int dgfs_vhs_variants(int32_t N, int32_t* out, int32_t max) {
   const int* v = nullptr;
   int n = 0;
   switch (N) {
-    case 8: v = Terms32Variants<8>::v; n = 2; break;
-    case 16: v = Terms32Variants<16>::v; n = 2; break;
-    case 24: v = Terms32Variants<24>::v; n = 3; break;
+    case 8: v = Terms32Variants<8>::v; n = 3; break;
+    case 16: v = Terms32Variants<16>::v; n = 3; break;
+    case 24: v = Terms32Variants<24>::v; n = 4; break;
     case 32: v = Terms32Variants<32>::v; n = 5; break;
-    case 48: v = Terms32Variants<48>::v; n = 1; break;
+    case 48: v = Terms32Variants<48>::v; n = 3; break;
     default: return fail(DGFS_ERR_UNSUPPORTED, "N not compiled in");
   }
   for (int i = 0; i < n && i < max; ++i) out[i] = v[i];
