@@ -166,12 +166,15 @@ template <int N> struct OneSlab { static constexpr bool value = N <= 32; };
 // spectra [3][N] (complex) and the moments [8].
 template <int N, int C>
 constexpr size_t prologue_smem() {
+  // ... + the N twiddles of the 1-D spectra (double2)
   return OneSlab<N>::value
              ? (size_t)Geo<N, C>::SLAB * sizeof(double2) +
                    (size_t)(6 * Geo<N, C>::NT + 8 + 3 * N) * sizeof(double) +
-                   (size_t)3 * N * sizeof(double2) + 8 * sizeof(double)
+                   (size_t)3 * N * sizeof(double2) + 8 * sizeof(double) +
+                   (size_t)N * sizeof(double2)
              : (size_t)2 * Geo<N, C>::SLAB * sizeof(double2) +
-                   (size_t)3 * N * sizeof(double2) + 8 * sizeof(double);
+                   (size_t)3 * N * sizeof(double2) + 8 * sizeof(double) +
+                   (size_t)N * sizeof(double2);
 }
 template <int N, int C>
 constexpr size_t epilogue_smem() {
@@ -192,6 +195,7 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
   T* mh = OS ? reinterpret_cast<T*>(red + 6 * G::NT + 8 + 3 * N)
              : A + 2 * G::SLAB;                              // [3][N]
   double* mom = reinterpret_cast<double*>(mh + 3 * N);      // [8]
+  T* tws = reinterpret_cast<T*>(mom + 8);                   // [N] twiddles
 
   const int t = threadIdx.x;
   const unsigned rank = cluster_rank();
@@ -226,11 +230,22 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
     }
 #pragma unroll
     for (int k = 0; k < 5; ++k) red[k * G::NT + t] = s[k];
+    // the spectra's twiddles into shared memory (read below with a
+    // different index on every lane, which constant memory serialises)
+    for (int i = t; i < N; i += G::NT) tws[i] = c_tw64[tw_offset(N) + i];
     __syncthreads();
-    if (t < 5) {
+    // this CTA's partial of moment k = t / 8: eight lanes each sum a strided
+    // eighth of the thread partials, then a three-step xor tree inside the
+    // eight-lane group (a fixed order: every run adds the same operands)
+    if (t < 40) {
+      const int k = t >> 3, sub = t & 7;
       double acc = 0;
-      for (int i = 0; i < G::NT; ++i) acc += red[t * G::NT + i];
-      red[5 * G::NT + t] = acc;  // this CTA's partial
+      for (int i = sub; i < G::NT; i += 8) acc += red[k * G::NT + i];
+      const unsigned grp = t < 32 ? 0xFFFFFFFFu : 0xFFu;  // lanes in this branch
+      acc += __shfl_xor_sync(grp, acc, 4, 8);
+      acc += __shfl_xor_sync(grp, acc, 2, 8);
+      acc += __shfl_xor_sync(grp, acc, 1, 8);
+      if (sub == 0) red[5 * G::NT + k] = acc;
     }
     cluster_sync_all();
     if (t < 5) {
@@ -271,8 +286,7 @@ vhs_prologue_kernel(VhsPrologueArgs a) {
       double re = 0, im = 0;
 #pragma unroll 8
       for (int j = 0; j < N; ++j) {
-        constexpr int off = tw_offset(N);
-        const double2 w = c_tw64[off + (j * k) % N];
+        const double2 w = tws[(j * k) % N];
         const double m = mv[ax * N + j];
         re += m * w.x;
         im += m * w.y;
@@ -1630,7 +1644,9 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
       }
     }
   }
-  for (int b0 = t; b0 < TOT2 && a.nt == 0; b0 += G::NT * UNR) {
+  // FP64 spectra (FP64 mode: one per radial point): UNR pairs per thread,
+  // two radial points' loads in flight per step
+  for (int b0 = t; b0 < TOT2 && a.nt == 0 && a.h_double; b0 += G::NT * UNR) {
     T acc[UNR][2];
 #pragma unroll
     for (int u = 0; u < UNR; ++u) {
@@ -1646,33 +1662,61 @@ vhs_epilogue_kernel(VhsEpilogueArgs a) {
 #pragma unroll 2
     for (int p = 0; p < a.Nrho; ++p) {
       const size_t hb = ((size_t)e * a.Nrho + p) * G::n + off;
-      if (a.h_double) {
-        const double2* Hp = static_cast<const double2*>(a.H) + hb;
+      const double2* Hp = static_cast<const double2*>(a.H) + hb;
 #pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-          const int j2 = b0 + u * G::NT;
-          if (j2 < TOT2) {
-            const double2 h0 = Hp[2 * j2], h1 = Hp[2 * j2 + 1];
-            acc[u][0].x += h0.x; acc[u][0].y += h0.y;
-            acc[u][1].x += h1.x; acc[u][1].y += h1.y;
-          }
-        }
-      } else {
-        const float4* Hp =
-            reinterpret_cast<const float4*>(static_cast<const float2*>(a.H) + hb);
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-          const int j2 = b0 + u * G::NT;
-          if (j2 < TOT2) {
-            const float4 h = Hp[j2];
-            acc[u][0].x += (double)h.x; acc[u][0].y += (double)h.y;
-            acc[u][1].x += (double)h.z; acc[u][1].y += (double)h.w;
-          }
+      for (int u = 0; u < UNR; ++u) {
+        const int j2 = b0 + u * G::NT;
+        if (j2 < TOT2) {
+          const double2 h0 = Hp[2 * j2], h1 = Hp[2 * j2 + 1];
+          acc[u][0].x += h0.x; acc[u][0].y += h0.y;
+          acc[u][1].x += h1.x; acc[u][1].y += h1.y;
         }
       }
     }
 #pragma unroll
     for (int u = 0; u < UNR; ++u) {
+      const int j2 = b0 + u * G::NT;
+      if (j2 < TOT2) {
+        const int si = slab_index<N, C>(2 * j2);
+        A[si] = acc[u][0];
+        A[si + 1] = acc[u][1];
+      }
+    }
+  }
+  // packed FP32 spectra (FP32 mode: one per radial pair, eight at Nrho=16):
+  // UNR32 pairs per thread with eight radial pairs' loads in flight per step,
+  // so that a thread's whole share of a step's loads overlaps
+  constexpr int UNR32 = 4;
+  for (int b0 = t; b0 < TOT2 && a.nt == 0 && !a.h_double; b0 += G::NT * UNR32) {
+    T acc[UNR32][2];
+#pragma unroll
+    for (int u = 0; u < UNR32; ++u) {
+      const int j2 = b0 + u * G::NT;
+      if (a.GM && j2 < TOT2) {
+        acc[u][0] = a.GM[(size_t)e * G::n + off + 2 * j2];
+        acc[u][1] = a.GM[(size_t)e * G::n + off + 2 * j2 + 1];
+      } else {
+        acc[u][0] = T{0, 0};
+        acc[u][1] = T{0, 0};
+      }
+    }
+#pragma unroll 8
+    for (int p = 0; p < a.Nrho; ++p) {
+      const size_t hb = ((size_t)e * a.Nrho + p) * G::n + off;
+      const float4* Hp =
+          reinterpret_cast<const float4*>(static_cast<const float2*>(a.H) + hb);
+#pragma unroll
+      for (int u = 0; u < UNR32; ++u) {
+        const int j2 = b0 + u * G::NT;
+        if (j2 < TOT2) {
+          const float4 h = Hp[j2];
+          acc[u][0].x += (double)h.x; acc[u][0].y += (double)h.y;
+          acc[u][1].x += (double)h.z; acc[u][1].y += (double)h.w;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UNR32; ++u) {
       const int j2 = b0 + u * G::NT;
       if (j2 < TOT2) {
         const int si = slab_index<N, C>(2 * j2);
