@@ -1,8 +1,9 @@
 """Checks of the oracle against properties of the Boltzmann operator itself
 (no reference data): the Bobylev-Krook-Wu (BKW) solution of the
 space-homogeneous equation for Maxwell molecules, the equilibrium of a
-Maxwellian, and the equivalence of the reference's half-sphere rule with the
-full design it is taken from."""
+Maxwellian, the equivalence of the reference's half-sphere rule with the
+full design it is taken from, and the equilibrium and conservation
+properties of a VSS mixture pair."""
 import math
 
 import numpy as np
@@ -104,3 +105,69 @@ def test_oracle_half_sphere_equals_full_design():
     Qh = vhs_gll_fs(_tables(half), half['prefac'], f)
     Qf = vhs_gll_fs(_tables(full), full['prefac'], f)
     assert np.linalg.norm(Qh - Qf) / np.linalg.norm(Qf) < 1e-12
+
+
+def vss_mixture_case(N=24, L=5.0, masses=(1.0, 2.0), M=12, Mpre=192):
+    """The VSS mixture of the uneven batch's problems (alpha 1.4, omega 0.81,
+    masses 1:2, 12-point design, 192-point precompute rule): grid, rules,
+    and Maxwellians n (m/(pi T))^{3/2} exp(-m |c - u|^2 / T)."""
+    from dgfs1d_gpu_b200.quadrature import gauss_jacobi
+    from dgfs1d_gpu_b200.sphericaldesign import get_sphquadrule
+    mr = max(masses)
+    S = min(L * 2.0 / (max(4. * mr / (1. + mr), 2.) + math.sqrt(1. + mr) + 1.),
+            L * 2.0 / (max(4. / (1. + mr), 2.) + math.sqrt(1. + 1.0 / mr) + 1.0))
+    z, w = gauss_jacobi(N // 2)
+    c0 = np.linspace(-L + L / N, L - L / N, N)
+    g = np.meshgrid(c0, c0, c0, indexing='ij')
+    cv = np.stack([x.ravel() for x in g])
+
+    def maxwellian(n, m, u, T):
+        d2 = np.sum((cv - np.asarray(u, dtype=float)[:, None]) ** 2, axis=0)
+        return n * (m / (np.pi * T)) ** 1.5 * np.exp(-m * d2 / T)
+    return dict(N=N, L=L, qz=S * (1 + z), qw=S * w, masses=list(masses),
+                sz=get_sphquadrule('symmetric', 'womersley', npts=M).pts,
+                sw=4 * np.pi / M,
+                szpre=get_sphquadrule('symmetric', 'womersley', npts=Mpre).pts,
+                omega=0.81, alpha=1.4, cv=cv, cw=(2 * L / N) ** 3,
+                maxwellian=maxwellian)
+
+
+def mixture_checks(Q01, Q10, E01, E10, case):
+    """Equilibrium (E: both species at one velocity and temperature) and the
+    exchange of mass, momentum and energy (Q: off equilibrium) of a pair."""
+    m0, m1 = case['masses']
+    cv = case['cv']
+    c2 = np.sum(cv ** 2, axis=0)
+    eq = (np.abs(E01).max() / np.abs(Q01).max(), np.abs(E10).max() / np.abs(Q10).max())
+    mass = max(abs(np.sum(Q01)), abs(np.sum(Q10))) / np.sum(np.abs(Q01))
+    mom = (np.abs(m0 * cv @ Q01 + m1 * cv @ Q10).max()
+           / (m0 * np.abs(cv) @ np.abs(Q01) + m1 * np.abs(cv) @ np.abs(Q10)).max())
+    en = (abs(m0 * c2 @ Q01 + m1 * c2 @ Q10)
+          / (m0 * c2 @ np.abs(Q01) + m1 * c2 @ np.abs(Q10)))
+    return eq, mass, mom, en
+
+
+def test_oracle_vss_mixture_equilibrium_and_exchange():
+    """24^3 grid, masses 1:2: the cross-collision operators of two
+    Maxwellians at one velocity and temperature vanish (1e-4 and 2e-3 of
+    their size off equilibrium), and off equilibrium the pair conserves each
+    species' mass and exchanges momentum and energy with zero sum (all to
+    about 1e-5 of their scales)."""
+    from oracle.collision import VSSTables, vss_fs
+    c = vss_mixture_case()
+    m = c['masses']
+    tabs = {}
+
+    def Q(p, q, fp, fq):
+        if (p, q) not in tabs:
+            tabs[(p, q)] = VSSTables(c['N'], c['L'], c['qz'], c['qw'], c['sz'],
+                                     c['sw'], c['szpre'], 2 * (1 - c['omega']),
+                                     c['alpha'] - 1, m[q] / (m[p] + m[q]))
+        return vss_fs(tabs[(p, q)], 0.1, m[p], m[q], fp, fq)
+    mx = c['maxwellian']
+    e0, e1 = mx(0.6, m[0], (0.1, 0, 0), 1.0), mx(0.4, m[1], (0.1, 0, 0), 1.0)
+    g0, g1 = mx(0.6, m[0], (0.2, 0, 0), 1.0), mx(0.4, m[1], (-0.1, 0.05, 0), 1.3)
+    eq, mass, mom, en = mixture_checks(Q(0, 1, g0, g1), Q(1, 0, g1, g0),
+                                       Q(0, 1, e0, e1), Q(1, 0, e1, e0), c)
+    assert eq[0] < 5e-4 and eq[1] < 5e-3, eq
+    assert mass < 1e-4 and mom < 1e-4 and en < 1e-4, (mass, mom, en)

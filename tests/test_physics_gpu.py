@@ -1,14 +1,16 @@
 """The CUDA path against properties of the Boltzmann operator and of the DG
 scheme (no reference data): the BKW solution of the space-homogeneous
 equation for Maxwell molecules, the equilibrium of a Maxwellian, the
-half-sphere rule against its full design, and zero net mass flux through
-diffuse walls."""
+half-sphere rule against its full design, the equilibrium and conservation
+properties of a VSS mixture pair, and zero net mass flux through diffuse
+walls."""
 import numpy as np
 import pytest
 import torch
 
 from dgfs1d_gpu_b200.workloads import vhs_mesh_params
-from tests.test_oracle_physics import _grid, _tables, bkw_run, loss_frequency
+from tests.test_oracle_physics import (_grid, _tables, bkw_run, loss_frequency,
+                                      mixture_checks, vss_mixture_case)
 
 pytestmark = pytest.mark.gpu
 
@@ -120,3 +122,36 @@ def test_diffuse_walls_carry_no_net_mass():
     rate = float(np.sum(wq * r.sum(axis=2)))
     scale = float(np.sum(wq * np.abs(r).sum(axis=2)))
     assert abs(rate) < 1e-12 * scale, (rate, scale)
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'fp32'])
+def test_vss_mixture_equilibrium_and_exchange(precision):
+    """The native VSS operator on the oracle's mixture case (24^3, masses
+    1:2): cross-collisions of Maxwellians at one velocity and temperature
+    vanish, and off equilibrium each species' mass is conserved and the
+    pair's momentum and energy exchanges cancel, to the grid's accuracy."""
+    from dgfs1d_gpu_b200 import build
+    build.build()
+    from dgfs1d_gpu_b200.collision import VSSOperator
+    c = vss_mixture_case()
+    m = c['masses']
+    full = np.full((2, 2), 1.0)
+    op = VSSOperator(c['N'], c['L'], c['qz'], c['qw'], c['sz'], c['sw'],
+                     c['szpre'], m, 2 * (1 - c['omega']) * full,
+                     (c['alpha'] - 1) * full, 0.1 * full, max_evals=1,
+                     precision=precision)
+    mx = c['maxwellian']
+    out = {}
+    for tag, (f0, f1) in (('E', (mx(0.6, m[0], (0.1, 0, 0), 1.0),
+                                 mx(0.4, m[1], (0.1, 0, 0), 1.0))),
+                          ('Q', (mx(0.6, m[0], (0.2, 0, 0), 1.0),
+                                 mx(0.4, m[1], (-0.1, 0.05, 0), 1.3)))):
+        fd = [torch.tensor(x[None, :], device='cuda') for x in (f0, f1)]
+        for p, q in ((0, 1), (1, 0)):
+            Q = torch.zeros_like(fd[p])
+            op.eval(p, q, fd[p], fd[q], Q)
+            out[tag + str(p) + str(q)] = Q.cpu().numpy()[0]
+    eq, mass, mom, en = mixture_checks(out['Q01'], out['Q10'], out['E01'],
+                                       out['E10'], c)
+    assert eq[0] < 5e-4 and eq[1] < 5e-3, eq
+    assert mass < 1e-4 and mom < 1e-4 and en < 1e-4, (mass, mom, en)
