@@ -250,6 +250,28 @@ def check(rc):
     return rc
 
 
+_deferred = []
+
+
+def release(destroy, handle):
+    """Destroy a native handle (``destroy`` is its dgfs_*_destroy).
+
+    Destroying frees device memory, which a CUDA stream capture does not
+    allow: a free issued while a graph is being captured ends that capture
+    with an error.  Python may collect an unreachable handle at any moment,
+    in the middle of a capture too, so a handle released while this thread's
+    current stream is capturing waits in a queue that the next release outside
+    a capture empties first."""
+    import torch
+    if torch.cuda.is_available() and torch.cuda.is_current_stream_capturing():
+        _deferred.append((destroy, handle))
+        return
+    while _deferred:
+        d, h = _deferred.pop()
+        d(h)
+    destroy(handle)
+
+
 def exported_symbols():
     """Names of every entry point the binding declares."""
     return [s[0] for s in _SIGNATURES]

@@ -182,7 +182,7 @@ class VHSOperator:
 
     def close(self):
         if getattr(self, '_h', None):
-            nat.lib().dgfs_vhs_destroy(self._h)
+            nat.release(nat.lib().dgfs_vhs_destroy, self._h)
             self._h = None
 
     def __del__(self):
@@ -293,7 +293,7 @@ class VSSOperator:
 
     def close(self):
         if getattr(self, '_h', None):
-            nat.lib().dgfs_vss_destroy(self._h)
+            nat.release(nat.lib().dgfs_vss_destroy, self._h)
             self._h = None
 
     def __del__(self):

@@ -143,7 +143,7 @@ class DGOperator:
 
     def close(self):
         if getattr(self, '_h', None):
-            nat.lib().dgfs_dg_destroy(self._h)
+            nat.release(nat.lib().dgfs_dg_destroy, self._h)
             self._h = None
 
     def __del__(self):

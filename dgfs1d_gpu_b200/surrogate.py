@@ -175,7 +175,7 @@ class FNOSurrogate:
 
     def close(self):
         if getattr(self, '_h', None):
-            nat.lib().dgfs_fno_destroy(self._h)
+            nat.release(nat.lib().dgfs_fno_destroy, self._h)
             self._h = None
 
     def __del__(self):
