@@ -639,7 +639,7 @@ def main():
     # the per-problem graph; error against the same problems in FP64
     from dgfs1d_gpu_b200.batch import StageGraph
     from dgfs1d_gpu_b200.workloads_c3 import build_c3
-    groups = build_c3(precision='fp32', merged=True)
+    groups = build_c3(precision='fp32', merged=True, autotune=True)
     members = [m for g in groups for m in g['members']]
     b_evals = sum(g['nevals'] for g in groups)
     b_steps = max(3, args.steps // 4)
@@ -676,6 +676,8 @@ def main():
     batch = {'value': b_evals * world / (ms_graph * 1e-3), 'unit': UNIT,
              'ms_per_stage': ms_graph, 'graph_launches_per_stage': 1,
              'groups': [g['name'] for g in groups],
+             'autotuned_variants': {g['name']: g.get('variant') for g in groups
+                                    if 'variant' in g},
              'serial_stream_ms_per_stage': ms_serial,
              'per_problem_graph_ms_per_stage': ms_graph1,
              'speedup_vs_serial_stream': ms_serial / ms_graph,

@@ -147,22 +147,27 @@ class VHSOperator:
         nat.check(nat.lib().dgfs_vhs_set_variant(self._h, int(cluster)))
         self.variant = int(cluster)
 
-    def autotune(self, f, Q, reps=3, stream=None):
-        """Time every terms-kernel variant on (f, Q) and keep the fastest.
+    def autotune(self, f=None, Q=None, reps=3, stream=None, call=None):
+        """Time every terms-kernel variant and keep the fastest: on the
+        evaluation of (f, Q), or on ``call()`` (any enqueue of this
+        operator's evaluations, e.g. a merged multi-problem call).
 
-        Returns {cluster: ms per evaluation call}.  Q is overwritten.
+        Returns {variant: ms per call}.  Q (or call's outputs) is overwritten.
         """
         if self.precision != 'fp32':
             return {}
+        if call is None:
+            def call():
+                self.eval(f, Q, stream=stream)
         times = {}
         for c in self.variants():
             self.set_variant(c)
-            self.eval(f, Q, stream=stream)           # warm-up
+            call()                                   # warm-up
             s = torch.cuda.Event(enable_timing=True)
             e = torch.cuda.Event(enable_timing=True)
             s.record()
             for _ in range(reps):
-                self.eval(f, Q, stream=stream)
+                call()
             e.record()
             e.synchronize()
             times[c] = s.elapsed_time(e) / reps

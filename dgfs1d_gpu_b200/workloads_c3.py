@@ -22,19 +22,22 @@ VHS_PROBLEMS = [(16, 12, 6), (24, 24, 12), (32, 40, 12),
 
 
 def build_c3(precision='fp32', device='cuda', seed=20261203, project=True,
-             merged=False):
+             merged=False, autotune=False):
     """The eight problems as dicts (name, op, f, Q, nevals, params, fn).
 
     merged=True instead returns one dict per group of problems that share
     an operator -- the VHS problems of equal N (equal grids and rules here)
     and the two mixtures -- with one operator per group, ``fn`` evaluating
     every member's points in one call per kernel, and the members' dicts
-    (without ops) under ``members``."""
+    (without ops) under ``members``.  ``autotune`` (merged only) lets the
+    project's autotuner pick each VHS group's terms-kernel variant (tile
+    shape, radix split, staging) on the group's own merged call; the
+    timings and the choice are under ``variant_ms`` and ``variant``."""
     if merged:
         if precision != 'fp32':
             raise ValueError('merged groups need the FP32 mode (the VSS array '
                              'lists are FP32 only)')
-        return _build_merged(precision, device, seed, project)
+        return _build_merged(precision, device, seed, project, autotune)
     problems = []
     for i, (N, pts, M) in enumerate(VHS_PROBLEMS):
         full = M == 12
@@ -96,7 +99,7 @@ def build_c3(precision='fp32', device='cuda', seed=20261203, project=True,
     return problems
 
 
-def _build_merged(precision, device, seed, project):
+def _build_merged(precision, device, seed, project, autotune=False):
     from .batch import merged_vhs, merged_vss
     single = build_c3(precision, device, seed, project)
     groups = []
@@ -114,8 +117,12 @@ def _build_merged(precision, device, seed, project):
             for p in members:
                 p['Q'].zero_()
             call()
-        groups.append(dict(name=f'vhs-N{N}-x{len(members)}', op=op, fn=fn,
-                           nevals=tot, members=members))
+        g = dict(name=f'vhs-N{N}-x{len(members)}', op=op, fn=fn,
+                 nevals=tot, members=members)
+        if autotune:
+            g['variant_ms'] = op.autotune(call=fn)
+            g['variant'] = op.variant
+        groups.append(g)
     vss = [p for p in single if p['name'].startswith('vss')]
     prm = vss[0]['params']
     tot = sum(p['nevals'] // 4 for p in vss)
